@@ -1,0 +1,303 @@
+"""Test infrastructure: the CPU oracle for the F3D objective-and-gradient path.
+
+Two CPU implementations sit here, both used only as checkers (by ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``), never by the product:
+
+* ``restated`` -- ``liboracle.so`` built from ``nrb_oracle.c``, a plain-C restatement of the
+  reference algorithm, each function citing the reference file:line it follows;
+* ``ref``      -- ``_ref/libnrref.so``, the reference NiftyReg CPU library itself, compiled from
+  its own sources by ``oracle/Makefile`` (target ``ref``) plus the adapter ``ref_shim.cpp``.
+
+Parity of the restatement is pinned against ``ref`` and against the reference's own
+known-answer tests (see ``tests/test_oracle_pins.py``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATED_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libnrref.so")
+
+_fp = ctypes.POINTER(ctypes.c_float)
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def _f(a):
+    return a.ctypes.data_as(_fp) if a is not None else None
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
+
+
+def _i3(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.int32))
+
+
+def _f3(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.float32))
+
+
+def _m(v):
+    return np.ascontiguousarray(np.asarray(v, dtype=np.float32).reshape(16))
+
+
+def build_restated():
+    if not os.path.exists(RESTATED_SO):
+        subprocess.check_call(["make", "-C", HERE, "liboracle.so"], stdout=subprocess.DEVNULL)
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+# ----------------------------------------------------------------------------------------------
+# the reference library (oracle/_ref)
+# ----------------------------------------------------------------------------------------------
+class Ref:
+    """ctypes view of oracle/_ref/libnrref.so (the reference CPU implementation)."""
+
+    def __init__(self, path: str = REF_SO):
+        self.lib = ctypes.CDLL(path)
+        self.lib.ref_nmi_value.restype = ctypes.c_double
+        self.lib.ref_be_value.restype = ctypes.c_double
+
+    def set_threads(self, n: int) -> int:
+        return self.lib.ref_set_threads(int(n))
+
+    def create_control_point_grid(self, rdim, rpix, rxyz, spacing):
+        cdim = np.zeros(3, np.int32)
+        cpix = np.zeros(3, np.float32)
+        cxyz = np.zeros(16, np.float32)
+        self.lib.ref_create_control_point_grid(_i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)),
+                                               _f(_f3(spacing)), _i(cdim), _f(cpix), _f(cxyz),
+                                               None, ctypes.c_size_t(0))
+        cpp = np.zeros(3 * int(np.prod(cdim)), np.float32)
+        self.lib.ref_create_control_point_grid(_i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)),
+                                               _f(_f3(spacing)), _i(cdim), _f(cpix), _f(cxyz),
+                                               _f(cpp), ctypes.c_size_t(cpp.size))
+        return cpp, cdim, cpix, cxyz.reshape(4, 4)
+
+    def deformation_field(self, cpp, cdim, cpix, cxyz, rdim, rpix, rxyz, mask=None):
+        out = np.zeros(3 * int(np.prod(rdim)), np.float32)
+        self.lib.ref_deformation_field(_f(_f3(cpp)), _i(_i3(cdim)), _f(_f3(cpix)), _f(_m(cxyz)),
+                                       _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)),
+                                       _i(_i3(mask)) if mask is not None else None, _f(out))
+        return out
+
+    def resample(self, flo, fdim, fpix, fxyz, dfield, rdim, rpix, rxyz, mask=None, pad=np.nan,
+                 warped_init=None):
+        w = np.zeros(int(np.prod(rdim)), np.float32) if warped_init is None else _f3(warped_init).copy()
+        self.lib.ref_resample(_f(_f3(flo)), _i(_i3(fdim)), _f(_f3(fpix)), _f(_m(fxyz)),
+                              _f(_f3(dfield)), _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)),
+                              _i(_i3(mask)) if mask is not None else None, ctypes.c_float(pad), _f(w))
+        return w
+
+    def image_gradient(self, flo, fdim, fpix, fxyz, dfield, rdim, rpix, rxyz, mask=None, pad=np.nan):
+        g = np.zeros(3 * int(np.prod(rdim)), np.float32)
+        self.lib.ref_image_gradient(_f(_f3(flo)), _i(_i3(fdim)), _f(_f3(fpix)), _f(_m(fxyz)),
+                                    _f(_f3(dfield)), _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)),
+                                    _i(_i3(mask)) if mask is not None else None,
+                                    ctypes.c_float(pad), _f(g))
+        return g
+
+    def intensity_rescale(self, img, dim, new_min, new_max):
+        x = _f3(img).copy()
+        self.lib.ref_intensity_rescale(_f(x), _i(_i3(dim)), ctypes.c_float(new_min), ctypes.c_float(new_max))
+        return x
+
+    def nmi_value(self, ref, war, dim, ref_bins, flo_bins, mask=None, approx=True):
+        total = ref_bins * flo_bins + ref_bins + flo_bins
+        pro = np.zeros(total, np.float64)
+        log = np.zeros(total, np.float64)
+        ent = np.zeros(4, np.float64)
+        v = self.lib.ref_nmi_value(_f(_f3(ref)), _f(_f3(war)), _i(_i3(dim)),
+                                   _i(_i3(mask)) if mask is not None else None,
+                                   int(ref_bins), int(flo_bins), int(bool(approx)),
+                                   _d(pro), _d(log), _d(ent))
+        return v, pro, log, ent
+
+    def nmi_voxel_gradient(self, ref, war, war_grad, dim, ref_bins, flo_bins, weight=1.0,
+                           mask=None, vgrad_init=None):
+        n = int(np.prod(dim))
+        vg = np.zeros(3 * n, np.float32) if vgrad_init is None else _f3(vgrad_init).copy()
+        self.lib.ref_nmi_voxel_gradient(_f(_f3(ref)), _f(_f3(war)), _f(_f3(war_grad)), _i(_i3(dim)),
+                                        _i(_i3(mask)) if mask is not None else None,
+                                        int(ref_bins), int(flo_bins), ctypes.c_double(weight), _f(vg))
+        return vg
+
+    def convolve_to_nodes(self, vgrad, rdim, rpix, rxyz, fdim, fpix, fxyz, cdim, cpix, cxyz, weight):
+        vg = _f3(vgrad).copy()
+        node = np.zeros(3 * int(np.prod(cdim)), np.float32)
+        self.lib.ref_convolve_to_nodes(_f(vg), _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)),
+                                       _i(_i3(fdim)), _f(_f3(fpix)), _f(_m(fxyz)),
+                                       _i(_i3(cdim)), _f(_f3(cpix)), _f(_m(cxyz)),
+                                       ctypes.c_float(weight), _f(node))
+        return vg, node
+
+    def kernel_convolution_cubic(self, img, nvol, dim, pix, spacing, axis):
+        x = _f3(img).copy()
+        self.lib.ref_kernel_convolution_cubic(_f(x), int(nvol), _i(_i3(dim)), _f(_f3(pix)),
+                                              ctypes.c_float(spacing), int(axis))
+        return x
+
+    def be_value(self, cpp, cdim, cpix, cxyz):
+        return self.lib.ref_be_value(_f(_f3(cpp)), _i(_i3(cdim)), _f(_f3(cpix)), _f(_m(cxyz)))
+
+    def be_gradient(self, cpp, cdim, cpix, cxyz, weight, grad_init=None):
+        g = np.zeros(3 * int(np.prod(cdim)), np.float32) if grad_init is None else _f3(grad_init).copy()
+        self.lib.ref_be_gradient(_f(_f3(cpp)), _i(_i3(cdim)), _f(_f3(cpix)), _f(_m(cxyz)),
+                                 ctypes.c_float(weight), _f(g))
+        return g
+
+    def refine_grid(self, cpp, cdim, cpix, cxyz, rdim, rpix, rxyz):
+        cap = 3 * int(np.prod([(int(c) - 3) * 2 + 8 for c in cdim]))
+        out = np.zeros(cap, np.float32)
+        cdo = np.zeros(3, np.int32)
+        cpo = np.zeros(3, np.float32)
+        cxo = np.zeros(16, np.float32)
+        rc = self.lib.ref_refine_grid(_f(_f3(cpp)), _i(_i3(cdim)), _f(_f3(cpix)), _f(_m(cxyz)),
+                                      _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)),
+                                      _i(cdo), _f(cpo), _f(cxo), _f(out), ctypes.c_size_t(cap))
+        if rc != 0:
+            raise RuntimeError("ref_refine_grid: capacity")
+        return out[:3 * int(np.prod(cdo))].copy(), cdo, cpo, cxo.reshape(4, 4)
+
+    def f3d_register(self, ref, flo, dim, pix, xyz, levels, maxit, be, le, bins, spacing,
+                     verbose=False):
+        params = np.array([levels, maxit, be, le, bins, spacing, 1 if verbose else 0], np.float64)
+        cap = 3 * int(np.prod([int(np.ceil(n * p / abs(spacing * (p if spacing < 0 else 1))) + 4)
+                               for n, p in zip(dim, pix)])) + 64
+        cpp = np.zeros(cap, np.float32)
+        cdim = np.zeros(3, np.int32)
+        stats = np.zeros(5, np.float64)
+        rc = self.lib.ref_f3d_register(_f(_f3(ref)), _f(_f3(flo)), _i(_i3(dim)), _f(_f3(pix)),
+                                       _f(_m(xyz)), _d(params), _i(cdim), _f(cpp),
+                                       ctypes.c_size_t(cap), _d(stats))
+        if rc != 0:
+            raise RuntimeError("ref_f3d_register failed")
+        return cpp[:3 * int(np.prod(cdim))].copy(), cdim, stats
+
+
+# ----------------------------------------------------------------------------------------------
+# the C restatement (oracle/liboracle.so)
+# ----------------------------------------------------------------------------------------------
+class Restated:
+    """ctypes view of oracle/liboracle.so (the plain-C restatement)."""
+
+    def __init__(self, path: str = RESTATED_SO):
+        build_restated()
+        self.lib = ctypes.CDLL(path)
+        for name in ("orc_nmi_value", "orc_be_value", "orc_max_length"):
+            getattr(self.lib, name).restype = ctypes.c_double
+
+    def deformation_field(self, cpp, cdim, cpix, rdim, rpix, mask=None):
+        out = np.zeros(3 * int(np.prod(rdim)), np.float32)
+        rc = self.lib.orc_deformation_field(_f(_f3(cpp)), _i(_i3(cdim)), _f(_f3(cpix)), _i(_i3(rdim)),
+                                            _f(_f3(rpix)), _i(_i3(mask)) if mask is not None else None,
+                                            _f(out))
+        if rc != 0:
+            raise ValueError("control-point grid does not cover the reference image")
+        return out
+
+    def resample(self, flo, fdim, flo_ijk, dfield, rdim, mask=None, pad=np.nan, warped_init=None):
+        w = np.zeros(int(np.prod(rdim)), np.float32) if warped_init is None else _f3(warped_init).copy()
+        self.lib.orc_resample_linear(_f(_f3(flo)), _i(_i3(fdim)), _f(_m(flo_ijk)), _f(_f3(dfield)),
+                                     _i(_i3(rdim)), _i(_i3(mask)) if mask is not None else None,
+                                     ctypes.c_float(pad), _f(w))
+        return w
+
+    def image_gradient(self, flo, fdim, flo_ijk, dfield, rdim, mask=None, pad=np.nan):
+        g = np.zeros(3 * int(np.prod(rdim)), np.float32)
+        self.lib.orc_image_gradient_linear(_f(_f3(flo)), _i(_i3(fdim)), _f(_m(flo_ijk)),
+                                           _f(_f3(dfield)), _i(_i3(rdim)),
+                                           _i(_i3(mask)) if mask is not None else None,
+                                           ctypes.c_float(pad), _f(g))
+        return g
+
+    def intensity_rescale(self, img, new_min, new_max):
+        x = _f3(img).copy()
+        self.lib.orc_intensity_rescale(_f(x), ctypes.c_size_t(x.size), ctypes.c_float(new_min),
+                                       ctypes.c_float(new_max))
+        return x
+
+    def nmi_value(self, ref, war, ref_bins, flo_bins, mask=None):
+        total = ref_bins * flo_bins + ref_bins + flo_bins
+        pro = np.zeros(total, np.float64)
+        log = np.zeros(total, np.float64)
+        ent = np.zeros(4, np.float64)
+        r = _f3(ref)
+        v = self.lib.orc_nmi_value(_f(r), _f(_f3(war)), ctypes.c_size_t(r.size),
+                                   _i(_i3(mask)) if mask is not None else None, int(ref_bins),
+                                   int(flo_bins), _d(pro), _d(log), _d(ent))
+        return v, pro, log, ent
+
+    def nmi_voxel_gradient(self, ref, war, war_grad, ref_bins, flo_bins, logh, ent, weight=1.0,
+                           mask=None, vgrad_init=None):
+        r = _f3(ref)
+        vg = np.zeros(3 * r.size, np.float32) if vgrad_init is None else _f3(vgrad_init).copy()
+        self.lib.orc_nmi_voxel_gradient(_f(r), _f(_f3(war)), _f(_f3(war_grad)), ctypes.c_size_t(r.size),
+                                        _i(_i3(mask)) if mask is not None else None, int(ref_bins),
+                                        int(flo_bins), _d(np.ascontiguousarray(logh, np.float64)),
+                                        _d(np.ascontiguousarray(ent, np.float64)),
+                                        ctypes.c_double(weight), _f(vg))
+        return vg
+
+    def kernel_convolution_cubic(self, img, nvol, dim, pix, spacing, axis, mask=None):
+        x = _f3(img).copy()
+        self.lib.orc_kernel_convolution_cubic(_f(x), int(nvol), _i(_i3(dim)), _f(_f3(pix)),
+                                              ctypes.c_float(spacing), int(axis),
+                                              _i(_i3(mask)) if mask is not None else None)
+        return x
+
+    def convolve_to_nodes(self, vgrad, rdim, rpix, ref_ijk, cdim, cpix, grid_xyz, flo_ijk, weight):
+        vg = _f3(vgrad).copy()
+        node = np.zeros(3 * int(np.prod(cdim)), np.float32)
+        self.lib.orc_convolve_to_nodes(_f(vg), _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(ref_ijk)),
+                                       _i(_i3(cdim)), _f(_f3(cpix)), _f(_m(grid_xyz)),
+                                       _f(_m(flo_ijk)), ctypes.c_float(weight), _f(node))
+        return vg, node
+
+    def voxel_to_node(self, voxel, rdim, rpix, ref_ijk, cdim, grid_xyz, reorient, weight):
+        node = np.zeros(3 * int(np.prod(cdim)), np.float32)
+        self.lib.orc_voxel_to_node(_f(node), _i(_i3(cdim)), _f(_m(grid_xyz)), _f(_f3(voxel)),
+                                   _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(ref_ijk)), _f(_m(reorient)),
+                                   ctypes.c_float(weight), 0)
+        return node
+
+    def be_value(self, cpp, cdim):
+        return self.lib.orc_be_value(_f(_f3(cpp)), _i(_i3(cdim)))
+
+    def be_gradient(self, cpp, cdim, grid_xyz, weight, grad_init=None):
+        g = np.zeros(3 * int(np.prod(cdim)), np.float32) if grad_init is None else _f3(grad_init).copy()
+        self.lib.orc_be_gradient(_f(_f3(cpp)), _i(_i3(cdim)), _f(_m(grid_xyz)), ctypes.c_float(weight), _f(g))
+        return g
+
+    def max_length(self, grad, nnode):
+        return self.lib.orc_max_length(_f(_f3(grad)), ctypes.c_size_t(nnode), 1, 1, 1)
+
+    def normalise_gradient(self, grad, nnode, maxlen):
+        g = _f3(grad).copy()
+        self.lib.orc_normalise_gradient(_f(g), ctypes.c_size_t(nnode), ctypes.c_double(maxlen), 1, 1, 1)
+        return g
+
+    def update_control_points(self, best, grad, scale):
+        cur = np.zeros_like(_f3(best))
+        self.lib.orc_update_control_points(_f(cur), _f(_f3(best)), _f(_f3(grad)), ctypes.c_float(scale),
+                                           ctypes.c_size_t(cur.size))
+        return cur
+
+    def cg_update(self, grad, g1, g2, first_call):
+        grad, g1, g2 = _f3(grad).copy(), _f3(g1).copy(), _f3(g2).copy()
+        self.lib.orc_cg_update(_f(grad), _f(g1), _f(g2), ctypes.c_size_t(grad.size), int(bool(first_call)))
+        return grad, g1, g2
