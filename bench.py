@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""F3D registrations/s on the brain-MR-sized workload.
+
+Workload: one plain single-pair F3D registration of a 182x218x182 float32, 1 mm 3-class
+phantom pair (floating = reference warped by a seeded 5 mm FFD with N(0, 3 mm) control
+displacements), 3 pyramid levels, 300 counted iterations at the finest level (the reference's
+budget doubling per coarser level: 300/600/1200), NMI with 64 bins, bending energy 0.005, 5 mm
+control spacing, linear interpolation, NaN padding. A "step" is one whole registration.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun every rank registers its own pair (replicas: registrations are independent) and
+rank 0 prints one JSON line with the whole-job rate and the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "F3D registrations/s & p99 latency, batched/served vs plain GPU, |ΔNMI|≤1e-4"
+SHAPE = (182, 218, 182)        # (nz, ny, nx)
+LEVELS, MAXIT, BE, BINS, SPACING = 3, 300, 0.005, 64, -5.0
+WORKLOAD = ("plain single-pair F3D, 182x218x182 float32 1 mm brain-MR-like 3-class phantom, "
+            "3 levels, 300 counted iterations at the finest level (600/1200 coarser), NMI 64 bins, "
+            "BE 0.005, 5 mm control spacing")
+L2_FLUSH_BYTES = 256 << 20
+REF_SAMPLE_MAXIT = 30          # reference arm: 1/10 of every level's iteration budget
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--kernel", choices=["objective", "gradient"], default=None,
+                    help="profiling mode: run only `--steps` fused evaluations at the finest level "
+                         "of the workload (for ncu captures); prints per-launch device times")
+    return ap.parse_args()
+
+
+def run_kernel_only(args):
+    """A short, deterministic launch sequence of one fused evaluation on the finest level of the
+    workload (rescaled images, 5 mm grid with N(0, 3 mm) displacements)."""
+    import torch
+    import niftyreg_b200 as nrb
+    from niftyreg_b200 import phantom
+
+    torch.cuda.set_device(0)
+    nrb.build()
+    pair = phantom.brain_pair(SHAPE, seed=args.seed)
+    nz, ny, nx = SHAPE
+    dim, pix = (nx, ny, nz), (1.0, 1.0, 1.0)
+    cdim, cpix, cxyz = nrb.control_grid_header(dim, pix, (5.0, 5.0, 5.0))
+    rng = np.random.default_rng(args.seed)
+    cx, cy, cz = cdim
+    zz, yy, xx = np.meshgrid(np.arange(cz), np.arange(cy), np.arange(cx), indexing="ij")
+    ident = np.concatenate([(5.0 * v - 5.0).ravel() for v in (xx, yy, zz)]).astype(np.float32)
+    cpp = ident + rng.normal(0, 3.0, ident.size).astype(np.float32)
+    g = nrb.make_geometry(dim, pix, nrb.identity_header(pix), dim, pix, nrb.identity_header(pix), cdim, cpix, cxyz)
+    ref = torch.from_numpy(pair.reference.ravel().copy()).cuda()
+    flo = torch.from_numpy(pair.floating.ravel().copy()).cuda()
+    n = nx * ny * nz
+    nrb.intensity_rescale(ref, n, 2.0, BINS + 1.0)
+    nrb.intensity_rescale(flo, n, 2.0, BINS + 1.0)
+    cppd = torch.from_numpy(cpp).cuda()
+    ws, nmi = nrb.Workspace(g), nrb.Nmi(BINS + 4, BINS + 4)
+    vg = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    node = torch.empty(ident.size, dtype=torch.float32, device="cuda")
+    nrb.timing_enable(True)
+    for _ in range(args.steps):
+        if args.kernel == "objective":
+            nrb.f3d_objective(ws, nmi, ref, flo, cppd, 1 - BE, BE)
+        else:
+            nrb.f3d_gradient(ws, nmi, ref, flo, cppd, vg, node, 1 - BE, BE)
+    torch.cuda.synchronize()
+    out = {k: nrb.timing_read(k) for k in ("objective", "gradient", "finalize", "conv", "be_value", "be_gradient")}
+    nrb.timing_enable(False)
+    print(json.dumps({"mode": f"kernel-only {args.kernel}", "voxels": n, "nodes": int(np.prod(cdim)),
+                      "timing": {k: {"launches": v[0], "avg_us": (v[1] / v[0] * 1e3) if v[0] else None,
+                                     "GBps": (v[2] / (v[1] / 1e3) / 1e9) if v[1] else None}
+                                 for k, v in out.items()}}))
+    return 0
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def traffic_per_launch(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/*.md line
+    'dram_bytes_per_voxel_<kernel>: X', bytes per reference voxel of one launch), or None."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for name in sorted(os.listdir(d)):
+        if not name.endswith(".md"):
+            continue
+        for line in open(os.path.join(d, name)):
+            if line.strip().startswith(f"dram_bytes_per_voxel_{kernel}:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+def reference_sample(pair, threads):
+    """The reference NiftyReg CPU registration (oracle/_ref, all host threads) on a bounded sample
+    of the workload: every level runs 1/10 of its counted-iteration budget; the registration time
+    is extrapolated per level by time per counted iteration x that level's full budget."""
+    import oracle
+    if not oracle.ref_available():
+        return None
+    R = oracle.Ref()
+    cores = R.set_threads(threads)
+    eye = np.eye(4, dtype=np.float32)
+    t0 = time.perf_counter()
+    _, _, st = R.f3d_register(pair.reference.ravel(), pair.floating.ravel(), pair.dim, pair.pixdim, eye, LEVELS,
+                              REF_SAMPLE_MAXIT, BE, 0.0, BINS, SPACING)
+    wall = time.perf_counter() - t0
+    est = 0.0
+    for level in range(LEVELS):
+        n_obj, n_grad, sec = st[5 + 3 * level: 8 + 3 * level]
+        counted = n_obj - 1 + n_grad  # the initial objective of a level is not counted
+        budget = MAXIT * 2 ** (LEVELS - 1 - level)
+        est += sec / max(counted, 1) * budget
+    return {"value": 1.0 / est, "unit": "registrations/s", "cores": int(cores), "kind": "reference",
+            "sample": (f"reference reg_f3d<float> (oracle/_ref, -O3 -msse3 OpenMP) on the same pair with "
+                       f"{REF_SAMPLE_MAXIT}/{2 * REF_SAMPLE_MAXIT}/{4 * REF_SAMPLE_MAXIT} counted iterations "
+                       f"(1/10 budget, {wall:.1f} s); time per counted iteration per level x full budget "
+                       f"{MAXIT}/{2 * MAXIT}/{4 * MAXIT} = {est:.1f} s per registration"),
+            "sample_seconds": wall, "estimated_seconds_per_registration": est}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from niftyreg_b200 import phantom
+    import oracle
+    pair = phantom.brain_pair(SHAPE, seed=args.seed)
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libnrref.so not built (needs the "
+                          "reference sources: make -C oracle ref)"}))
+        return 0
+    threads = os.cpu_count() or 1
+    vals = []
+    last = None
+    for i in range(args.warmup + args.steps):
+        s = reference_sample(pair, threads)
+        if i >= args.warmup:
+            vals.append(s["estimated_seconds_per_registration"])
+        last = s
+    sec = float(np.mean(vals))
+    v = 1.0 / sec
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "registrations/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "replicas", "host_threads": threads},
+            "cpu_baseline": {"value": v, "unit": "registrations/s", "cores": last["cores"], "kind": "reference",
+                             "sample": last["sample"]},
+            "e2e": {"value": v, "unit": "registrations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_b200(args):
+    import torch
+    import niftyreg_b200 as nrb
+    from niftyreg_b200 import phantom
+
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1 and not torch.distributed.is_initialized():
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=dev)
+    nrb.build()
+    nrb.lib()
+    pair = phantom.brain_pair(SHAPE, seed=args.seed + rank)
+    nz, ny, nx = SHAPE
+    dim, pix = (nx, ny, nz), pair.pixdim
+    ref_h = torch.from_numpy(pair.reference.ravel().copy()).pin_memory()
+    flo_h = torch.from_numpy(pair.floating.ravel().copy()).pin_memory()
+    ref_d, flo_d = ref_h.to(dev), flo_h.to(dev)
+    params = nrb.default_params(levels=LEVELS, max_iterations=MAXIT, bending_energy=BE, spacing=(SPACING,),
+                                ref_bins=BINS, flo_bins=BINS)
+    cdim = nrb.grid_dims(dim, pix, params)
+    ncpp = 3 * int(np.prod(cdim))
+    cpp_d = torch.empty(ncpp, dtype=torch.float32, device=dev)
+    cpp_h = torch.empty(ncpp, dtype=torch.float32).pin_memory()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def step():
+        return nrb.register_device(ref_d, flo_d, dim, pix, params, cpp_d, ncpp, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+
+    # ---- timed: device-resident inputs -------------------------------------------------------
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    launches0 = nrb.kernel_launch_count()
+    nrb.timing_enable(True)
+    events, results = [], []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()  # L2 flush between timed steps, outside the events
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        results.append(step())
+        e1.record(stream)
+        events.append((e0, e1))
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = nrb.kernel_launch_count() - launches0
+    step_ms = [a.elapsed_time(b) for a, b in events]
+    timed = {k: nrb.timing_read(k) for k in ("objective", "gradient", "finalize", "conv", "be_value", "be_gradient")}
+    nrb.timing_enable(False)
+    total_ms = float(sum(step_ms))
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_max = float(t.item())
+    value = world * args.steps / (total_max / 1e3)
+
+    # ---- e2e: host buffers through the C ABI, copies inside the timed region ------------------
+    barrier()
+    e2e_s = []
+    for _ in range(0 if args.no_e2e else args.steps):
+        t0 = time.perf_counter()
+        cpp_np, res = nrb.register_host(ref_h.numpy().reshape(SHAPE), flo_h.numpy().reshape(SHAPE), pix, params)
+        e2e_s.append(time.perf_counter() - t0)
+    t = torch.tensor([sum(e2e_s)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world * len(e2e_s) / float(t.item()) if e2e_s else None
+
+    # ---- roofline of the dominant kernel ------------------------------------------------------
+    dom = max(timed, key=lambda k: timed[k][1])
+    n_l, ms_l, bytes_l = timed[dom]
+    peak, peak_kind = peaks()
+    achieved = (bytes_l / n_l) / (ms_l / n_l / 1e3) / 1e9 if n_l else 0.0
+    per_voxel = traffic_per_launch(dom)
+    voxels_per_launch = None
+    traffic = None
+    if per_voxel is not None and n_l:
+        # units of one launch: the reference voxels of that launch (time-weighted mix of levels)
+        voxels_per_launch = (bytes_l / n_l) / (8.0 if dom == "objective" else 20.0)
+        traffic = per_voxel * voxels_per_launch
+    share = {k: round(v[1] / sum(x[1] for x in timed.values()), 4) for k, v in timed.items()}
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": "registrations/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "shape_zyx": list(SHAPE), "levels": LEVELS, "max_iterations": MAXIT,
+                   "bins": BINS, "bending_energy": BE, "spacing_mm": 5.0, "parallelism": "replicas",
+                   "l2": f"{L2_FLUSH_BYTES >> 20} MiB buffer written between timed steps"},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                     "launches": n_l, "avg_launch_us": ms_l / n_l * 1e3 if n_l else None,
+                     "algorithmic_bytes_per_launch": bytes_l / n_l if n_l else None,
+                     "time_share": share},
+        "e2e": {"value": e2e_value, "unit": "registrations/s", "h2d_bytes_per_step": 2 * 4 * nx * ny * nz,
+                "d2h_bytes_per_step": 4 * ncpp},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "registration": {"final_nmi": results[-1].final_nmi, "objective_evaluations": results[-1].objective_evaluations,
+                         "gradient_evaluations": results[-1].gradient_evaluations,
+                         "step_ms": [round(s, 3) for s in step_ms]},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        cb = reference_sample(pair, os.cpu_count() or 1)
+        if cb is not None:
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.kernel:
+        return run_kernel_only(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,277 @@
+/* niftyreg_b200: B200-native F3D objective-and-gradient evaluation behind a C ABI.
+ *
+ * Every entry point takes plain pointers and sizes and returns an nrb_status. Array arguments
+ * are DEVICE pointers unless the parameter name ends in _host. `stream` is a cudaStream_t passed
+ * as void* (NULL = the legacy default stream); every call is asynchronous on that stream unless
+ * it returns a host value, in which case it synchronises the stream first.
+ *
+ * Data layout (identical to NiftyReg's NIfTI buffers, so a platform plugin can hand over its
+ * arrays without reshaping):
+ *   - scalar volume: float32, x fastest, [nz][ny][nx];
+ *   - vector image (deformation field, spatial/voxel gradient, control-point grid and its
+ *     gradient): three planes [x | y | z], each laid out as a scalar volume;
+ *   - mask: int32 per reference voxel, -1 = inactive, NULL = every voxel active;
+ *   - matrices: row-major float[16] in the NIfTI mat44 layout.
+ *
+ * Each declaration names the reference interface it replaces (paths relative to the NiftyReg
+ * source tree). */
+#ifndef NIFTYREG_B200_H
+#define NIFTYREG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum nrb_status {
+    NRB_OK = 0,
+    NRB_ERR_INVALID = 1,      /* bad argument: null pointer, non-positive size, bins < 5 ... */
+    NRB_ERR_UNSUPPORTED = 2,  /* geometry outside the F3D layout (grid not axis-aligned ...) */
+    NRB_ERR_CUDA = 3,         /* a CUDA call failed; nrb_last_error() has the text */
+    NRB_ERR_NO_DEVICE = 4,    /* no CUDA device, or not an sm_100 device */
+    NRB_ERR_OOM = 5           /* device allocation failed */
+} nrb_status;
+
+/* Geometry of one registration level: the reference image (which is also the geometry of the
+ * warped image, the deformation field and the voxel-based gradients), the floating image and
+ * the cubic B-spline control-point grid. *_xyz is voxel->mm, *_ijk mm->voxel (NiftyReg picks
+ * the sform when sform_code > 0, else the qform: reg-lib/Content.h GetXYZMatrix/GetIJKMatrix).
+ * Mirrors the three NiftiImage members of F3dContent (reg-lib/F3dContent.h:5-30). */
+typedef struct nrb_geometry {
+    int32_t ref_dim[3];
+    float ref_pixdim[3];
+    float ref_xyz[16];
+    float ref_ijk[16];
+    int32_t flo_dim[3];
+    float flo_pixdim[3];
+    float flo_xyz[16];
+    float flo_ijk[16];
+    int32_t cpp_dim[3];
+    float cpp_pixdim[3]; /* control-point spacing in mm */
+    float cpp_xyz[16];
+    float cpp_ijk[16];
+} nrb_geometry;
+
+/* Packed per-evaluation scalars written by the objective kernels (device memory). */
+typedef struct nrb_objective {
+    double nmi;          /* (H_ref + H_war) / H_joint, unweighted */
+    double entropy[4];   /* H_ref, H_war, H_joint, total histogram mass (_reg_nmi.cpp:303-346) */
+    double be;           /* approximate bending energy, unweighted (_regul.cpp:72-153) */
+    double objective;    /* sim_weight * nmi - be_weight * be (_reg_f3d.cpp:443-462) */
+    double max_grad_len; /* largest node-gradient length of the last gradient evaluation */
+} nrb_objective;
+
+/* ---- library ------------------------------------------------------------------------------ */
+
+/* Text of the last error on this thread (empty string when none). */
+const char *nrb_last_error(void);
+/* Selects and checks the CUDA device (replaces CudaContext::SetCudaIdx,
+ * reg-lib/cuda/CudaContext.cpp:38-91 and Platform::SetGpuIdx, reg-lib/Platform.cpp:66-93). */
+nrb_status nrb_set_device(int device);
+/* 1 when the library was built for sm_100a and a B200-class device is present. */
+int nrb_device_ok(void);
+
+/* ---- deformation and resampling (Compute, reg-lib/Compute.h:6-49) ------------------------ */
+
+/* Cubic B-spline deformation field (positions in mm) from the control-point positions.
+ * Replaces Compute::GetDeformationField(false, true) (reg-lib/Compute.cpp:83-90) ->
+ * reg_spline_getDeformationField (reg-lib/cpu/_reg_localTrans.cpp:1457-1538).
+ * def: 3 * nvox(ref) floats. Masked voxels receive 0. */
+nrb_status nrb_get_deformation_field(const nrb_geometry *g, const float *cpp, const int32_t *mask,
+                                     float *def, void *stream);
+
+/* Trilinear warp of the floating image by a deformation field, padding outside the floating
+ * volume. Replaces Compute::ResampleImage(1, padding) (reg-lib/Compute.cpp:8-15) ->
+ * ResampleImage3D (reg-lib/cpu/_reg_resampling.cpp:316-464). Masked voxels are untouched. */
+nrb_status nrb_resample_image(const nrb_geometry *g, const float *flo, const float *def,
+                              const int32_t *mask, float padding, float *warped, void *stream);
+
+/* Spatial gradient (floating voxel units) of the trilinearly warped floating image, NaN -> 0.
+ * Replaces Compute::GetImageGradient(1, padding, 0) (reg-lib/Compute.cpp:129-138) ->
+ * TrilinearImageGradient (reg-lib/cpu/_reg_resampling.cpp:1797-1915). grad: 3 * nvox(ref). */
+nrb_status nrb_get_image_gradient(const nrb_geometry *g, const float *flo, const float *def,
+                                  const int32_t *mask, float padding, float *grad, void *stream);
+
+/* ---- intensity rescale (reg_nmi::InitialiseMeasure, reg-lib/cpu/_reg_nmi.cpp:91-158) ------ */
+
+/* In-place rescale of the finite values of a volume to [new_min, new_max] in double precision.
+ * Replaces reg_intensityRescale (reg-lib/cpu/_reg_tools.cpp:92-174). */
+nrb_status nrb_intensity_rescale(float *img, int64_t nvox, float new_min, float new_max,
+                                 void *stream);
+
+/* ---- NMI measure (reg_nmi, reg-lib/cpu/_reg_nmi.h:19-84) ---------------------------------- */
+
+/* Workspace of one NMI measure: joint histogram counts, FP64 probability/log tables,
+ * entropies. Replaces the histogram arrays reg_nmi allocates in InitialiseMeasure. */
+typedef struct nrb_nmi nrb_nmi;
+nrb_status nrb_nmi_create(int ref_bins, int flo_bins, nrb_nmi **out);
+void nrb_nmi_destroy(nrb_nmi *nmi);
+
+/* Joint histogram of (reference, warped) over active voxels, 3-tap B-spline smoothing, FP64
+ * entropies; writes the log table used by the gradient and the scalars into `obj` (device,
+ * may be NULL). Replaces reg_nmi::GetSimilarityMeasureValueFw (reg-lib/cpu/_reg_nmi.cpp:385-398
+ * -> reg_getNmiValue :160-347, approximated Parzen window). If nmi_host is non-NULL the stream
+ * is synchronised and the NMI is returned there. */
+nrb_status nrb_nmi_value(nrb_nmi *nmi, const nrb_geometry *g, const float *ref,
+                         const float *warped, const int32_t *mask, nrb_objective *obj,
+                         double *nmi_host, void *stream);
+
+/* Adds weight * dNMI/d(warped) * spatial gradient to vgrad, using the log table of the last
+ * nrb_nmi_value call. Replaces reg_getVoxelBasedNmiGradient3d (reg-lib/cpu/_reg_nmi.cpp:501-593),
+ * which reg_nmi::GetVoxelBasedSimilarityMeasureGradientFw (:623-638) runs after recomputing the
+ * histogram. */
+nrb_status nrb_nmi_voxel_gradient(nrb_nmi *nmi, const nrb_geometry *g, const float *ref,
+                                  const float *warped, const float *warped_grad,
+                                  const int32_t *mask, double weight, float *vgrad, void *stream);
+
+/* Copies the last histogram state to the host: pro/log are ref_bins*flo_bins + ref_bins +
+ * flo_bins doubles (joint | reference marginal | floating marginal), ent is 4 doubles. Any
+ * pointer may be NULL. Synchronises the stream. Test and debug use. */
+nrb_status nrb_nmi_read_tables(nrb_nmi *nmi, double *pro_host, double *log_host,
+                               double *ent_host, void *stream);
+
+/* ---- voxel -> node gradient (Compute::ConvolveVoxelBasedMeasureGradient) ------------------ */
+
+/* One axis (0, 1, 2) of the density-normalised cubic B-spline convolution of a vector image,
+ * spacing in mm; in place over the whole volume. Replaces reg_tools_kernelConvolution with
+ * ConvKernelType::Cubic and one active axis (reg-lib/cpu/_reg_tools.cpp:831-1112). */
+nrb_status nrb_kernel_convolution_cubic(float *img, int nvol, const int32_t dim[3],
+                                        const float pixdim[3], float spacing_mm, int axis,
+                                        void *stream);
+
+/* Node gradient = weight * reorient(trilinear sample at the node of the x-, y- then z-convolved
+ * voxel gradient). The convolution is evaluated only at the voxels the node sampling reads.
+ * Overwrites node_grad (3 * nvox(cpp)). vgrad is read only. Replaces
+ * Compute::ConvolveVoxelBasedMeasureGradient (reg-lib/Compute.cpp:230-281) ->
+ * reg_tools_kernelConvolution x3 + reg_voxelCentricToNodeCentric
+ * (reg-lib/cpu/_reg_localTrans.cpp:1540-1685). Scratch comes from `ws`
+ * (nrb_workspace_create). */
+typedef struct nrb_workspace nrb_workspace;
+nrb_status nrb_workspace_create(const nrb_geometry *g, nrb_workspace **out);
+void nrb_workspace_destroy(nrb_workspace *ws);
+nrb_status nrb_convolve_voxel_based_gradient(nrb_workspace *ws, const nrb_geometry *g,
+                                             const float *vgrad, float weight, float *node_grad,
+                                             void *stream);
+
+/* ---- regularisation (Compute::ApproxBendingEnergy*, reg-lib/Compute.cpp:40-51) ------------- */
+
+/* Approximate bending energy of the grid positions, unweighted, FP64 sum. Written to
+ * obj->be when obj is non-NULL; returned in be_host (synchronising) when non-NULL.
+ * Replaces reg_spline_approxBendingEnergy (reg-lib/cpu/_reg_localTrans_regul.cpp:155-177). */
+nrb_status nrb_approx_bending_energy(nrb_workspace *ws, const nrb_geometry *g, const float *cpp,
+                                     nrb_objective *obj, double *be_host, void *stream);
+
+/* node_grad += weight/#nodes * d(BE)/d(displacement). Replaces
+ * reg_spline_approxBendingEnergyGradient (reg-lib/cpu/_reg_localTrans_regul.cpp:453-482). */
+nrb_status nrb_approx_bending_energy_gradient(nrb_workspace *ws, const nrb_geometry *g,
+                                              const float *cpp, float weight, float *node_grad,
+                                              void *stream);
+
+/* ---- optimiser support (Compute.cpp:91-183, Optimiser.cpp:231-317) ------------------------- */
+
+/* Largest Euclidean length of the node gradient (float), into obj->max_grad_len and/or
+ * max_host. Replaces Compute::GetMaximalLength (reg-lib/Compute.cpp:140-146). */
+nrb_status nrb_get_maximal_length(const float *node_grad, int64_t nnode, nrb_objective *obj,
+                                  double *max_host, void *stream);
+/* node_grad /= max length; the length is read from obj->max_grad_len when max_len < 0.
+ * Replaces Compute::NormaliseGradient (reg-lib/Compute.cpp:148-176). */
+nrb_status nrb_normalise_gradient(float *node_grad, int64_t nnode, double max_len,
+                                  const nrb_objective *obj, void *stream);
+/* cur = best + scale * grad over n values. Replaces Compute::UpdateControlPointPosition
+ * (reg-lib/Compute.cpp:91-127, all axes optimised). */
+nrb_status nrb_update_control_point_position(float *cur, const float *best, const float *grad,
+                                             float scale, int64_t n, void *stream);
+/* Conjugate-gradient direction update with FP64 dot products in a fixed reduction order.
+ * first_call != 0: g1 = g2 = -grad. Replaces ConjugateGradient<float>::UpdateGradientValues
+ * (reg-lib/Optimiser.cpp:231-317; CUDA counterpart reg-lib/cuda/CudaOptimiser.cu:198-290). */
+nrb_status nrb_conjugate_gradient(nrb_workspace *ws, float *grad, float *g1, float *g2, int64_t n,
+                                  int first_call, void *stream);
+
+/* ---- fused F3D evaluations (reg_f3d, reg-lib/_reg_f3d.cpp) -------------------------------- */
+
+/* One objective evaluation: bending energy of cpp, deformation field, trilinear warp, joint
+ * histogram and entropies fused into one pass over the reference voxels (the deformation field
+ * and warped image are never written to HBM). Replaces reg_f3d::GetObjectiveFunctionValue
+ * (reg-lib/_reg_f3d.cpp:443-462) with WarpFloatingImage (reg-lib/_reg_base.cpp:688-708) and
+ * ComputeSimilarityMeasure (:469-494). Writes obj on the device; obj_host (optional) receives a
+ * copy after a stream synchronisation. */
+nrb_status nrb_f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
+                             const float *ref, const float *flo, const int32_t *mask,
+                             const float *cpp, float padding, double sim_weight,
+                             double be_weight, nrb_objective *obj, nrb_objective *obj_host,
+                             void *stream);
+
+/* One gradient evaluation into node_grad: the joint histogram is recomputed at cpp (as
+ * reg_nmi::GetVoxelBasedSimilarityMeasureGradientFw does), then warp + spatial gradient + NMI
+ * voxel gradient run fused in one pass into vgrad (3 * nvox(ref) floats of caller memory),
+ * then the voxel->node convolution (weighted by sim_weight) overwrites node_grad and the
+ * bending-energy gradient (be_weight) is added. Replaces reg_f3d::GetObjectiveFunctionGradient
+ * (reg-lib/_reg_f3d.cpp:553-576). */
+nrb_status nrb_f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
+                            const float *ref, const float *flo, const int32_t *mask,
+                            const float *cpp, float padding, double sim_weight,
+                            double be_weight, float *vgrad, float *node_grad, void *stream);
+
+/* ---- whole registration (reg_f3d<float>::Run, reg-lib/_reg_base.cpp:727-818) -------------- */
+
+typedef struct nrb_f3d_params {
+    int32_t levels;           /* -ln: pyramid levels (all performed) */
+    int32_t max_iterations;   /* -maxit: finest-level budget, doubled per coarser level */
+    float bending_energy;     /* -be */
+    float spacing[3];         /* -sx/-sy/-sz: negative = voxels, positive = mm */
+    int32_t ref_bins;         /* --rbn (the +4 Parzen margin is added internally) */
+    int32_t flo_bins;         /* --fbn */
+    float padding;            /* -pad: warped padding value (NaN by default) */
+    int32_t verbose;
+} nrb_f3d_params;
+
+typedef struct nrb_f3d_result {
+    int32_t cpp_dim[3];       /* final grid dims; the grid is 3 * prod(cpp_dim) floats */
+    double final_nmi;         /* NMI at the best position of the finest level */
+    double final_be;          /* unweighted BE there */
+    double final_objective;
+    int64_t objective_evaluations;
+    int64_t gradient_evaluations;
+    double seconds;           /* host wall time of the whole call */
+} nrb_f3d_result;
+
+/* Default parameters of reg_f3d<float> (reg-lib/_reg_base.cpp:17-70, _reg_f3d.cpp:18-40). */
+void nrb_f3d_default_params(nrb_f3d_params *p);
+
+/* Final grid dims for a registration of this reference (for sizing cpp_out_host). */
+nrb_status nrb_f3d_grid_dims(const int32_t ref_dim[3], const float ref_pixdim[3],
+                             const nrb_f3d_params *p, int32_t cpp_dim_out[3]);
+
+/* Full F3D registration from HOST images (identity orientation, origin 0, the given voxel
+ * size): pyramid, per-level grid refinement, conjugate-gradient line search, all on the
+ * device. Host<->device copies are part of the call. cpp_out_host receives the final
+ * control-point positions (3 * prod(cpp_dim) floats, capacity cpp_capacity floats). */
+nrb_status nrb_f3d_register_host(const float *ref_host, const float *flo_host,
+                                 const int32_t dim[3], const float pixdim[3],
+                                 const nrb_f3d_params *p, float *cpp_out_host,
+                                 int64_t cpp_capacity, nrb_f3d_result *result);
+
+/* The same registration from images already resident on the device. */
+nrb_status nrb_f3d_register_device(const float *ref, const float *flo, const int32_t dim[3],
+                                   const float pixdim[3], const nrb_f3d_params *p,
+                                   float *cpp_out, int64_t cpp_capacity, nrb_f3d_result *result,
+                                   void *stream);
+
+/* Number of kernel launches issued by this library in this process so far. */
+int64_t nrb_kernel_launch_count(void);
+
+/* Per-kernel CUDA-event timing (no counterpart in the reference, which only offers the wall
+ * clocks of reg-apps/reg_benchmark.cpp). While enabled, every launch of the timed kernels is
+ * bracketed by events on its own stream; enabling clears the counters. nrb_timing_read returns,
+ * for "objective", "gradient", "finalize", "conv", "be_value" or "be_gradient", the launches,
+ * their summed device time and the algorithmic bytes those launches had to move. */
+void nrb_timing_enable(int on);
+nrb_status nrb_timing_read(const char *kernel, int64_t *launches, double *total_ms,
+                           double *algorithmic_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NIFTYREG_B200_H */

@@ -1,0 +1,361 @@
+"""niftyreg_b200 -- B200-native F3D objective-and-gradient evaluation (NiftyReg reg_f3d path).
+
+The product is the shared library ``libniftyreg_b200.so`` (CUDA kernels for sm_100a, the C ABI
+declared in ``include/niftyreg_b200.h`` and the registration driver). This module is a thin
+ctypes binding to that ABI: array arguments are device pointers (``int`` addresses, e.g.
+``tensor.data_ptr()``) unless a function says it takes host arrays. There is no fallback: if the
+library is missing or no sm_100 device is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libniftyreg_b200.so")
+
+__all__ = [
+    "NrbError", "Geometry", "Objective", "F3dParams", "F3dResult", "lib", "build",
+    "make_geometry", "identity_header", "Nmi", "Workspace",
+]
+
+
+class NrbError(RuntimeError):
+    """A C-ABI call returned a non-zero nrb_status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"nrb_status {status}: {message}")
+        self.status = status
+
+
+_M16 = ctypes.c_float * 16
+_I3 = ctypes.c_int32 * 3
+_F3 = ctypes.c_float * 3
+
+
+class Geometry(ctypes.Structure):
+    _fields_ = [
+        ("ref_dim", _I3), ("ref_pixdim", _F3), ("ref_xyz", _M16), ("ref_ijk", _M16),
+        ("flo_dim", _I3), ("flo_pixdim", _F3), ("flo_xyz", _M16), ("flo_ijk", _M16),
+        ("cpp_dim", _I3), ("cpp_pixdim", _F3), ("cpp_xyz", _M16), ("cpp_ijk", _M16),
+    ]
+
+    @property
+    def ref_nvox(self) -> int:
+        return int(np.prod(list(self.ref_dim)))
+
+    @property
+    def cpp_nvox(self) -> int:
+        return int(np.prod(list(self.cpp_dim)))
+
+
+class Objective(ctypes.Structure):
+    _fields_ = [("nmi", ctypes.c_double), ("entropy", ctypes.c_double * 4), ("be", ctypes.c_double),
+                ("objective", ctypes.c_double), ("max_grad_len", ctypes.c_double)]
+
+
+class F3dParams(ctypes.Structure):
+    _fields_ = [("levels", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
+                ("bending_energy", ctypes.c_float), ("spacing", _F3), ("ref_bins", ctypes.c_int32),
+                ("flo_bins", ctypes.c_int32), ("padding", ctypes.c_float), ("verbose", ctypes.c_int32)]
+
+
+class F3dResult(ctypes.Structure):
+    _fields_ = [("cpp_dim", _I3), ("final_nmi", ctypes.c_double), ("final_be", ctypes.c_double),
+                ("final_objective", ctypes.c_double), ("objective_evaluations", ctypes.c_int64),
+                ("gradient_evaluations", ctypes.c_int64), ("seconds", ctypes.c_double)]
+
+
+_LIB = None
+
+
+def build(force: bool = False) -> str:
+    """Compiles libniftyreg_b200.so for sm_100a with nvcc (no GPU needed)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.check_call(["make", "-C", HERE, "-j4"], stdout=subprocess.DEVNULL)
+    return LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded C ABI. Raises if the shared library has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run niftyreg_b200.build() (nvcc, sm_100a)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.nrb_last_error.restype = ctypes.c_char_p
+        L.nrb_kernel_launch_count.restype = ctypes.c_int64
+        L.nrb_nmi_destroy.restype = None
+        L.nrb_workspace_destroy.restype = None
+        L.nrb_f3d_default_params.restype = None
+        _LIB = L
+    return _LIB
+
+
+def check(status: int):
+    if status != 0:
+        raise NrbError(status, lib().nrb_last_error().decode())
+
+
+def _p(x):
+    """Device pointer argument: an int address, an object with data_ptr(), or None."""
+    if x is None:
+        return None
+    if hasattr(x, "data_ptr"):
+        return ctypes.c_void_p(x.data_ptr())
+    return ctypes.c_void_p(int(x))
+
+
+def _s(stream):
+    if stream is None:
+        return None
+    if hasattr(stream, "cuda_stream"):
+        return ctypes.c_void_p(stream.cuda_stream)
+    return ctypes.c_void_p(int(stream))
+
+
+def _inv(m):
+    return np.linalg.inv(np.asarray(m, np.float64).reshape(4, 4)).astype(np.float32)
+
+
+def identity_header(pixdim, origin=(0.0, 0.0, 0.0)):
+    """voxel->mm matrix of an image with identity orientation."""
+    m = np.eye(4, dtype=np.float32)
+    for i in range(3):
+        m[i, i] = pixdim[i]
+        m[i, 3] = origin[i]
+    return m
+
+
+def make_geometry(ref_dim, ref_pixdim, ref_xyz, flo_dim, flo_pixdim, flo_xyz, cpp_dim, cpp_pixdim,
+                  cpp_xyz) -> Geometry:
+    g = Geometry()
+    for name, dim, pix, xyz in (("ref", ref_dim, ref_pixdim, ref_xyz), ("flo", flo_dim, flo_pixdim, flo_xyz),
+                                ("cpp", cpp_dim, cpp_pixdim, cpp_xyz)):
+        getattr(g, name + "_dim")[:] = [int(v) for v in dim]
+        getattr(g, name + "_pixdim")[:] = [float(v) for v in pix]
+        getattr(g, name + "_xyz")[:] = [float(v) for v in np.asarray(xyz, np.float32).reshape(16)]
+        getattr(g, name + "_ijk")[:] = [float(v) for v in _inv(xyz).reshape(16)]
+    return g
+
+
+def control_grid_header(ref_dim, ref_pixdim, spacing_mm):
+    """Dims, spacing and voxel->mm of reg_createControlPointGrid for an identity-oriented
+    reference (node 0 one spacing before voxel 0)."""
+    dim = []
+    for n, d, s in zip(ref_dim, ref_pixdim, spacing_mm):
+        v = np.float32(np.float32(n) * np.float32(d) / np.float32(s) + np.float32(3.0))
+        i = int(v)
+        dim.append(i + (1 if v > i else 0))
+    xyz = identity_header(spacing_mm, [-float(s) for s in spacing_mm])
+    return dim, [float(s) for s in spacing_mm], xyz
+
+
+class Nmi:
+    """NMI measure workspace (joint histogram, FP64 tables) on the current device."""
+
+    def __init__(self, ref_bins: int, flo_bins: int):
+        self.h = ctypes.c_void_p()
+        self.ref_bins, self.flo_bins = ref_bins, flo_bins
+        check(lib().nrb_nmi_create(int(ref_bins), int(flo_bins), ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().nrb_nmi_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def tables(self, stream=None):
+        total = self.ref_bins * self.flo_bins + self.ref_bins + self.flo_bins
+        pro = np.zeros(total, np.float64)
+        log = np.zeros(total, np.float64)
+        ent = np.zeros(4, np.float64)
+        check(lib().nrb_nmi_read_tables(self.h, pro.ctypes.data_as(ctypes.c_void_p),
+                                        log.ctypes.data_as(ctypes.c_void_p),
+                                        ent.ctypes.data_as(ctypes.c_void_p), _s(stream)))
+        return pro, log, ent
+
+
+class Workspace:
+    """Scratch buffers of one registration level (nrb_workspace_create)."""
+
+    def __init__(self, g: Geometry):
+        self.h = ctypes.c_void_p()
+        self.g = g
+        check(lib().nrb_workspace_create(ctypes.byref(g), ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().nrb_workspace_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------------------------------------
+# Compute / reg_nmi operations (device pointers)
+# ------------------------------------------------------------------------------------------------
+def get_deformation_field(g, cpp, deformation, mask=None, stream=None):
+    check(lib().nrb_get_deformation_field(ctypes.byref(g), _p(cpp), _p(mask), _p(deformation), _s(stream)))
+
+
+def resample_image(g, flo, deformation, warped, padding=math.nan, mask=None, stream=None):
+    check(lib().nrb_resample_image(ctypes.byref(g), _p(flo), _p(deformation), _p(mask), ctypes.c_float(padding),
+                                   _p(warped), _s(stream)))
+
+
+def get_image_gradient(g, flo, deformation, grad, padding=math.nan, mask=None, stream=None):
+    check(lib().nrb_get_image_gradient(ctypes.byref(g), _p(flo), _p(deformation), _p(mask), ctypes.c_float(padding),
+                                       _p(grad), _s(stream)))
+
+
+def intensity_rescale(img, nvox, new_min, new_max, stream=None):
+    check(lib().nrb_intensity_rescale(_p(img), ctypes.c_int64(nvox), ctypes.c_float(new_min),
+                                      ctypes.c_float(new_max), _s(stream)))
+
+
+def nmi_value(nmi: Nmi, g, ref, warped, mask=None, obj=None, stream=None) -> float:
+    out = ctypes.c_double()
+    check(lib().nrb_nmi_value(nmi.h, ctypes.byref(g), _p(ref), _p(warped), _p(mask), _p(obj), ctypes.byref(out),
+                              _s(stream)))
+    return out.value
+
+
+def nmi_voxel_gradient(nmi: Nmi, g, ref, warped, warped_grad, vgrad, weight=1.0, mask=None, stream=None):
+    check(lib().nrb_nmi_voxel_gradient(nmi.h, ctypes.byref(g), _p(ref), _p(warped), _p(warped_grad), _p(mask),
+                                       ctypes.c_double(weight), _p(vgrad), _s(stream)))
+
+
+def kernel_convolution_cubic(img, nvol, dim, pixdim, spacing_mm, axis, stream=None):
+    d = _I3(*[int(v) for v in dim])
+    p = _F3(*[float(v) for v in pixdim])
+    check(lib().nrb_kernel_convolution_cubic(_p(img), int(nvol), d, p, ctypes.c_float(spacing_mm), int(axis),
+                                             _s(stream)))
+
+
+def convolve_voxel_based_gradient(ws: Workspace, vgrad, node_grad, weight, stream=None):
+    check(lib().nrb_convolve_voxel_based_gradient(ws.h, ctypes.byref(ws.g), _p(vgrad), ctypes.c_float(weight),
+                                                  _p(node_grad), _s(stream)))
+
+
+def approx_bending_energy(ws: Workspace, cpp, stream=None) -> float:
+    out = ctypes.c_double()
+    check(lib().nrb_approx_bending_energy(ws.h, ctypes.byref(ws.g), _p(cpp), None, ctypes.byref(out), _s(stream)))
+    return out.value
+
+
+def approx_bending_energy_gradient(ws: Workspace, cpp, node_grad, weight, stream=None):
+    check(lib().nrb_approx_bending_energy_gradient(ws.h, ctypes.byref(ws.g), _p(cpp), ctypes.c_float(weight),
+                                                   _p(node_grad), _s(stream)))
+
+
+def get_maximal_length(node_grad, nnode, stream=None) -> float:
+    out = ctypes.c_double()
+    check(lib().nrb_get_maximal_length(_p(node_grad), ctypes.c_int64(nnode), None, ctypes.byref(out), _s(stream)))
+    return out.value
+
+
+def normalise_gradient(node_grad, nnode, max_len, stream=None):
+    check(lib().nrb_normalise_gradient(_p(node_grad), ctypes.c_int64(nnode), ctypes.c_double(max_len), None,
+                                       _s(stream)))
+
+
+def update_control_point_position(cur, best, grad, scale, n, stream=None):
+    check(lib().nrb_update_control_point_position(_p(cur), _p(best), _p(grad), ctypes.c_float(scale),
+                                                  ctypes.c_int64(n), _s(stream)))
+
+
+def conjugate_gradient(ws: Workspace, grad, g1, g2, n, first_call, stream=None):
+    check(lib().nrb_conjugate_gradient(ws.h, _p(grad), _p(g1), _p(g2), ctypes.c_int64(n), int(bool(first_call)),
+                                       _s(stream)))
+
+
+def f3d_objective(ws: Workspace, nmi: Nmi, ref, flo, cpp, sim_weight, be_weight, padding=math.nan, mask=None,
+                  obj=None, stream=None) -> Objective:
+    out = Objective()
+    check(lib().nrb_f3d_objective(ws.h, nmi.h, ctypes.byref(ws.g), _p(ref), _p(flo), _p(mask), _p(cpp),
+                                  ctypes.c_float(padding), ctypes.c_double(sim_weight), ctypes.c_double(be_weight),
+                                  _p(obj), ctypes.byref(out), _s(stream)))
+    return out
+
+
+def f3d_gradient(ws: Workspace, nmi: Nmi, ref, flo, cpp, vgrad, node_grad, sim_weight, be_weight,
+                 padding=math.nan, mask=None, stream=None):
+    check(lib().nrb_f3d_gradient(ws.h, nmi.h, ctypes.byref(ws.g), _p(ref), _p(flo), _p(mask), _p(cpp),
+                                 ctypes.c_float(padding), ctypes.c_double(sim_weight), ctypes.c_double(be_weight),
+                                 _p(vgrad), _p(node_grad), _s(stream)))
+
+
+def default_params(**kw) -> F3dParams:
+    p = F3dParams()
+    lib().nrb_f3d_default_params(ctypes.byref(p))
+    for k, v in kw.items():
+        if k == "spacing":
+            v = list(v) + [math.nan] * (3 - len(v))
+            p.spacing[:] = [float(x) for x in v]
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def grid_dims(dim, pixdim, params: F3dParams):
+    out = _I3()
+    check(lib().nrb_f3d_grid_dims(_I3(*[int(v) for v in dim]), _F3(*[float(v) for v in pixdim]),
+                                  ctypes.byref(params), out))
+    return [int(v) for v in out]
+
+
+def register_host(ref: np.ndarray, flo: np.ndarray, pixdim, params: F3dParams):
+    """Full F3D registration of host volumes ([nz, ny, nx] float32). Returns (cpp, result):
+    cpp is [3, cz, cy, cx] float32 (control-point positions in mm)."""
+    ref = np.ascontiguousarray(ref, np.float32)
+    flo = np.ascontiguousarray(flo, np.float32)
+    nz, ny, nx = ref.shape
+    dim = _I3(nx, ny, nz)
+    cd = grid_dims((nx, ny, nz), pixdim, params)
+    cpp = np.zeros((3, cd[2], cd[1], cd[0]), np.float32)
+    res = F3dResult()
+    check(lib().nrb_f3d_register_host(ref.ctypes.data_as(ctypes.c_void_p), flo.ctypes.data_as(ctypes.c_void_p), dim,
+                                      _F3(*[float(v) for v in pixdim]), ctypes.byref(params),
+                                      cpp.ctypes.data_as(ctypes.c_void_p), ctypes.c_int64(cpp.size),
+                                      ctypes.byref(res)))
+    return cpp, res
+
+
+def register_device(ref, flo, dim, pixdim, params: F3dParams, cpp_out, capacity, stream=None) -> F3dResult:
+    """Full F3D registration of device-resident volumes; cpp_out is a device buffer."""
+    res = F3dResult()
+    check(lib().nrb_f3d_register_device(_p(ref), _p(flo), _I3(*[int(v) for v in dim]),
+                                        _F3(*[float(v) for v in pixdim]), ctypes.byref(params), _p(cpp_out),
+                                        ctypes.c_int64(capacity), ctypes.byref(res), _s(stream)))
+    return res
+
+
+def kernel_launch_count() -> int:
+    return int(lib().nrb_kernel_launch_count())
+
+
+def timing_enable(on: bool = True):
+    """Brackets every launch of the timed kernels with CUDA events (clears counters)."""
+    lib().nrb_timing_enable.restype = None
+    lib().nrb_timing_enable(int(bool(on)))
+
+
+def timing_read(kernel: str):
+    """(launches, total device ms, algorithmic bytes) of one timed kernel."""
+    n, ms, by = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+    check(lib().nrb_timing_read(kernel.encode(), ctypes.byref(n), ctypes.byref(ms), ctypes.byref(by)))
+    return n.value, ms.value, by.value

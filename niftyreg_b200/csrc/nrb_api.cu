@@ -1,0 +1,261 @@
+// Library-level C ABI: error state, device selection, NMI handles and the fused F3D
+// objective / gradient evaluations.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "nrb_state.cuh"
+
+namespace nrb {
+
+static thread_local std::string g_error;
+std::atomic<long long> g_launch_count{0};
+
+void set_error(const std::string& msg) { g_error = msg; }
+
+nrb_status fail(nrb_status code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+nrb_status check_cuda(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return NRB_OK;
+    g_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? NRB_ERR_OOM : NRB_ERR_CUDA;
+}
+
+int sm_count() {
+    static std::mutex mu;
+    static std::vector<int> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)cache.size() <= dev) cache.resize(dev + 1, 0);
+    if (cache[dev] == 0) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cache[dev] = n > 0 ? n : 148;
+    }
+    return cache[dev];
+}
+
+// ---- per-kernel timing ----------------------------------------------------------------------
+namespace {
+struct Pending {
+    cudaEvent_t a, b;
+    int k;
+    double bytes;
+};
+std::mutex g_tmu;
+bool g_timing = false;
+std::vector<Pending> g_pending;
+std::vector<cudaEvent_t> g_pool;
+long long g_tlaunch[TK_COUNT] = {};
+double g_tms[TK_COUNT] = {}, g_tbytes[TK_COUNT] = {};
+const char *g_tnames[TK_COUNT] = { "objective", "gradient", "finalize", "conv", "be_value", "be_gradient" };
+
+cudaEvent_t pooled_event() {
+    if (!g_pool.empty()) {
+        cudaEvent_t e = g_pool.back();
+        g_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void resolve_pending() {
+    for (const Pending& p : g_pending) {
+        float ms = 0;
+        if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            g_tlaunch[p.k] += 1;
+            g_tms[p.k] += ms;
+            g_tbytes[p.k] += p.bytes;
+        }
+        g_pool.push_back(p.a);
+        g_pool.push_back(p.b);
+    }
+    g_pending.clear();
+}
+}  // namespace
+
+KernelTimer::KernelTimer(TimedKernel k, double bytes, cudaStream_t st): k_(k), bytes_(bytes), st_(st) {
+    std::lock_guard<std::mutex> lock(g_tmu);
+    if (!g_timing) return;
+    if (g_pending.size() > 4096) resolve_pending();
+    a_ = pooled_event();
+    cudaEventRecord(a_, st_);
+}
+
+KernelTimer::~KernelTimer() {
+    if (!a_) return;
+    std::lock_guard<std::mutex> lock(g_tmu);
+    cudaEvent_t b = pooled_event();
+    cudaEventRecord(b, st_);
+    g_pending.push_back({ a_, b, (int)k_, bytes_ });
+}
+
+// defined in nrb_ops.cu
+int be_partial_count(const nrb_geometry *g);
+nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float *cpp, cudaStream_t st);
+
+}  // namespace nrb
+
+using namespace nrb;
+
+extern "C" const char *nrb_last_error(void) { return g_error.c_str(); }
+
+extern "C" int64_t nrb_kernel_launch_count(void) { return g_launch_count.load(); }
+
+extern "C" void nrb_timing_enable(int on) {
+    std::lock_guard<std::mutex> lock(g_tmu);
+    resolve_pending();
+    if (on) {
+        for (int k = 0; k < TK_COUNT; ++k) {
+            g_tlaunch[k] = 0;
+            g_tms[k] = 0;
+            g_tbytes[k] = 0;
+        }
+    }
+    g_timing = on != 0;
+}
+
+extern "C" nrb_status nrb_timing_read(const char *kernel, int64_t *launches, double *total_ms,
+                                      double *algorithmic_bytes) {
+    if (!kernel) return fail(NRB_ERR_INVALID, "nrb_timing_read: null name");
+    std::lock_guard<std::mutex> lock(g_tmu);
+    resolve_pending();
+    for (int k = 0; k < TK_COUNT; ++k) {
+        if (strcmp(kernel, g_tnames[k]) != 0) continue;
+        if (launches) *launches = g_tlaunch[k];
+        if (total_ms) *total_ms = g_tms[k];
+        if (algorithmic_bytes) *algorithmic_bytes = g_tbytes[k];
+        return NRB_OK;
+    }
+    return fail(NRB_ERR_INVALID, std::string("nrb_timing_read: unknown kernel ") + kernel);
+}
+
+extern "C" nrb_status nrb_set_device(int device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(NRB_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    if (device < 0 || device >= n) return fail(NRB_ERR_INVALID, "device index out of range");
+    NRB_CUDA(cudaSetDevice(device));
+    int major = 0;
+    NRB_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    if (major != 10) return fail(NRB_ERR_NO_DEVICE, "device is not compute capability 10.x (sm_100a build)");
+    return NRB_OK;
+}
+
+extern "C" int nrb_device_ok(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return 0;
+    }
+    int dev = 0, major = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    return major == 10 ? 1 : 0;
+}
+
+extern "C" nrb_status nrb_nmi_create(int ref_bins, int flo_bins, nrb_nmi **out) {
+    if (!out || ref_bins < 5 || flo_bins < 5 || ref_bins > 1024 || flo_bins > 1024)
+        return fail(NRB_ERR_INVALID, "nrb_nmi_create: bins must be in [5, 1024] (internal counts, user bins + 4)");
+    if ((size_t)ref_bins * flo_bins * 4 > 180 * 1024)
+        return fail(NRB_ERR_UNSUPPORTED, "nrb_nmi_create: joint histogram larger than one SM's shared memory");
+    nrb_nmi *n = new nrb_nmi();
+    n->rb = ref_bins;
+    n->fb = flo_bins;
+    n->total = ref_bins * flo_bins + ref_bins + flo_bins;
+    cudaGetDevice(&n->device);
+    if (cudaMalloc(&n->hist, (size_t)ref_bins * flo_bins * 4) != cudaSuccess ||
+        cudaMalloc(&n->pro, (size_t)n->total * 8) != cudaSuccess ||
+        cudaMalloc(&n->logt, (size_t)n->total * 8) != cudaSuccess ||
+        cudaMalloc(&n->last, sizeof(nrb_objective)) != cudaSuccess ||
+        cudaMemset(n->hist, 0, (size_t)ref_bins * flo_bins * 4) != cudaSuccess ||
+        cudaMemset(n->pro, 0, (size_t)n->total * 8) != cudaSuccess ||
+        cudaMemset(n->logt, 0, (size_t)n->total * 8) != cudaSuccess ||
+        cudaMemset(n->last, 0, sizeof(nrb_objective)) != cudaSuccess) {
+        cudaGetLastError();
+        nrb_nmi_destroy(n);
+        return fail(NRB_ERR_OOM, "nrb_nmi_create: device allocation failed");
+    }
+    *out = n;
+    return NRB_OK;
+}
+
+extern "C" void nrb_nmi_destroy(nrb_nmi *nmi) {
+    if (!nmi) return;
+    cudaFree(nmi->hist);
+    cudaFree(nmi->pro);
+    cudaFree(nmi->logt);
+    cudaFree(nmi->last);
+    delete nmi;
+}
+
+extern "C" nrb_status nrb_nmi_read_tables(nrb_nmi *nmi, double *pro_host, double *log_host, double *ent_host,
+                                          void *stream) {
+    if (!nmi) return fail(NRB_ERR_INVALID, "nrb_nmi_read_tables: null handle");
+    cudaStream_t st = as_stream(stream);
+    if (pro_host) NRB_CUDA(cudaMemcpyAsync(pro_host, nmi->pro, (size_t)nmi->total * 8, cudaMemcpyDeviceToHost, st));
+    if (log_host) NRB_CUDA(cudaMemcpyAsync(log_host, nmi->logt, (size_t)nmi->total * 8, cudaMemcpyDeviceToHost, st));
+    nrb_objective o;
+    NRB_CUDA(cudaMemcpyAsync(&o, nmi->last, sizeof(o), cudaMemcpyDeviceToHost, st));
+    NRB_CUDA(cudaStreamSynchronize(st));
+    if (ent_host) memcpy(ent_host, o.entropy, 4 * sizeof(double));
+    return NRB_OK;
+}
+
+static nrb_status check_fused_args(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g, const float *ref,
+                                   const float *flo, const float *cpp) {
+    if (!ws || !nmi || !g || !ref || !flo || !cpp) return fail(NRB_ERR_INVALID, "null pointer");
+    if (memcmp(&ws->g, g, sizeof(nrb_geometry)) != 0)
+        return fail(NRB_ERR_INVALID, "workspace was created for another geometry");
+    return NRB_OK;
+}
+
+extern "C" nrb_status nrb_f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
+                                        const float *ref, const float *flo, const int32_t *mask,
+                                        const float *cpp, float padding, double sim_weight,
+                                        double be_weight, nrb_objective *obj, nrb_objective *obj_host,
+                                        void *stream) {
+    NRB_TRY(check_fused_args(ws, nmi, g, ref, flo, cpp));
+    cudaStream_t st = as_stream(stream);
+    int n_be = 0;
+    if (be_weight > 0) {
+        NRB_TRY(launch_be_value(ws, g, cpp, st));
+        n_be = be_partial_count(g);
+    }
+    if (sim_weight > 0) NRB_TRY(launch_fused_objective(ws, nmi, g, ref, flo, mask, cpp, padding, st));
+    NRB_TRY(launch_nmi_finalize(nmi, ws->be_partials, n_be, 3 * nvox(g->cpp_dim), sim_weight, be_weight, obj, st));
+    if (obj_host) {
+        NRB_CUDA(cudaMemcpyAsync(obj_host, obj ? obj : nmi->last, sizeof(nrb_objective), cudaMemcpyDeviceToHost, st));
+        NRB_CUDA(cudaStreamSynchronize(st));
+    }
+    return NRB_OK;
+}
+
+extern "C" nrb_status nrb_f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
+                                       const float *ref, const float *flo, const int32_t *mask,
+                                       const float *cpp, float padding, double sim_weight,
+                                       double be_weight, float *vgrad, float *node_grad, void *stream) {
+    NRB_TRY(check_fused_args(ws, nmi, g, ref, flo, cpp));
+    if (!vgrad || !node_grad) return fail(NRB_ERR_INVALID, "nrb_f3d_gradient: null buffer");
+    cudaStream_t st = as_stream(stream);
+    if (sim_weight > 0) {
+        // the histogram of the current position feeds the log table of the voxel gradient
+        NRB_TRY(launch_fused_objective(ws, nmi, g, ref, flo, mask, cpp, padding, st));
+        NRB_TRY(launch_nmi_finalize(nmi, nullptr, 0, 3 * nvox(g->cpp_dim), sim_weight, 0.0, nullptr, st));
+        NRB_TRY(launch_fused_gradient(ws, nmi, g, ref, flo, mask, cpp, padding, 1.0, vgrad, st));
+        NRB_TRY(launch_convolve_to_nodes(ws, g, vgrad, (float)sim_weight, node_grad, st));
+    } else {
+        NRB_CUDA(cudaMemsetAsync(node_grad, 0, 3 * nvox(g->cpp_dim) * sizeof(float), st));
+    }
+    if (be_weight > 0) NRB_TRY(nrb_approx_bending_energy_gradient(ws, g, cpp, (float)be_weight, node_grad, stream));
+    return NRB_OK;
+}

@@ -1,0 +1,143 @@
+// Internal helpers shared by the niftyreg_b200 CUDA sources (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <string>
+
+#include "niftyreg_b200.h"
+
+namespace nrb {
+
+// ------------------------------------------------------------------------------------------
+// error state and launch accounting
+// ------------------------------------------------------------------------------------------
+void set_error(const std::string& msg);
+nrb_status fail(nrb_status code, const std::string& msg);
+nrb_status check_cuda(cudaError_t e, const char *what);
+extern std::atomic<long long> g_launch_count;
+
+// Call after every kernel launch: counts it and turns a launch error into a status.
+#define NRB_LAUNCHED(what)                                                   \
+    do {                                                                     \
+        ::nrb::g_launch_count.fetch_add(1, std::memory_order_relaxed);       \
+        cudaError_t e_ = cudaGetLastError();                                 \
+        if (e_ != cudaSuccess) return ::nrb::check_cuda(e_, what);           \
+    } while (0)
+
+#define NRB_TRY(expr)                                                        \
+    do {                                                                     \
+        nrb_status s_ = (expr);                                              \
+        if (s_ != NRB_OK) return s_;                                         \
+    } while (0)
+
+#define NRB_CUDA(expr)                                                       \
+    do {                                                                     \
+        cudaError_t e_ = (expr);                                             \
+        if (e_ != cudaSuccess) return ::nrb::check_cuda(e_, #expr);          \
+    } while (0)
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Optional per-kernel CUDA-event timing (nrb_timing_enable). A KernelTimer brackets one launch
+// with events on its stream and records the algorithmic bytes that launch must move.
+enum TimedKernel { TK_OBJECTIVE = 0, TK_GRADIENT, TK_FINALIZE, TK_CONV, TK_BE_VALUE, TK_BE_GRADIENT, TK_COUNT };
+class KernelTimer {
+public:
+    KernelTimer(TimedKernel k, double bytes, cudaStream_t st);
+    ~KernelTimer();
+private:
+    TimedKernel k_;
+    double bytes_;
+    cudaStream_t st_;
+    cudaEvent_t a_ = nullptr;
+};
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+// ------------------------------------------------------------------------------------------
+// device-side geometry
+// ------------------------------------------------------------------------------------------
+struct Mat34 {  // the first three rows of a NIfTI mat44
+    float m[12];
+};
+
+inline Mat34 to_mat34(const float *m16) {
+    Mat34 r;
+    for (int i = 0; i < 12; ++i) r.m[i] = m16[i];
+    return r;
+}
+
+__host__ __device__ inline void mat34_apply(const Mat34& M, float x, float y, float z, float& ox,
+                                            float& oy, float& oz) {
+    ox = M.m[0] * x + M.m[1] * y + M.m[2] * z + M.m[3];
+    oy = M.m[4] * x + M.m[5] * y + M.m[6] * z + M.m[7];
+    oz = M.m[8] * x + M.m[9] * y + M.m[10] * z + M.m[11];
+}
+
+// Cubic B-spline basis at fractional offset t in [0, 1): weights of nodes pre..pre+3
+// (reg-lib/cpu/_reg_splineBasis.cpp:17-26 evaluates the same polynomials).
+__host__ __device__ inline void bspline_basis(float t, float b[4]) {
+    const float ff = t * t, fff = ff * t, mf = 1.f - t;
+    b[0] = mf * mf * mf * (1.f / 6.f);
+    b[1] = (3.f * fff - 6.f * ff + 4.f) * (1.f / 6.f);
+    b[2] = (-3.f * fff + 3.f * ff + 3.f * t + 1.f) * (1.f / 6.f);
+    b[3] = fff * (1.f / 6.f);
+}
+
+// Parzen window: cubic B-spline and its derivative (reg-lib/cpu/_reg_nmi.h:116-145). The
+// centre constant is float(2/3) exactly as the reference writes it (2.f/3.f).
+__host__ __device__ inline double parzen(double x) {
+    x = x < 0 ? -x : x;
+    if (x < 2.0) {
+        if (x < 1.0) return (double)(2.0f / 3.0f) + (0.5 * x - 1.0) * x * x;
+        x -= 2.0;
+        return -x * x * x / 6.0;
+    }
+    return 0.0;
+}
+__host__ __device__ inline double parzen_deriv(double ox) {
+    double x = ox < 0 ? -ox : ox;
+    if (x < 2.0) {
+        if (x < 1.0) return (1.5 * x - 2.0) * ox;
+        x -= 2.0;
+        const double v = -0.5 * x * x;
+        return ox < 0 ? -v : v;
+    }
+    return 0.0;
+}
+__device__ inline float parzenf(float x) {
+    x = fabsf(x);
+    if (x < 2.f) {
+        if (x < 1.f) return (2.0f / 3.0f) + (0.5f * x - 1.f) * x * x;
+        x -= 2.f;
+        return -x * x * x * (1.f / 6.f);
+    }
+    return 0.f;
+}
+__device__ inline float parzen_derivf(float ox) {
+    float x = fabsf(ox);
+    if (x < 2.f) {
+        if (x < 1.f) return (1.5f * x - 2.f) * ox;
+        x -= 2.f;
+        const float v = -0.5f * x * x;
+        return ox < 0 ? -v : v;
+    }
+    return 0.f;
+}
+
+inline int64_t nvox(const int32_t d[3]) { return (int64_t)d[0] * d[1] * d[2]; }
+
+// ------------------------------------------------------------------------------------------
+// cross-file launchers
+// ------------------------------------------------------------------------------------------
+// Workspace of scratch buffers sized for one geometry (owned by nrb_workspace).
+struct Workspace;
+nrb_status be_value_partials(Workspace *ws, const nrb_geometry *g, const float *cpp,
+                             cudaStream_t st);
+nrb_status be_value_finish(Workspace *ws, nrb_objective *obj, double *be_host, cudaStream_t st);
+
+}  // namespace nrb

@@ -1,0 +1,451 @@
+// Whole F3D registration on the device: the pyramid, per-level grid refinement and the
+// conjugate-gradient line search of reg_f3d<float>::Run, with every image, grid and optimiser
+// array resident in HBM. Each objective evaluation returns one packed struct to the host, which
+// takes the line-search branch exactly as Optimiser::Optimise does.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "nrb_state.cuh"
+
+namespace nrb {
+
+// defined in nrb_ops.cu
+nrb_status smooth_and_downsample(const float *in, const int32_t idim[3], float *out, const int32_t odim[3],
+                                 const float new_xyz[16], const float old_ijk[16], float *tmp, cudaStream_t st);
+nrb_status grid_identity(const int32_t cdim[3], const float cxyz[16], float *cpp, cudaStream_t st);
+nrb_status grid_refine(const int32_t odim[3], const float *old, const int32_t ndim[3], float *out, cudaStream_t st);
+nrb_status rescale_with(float *img, int64_t n, float lo, float hi, float *fred, cudaStream_t st);
+nrb_status max_and_normalise(nrb_workspace *ws, float *grad, int64_t nnode, nrb_objective *obj, cudaStream_t st);
+
+namespace {
+
+// Ceil<int>(float) and the like of reg-lib/cpu/Maths.hpp:63-85
+int ceil_ref(float x) {
+    const int i = (int)x;
+    return i + (x > (float)i);
+}
+
+// Voxel <-> mm of an image with identity orientation and origin `origin` (qform code 1, no
+// sform): qto_xyz = diag(pixdim) + origin, qto_ijk its inverse (nifti_mat44_inverse rounds the
+// double-precision inverse to float).
+struct Header {
+    int32_t dim[3];
+    float pixdim[3];
+    float origin[3];
+    void xyz(float m[16]) const {
+        memset(m, 0, 16 * sizeof(float));
+        for (int i = 0; i < 3; ++i) {
+            m[5 * i] = pixdim[i];
+            m[4 * i + 3] = origin[i];
+        }
+        m[15] = 1.f;
+    }
+    void ijk(float m[16]) const {
+        memset(m, 0, 16 * sizeof(float));
+        for (int i = 0; i < 3; ++i) {
+            const double inv = 1.0 / (double)pixdim[i];
+            m[5 * i] = (float)inv;
+            m[4 * i + 3] = (float)(-(double)origin[i] * inv);
+        }
+        m[15] = 1.f;
+    }
+    int64_t n() const { return (int64_t)dim[0] * dim[1] * dim[2]; }
+};
+
+struct DevBuf {
+    float *p = nullptr;
+    ~DevBuf() { cudaFree(p); }
+    nrb_status alloc(size_t n) {
+        cudaFree(p);
+        p = nullptr;
+        if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(NRB_ERR_OOM, "registration: device allocation failed");
+        }
+        return NRB_OK;
+    }
+};
+
+struct NmiHandle {
+    nrb_nmi *h = nullptr;
+    ~NmiHandle() { nrb_nmi_destroy(h); }
+};
+struct WsHandle {
+    nrb_workspace *h = nullptr;
+    ~WsHandle() { nrb_workspace_destroy(h); }
+};
+
+// reg_f3d<float> with the NMI measure and the bending-energy penalty on the B200 platform.
+class F3dRegistration {
+public:
+    F3dRegistration(const nrb_f3d_params& p, cudaStream_t st): p_(p), st_(st) {}
+
+    nrb_status Run(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3],
+                   float *cpp_out, int64_t cap, nrb_f3d_result *res);
+
+private:
+    // reg_f3d::GetObjectiveFunctionValue (_reg_f3d.cpp:443-462)
+    nrb_status GetObjectiveFunctionValue(double& value) {
+        nrb_objective o;
+        NRB_TRY(nrb_f3d_objective(ws_.h, nmi_.h, &g_, ref_.p, flo_.p, nullptr, cur_.p, pad_, sim_w_, be_w_,
+                                  obj_, &o, st_));
+        cur_w_measure_ = sim_w_ > 0 ? (double)sim_w_ * o.nmi : 0.0;
+        cur_w_be_ = be_w_ > 0 ? (double)be_w_ * o.be : 0.0;
+        cur_nmi_ = o.nmi;
+        cur_be_ = o.be;
+        ++n_obj_;
+        value = cur_w_measure_ - cur_w_be_;
+        return NRB_OK;
+    }
+    // reg_f3d::GetObjectiveFunctionGradient (_reg_f3d.cpp:553-576) + NormaliseGradient (:395-410)
+    nrb_status GetObjectiveFunctionGradient() {
+        NRB_TRY(nrb_f3d_gradient(ws_.h, nmi_.h, &g_, ref_.p, flo_.p, nullptr, cur_.p, pad_, sim_w_, be_w_, vgrad_.p,
+                                 grad_.p, st_));
+        ++it_;
+        ++n_grad_;
+        return max_and_normalise(ws_.h, grad_.p, nc_, obj_, st_);
+    }
+    void UpdateBestObjFunctionValue() {
+        best_w_measure_ = cur_w_measure_;
+        best_w_be_ = cur_w_be_;
+        best_nmi_ = cur_nmi_;
+        best_be_ = cur_be_;
+    }
+    nrb_status StoreCurrentDof() {
+        NRB_CUDA(cudaMemcpyAsync(best_.p, cur_.p, 3 * nc_ * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+        return NRB_OK;
+    }
+    nrb_status RestoreBestDof() {
+        NRB_CUDA(cudaMemcpyAsync(cur_.p, best_.p, 3 * nc_ * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+        return NRB_OK;
+    }
+    // ConjugateGradient::Optimise = UpdateGradientValues + Optimiser::Optimise
+    // (reg-lib/Optimiser.cpp:320-323, :129-173)
+    nrb_status Optimise(float max_length, float small_length, float& start_length) {
+        NRB_TRY(nrb_conjugate_gradient(ws_.h, grad_.p, g1_.p, g2_.p, 3 * nc_, first_call_ ? 1 : 0, st_));
+        first_call_ = false;
+        size_t line_iteration = 0;
+        float added_length = 0;
+        float current_length = start_length;
+        while (current_length > small_length && line_iteration < 12 && it_ < max_it_) {
+            NRB_TRY(nrb_update_control_point_position(cur_.p, best_.p, grad_.p, -current_length, 3 * nc_, st_));
+            double value = 0;
+            NRB_TRY(GetObjectiveFunctionValue(value));
+            if (value > best_obj_) {
+                UpdateBestObjFunctionValue();
+                best_obj_ = value;
+                added_length += current_length;
+                current_length *= 1.1f;
+                current_length = std::min(current_length, max_length);
+                NRB_TRY(StoreCurrentDof());
+            } else {
+                current_length *= 0.5;
+            }
+            ++it_;
+            ++line_iteration;
+        }
+        start_length = added_length;
+        return RestoreBestDof();
+    }
+
+    nrb_status BuildPyramid(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3]);
+    nrb_status CreateGrid();
+    nrb_status InitLevel(int level, float& max_step);
+
+    nrb_f3d_params p_;
+    cudaStream_t st_;
+    int levels_ = 0;
+    std::vector<Header> hdr_;
+    std::vector<DevBuf> ref_pyr_, flo_pyr_;
+    // current level
+    nrb_geometry g_{};
+    DevBuf ref_, flo_, vgrad_, grad_, best_, g1_, g2_, cur_;
+    NmiHandle nmi_;
+    WsHandle ws_;
+    nrb_objective *obj_ = nullptr;
+    int64_t nc_ = 0;
+    // grid
+    Header grid_{};
+    float pad_ = std::numeric_limits<float>::quiet_NaN();
+    float sim_w_ = 1, be_w_ = 0;
+    float spacing_mm_[3] = { 0, 0, 0 };
+    // optimiser state
+    size_t it_ = 0, max_it_ = 0;
+    bool first_call_ = true;
+    double best_obj_ = 0;
+    double cur_w_measure_ = 0, cur_w_be_ = 0, best_w_measure_ = 0, best_w_be_ = 0;
+    double cur_nmi_ = 0, cur_be_ = 0, best_nmi_ = 0, best_be_ = 0;
+    int64_t n_obj_ = 0, n_grad_ = 0;
+};
+
+// reg_createImagePyramid (reg-lib/cpu/_reg_tools.cpp:1705-1733): the finest level is the input,
+// each coarser level halves (ceil) every axis whose current size / 2 is at least 32, after a
+// Gaussian smoothing.
+nrb_status F3dRegistration::BuildPyramid(const float *ref, const float *flo, const int32_t dim[3],
+                                         const float pixdim[3]) {
+    hdr_.assign(levels_, Header{});
+    ref_pyr_ = std::vector<DevBuf>(levels_);
+    flo_pyr_ = std::vector<DevBuf>(levels_);
+    Header& fine = hdr_[levels_ - 1];
+    for (int i = 0; i < 3; ++i) {
+        fine.dim[i] = dim[i];
+        fine.pixdim[i] = pixdim[i];
+        fine.origin[i] = 0.f;
+    }
+    NRB_TRY(ref_pyr_[levels_ - 1].alloc(fine.n()));
+    NRB_TRY(flo_pyr_[levels_ - 1].alloc(fine.n()));
+    NRB_CUDA(cudaMemcpyAsync(ref_pyr_[levels_ - 1].p, ref, fine.n() * 4, cudaMemcpyDefault, st_));
+    NRB_CUDA(cudaMemcpyAsync(flo_pyr_[levels_ - 1].p, flo, fine.n() * 4, cudaMemcpyDefault, st_));
+    if (levels_ == 1) return NRB_OK;
+    DevBuf tmp;
+    NRB_TRY(tmp.alloc(4 * fine.n()));
+    for (int l = levels_ - 2; l >= 0; --l) {
+        const Header& src = hdr_[l + 1];
+        Header& dst = hdr_[l];
+        for (int i = 0; i < 3; ++i) {
+            const bool down = src.dim[i] / 2 >= 32;
+            dst.dim[i] = down && src.dim[i] > 1 ? ceil_ref((float)(src.dim[i] / 2.0)) : src.dim[i];
+            dst.pixdim[i] = down ? src.pixdim[i] * 2.0f : src.pixdim[i];
+            dst.origin[i] = src.origin[i];
+        }
+        float nxyz[16], oijk[16];
+        dst.xyz(nxyz);
+        src.ijk(oijk);
+        NRB_TRY(ref_pyr_[l].alloc(dst.n()));
+        NRB_TRY(flo_pyr_[l].alloc(dst.n()));
+        NRB_TRY(smooth_and_downsample(ref_pyr_[l + 1].p, src.dim, ref_pyr_[l].p, dst.dim, nxyz, oijk, tmp.p, st_));
+        NRB_TRY(smooth_and_downsample(flo_pyr_[l + 1].p, src.dim, flo_pyr_[l].p, dst.dim, nxyz, oijk, tmp.p, st_));
+    }
+    NRB_CUDA(cudaStreamSynchronize(st_));  // tmp is freed on return
+    return NRB_OK;
+}
+
+// reg_f3d::Initialise (_reg_f3d.cpp:161-200) -> reg_createControlPointGrid
+// (reg-lib/cpu/_reg_localTrans.cpp:21-128) on the coarsest reference.
+nrb_status F3dRegistration::CreateGrid() {
+    const Header& r = hdr_[0];
+    float spacing[3];
+    for (int i = 0; i < 3; ++i) {
+        float s = p_.spacing[i];
+        if (s != s) s = p_.spacing[0];
+        spacing_mm_[i] = s < 0 ? s * -hdr_[levels_ - 1].pixdim[i] : s;
+        spacing[i] = spacing_mm_[i] * powf(2.f, (float)(levels_ - 1));
+    }
+    for (int i = 0; i < 3; ++i) {
+        grid_.dim[i] = ceil_ref((float)r.dim[i] * r.pixdim[i] / spacing[i] + 3.f);
+        grid_.pixdim[i] = spacing[i];
+        // the origin shifted by one node: Mat44Mul(qto_xyz, (-1,-1,-1)) in double
+        grid_.origin[i] = (float)((double)spacing[i] * -1.0 + (double)r.origin[i]);
+    }
+    float cxyz[16];
+    grid_.xyz(cxyz);
+    NRB_TRY(cur_.alloc(3 * grid_.n()));
+    return grid_identity(grid_.dim, cxyz, cur_.p, st_);
+}
+
+// reg_f3d::InitCurrentLevel (_reg_f3d.cpp:92-132) + InitialiseSimilarity + SetOptimiser
+nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
+    const Header& r = hdr_[level];
+    max_step = r.pixdim[0] > r.pixdim[1] ? r.pixdim[0] : r.pixdim[1];
+    max_step = r.pixdim[2] > max_step ? r.pixdim[2] : max_step;
+    if (level == 0) {
+        be_w_ = be_w_ / powf(16.f, (float)(levels_ - 1));
+    } else {
+        be_w_ = be_w_ * 16.f;
+        // reg_spline_refineControlPointGrid onto this level's reference
+        Header ng;
+        for (int i = 0; i < 3; ++i) {
+            ng.pixdim[i] = grid_.pixdim[i] / 2.0f;
+            ng.dim[i] = ceil_ref((float)r.dim[i] * r.pixdim[i] / ng.pixdim[i] + 3.f);
+            ng.origin[i] = (float)((double)ng.pixdim[i] * -1.0 + (double)r.origin[i]);
+        }
+        DevBuf refined;
+        NRB_TRY(refined.alloc(3 * ng.n()));
+        NRB_TRY(grid_refine(grid_.dim, cur_.p, ng.dim, refined.p, st_));
+        std::swap(cur_.p, refined.p);
+        grid_ = ng;
+    }
+    // content of this level
+    nrb_geometry& g = g_;
+    for (int i = 0; i < 3; ++i) {
+        g.ref_dim[i] = r.dim[i];
+        g.ref_pixdim[i] = r.pixdim[i];
+        g.flo_dim[i] = r.dim[i];
+        g.flo_pixdim[i] = r.pixdim[i];
+        g.cpp_dim[i] = grid_.dim[i];
+        g.cpp_pixdim[i] = grid_.pixdim[i];
+    }
+    r.xyz(g.ref_xyz);
+    r.ijk(g.ref_ijk);
+    r.xyz(g.flo_xyz);
+    r.ijk(g.flo_ijk);
+    grid_.xyz(g.cpp_xyz);
+    grid_.ijk(g.cpp_ijk);
+    nc_ = grid_.n();
+    std::swap(ref_.p, ref_pyr_[level].p);
+    std::swap(flo_.p, flo_pyr_[level].p);
+    NRB_TRY(vgrad_.alloc(3 * r.n()));
+    NRB_TRY(grad_.alloc(3 * nc_));
+    NRB_TRY(best_.alloc(3 * nc_));
+    NRB_TRY(g1_.alloc(3 * nc_));
+    NRB_TRY(g2_.alloc(3 * nc_));
+    nrb_workspace_destroy(ws_.h);
+    ws_.h = nullptr;
+    NRB_TRY(nrb_workspace_create(&g_, &ws_.h));
+    if (!nmi_.h) NRB_TRY(nrb_nmi_create(p_.ref_bins + 4, p_.flo_bins + 4, &nmi_.h));
+    // reg_nmi::InitialiseMeasure: rescale both images to [2, bins - 3]
+    NRB_TRY(rescale_with(ref_.p, r.n(), 2.f, (float)(p_.ref_bins + 4) - 3.f, ws_.h->fred, st_));
+    NRB_TRY(rescale_with(flo_.p, r.n(), 2.f, (float)(p_.flo_bins + 4) - 3.f, ws_.h->fred, st_));
+    // ConjugateGradient::Initialise: best = current, objective at the starting point
+    it_ = 0;
+    first_call_ = true;
+    NRB_TRY(StoreCurrentDof());
+    double v = 0;
+    NRB_TRY(GetObjectiveFunctionValue(v));
+    best_obj_ = v;
+    return NRB_OK;
+}
+
+nrb_status F3dRegistration::Run(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3],
+                                float *cpp_out, int64_t cap, nrb_f3d_result *res) {
+    const auto t0 = std::chrono::steady_clock::now();
+    levels_ = p_.levels;
+    if (levels_ < 1) return fail(NRB_ERR_INVALID, "registration: levels must be >= 1");
+    if (p_.ref_bins < 1 || p_.flo_bins < 1) return fail(NRB_ERR_INVALID, "registration: bins must be >= 1");
+    pad_ = p_.padding;
+    // reg_f3d::CheckParameters (_reg_f3d.cpp:142-158): weights normalised by the penalty sum
+    be_w_ = p_.bending_energy;
+    const float penalty = be_w_;
+    if (penalty >= 1) {
+        sim_w_ = 0;
+        be_w_ /= penalty;
+    } else {
+        sim_w_ = 1 - penalty;
+    }
+    NRB_CUDA(cudaMallocAsync(&obj_, sizeof(nrb_objective), st_));
+    NRB_CUDA(cudaMemsetAsync(obj_, 0, sizeof(nrb_objective), st_));
+    NRB_TRY(BuildPyramid(ref, flo, dim, pixdim));
+    NRB_TRY(CreateGrid());
+    max_it_ = (size_t)p_.max_iterations;
+    max_it_ *= (size_t)std::pow(2, levels_ - 1);
+    for (int level = 0; level < levels_; ++level) {
+        float max_step = 0;
+        NRB_TRY(InitLevel(level, max_step));
+        float current_size = max_step;
+        const float smallest_size = max_step / 100.0f;
+        UpdateBestObjFunctionValue();
+        if (p_.verbose)
+            printf("[nrb] level %d/%d grid %dx%dx%d, initial objective %.6f = (wSIM)%.6f - (wBE)%.6g\n", level + 1,
+                   levels_, grid_.dim[0], grid_.dim[1], grid_.dim[2], best_obj_, best_w_measure_, best_w_be_);
+        bool just_restarted = false;
+        while (current_size) {
+            if (it_ >= max_it_) break;
+            NRB_TRY(GetObjectiveFunctionGradient());
+            current_size = std::min(current_size, max_step);
+            NRB_TRY(Optimise(max_step, smallest_size, current_size));
+            if (p_.verbose)
+                printf("[nrb] [%zu] objective %.6f = (wSIM)%.6f - (wBE)%.6g [+ %g mm]\n", it_, best_obj_,
+                       best_w_measure_, best_w_be_, current_size);
+            // _reg_base.cpp:784-793: one restart to steepest descent on a stalled line search
+            if (current_size == 0) {
+                if (!just_restarted && it_ < max_it_) {
+                    first_call_ = true;
+                    current_size = max_step;
+                    just_restarted = true;
+                }
+            } else {
+                just_restarted = false;
+            }
+        }
+        max_it_ /= 2;
+    }
+    const int64_t n = 3 * nc_;
+    if (cpp_out) {
+        if (cap < n) return fail(NRB_ERR_INVALID, "registration: cpp_out capacity too small");
+        NRB_CUDA(cudaMemcpyAsync(cpp_out, cur_.p, n * sizeof(float), cudaMemcpyDefault, st_));
+    }
+    NRB_CUDA(cudaFreeAsync(obj_, st_));
+    obj_ = nullptr;
+    NRB_CUDA(cudaStreamSynchronize(st_));
+    if (res) {
+        for (int i = 0; i < 3; ++i) res->cpp_dim[i] = grid_.dim[i];
+        res->final_nmi = best_nmi_;
+        res->final_be = best_be_;
+        res->final_objective = best_obj_;
+        res->objective_evaluations = n_obj_;
+        res->gradient_evaluations = n_grad_;
+        res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return NRB_OK;
+}
+
+}  // namespace
+}  // namespace nrb
+
+using namespace nrb;
+
+extern "C" void nrb_f3d_default_params(nrb_f3d_params *p) {
+    if (!p) return;
+    p->levels = 3;
+    p->max_iterations = 150;
+    p->bending_energy = 0.001f;
+    p->spacing[0] = -5.f;
+    p->spacing[1] = std::numeric_limits<float>::quiet_NaN();
+    p->spacing[2] = std::numeric_limits<float>::quiet_NaN();
+    p->ref_bins = 64;
+    p->flo_bins = 64;
+    p->padding = std::numeric_limits<float>::quiet_NaN();
+    p->verbose = 0;
+}
+
+extern "C" nrb_status nrb_f3d_grid_dims(const int32_t ref_dim[3], const float ref_pixdim[3], const nrb_f3d_params *p,
+                                        int32_t cpp_dim_out[3]) {
+    if (!ref_dim || !ref_pixdim || !p || !cpp_dim_out) return fail(NRB_ERR_INVALID, "nrb_f3d_grid_dims: null pointer");
+    for (int i = 0; i < 3; ++i) {
+        float s = p->spacing[i];
+        if (s != s) s = p->spacing[0];
+        const float mm = s < 0 ? s * -ref_pixdim[i] : s;
+        cpp_dim_out[i] = ceil_ref((float)ref_dim[i] * ref_pixdim[i] / mm + 3.f);
+    }
+    return NRB_OK;
+}
+
+static nrb_status check_register_args(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3],
+                                      const nrb_f3d_params *p) {
+    if (!ref || !flo || !dim || !pixdim || !p) return fail(NRB_ERR_INVALID, "registration: null pointer");
+    for (int i = 0; i < 3; ++i)
+        if (dim[i] < 2 || !(pixdim[i] > 0)) return fail(NRB_ERR_INVALID, "registration: 3D volumes with positive voxel size expected");
+    return NRB_OK;
+}
+
+extern "C" nrb_status nrb_f3d_register_device(const float *ref, const float *flo, const int32_t dim[3],
+                                              const float pixdim[3], const nrb_f3d_params *p, float *cpp_out,
+                                              int64_t cpp_capacity, nrb_f3d_result *result, void *stream) {
+    NRB_TRY(check_register_args(ref, flo, dim, pixdim, p));
+    F3dRegistration reg(*p, as_stream(stream));
+    return reg.Run(ref, flo, dim, pixdim, cpp_out, cpp_capacity, result);
+}
+
+extern "C" nrb_status nrb_f3d_register_host(const float *ref_host, const float *flo_host, const int32_t dim[3],
+                                            const float pixdim[3], const nrb_f3d_params *p, float *cpp_out_host,
+                                            int64_t cpp_capacity, nrb_f3d_result *result) {
+    NRB_TRY(check_register_args(ref_host, flo_host, dim, pixdim, p));
+    const auto t0 = std::chrono::steady_clock::now();
+    cudaStream_t st = nullptr;
+    NRB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    nrb_status s;
+    {
+        F3dRegistration reg(*p, st);
+        // the pyramid's finest level is copied straight from the host buffers
+        s = reg.Run(ref_host, flo_host, dim, pixdim, cpp_out_host, cpp_capacity, result);
+    }
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (s == NRB_OK && result)
+        result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return s;
+}

@@ -1,0 +1,84 @@
+// Device-side state objects behind the opaque handles of the C ABI.
+#pragma once
+
+#include <vector>
+
+#include "nrb_common.cuh"
+
+// Fixed number of partial sums every reduction in this library produces before its final
+// fixed-order pass; it bounds the grid of the reduction kernels so results never depend on the
+// device's SM count.
+constexpr int NRB_RED_BLOCKS = 512;
+constexpr int NRB_RED_THREADS = 256;
+
+// One NMI measure: histogram counts (kept zero between evaluations), FP64 tables, entropies.
+struct nrb_nmi {
+    int rb = 0, fb = 0;            // internal bin counts (user bins + 4)
+    int total = 0;                 // rb*fb + rb + fb
+    uint32_t *hist = nullptr;      // rb*fb joint counts
+    double *pro = nullptr;         // total: smoothed, normalised joint | ref marginal | flo marginal
+    double *logt = nullptr;        // total: log of pro (0 where pro == 0)
+    nrb_objective *last = nullptr; // entropies / NMI of the last evaluation
+    int device = 0;
+};
+
+// Per-axis description of where the node sampling of Compute::VoxelCentricToNodeCentric reads
+// the convolved voxel gradient: the sorted distinct voxel indices ("samples") and, per node,
+// up to two (sample slot, trilinear weight) taps.
+struct AxisSampling {
+    int nsamples = 0;
+    std::vector<int> samples;       // voxel index of each slot
+    std::vector<int> tap_slot;      // 2 per node (-1 = no tap)
+    std::vector<float> tap_weight;  // 2 per node
+    std::vector<float> kernel;      // cubic kernel taps, 2*radius+1
+    int radius = 0;
+};
+
+struct nrb_workspace {
+    nrb_geometry g{};
+    int device = 0;
+    // reduction partials (double pairs) and scalars
+    double *red = nullptr;          // 2 * NRB_RED_BLOCKS doubles
+    double *be_partials = nullptr;  // NRB_RED_BLOCKS doubles
+    float *fred = nullptr;          // NRB_RED_BLOCKS floats (max / min partials)
+    // bending-energy gradient: 18 derivative values per node
+    float *be_deriv = nullptr;
+    // convolution-at-nodes scratch
+    AxisSampling ax[3];
+    int *d_samples[3] = { nullptr, nullptr, nullptr };
+    int *d_tap_slot[3] = { nullptr, nullptr, nullptr };
+    float *d_tap_weight[3] = { nullptr, nullptr, nullptr };
+    float *d_kernel[3] = { nullptr, nullptr, nullptr };
+    float *conv1 = nullptr;         // [3][nz][ny][nsx]
+    float *conv2 = nullptr;         // [3][nz][nsy][nsx]
+    // fused voxel pass geometry
+    int span[3] = { 0, 0, 0 };      // max control-point span of a voxel tile per axis
+    size_t bytes = 0;
+};
+
+namespace nrb {
+
+// Voxel tile of the fused kernels: 32 (x) by 4 (y) by 4 (z) voxels, 128 threads.
+constexpr int TILE_X = 32, TILE_Y = 4, TILE_Z = 4, TILE_THREADS = 128;
+
+nrb_status workspace_init(nrb_workspace *ws, const nrb_geometry *g);
+void workspace_free(nrb_workspace *ws);
+nrb_status validate_geometry(const nrb_geometry *g);
+
+// launchers shared between translation units
+nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be_partials,
+                               int64_t cpp_nvox3, double sim_weight, double be_weight,
+                               nrb_objective *obj, cudaStream_t st);
+nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
+                                  const float *ref, const float *flo, const int32_t *mask,
+                                  const float *cpp, float padding, cudaStream_t st);
+nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
+                                 const float *ref, const float *flo, const int32_t *mask,
+                                 const float *cpp, float padding, double weight, float *vgrad,
+                                 cudaStream_t st);
+nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float *cpp,
+                           cudaStream_t st);
+nrb_status launch_convolve_to_nodes(nrb_workspace *ws, const nrb_geometry *g, const float *vgrad,
+                                    float weight, float *node, cudaStream_t st);
+
+}  // namespace nrb

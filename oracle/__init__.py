@@ -180,7 +180,7 @@ class Ref:
                                for n, p in zip(dim, pix)])) + 64
         cpp = np.zeros(cap, np.float32)
         cdim = np.zeros(3, np.int32)
-        stats = np.zeros(5, np.float64)
+        stats = np.zeros(5 + 3 * int(levels), np.float64)
         rc = self.lib.ref_f3d_register(_f(_f3(ref)), _f(_f3(flo)), _i(_i3(dim)), _f(_f3(pix)),
                                        _f(_m(xyz)), _d(params), _i(cdim), _f(cpp),
                                        ctypes.c_size_t(cap), _d(stats))

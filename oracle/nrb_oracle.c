@@ -13,9 +13,11 @@
 
 static size_t nvox3(const int d[3]) { return (size_t)d[0] * d[1] * d[2]; }
 
+/* Mat44Mul, reg-lib/cpu/Maths.hpp:272-286: evaluated in double, rounded to float */
 static void mat44_apply(const float m[16], const float in[3], float out[3]) {
     for (int i = 0; i < 3; ++i)
-        out[i] = m[4 * i + 0] * in[0] + m[4 * i + 1] * in[1] + m[4 * i + 2] * in[2] + m[4 * i + 3];
+        out[i] = (float)((double)m[4 * i + 0] * in[0] + (double)m[4 * i + 1] * in[1]
+                         + (double)m[4 * i + 2] * in[2] + (double)m[4 * i + 3]);
 }
 
 /* reg-lib/cpu/_reg_splineBasis.cpp:17-26 */

@@ -85,9 +85,19 @@ public:
     ShimF3d(): reg_f3d<float>(1, 1) {}
     double GetObjectiveFunctionValue() override { ++objCalls; return reg_f3d<float>::GetObjectiveFunctionValue(); }
     void GetObjectiveFunctionGradient() override { ++gradCalls; reg_f3d<float>::GetObjectiveFunctionGradient(); }
+    // marks the start of every pyramid level for the per-level statistics
+    float InitCurrentLevel(int level) override {
+        if (level >= 0) marks.push_back({ std::chrono::steady_clock::now(), objCalls, gradCalls });
+        return reg_f3d<float>::InitCurrentLevel(level);
+    }
     double FinalWMeasure() const { return this->bestWMeasure; }
     double FinalWBE() const { return bestWBE; }
     double SimilarityWeight() const { return this->similarityWeight; }
+    struct Mark {
+        std::chrono::steady_clock::time_point t;
+        long obj, grad;
+    };
+    std::vector<Mark> marks;
     long objCalls = 0, gradCalls = 0;
 };
 
@@ -283,7 +293,9 @@ int ref_refine_grid(const float *cpp, const int *cdim, const float *cpix, const 
 // params: [0] levels, [1] max iterations (finest level), [2] bending-energy weight,
 //         [3] linear-energy weight, [4] bins, [5] spacing (negative: voxels), [6] verbose
 // stats:  [0] final NMI (best wSIM / similarity weight), [1] final wBE, [2] objective
-//         evaluations, [3] gradient evaluations, [4] wall seconds
+//         evaluations, [3] gradient evaluations, [4] wall seconds, then per level l
+//         [5 + 3l] objective evaluations, [6 + 3l] gradient evaluations, [7 + 3l] seconds
+//         (stats must hold 5 + 3 * levels doubles)
 int ref_f3d_register(const float *ref, const float *flo, const int *dim, const float *pix,
                      const float *xyz, const double *params, int *cdim_out, float *cpp_out,
                      size_t cap, double *stats) {
@@ -316,6 +328,12 @@ int ref_f3d_register(const float *ref, const float *flo, const int *dim, const f
     stats[2] = double(reg.objCalls);
     stats[3] = double(reg.gradCalls);
     stats[4] = std::chrono::duration<double>(t1 - t0).count();
+    reg.marks.push_back({ t1, reg.objCalls, reg.gradCalls });
+    for (size_t l = 0; l + 1 < reg.marks.size(); ++l) {
+        stats[5 + 3 * l] = double(reg.marks[l + 1].obj - reg.marks[l].obj);
+        stats[6 + 3 * l] = double(reg.marks[l + 1].grad - reg.marks[l].grad);
+        stats[7 + 3 * l] = std::chrono::duration<double>(reg.marks[l + 1].t - reg.marks[l].t).count();
+    }
     return 0;
 }
 

@@ -1,0 +1,53 @@
+"""The C ABI: the shared library builds for sm_100a, loads without a GPU, exports every
+function include/niftyreg_b200.h declares, and host-only entry points behave."""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+import niftyreg_b200 as nrb
+from tests.helpers import ROOT, ensure_built
+
+
+def declared_functions():
+    text = open(os.path.join(ROOT, "include", "niftyreg_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nrb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    ensure_built()
+    lib = nrb.lib()
+    names = declared_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_library_is_sm100a_only():
+    ensure_built()
+    out = os.popen(f"/usr/local/cuda/bin/cuobjdump --list-elf {nrb.LIB_PATH} 2>/dev/null").read()
+    archs = set(re.findall(r"sm_(\d+a?)", out))
+    assert archs == {"100a"}, archs
+
+
+def test_host_entry_points_without_gpu():
+    ensure_built()
+    p = nrb.default_params()
+    assert p.levels == 3 and p.max_iterations == 150 and abs(p.bending_energy - 0.001) < 1e-9
+    assert np.isnan(p.padding) and p.ref_bins == 64
+    p = nrb.default_params(spacing=(-5.0,))
+    # reg_createControlPointGrid: ceil(n * d / s + 3)
+    assert nrb.grid_dims((182, 218, 182), (1.0, 1.0, 1.0), p) == [40, 47, 40]
+    assert nrb.grid_dims((64, 64, 64), (1.0, 1.0, 1.0), p) == [16, 16, 16]
+    assert nrb.grid_dims((512, 512, 320), (0.8, 0.8, 1.5), nrb.default_params(spacing=(10.0,))) == [44, 44, 51]
+
+
+def test_invalid_arguments_are_reported():
+    ensure_built()
+    lib = nrb.lib()
+    out = ctypes.c_void_p()
+    assert lib.nrb_nmi_create(2, 68, ctypes.byref(out)) == 1  # NRB_ERR_INVALID
+    assert b"bins" in lib.nrb_last_error()
+    assert lib.nrb_get_deformation_field(None, None, None, None, None) == 1
