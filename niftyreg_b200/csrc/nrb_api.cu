@@ -113,6 +113,12 @@ extern "C" void nrb_timing_enable(int on) {
     std::lock_guard<std::mutex> lock(g_tmu);
     resolve_pending();
     if (on) {
+        // events are created here, never between a timed launch's two records
+        while (g_pool.size() < 16384) {
+            cudaEvent_t e = nullptr;
+            if (cudaEventCreate(&e) != cudaSuccess) break;
+            g_pool.push_back(e);
+        }
         for (int k = 0; k < TK_COUNT; ++k) {
             g_tlaunch[k] = 0;
             g_tms[k] = 0;

@@ -61,7 +61,8 @@ __device__ double block_sum_d(double v, double *red) {
 
 // reg_spline_approxBendingEnergyValue3D (reg-lib/cpu/_reg_localTrans_regul.cpp:72-153): per
 // interior node the 6 second derivatives of each component from 27-point stencils of the
-// positions, summed squares (cross terms doubled) accumulated in double.
+// positions, summed squares (cross terms doubled) accumulated in double. The stencil sums use
+// the reference's order without contraction: each node's terms are bit-identical to the CPU's.
 __global__ void __launch_bounds__(NRB_RED_THREADS)
 k_be_value(int cx, int cy, int cz, const float *__restrict__ cpp, BeBasis B,
            double *__restrict__ partials) {
@@ -89,17 +90,20 @@ k_be_value(int cx, int cy, int cz, const float *__restrict__ cpp, BeBasis B,
                     for (int k = 0; k < 3; ++k) {
                         const float v = __ldg(&cpp[k * nc + idx]);
 #pragma unroll
-                        for (int t = 0; t < 6; ++t) d[k][t] = fmaf(B.v[t][i], v, d[k][t]);
+                        for (int t = 0; t < 6; ++t) d[k][t] = __fadd_rn(d[k][t], __fmul_rn(B.v[t][i], v));
                     }
                 }
-        double s = (double)(d[0][0] * d[0][0] + d[0][1] * d[0][1] + d[0][2] * d[0][2])
-                   + 2.0 * (double)(d[0][3] * d[0][3] + d[0][4] * d[0][4] + d[0][5] * d[0][5]);
+        // the reference expression's order: the first three squares summed in float, every
+        // later term added in double
+        auto sq = [](float v) { return __fmul_rn(v, v); };
+        auto sum3 = [&](int k, int t) { return __fadd_rn(__fadd_rn(sq(d[k][t]), sq(d[k][t + 1])), sq(d[k][t + 2])); };
+        double s = __dadd_rn((double)sum3(0, 0), __dmul_rn(2.0, (double)sum3(0, 3)));
 #pragma unroll
         for (int k = 1; k < 3; ++k) {
-            s += (double)(d[k][0] * d[k][0]);
-            s += (double)(d[k][1] * d[k][1]);
-            s += (double)(d[k][2] * d[k][2]);
-            s += 2.0 * (double)(d[k][3] * d[k][3] + d[k][4] * d[k][4] + d[k][5] * d[k][5]);
+            s = __dadd_rn(s, (double)sq(d[k][0]));
+            s = __dadd_rn(s, (double)sq(d[k][1]));
+            s = __dadd_rn(s, (double)sq(d[k][2]));
+            s = __dadd_rn(s, __dmul_rn(2.0, (double)sum3(k, 3)));
         }
         acc += s;
     }
@@ -151,7 +155,7 @@ __global__ void k_be_derivatives(int cx, int cy, int cz, Mat34 M, const float *_
                     for (int k = 0; k < 3; ++k) {
                         const float v = __fsub_rn(__ldg(&cpp[k * nc + idx]), identity_pos(M, k, X, Y, Z));
 #pragma unroll
-                        for (int t = 0; t < 6; ++t) d[k][t] = fmaf(B.v[t][i], v, d[k][t]);
+                        for (int t = 0; t < 6; ++t) d[k][t] = __fadd_rn(d[k][t], __fmul_rn(B.v[t][i], v));
                     }
                 }
 #pragma unroll
@@ -185,10 +189,10 @@ __global__ void k_be_accumulate(int cx, int cy, int cz, const float *__restrict_
 #pragma unroll
                     for (int t = 0; t < 6; ++t)
 #pragma unroll
-                        for (int k = 0; k < 3; ++k) g[k] = fmaf(__ldg(&der[(3 * t + k) * nc + j]), B.v[t][a], g[k]);
+                        for (int k = 0; k < 3; ++k) g[k] = __fadd_rn(g[k], __fmul_rn(__ldg(&der[(3 * t + k) * nc + j]), B.v[t][a]));
                 }
 #pragma unroll
-        for (int k = 0; k < 3; ++k) grad[k * nc + n] = fmaf(ratio, g[k], grad[k * nc + n]);
+        for (int k = 0; k < 3; ++k) grad[k * nc + n] = __fadd_rn(grad[k * nc + n], __fmul_rn(ratio, g[k]));
     }
 }
 
@@ -621,6 +625,9 @@ static std::vector<float> cubic_kernel(float spacing_mm, float pixdim, int& radi
 }
 
 nrb_status validate_geometry(const nrb_geometry *g) {
+    // voxel and node indices are 32-bit in the kernels
+    if (nvox(g->ref_dim) >= (1LL << 31) / 3 || nvox(g->flo_dim) >= (1LL << 31) || nvox(g->cpp_dim) >= (1LL << 31) / 3)
+        return fail(NRB_ERR_UNSUPPORTED, "geometry: volume too large for 32-bit indexing");
     for (int d = 0; d < 3; ++d) {
         if (g->ref_dim[d] <= 0 || g->flo_dim[d] <= 0 || g->cpp_dim[d] <= 0)
             return fail(NRB_ERR_INVALID, "geometry: non-positive dimension");
@@ -704,13 +711,32 @@ static nrb_status upload(T *&dst, const std::vector<T>& src, size_t& bytes) {
     return NRB_OK;
 }
 
-nrb_status workspace_init(nrb_workspace *ws, const nrb_geometry *g) {
-    ws->g = *g;
+// Items of the voxel walk: enough z-chunks that the persistent blocks get several items each
+// (load balance), but chunks of at least 8 slices so the staged control points are reused.
+WalkPlan plan_walk(const nrb_geometry *g) {
+    WalkPlan p;
+    const int nx = g->ref_dim[0], ny = g->ref_dim[1], nz = g->ref_dim[2];
     const float gs[3] = { g->cpp_pixdim[0] / g->ref_pixdim[0], g->cpp_pixdim[1] / g->ref_pixdim[1],
                           g->cpp_pixdim[2] / g->ref_pixdim[2] };
-    ws->span[0] = tile_span(g->ref_dim[0], TILE_X, gs[0]);
-    ws->span[1] = tile_span(g->ref_dim[1], TILE_Y, gs[1]);
-    ws->span[2] = tile_span(g->ref_dim[2], TILE_Z, gs[2]);
+    p.tiles_x = (nx + COL_X - 1) / COL_X;
+    p.tiles_y = (ny + COL_Y - 1) / COL_Y;
+    const long long xy = (long long)p.tiles_x * p.tiles_y;
+    const long long want = 12LL * sm_count();
+    int chunks = (int)std::max<long long>(1, (want + xy - 1) / xy);
+    chunks = std::min(chunks, std::max(1, nz / 8));
+    p.zchunk = (nz + chunks - 1) / chunks;
+    p.nchunks = (nz + p.zchunk - 1) / p.zchunk;
+    p.nitems = (int)(xy * p.nchunks);
+    p.sa = tile_span(nx, COL_X, gs[0]);
+    p.sb = tile_span(ny, COL_Y, gs[1]);
+    p.sc = tile_span(nz, p.zchunk, gs[2]);
+    p.cp_floats = 3 * p.sa * p.sb * p.sc;
+    return p;
+}
+
+nrb_status workspace_init(nrb_workspace *ws, const nrb_geometry *g) {
+    ws->g = *g;
+    ws->walk = plan_walk(g);
     return NRB_OK;
 }
 

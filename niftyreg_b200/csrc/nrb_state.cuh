@@ -11,6 +11,23 @@
 constexpr int NRB_RED_BLOCKS = 512;
 constexpr int NRB_RED_THREADS = 256;
 
+namespace nrb {
+
+// Work decomposition of the voxel passes: an item is a column of COL_X x COL_Y voxels over a
+// chunk of `zchunk` slices; a 128-thread block stages the item's control points once and each
+// thread walks its voxel column along z.
+constexpr int COL_X = 32, COL_Y = 4, COL_THREADS = COL_X * COL_Y;
+constexpr int HIST_CLUSTER = 8;  // blocks whose shared-memory histograms merge through DSMEM
+
+struct WalkPlan {
+    int tiles_x = 0, tiles_y = 0, zchunk = 0, nchunks = 0, nitems = 0;
+    int sa = 0, sb = 0, sc = 0;  // max control-point span of an item along x, y, z
+    int cp_floats = 0;           // shared floats of the staged control-point block
+};
+WalkPlan plan_walk(const nrb_geometry *g);
+
+}  // namespace nrb
+
 // One NMI measure: histogram counts (kept zero between evaluations), FP64 tables, entropies.
 struct nrb_nmi {
     int rb = 0, fb = 0;            // internal bin counts (user bins + 4)
@@ -37,10 +54,11 @@ struct AxisSampling {
 struct nrb_workspace {
     nrb_geometry g{};
     int device = 0;
+    nrb::WalkPlan walk;
     // reduction partials (double pairs) and scalars
     double *red = nullptr;          // 2 * NRB_RED_BLOCKS doubles
     double *be_partials = nullptr;  // NRB_RED_BLOCKS doubles
-    float *fred = nullptr;          // NRB_RED_BLOCKS floats (max / min partials)
+    float *fred = nullptr;          // 2 * NRB_RED_BLOCKS floats (min | max partials)
     // bending-energy gradient: 18 derivative values per node
     float *be_deriv = nullptr;
     // convolution-at-nodes scratch
@@ -51,15 +69,10 @@ struct nrb_workspace {
     float *d_kernel[3] = { nullptr, nullptr, nullptr };
     float *conv1 = nullptr;         // [3][nz][ny][nsx]
     float *conv2 = nullptr;         // [3][nz][nsy][nsx]
-    // fused voxel pass geometry
-    int span[3] = { 0, 0, 0 };      // max control-point span of a voxel tile per axis
     size_t bytes = 0;
 };
 
 namespace nrb {
-
-// Voxel tile of the fused kernels: 32 (x) by 4 (y) by 4 (z) voxels, 128 threads.
-constexpr int TILE_X = 32, TILE_Y = 4, TILE_Z = 4, TILE_THREADS = 128;
 
 nrb_status workspace_init(nrb_workspace *ws, const nrb_geometry *g);
 void workspace_free(nrb_workspace *ws);

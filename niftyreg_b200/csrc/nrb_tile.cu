@@ -1,30 +1,45 @@
 // Voxel-pass kernels of the F3D objective and gradient.
 //
-// Every kernel here walks the reference volume in 32x4x4-voxel tiles. For a tile, the block of
-// control points its voxels depend on is staged in shared memory and the cubic B-spline sum
-// sum_{a,b,c} Bx_a By_b Bz_c CP is evaluated separably (z, then y, then x), about 21 FMAs per
-// voxel instead of 192. The deformation field never leaves the SM in the fused kernels: it is
-// consumed at once by the trilinear warp, the joint histogram (objective) or the spatial
-// gradient and NMI voxel gradient (gradient).
+// Work item: a column of 32 (x) by 4 (y) reference voxels over a chunk of z slices. The block
+// stages the control points the item depends on in shared memory once (asynchronous copies),
+// together with the z basis of every slice of the chunk; then every thread walks its own voxel
+// column along z. The cubic B-spline sum sum_{a,b,c} Bx_a By_b Bz_c CP is evaluated
+// separably: for each node plane k the thread contracts the 4x4 (a, b) neighbourhood with its
+// fixed x/y weights into S(k) (20 FMAs per component), keeps a rolling window of the four planes
+// the current slice needs, and contracts z with 4 FMAs per component. z is uniform across the
+// block, so the window shifts without divergence and the walk needs no barrier.
+//
+// The deformation field never leaves the SM in the fused kernels: it is consumed at once by the
+// trilinear warp and then by the joint histogram (objective) or by the spatial gradient and the
+// NMI voxel gradient (gradient). Blocks are persistent; in the objective kernel they run in
+// clusters of 8 that merge their shared-memory histograms through distributed shared memory
+// before one flush per cluster.
+#include <cooperative_groups.h>
+#include <cuda_pipeline.h>
+
 #include <cfloat>
+#include <climits>
 #include <cmath>
 
 #include "nrb_state.cuh"
 
+namespace cg = cooperative_groups;
+
 namespace nrb {
 
-struct TileParams {
+struct WalkParams {
     int nx, ny, nz;          // reference / deformation-field dims
     int cx, cy, cz;          // control-point grid dims
     float gsx, gsy, gsz;     // grid spacing in reference voxels (grid pixdim / ref pixdim)
-    int sa, sb, sc;          // shared-memory strides: max node span of a tile per axis
-    int tiles_x, tiles_y, tiles_z, ntiles;
+    int tiles_x, tiles_y, zchunk, nitems;
+    int sa, sb, sc;          // shared strides of the staged block (max spans)
     int fnx, fny, fnz;       // floating dims
     Mat34 flo_ijk;           // mm -> floating voxel
+    int flo_diag;            // flo_ijk has no off-diagonal terms
     float pad;               // padding value of out-of-volume taps
     int rb, fb;              // internal bin counts
-    int tile_floats;         // shared floats used by the tile machinery
-    long long cnv;           // control points per component
+    int cnv;                 // control points per component
+    int log_in_smem;         // gradient: the FP64 log table is staged in shared memory
 };
 
 __device__ __forceinline__ int pre_of(int v, float gs) { return (int)((float)v / gs); }
@@ -34,145 +49,151 @@ __device__ __forceinline__ float frac_of(int v, float gs, int pre) {
     return t < 0.f ? 0.f : t;
 }
 
-// Shared-memory layout of one tile (in floats):
-//   cp  [3][sc][sb][sa]  control points minus the tile offset; later reused for
-//   r   [3][TZ][TY][sa]  the y- and z-contracted sums
-//   q   [3][TZ][sb][sa]  the z-contracted sums
-//   bz[TZ][4], by[TY][4], zo[TZ], yo[TY], off[3]
-__host__ __device__ inline int tile_smem_floats(int sa, int sb, int sc) {
-    return 3 * sc * sb * sa + 3 * TILE_Z * sb * sa + TILE_Z * 4 + TILE_Y * 4 + TILE_Z + TILE_Y + 4;
-}
+// shared floats of the per-item tables: z basis [zchunk][4] and z node index [zchunk]
+__host__ __device__ inline int walk_table_floats(int zchunk) { return 5 * zchunk; }
 
-struct TileCtx {
-    int x0, y0, z0, xa0, yb0, zc0;
+struct Item {
+    int x0, y0, z0, z1, xa0, yb0, zc0;
+    float off[3];
 };
 
-// Stages the control points of `tile` and leaves the y/z-contracted sums r[c][z'][y'][a] and
-// the offsets in shared memory. Must be called by all threads of the block.
-__device__ void tile_positions(const TileParams& P, const float *__restrict__ cpp, int tile,
-                               float *sm, TileCtx& T) {
-    const int tid = threadIdx.x;
-    const int tx = tile % P.tiles_x;
-    const int t2 = tile / P.tiles_x;
-    const int ty = t2 % P.tiles_y;
-    const int tz = t2 / P.tiles_y;
-    T.x0 = tx * TILE_X;
-    T.y0 = ty * TILE_Y;
-    T.z0 = tz * TILE_Z;
-    T.xa0 = pre_of(T.x0, P.gsx);
-    T.yb0 = pre_of(T.y0, P.gsy);
-    T.zc0 = pre_of(T.z0, P.gsz);
-    const int na = pre_of(min(T.x0 + TILE_X - 1, P.nx - 1), P.gsx) + 4 - T.xa0;
-    const int nb = pre_of(min(T.y0 + TILE_Y - 1, P.ny - 1), P.gsy) + 4 - T.yb0;
-    const int nc = pre_of(min(T.z0 + TILE_Z - 1, P.nz - 1), P.gsz) + 4 - T.zc0;
-
-    float *cp = sm;
-    float *q = sm + 3 * P.sc * P.sb * P.sa;
-    float *bz = q + 3 * TILE_Z * P.sb * P.sa;
-    float *by = bz + TILE_Z * 4;
-    int *zo = reinterpret_cast<int *>(by + TILE_Y * 4);
-    int *yo = zo + TILE_Z;
-    float *off = reinterpret_cast<float *>(yo + TILE_Y);
-
-    __syncthreads();  // the previous tile's readers are done with r / off
-    const long long cnv = P.cnv;
-    if (tid < 3) off[tid] = __ldg(&cpp[tid * cnv + ((long long)T.zc0 * P.cy + T.yb0) * P.cx + T.xa0]);
-    if (tid >= 32 && tid < 32 + TILE_Z) {
-        const int zp = tid - 32, z = T.z0 + zp;
-        const int pre = pre_of(min(z, P.nz - 1), P.gsz);
-        zo[zp] = pre - T.zc0;
-        bspline_basis(frac_of(min(z, P.nz - 1), P.gsz, pre), bz + 4 * zp);
-    }
-    if (tid >= 64 && tid < 64 + TILE_Y) {
-        const int yp = tid - 64, y = T.y0 + yp;
-        const int pre = pre_of(min(y, P.ny - 1), P.gsy);
-        yo[yp] = pre - T.yb0;
-        bspline_basis(frac_of(min(y, P.ny - 1), P.gsy, pre), by + 4 * yp);
-    }
-    __syncthreads();
-    // stage the control-point block (relative to the tile offset, which keeps the magnitudes
-    // of the partial sums small)
-    const int ncp = 3 * nc * nb * na;
-    for (int i = tid; i < ncp; i += TILE_THREADS) {
-        const int ia = i % na;
-        int rest = i / na;
-        const int jb = rest % nb;
-        rest /= nb;
-        const int kc = rest % nc;
-        const int c = rest / nc;
-        const float v = __ldg(&cpp[c * cnv + ((long long)(T.zc0 + kc) * P.cy + (T.yb0 + jb)) * P.cx + T.xa0 + ia]);
-        cp[((c * P.sc + kc) * P.sb + jb) * P.sa + ia] = v - off[c];
-    }
-    __syncthreads();
-    // z contraction
-    const int nq = 3 * TILE_Z * nb * na;
-    for (int i = tid; i < nq; i += TILE_THREADS) {
-        const int ia = i % na;
-        int rest = i / na;
-        const int jb = rest % nb;
-        rest /= nb;
-        const int zp = rest % TILE_Z;
-        const int c = rest / TILE_Z;
-        const float *src = cp + ((c * P.sc + zo[zp]) * P.sb + jb) * P.sa + ia;
-        const float *w = bz + 4 * zp;
-        const int st = P.sb * P.sa;
-        float s = w[0] * src[0];
-        s = fmaf(w[1], src[st], s);
-        s = fmaf(w[2], src[2 * st], s);
-        s = fmaf(w[3], src[3 * st], s);
-        q[((c * TILE_Z + zp) * P.sb + jb) * P.sa + ia] = s;
-    }
-    __syncthreads();
-    // y contraction into r (aliases cp, which is dead now)
-    float *r = cp;
-    const int nr = 3 * TILE_Z * TILE_Y * na;
-    for (int i = tid; i < nr; i += TILE_THREADS) {
-        const int ia = i % na;
-        int rest = i / na;
-        const int yp = rest % TILE_Y;
-        rest /= TILE_Y;
-        const int zp = rest % TILE_Z;
-        const int c = rest / TILE_Z;
-        const float *src = q + ((c * TILE_Z + zp) * P.sb + yo[yp]) * P.sa + ia;
-        const float *w = by + 4 * yp;
-        float s = w[0] * src[0];
-        s = fmaf(w[1], src[P.sa], s);
-        s = fmaf(w[2], src[2 * P.sa], s);
-        s = fmaf(w[3], src[3 * P.sa], s);
-        r[((c * TILE_Z + zp) * TILE_Y + yp) * P.sa + ia] = s;
-    }
-    __syncthreads();
-}
-
-__device__ __forceinline__ const float *tile_offsets(const TileParams& P, const float *sm) {
-    const float *q = sm + 3 * P.sc * P.sb * P.sa;
-    const float *bz = q + 3 * TILE_Z * P.sb * P.sa;
-    return bz + TILE_Z * 4 + TILE_Y * 4 + TILE_Z + TILE_Y;
-}
-
-// Final x contraction for voxel (lx, ly, zp) of the tile: world position in mm.
-__device__ __forceinline__ void voxel_position(const TileParams& P, const float *sm,
-                                               const float *off, int ly, int zp, int xo,
-                                               const float bx[4], float& px, float& py,
-                                               float& pz) {
-    const int cs = TILE_Z * TILE_Y * P.sa;
-    const float *r = sm + (zp * TILE_Y + ly) * P.sa + xo;
-    float s0 = bx[0] * r[0], s1 = bx[0] * r[cs], s2 = bx[0] * r[2 * cs];
+// Stages the control points of `item` relative to the item's first node (which keeps the
+// partial sums small) into cp[3][sc][sb][sa], and the z basis of each slice into the tables.
+// Called by every thread of the block.
+__device__ __forceinline__ void stage_item(const WalkParams& P, const float *__restrict__ cpp, int item,
+                                           float *cp, float *zb, int *zk, Item& I) {
+    const int tx = item % P.tiles_x;
+    const int rest = item / P.tiles_x;
+    const int ty = rest % P.tiles_y;
+    const int tz = rest / P.tiles_y;
+    I.x0 = tx * COL_X;
+    I.y0 = ty * COL_Y;
+    I.z0 = tz * P.zchunk;
+    I.z1 = min(I.z0 + P.zchunk, P.nz);
+    I.xa0 = pre_of(I.x0, P.gsx);
+    I.yb0 = pre_of(I.y0, P.gsy);
+    I.zc0 = pre_of(I.z0, P.gsz);
+    const int na = pre_of(min(I.x0 + COL_X - 1, P.nx - 1), P.gsx) + 4 - I.xa0;
+    const int nb = pre_of(min(I.y0 + COL_Y - 1, P.ny - 1), P.gsy) + 4 - I.yb0;
+    const int nc = pre_of(I.z1 - 1, P.gsz) + 4 - I.zc0;
+    const int first = (I.zc0 * P.cy + I.yb0) * P.cx + I.xa0;
 #pragma unroll
-    for (int t = 1; t < 4; ++t) {
-        s0 = fmaf(bx[t], r[t], s0);
-        s1 = fmaf(bx[t], r[cs + t], s1);
-        s2 = fmaf(bx[t], r[2 * cs + t], s2);
+    for (int c = 0; c < 3; ++c) I.off[c] = __ldg(&cpp[c * P.cnv + first]);
+    const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+    __syncthreads();  // the previous item's readers are done
+    // asynchronous global -> shared copies: no register round trip, all in flight together
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        for (int kc = 0; kc < nc; ++kc)
+            for (int jb = ly; jb < nb; jb += COL_Y) {
+                const float *src = cpp + c * P.cnv + ((I.zc0 + kc) * P.cy + I.yb0 + jb) * P.cx + I.xa0;
+                float *dst = cp + ((c * P.sc + kc) * P.sb + jb) * P.sa;
+                for (int ia = lx; ia < na; ia += 32) __pipeline_memcpy_async(dst + ia, src + ia, sizeof(float));
+            }
+    __pipeline_commit();
+    for (int zi = threadIdx.x; zi < I.z1 - I.z0; zi += COL_THREADS) {
+        const int z = I.z0 + zi;
+        const int pz = pre_of(z, P.gsz);
+        zk[zi] = pz - I.zc0;
+        bspline_basis(frac_of(z, P.gsz, pz), zb + 4 * zi);
     }
-    px = off[0] + s0;
-    py = off[1] + s1;
-    pz = off[2] + s2;
+    __pipeline_wait_prior(0);
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        for (int kc = 0; kc < nc; ++kc)
+            for (int jb = ly; jb < nb; jb += COL_Y) {
+                float *dst = cp + ((c * P.sc + kc) * P.sb + jb) * P.sa;
+                for (int ia = lx; ia < na; ia += 32) dst[ia] -= I.off[c];
+            }
+    __syncthreads();
+}
+
+// Per-thread walker: x/y weights of the thread's column and the rolling window of the four
+// node planes contracted over (a, b).
+struct Column {
+    int x, y;
+    bool inside;     // the column lies inside the reference volume
+    float bx[4], by[4];
+    const float *base;
+    int win;         // relative z node index of S[0]
+    float S[4][3];
+};
+
+__device__ __forceinline__ void column_init(const WalkParams& P, const Item& I, const float *cp, Column& C) {
+    const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+    C.x = I.x0 + lx;
+    C.y = I.y0 + ly;
+    C.inside = C.x < P.nx && C.y < P.ny;
+    const int xc = min(C.x, P.nx - 1), yc = min(C.y, P.ny - 1);
+    const int px = pre_of(xc, P.gsx), py = pre_of(yc, P.gsy);
+    bspline_basis(frac_of(xc, P.gsx, px), C.bx);
+    bspline_basis(frac_of(yc, P.gsy, py), C.by);
+    C.base = cp + (py - I.yb0) * P.sa + (px - I.xa0);
+    C.win = INT_MIN;
+}
+
+// S for relative node plane k
+__device__ __forceinline__ void column_plane(const WalkParams& P, const Column& C, int k, float out[3]) {
+    const int cs = P.sc * P.sb * P.sa;
+    const float *p = C.base + k * P.sb * P.sa;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float *q = p + c * cs;
+        float s = 0.f;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const float *r = q + b * P.sa;
+            float t = C.bx[0] * r[0];
+            t = fmaf(C.bx[1], r[1], t);
+            t = fmaf(C.bx[2], r[2], t);
+            t = fmaf(C.bx[3], r[3], t);
+            s = fmaf(C.by[b], t, s);
+        }
+        out[c] = s;
+    }
+}
+
+// World position (mm) of slice index zi (relative to the item) of the thread's column; zi must
+// not decrease between calls.
+__device__ __forceinline__ void column_position(const WalkParams& P, const Item& I, Column& C, const float *zb,
+                                                const int *zk, int zi, float pos[3]) {
+    const int pz = zk[zi];
+    if (pz != C.win) {
+        if (pz == C.win + 1) {
+#pragma unroll
+            for (int t = 0; t < 3; ++t)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) C.S[t][c] = C.S[t + 1][c];
+            column_plane(P, C, pz + 3, C.S[3]);
+        } else {
+#pragma unroll
+            for (int t = 0; t < 4; ++t) column_plane(P, C, pz + t, C.S[t]);
+        }
+        C.win = pz;
+    }
+    const float *bz = zb + 4 * zi;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float s = bz[0] * C.S[0][c];
+        s = fmaf(bz[1], C.S[1][c], s);
+        s = fmaf(bz[2], C.S[2][c], s);
+        s = fmaf(bz[3], C.S[3][c], s);
+        pos[c] = I.off[c] + s;
+    }
 }
 
 // mm -> floating voxel as Mat44Mul does it (reg-lib/cpu/Maths.hpp:272-286): the products of
-// two floats are exact in double, the sum is rounded once to double and then to float.
-__device__ __forceinline__ void to_floating_voxel(const Mat34& M, float x, float y, float z,
+// two floats are exact in double, so one rounding to double and one to float. With no
+// off-diagonal terms the zero products are skipped (adding exact zeros changes nothing).
+__device__ __forceinline__ void to_floating_voxel(const Mat34& M, int diag, float x, float y, float z,
                                                   float& fx, float& fy, float& fz) {
+    if (diag) {
+        fx = (float)fma((double)M.m[0], (double)x, (double)M.m[3]);
+        fy = (float)fma((double)M.m[5], (double)y, (double)M.m[7]);
+        fz = (float)fma((double)M.m[10], (double)z, (double)M.m[11]);
+        return;
+    }
     const double dx = x, dy = y, dz = z;
     fx = (float)((double)M.m[0] * dx + (double)M.m[1] * dy + (double)M.m[2] * dz + (double)M.m[3]);
     fy = (float)((double)M.m[4] * dx + (double)M.m[5] * dy + (double)M.m[6] * dz + (double)M.m[7]);
@@ -180,22 +201,24 @@ __device__ __forceinline__ void to_floating_voxel(const Mat34& M, float x, float
 }
 
 // Trilinear sample of the floating image at world position (x, y, z) with the padding rule of
-// ResampleImage3D (an out-of-volume tap contributes padding * weight) and, when kGrad, the
-// spatial derivative of TrilinearImageGradient (NaN components -> 0).
+// ResampleImage3D (an out-of-volume tap contributes padding * weight, so NaN padding poisons a
+// border voxel even through a zero weight) and, when kGrad, the spatial derivative of
+// TrilinearImageGradient (NaN components -> 0).
 template <bool kGrad>
 __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, int fnx, int fny,
-                                                int fnz, const Mat34& M, float pad, float x,
+                                                int fnz, const Mat34& M, int diag, float pad, float x,
                                                 float y, float z, float& val, float g[3]) {
     float fx, fy, fz;
-    to_floating_voxel(M, x, y, z, fx, fy, fz);
-    const int px = (int)floorf(fx), py = (int)floorf(fy), pz = (int)floorf(fz);
-    const float rx = fx - (float)px, ry = fy - (float)py, rz = fz - (float)pz;
+    to_floating_voxel(M, diag, x, y, z, fx, fy, fz);
+    const float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
+    const int px = (int)flx, py = (int)fly, pz = (int)flz;
+    const float rx = fx - flx, ry = fy - fly, rz = fz - flz;
     const float bx0 = 1.f - rx, by0 = 1.f - ry, bz0 = 1.f - rz;
     float v[2][2][2];
     const bool interior = px >= 0 && py >= 0 && pz >= 0 && px + 1 < fnx && py + 1 < fny && pz + 1 < fnz;
     if (interior) {
-        const float *p = flo + ((long long)pz * fny + py) * fnx + px;
-        const long long sy = fnx, sz = (long long)fnx * fny;
+        const float *p = flo + (pz * fny + py) * fnx + px;
+        const int sy = fnx, sz = fnx * fny;
         v[0][0][0] = __ldg(p);
         v[0][0][1] = __ldg(p + 1);
         v[0][1][0] = __ldg(p + sy);
@@ -213,18 +236,17 @@ __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, i
                 for (int a = 0; a < 2; ++a) {
                     const int X = px + a, Y = py + b, Z = pz + c;
                     const bool in = X >= 0 && X < fnx && Y >= 0 && Y < fny && Z >= 0 && Z < fnz;
-                    v[c][b][a] = in ? __ldg(&flo[((long long)Z * fny + Y) * fnx + X]) : pad;
+                    v[c][b][a] = in ? __ldg(&flo[(Z * fny + Y) * fnx + X]) : pad;
                 }
     }
-    float yv0 = fmaf(v[0][0][1], rx, v[0][0][0] * bx0);
-    float yv1 = fmaf(v[0][1][1], rx, v[0][1][0] * bx0);
+    const float yv0 = fmaf(v[0][0][1], rx, v[0][0][0] * bx0);
+    const float yv1 = fmaf(v[0][1][1], rx, v[0][1][0] * bx0);
     const float zv0 = fmaf(yv1, ry, yv0 * by0);
-    float yw0 = fmaf(v[1][0][1], rx, v[1][0][0] * bx0);
-    float yw1 = fmaf(v[1][1][1], rx, v[1][1][0] * bx0);
+    const float yw0 = fmaf(v[1][0][1], rx, v[1][0][0] * bx0);
+    const float yw1 = fmaf(v[1][1][1], rx, v[1][1][0] * bx0);
     const float zv1 = fmaf(yw1, ry, yw0 * by0);
     val = fmaf(zv1, rz, zv0 * bz0);
     if (kGrad) {
-        // d/dx: (v1 - v0) along x, weighted by y and z; d/dy, d/dz from the x-interpolated rows
         const float dx00 = v[0][0][1] - v[0][0][0], dx01 = v[0][1][1] - v[0][1][0];
         const float dx10 = v[1][0][1] - v[1][0][0], dx11 = v[1][1][1] - v[1][1][0];
         const float gx0 = fmaf(dx01, ry, dx00 * by0), gx1 = fmaf(dx11, ry, dx10 * by0);
@@ -237,78 +259,133 @@ __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, i
     }
 }
 
+constexpr int WALK_GROUP = 2;  // slices per step of the walk: their gathers are in flight together
+
+// shared-memory layout of a walk block: cp block | z basis | z node index | kernel-specific
+struct WalkSmem {
+    float *cp, *zb;
+    int *zk;
+    char *tail;
+};
+
+__device__ __forceinline__ WalkSmem walk_smem(const WalkParams& P, void *base) {
+    WalkSmem s;
+    s.cp = reinterpret_cast<float *>(base);
+    s.zb = s.cp + 3 * P.sc * P.sb * P.sa;
+    s.zk = reinterpret_cast<int *>(s.zb + 4 * P.zchunk);
+    s.tail = reinterpret_cast<char *>(s.zk + P.zchunk);
+    // 16-byte alignment of the tail
+    s.tail = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(s.tail) + 15) & ~uintptr_t(15));
+    return s;
+}
+
+__host__ inline size_t walk_smem_bytes(const WalkPlan& W) {
+    return ((size_t)W.cp_floats + (size_t)walk_table_floats(W.zchunk)) * 4 + 16;
+}
+
 // ---------------------------------------------------------------------------------------------
 // fused objective: deformation + warp + joint histogram
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(TILE_THREADS)
-k_objective(TileParams P, const float *__restrict__ ref, const float *__restrict__ flo,
+__global__ void __launch_bounds__(COL_THREADS, 8)
+k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
             const int32_t *__restrict__ mask, const float *__restrict__ cpp,
             uint32_t *__restrict__ ghist) {
     extern __shared__ float4 sm4[];
-    float *sm = reinterpret_cast<float *>(sm4);
-    uint32_t *h = reinterpret_cast<uint32_t *>(sm + P.tile_floats);
+    const WalkSmem S = walk_smem(P, sm4);
+    uint32_t *h = reinterpret_cast<uint32_t *>(S.tail);
     const int nbins = P.rb * P.fb;
-    for (int i = threadIdx.x; i < nbins; i += TILE_THREADS) h[i] = 0u;
-    const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
-    for (int tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
-        TileCtx T;
-        tile_positions(P, cpp, tile, sm, T);
-        const float *off = tile_offsets(P, sm);
-        const int x = T.x0 + lx, y = T.y0 + ly;
-        const bool xyin = x < P.nx && y < P.ny;
-        float bx[4] = { 0, 0, 0, 0 };
-        int xo = 0;
-        if (xyin) {
-            const int pre = pre_of(x, P.gsx);
-            bspline_basis(frac_of(x, P.gsx, pre), bx);
-            xo = pre - T.xa0;
-        }
-#pragma unroll 1
-        for (int zp = 0; zp < TILE_Z; ++zp) {
-            const int z = T.z0 + zp;
-            int bin = -1;
-            if (xyin && z < P.nz) {
-                const long long idx = ((long long)z * P.ny + y) * P.nx + x;
-                if (mask == nullptr || __ldg(&mask[idx]) > -1) {
-                    float wx, wy, wz, w, g[3];
-                    voxel_position(P, sm, off, ly, zp, xo, bx, wx, wy, wz);
-                    sample_floating<false>(flo, P.fnx, P.fny, P.fnz, P.flo_ijk, P.pad, wx, wy, wz, w, g);
-                    const float rv = __ldg(&ref[idx]);
-                    if (rv == rv && w == w && 0.f <= rv && rv < (float)P.rb && 0.f <= w && w < (float)P.fb)
-                        bin = (int)rv + (int)w * P.rb;
+    for (int i = threadIdx.x; i < nbins; i += COL_THREADS) h[i] = 0u;
+    const int lane = threadIdx.x & 31;
+    const float frb = (float)P.rb, ffb = (float)P.fb;
+    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
+        Item I;
+        stage_item(P, cpp, item, S.cp, S.zb, S.zk, I);
+        Column C;
+        column_init(P, I, S.cp, C);
+        const int nzi = I.z1 - I.z0;
+        int idx = (I.z0 * P.ny + C.y) * P.nx + C.x;
+        const int zstride = P.nx * P.ny;
+        for (int zi = 0; zi < nzi; zi += WALK_GROUP) {
+            int bin[WALK_GROUP];
+#pragma unroll
+            for (int u = 0; u < WALK_GROUP; ++u) {
+                const int zu = min(zi + u, nzi - 1);
+                float pos[3];
+                column_position(P, I, C, S.zb, S.zk, zu, pos);
+                bin[u] = -1;
+                if (C.inside && zi + u < nzi) {
+                    const int vi = idx + u * zstride;
+                    if (mask == nullptr || __ldg(&mask[vi]) > -1) {
+                        float w, g[3];
+                        sample_floating<false>(flo, P.fnx, P.fny, P.fnz, P.flo_ijk, P.flo_diag, P.pad, pos[0], pos[1],
+                                               pos[2], w, g);
+                        const float rv = __ldg(&ref[vi]);
+                        if (rv == rv && w == w && 0.f <= rv && rv < frb && 0.f <= w && w < ffb)
+                            bin[u] = (int)rv + (int)w * P.rb;
+                    }
                 }
             }
-            // warp-aggregated shared-memory increment: one atomic per distinct bin
-            const unsigned peers = __match_any_sync(0xffffffffu, bin);
-            if (bin >= 0 && lx == __ffs(peers) - 1) atomicAdd(&h[bin], (uint32_t)__popc(peers));
+            idx += WALK_GROUP * zstride;
+#pragma unroll
+            for (int u = 0; u < WALK_GROUP; ++u) {
+                // a warp whose 32 voxels share one bin (background) adds 32 with one atomic
+                const int b0 = __shfl_sync(0xffffffffu, bin[u], 0);
+                if (__all_sync(0xffffffffu, bin[u] == b0)) {
+                    if (lane == 0 && b0 >= 0) atomicAdd(&h[b0], 32u);
+                } else if (bin[u] >= 0) {
+                    atomicAdd(&h[bin[u]], 1u);
+                }
+            }
         }
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < nbins; i += TILE_THREADS) {
-        const uint32_t v = h[i];
-        if (v) atomicAdd(&ghist[i], v);
+    // merge the cluster's histograms through distributed shared memory: block r of the cluster
+    // owns bins r, r + 8, r + 16, ... and flushes their sums with one atomic each
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    const int rank = (int)cluster.block_rank();
+    const int nblk = (int)cluster.num_blocks();
+    for (int i = rank + nblk * threadIdx.x; i < nbins; i += nblk * COL_THREADS) {
+        uint32_t s = 0;
+        for (int q = 0; q < nblk; ++q) s += cluster.map_shared_rank(h, q)[i];
+        if (s) atomicAdd(&ghist[i], s);
     }
+    cluster.sync();  // no block leaves while another still reads its shared memory
 }
 
 // Sum over the 4x4 Parzen window of reg_getVoxelBasedNmiGradient3d (_reg_nmi.cpp:548-571):
-// returns refDeriv + warDeriv - nmi * jointDeriv for a unit spatial gradient.
-__device__ __forceinline__ double nmi_window(float rv, float wv, const double *__restrict__ logt,
-                                             int rb, int fb, double nmi) {
+// returns refDeriv + warDeriv - nmi * jointDeriv for a unit spatial gradient. The window's
+// basis values are evaluated once (4 + 4), then its 16 (r, w) pairs are summed in the
+// reference's r-major order.
+__device__ __forceinline__ double nmi_window(float rv, float wv, const double *logt, int rb, int fb, double nmi) {
     const double *rlog = logt + rb * fb;
     const double *wlog = rlog + rb;
-    double sr = 0, sw = 0, sj = 0;
     const int r0 = (int)(rv - 1.f), r1 = (int)(rv + 3.f);
     const int w0 = (int)(wv - 1.f), w1 = (int)(wv + 3.f);
-    for (int r = r0; r < r1; ++r) {
-        if (!(-1 < r && r < rb)) continue;
-        const double br = parzen((double)rv - r);
-        const double rl = __ldg(&rlog[r]);
-        for (int w = w0; w < w1; ++w) {
-            if (!(-1 < w && w < fb)) continue;
-            const double c = br * parzen_deriv((double)wv - w);
+    double br[4], dw[4], wl[4];
+    int wok[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int r = r0 + t, w = w0 + t;
+        const bool rok = r < r1 && -1 < r && r < rb;
+        br[t] = rok ? parzen((double)rv - r) : 0.0;
+        wok[t] = w < w1 && -1 < w && w < fb;
+        dw[t] = wok[t] ? parzen_deriv((double)wv - w) : 0.0;
+        wl[t] = wok[t] ? wlog[w] : 0.0;
+    }
+    double sr = 0, sw = 0, sj = 0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int r = r0 + t;
+        if (!(r < r1 && -1 < r && r < rb)) continue;
+        const double rl = rlog[r];
+        const double *jrow = logt + r;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (!wok[u]) continue;
+            const double c = br[t] * dw[u];
             sr = fma(c, rl, sr);
-            sw = fma(c, __ldg(&wlog[w]), sw);
-            sj = fma(c, __ldg(&logt[r + w * rb]), sj);
+            sw = fma(c, wl[u], sw);
+            sj = fma(c, jrow[(w0 + u) * rb], sj);
         }
     }
     return sr + sw - nmi * sj;
@@ -317,37 +394,40 @@ __device__ __forceinline__ double nmi_window(float rv, float wv, const double *_
 // ---------------------------------------------------------------------------------------------
 // fused gradient: deformation + warp + spatial gradient + NMI voxel gradient
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(TILE_THREADS)
-k_gradient(TileParams P, const float *__restrict__ ref, const float *__restrict__ flo,
+__global__ void __launch_bounds__(COL_THREADS, 4)
+k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
            const int32_t *__restrict__ mask, const float *__restrict__ cpp,
-           const double *__restrict__ logt, const nrb_objective *__restrict__ last,
+           const double *__restrict__ logt_g, const nrb_objective *__restrict__ last,
            double weight, float *__restrict__ vgrad) {
     extern __shared__ float4 sm4[];
-    float *sm = reinterpret_cast<float *>(sm4);
-    const long long nv = (long long)P.nx * P.ny * P.nz;
+    const WalkSmem S = walk_smem(P, sm4);
+    const int nv = P.nx * P.ny * P.nz;
     const double nmi = last->nmi;
     const double scale = weight / (last->entropy[2] * last->entropy[3]);
-    const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
-    for (int tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
-        TileCtx T;
-        tile_positions(P, cpp, tile, sm, T);
-        const float *off = tile_offsets(P, sm);
-        const int x = T.x0 + lx, y = T.y0 + ly;
-        if (x >= P.nx || y >= P.ny) continue;  // no warp-collective operation below
-        const int pre = pre_of(x, P.gsx);
-        float bx[4];
-        bspline_basis(frac_of(x, P.gsx, pre), bx);
-        const int xo = pre - T.xa0;
-#pragma unroll 1
-        for (int zp = 0; zp < TILE_Z; ++zp) {
-            const int z = T.z0 + zp;
-            if (z >= P.nz) break;
-            const long long idx = ((long long)z * P.ny + y) * P.nx + x;
+    const double *logt = logt_g;
+    if (P.log_in_smem) {
+        double *ls = reinterpret_cast<double *>(S.tail);
+        const int total = P.rb * P.fb + P.rb + P.fb;
+        for (int i = threadIdx.x; i < total; i += COL_THREADS) ls[i] = logt_g[i];
+        logt = ls;  // visible after the first stage_item barrier
+    }
+    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
+        Item I;
+        stage_item(P, cpp, item, S.cp, S.zb, S.zk, I);
+        Column C;
+        column_init(P, I, S.cp, C);
+        const int nzi = I.z1 - I.z0;
+        const int zstride = P.nx * P.ny;
+        int idx = (I.z0 * P.ny + C.y) * P.nx + C.x;
+        for (int zi = 0; zi < nzi; ++zi, idx += zstride) {
+            float pos[3];
+            column_position(P, I, C, S.zb, S.zk, zi, pos);
+            if (!C.inside) continue;
             float out[3] = { 0.f, 0.f, 0.f };
             if (mask == nullptr || __ldg(&mask[idx]) > -1) {
-                float wx, wy, wz, w, g[3];
-                voxel_position(P, sm, off, ly, zp, xo, bx, wx, wy, wz);
-                sample_floating<true>(flo, P.fnx, P.fny, P.fnz, P.flo_ijk, P.pad, wx, wy, wz, w, g);
+                float w, g[3];
+                sample_floating<true>(flo, P.fnx, P.fny, P.fnz, P.flo_ijk, P.flo_diag, P.pad, pos[0], pos[1], pos[2],
+                                      w, g);
                 const float rv = __ldg(&ref[idx]);
                 if (rv == rv && w == w) {
                     const double s = nmi_window(rv, w, logt, P.rb, P.fb, nmi);
@@ -362,41 +442,189 @@ k_gradient(TileParams P, const float *__restrict__ ref, const float *__restrict_
     }
 }
 
-// ---------------------------------------------------------------------------------------------
-// standalone Compute operations (same arithmetic, materialised intermediates)
-// ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(TILE_THREADS)
-k_deformation(TileParams P, const int32_t *__restrict__ mask, const float *__restrict__ cpp,
+// standalone deformation field (Compute::GetDeformationField) with the same arithmetic
+__global__ void __launch_bounds__(COL_THREADS)
+k_deformation(WalkParams P, const int32_t *__restrict__ mask, const float *__restrict__ cpp,
               float *__restrict__ def) {
     extern __shared__ float4 sm4[];
-    float *sm = reinterpret_cast<float *>(sm4);
-    const long long nv = (long long)P.nx * P.ny * P.nz;
-    const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
-    for (int tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
-        TileCtx T;
-        tile_positions(P, cpp, tile, sm, T);
-        const float *off = tile_offsets(P, sm);
-        const int x = T.x0 + lx, y = T.y0 + ly;
-        if (x >= P.nx || y >= P.ny) continue;
-        const int pre = pre_of(x, P.gsx);
-        float bx[4];
-        bspline_basis(frac_of(x, P.gsx, pre), bx);
-        const int xo = pre - T.xa0;
-        for (int zp = 0; zp < TILE_Z; ++zp) {
-            const int z = T.z0 + zp;
-            if (z >= P.nz) break;
-            const long long idx = ((long long)z * P.ny + y) * P.nx + x;
-            float wx = 0, wy = 0, wz = 0;
-            if (mask == nullptr || __ldg(&mask[idx]) > -1) voxel_position(P, sm, off, ly, zp, xo, bx, wx, wy, wz);
-            def[idx] = wx;
-            def[nv + idx] = wy;
-            def[2 * nv + idx] = wz;
+    const WalkSmem S = walk_smem(P, sm4);
+    const int nv = P.nx * P.ny * P.nz;
+    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
+        Item I;
+        stage_item(P, cpp, item, S.cp, S.zb, S.zk, I);
+        Column C;
+        column_init(P, I, S.cp, C);
+        const int nzi = I.z1 - I.z0;
+        for (int zi = 0; zi < nzi; ++zi) {
+            float pos[3];
+            column_position(P, I, C, S.zb, S.zk, zi, pos);
+            if (!C.inside) continue;
+            const int idx = ((I.z0 + zi) * P.ny + C.y) * P.nx + C.x;
+            if (mask != nullptr && __ldg(&mask[idx]) <= -1) pos[0] = pos[1] = pos[2] = 0.f;
+            def[idx] = pos[0];
+            def[nv + idx] = pos[1];
+            def[2 * nv + idx] = pos[2];
         }
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// histogram -> smoothed probabilities, FP64 entropies, log table (one block, tables in smem)
+// ---------------------------------------------------------------------------------------------
+constexpr int FIN_THREADS = 1024;
+
+// fixed-shape block sum of three doubles: warp shuffles, then one warp over the partials
+__device__ __forceinline__ void block_sum3(double& a, double& b, double& c, double *red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    }
+    __syncthreads();  // red is free
+    if (lane == 0) {
+        red[3 * wid] = a;
+        red[3 * wid + 1] = b;
+        red[3 * wid + 2] = c;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        a = red[3 * lane];
+        b = red[3 * lane + 1];
+        c = red[3 * lane + 2];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+            c += __shfl_down_sync(0xffffffffu, c, o);
+        }
+        if (lane == 0) {
+            red[0] = a;
+            red[1] = b;
+            red[2] = c;
+        }
+    }
+    __syncthreads();
+    a = red[0];
+    b = red[1];
+    c = red[2];
+}
+
+// one 3-tap smoothing output in the reference's accumulation order (value = 0; value +=
+// left*k0; value += centre*k1; value += right*k0, in-range taps only), no contraction
+__device__ __forceinline__ double smooth3(bool has_l, double l, double m, bool has_r, double r, double k0, double k1) {
+    double v = 0.0;
+    if (has_l) v = __dadd_rn(v, __dmul_rn(l, k0));
+    v = __dadd_rn(v, __dmul_rn(m, k1));
+    if (has_r) v = __dadd_rn(v, __dmul_rn(r, k0));
+    return v;
+}
+
+// _reg_nmi.cpp:249-346 with the histogram as integer counts: 3-tap [1/6, float(2/3), 1/6]
+// smoothing along the reference axis then the floating axis (each entry bit-identical to the
+// reference's), normalisation by the total, marginals summed in the reference's sequential
+// order, entropies and the log table. The bending-energy partials of the same evaluation are
+// summed here too. Shared memory: T = the joint table plus marginals; U = a second joint table
+// for the parallel smoothing pass (omitted when two tables do not fit, then the smoothing along
+// the floating axis rolls a window in place, one thread per reference bin).
+__global__ void __launch_bounds__(FIN_THREADS)
+k_nmi_finalize(int rb, int fb, int two_tables, uint32_t *__restrict__ hist, double *__restrict__ pro,
+               double *__restrict__ logt, nrb_objective *__restrict__ last,
+               const double *__restrict__ be_partials, int n_be, double be_norm,
+               double sim_weight, double be_weight, nrb_objective *__restrict__ obj) {
+    extern __shared__ double T[];
+    __shared__ double red[3 * 32];
+    const int tid = threadIdx.x;
+    const int nj = rb * fb, total = nj + rb + fb;
+    double *U = T + total;
+    const double k0 = parzen(-1.0), k1 = parzen(0.0);
+    // smoothing along the reference axis straight from the integer counts
+    for (int i = tid; i < nj; i += FIN_THREADS) {
+        const int r = i % rb;
+        const double m = (double)hist[i];
+        const double l = r > 0 ? (double)hist[i - 1] : 0.0;
+        const double rr = r + 1 < rb ? (double)hist[i + 1] : 0.0;
+        (two_tables ? U : T)[i] = smooth3(r > 0, l, m, r + 1 < rb, rr, k0, k1);
+    }
+    __syncthreads();
+    for (int i = tid; i < nj; i += FIN_THREADS) hist[i] = 0u;  // ready for the next evaluation
+    for (int i = nj + tid; i < total; i += FIN_THREADS) T[i] = 0.0;
+    double mass = 0.0, u1 = 0.0, u2 = 0.0;
+    if (two_tables) {
+        for (int i = tid; i < nj; i += FIN_THREADS) {
+            const int f = i / rb;
+            const double v = smooth3(f > 0, f > 0 ? U[i - rb] : 0.0, U[i], f + 1 < fb, f + 1 < fb ? U[i + rb] : 0.0, k0, k1);
+            T[i] = v;
+            mass += v;
+        }
+    } else {
+        for (int r = tid; r < rb; r += FIN_THREADS) {
+            double prev = 0.0, cur = T[r];
+            for (int f = 0; f < fb; ++f) {
+                const double next = f + 1 < fb ? T[r + (f + 1) * rb] : 0.0;
+                const double v = smooth3(f > 0, prev, cur, f + 1 < fb, next, k0, k1);
+                T[r + f * rb] = v;
+                prev = cur;
+                cur = next;
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < nj; i += FIN_THREADS) mass += T[i];
+    }
+    block_sum3(mass, u1, u2, red);  // also orders the T writes before the reads below
+    for (int i = tid; i < nj; i += FIN_THREADS) T[i] /= mass;
+    __syncthreads();
+    for (int i = tid; i < rb + fb; i += FIN_THREADS) {
+        double s = 0.0;
+        if (i < rb) {
+            for (int f = 0; f < fb; ++f) s += T[i + rb * f];
+        } else {
+            const int f = i - rb;
+            for (int r = 0; r < rb; ++r) s += T[r + rb * f];
+        }
+        T[nj + i] = s;
+    }
+    __syncthreads();
+    double hr = 0.0, hw = 0.0, hj = 0.0;
+    for (int i = tid; i < total; i += FIN_THREADS) {
+        const double p = T[i];
+        double l = 0.0;
+        if (p > 0) {
+            l = log(p);
+            if (i < nj) hj -= p * l;
+            else if (i < nj + rb) hr -= p * l;
+            else hw -= p * l;
+        }
+        logt[i] = l;
+        pro[i] = p;
+    }
+    block_sum3(hr, hw, hj, red);
+    double be = 0.0, d1 = 0.0, d2 = 0.0;
+    for (int i = tid; i < n_be; i += FIN_THREADS) be += be_partials[i];
+    block_sum3(be, d1, d2, red);
+    if (tid == 0) {
+        nrb_objective o;
+        // with a zero similarity weight the reference never evaluates the measure
+        // (_reg_f3d.cpp:450-454): its weighted term is 0, not 0 * NaN
+        o.nmi = sim_weight > 0 ? (hr + hw) / hj : 0.0;
+        o.entropy[0] = hr;
+        o.entropy[1] = hw;
+        o.entropy[2] = hj;
+        o.entropy[3] = mass;
+        o.be = n_be > 0 ? be / be_norm : 0.0;
+        o.objective = (sim_weight > 0 ? sim_weight * o.nmi : 0.0) - (be_weight > 0 ? be_weight * o.be : 0.0);
+        o.max_grad_len = last->max_grad_len;
+        *last = o;
+        if (obj) *obj = o;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// standalone resampling / histogram / voxel gradient (materialised intermediates)
+// ---------------------------------------------------------------------------------------------
 template <bool kGrad>
-__global__ void k_resample(long long nv, int fnx, int fny, int fnz, Mat34 M, float pad,
+__global__ void k_resample(long long nv, int fnx, int fny, int fnz, Mat34 M, int diag, float pad,
                            const float *__restrict__ flo, const float *__restrict__ def,
                            const int32_t *__restrict__ mask, float *__restrict__ out) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
@@ -405,7 +633,7 @@ __global__ void k_resample(long long nv, int fnx, int fny, int fnz, Mat34 M, flo
         if (!kGrad && !active) continue;
         float w = 0.f, g[3] = { 0.f, 0.f, 0.f };
         if (active)
-            sample_floating<kGrad>(flo, fnx, fny, fnz, M, pad, def[i], def[nv + i], def[2 * nv + i], w, g);
+            sample_floating<kGrad>(flo, fnx, fny, fnz, M, diag, pad, def[i], def[nv + i], def[2 * nv + i], w, g);
         if (kGrad) {
             out[i] = g[0];
             out[nv + i] = g[1];
@@ -423,18 +651,12 @@ __global__ void k_histogram(long long nv, int rb, int fb, const float *__restric
     const int nbins = rb * fb;
     for (int i = threadIdx.x; i < nbins; i += blockDim.x) hs[i] = 0u;
     __syncthreads();
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long nround = (nv + stride - 1) / stride;
-    for (long long k = 0; k < nround; ++k) {
-        const long long i = k * stride + blockIdx.x * (long long)blockDim.x + threadIdx.x;
-        int bin = -1;
-        if (i < nv && (mask == nullptr || mask[i] > -1)) {
-            const float r = ref[i], w = war[i];
-            if (r == r && w == w && 0.f <= r && r < (float)rb && 0.f <= w && w < (float)fb)
-                bin = (int)r + (int)w * rb;
-        }
-        const unsigned peers = __match_any_sync(0xffffffffu, bin);
-        if (bin >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hs[bin], (uint32_t)__popc(peers));
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (mask != nullptr && mask[i] <= -1) continue;
+        const float r = ref[i], w = war[i];
+        if (r == r && w == w && 0.f <= r && r < (float)rb && 0.f <= w && w < (float)fb)
+            atomicAdd(&hs[(int)r + (int)w * rb], 1u);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
@@ -464,118 +686,10 @@ __global__ void k_nmi_voxel_gradient(long long nv, int rb, int fb, const float *
 }
 
 // ---------------------------------------------------------------------------------------------
-// histogram -> smoothed probabilities, FP64 entropies, log table (one block)
-// ---------------------------------------------------------------------------------------------
-constexpr int FIN_THREADS = 1024;
-
-__device__ double block_sum(double v, double *red) {
-    // fixed-shape tree: deterministic for a given block size
-    const int tid = threadIdx.x;
-    red[tid] = v;
-    __syncthreads();
-    for (int s = FIN_THREADS / 2; s > 0; s >>= 1) {
-        if (tid < s) red[tid] += red[tid + s];
-        __syncthreads();
-    }
-    const double r = red[0];
-    __syncthreads();
-    return r;
-}
-
-// _reg_nmi.cpp:249-346 with the histogram as integer counts: 3-tap [1/6, float(2/3), 1/6]
-// smoothing along the reference axis then the floating axis, normalisation by the total,
-// marginals, entropies and the log table. The bending-energy partials of the same
-// evaluation are summed here too, so one block produces the whole objective.
-__global__ void __launch_bounds__(FIN_THREADS)
-k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *__restrict__ pro,
-               double *__restrict__ logt, nrb_objective *__restrict__ last,
-               const double *__restrict__ be_partials, int n_be, double be_norm,
-               double sim_weight, double be_weight, nrb_objective *__restrict__ obj) {
-    __shared__ double red[FIN_THREADS];
-    const int tid = threadIdx.x;
-    const int nj = rb * fb, total = nj + rb + fb;
-    const double k0 = parzen(-1.0), k1 = parzen(0.0);
-    // smoothing along the reference axis into logt (scratch)
-    for (int i = tid; i < nj; i += FIN_THREADS) {
-        const int r = i % rb;
-        double v = 0;
-        if (r > 0) v += (double)hist[i - 1] * k0;
-        v += (double)hist[i] * k1;
-        if (r + 1 < rb) v += (double)hist[i + 1] * k0;
-        logt[i] = v;
-    }
-    __syncthreads();
-    double part = 0;
-    for (int i = tid; i < total; i += FIN_THREADS) {
-        double v = 0;
-        if (i < nj) {
-            const int f = i / rb;
-            if (f > 0) v += logt[i - rb] * k0;
-            v += logt[i] * k1;
-            if (f + 1 < fb) v += logt[i + rb] * k0;
-        }
-        pro[i] = v;
-        part += v;
-    }
-    const double mass = block_sum(part, red);  // syncs: pro complete, logt reads done
-    for (int i = tid; i < nj; i += FIN_THREADS) {
-        pro[i] /= mass;
-        hist[i] = 0u;  // ready for the next evaluation
-    }
-    __syncthreads();
-    // marginals, summed in the reference's sequential order
-    for (int i = tid; i < rb + fb; i += FIN_THREADS) {
-        double s = 0;
-        if (i < rb) {
-            for (int f = 0; f < fb; ++f) s += pro[i + rb * f];
-        } else {
-            const int f = i - rb;
-            for (int r = 0; r < rb; ++r) s += pro[r + rb * f];
-        }
-        pro[nj + i] = s;
-    }
-    __syncthreads();
-    double hr = 0, hw = 0, hj = 0;
-    for (int i = tid; i < total; i += FIN_THREADS) {
-        const double p = pro[i];
-        double l = 0;
-        if (p > 0) {
-            l = log(p);
-            if (i < nj) hj -= p * l;
-            else if (i < nj + rb) hr -= p * l;
-            else hw -= p * l;
-        }
-        logt[i] = l;
-    }
-    hr = block_sum(hr, red);
-    hw = block_sum(hw, red);
-    hj = block_sum(hj, red);
-    double be = 0;
-    for (int i = tid; i < n_be; i += FIN_THREADS) be += be_partials[i];
-    be = block_sum(be, red) / be_norm;
-    if (tid == 0) {
-        nrb_objective o;
-        // with a zero similarity weight the reference never evaluates the measure
-        // (_reg_f3d.cpp:450-454): its weighted term is 0, not 0 * NaN
-        o.nmi = sim_weight > 0 ? (hr + hw) / hj : 0.0;
-        o.entropy[0] = hr;
-        o.entropy[1] = hw;
-        o.entropy[2] = hj;
-        o.entropy[3] = mass;
-        o.be = n_be > 0 ? be : 0.0;
-        o.objective = (sim_weight > 0 ? sim_weight * o.nmi : 0.0) - (be_weight > 0 ? be_weight * o.be : 0.0);
-        o.max_grad_len = last->max_grad_len;
-        *last = o;
-        if (obj) *obj = o;
-    }
-}
-
-// ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
-static TileParams make_tile_params(const nrb_workspace *ws, const nrb_geometry *g, float pad,
-                                   int rb, int fb) {
-    TileParams P{};
+static WalkParams make_params(const WalkPlan& W, const nrb_geometry *g, float pad, int rb, int fb) {
+    WalkParams P{};
     P.nx = g->ref_dim[0];
     P.ny = g->ref_dim[1];
     P.nz = g->ref_dim[2];
@@ -585,13 +699,13 @@ static TileParams make_tile_params(const nrb_workspace *ws, const nrb_geometry *
     P.gsx = g->cpp_pixdim[0] / g->ref_pixdim[0];
     P.gsy = g->cpp_pixdim[1] / g->ref_pixdim[1];
     P.gsz = g->cpp_pixdim[2] / g->ref_pixdim[2];
-    P.sa = ws->span[0];
-    P.sb = ws->span[1];
-    P.sc = ws->span[2];
-    P.tiles_x = (P.nx + TILE_X - 1) / TILE_X;
-    P.tiles_y = (P.ny + TILE_Y - 1) / TILE_Y;
-    P.tiles_z = (P.nz + TILE_Z - 1) / TILE_Z;
-    P.ntiles = P.tiles_x * P.tiles_y * P.tiles_z;
+    P.tiles_x = W.tiles_x;
+    P.tiles_y = W.tiles_y;
+    P.zchunk = W.zchunk;
+    P.nitems = W.nitems;
+    P.sa = W.sa;
+    P.sb = W.sb;
+    P.sc = W.sc;
     P.fnx = g->flo_dim[0];
     P.fny = g->flo_dim[1];
     P.fnz = g->flo_dim[2];
@@ -599,39 +713,52 @@ static TileParams make_tile_params(const nrb_workspace *ws, const nrb_geometry *
     P.pad = pad;
     P.rb = rb;
     P.fb = fb;
-    P.tile_floats = tile_smem_floats(P.sa, P.sb, P.sc);
-    P.cnv = (long long)P.cx * P.cy * P.cz;
+    P.cnv = P.cx * P.cy * P.cz;
+    const float *m = g->flo_ijk;
+    P.flo_diag = m[1] == 0.f && m[2] == 0.f && m[4] == 0.f && m[6] == 0.f && m[8] == 0.f && m[9] == 0.f;
+    P.log_in_smem = 0;
     return P;
 }
 
 template <typename K>
-static nrb_status tile_grid(K kernel, size_t smem, int ntiles, int& grid) {
-    static thread_local int configured_device = -1;
-    int dev = 0;
-    NRB_CUDA(cudaGetDevice(&dev));
-    (void)configured_device;
+static nrb_status persistent_grid(K kernel, size_t smem, int nitems, int& grid) {
     NRB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     int per_sm = 0;
-    NRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, TILE_THREADS, smem));
-    if (per_sm < 1) return fail(NRB_ERR_UNSUPPORTED, "voxel tile does not fit in shared memory");
-    grid = std::min(ntiles, per_sm * sm_count());
+    NRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, COL_THREADS, smem));
+    if (per_sm < 1) return fail(NRB_ERR_UNSUPPORTED, "voxel walk does not fit in shared memory");
+    grid = std::min(nitems, per_sm * sm_count());
     return NRB_OK;
 }
 
 nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                   const float *ref, const float *flo, const int32_t *mask,
                                   const float *cpp, float padding, cudaStream_t st) {
-    const TileParams P = make_tile_params(ws, g, padding, nmi->rb, nmi->fb);
-    const size_t smem = (size_t)P.tile_floats * 4 + (size_t)nmi->rb * nmi->fb * 4;
+    const WalkParams P = make_params(ws->walk, g, padding, nmi->rb, nmi->fb);
+    const size_t smem = walk_smem_bytes(ws->walk) + (size_t)nmi->rb * nmi->fb * 4;
     int grid = 0;
-    NRB_TRY(tile_grid(k_objective, smem, P.ntiles, grid));
+    NRB_TRY(persistent_grid(k_objective, smem, P.nitems, grid));
+    grid = ((grid + HIST_CLUSTER - 1) / HIST_CLUSTER) * HIST_CLUSTER;  // whole clusters
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(COL_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = HIST_CLUSTER;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     // algorithmic bytes: reference + floating (+ mask) per voxel, the grid once
     const double nv = (double)P.nx * P.ny * P.nz;
     const double bytes = nv * (mask ? 12.0 : 8.0) + 12.0 * (double)P.cnv;
+    cudaError_t e;
     {
         KernelTimer timer(TK_OBJECTIVE, bytes, st);
-        k_objective<<<grid, TILE_THREADS, smem, st>>>(P, ref, flo, mask, cpp, nmi->hist);
+        e = cudaLaunchKernelEx(&cfg, k_objective, P, ref, flo, mask, cpp, nmi->hist);
     }
+    NRB_CUDA(e);
     NRB_LAUNCHED("k_objective");
     return NRB_OK;
 }
@@ -640,16 +767,19 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
                                  const float *ref, const float *flo, const int32_t *mask,
                                  const float *cpp, float padding, double weight, float *vgrad,
                                  cudaStream_t st) {
-    const TileParams P = make_tile_params(ws, g, padding, nmi->rb, nmi->fb);
-    const size_t smem = (size_t)P.tile_floats * 4;
+    WalkParams P = make_params(ws->walk, g, padding, nmi->rb, nmi->fb);
+    // the FP64 log table rides in shared memory when it is small (64 bins: 38 KB)
+    const size_t log_bytes = (size_t)nmi->total * sizeof(double);
+    P.log_in_smem = log_bytes <= 48 * 1024;
+    const size_t smem = walk_smem_bytes(ws->walk) + (P.log_in_smem ? log_bytes : 0);
     int grid = 0;
-    NRB_TRY(tile_grid(k_gradient, smem, P.ntiles, grid));
+    NRB_TRY(persistent_grid(k_gradient, smem, P.nitems, grid));
     // algorithmic bytes: reference + floating (+ mask) read, voxel gradient written, grid once
     const double nv = (double)P.nx * P.ny * P.nz;
     const double bytes = nv * (mask ? 24.0 : 20.0) + 12.0 * (double)P.cnv;
     {
         KernelTimer timer(TK_GRADIENT, bytes, st);
-        k_gradient<<<grid, TILE_THREADS, smem, st>>>(P, ref, flo, mask, cpp, nmi->logt, nmi->last, weight, vgrad);
+        k_gradient<<<grid, COL_THREADS, smem, st>>>(P, ref, flo, mask, cpp, nmi->logt, nmi->last, weight, vgrad);
     }
     NRB_LAUNCHED("k_gradient");
     return NRB_OK;
@@ -658,10 +788,14 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
 nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be_partials,
                                int64_t cpp_nvox3, double sim_weight, double be_weight,
                                nrb_objective *obj, cudaStream_t st) {
-    KernelTimer timer(TK_FINALIZE, (double)nmi->rb * nmi->fb * 4 + (double)nmi->total * 16, st);
-    k_nmi_finalize<<<1, FIN_THREADS, 0, st>>>(nmi->rb, nmi->fb, nmi->hist, nmi->pro, nmi->logt, nmi->last,
-                                               be_partials, n_be_partials, (double)cpp_nvox3, sim_weight,
-                                               be_weight, obj);
+    // two joint tables for the parallel smoothing pass when they fit, else one (rolling pass)
+    const int two = (size_t)(nmi->total + nmi->rb * nmi->fb) * sizeof(double) <= 180 * 1024;
+    const size_t smem = (size_t)(nmi->total + (two ? nmi->rb * nmi->fb : 0)) * sizeof(double);
+    NRB_CUDA(cudaFuncSetAttribute(k_nmi_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    KernelTimer timer(TK_FINALIZE, (double)nmi->rb * nmi->fb * 8 + (double)nmi->total * 16, st);
+    k_nmi_finalize<<<1, FIN_THREADS, smem, st>>>(nmi->rb, nmi->fb, two, nmi->hist, nmi->pro, nmi->logt, nmi->last,
+                                                  be_partials, n_be_partials, (double)cpp_nvox3, sim_weight,
+                                                  be_weight, obj);
     NRB_LAUNCHED("k_nmi_finalize");
     return NRB_OK;
 }
@@ -673,14 +807,13 @@ using namespace nrb;
 extern "C" nrb_status nrb_get_deformation_field(const nrb_geometry *g, const float *cpp,
                                                 const int32_t *mask, float *def, void *stream) {
     if (!g || !cpp || !def) return fail(NRB_ERR_INVALID, "nrb_get_deformation_field: null pointer");
-    nrb_workspace ws;
     NRB_TRY(validate_geometry(g));
-    NRB_TRY(workspace_init(&ws, g));  // spans only; no allocation for this call
-    const TileParams P = make_tile_params(&ws, g, 0.f, 0, 0);
-    const size_t smem = (size_t)P.tile_floats * 4;
+    const WalkPlan W = plan_walk(g);
+    const WalkParams P = make_params(W, g, 0.f, 0, 0);
+    const size_t smem = walk_smem_bytes(W);
     int grid = 0;
-    NRB_TRY(tile_grid(k_deformation, smem, P.ntiles, grid));
-    k_deformation<<<grid, TILE_THREADS, smem, as_stream(stream)>>>(P, mask, cpp, def);
+    NRB_TRY(persistent_grid(k_deformation, smem, P.nitems, grid));
+    k_deformation<<<grid, COL_THREADS, smem, as_stream(stream)>>>(P, mask, cpp, def);
     NRB_LAUNCHED("k_deformation");
     return NRB_OK;
 }
@@ -692,14 +825,16 @@ static nrb_status resample_common(const nrb_geometry *g, const float *flo, const
     const long long nv = nvox(g->ref_dim);
     if (nv <= 0) return fail(NRB_ERR_INVALID, "resample: empty reference");
     const int threads = 256;
-    const int grid = (int)std::min<long long>((nv + threads - 1) / threads, 8LL * sm_count() * 8);
+    const int grid = (int)std::min<long long>((nv + threads - 1) / threads, 64LL * sm_count());
     const Mat34 M = to_mat34(g->flo_ijk);
+    const float *m = g->flo_ijk;
+    const int diag = m[1] == 0.f && m[2] == 0.f && m[4] == 0.f && m[6] == 0.f && m[8] == 0.f && m[9] == 0.f;
     if (grad)
         k_resample<true><<<grid, threads, 0, as_stream(stream)>>>(nv, g->flo_dim[0], g->flo_dim[1], g->flo_dim[2], M,
-                                                                  pad, flo, def, mask, out);
+                                                                  diag, pad, flo, def, mask, out);
     else
         k_resample<false><<<grid, threads, 0, as_stream(stream)>>>(nv, g->flo_dim[0], g->flo_dim[1], g->flo_dim[2], M,
-                                                                   pad, flo, def, mask, out);
+                                                                   diag, pad, flo, def, mask, out);
     NRB_LAUNCHED("k_resample");
     return NRB_OK;
 }
