@@ -713,22 +713,23 @@ static nrb_status upload(T *&dst, const std::vector<T>& src, size_t& bytes) {
 
 // Items of the voxel walk: enough z-chunks that the persistent blocks get several items each
 // (load balance), but chunks of at least 8 slices so the staged control points are reused.
-WalkPlan plan_walk(const nrb_geometry *g) {
+WalkPlan plan_walk(const nrb_geometry *g, int ty) {
     WalkPlan p;
+    p.ty = ty;
     const int nx = g->ref_dim[0], ny = g->ref_dim[1], nz = g->ref_dim[2];
     const float gs[3] = { g->cpp_pixdim[0] / g->ref_pixdim[0], g->cpp_pixdim[1] / g->ref_pixdim[1],
                           g->cpp_pixdim[2] / g->ref_pixdim[2] };
     p.tiles_x = (nx + COL_X - 1) / COL_X;
-    p.tiles_y = (ny + COL_Y - 1) / COL_Y;
+    p.tiles_y = (ny + ty - 1) / ty;
     const long long xy = (long long)p.tiles_x * p.tiles_y;
-    const long long want = 12LL * sm_count();
+    const long long want = (48LL / ty) * sm_count();
     int chunks = (int)std::max<long long>(1, (want + xy - 1) / xy);
     chunks = std::min(chunks, std::max(1, nz / 8));
     p.zchunk = (nz + chunks - 1) / chunks;
     p.nchunks = (nz + p.zchunk - 1) / p.zchunk;
     p.nitems = (int)(xy * p.nchunks);
     p.sa = tile_span(nx, COL_X, gs[0]);
-    p.sb = tile_span(ny, COL_Y, gs[1]);
+    p.sb = tile_span(ny, ty, gs[1]);
     p.sc = tile_span(nz, p.zchunk, gs[2]);
     p.cp_floats = 3 * p.sa * p.sb * p.sc;
     return p;
@@ -736,7 +737,8 @@ WalkPlan plan_walk(const nrb_geometry *g) {
 
 nrb_status workspace_init(nrb_workspace *ws, const nrb_geometry *g) {
     ws->g = *g;
-    ws->walk = plan_walk(g);
+    ws->walk_obj = plan_walk(g, TY_OBJECTIVE);
+    ws->walk_grad = plan_walk(g, TY_GRADIENT);
     return NRB_OK;
 }
 

@@ -13,18 +13,22 @@ constexpr int NRB_RED_THREADS = 256;
 
 namespace nrb {
 
-// Work decomposition of the voxel passes: an item is a column of COL_X x COL_Y voxels over a
-// chunk of `zchunk` slices; a 128-thread block stages the item's control points once and each
-// thread walks its voxel column along z.
-constexpr int COL_X = 32, COL_Y = 4, COL_THREADS = COL_X * COL_Y;
+// Work decomposition of the voxel passes: an item is a column of 32 x ty voxels over a chunk of
+// `zchunk` slices; a block of ty warps stages the item's control points once and each thread
+// walks its voxel column along z. The objective pass uses tall blocks (one shared histogram for
+// 16 warps leaves most of the SM's L1 to the floating-image gathers); the gradient pass, whose
+// threads carry more registers, uses 4 warps.
+constexpr int COL_X = 32;
+constexpr int TY_OBJECTIVE = 16, TY_GRADIENT = 4, TY_DEFORMATION = 4;
 constexpr int HIST_CLUSTER = 8;  // blocks whose shared-memory histograms merge through DSMEM
 
 struct WalkPlan {
+    int ty = 0;  // warps per block = voxel rows per item
     int tiles_x = 0, tiles_y = 0, zchunk = 0, nchunks = 0, nitems = 0;
     int sa = 0, sb = 0, sc = 0;  // max control-point span of an item along x, y, z
     int cp_floats = 0;           // shared floats of the staged control-point block
 };
-WalkPlan plan_walk(const nrb_geometry *g);
+WalkPlan plan_walk(const nrb_geometry *g, int ty);
 
 }  // namespace nrb
 
@@ -54,7 +58,7 @@ struct AxisSampling {
 struct nrb_workspace {
     nrb_geometry g{};
     int device = 0;
-    nrb::WalkPlan walk;
+    nrb::WalkPlan walk_obj, walk_grad;
     // reduction partials (double pairs) and scalars
     double *red = nullptr;          // 2 * NRB_RED_BLOCKS doubles
     double *be_partials = nullptr;  // NRB_RED_BLOCKS doubles

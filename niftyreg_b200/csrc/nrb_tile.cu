@@ -31,7 +31,7 @@ struct WalkParams {
     int nx, ny, nz;          // reference / deformation-field dims
     int cx, cy, cz;          // control-point grid dims
     float gsx, gsy, gsz;     // grid spacing in reference voxels (grid pixdim / ref pixdim)
-    int tiles_x, tiles_y, zchunk, nitems;
+    int ty, tiles_x, tiles_y, zchunk, nitems;
     int sa, sb, sc;          // shared strides of the staged block (max spans)
     int fnx, fny, fnz;       // floating dims
     Mat34 flo_ijk;           // mm -> floating voxel
@@ -67,45 +67,46 @@ __device__ __forceinline__ void stage_item(const WalkParams& P, const float *__r
     const int ty = rest % P.tiles_y;
     const int tz = rest / P.tiles_y;
     I.x0 = tx * COL_X;
-    I.y0 = ty * COL_Y;
+    I.y0 = ty * P.ty;
     I.z0 = tz * P.zchunk;
     I.z1 = min(I.z0 + P.zchunk, P.nz);
     I.xa0 = pre_of(I.x0, P.gsx);
     I.yb0 = pre_of(I.y0, P.gsy);
     I.zc0 = pre_of(I.z0, P.gsz);
     const int na = pre_of(min(I.x0 + COL_X - 1, P.nx - 1), P.gsx) + 4 - I.xa0;
-    const int nb = pre_of(min(I.y0 + COL_Y - 1, P.ny - 1), P.gsy) + 4 - I.yb0;
+    const int nb = pre_of(min(I.y0 + P.ty - 1, P.ny - 1), P.gsy) + 4 - I.yb0;
     const int nc = pre_of(I.z1 - 1, P.gsz) + 4 - I.zc0;
     const int first = (I.zc0 * P.cy + I.yb0) * P.cx + I.xa0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) I.off[c] = __ldg(&cpp[c * P.cnv + first]);
     const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
     __syncthreads();  // the previous item's readers are done
-    // asynchronous global -> shared copies: no register round trip, all in flight together
+    // one pass: the node planes of one (component, row, column) are independent loads, batched
+    // four at a time so their latencies overlap
+    const int gplane = P.cx * P.cy, splane = P.sb * P.sa;
 #pragma unroll
     for (int c = 0; c < 3; ++c)
-        for (int kc = 0; kc < nc; ++kc)
-            for (int jb = ly; jb < nb; jb += COL_Y) {
-                const float *src = cpp + c * P.cnv + ((I.zc0 + kc) * P.cy + I.yb0 + jb) * P.cx + I.xa0;
-                float *dst = cp + ((c * P.sc + kc) * P.sb + jb) * P.sa;
-                for (int ia = lx; ia < na; ia += 32) __pipeline_memcpy_async(dst + ia, src + ia, sizeof(float));
+        for (int jb = ly; jb < nb; jb += P.ty)
+            for (int ia = lx; ia < na; ia += 32) {
+                const float *src = cpp + c * P.cnv + (I.zc0 * P.cy + I.yb0 + jb) * P.cx + I.xa0 + ia;
+                float *dst = cp + (c * P.sc * P.sb + jb) * P.sa + ia;
+                int kc = 0;
+                for (; kc + 4 <= nc; kc += 4) {
+                    const float v0 = __ldg(src + kc * gplane), v1 = __ldg(src + (kc + 1) * gplane);
+                    const float v2 = __ldg(src + (kc + 2) * gplane), v3 = __ldg(src + (kc + 3) * gplane);
+                    dst[kc * splane] = v0 - I.off[c];
+                    dst[(kc + 1) * splane] = v1 - I.off[c];
+                    dst[(kc + 2) * splane] = v2 - I.off[c];
+                    dst[(kc + 3) * splane] = v3 - I.off[c];
+                }
+                for (; kc < nc; ++kc) dst[kc * splane] = __ldg(src + kc * gplane) - I.off[c];
             }
-    __pipeline_commit();
-    for (int zi = threadIdx.x; zi < I.z1 - I.z0; zi += COL_THREADS) {
+    for (int zi = threadIdx.x; zi < I.z1 - I.z0; zi += blockDim.x) {
         const int z = I.z0 + zi;
         const int pz = pre_of(z, P.gsz);
         zk[zi] = pz - I.zc0;
         bspline_basis(frac_of(z, P.gsz, pz), zb + 4 * zi);
     }
-    __pipeline_wait_prior(0);
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-        for (int kc = 0; kc < nc; ++kc)
-            for (int jb = ly; jb < nb; jb += COL_Y) {
-                float *dst = cp + ((c * P.sc + kc) * P.sb + jb) * P.sa;
-                for (int ia = lx; ia < na; ia += 32) dst[ia] -= I.off[c];
-            }
     __syncthreads();
 }
 
@@ -185,13 +186,15 @@ __device__ __forceinline__ void column_position(const WalkParams& P, const Item&
 
 // mm -> floating voxel as Mat44Mul does it (reg-lib/cpu/Maths.hpp:272-286): the products of
 // two floats are exact in double, so one rounding to double and one to float. With no
-// off-diagonal terms the zero products are skipped (adding exact zeros changes nothing).
+// off-diagonal terms the single-precision FMA rounds the same exact value once instead of twice
+// (the two agree except when the exact value falls within 2^-53 of a float rounding boundary)
+// and keeps the conversions off the XU pipe.
 __device__ __forceinline__ void to_floating_voxel(const Mat34& M, int diag, float x, float y, float z,
                                                   float& fx, float& fy, float& fz) {
     if (diag) {
-        fx = (float)fma((double)M.m[0], (double)x, (double)M.m[3]);
-        fy = (float)fma((double)M.m[5], (double)y, (double)M.m[7]);
-        fz = (float)fma((double)M.m[10], (double)z, (double)M.m[11]);
+        fx = __fmaf_rn(M.m[0], x, M.m[3]);
+        fy = __fmaf_rn(M.m[5], y, M.m[7]);
+        fz = __fmaf_rn(M.m[10], z, M.m[11]);
         return;
     }
     const double dx = x, dy = y, dz = z;
@@ -200,25 +203,50 @@ __device__ __forceinline__ void to_floating_voxel(const Mat34& M, int diag, floa
     fz = (float)((double)M.m[8] * dx + (double)M.m[9] * dy + (double)M.m[10] * dz + (double)M.m[11]);
 }
 
+// floor(v) as float and as int without the XU pipe: adding 1.5 * 2^23 rounds v to the nearest
+// integer in the FMA pipe, one compare fixes the rounding direction. v is clamped to +-2^21
+// first; every position that far out lies outside any volume this library accepts.
+__device__ __forceinline__ int floor_split(float v, float& fl) {
+    const float magic = 12582912.0f;  // 1.5 * 2^23
+    v = fminf(fmaxf(v, -2097152.0f), 2097152.0f);
+    const float t = __fadd_rn(v, magic);
+    int n = __float_as_int(t) - 0x4B400000;
+    float r = __fsub_rn(t, magic);
+    if (r > v) {
+        r = __fsub_rn(r, 1.0f);
+        n -= 1;
+    }
+    fl = r;
+    return n;
+}
+
+// (int)v for 0 <= v < 2^22 (truncation == floor there), again without the XU pipe
+__device__ __forceinline__ int trunc_nonneg(float v) {
+    float fl;
+    return floor_split(v, fl);
+}
+
 // Trilinear sample of the floating image at world position (x, y, z) with the padding rule of
 // ResampleImage3D (an out-of-volume tap contributes padding * weight, so NaN padding poisons a
 // border voxel even through a zero weight) and, when kGrad, the spatial derivative of
-// TrilinearImageGradient (NaN components -> 0).
+// TrilinearImageGradient (NaN components -> 0). Warps whose 32 samples are all interior take
+// the plain 8-load path; otherwise every lane reads clamped in-bounds addresses and selects the
+// padding value for out-of-volume taps, with no divergence.
 template <bool kGrad>
 __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, int fnx, int fny,
                                                 int fnz, const Mat34& M, int diag, float pad, float x,
                                                 float y, float z, float& val, float g[3]) {
     float fx, fy, fz;
     to_floating_voxel(M, diag, x, y, z, fx, fy, fz);
-    const float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
-    const int px = (int)flx, py = (int)fly, pz = (int)flz;
+    float flx, fly, flz;
+    const int px = floor_split(fx, flx), py = floor_split(fy, fly), pz = floor_split(fz, flz);
     const float rx = fx - flx, ry = fy - fly, rz = fz - flz;
     const float bx0 = 1.f - rx, by0 = 1.f - ry, bz0 = 1.f - rz;
     float v[2][2][2];
     const bool interior = px >= 0 && py >= 0 && pz >= 0 && px + 1 < fnx && py + 1 < fny && pz + 1 < fnz;
-    if (interior) {
+    const int sy = fnx, sz = fnx * fny;
+    if (__all_sync(__activemask(), interior)) {
         const float *p = flo + (pz * fny + py) * fnx + px;
-        const int sy = fnx, sz = fnx * fny;
         v[0][0][0] = __ldg(p);
         v[0][0][1] = __ldg(p + 1);
         v[0][1][0] = __ldg(p + sy);
@@ -228,16 +256,23 @@ __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, i
         v[1][1][0] = __ldg(p + sz + sy);
         v[1][1][1] = __ldg(p + sz + sy + 1);
     } else {
+        const bool inx[2] = { (unsigned)px < (unsigned)fnx, (unsigned)(px + 1) < (unsigned)fnx };
+        const bool iny[2] = { (unsigned)py < (unsigned)fny, (unsigned)(py + 1) < (unsigned)fny };
+        const bool inz[2] = { (unsigned)pz < (unsigned)fnz, (unsigned)(pz + 1) < (unsigned)fnz };
+        const int cx[2] = { min(max(px, 0), fnx - 1), min(max(px + 1, 0), fnx - 1) };
+        const int cy[2] = { min(max(py, 0), fny - 1), min(max(py + 1, 0), fny - 1) };
+        const int cz[2] = { min(max(pz, 0), fnz - 1), min(max(pz + 1, 0), fnz - 1) };
 #pragma unroll
         for (int c = 0; c < 2; ++c)
 #pragma unroll
-            for (int b = 0; b < 2; ++b)
+            for (int b = 0; b < 2; ++b) {
+                const float *row = flo + cz[c] * sz + cy[b] * sy;
 #pragma unroll
                 for (int a = 0; a < 2; ++a) {
-                    const int X = px + a, Y = py + b, Z = pz + c;
-                    const bool in = X >= 0 && X < fnx && Y >= 0 && Y < fny && Z >= 0 && Z < fnz;
-                    v[c][b][a] = in ? __ldg(&flo[(Z * fny + Y) * fnx + X]) : pad;
+                    const float t = __ldg(row + cx[a]);
+                    v[c][b][a] = (inx[a] && iny[b] && inz[c]) ? t : pad;
                 }
+            }
     }
     const float yv0 = fmaf(v[0][0][1], rx, v[0][0][0] * bx0);
     const float yv1 = fmaf(v[0][1][1], rx, v[0][1][0] * bx0);
@@ -286,7 +321,7 @@ __host__ inline size_t walk_smem_bytes(const WalkPlan& W) {
 // ---------------------------------------------------------------------------------------------
 // fused objective: deformation + warp + joint histogram
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(COL_THREADS, 8)
+__global__ void __launch_bounds__(32 * TY_OBJECTIVE, 2)
 k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
             const int32_t *__restrict__ mask, const float *__restrict__ cpp,
             uint32_t *__restrict__ ghist) {
@@ -294,7 +329,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
     const WalkSmem S = walk_smem(P, sm4);
     uint32_t *h = reinterpret_cast<uint32_t *>(S.tail);
     const int nbins = P.rb * P.fb;
-    for (int i = threadIdx.x; i < nbins; i += COL_THREADS) h[i] = 0u;
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x) h[i] = 0u;
     const int lane = threadIdx.x & 31;
     const float frb = (float)P.rb, ffb = (float)P.fb;
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
@@ -321,7 +356,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
                                                pos[2], w, g);
                         const float rv = __ldg(&ref[vi]);
                         if (rv == rv && w == w && 0.f <= rv && rv < frb && 0.f <= w && w < ffb)
-                            bin[u] = (int)rv + (int)w * P.rb;
+                            bin[u] = trunc_nonneg(rv) + trunc_nonneg(w) * P.rb;
                     }
                 }
             }
@@ -344,7 +379,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
     cluster.sync();
     const int rank = (int)cluster.block_rank();
     const int nblk = (int)cluster.num_blocks();
-    for (int i = rank + nblk * threadIdx.x; i < nbins; i += nblk * COL_THREADS) {
+    for (int i = rank + nblk * threadIdx.x; i < nbins; i += nblk * blockDim.x) {
         uint32_t s = 0;
         for (int q = 0; q < nblk; ++q) s += cluster.map_shared_rank(h, q)[i];
         if (s) atomicAdd(&ghist[i], s);
@@ -394,7 +429,7 @@ __device__ __forceinline__ double nmi_window(float rv, float wv, const double *l
 // ---------------------------------------------------------------------------------------------
 // fused gradient: deformation + warp + spatial gradient + NMI voxel gradient
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(COL_THREADS, 4)
+__global__ void __launch_bounds__(32 * TY_GRADIENT, 4)
 k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
            const int32_t *__restrict__ mask, const float *__restrict__ cpp,
            const double *__restrict__ logt_g, const nrb_objective *__restrict__ last,
@@ -408,7 +443,7 @@ k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict_
     if (P.log_in_smem) {
         double *ls = reinterpret_cast<double *>(S.tail);
         const int total = P.rb * P.fb + P.rb + P.fb;
-        for (int i = threadIdx.x; i < total; i += COL_THREADS) ls[i] = logt_g[i];
+        for (int i = threadIdx.x; i < total; i += blockDim.x) ls[i] = logt_g[i];
         logt = ls;  // visible after the first stage_item barrier
     }
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
@@ -443,7 +478,7 @@ k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict_
 }
 
 // standalone deformation field (Compute::GetDeformationField) with the same arithmetic
-__global__ void __launch_bounds__(COL_THREADS)
+__global__ void __launch_bounds__(32 * TY_DEFORMATION)
 k_deformation(WalkParams P, const int32_t *__restrict__ mask, const float *__restrict__ cpp,
               float *__restrict__ def) {
     extern __shared__ float4 sm4[];
@@ -699,6 +734,7 @@ static WalkParams make_params(const WalkPlan& W, const nrb_geometry *g, float pa
     P.gsx = g->cpp_pixdim[0] / g->ref_pixdim[0];
     P.gsy = g->cpp_pixdim[1] / g->ref_pixdim[1];
     P.gsz = g->cpp_pixdim[2] / g->ref_pixdim[2];
+    P.ty = W.ty;
     P.tiles_x = W.tiles_x;
     P.tiles_y = W.tiles_y;
     P.zchunk = W.zchunk;
@@ -721,26 +757,31 @@ static WalkParams make_params(const WalkPlan& W, const nrb_geometry *g, float pa
 }
 
 template <typename K>
-static nrb_status persistent_grid(K kernel, size_t smem, int nitems, int& grid) {
+static nrb_status persistent_grid(K kernel, int threads, size_t smem, int nitems, int& grid) {
     NRB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     int per_sm = 0;
-    NRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, COL_THREADS, smem));
+    NRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
     if (per_sm < 1) return fail(NRB_ERR_UNSUPPORTED, "voxel walk does not fit in shared memory");
-    grid = std::min(nitems, per_sm * sm_count());
+    // every block gets the same number of items: as many rounds as the resident blocks need,
+    // then the smallest grid that covers the items in that many rounds
+    const int resident = per_sm * sm_count();
+    const int rounds = (nitems + resident - 1) / resident;
+    grid = (nitems + rounds - 1) / rounds;
     return NRB_OK;
 }
 
 nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                   const float *ref, const float *flo, const int32_t *mask,
                                   const float *cpp, float padding, cudaStream_t st) {
-    const WalkParams P = make_params(ws->walk, g, padding, nmi->rb, nmi->fb);
-    const size_t smem = walk_smem_bytes(ws->walk) + (size_t)nmi->rb * nmi->fb * 4;
+    const WalkParams P = make_params(ws->walk_obj, g, padding, nmi->rb, nmi->fb);
+    const size_t smem = walk_smem_bytes(ws->walk_obj) + (size_t)nmi->rb * nmi->fb * 4;
+    const int threads = 32 * ws->walk_obj.ty;
     int grid = 0;
-    NRB_TRY(persistent_grid(k_objective, smem, P.nitems, grid));
+    NRB_TRY(persistent_grid(k_objective, threads, smem, P.nitems, grid));
     grid = ((grid + HIST_CLUSTER - 1) / HIST_CLUSTER) * HIST_CLUSTER;  // whole clusters
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(COL_THREADS);
+    cfg.blockDim = dim3(threads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
@@ -767,19 +808,20 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
                                  const float *ref, const float *flo, const int32_t *mask,
                                  const float *cpp, float padding, double weight, float *vgrad,
                                  cudaStream_t st) {
-    WalkParams P = make_params(ws->walk, g, padding, nmi->rb, nmi->fb);
+    WalkParams P = make_params(ws->walk_grad, g, padding, nmi->rb, nmi->fb);
     // the FP64 log table rides in shared memory when it is small (64 bins: 38 KB)
     const size_t log_bytes = (size_t)nmi->total * sizeof(double);
     P.log_in_smem = log_bytes <= 48 * 1024;
-    const size_t smem = walk_smem_bytes(ws->walk) + (P.log_in_smem ? log_bytes : 0);
+    const size_t smem = walk_smem_bytes(ws->walk_grad) + (P.log_in_smem ? log_bytes : 0);
+    const int threads = 32 * ws->walk_grad.ty;
     int grid = 0;
-    NRB_TRY(persistent_grid(k_gradient, smem, P.nitems, grid));
+    NRB_TRY(persistent_grid(k_gradient, threads, smem, P.nitems, grid));
     // algorithmic bytes: reference + floating (+ mask) read, voxel gradient written, grid once
     const double nv = (double)P.nx * P.ny * P.nz;
     const double bytes = nv * (mask ? 24.0 : 20.0) + 12.0 * (double)P.cnv;
     {
         KernelTimer timer(TK_GRADIENT, bytes, st);
-        k_gradient<<<grid, COL_THREADS, smem, st>>>(P, ref, flo, mask, cpp, nmi->logt, nmi->last, weight, vgrad);
+        k_gradient<<<grid, threads, smem, st>>>(P, ref, flo, mask, cpp, nmi->logt, nmi->last, weight, vgrad);
     }
     NRB_LAUNCHED("k_gradient");
     return NRB_OK;
@@ -808,12 +850,12 @@ extern "C" nrb_status nrb_get_deformation_field(const nrb_geometry *g, const flo
                                                 const int32_t *mask, float *def, void *stream) {
     if (!g || !cpp || !def) return fail(NRB_ERR_INVALID, "nrb_get_deformation_field: null pointer");
     NRB_TRY(validate_geometry(g));
-    const WalkPlan W = plan_walk(g);
+    const WalkPlan W = plan_walk(g, TY_DEFORMATION);
     const WalkParams P = make_params(W, g, 0.f, 0, 0);
     const size_t smem = walk_smem_bytes(W);
     int grid = 0;
-    NRB_TRY(persistent_grid(k_deformation, smem, P.nitems, grid));
-    k_deformation<<<grid, COL_THREADS, smem, as_stream(stream)>>>(P, mask, cpp, def);
+    NRB_TRY(persistent_grid(k_deformation, 32 * W.ty, smem, P.nitems, grid));
+    k_deformation<<<grid, 32 * W.ty, smem, as_stream(stream)>>>(P, mask, cpp, def);
     NRB_LAUNCHED("k_deformation");
     return NRB_OK;
 }
