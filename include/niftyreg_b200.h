@@ -141,6 +141,25 @@ nrb_status nrb_kernel_convolution_cubic(float *img, int nvol, const int32_t dim[
                                         const float pixdim[3], float spacing_mm, int axis,
                                         void *stream);
 
+/* Same result as nrb_kernel_convolution_cubic, but it allocates nothing: no device or host
+ * allocation, no allocator of any library. It has no counterpart in the reference; it exists
+ * for callers that must not allocate at the time of the call (while recording a stream
+ * capture, under an exhausted memory cap, inside a memory pool the caller owns). Its scratch
+ * is one fixed array per device, reserved when the library's module loads (16 MiB + 2 KiB):
+ *  - one volume of at most NRB_STATIC_CONV_MAX_VOXELS voxels, a kernel of at most
+ *    NRB_STATIC_CONV_MAX_TAPS taps (radius 255); larger requests return NRB_ERR_UNSUPPORTED
+ *    and launch nothing;
+ *  - the first call on each device looks the scratch up (cudaGetSymbolAddress) with that
+ *    device current; make that first call before any stream capture begins;
+ *  - nothing in the scratch has to start at zero;
+ *  - calls on one device share the scratch: two calls whose work can overlap (unordered
+ *    streams, several host threads) race and produce garbage. Order them on one stream. */
+#define NRB_STATIC_CONV_MAX_VOXELS 2097152
+#define NRB_STATIC_CONV_MAX_TAPS 511
+nrb_status nrb_kernel_convolution_cubic_static(float *img, int nvol, const int32_t dim[3],
+                                               const float pixdim[3], float spacing_mm, int axis,
+                                               void *stream);
+
 /* Node gradient = weight * reorient(trilinear sample at the node of the x-, y- then z-convolved
  * voxel gradient). The convolution is evaluated only at the voxels the node sampling reads.
  * Overwrites node_grad (3 * nvox(cpp)). vgrad is read only. Replaces

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "nrb_state.cuh"
@@ -898,6 +899,111 @@ extern "C" nrb_status nrb_kernel_convolution_cubic(float *img, int nvol, const i
     NRB_CUDA(cudaFreeAsync(dk, st));
     NRB_CUDA(cudaFreeAsync(tv, st));
     NRB_CUDA(cudaFreeAsync(td, st));
+    return NRB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// The same convolution with its scratch in a fixed, module-level device array.
+//
+// Some callers cannot allocate device memory at the moment they need this convolution: code
+// that is recording a CUDA stream capture (an allocation there either fails or becomes part of
+// the graph), code running under a hard per-process memory cap that is already spent, or code
+// that hands out device memory from its own pool and forbids the library from touching the
+// driver's allocator. For them the scratch (the kernel taps and the value/density pair of one
+// volume) lives in `g_static_scratch`, which the module reserves when it is loaded.
+//
+// Layout: [taps: NRB_STATIC_CONV_MAX_TAPS floats, padded to 256 B][value: max voxels floats]
+// [density: max voxels floats]. Nothing in it has to start at zero: every call writes the taps
+// and then both temporaries of a volume in full before it reads them.
+//
+// There is one scratch per device and no lock: two calls whose kernels can overlap on the same
+// device (different streams without ordering, or different host threads) race on it.
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kStaticTapBytes = 256 * ((NRB_STATIC_CONV_MAX_TAPS * sizeof(float) + 255) / 256);
+constexpr size_t kStaticScratchBytes = kStaticTapBytes + 2 * sizeof(float) * (size_t)NRB_STATIC_CONV_MAX_VOXELS;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// the taps travel as a kernel argument, so no host-to-device copy is needed for them
+struct StaticTaps {
+    float k[NRB_STATIC_CONV_MAX_TAPS];
+};
+
+__global__ void k_static_taps(const __grid_constant__ StaticTaps t, int n, float *__restrict__ dst) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = t.k[i];
+}
+
+// cubic B-spline taps with the values and radius rule of cubic_kernel(), into a fixed array;
+// returns the radius, or -1 when 2 * radius + 1 taps do not fit in `cap`
+int cubic_taps_fixed(float spacing_mm, float pixdim, float *out, int cap) {
+    const double temp = spacing_mm > 0 ? (double)(spacing_mm / pixdim) : std::fabs((double)spacing_mm);
+    const int radius = (int)(temp * 2.0f);
+    if (2 * radius + 1 > cap) return -1;
+    for (int i = -radius; i <= radius; ++i) {
+        const double rel = std::fabs(i / temp);
+        float v;
+        if (rel < 1.0) v = (float)(2.0 / 3.0 - rel * rel + 0.5 * rel * rel * rel);
+        else if (rel < 2.0) v = (float)(-(rel - 2.0) * (rel - 2.0) * (rel - 2.0) / 6.0);
+        else v = 0.f;
+        out[i + radius] = v;
+    }
+    return radius;
+}
+
+// Address of this device's scratch. cudaGetSymbolAddress runs once per device, with that device
+// current (the caller's current device); later calls read the cached pointer.
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mutex;
+unsigned char *g_static_addr[kMaxDevices] = {};
+
+nrb_status static_scratch(unsigned char **out) {
+    int dev = 0;
+    NRB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(NRB_ERR_UNSUPPORTED, "static scratch: device index above 63");
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_addr[dev]) {
+        void *p = nullptr;
+        NRB_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
+        g_static_addr[dev] = static_cast<unsigned char *>(p);
+    }
+    *out = g_static_addr[dev];
+    return NRB_OK;
+}
+
+}  // namespace
+
+extern "C" nrb_status nrb_kernel_convolution_cubic_static(float *img, int nvol, const int32_t dim[3],
+                                                          const float pixdim[3], float spacing_mm, int axis,
+                                                          void *stream) {
+    if (!img || !dim || !pixdim || nvol <= 0 || axis < 0 || axis > 2 || dim[0] <= 0 || dim[1] <= 0 || dim[2] <= 0)
+        return fail(NRB_ERR_INVALID, "nrb_kernel_convolution_cubic_static: bad argument");
+    const long long nv = (long long)dim[0] * dim[1] * dim[2];
+    if (nv > NRB_STATIC_CONV_MAX_VOXELS)
+        return fail(NRB_ERR_UNSUPPORTED, "nrb_kernel_convolution_cubic_static: volume has more voxels than the "
+                                         "static scratch holds (NRB_STATIC_CONV_MAX_VOXELS = 2097152)");
+    StaticTaps taps;
+    const int radius = cubic_taps_fixed(spacing_mm, pixdim[axis], taps.k, NRB_STATIC_CONV_MAX_TAPS);
+    if (radius < 0)
+        return fail(NRB_ERR_UNSUPPORTED, "nrb_kernel_convolution_cubic_static: kernel wider than the static "
+                                         "scratch holds (NRB_STATIC_CONV_MAX_TAPS = 511 taps)");
+    if (radius <= 0 || dim[axis] <= 1) return NRB_OK;  // the reference leaves the image as is
+    unsigned char *base = nullptr;
+    NRB_TRY(static_scratch(&base));
+    float *dk = reinterpret_cast<float *>(base);
+    float *tv = reinterpret_cast<float *>(base + kStaticTapBytes);
+    float *td = tv + NRB_STATIC_CONV_MAX_VOXELS;
+    cudaStream_t st = as_stream(stream);
+    k_static_taps<<<1, 256, 0, st>>>(taps, 2 * radius + 1, dk);
+    NRB_LAUNCHED("k_static_taps");
+    for (int t = 0; t < nvol; ++t) {
+        float *v = img + t * nv;
+        k_conv_axis<<<grid_for(nv, 256), 256, 0, st>>>(dim[0], dim[1], dim[2], axis, v, nullptr, dk, radius, tv, td);
+        NRB_LAUNCHED("k_conv_axis");
+        k_conv_normalise<<<grid_for(nv, 256), 256, 0, st>>>(nv, v, tv, td, v);
+        NRB_LAUNCHED("k_conv_normalise");
+    }
     return NRB_OK;
 }
 
