@@ -8,6 +8,8 @@ budget doubling per coarser level: 300/600/1200), NMI with 64 bins, bending ener
 control spacing, linear interpolation, NaN padding. A "step" is one whole registration.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+  python bench.py --mode batched   # many uneven pairs at once vs the same pairs one by one
+  python bench.py --mode served    # open-loop Poisson requests: p50/p95/p99 latency
 
 Under torchrun every rank registers its own pair (replicas: registrations are independent) and
 rank 0 prints one JSON line with the whole-job rate and the slowest rank's device time.
@@ -48,6 +50,11 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--mode", choices=["plain", "batched", "served"], default="plain")
+    ap.add_argument("--pairs", type=int, default=64, help="batched: number of pairs")
+    ap.add_argument("--concurrency", type=int, default=16, help="batched/served: concurrent registrations")
+    ap.add_argument("--requests", type=int, default=300, help="served: requests per arrival rate")
+    ap.add_argument("--rates", default="5,20,50", help="served: Poisson arrival rates (requests/s)")
     ap.add_argument("--kernel", choices=["objective", "gradient"], default=None,
                     help="profiling mode: run only `--steps` fused evaluations at the finest level "
                          "of the workload (for ncu captures); prints per-launch device times")
@@ -240,6 +247,21 @@ def run_reference(args):
     return 0
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The slowest rank's value (every rank calls this at the same point)."""
+    if world <= 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world: int, per_rank_units: int, seconds_max: float) -> float:
+    """Whole-job rate of independent replicas: every rank's units over the slowest rank's time."""
+    return world * per_rank_units / seconds_max
+
+
 def run_b200(args):
     import torch
     import niftyreg_b200 as nrb
@@ -312,12 +334,8 @@ def run_b200(args):
     torch.cuda.synchronize()
     timed = {k: nrb.timing_read(k) for k in ("objective", "gradient", "finalize", "conv", "be_value", "be_gradient")}
     nrb.timing_enable(False)
-    total_ms = float(sum(step_ms))
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_max = float(t.item())
-    value = world * args.steps / (total_max / 1e3)
+    total_max = max_over_ranks(float(sum(step_ms)), world, dev)
+    value = replica_rate(world, args.steps, total_max / 1e3)
 
     # ---- e2e: host buffers through the C ABI, copies inside the timed region ------------------
     barrier()
@@ -326,10 +344,8 @@ def run_b200(args):
         t0 = time.perf_counter()
         cpp_np, res = nrb.register_host(ref_h.numpy().reshape(SHAPE), flo_h.numpy().reshape(SHAPE), pix, params)
         e2e_s.append(time.perf_counter() - t0)
-    t = torch.tensor([sum(e2e_s)], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * len(e2e_s) / float(t.item()) if e2e_s else None
+    e2e_max = max_over_ranks(float(sum(e2e_s)), world, dev)
+    e2e_value = replica_rate(world, len(e2e_s), e2e_max) if e2e_s else None
 
     # ---- roofline of the dominant kernel ------------------------------------------------------
     dom = max(timed, key=lambda k: timed[k][1])
@@ -379,12 +395,169 @@ def run_b200(args):
     return 0
 
 
+# ---- batched and served modes --------------------------------------------------------------
+BATCH_SHAPES = [(96, 96, 96), (96, 128, 128), (160, 192, 160), (182, 218, 182)]  # (nz, ny, nx)
+BATCH_LEVELS, BATCH_MAXIT = 2, 150
+SERVE_MIX = [((64, 64, 64), 0.30), ((128, 128, 128), 0.40), ((182, 218, 182), 0.25), ((256, 256, 256), 0.05)]
+SERVE_LEVELS, SERVE_MAXIT = 2, 100
+
+
+def _phantom_pool(shapes, per_shape, seed, spacing_vox=5.0, disp_vox=3.0):
+    """Seeded blob phantoms (floating = reference warped by a 5-voxel FFD), `per_shape` distinct
+    pairs per size; requests draw from this pool (the device work per request is the same as
+    for a fresh pair of that size)."""
+    from niftyreg_b200 import phantom
+    pool = {}
+    for k, shp in enumerate(shapes):
+        pool[shp] = [phantom.blobs_pair(shp, seed=seed + 100 * k + j, spacing_vox=spacing_vox,
+                                        disp_sigma_vox=disp_vox) for j in range(per_shape)]
+    return pool
+
+
+def _gpu_clock_sampler():
+    import torch
+    return ClockSampler(torch.cuda.current_device())
+
+
+def run_batched(args):
+    """`--pairs` registrations with sizes drawn uniformly from BATCH_SHAPES: first one by one
+    through the plain path (nrb_f3d_register_host), then all at once through
+    nrb_f3d_register_batch with `--concurrency` registrations in flight. Reports both rates and
+    the largest |dNMI| between a pair's plain and batched results."""
+    import torch
+    import niftyreg_b200 as nrb
+    torch.cuda.set_device(0)
+    nrb.build()
+    rng = np.random.default_rng(args.seed)
+    pool = _phantom_pool(BATCH_SHAPES, 2, args.seed)
+    picks = [BATCH_SHAPES[i] for i in rng.integers(0, len(BATCH_SHAPES), args.pairs)]
+    pairs = [pool[s][int(rng.integers(0, 2))] for s in picks]
+    params = nrb.default_params(levels=BATCH_LEVELS, max_iterations=BATCH_MAXIT, bending_energy=BE,
+                                spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS)
+    # warm-up: one registration of every size
+    for s in BATCH_SHAPES:
+        p = pool[s][0]
+        nrb.register_host(p.reference, p.floating, p.pixdim, params)
+    sampler = _gpu_clock_sampler()
+    sampler.start()
+    t0 = time.perf_counter()
+    plain = [nrb.register_host(p.reference, p.floating, p.pixdim, params) for p in pairs]
+    t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    batched = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], params, args.concurrency)
+    t_batch = time.perf_counter() - t0
+    clocks = sampler.stop()
+    dnmi = max(abs(a[1].final_nmi - b[1].final_nmi) for a, b in zip(plain, batched))
+    identical = all(np.array_equal(a[0], b[0]) for a, b in zip(plain, batched))
+    line = {"mode": "batched", "metric": METRIC, "value": args.pairs / t_batch, "unit": "registrations/s",
+            "plain_value": args.pairs / t_plain, "speedup_vs_plain": t_plain / t_batch, "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.pairs} pairs, sizes uniform over {BATCH_SHAPES} (nz, ny, nx), blob "
+                                   f"phantoms (2 distinct pairs per size), {BATCH_LEVELS} levels, {BATCH_MAXIT} "
+                                   f"counted iterations at the finest level, NMI {BINS} bins, BE {BE}, 5-voxel grid",
+                       "concurrency": args.concurrency, "timing": "host wall clock, host images, copies included"},
+            "max_abs_dnmi_vs_plain": dnmi, "bitwise_identical_to_plain": identical, "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
+def run_served(args):
+    """Open-loop Poisson request streams at each rate of `--rates`: sizes drawn from SERVE_MIX,
+    admitted by a server with `--concurrency` slots under 80% of free HBM. Reports latency
+    percentiles (submit -> result) and the achieved rate; the plain rate is the same request mix
+    registered one by one."""
+    import queue
+    import threading
+    import torch
+    import niftyreg_b200 as nrb
+    torch.cuda.set_device(0)
+    nrb.build()
+    rng = np.random.default_rng(args.seed)
+    shapes = [s for s, _ in SERVE_MIX]
+    probs = np.array([w for _, w in SERVE_MIX])
+    pool = _phantom_pool(shapes, 2, args.seed)
+    params = nrb.default_params(levels=SERVE_LEVELS, max_iterations=SERVE_MAXIT, bending_energy=BE,
+                                spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS)
+    for s in shapes:
+        p = pool[s][0]
+        nrb.register_host(p.reference, p.floating, p.pixdim, params)
+    # plain reference rate of the mix, one by one
+    n_plain = 40
+    mix = [pool[shapes[int(i)]][int(rng.integers(0, 2))] for i in rng.choice(len(shapes), n_plain, p=probs)]
+    t0 = time.perf_counter()
+    alone = {}
+    for p in mix:
+        _, r = nrb.register_host(p.reference, p.floating, p.pixdim, params)
+        alone[id(p)] = r.final_nmi
+    plain_rate = n_plain / (time.perf_counter() - t0)
+    results = []
+    sampler = _gpu_clock_sampler()
+    sampler.start()
+    for rate in [float(x) for x in args.rates.split(",")]:
+        reqs = [pool[shapes[int(i)]][int(rng.integers(0, 2))]
+                for i in rng.choice(len(shapes), args.requests, p=probs)]
+        gaps = rng.exponential(1.0 / rate, args.requests)
+        lat, dn = [], []
+        with nrb.Server(slots=args.concurrency) as srv:
+            tq = queue.Queue()
+
+            def drain():
+                # waits in submission order; latency is measured by the server (submit -> result)
+                while True:
+                    item = tq.get()
+                    if item is None:
+                        return
+                    t, p = item
+                    _, r, _, l = srv.wait(t)
+                    lat.append(l)
+                    if id(p) in alone:
+                        dn.append(abs(r.final_nmi - alone[id(p)]))
+
+            th = threading.Thread(target=drain)
+            th.start()
+            t_start = time.perf_counter()
+            due = t_start
+            for p, g in zip(reqs, gaps):
+                due += g
+                now = time.perf_counter()
+                if due > now:
+                    time.sleep(due - now)
+                tq.put((srv.submit(p.reference, p.floating, p.pixdim, params), p))
+            tq.put(None)
+            th.join()
+            t_end = time.perf_counter()
+            peak_bytes, peak_active = srv.stats()
+        lat_ms = np.array(lat) * 1e3
+        results.append({"rate_req_s": rate, "requests": args.requests,
+                        "achieved_req_s": args.requests / (t_end - t_start),
+                        "p50_ms": float(np.percentile(lat_ms, 50)), "p95_ms": float(np.percentile(lat_ms, 95)),
+                        "p99_ms": float(np.percentile(lat_ms, 99)), "peak_concurrent": peak_active,
+                        "peak_admitted_gb": peak_bytes / 1e9,
+                        "max_abs_dnmi_vs_alone": float(max(dn)) if dn else None})
+    clocks = sampler.stop()
+    best = max(results, key=lambda r: r["achieved_req_s"])
+    line = {"mode": "served", "metric": METRIC, "value": best["achieved_req_s"], "unit": "registrations/s",
+            "p99_ms": best["p99_ms"], "plain_value": plain_rate, "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"open-loop Poisson requests, sizes {SERVE_MIX} ((nz, ny, nx), probability), "
+                                   f"blob phantoms (2 distinct pairs per size), {SERVE_LEVELS} levels, {SERVE_MAXIT} "
+                                   f"counted iterations at the finest level, NMI {BINS} bins, BE {BE}, 5-voxel grid",
+                       "slots": args.concurrency, "admission": "FIFO against 80% of free HBM"},
+            "sweep": results, "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.kernel:
         return run_kernel_only(args)
+    if args.mode == "batched":
+        return run_batched(args)
+    if args.mode == "served":
+        return run_served(args)
     return run_b200(args)
 
 

@@ -244,6 +244,10 @@ typedef struct nrb_f3d_params {
     int32_t flo_bins;         /* --fbn */
     float padding;            /* -pad: warped padding value (NaN by default) */
     int32_t verbose;
+    int32_t host_loop;        /* 0 (default): each level's optimisation runs as one CUDA graph
+                               * with the optimiser state on the device; 1: the host takes every
+                               * line-search branch (one synchronising read per evaluation).
+                               * Both take the same steps. Per-kernel timing forces 1. */
 } nrb_f3d_params;
 
 typedef struct nrb_f3d_result {
@@ -277,6 +281,46 @@ nrb_status nrb_f3d_register_device(const float *ref, const float *flo, const int
                                    const float pixdim[3], const nrb_f3d_params *p,
                                    float *cpp_out, int64_t cpp_capacity, nrb_f3d_result *result,
                                    void *stream);
+
+/* ---- batched and served registrations (no counterpart in the reference) -------------------- */
+
+/* One registration request: host images (valid until the request completes), the reference's
+ * geometry (identity orientation, origin 0) and where the final grid goes. */
+typedef struct nrb_pair {
+    const float *ref_host;
+    const float *flo_host;
+    int32_t dim[3];
+    float pixdim[3];
+    float *cpp_out_host;      /* 3 * prod(cpp_dim) floats (nrb_f3d_grid_dims), or NULL */
+    int64_t cpp_capacity;
+} nrb_pair;
+
+/* Peak device bytes one registration of this size needs (the admission unit of a server). */
+nrb_status nrb_f3d_footprint(const int32_t dim[3], const float pixdim[3], const nrb_f3d_params *p,
+                             int64_t *bytes);
+
+/* A registration server on the current device: `slots` workers, each with its own stream, take
+ * requests in arrival order as soon as a worker is free and the request's footprint fits in
+ * what is left of hbm_budget_bytes (<= 0: 80% of the free device memory). Admitted requests run
+ * concurrently and their kernels overlap; each result is the one nrb_f3d_register_host gives
+ * for the same request alone. */
+typedef struct nrb_server nrb_server;
+nrb_status nrb_server_create(int slots, int64_t hbm_budget_bytes, nrb_server **out);
+nrb_status nrb_server_submit(nrb_server *s, const nrb_pair *req, const nrb_f3d_params *p,
+                             int64_t *ticket);
+/* Blocks until the request ends; queue_seconds = submit -> admission, latency_seconds =
+ * submit -> result. */
+nrb_status nrb_server_wait(nrb_server *s, int64_t ticket, nrb_f3d_result *result,
+                           double *queue_seconds, double *latency_seconds);
+/* Peak admitted footprint and peak number of concurrent registrations so far. */
+nrb_status nrb_server_stats(nrb_server *s, int64_t *peak_bytes, int32_t *peak_active);
+/* Finishes the queued requests, then stops the workers. */
+void nrb_server_destroy(nrb_server *s);
+
+/* n registrations, up to `concurrency` at once under hbm_budget_bytes (<= 0: 80% of free). */
+nrb_status nrb_f3d_register_batch(const nrb_pair *pairs, int n, const nrb_f3d_params *p,
+                                  int concurrency, int64_t hbm_budget_bytes,
+                                  nrb_f3d_result *results);
 
 /* Number of kernel launches issued by this library in this process so far. */
 int64_t nrb_kernel_launch_count(void);

@@ -61,7 +61,8 @@ class Objective(ctypes.Structure):
 class F3dParams(ctypes.Structure):
     _fields_ = [("levels", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
                 ("bending_energy", ctypes.c_float), ("spacing", _F3), ("ref_bins", ctypes.c_int32),
-                ("flo_bins", ctypes.c_int32), ("padding", ctypes.c_float), ("verbose", ctypes.c_int32)]
+                ("flo_bins", ctypes.c_int32), ("padding", ctypes.c_float), ("verbose", ctypes.c_int32),
+                ("host_loop", ctypes.c_int32)]
 
 
 class F3dResult(ctypes.Structure):
@@ -333,6 +334,92 @@ def register_host(ref: np.ndarray, flo: np.ndarray, pixdim, params: F3dParams):
                                       cpp.ctypes.data_as(ctypes.c_void_p), ctypes.c_int64(cpp.size),
                                       ctypes.byref(res)))
     return cpp, res
+
+
+class PairDesc(ctypes.Structure):
+    """nrb_pair: one registration request with host images."""
+    _fields_ = [("ref_host", ctypes.c_void_p), ("flo_host", ctypes.c_void_p), ("dim", _I3), ("pixdim", _F3),
+                ("cpp_out_host", ctypes.c_void_p), ("cpp_capacity", ctypes.c_int64)]
+
+
+def footprint(dim, pixdim, params: F3dParams) -> int:
+    """Peak device bytes of one registration (the server's admission unit)."""
+    out = ctypes.c_int64()
+    check(lib().nrb_f3d_footprint(_I3(*[int(v) for v in dim]), _F3(*[float(v) for v in pixdim]),
+                                  ctypes.byref(params), ctypes.byref(out)))
+    return int(out.value)
+
+
+class _Request:
+    """Host buffers of one request, kept alive until its result is read."""
+
+    def __init__(self, ref, flo, pixdim, params):
+        self.ref = np.ascontiguousarray(ref, np.float32)
+        self.flo = np.ascontiguousarray(flo, np.float32)
+        nz, ny, nx = self.ref.shape
+        cd = grid_dims((nx, ny, nz), pixdim, params)
+        self.cpp = np.zeros((3, cd[2], cd[1], cd[0]), np.float32)
+        self.params = params
+        self.desc = PairDesc(self.ref.ctypes.data, self.flo.ctypes.data, _I3(nx, ny, nz),
+                             _F3(*[float(v) for v in pixdim]), self.cpp.ctypes.data, self.cpp.size)
+
+
+class Server:
+    """Continuous-batching registration server on the current device (nrb_server_*): `slots`
+    concurrent registrations, admitted in arrival order against an HBM budget in bytes
+    (0 = 80% of the free device memory)."""
+
+    def __init__(self, slots: int, budget_bytes: int = 0):
+        self.h = ctypes.c_void_p()
+        L = lib()
+        L.nrb_server_destroy.restype = None
+        check(L.nrb_server_create(int(slots), ctypes.c_int64(budget_bytes), ctypes.byref(self.h)))
+        self._pending = {}
+
+    def submit(self, ref, flo, pixdim, params: F3dParams) -> int:
+        req = _Request(ref, flo, pixdim, params)
+        t = ctypes.c_int64()
+        check(lib().nrb_server_submit(self.h, ctypes.byref(req.desc), ctypes.byref(params), ctypes.byref(t)))
+        self._pending[t.value] = req
+        return int(t.value)
+
+    def wait(self, ticket: int):
+        """(cpp [3, cz, cy, cx], F3dResult, queue seconds, latency seconds)."""
+        res, q, lat = F3dResult(), ctypes.c_double(), ctypes.c_double()
+        try:
+            check(lib().nrb_server_wait(self.h, ctypes.c_int64(ticket), ctypes.byref(res), ctypes.byref(q),
+                                        ctypes.byref(lat)))
+        finally:
+            req = self._pending.pop(ticket, None)
+        return req.cpp, res, q.value, lat.value
+
+    def stats(self):
+        """(peak admitted bytes, peak concurrent registrations)."""
+        b, a = ctypes.c_int64(), ctypes.c_int32()
+        check(lib().nrb_server_stats(self.h, ctypes.byref(b), ctypes.byref(a)))
+        return int(b.value), int(a.value)
+
+    def close(self):
+        if self.h:
+            lib().nrb_server_destroy(self.h)
+            self.h = ctypes.c_void_p()
+            self._pending.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def register_batch(pairs, params: F3dParams, concurrency: int, budget_bytes: int = 0):
+    """pairs: list of (ref, flo, pixdim) host volumes. Returns [(cpp, F3dResult)] in order."""
+    reqs = [_Request(r, f, p, params) for r, f, p in pairs]
+    descs = (PairDesc * len(reqs))(*[q.desc for q in reqs])
+    results = (F3dResult * len(reqs))()
+    check(lib().nrb_f3d_register_batch(descs, len(reqs), ctypes.byref(params), int(concurrency),
+                                       ctypes.c_int64(budget_bytes), results))
+    return [(q.cpp, results[i]) for i, q in enumerate(reqs)]
 
 
 def register_device(ref, flo, dim, pixdim, params: F3dParams, cpp_out, capacity, stream=None) -> F3dResult:

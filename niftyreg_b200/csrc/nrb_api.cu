@@ -81,6 +81,11 @@ void resolve_pending() {
 }
 }  // namespace
 
+bool timing_enabled() {
+    std::lock_guard<std::mutex> lock(g_tmu);
+    return g_timing;
+}
+
 KernelTimer::KernelTimer(TimedKernel k, double bytes, cudaStream_t st): k_(k), bytes_(bytes), st_(st) {
     std::lock_guard<std::mutex> lock(g_tmu);
     if (!g_timing) return;
@@ -169,7 +174,8 @@ extern "C" int nrb_device_ok(void) {
     return major == 10 ? 1 : 0;
 }
 
-extern "C" nrb_status nrb_nmi_create(int ref_bins, int flo_bins, nrb_nmi **out) {
+namespace nrb {
+nrb_status nmi_create_on(int ref_bins, int flo_bins, cudaStream_t st, nrb_nmi **out) {
     if (!out || ref_bins < 5 || flo_bins < 5 || ref_bins > 1024 || flo_bins > 1024)
         return fail(NRB_ERR_INVALID, "nrb_nmi_create: bins must be in [5, 1024] (internal counts, user bins + 4)");
     if ((size_t)ref_bins * flo_bins * 4 > 180 * 1024)
@@ -178,15 +184,20 @@ extern "C" nrb_status nrb_nmi_create(int ref_bins, int flo_bins, nrb_nmi **out) 
     n->rb = ref_bins;
     n->fb = flo_bins;
     n->total = ref_bins * flo_bins + ref_bins + flo_bins;
+    n->st = st;
     cudaGetDevice(&n->device);
-    if (cudaMalloc(&n->hist, (size_t)ref_bins * flo_bins * 4) != cudaSuccess ||
-        cudaMalloc(&n->pro, (size_t)n->total * 8) != cudaSuccess ||
-        cudaMalloc(&n->logt, (size_t)n->total * 8) != cudaSuccess ||
-        cudaMalloc(&n->last, sizeof(nrb_objective)) != cudaSuccess ||
-        cudaMemset(n->hist, 0, (size_t)ref_bins * flo_bins * 4) != cudaSuccess ||
-        cudaMemset(n->pro, 0, (size_t)n->total * 8) != cudaSuccess ||
-        cudaMemset(n->logt, 0, (size_t)n->total * 8) != cudaSuccess ||
-        cudaMemset(n->last, 0, sizeof(nrb_objective)) != cudaSuccess) {
+    const size_t hb = (size_t)ref_bins * flo_bins * 4, tb = (size_t)n->total * 8;
+    bool ok = dev_alloc(&n->hist, hb, st) == cudaSuccess && dev_alloc(&n->pro, tb, st) == cudaSuccess &&
+              dev_alloc(&n->logt, tb, st) == cudaSuccess && dev_alloc(&n->last, sizeof(nrb_objective), st) == cudaSuccess;
+    if (ok && st) {
+        ok = cudaMemsetAsync(n->hist, 0, hb, st) == cudaSuccess && cudaMemsetAsync(n->pro, 0, tb, st) == cudaSuccess &&
+             cudaMemsetAsync(n->logt, 0, tb, st) == cudaSuccess &&
+             cudaMemsetAsync(n->last, 0, sizeof(nrb_objective), st) == cudaSuccess;
+    } else if (ok) {
+        ok = cudaMemset(n->hist, 0, hb) == cudaSuccess && cudaMemset(n->pro, 0, tb) == cudaSuccess &&
+             cudaMemset(n->logt, 0, tb) == cudaSuccess && cudaMemset(n->last, 0, sizeof(nrb_objective)) == cudaSuccess;
+    }
+    if (!ok) {
         cudaGetLastError();
         nrb_nmi_destroy(n);
         return fail(NRB_ERR_OOM, "nrb_nmi_create: device allocation failed");
@@ -194,13 +205,18 @@ extern "C" nrb_status nrb_nmi_create(int ref_bins, int flo_bins, nrb_nmi **out) 
     *out = n;
     return NRB_OK;
 }
+}  // namespace nrb
+
+extern "C" nrb_status nrb_nmi_create(int ref_bins, int flo_bins, nrb_nmi **out) {
+    return nmi_create_on(ref_bins, flo_bins, nullptr, out);
+}
 
 extern "C" void nrb_nmi_destroy(nrb_nmi *nmi) {
     if (!nmi) return;
-    cudaFree(nmi->hist);
-    cudaFree(nmi->pro);
-    cudaFree(nmi->logt);
-    cudaFree(nmi->last);
+    dev_free(nmi->hist, nmi->st);
+    dev_free(nmi->pro, nmi->st);
+    dev_free(nmi->logt, nmi->st);
+    dev_free(nmi->last, nmi->st);
     delete nmi;
 }
 
@@ -233,11 +249,15 @@ extern "C" nrb_status nrb_f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const n
     NRB_TRY(check_fused_args(ws, nmi, g, ref, flo, cpp));
     cudaStream_t st = as_stream(stream);
     int n_be = 0;
+    const bool overlap = be_weight > 0 && sim_weight > 0;
     if (be_weight > 0) {
-        NRB_TRY(launch_be_value(ws, g, cpp, st));
+        // the bending energy reads only the grid: it runs beside the voxel pass
+        if (overlap) NRB_TRY(fork_side(ws, st));
+        NRB_TRY(launch_be_value(ws, g, cpp, overlap ? ws->side : st));
         n_be = be_partial_count(g);
     }
     if (sim_weight > 0) NRB_TRY(launch_fused_objective(ws, nmi, g, ref, flo, mask, cpp, padding, st));
+    if (overlap) NRB_TRY(join_side(ws, st));
     NRB_TRY(launch_nmi_finalize(nmi, ws->be_partials, n_be, 3 * nvox(g->cpp_dim), sim_weight, be_weight, obj, st));
     if (obj_host) {
         NRB_CUDA(cudaMemcpyAsync(obj_host, obj ? obj : nmi->last, sizeof(nrb_objective), cudaMemcpyDeviceToHost, st));
@@ -253,6 +273,12 @@ extern "C" nrb_status nrb_f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nr
     NRB_TRY(check_fused_args(ws, nmi, g, ref, flo, cpp));
     if (!vgrad || !node_grad) return fail(NRB_ERR_INVALID, "nrb_f3d_gradient: null buffer");
     cudaStream_t st = as_stream(stream);
+    const bool overlap = be_weight > 0 && sim_weight > 0;
+    if (overlap) {
+        // the bending-energy derivatives read only the grid: they run beside the voxel passes
+        NRB_TRY(fork_side(ws, st));
+        NRB_TRY(launch_be_derivatives(ws, g, cpp, ws->side));
+    }
     if (sim_weight > 0) {
         // the histogram of the current position feeds the log table of the voxel gradient
         NRB_TRY(launch_fused_objective(ws, nmi, g, ref, flo, mask, cpp, padding, st));
@@ -262,6 +288,10 @@ extern "C" nrb_status nrb_f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nr
     } else {
         NRB_CUDA(cudaMemsetAsync(node_grad, 0, 3 * nvox(g->cpp_dim) * sizeof(float), st));
     }
-    if (be_weight > 0) NRB_TRY(nrb_approx_bending_energy_gradient(ws, g, cpp, (float)be_weight, node_grad, stream));
+    if (be_weight > 0) {
+        if (overlap) NRB_TRY(join_side(ws, st));
+        else NRB_TRY(launch_be_derivatives(ws, g, cpp, st));
+        NRB_TRY(launch_be_accumulate(ws, g, (float)be_weight, node_grad, st));
+    }
     return NRB_OK;
 }

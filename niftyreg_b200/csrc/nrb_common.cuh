@@ -41,6 +41,18 @@ extern std::atomic<long long> g_launch_count;
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Device allocation tied to an owner's stream: stream-ordered (no device-wide synchronisation,
+// so registrations on other streams keep running) when `st` is set, plain otherwise.
+template <typename T>
+inline cudaError_t dev_alloc(T **p, size_t bytes, cudaStream_t st) {
+    return st ? cudaMallocAsync(reinterpret_cast<void **>(p), bytes, st) : cudaMalloc(reinterpret_cast<void **>(p), bytes);
+}
+inline void dev_free(void *p, cudaStream_t st) {
+    if (!p) return;
+    if (st) cudaFreeAsync(p, st);
+    else cudaFree(p);
+}
+
 // Optional per-kernel CUDA-event timing (nrb_timing_enable). A KernelTimer brackets one launch
 // with events on its stream and records the algorithmic bytes that launch must move.
 enum TimedKernel { TK_OBJECTIVE = 0, TK_GRADIENT, TK_FINALIZE, TK_CONV, TK_BE_VALUE, TK_BE_GRADIENT, TK_COUNT };
@@ -54,6 +66,10 @@ private:
     cudaStream_t st_;
     cudaEvent_t a_ = nullptr;
 };
+
+// True while nrb_timing_enable(1) is in force (launch sequences that are captured into CUDA
+// graphs then run eagerly instead, so each launch keeps its events).
+bool timing_enabled();
 
 // Number of SMs of the current device (cached per device).
 int sm_count();

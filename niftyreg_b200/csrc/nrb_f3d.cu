@@ -20,6 +20,142 @@ nrb_status grid_identity(const int32_t cdim[3], const float cxyz[16], float *cpp
 nrb_status grid_refine(const int32_t odim[3], const float *old, const int32_t ndim[3], float *out, cudaStream_t st);
 nrb_status rescale_with(float *img, int64_t n, float lo, float hi, float *fred, cudaStream_t st);
 nrb_status max_and_normalise(nrb_workspace *ws, float *grad, int64_t nnode, nrb_objective *obj, cudaStream_t st);
+nrb_status cg_update_flagged(nrb_workspace *ws, float *grad, float *g1, float *g2, int64_t n, const int *first_call,
+                             cudaStream_t st);
+
+// ---------------------------------------------------------------------------------------------
+// Device-resident optimiser: the state of ConjugateGradient<float>::Optimise and of the level
+// loop of reg_base::Run (reg-lib/Optimiser.cpp:129-173, reg-lib/_reg_base.cpp:760-800), kept in
+// device memory and advanced by single-thread control kernels, so a whole level runs as one
+// CUDA graph whose two WHILE nodes (iterations, line-search steps) read conditions the control
+// kernels set. The arithmetic on the step lengths and objective values is the host loop's,
+// operation for operation.
+// ---------------------------------------------------------------------------------------------
+struct OptState {
+    double best_obj, best_w_measure, best_w_be, best_nmi, best_be;
+    long long it, max_it, n_obj, n_grad;
+    float current_size, max_step, small_step, cur_len, added_len;
+    int line_iter, first_call, just_restarted, accepted;
+};
+
+__device__ __forceinline__ bool outer_continues(const OptState& s) { return s.current_size != 0.f && s.it < s.max_it; }
+__device__ __forceinline__ bool line_continues(const OptState& s) {
+    return s.cur_len > s.small_step && s.line_iter < 12 && s.it < s.max_it;
+}
+
+__global__ void k_ctl_level(OptState *s, OptState init, cudaGraphConditionalHandle outer) {
+    *s = init;
+    cudaGraphSetConditional(outer, outer_continues(init) ? 1u : 0u);
+}
+
+// after GetObjectiveFunctionGradient: iteration counted; current_size = min(current_size, max_step)
+__global__ void k_ctl_gradient_done(OptState *s) {
+    s->it += 1;
+    s->n_grad += 1;
+    s->current_size = s->max_step < s->current_size ? s->max_step : s->current_size;
+}
+
+// Optimiser::Optimise entry (after UpdateGradientValues consumed first_call)
+__global__ void k_ctl_line_start(OptState *s, cudaGraphConditionalHandle inner) {
+    s->first_call = 0;
+    s->line_iter = 0;
+    s->added_len = 0.f;
+    s->cur_len = s->current_size;
+    cudaGraphSetConditional(inner, line_continues(*s) ? 1u : 0u);
+}
+
+// one line-search step after its objective evaluation
+__global__ void k_ctl_line_step(OptState *s, const nrb_objective *o, float sim_w, float be_w,
+                                cudaGraphConditionalHandle inner) {
+    const double wm = sim_w > 0 ? (double)sim_w * o->nmi : 0.0;
+    const double wb = be_w > 0 ? (double)be_w * o->be : 0.0;
+    const double value = __dsub_rn(wm, wb);
+    s->n_obj += 1;
+    if (value > s->best_obj) {
+        s->best_w_measure = wm;
+        s->best_w_be = wb;
+        s->best_nmi = o->nmi;
+        s->best_be = o->be;
+        s->best_obj = value;
+        s->added_len = __fadd_rn(s->added_len, s->cur_len);
+        const float c = __fmul_rn(s->cur_len, 1.1f);
+        s->cur_len = s->max_step < c ? s->max_step : c;
+        s->accepted = 1;
+    } else {
+        s->cur_len = __fmul_rn(s->cur_len, 0.5f);
+        s->accepted = 0;
+    }
+    s->it += 1;
+    s->line_iter += 1;
+    cudaGraphSetConditional(inner, line_continues(*s) ? 1u : 0u);
+}
+
+// end of Optimise (start length = added length) and the restart rule of _reg_base.cpp:784-793
+__global__ void k_ctl_line_end(OptState *s, cudaGraphConditionalHandle outer) {
+    s->current_size = s->added_len;
+    if (s->current_size == 0.f) {
+        if (!s->just_restarted && s->it < s->max_it) {
+            s->first_call = 1;
+            s->current_size = s->max_step;
+            s->just_restarted = 1;
+        }
+    } else {
+        s->just_restarted = 0;
+    }
+    cudaGraphSetConditional(outer, outer_continues(*s) ? 1u : 0u);
+}
+
+// cur = best + (-len) * grad, len read from the state (UpdateControlPointPosition)
+__global__ void k_update_from_state(long long n, float *__restrict__ cur, const float *__restrict__ best,
+                                    const float *__restrict__ grad, const OptState *__restrict__ s) {
+    const float scale = -s->cur_len;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        cur[i] = __fadd_rn(best[i], __fmul_rn(scale, grad[i]));
+}
+
+// dst = src; with `s`, only after an accepted step (StoreCurrentDof)
+__global__ void k_copy_dof(long long n, float *__restrict__ dst, const float *__restrict__ src,
+                           const OptState *__restrict__ s) {
+    if (s && !s->accepted) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+int elementwise_grid(long long n) {
+    return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 4LL * 148));
+}
+
+struct GraphHolder {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~GraphHolder() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (g) cudaGraphDestroy(g);
+    }
+};
+
+// Appends a WHILE node driven by `h` to the graph `st` is capturing, after everything captured
+// so far, and returns its body graph; capture then continues after the node.
+nrb_status capture_while(cudaStream_t st, cudaGraphConditionalHandle h, cudaGraph_t *body) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t capg = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    NRB_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &capg, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return fail(NRB_ERR_CUDA, "registration: stream capture not active");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    NRB_CUDA(cudaGraphAddNode(&node, capg, deps, nd, &cp));
+    *body = cp.conditional.phGraph_out[0];
+    NRB_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return NRB_OK;
+}
 
 namespace {
 
@@ -56,13 +192,17 @@ struct Header {
     int64_t n() const { return (int64_t)dim[0] * dim[1] * dim[2]; }
 };
 
+// Every buffer of a registration is allocated and freed in the order of the registration's
+// stream, so concurrent registrations on other streams never wait for each other's frees.
 struct DevBuf {
     float *p = nullptr;
-    ~DevBuf() { cudaFree(p); }
-    nrb_status alloc(size_t n) {
-        cudaFree(p);
+    cudaStream_t st = nullptr;
+    ~DevBuf() { dev_free(p, st); }
+    nrb_status alloc(size_t n, cudaStream_t s) {
+        dev_free(p, st);
         p = nullptr;
-        if (cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(float)) != cudaSuccess) {
+        st = s;
+        if (dev_alloc(&p, std::max<size_t>(n, 1) * sizeof(float), st) != cudaSuccess) {
             cudaGetLastError();
             return fail(NRB_ERR_OOM, "registration: device allocation failed");
         }
@@ -152,6 +292,34 @@ private:
         return RestoreBestDof();
     }
 
+    // the level loop of reg_base::Run on the host (one synchronising read per evaluation)
+    nrb_status RunLevelHost(float max_step, float smallest_size, float current_size) {
+        bool just_restarted = false;
+        while (current_size) {
+            if (it_ >= max_it_) break;
+            NRB_TRY(GetObjectiveFunctionGradient());
+            current_size = std::min(current_size, max_step);
+            NRB_TRY(Optimise(max_step, smallest_size, current_size));
+            if (p_.verbose)
+                printf("[nrb] [%zu] objective %.6f = (wSIM)%.6f - (wBE)%.6g [+ %g mm]\n", it_, best_obj_,
+                       best_w_measure_, best_w_be_, current_size);
+            // _reg_base.cpp:784-793: one restart to steepest descent on a stalled line search
+            if (current_size == 0) {
+                if (!just_restarted && it_ < max_it_) {
+                    first_call_ = true;
+                    current_size = max_step;
+                    just_restarted = true;
+                }
+            } else {
+                just_restarted = false;
+            }
+        }
+        return NRB_OK;
+    }
+    nrb_status RunLevelGraph(float max_step, float smallest_size, float current_size);
+    nrb_status CaptureGradient(cudaStream_t cs);
+    nrb_status CaptureObjective(cudaStream_t cs);
+
     nrb_status BuildPyramid(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3]);
     nrb_status CreateGrid();
     nrb_status InitLevel(int level, float& max_step);
@@ -180,7 +348,144 @@ private:
     double cur_w_measure_ = 0, cur_w_be_ = 0, best_w_measure_ = 0, best_w_be_ = 0;
     double cur_nmi_ = 0, cur_be_ = 0, best_nmi_ = 0, best_be_ = 0;
     int64_t n_obj_ = 0, n_grad_ = 0;
+    // device-resident optimiser
+    bool graph_ok_ = true;
+    OptState *dstate_ = nullptr;
+    cudaStream_t cap_st_ = nullptr;
+
+public:
+    ~F3dRegistration() {
+        dev_free(dstate_, st_);
+        if (cap_st_) cudaStreamDestroy(cap_st_);
+    }
+    void UseGraphs(bool on) { graph_ok_ = on; }
 };
+
+// GetObjectiveFunctionGradient as captured launches: fused gradient, then NormaliseGradient
+nrb_status F3dRegistration::CaptureGradient(cudaStream_t cs) {
+    NRB_TRY(nrb_f3d_gradient(ws_.h, nmi_.h, &g_, ref_.p, flo_.p, nullptr, cur_.p, pad_, sim_w_, be_w_, vgrad_.p,
+                             grad_.p, cs));
+    NRB_TRY(max_and_normalise(ws_.h, grad_.p, nc_, obj_, cs));
+    k_ctl_gradient_done<<<1, 1, 0, cs>>>(dstate_);
+    NRB_LAUNCHED("k_ctl_gradient_done");
+    return NRB_OK;
+}
+
+// GetObjectiveFunctionValue as captured launches (the value stays on the device)
+nrb_status F3dRegistration::CaptureObjective(cudaStream_t cs) {
+    return nrb_f3d_objective(ws_.h, nmi_.h, &g_, ref_.p, flo_.p, nullptr, cur_.p, pad_, sim_w_, be_w_, obj_,
+                             nullptr, cs);
+}
+
+// One level of reg_base::Run as one CUDA graph:
+//   level init -> WHILE(iterations) { gradient, CG direction, line start,
+//                                     WHILE(line search) { update, objective, step, store },
+//                                     line end + restart rule, restore best }
+// launched once; the host reads the optimiser state back when it ends.
+nrb_status F3dRegistration::RunLevelGraph(float max_step, float smallest_size, float current_size) {
+    if (!cap_st_) NRB_CUDA(cudaStreamCreateWithFlags(&cap_st_, cudaStreamNonBlocking));
+    if (!dstate_) NRB_CUDA(dev_alloc(&dstate_, sizeof(OptState), st_));
+    const long long n = 3 * nc_;
+    OptState init = {};
+    init.best_obj = best_obj_;
+    init.best_w_measure = best_w_measure_;
+    init.best_w_be = best_w_be_;
+    init.best_nmi = best_nmi_;
+    init.best_be = best_be_;
+    init.it = (long long)it_;
+    init.max_it = (long long)max_it_;
+    init.n_obj = n_obj_;
+    init.n_grad = n_grad_;
+    init.current_size = current_size;
+    init.max_step = max_step;
+    init.small_step = smallest_size;
+    init.first_call = first_call_ ? 1 : 0;
+
+    GraphHolder top;
+    cudaGraph_t outer_body = nullptr, inner_body = nullptr;
+    cudaGraphConditionalHandle h_outer, h_inner;
+    NRB_CUDA(cudaGraphCreate(&top.g, 0));
+    NRB_CUDA(cudaGraphConditionalHandleCreate(&h_outer, top.g, 0, 0));
+    const long long c0 = g_launch_count.load();
+    auto abort_capture = [&](nrb_status s) {
+        cudaGraph_t dummy = nullptr;
+        cudaStreamEndCapture(cap_st_, &dummy);
+        cudaGetLastError();
+        return s;
+    };
+    // top level
+    NRB_CUDA(cudaStreamBeginCaptureToGraph(cap_st_, top.g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    k_ctl_level<<<1, 1, 0, cap_st_>>>(dstate_, init, h_outer);
+    if (cudaGetLastError() != cudaSuccess) return abort_capture(fail(NRB_ERR_CUDA, "registration: level init launch"));
+    g_launch_count.fetch_add(1);
+    {
+        nrb_status s = capture_while(cap_st_, h_outer, &outer_body);
+        if (s != NRB_OK) return abort_capture(s);
+    }
+    NRB_CUDA(cudaStreamEndCapture(cap_st_, &top.g));
+    const long long c_top = g_launch_count.load() - c0;
+    // one iteration
+    NRB_CUDA(cudaGraphConditionalHandleCreate(&h_inner, outer_body, 0, 0));
+    NRB_CUDA(cudaStreamBeginCaptureToGraph(cap_st_, outer_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    {
+        nrb_status s = CaptureGradient(cap_st_);
+        if (s == NRB_OK) s = cg_update_flagged(ws_.h, grad_.p, g1_.p, g2_.p, n, &dstate_->first_call, cap_st_);
+        if (s == NRB_OK) {
+            k_ctl_line_start<<<1, 1, 0, cap_st_>>>(dstate_, h_inner);
+            g_launch_count.fetch_add(1);
+            if (cudaGetLastError() != cudaSuccess) s = fail(NRB_ERR_CUDA, "registration: line start launch");
+        }
+        if (s == NRB_OK) s = capture_while(cap_st_, h_inner, &inner_body);
+        if (s == NRB_OK) {
+            k_ctl_line_end<<<1, 1, 0, cap_st_>>>(dstate_, h_outer);
+            k_copy_dof<<<elementwise_grid(n), 256, 0, cap_st_>>>(n, cur_.p, best_.p, nullptr);  // RestoreBestDof
+            g_launch_count.fetch_add(2);
+            if (cudaGetLastError() != cudaSuccess) s = fail(NRB_ERR_CUDA, "registration: line end launch");
+        }
+        if (s != NRB_OK) return abort_capture(s);
+    }
+    NRB_CUDA(cudaStreamEndCapture(cap_st_, &outer_body));
+    const long long c_outer = g_launch_count.load() - c0 - c_top;
+    // one line-search step
+    NRB_CUDA(cudaStreamBeginCaptureToGraph(cap_st_, inner_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    {
+        k_update_from_state<<<elementwise_grid(n), 256, 0, cap_st_>>>(n, cur_.p, best_.p, grad_.p, dstate_);
+        g_launch_count.fetch_add(1);
+        nrb_status s = cudaGetLastError() == cudaSuccess ? NRB_OK : fail(NRB_ERR_CUDA, "registration: update launch");
+        if (s == NRB_OK) s = CaptureObjective(cap_st_);
+        if (s == NRB_OK) {
+            k_ctl_line_step<<<1, 1, 0, cap_st_>>>(dstate_, obj_, sim_w_, be_w_, h_inner);
+            k_copy_dof<<<elementwise_grid(n), 256, 0, cap_st_>>>(n, best_.p, cur_.p, dstate_);  // StoreCurrentDof
+            g_launch_count.fetch_add(2);
+            if (cudaGetLastError() != cudaSuccess) s = fail(NRB_ERR_CUDA, "registration: line step launch");
+        }
+        if (s != NRB_OK) return abort_capture(s);
+    }
+    NRB_CUDA(cudaStreamEndCapture(cap_st_, &inner_body));
+    const long long c_inner = g_launch_count.load() - c0 - c_top - c_outer;
+    g_launch_count.fetch_sub(c_top + c_outer + c_inner);  // counted again below, per execution
+
+    NRB_CUDA(cudaGraphInstantiate(&top.exec, top.g, 0));
+    NRB_CUDA(cudaGraphLaunch(top.exec, st_));
+    OptState out;
+    NRB_CUDA(cudaMemcpyAsync(&out, dstate_, sizeof(OptState), cudaMemcpyDeviceToHost, st_));
+    NRB_CUDA(cudaStreamSynchronize(st_));
+    const long long iters = out.n_grad - n_grad_, steps = out.n_obj - n_obj_;
+    g_launch_count.fetch_add(c_top + iters * c_outer + steps * c_inner);
+    best_obj_ = out.best_obj;
+    best_w_measure_ = out.best_w_measure;
+    best_w_be_ = out.best_w_be;
+    best_nmi_ = out.best_nmi;
+    best_be_ = out.best_be;
+    it_ = (size_t)out.it;
+    n_obj_ = out.n_obj;
+    n_grad_ = out.n_grad;
+    first_call_ = out.first_call != 0;
+    if (p_.verbose)
+        printf("[nrb] level done: %lld iterations, objective %.6f = (wSIM)%.6f - (wBE)%.6g\n", (long long)it_,
+               best_obj_, best_w_measure_, best_w_be_);
+    return NRB_OK;
+}
 
 // reg_createImagePyramid (reg-lib/cpu/_reg_tools.cpp:1705-1733): the finest level is the input,
 // each coarser level halves (ceil) every axis whose current size / 2 is at least 32, after a
@@ -196,13 +501,13 @@ nrb_status F3dRegistration::BuildPyramid(const float *ref, const float *flo, con
         fine.pixdim[i] = pixdim[i];
         fine.origin[i] = 0.f;
     }
-    NRB_TRY(ref_pyr_[levels_ - 1].alloc(fine.n()));
-    NRB_TRY(flo_pyr_[levels_ - 1].alloc(fine.n()));
+    NRB_TRY(ref_pyr_[levels_ - 1].alloc(fine.n(), st_));
+    NRB_TRY(flo_pyr_[levels_ - 1].alloc(fine.n(), st_));
     NRB_CUDA(cudaMemcpyAsync(ref_pyr_[levels_ - 1].p, ref, fine.n() * 4, cudaMemcpyDefault, st_));
     NRB_CUDA(cudaMemcpyAsync(flo_pyr_[levels_ - 1].p, flo, fine.n() * 4, cudaMemcpyDefault, st_));
     if (levels_ == 1) return NRB_OK;
     DevBuf tmp;
-    NRB_TRY(tmp.alloc(4 * fine.n()));
+    NRB_TRY(tmp.alloc(4 * fine.n(), st_));
     for (int l = levels_ - 2; l >= 0; --l) {
         const Header& src = hdr_[l + 1];
         Header& dst = hdr_[l];
@@ -215,13 +520,12 @@ nrb_status F3dRegistration::BuildPyramid(const float *ref, const float *flo, con
         float nxyz[16], oijk[16];
         dst.xyz(nxyz);
         src.ijk(oijk);
-        NRB_TRY(ref_pyr_[l].alloc(dst.n()));
-        NRB_TRY(flo_pyr_[l].alloc(dst.n()));
+        NRB_TRY(ref_pyr_[l].alloc(dst.n(), st_));
+        NRB_TRY(flo_pyr_[l].alloc(dst.n(), st_));
         NRB_TRY(smooth_and_downsample(ref_pyr_[l + 1].p, src.dim, ref_pyr_[l].p, dst.dim, nxyz, oijk, tmp.p, st_));
         NRB_TRY(smooth_and_downsample(flo_pyr_[l + 1].p, src.dim, flo_pyr_[l].p, dst.dim, nxyz, oijk, tmp.p, st_));
     }
-    NRB_CUDA(cudaStreamSynchronize(st_));  // tmp is freed on return
-    return NRB_OK;
+    return NRB_OK;  // tmp is freed in stream order
 }
 
 // reg_f3d::Initialise (_reg_f3d.cpp:161-200) -> reg_createControlPointGrid
@@ -243,7 +547,7 @@ nrb_status F3dRegistration::CreateGrid() {
     }
     float cxyz[16];
     grid_.xyz(cxyz);
-    NRB_TRY(cur_.alloc(3 * grid_.n()));
+    NRB_TRY(cur_.alloc(3 * grid_.n(), st_));
     return grid_identity(grid_.dim, cxyz, cur_.p, st_);
 }
 
@@ -264,7 +568,7 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
             ng.origin[i] = (float)((double)ng.pixdim[i] * -1.0 + (double)r.origin[i]);
         }
         DevBuf refined;
-        NRB_TRY(refined.alloc(3 * ng.n()));
+        NRB_TRY(refined.alloc(3 * ng.n(), st_));
         NRB_TRY(grid_refine(grid_.dim, cur_.p, ng.dim, refined.p, st_));
         std::swap(cur_.p, refined.p);
         grid_ = ng;
@@ -288,15 +592,16 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
     nc_ = grid_.n();
     std::swap(ref_.p, ref_pyr_[level].p);
     std::swap(flo_.p, flo_pyr_[level].p);
-    NRB_TRY(vgrad_.alloc(3 * r.n()));
-    NRB_TRY(grad_.alloc(3 * nc_));
-    NRB_TRY(best_.alloc(3 * nc_));
-    NRB_TRY(g1_.alloc(3 * nc_));
-    NRB_TRY(g2_.alloc(3 * nc_));
+    ref_.st = flo_.st = st_;
+    NRB_TRY(vgrad_.alloc(3 * r.n(), st_));
+    NRB_TRY(grad_.alloc(3 * nc_, st_));
+    NRB_TRY(best_.alloc(3 * nc_, st_));
+    NRB_TRY(g1_.alloc(3 * nc_, st_));
+    NRB_TRY(g2_.alloc(3 * nc_, st_));
     nrb_workspace_destroy(ws_.h);
     ws_.h = nullptr;
-    NRB_TRY(nrb_workspace_create(&g_, &ws_.h));
-    if (!nmi_.h) NRB_TRY(nrb_nmi_create(p_.ref_bins + 4, p_.flo_bins + 4, &nmi_.h));
+    NRB_TRY(workspace_create_on(&g_, st_, &ws_.h));
+    if (!nmi_.h) NRB_TRY(nmi_create_on(p_.ref_bins + 4, p_.flo_bins + 4, st_, &nmi_.h));
     // reg_nmi::InitialiseMeasure: rescale both images to [2, bins - 3]
     NRB_TRY(rescale_with(ref_.p, r.n(), 2.f, (float)(p_.ref_bins + 4) - 3.f, ws_.h->fred, st_));
     NRB_TRY(rescale_with(flo_.p, r.n(), 2.f, (float)(p_.flo_bins + 4) - 3.f, ws_.h->fred, st_));
@@ -341,25 +646,12 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const int32_
         if (p_.verbose)
             printf("[nrb] level %d/%d grid %dx%dx%d, initial objective %.6f = (wSIM)%.6f - (wBE)%.6g\n", level + 1,
                    levels_, grid_.dim[0], grid_.dim[1], grid_.dim[2], best_obj_, best_w_measure_, best_w_be_);
-        bool just_restarted = false;
-        while (current_size) {
-            if (it_ >= max_it_) break;
-            NRB_TRY(GetObjectiveFunctionGradient());
-            current_size = std::min(current_size, max_step);
-            NRB_TRY(Optimise(max_step, smallest_size, current_size));
-            if (p_.verbose)
-                printf("[nrb] [%zu] objective %.6f = (wSIM)%.6f - (wBE)%.6g [+ %g mm]\n", it_, best_obj_,
-                       best_w_measure_, best_w_be_, current_size);
-            // _reg_base.cpp:784-793: one restart to steepest descent on a stalled line search
-            if (current_size == 0) {
-                if (!just_restarted && it_ < max_it_) {
-                    first_call_ = true;
-                    current_size = max_step;
-                    just_restarted = true;
-                }
-            } else {
-                just_restarted = false;
-            }
+        // the graph path needs a non-zero similarity weight (its gradient has no memset branch)
+        // and no per-launch timing; both loops take the same steps
+        if (graph_ok_ && sim_w_ > 0 && !timing_enabled()) {
+            NRB_TRY(RunLevelGraph(max_step, smallest_size, current_size));
+        } else {
+            NRB_TRY(RunLevelHost(max_step, smallest_size, current_size));
         }
         max_it_ /= 2;
     }
@@ -384,6 +676,40 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const int32_
 }
 
 }  // namespace
+
+// One registration of host or device images on `st` (the entry point of the batch and serving
+// drivers, which run several of these concurrently on their own streams).
+nrb_status register_on_stream(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3],
+                              const nrb_f3d_params *p, float *cpp_out, int64_t cap, nrb_f3d_result *res,
+                              cudaStream_t st) {
+    F3dRegistration reg(*p, st);
+    reg.UseGraphs(p->host_loop == 0);
+    return reg.Run(ref, flo, dim, pixdim, cpp_out, cap, res);
+}
+
+// Peak device bytes of one registration: the resident pyramid plus the larger of the pyramid
+// construction scratch and the finest level's working set (voxel gradient, convolution scratch,
+// node arrays, bending-energy derivatives), with slack for the small tables.
+int64_t registration_footprint(const int32_t dim[3], const float pixdim[3], const nrb_f3d_params *p) {
+    int32_t d[3] = { dim[0], dim[1], dim[2] };
+    const int64_t fine = (int64_t)d[0] * d[1] * d[2];
+    int64_t pyramid = 0;
+    for (int l = 0; l < std::max(1, (int)p->levels); ++l) {
+        pyramid += 2 * 4 * (int64_t)d[0] * d[1] * d[2];
+        for (int i = 0; i < 3; ++i)
+            if (d[i] / 2 >= 32) d[i] = ceil_ref((float)(d[i] / 2.0));
+    }
+    int64_t nodes = 1;
+    for (int i = 0; i < 3; ++i) {
+        float s = p->spacing[i];
+        if (s != s) s = p->spacing[0];
+        const float mm = s < 0 ? s * -pixdim[i] : s;
+        nodes *= (int64_t)ceil_ref((float)dim[i] * pixdim[i] / mm + 3.f);
+    }
+    const int64_t build = 16 * fine;
+    const int64_t level = 12 * fine + 24 * fine + (6 * 12 + 72) * nodes;
+    return pyramid + std::max(build, level) + (4 << 20);
+}
 }  // namespace nrb
 
 using namespace nrb;
@@ -400,6 +726,7 @@ extern "C" void nrb_f3d_default_params(nrb_f3d_params *p) {
     p->flo_bins = 64;
     p->padding = std::numeric_limits<float>::quiet_NaN();
     p->verbose = 0;
+    p->host_loop = 0;
 }
 
 extern "C" nrb_status nrb_f3d_grid_dims(const int32_t ref_dim[3], const float ref_pixdim[3], const nrb_f3d_params *p,
@@ -426,8 +753,7 @@ extern "C" nrb_status nrb_f3d_register_device(const float *ref, const float *flo
                                               const float pixdim[3], const nrb_f3d_params *p, float *cpp_out,
                                               int64_t cpp_capacity, nrb_f3d_result *result, void *stream) {
     NRB_TRY(check_register_args(ref, flo, dim, pixdim, p));
-    F3dRegistration reg(*p, as_stream(stream));
-    return reg.Run(ref, flo, dim, pixdim, cpp_out, cpp_capacity, result);
+    return register_on_stream(ref, flo, dim, pixdim, p, cpp_out, cpp_capacity, result, as_stream(stream));
 }
 
 extern "C" nrb_status nrb_f3d_register_host(const float *ref_host, const float *flo_host, const int32_t dim[3],
@@ -438,11 +764,8 @@ extern "C" nrb_status nrb_f3d_register_host(const float *ref_host, const float *
     cudaStream_t st = nullptr;
     NRB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     nrb_status s;
-    {
-        F3dRegistration reg(*p, st);
-        // the pyramid's finest level is copied straight from the host buffers
-        s = reg.Run(ref_host, flo_host, dim, pixdim, cpp_out_host, cpp_capacity, result);
-    }
+    // the pyramid's finest level is copied straight from the host buffers
+    s = register_on_stream(ref_host, flo_host, dim, pixdim, p, cpp_out_host, cpp_capacity, result, st);
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
     if (s == NRB_OK && result)

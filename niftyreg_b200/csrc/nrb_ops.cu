@@ -512,8 +512,20 @@ k_cg_dots(long long n, const float *__restrict__ g, const float *__restrict__ g1
     }
 }
 
+// first_call (optional, device flag): when set, the first-call initialisation g1 = g2 = -g
+// runs instead, so one captured launch serves both branches of UpdateGradientValues.
 __global__ void k_cg_update(long long n, float *__restrict__ g, float *__restrict__ g1,
-                            float *__restrict__ g2, const double *__restrict__ partials, int np) {
+                            float *__restrict__ g2, const double *__restrict__ partials, int np,
+                            const int *__restrict__ first_call) {
+    if (first_call && *first_call) {
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+             i += (long long)gridDim.x * blockDim.x) {
+            const float v = -g[i];
+            g1[i] = v;
+            g2[i] = v;
+        }
+        return;
+    }
     __shared__ double gam;
     if (threadIdx.x == 0) {
         double gg = 0, dgg = 0;
@@ -704,10 +716,14 @@ static nrb_status make_sampling(const nrb_geometry *g, AxisSampling ax[3]) {
     return NRB_OK;
 }
 
+// The source vectors live as long as the workspace, so the stream-ordered copy may finish later.
 template <typename T>
-static nrb_status upload(T *&dst, const std::vector<T>& src, size_t& bytes) {
-    NRB_CUDA(cudaMalloc(&dst, std::max<size_t>(1, src.size()) * sizeof(T)));
-    if (!src.empty()) NRB_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+static nrb_status upload(T *&dst, const std::vector<T>& src, size_t& bytes, cudaStream_t st) {
+    NRB_CUDA(dev_alloc(&dst, std::max<size_t>(1, src.size()) * sizeof(T), st));
+    if (!src.empty()) {
+        if (st) NRB_CUDA(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        else NRB_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
     bytes += src.size() * sizeof(T);
     return NRB_OK;
 }
@@ -749,10 +765,10 @@ static nrb_status workspace_alloc(nrb_workspace *ws) {
     NRB_TRY(make_sampling(g, ws->ax));
     size_t bytes = 0;
     for (int d = 0; d < 3; ++d) {
-        NRB_TRY(upload(ws->d_samples[d], ws->ax[d].samples, bytes));
-        NRB_TRY(upload(ws->d_tap_slot[d], ws->ax[d].tap_slot, bytes));
-        NRB_TRY(upload(ws->d_tap_weight[d], ws->ax[d].tap_weight, bytes));
-        NRB_TRY(upload(ws->d_kernel[d], ws->ax[d].kernel, bytes));
+        NRB_TRY(upload(ws->d_samples[d], ws->ax[d].samples, bytes, ws->st));
+        NRB_TRY(upload(ws->d_tap_slot[d], ws->ax[d].tap_slot, bytes, ws->st));
+        NRB_TRY(upload(ws->d_tap_weight[d], ws->ax[d].tap_weight, bytes, ws->st));
+        NRB_TRY(upload(ws->d_kernel[d], ws->ax[d].kernel, bytes, ws->st));
     }
     const long long nx = g->ref_dim[0], ny = g->ref_dim[1], nz = g->ref_dim[2];
     const long long c1 = 3LL * nz * ny * ws->ax[0].nsamples;
@@ -761,32 +777,53 @@ static nrb_status workspace_alloc(nrb_workspace *ws) {
     (void)nx;
     const long long nc = nvox(g->cpp_dim);
     const size_t sz1 = (size_t)std::max(c1, c3) * 4, sz2 = (size_t)c2 * 4;
-    if (cudaMalloc(&ws->conv1, sz1) != cudaSuccess || cudaMalloc(&ws->conv2, sz2) != cudaSuccess ||
-        cudaMalloc(&ws->be_deriv, (size_t)18 * nc * 4) != cudaSuccess ||
-        cudaMalloc(&ws->red, 2 * NRB_RED_BLOCKS * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&ws->be_partials, NRB_RED_BLOCKS * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&ws->fred, 2 * NRB_RED_BLOCKS * sizeof(float)) != cudaSuccess) {
+    cudaStream_t st = ws->st;
+    if (dev_alloc(&ws->conv1, sz1, st) != cudaSuccess || dev_alloc(&ws->conv2, sz2, st) != cudaSuccess ||
+        dev_alloc(&ws->be_deriv, (size_t)18 * nc * 4, st) != cudaSuccess ||
+        dev_alloc(&ws->red, 2 * NRB_RED_BLOCKS * sizeof(double), st) != cudaSuccess ||
+        dev_alloc(&ws->be_partials, NRB_RED_BLOCKS * sizeof(double), st) != cudaSuccess ||
+        dev_alloc(&ws->fred, 2 * NRB_RED_BLOCKS * sizeof(float), st) != cudaSuccess) {
         cudaGetLastError();
         return fail(NRB_ERR_OOM, "workspace allocation failed");
     }
     bytes += sz1 + sz2 + (size_t)18 * nc * 4 + 3 * NRB_RED_BLOCKS * sizeof(double) + 2 * NRB_RED_BLOCKS * 4;
     ws->bytes = bytes;
+    NRB_CUDA(cudaStreamCreateWithFlags(&ws->side, cudaStreamNonBlocking));
+    NRB_CUDA(cudaEventCreateWithFlags(&ws->ev_fork, cudaEventDisableTiming));
+    NRB_CUDA(cudaEventCreateWithFlags(&ws->ev_join, cudaEventDisableTiming));
+    return NRB_OK;
+}
+
+nrb_status fork_side(nrb_workspace *ws, cudaStream_t st) {
+    NRB_CUDA(cudaEventRecord(ws->ev_fork, st));
+    NRB_CUDA(cudaStreamWaitEvent(ws->side, ws->ev_fork, 0));
+    return NRB_OK;
+}
+
+nrb_status join_side(nrb_workspace *ws, cudaStream_t st) {
+    NRB_CUDA(cudaEventRecord(ws->ev_join, ws->side));
+    NRB_CUDA(cudaStreamWaitEvent(st, ws->ev_join, 0));
     return NRB_OK;
 }
 
 void workspace_free(nrb_workspace *ws) {
+    cudaStream_t st = ws->st;
     for (int d = 0; d < 3; ++d) {
-        cudaFree(ws->d_samples[d]);
-        cudaFree(ws->d_tap_slot[d]);
-        cudaFree(ws->d_tap_weight[d]);
-        cudaFree(ws->d_kernel[d]);
+        dev_free(ws->d_samples[d], st);
+        dev_free(ws->d_tap_slot[d], st);
+        dev_free(ws->d_tap_weight[d], st);
+        dev_free(ws->d_kernel[d], st);
     }
-    cudaFree(ws->conv1);
-    cudaFree(ws->conv2);
-    cudaFree(ws->be_deriv);
-    cudaFree(ws->red);
-    cudaFree(ws->be_partials);
-    cudaFree(ws->fred);
+    dev_free(ws->conv1, st);
+    dev_free(ws->conv2, st);
+    dev_free(ws->be_deriv, st);
+    dev_free(ws->red, st);
+    dev_free(ws->be_partials, st);
+    dev_free(ws->fred, st);
+    // the side stream's work is ordered before st's last join; its frees above are on st
+    if (ws->ev_fork) cudaEventDestroy(ws->ev_fork);
+    if (ws->ev_join) cudaEventDestroy(ws->ev_join);
+    if (ws->side) cudaStreamDestroy(ws->side);
 }
 
 static int be_grid(const nrb_geometry *g) {
@@ -846,6 +883,22 @@ using namespace nrb;
 // ---------------------------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------------------------
+nrb_status nrb::workspace_create_on(const nrb_geometry *g, cudaStream_t st, nrb_workspace **out) {
+    if (!g || !out) return fail(NRB_ERR_INVALID, "nrb_workspace_create: null pointer");
+    NRB_TRY(validate_geometry(g));
+    nrb_workspace *ws = new nrb_workspace();
+    ws->st = st;
+    nrb_status s = workspace_init(ws, g);
+    if (s == NRB_OK) s = workspace_alloc(ws);
+    if (s != NRB_OK) {
+        workspace_free(ws);
+        delete ws;
+        return s;
+    }
+    *out = ws;
+    return NRB_OK;
+}
+
 extern "C" nrb_status nrb_workspace_create(const nrb_geometry *g, nrb_workspace **out) {
     if (!g || !out) return fail(NRB_ERR_INVALID, "nrb_workspace_create: null pointer");
     NRB_TRY(validate_geometry(g));
@@ -1028,23 +1081,39 @@ extern "C" nrb_status nrb_approx_bending_energy(nrb_workspace *ws, const nrb_geo
     return NRB_OK;
 }
 
-extern "C" nrb_status nrb_approx_bending_energy_gradient(nrb_workspace *ws, const nrb_geometry *g,
-                                                         const float *cpp, float weight, float *node_grad,
-                                                         void *stream) {
-    if (!ws || !g || !cpp || !node_grad) return fail(NRB_ERR_INVALID, "nrb_approx_bending_energy_gradient: null pointer");
-    cudaStream_t st = as_stream(stream);
+namespace nrb {
+// reg_spline_approxBendingEnergyGradient3D, first half: the 18 second-derivative values of
+// every node (grid read, derivatives written)
+nrb_status launch_be_derivatives(nrb_workspace *ws, const nrb_geometry *g, const float *cpp, cudaStream_t st) {
     const long long nc = nvox(g->cpp_dim);
-    const Mat34 M = to_mat34(g->cpp_xyz);
-    // grid read, gradient read-modify-write, 18 derivative values written and read back
-    KernelTimer timer(TK_BE_GRADIENT, (12.0 + 24.0 + 2 * 72.0) * (double)nc, st);
-    k_be_derivatives<<<grid_for(nc, 128), 128, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2], M, cpp,
-                                                        be_basis(), ws->be_deriv);
+    KernelTimer timer(TK_BE_GRADIENT, (12.0 + 72.0) * (double)nc, st);
+    k_be_derivatives<<<grid_for(nc, 128), 128, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2],
+                                                        to_mat34(g->cpp_xyz), cpp, be_basis(), ws->be_deriv);
     NRB_LAUNCHED("k_be_derivatives");
+    return NRB_OK;
+}
+
+// second half: the adjoint stencil, node_grad += weight / #nodes * sum (derivatives read,
+// gradient read-modify-write)
+nrb_status launch_be_accumulate(nrb_workspace *ws, const nrb_geometry *g, float weight, float *node_grad,
+                                cudaStream_t st) {
+    const long long nc = nvox(g->cpp_dim);
+    KernelTimer timer(TK_BE_GRADIENT, (72.0 + 24.0) * (double)nc, st);
     const float ratio = weight / (float)nc;
     k_be_accumulate<<<grid_for(nc, 128), 128, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2], ws->be_deriv,
                                                        be_basis(), ratio, node_grad);
     NRB_LAUNCHED("k_be_accumulate");
     return NRB_OK;
+}
+}  // namespace nrb
+
+extern "C" nrb_status nrb_approx_bending_energy_gradient(nrb_workspace *ws, const nrb_geometry *g,
+                                                         const float *cpp, float weight, float *node_grad,
+                                                         void *stream) {
+    if (!ws || !g || !cpp || !node_grad) return fail(NRB_ERR_INVALID, "nrb_approx_bending_energy_gradient: null pointer");
+    cudaStream_t st = as_stream(stream);
+    NRB_TRY(launch_be_derivatives(ws, g, cpp, st));
+    return launch_be_accumulate(ws, g, weight, node_grad, st);
 }
 
 // fred holds two partial arrays of NRB_RED_BLOCKS floats (min | max)
@@ -1097,6 +1166,17 @@ extern "C" nrb_status nrb_get_maximal_length(const float *node_grad, int64_t nno
 
 namespace nrb {
 // max length into obj->max_grad_len then normalisation by it, scratch from the workspace
+// UpdateGradientValues with the first-call branch taken on the device (flag read at run time)
+nrb_status cg_update_flagged(nrb_workspace *ws, float *grad, float *g1, float *g2, int64_t n, const int *first_call,
+                             cudaStream_t st) {
+    const int np = (int)std::max<long long>(1, std::min<long long>((n + NRB_RED_THREADS - 1) / NRB_RED_THREADS, NRB_RED_BLOCKS));
+    k_cg_dots<<<np, NRB_RED_THREADS, 0, st>>>(n, grad, g1, g2, ws->red);
+    NRB_LAUNCHED("k_cg_dots");
+    k_cg_update<<<grid_for(n, 256), 256, 0, st>>>(n, grad, g1, g2, ws->red, np, first_call);
+    NRB_LAUNCHED("k_cg_update");
+    return NRB_OK;
+}
+
 nrb_status max_and_normalise(nrb_workspace *ws, float *grad, int64_t nnode, nrb_objective *obj, cudaStream_t st) {
     const int np = (int)std::max<long long>(1, std::min<long long>((nnode + NRB_RED_THREADS - 1) / NRB_RED_THREADS, NRB_RED_BLOCKS));
     k_maxlen<<<np, NRB_RED_THREADS, 0, st>>>(nnode, grad, ws->fred);
@@ -1138,7 +1218,7 @@ extern "C" nrb_status nrb_conjugate_gradient(nrb_workspace *ws, float *grad, flo
     const int np = (int)std::max<long long>(1, std::min<long long>((n + NRB_RED_THREADS - 1) / NRB_RED_THREADS, NRB_RED_BLOCKS));
     k_cg_dots<<<np, NRB_RED_THREADS, 0, st>>>(n, grad, g1, g2, ws->red);
     NRB_LAUNCHED("k_cg_dots");
-    k_cg_update<<<grid_for(n, 256), 256, 0, st>>>(n, grad, g1, g2, ws->red, np);
+    k_cg_update<<<grid_for(n, 256), 256, 0, st>>>(n, grad, g1, g2, ws->red, np, nullptr);
     NRB_LAUNCHED("k_cg_update");
     return NRB_OK;
 }

@@ -1,0 +1,226 @@
+// Batched and served F3D registrations on one device.
+//
+// A server owns `slots` worker threads, each with its own CUDA stream. Requests queue in
+// arrival order; the head of the queue is admitted when a worker is free and its device
+// footprint fits in what the HBM budget has left, so requests that arrive while others run are
+// taken up as soon as a slot and memory free up, and their kernels overlap on the device with
+// the running ones. Each registration is the same sequence of launches as a plain
+// nrb_f3d_register_host call (deterministic kernels, no state shared between registrations), so
+// its result does not depend on what else runs.
+//
+// The batch entry point is a server sized to the batch that takes every pair at once.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "nrb_state.cuh"
+
+namespace nrb {
+nrb_status register_on_stream(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3],
+                              const nrb_f3d_params *p, float *cpp_out, int64_t cap, nrb_f3d_result *res,
+                              cudaStream_t st);
+int64_t registration_footprint(const int32_t dim[3], const float pixdim[3], const nrb_f3d_params *p);
+}  // namespace nrb
+
+using namespace nrb;
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+struct Job {
+    int64_t ticket = 0;
+    nrb_pair pair{};
+    nrb_f3d_params params{};
+    int64_t footprint = 0;
+    Clock::time_point submitted, started, finished;
+    bool done = false;
+    nrb_status status = NRB_OK;
+    std::string error;
+    nrb_f3d_result result{};
+};
+
+}  // namespace
+
+struct nrb_server {
+    int device = 0;
+    int64_t budget = 0;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Job *> queue;
+    std::map<int64_t, Job *> jobs;
+    std::vector<std::thread> workers;
+    int64_t next_ticket = 1, used = 0, peak_used = 0;
+    int active = 0, peak_active = 0;
+    bool stop = false;
+
+    void worker() {
+        cudaSetDevice(device);
+        cudaStream_t st = nullptr;
+        const bool have_stream = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+        for (;;) {
+            Job *job = nullptr;
+            {
+                std::unique_lock<std::mutex> lock(mu);
+                // FIFO admission: the head waits for memory rather than being overtaken
+                cv.wait(lock, [&] {
+                    return (stop && queue.empty()) || (!queue.empty() && used + queue.front()->footprint <= budget);
+                });
+                if (queue.empty()) break;  // stopping and drained
+                job = queue.front();
+                queue.pop_front();
+                used += job->footprint;
+                ++active;
+                peak_used = std::max(peak_used, used);
+                peak_active = std::max(peak_active, active);
+            }
+            job->started = Clock::now();
+            nrb_status s = have_stream ? NRB_OK : fail(NRB_ERR_CUDA, "server: stream creation failed");
+            if (s == NRB_OK)
+                s = register_on_stream(job->pair.ref_host, job->pair.flo_host, job->pair.dim, job->pair.pixdim,
+                                       &job->params, job->pair.cpp_out_host, job->pair.cpp_capacity, &job->result, st);
+            const std::string err = s == NRB_OK ? std::string() : std::string(nrb_last_error());
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                job->finished = Clock::now();
+                job->status = s;
+                job->error = err;
+                job->done = true;
+                used -= job->footprint;
+                --active;
+            }
+            cv.notify_all();
+        }
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+extern "C" nrb_status nrb_f3d_footprint(const int32_t dim[3], const float pixdim[3], const nrb_f3d_params *p,
+                                        int64_t *bytes) {
+    if (!dim || !pixdim || !p || !bytes) return fail(NRB_ERR_INVALID, "nrb_f3d_footprint: null pointer");
+    *bytes = registration_footprint(dim, pixdim, p);
+    return NRB_OK;
+}
+
+extern "C" nrb_status nrb_server_create(int slots, int64_t hbm_budget_bytes, nrb_server **out) {
+    if (!out || slots < 1 || slots > 256) return fail(NRB_ERR_INVALID, "nrb_server_create: slots must be in [1, 256]");
+    int dev = 0;
+    NRB_CUDA(cudaGetDevice(&dev));
+    size_t free_b = 0, total_b = 0;
+    NRB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    nrb_server *s = new nrb_server();
+    s->device = dev;
+    s->budget = hbm_budget_bytes > 0 ? hbm_budget_bytes : (int64_t)(0.8 * (double)free_b);
+    // keep freed registration buffers in the device's default pool up to the budget, so the
+    // next admitted request reuses them instead of mapping new memory
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = (uint64_t)s->budget;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+    for (int i = 0; i < slots; ++i) s->workers.emplace_back([s] { s->worker(); });
+    *out = s;
+    return NRB_OK;
+}
+
+extern "C" nrb_status nrb_server_submit(nrb_server *s, const nrb_pair *req, const nrb_f3d_params *p,
+                                        int64_t *ticket) {
+    if (!s || !req || !p || !ticket || !req->ref_host || !req->flo_host)
+        return fail(NRB_ERR_INVALID, "nrb_server_submit: null pointer");
+    for (int i = 0; i < 3; ++i)
+        if (req->dim[i] < 2 || !(req->pixdim[i] > 0))
+            return fail(NRB_ERR_INVALID, "nrb_server_submit: 3D volumes with positive voxel size expected");
+    Job *job = new Job();
+    job->pair = *req;
+    job->params = *p;
+    job->footprint = registration_footprint(req->dim, req->pixdim, p);
+    if (job->footprint > s->budget) {
+        delete job;
+        return fail(NRB_ERR_OOM, "nrb_server_submit: request larger than the server's HBM budget");
+    }
+    job->submitted = Clock::now();
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        job->ticket = s->next_ticket++;
+        s->jobs[job->ticket] = job;
+        s->queue.push_back(job);
+    }
+    s->cv.notify_all();
+    *ticket = job->ticket;
+    return NRB_OK;
+}
+
+extern "C" nrb_status nrb_server_wait(nrb_server *s, int64_t ticket, nrb_f3d_result *res, double *queue_seconds,
+                                      double *latency_seconds) {
+    if (!s) return fail(NRB_ERR_INVALID, "nrb_server_wait: null server");
+    Job *job = nullptr;
+    {
+        std::unique_lock<std::mutex> lock(s->mu);
+        auto it = s->jobs.find(ticket);
+        if (it == s->jobs.end()) return fail(NRB_ERR_INVALID, "nrb_server_wait: unknown ticket");
+        job = it->second;
+        s->cv.wait(lock, [&] { return job->done; });
+        s->jobs.erase(it);
+    }
+    const nrb_status st = job->status;
+    const std::string err = job->error;
+    if (res) *res = job->result;
+    if (queue_seconds) *queue_seconds = std::chrono::duration<double>(job->started - job->submitted).count();
+    if (latency_seconds) *latency_seconds = std::chrono::duration<double>(job->finished - job->submitted).count();
+    delete job;
+    if (st != NRB_OK) return fail(st, err.c_str());
+    return NRB_OK;
+}
+
+extern "C" nrb_status nrb_server_stats(nrb_server *s, int64_t *peak_bytes, int32_t *peak_active) {
+    if (!s) return fail(NRB_ERR_INVALID, "nrb_server_stats: null server");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (peak_bytes) *peak_bytes = s->peak_used;
+    if (peak_active) *peak_active = s->peak_active;
+    return NRB_OK;
+}
+
+extern "C" void nrb_server_destroy(nrb_server *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    for (auto& t : s->workers) t.join();
+    for (auto& kv : s->jobs) delete kv.second;
+    delete s;
+}
+
+extern "C" nrb_status nrb_f3d_register_batch(const nrb_pair *pairs, int n, const nrb_f3d_params *p, int concurrency,
+                                             int64_t hbm_budget_bytes, nrb_f3d_result *results) {
+    if (!pairs || n < 0 || !p) return fail(NRB_ERR_INVALID, "nrb_f3d_register_batch: bad argument");
+    if (n == 0) return NRB_OK;
+    nrb_server *s = nullptr;
+    NRB_TRY(nrb_server_create(std::max(1, std::min(concurrency, n)), hbm_budget_bytes, &s));
+    std::vector<int64_t> tickets(n, 0);
+    nrb_status first = NRB_OK;
+    std::string first_err;
+    for (int i = 0; i < n; ++i) {
+        const nrb_status st = nrb_server_submit(s, &pairs[i], p, &tickets[i]);
+        if (st != NRB_OK && first == NRB_OK) {
+            first = st;
+            first_err = nrb_last_error();
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        if (!tickets[i]) continue;
+        const nrb_status st = nrb_server_wait(s, tickets[i], results ? &results[i] : nullptr, nullptr, nullptr);
+        if (st != NRB_OK && first == NRB_OK) {
+            first = st;
+            first_err = nrb_last_error();
+        }
+    }
+    nrb_server_destroy(s);
+    if (first != NRB_OK) return fail(first, first_err.c_str());
+    return NRB_OK;
+}

@@ -41,6 +41,7 @@ struct nrb_nmi {
     double *logt = nullptr;        // total: log of pro (0 where pro == 0)
     nrb_objective *last = nullptr; // entropies / NMI of the last evaluation
     int device = 0;
+    cudaStream_t st = nullptr;     // owner's stream for stream-ordered allocation (or none)
 };
 
 // Per-axis description of where the node sampling of Compute::VoxelCentricToNodeCentric reads
@@ -74,11 +75,19 @@ struct nrb_workspace {
     float *conv1 = nullptr;         // [3][nz][ny][nsx]
     float *conv2 = nullptr;         // [3][nz][nsy][nsx]
     size_t bytes = 0;
+    cudaStream_t st = nullptr;      // owner's stream for stream-ordered allocation (or none)
+    // the node-grid kernels (bending energy) run on a side stream, overlapped with the voxel
+    // passes of the same evaluation: fork/join through two events
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 namespace nrb {
 
 nrb_status workspace_init(nrb_workspace *ws, const nrb_geometry *g);
+// creators whose buffers are allocated and freed in the order of `st` (st may be null)
+nrb_status workspace_create_on(const nrb_geometry *g, cudaStream_t st, nrb_workspace **out);
+nrb_status nmi_create_on(int ref_bins, int flo_bins, cudaStream_t st, nrb_nmi **out);
 void workspace_free(nrb_workspace *ws);
 nrb_status validate_geometry(const nrb_geometry *g);
 
@@ -95,6 +104,12 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
                                  cudaStream_t st);
 nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float *cpp,
                            cudaStream_t st);
+nrb_status launch_be_derivatives(nrb_workspace *ws, const nrb_geometry *g, const float *cpp, cudaStream_t st);
+nrb_status launch_be_accumulate(nrb_workspace *ws, const nrb_geometry *g, float weight, float *node_grad,
+                                cudaStream_t st);
+// side stream of `ws` starts after the work queued so far on st / st waits for the side stream
+nrb_status fork_side(nrb_workspace *ws, cudaStream_t st);
+nrb_status join_side(nrb_workspace *ws, cudaStream_t st);
 nrb_status launch_convolve_to_nodes(nrb_workspace *ws, const nrb_geometry *g, const float *vgrad,
                                     float weight, float *node, cudaStream_t st);
 

@@ -39,7 +39,7 @@ struct WalkParams {
     float pad;               // padding value of out-of-volume taps
     int rb, fb;              // internal bin counts
     int cnv;                 // control points per component
-    int log_in_smem;         // gradient: the FP64 log table is staged in shared memory
+    int log_in_smem;         // gradient: an FP32 copy of the log table is staged in shared memory
 };
 
 __device__ __forceinline__ int pre_of(int v, float gs) { return (int)((float)v / gs); }
@@ -426,10 +426,49 @@ __device__ __forceinline__ double nmi_window(float rv, float wv, const double *l
     return sr + sw - nmi * sj;
 }
 
+// The same window in FP32 on an FP32 copy of the log table (the fused gradient pass): the
+// per-voxel terms are a 16-tap weighted sum whose FP32 rounding (~1e-6 relative) stays far
+// below the voxel-face jumps of the trilinear spatial gradient, while the FP64 normalisation
+// constant (weight / (H_joint * total)) multiplies it afterwards.
+__device__ __forceinline__ float nmi_window_f(float rv, float wv, const float *logt, int rb, int fb, float nmi) {
+    const float *rlog = logt + rb * fb;
+    const float *wlog = rlog + rb;
+    const int r0 = (int)(rv - 1.f), r1 = (int)(rv + 3.f);
+    const int w0 = (int)(wv - 1.f), w1 = (int)(wv + 3.f);
+    float dw[4], wl[4];
+    bool wok[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int w = w0 + u;
+        wok[u] = w < w1 && -1 < w && w < fb;
+        dw[u] = wok[u] ? parzen_derivf(wv - (float)w) : 0.f;
+        wl[u] = wok[u] ? wlog[w] : 0.f;
+    }
+    float sr = 0.f, sw = 0.f, sj = 0.f;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int r = r0 + t;
+        if (!(r < r1 && -1 < r && r < rb)) continue;
+        const float br = parzenf(rv - (float)r);
+        const float rl = rlog[r];
+        const float *jrow = logt + r;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (!wok[u]) continue;
+            const float c = br * dw[u];
+            sr = fmaf(c, rl, sr);
+            sw = fmaf(c, wl[u], sw);
+            sj = fmaf(c, jrow[(w0 + u) * rb], sj);
+        }
+    }
+    return sr + sw - nmi * sj;
+}
+
 // ---------------------------------------------------------------------------------------------
 // fused gradient: deformation + warp + spatial gradient + NMI voxel gradient
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(32 * TY_GRADIENT, 4)
+template <bool kF32>
+__global__ void __launch_bounds__(32 * TY_GRADIENT, kF32 ? 6 : 4)
 k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
            const int32_t *__restrict__ mask, const float *__restrict__ cpp,
            const double *__restrict__ logt_g, const nrb_objective *__restrict__ last,
@@ -439,12 +478,13 @@ k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict_
     const int nv = P.nx * P.ny * P.nz;
     const double nmi = last->nmi;
     const double scale = weight / (last->entropy[2] * last->entropy[3]);
-    const double *logt = logt_g;
-    if (P.log_in_smem) {
-        double *ls = reinterpret_cast<double *>(S.tail);
+    const float nmi_f = (float)nmi, scale_f = (float)scale;
+    float *logf = nullptr;
+    if (kF32) {  // FP32 copy of the log table for the FP32 window
+        logf = reinterpret_cast<float *>(S.tail);
         const int total = P.rb * P.fb + P.rb + P.fb;
-        for (int i = threadIdx.x; i < total; i += blockDim.x) ls[i] = logt_g[i];
-        logt = ls;  // visible after the first stage_item barrier
+        for (int i = threadIdx.x; i < total; i += blockDim.x) logf[i] = (float)logt_g[i];
+        // visible after the first stage_item barrier
     }
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
         Item I;
@@ -465,9 +505,15 @@ k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict_
                                       w, g);
                 const float rv = __ldg(&ref[idx]);
                 if (rv == rv && w == w) {
-                    const double s = nmi_window(rv, w, logt, P.rb, P.fb, nmi);
+                    if (kF32) {
+                        const float s = nmi_window_f(rv, w, logf, P.rb, P.fb, nmi_f);
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) out[d] = (float)(scale * ((double)g[d] * s));
+                        for (int d = 0; d < 3; ++d) out[d] = scale_f * (g[d] * s);
+                    } else {
+                        const double s = nmi_window(rv, w, logt_g, P.rb, P.fb, nmi);
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) out[d] = (float)(scale * ((double)g[d] * s));
+                    }
                 }
             }
             vgrad[idx] = out[0];
@@ -504,12 +550,21 @@ k_deformation(WalkParams P, const int32_t *__restrict__ mask, const float *__res
 }
 
 // ---------------------------------------------------------------------------------------------
-// histogram -> smoothed probabilities, FP64 entropies, log table (one block, tables in smem)
+// histogram -> smoothed probabilities, FP64 entropies, log table (one cluster, tables in smem)
 // ---------------------------------------------------------------------------------------------
-constexpr int FIN_THREADS = 1024;
+// one 3-tap smoothing output in the reference's accumulation order (value = 0; value +=
+// left*k0; value += centre*k1; value += right*k0, in-range taps only), no contraction
+__device__ __forceinline__ double smooth3(bool has_l, double l, double m, bool has_r, double r, double k0, double k1) {
+    double v = 0.0;
+    if (has_l) v = __dadd_rn(v, __dmul_rn(l, k0));
+    v = __dadd_rn(v, __dmul_rn(m, k1));
+    if (has_r) v = __dadd_rn(v, __dmul_rn(r, k0));
+    return v;
+}
 
-// fixed-shape block sum of three doubles: warp shuffles, then one warp over the partials
-__device__ __forceinline__ void block_sum3(double& a, double& b, double& c, double *red) {
+// fixed-shape block sum of three doubles over NW warps
+template <int NW>
+__device__ __forceinline__ void block_sum3w(double& a, double& b, double& c, double *red) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -525,9 +580,9 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, doub
     }
     __syncthreads();
     if (wid == 0) {
-        a = red[3 * lane];
-        b = red[3 * lane + 1];
-        c = red[3 * lane + 2];
+        a = lane < NW ? red[3 * lane] : 0.0;
+        b = lane < NW ? red[3 * lane + 1] : 0.0;
+        c = lane < NW ? red[3 * lane + 2] : 0.0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             a += __shfl_down_sync(0xffffffffu, a, o);
@@ -546,113 +601,140 @@ __device__ __forceinline__ void block_sum3(double& a, double& b, double& c, doub
     c = red[2];
 }
 
-// one 3-tap smoothing output in the reference's accumulation order (value = 0; value +=
-// left*k0; value += centre*k1; value += right*k0, in-range taps only), no contraction
-__device__ __forceinline__ double smooth3(bool has_l, double l, double m, bool has_r, double r, double k0, double k1) {
-    double v = 0.0;
-    if (has_l) v = __dadd_rn(v, __dmul_rn(l, k0));
-    v = __dadd_rn(v, __dmul_rn(m, k1));
-    if (has_r) v = __dadd_rn(v, __dmul_rn(r, k0));
-    return v;
-}
-
 // _reg_nmi.cpp:249-346 with the histogram as integer counts: 3-tap [1/6, float(2/3), 1/6]
 // smoothing along the reference axis then the floating axis (each entry bit-identical to the
 // reference's), normalisation by the total, marginals summed in the reference's sequential
 // order, entropies and the log table. The bending-energy partials of the same evaluation are
-// summed here too. Shared memory: T = the joint table plus marginals; U = a second joint table
-// for the parallel smoothing pass (omitted when two tables do not fit, then the smoothing along
-// the floating axis rolls a window in place, one thread per reference bin).
-__global__ void __launch_bounds__(FIN_THREADS)
-k_nmi_finalize(int rb, int fb, int two_tables, uint32_t *__restrict__ hist, double *__restrict__ pro,
+// summed here too.
+//
+// One cluster of FIN_CLUSTER blocks: block c owns the floating-bin rows [c*rpc, (c+1)*rpc) of
+// the joint table (rows are reference-bin contiguous). It smooths its rows (reading one halo row
+// of counts on each side), and the blocks exchange partial sums and the normalised rows through
+// distributed shared memory. Shared memory per block: T = own rows, U = own rows + 2 halo rows.
+constexpr int FIN_CLUSTER = 8, FIN_CTA_THREADS = 256, FIN_WARPS = FIN_CTA_THREADS / 32;
+
+__global__ void __cluster_dims__(FIN_CLUSTER, 1, 1) __launch_bounds__(FIN_CTA_THREADS)
+k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *__restrict__ pro,
                double *__restrict__ logt, nrb_objective *__restrict__ last,
                const double *__restrict__ be_partials, int n_be, double be_norm,
                double sim_weight, double be_weight, nrb_objective *__restrict__ obj) {
-    extern __shared__ double T[];
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ double sm[];
     __shared__ double red[3 * 32];
-    const int tid = threadIdx.x;
-    const int nj = rb * fb, total = nj + rb + fb;
-    double *U = T + total;
+    __shared__ double part[4];  // this block's partial mass, H_ref, H_war, H_joint
+    const int tid = threadIdx.x, c = (int)cluster.block_rank();
+    const int nj = rb * fb;
+    const int rpc = (fb + FIN_CLUSTER - 1) / FIN_CLUSTER;
+    const int f0 = min(fb, c * rpc), f1 = min(fb, f0 + rpc), nrow = f1 - f0;
+    double *T = sm;               // rpc rows
+    double *U = sm + rpc * rb;    // rpc + 2 rows: U row k = floating bin f0 - 1 + k
     const double k0 = parzen(-1.0), k1 = parzen(0.0);
-    // smoothing along the reference axis straight from the integer counts
-    for (int i = tid; i < nj; i += FIN_THREADS) {
-        const int r = i % rb;
-        const double m = (double)hist[i];
-        const double l = r > 0 ? (double)hist[i - 1] : 0.0;
-        const double rr = r + 1 < rb ? (double)hist[i + 1] : 0.0;
-        (two_tables ? U : T)[i] = smooth3(r > 0, l, m, r + 1 < rb, rr, k0, k1);
+    // smoothing along the reference axis straight from the integer counts, own rows + halo
+    const int ua = max(0, f0 - 1), ub = min(fb, f1 + 1);
+    for (int i = tid; i < (ub - ua) * rb; i += FIN_CTA_THREADS) {
+        const int f = ua + i / rb, r = i % rb;
+        const uint32_t *row = hist + (size_t)f * rb;
+        const double m = (double)row[r];
+        const double l = r > 0 ? (double)row[r - 1] : 0.0;
+        const double rr = r + 1 < rb ? (double)row[r + 1] : 0.0;
+        U[(f - f0 + 1) * rb + r] = smooth3(r > 0, l, m, r + 1 < rb, rr, k0, k1);
     }
     __syncthreads();
-    for (int i = tid; i < nj; i += FIN_THREADS) hist[i] = 0u;  // ready for the next evaluation
-    for (int i = nj + tid; i < total; i += FIN_THREADS) T[i] = 0.0;
-    double mass = 0.0, u1 = 0.0, u2 = 0.0;
-    if (two_tables) {
-        for (int i = tid; i < nj; i += FIN_THREADS) {
-            const int f = i / rb;
-            const double v = smooth3(f > 0, f > 0 ? U[i - rb] : 0.0, U[i], f + 1 < fb, f + 1 < fb ? U[i + rb] : 0.0, k0, k1);
-            T[i] = v;
-            mass += v;
-        }
-    } else {
-        for (int r = tid; r < rb; r += FIN_THREADS) {
-            double prev = 0.0, cur = T[r];
-            for (int f = 0; f < fb; ++f) {
-                const double next = f + 1 < fb ? T[r + (f + 1) * rb] : 0.0;
-                const double v = smooth3(f > 0, prev, cur, f + 1 < fb, next, k0, k1);
-                T[r + f * rb] = v;
-                prev = cur;
-                cur = next;
-            }
-        }
-        __syncthreads();
-        for (int i = tid; i < nj; i += FIN_THREADS) mass += T[i];
+    // smoothing along the floating axis of the own rows
+    double mass = 0.0, z1 = 0.0, z2 = 0.0;
+    for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) {
+        const int f = f0 + i / rb;
+        const double *u = U + (i / rb + 1) * rb + i % rb;
+        const double v = smooth3(f > 0, f > 0 ? u[-rb] : 0.0, u[0], f + 1 < fb, f + 1 < fb ? u[rb] : 0.0, k0, k1);
+        T[i] = v;
+        mass += v;
     }
-    block_sum3(mass, u1, u2, red);  // also orders the T writes before the reads below
-    for (int i = tid; i < nj; i += FIN_THREADS) T[i] /= mass;
-    __syncthreads();
-    for (int i = tid; i < rb + fb; i += FIN_THREADS) {
-        double s = 0.0;
-        if (i < rb) {
-            for (int f = 0; f < fb; ++f) s += T[i + rb * f];
-        } else {
-            const int f = i - rb;
-            for (int r = 0; r < rb; ++r) s += T[r + rb * f];
-        }
-        T[nj + i] = s;
-    }
-    __syncthreads();
-    double hr = 0.0, hw = 0.0, hj = 0.0;
-    for (int i = tid; i < total; i += FIN_THREADS) {
-        const double p = T[i];
+    block_sum3w<FIN_WARPS>(mass, z1, z2, red);
+    if (tid == 0) part[0] = mass;
+    cluster.sync();  // every block has read its halo counts; partial masses visible
+    for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) hist[(size_t)f0 * rb + i] = 0u;  // next evaluation
+    double total = 0.0;
+    for (int q = 0; q < FIN_CLUSTER; ++q) total += cluster.map_shared_rank(part, q)[0];
+    // normalised own rows, their logs and the joint entropy
+    double hj = 0.0;
+    for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) {
+        const double p = T[i] / total;
+        T[i] = p;
         double l = 0.0;
         if (p > 0) {
             l = log(p);
-            if (i < nj) hj -= p * l;
-            else if (i < nj + rb) hr -= p * l;
-            else hw -= p * l;
+            hj -= p * l;
         }
-        logt[i] = l;
-        pro[i] = p;
+        pro[(size_t)f0 * rb + i] = p;
+        logt[(size_t)f0 * rb + i] = l;
     }
-    block_sum3(hr, hw, hj, red);
-    double be = 0.0, d1 = 0.0, d2 = 0.0;
-    for (int i = tid; i < n_be; i += FIN_THREADS) be += be_partials[i];
-    block_sum3(be, d1, d2, red);
+    __syncthreads();
+    // floating marginal of the own rows, summed over the reference bins in order
+    double hw = 0.0;
+    for (int k = tid; k < nrow; k += FIN_CTA_THREADS) {
+        double sum = 0.0;
+        for (int r = 0; r < rb; ++r) sum += T[k * rb + r];
+        double l = 0.0;
+        if (sum > 0) {
+            l = log(sum);
+            hw -= sum * l;
+        }
+        pro[nj + rb + f0 + k] = sum;
+        logt[nj + rb + f0 + k] = l;
+    }
+    cluster.sync();  // normalised rows of every block visible
+    // reference marginal: bin r summed over the floating bins in order, across the blocks
+    double hr = 0.0;
+    for (int r = c + FIN_CLUSTER * tid; r < rb; r += FIN_CLUSTER * FIN_CTA_THREADS) {
+        double sum = 0.0;
+        for (int q = 0; q < FIN_CLUSTER; ++q) {
+            const int qa = min(fb, q * rpc), qb = min(fb, qa + rpc);
+            const double *Tq = cluster.map_shared_rank(T, q);
+            for (int f = qa; f < qb; ++f) sum += Tq[(f - qa) * rb + r];
+        }
+        double l = 0.0;
+        if (sum > 0) {
+            l = log(sum);
+            hr -= sum * l;
+        }
+        pro[nj + r] = sum;
+        logt[nj + r] = l;
+    }
+    block_sum3w<FIN_WARPS>(hr, hw, hj, red);
     if (tid == 0) {
-        nrb_objective o;
-        // with a zero similarity weight the reference never evaluates the measure
-        // (_reg_f3d.cpp:450-454): its weighted term is 0, not 0 * NaN
-        o.nmi = sim_weight > 0 ? (hr + hw) / hj : 0.0;
-        o.entropy[0] = hr;
-        o.entropy[1] = hw;
-        o.entropy[2] = hj;
-        o.entropy[3] = mass;
-        o.be = n_be > 0 ? be / be_norm : 0.0;
-        o.objective = (sim_weight > 0 ? sim_weight * o.nmi : 0.0) - (be_weight > 0 ? be_weight * o.be : 0.0);
-        o.max_grad_len = last->max_grad_len;
-        *last = o;
-        if (obj) *obj = o;
+        part[1] = hr;
+        part[2] = hw;
+        part[3] = hj;
     }
+    cluster.sync();
+    if (c == 0) {
+        double be = 0.0, d1 = 0.0, d2 = 0.0;
+        for (int i = tid; i < n_be; i += FIN_CTA_THREADS) be += be_partials[i];
+        block_sum3w<FIN_WARPS>(be, d1, d2, red);
+        if (tid == 0) {
+            double h[3] = { 0.0, 0.0, 0.0 };
+            for (int q = 0; q < FIN_CLUSTER; ++q) {
+                const double *pq = cluster.map_shared_rank(part, q);
+                h[0] += pq[1];
+                h[1] += pq[2];
+                h[2] += pq[3];
+            }
+            nrb_objective o;
+            // with a zero similarity weight the reference never evaluates the measure
+            // (_reg_f3d.cpp:450-454): its weighted term is 0, not 0 * NaN
+            o.nmi = sim_weight > 0 ? (h[0] + h[1]) / h[2] : 0.0;
+            o.entropy[0] = h[0];
+            o.entropy[1] = h[1];
+            o.entropy[2] = h[2];
+            o.entropy[3] = total;
+            o.be = n_be > 0 ? be / be_norm : 0.0;
+            o.objective = (sim_weight > 0 ? sim_weight * o.nmi : 0.0) - (be_weight > 0 ? be_weight * o.be : 0.0);
+            o.max_grad_len = last->max_grad_len;
+            *last = o;
+            if (obj) *obj = o;
+        }
+    }
+    cluster.sync();  // every block's shared memory stays alive until block 0 has read it
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -809,19 +891,21 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
                                  const float *cpp, float padding, double weight, float *vgrad,
                                  cudaStream_t st) {
     WalkParams P = make_params(ws->walk_grad, g, padding, nmi->rb, nmi->fb);
-    // the FP64 log table rides in shared memory when it is small (64 bins: 38 KB)
-    const size_t log_bytes = (size_t)nmi->total * sizeof(double);
-    P.log_in_smem = log_bytes <= 48 * 1024;
+    // an FP32 copy of the log table rides in shared memory when it fits (64 bins: 19 KB,
+    // 128 bins: 70 KB); larger tables use the FP64 window on the global table
+    const size_t log_bytes = (size_t)nmi->total * sizeof(float);
+    P.log_in_smem = log_bytes <= 96 * 1024;
     const size_t smem = walk_smem_bytes(ws->walk_grad) + (P.log_in_smem ? log_bytes : 0);
     const int threads = 32 * ws->walk_grad.ty;
     int grid = 0;
-    NRB_TRY(persistent_grid(k_gradient, threads, smem, P.nitems, grid));
+    auto kernel = P.log_in_smem ? k_gradient<true> : k_gradient<false>;
+    NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid));
     // algorithmic bytes: reference + floating (+ mask) read, voxel gradient written, grid once
     const double nv = (double)P.nx * P.ny * P.nz;
     const double bytes = nv * (mask ? 24.0 : 20.0) + 12.0 * (double)P.cnv;
     {
         KernelTimer timer(TK_GRADIENT, bytes, st);
-        k_gradient<<<grid, threads, smem, st>>>(P, ref, flo, mask, cpp, nmi->logt, nmi->last, weight, vgrad);
+        kernel<<<grid, threads, smem, st>>>(P, ref, flo, mask, cpp, nmi->logt, nmi->last, weight, vgrad);
     }
     NRB_LAUNCHED("k_gradient");
     return NRB_OK;
@@ -830,14 +914,13 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
 nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be_partials,
                                int64_t cpp_nvox3, double sim_weight, double be_weight,
                                nrb_objective *obj, cudaStream_t st) {
-    // two joint tables for the parallel smoothing pass when they fit, else one (rolling pass)
-    const int two = (size_t)(nmi->total + nmi->rb * nmi->fb) * sizeof(double) <= 180 * 1024;
-    const size_t smem = (size_t)(nmi->total + (two ? nmi->rb * nmi->fb : 0)) * sizeof(double);
-    NRB_CUDA(cudaFuncSetAttribute(k_nmi_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    const int rpc = (nmi->fb + FIN_CLUSTER - 1) / FIN_CLUSTER;
+    const size_t smem = (size_t)(2 * rpc + 2) * nmi->rb * sizeof(double);
+    NRB_CUDA(cudaFuncSetAttribute(k_nmi_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     KernelTimer timer(TK_FINALIZE, (double)nmi->rb * nmi->fb * 8 + (double)nmi->total * 16, st);
-    k_nmi_finalize<<<1, FIN_THREADS, smem, st>>>(nmi->rb, nmi->fb, two, nmi->hist, nmi->pro, nmi->logt, nmi->last,
-                                                  be_partials, n_be_partials, (double)cpp_nvox3, sim_weight,
-                                                  be_weight, obj);
+    k_nmi_finalize<<<FIN_CLUSTER, FIN_CTA_THREADS, smem, st>>>(nmi->rb, nmi->fb, nmi->hist, nmi->pro, nmi->logt,
+                                                               nmi->last, be_partials, n_be_partials,
+                                                               (double)cpp_nvox3, sim_weight, be_weight, obj);
     NRB_LAUNCHED("k_nmi_finalize");
     return NRB_OK;
 }

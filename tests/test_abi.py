@@ -51,3 +51,17 @@ def test_invalid_arguments_are_reported():
     assert lib.nrb_nmi_create(2, 68, ctypes.byref(out)) == 1  # NRB_ERR_INVALID
     assert b"bins" in lib.nrb_last_error()
     assert lib.nrb_get_deformation_field(None, None, None, None, None) == 1
+
+
+def test_footprint_is_host_only_and_monotone():
+    """Admission unit of the server: computed on the host, grows with the volume, and covers at
+    least the resident pyramid (2 images x 4 bytes x the finest level)."""
+    ensure_built()
+    p = nrb.default_params(levels=2, spacing=(-5.0,))
+    assert p.host_loop == 0
+    sizes = [(64, 64, 64), (128, 128, 96), (182, 218, 182), (256, 256, 256)]
+    fps = [nrb.footprint(d, (1.0, 1.0, 1.0), p) for d in sizes]
+    assert fps == sorted(fps)
+    for d, f in zip(sizes, fps):
+        n = d[0] * d[1] * d[2]
+        assert 8 * n < f < 80 * n + (8 << 20)

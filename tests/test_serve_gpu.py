@@ -1,0 +1,79 @@
+"""Batched and served registrations: every result equals the plain single-pair result for the
+same request, bit for bit, whatever else runs beside it; admission respects the HBM budget."""
+import numpy as np
+import pytest
+
+import niftyreg_b200 as nrb
+from niftyreg_b200 import phantom
+from tests.helpers import ensure_built
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(40, 48, 56), (64, 64, 64), (48, 40, 36), (56, 64, 48)]  # (nz, ny, nx), uneven sizes
+
+
+@pytest.fixture(scope="module")
+def pairs():
+    ensure_built()
+    import torch
+    torch.cuda.set_device(0)
+    return [phantom.blobs_pair(s, seed=10 + i) for i, s in enumerate(SHAPES)]
+
+
+def _params():
+    return nrb.default_params(levels=2, max_iterations=30, bending_energy=0.005, spacing=(-5.0,),
+                              ref_bins=64, flo_bins=64)
+
+
+@pytest.fixture(scope="module")
+def plain(pairs):
+    return [nrb.register_host(p.reference, p.floating, p.pixdim, _params()) for p in pairs]
+
+
+def _same(a, b):
+    (ca, ra), (cb, rb) = a, b
+    assert np.array_equal(ca, cb)
+    assert ra.final_nmi == rb.final_nmi
+    assert ra.objective_evaluations == rb.objective_evaluations
+    assert ra.gradient_evaluations == rb.gradient_evaluations
+
+
+def test_batch_equals_plain(pairs, plain):
+    out = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], _params(), concurrency=4)
+    for a, b in zip(out, plain):
+        _same(a, b)
+
+
+def test_server_mix_equals_plain(pairs, plain):
+    """Requests submitted while others run; each result as when run alone."""
+    with nrb.Server(slots=3) as srv:
+        tickets = [srv.submit(p.reference, p.floating, p.pixdim, _params()) for p in pairs * 2]
+        outs = [srv.wait(t) for t in tickets]
+        _, peak_active = srv.stats()
+    assert peak_active >= 2
+    for i, (cpp, res, q, lat) in enumerate(outs):
+        _same((cpp, res), plain[i % len(pairs)])
+        assert lat >= q >= 0.0
+
+
+def test_server_budget_serialises(pairs, plain):
+    """A budget that holds one request at a time admits one at a time."""
+    prm = _params()
+    fps = [nrb.footprint(p.dim, p.pixdim, prm) for p in pairs]
+    budget = max(fps) + min(fps) // 2
+    with nrb.Server(slots=4, budget_bytes=budget) as srv:
+        tickets = [srv.submit(p.reference, p.floating, p.pixdim, prm) for p in pairs]
+        outs = [srv.wait(t) for t in tickets]
+        peak_bytes, peak_active = srv.stats()
+    assert peak_bytes <= budget
+    assert peak_active == 1
+    for (cpp, res, _, _), b in zip(outs, plain):
+        _same((cpp, res), b)
+
+
+def test_server_rejects_oversized(pairs):
+    prm = _params()
+    p = pairs[1]
+    with nrb.Server(slots=1, budget_bytes=nrb.footprint(p.dim, p.pixdim, prm) - 1) as srv:
+        with pytest.raises(nrb.NrbError):
+            srv.submit(p.reference, p.floating, p.pixdim, prm)
