@@ -102,9 +102,7 @@ KernelTimer::~KernelTimer() {
     g_pending.push_back({ a_, b, (int)k_, bytes_ });
 }
 
-// defined in nrb_ops.cu
-int be_partial_count(const nrb_geometry *g);
-nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float *cpp, cudaStream_t st);
+
 
 }  // namespace nrb
 

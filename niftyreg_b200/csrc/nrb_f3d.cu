@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <vector>
 
 #include "nrb_state.cuh"
@@ -31,13 +32,6 @@ nrb_status cg_update_flagged(nrb_workspace *ws, float *grad, float *g1, float *g
 // kernels set. The arithmetic on the step lengths and objective values is the host loop's,
 // operation for operation.
 // ---------------------------------------------------------------------------------------------
-struct OptState {
-    double best_obj, best_w_measure, best_w_be, best_nmi, best_be;
-    long long it, max_it, n_obj, n_grad;
-    float current_size, max_step, small_step, cur_len, added_len;
-    int line_iter, first_call, just_restarted, accepted;
-};
-
 __device__ __forceinline__ bool outer_continues(const OptState& s) { return s.current_size != 0.f && s.it < s.max_it; }
 __device__ __forceinline__ bool line_continues(const OptState& s) {
     return s.cur_len > s.small_step && s.line_iter < 12 && s.it < s.max_it;
@@ -64,32 +58,6 @@ __global__ void k_ctl_line_start(OptState *s, cudaGraphConditionalHandle inner) 
     cudaGraphSetConditional(inner, line_continues(*s) ? 1u : 0u);
 }
 
-// one line-search step after its objective evaluation
-__global__ void k_ctl_line_step(OptState *s, const nrb_objective *o, float sim_w, float be_w,
-                                cudaGraphConditionalHandle inner) {
-    const double wm = sim_w > 0 ? (double)sim_w * o->nmi : 0.0;
-    const double wb = be_w > 0 ? (double)be_w * o->be : 0.0;
-    const double value = __dsub_rn(wm, wb);
-    s->n_obj += 1;
-    if (value > s->best_obj) {
-        s->best_w_measure = wm;
-        s->best_w_be = wb;
-        s->best_nmi = o->nmi;
-        s->best_be = o->be;
-        s->best_obj = value;
-        s->added_len = __fadd_rn(s->added_len, s->cur_len);
-        const float c = __fmul_rn(s->cur_len, 1.1f);
-        s->cur_len = s->max_step < c ? s->max_step : c;
-        s->accepted = 1;
-    } else {
-        s->cur_len = __fmul_rn(s->cur_len, 0.5f);
-        s->accepted = 0;
-    }
-    s->it += 1;
-    s->line_iter += 1;
-    cudaGraphSetConditional(inner, line_continues(*s) ? 1u : 0u);
-}
-
 // end of Optimise (start length = added length) and the restart rule of _reg_base.cpp:784-793
 __global__ void k_ctl_line_end(OptState *s, cudaGraphConditionalHandle outer) {
     s->current_size = s->added_len;
@@ -105,22 +73,15 @@ __global__ void k_ctl_line_end(OptState *s, cudaGraphConditionalHandle outer) {
     cudaGraphSetConditional(outer, outer_continues(*s) ? 1u : 0u);
 }
 
-// cur = best + (-len) * grad, len read from the state (UpdateControlPointPosition)
-__global__ void k_update_from_state(long long n, float *__restrict__ cur, const float *__restrict__ best,
-                                    const float *__restrict__ grad, const OptState *__restrict__ s) {
-    const float scale = -s->cur_len;
+// StoreCurrentDof after an accepted step: best = best + (-len) * grad, the trial position the
+// objective kernel formed on the fly (same float operations)
+__global__ void k_accept(long long n, float *__restrict__ best, const float *__restrict__ grad,
+                         const OptState *__restrict__ s) {
+    if (!s->accepted) return;
+    const float scale = -s->step_len;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x)
-        cur[i] = __fadd_rn(best[i], __fmul_rn(scale, grad[i]));
-}
-
-// dst = src; with `s`, only after an accepted step (StoreCurrentDof)
-__global__ void k_copy_dof(long long n, float *__restrict__ dst, const float *__restrict__ src,
-                           const OptState *__restrict__ s) {
-    if (s && !s->accepted) return;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x)
-        dst[i] = src[i];
+        best[i] = __fadd_rn(best[i], __fmul_rn(scale, grad[i]));
 }
 
 int elementwise_grid(long long n) {
@@ -318,7 +279,7 @@ private:
     }
     nrb_status RunLevelGraph(float max_step, float smallest_size, float current_size);
     nrb_status CaptureGradient(cudaStream_t cs);
-    nrb_status CaptureObjective(cudaStream_t cs);
+    nrb_status CaptureLineStep(cudaStream_t cs, cudaGraphConditionalHandle line);
 
     nrb_status BuildPyramid(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3]);
     nrb_status CreateGrid();
@@ -361,9 +322,11 @@ public:
     void UseGraphs(bool on) { graph_ok_ = on; }
 };
 
-// GetObjectiveFunctionGradient as captured launches: fused gradient, then NormaliseGradient
+// GetObjectiveFunctionGradient as captured launches: fused gradient, then NormaliseGradient. In
+// the graph the current position is never materialised: after every line search it equals the
+// best one (RestoreBestDof), which the gradient reads directly.
 nrb_status F3dRegistration::CaptureGradient(cudaStream_t cs) {
-    NRB_TRY(nrb_f3d_gradient(ws_.h, nmi_.h, &g_, ref_.p, flo_.p, nullptr, cur_.p, pad_, sim_w_, be_w_, vgrad_.p,
+    NRB_TRY(nrb_f3d_gradient(ws_.h, nmi_.h, &g_, ref_.p, flo_.p, nullptr, best_.p, pad_, sim_w_, be_w_, vgrad_.p,
                              grad_.p, cs));
     NRB_TRY(max_and_normalise(ws_.h, grad_.p, nc_, obj_, cs));
     k_ctl_gradient_done<<<1, 1, 0, cs>>>(dstate_);
@@ -371,10 +334,26 @@ nrb_status F3dRegistration::CaptureGradient(cudaStream_t cs) {
     return NRB_OK;
 }
 
-// GetObjectiveFunctionValue as captured launches (the value stays on the device)
-nrb_status F3dRegistration::CaptureObjective(cudaStream_t cs) {
-    return nrb_f3d_objective(ws_.h, nmi_.h, &g_, ref_.p, flo_.p, nullptr, cur_.p, pad_, sim_w_, be_w_, obj_,
-                             nullptr, cs);
+// One line-search step as captured launches: the objective at the trial position
+// best - cur_len * grad formed inside the kernels (UpdateControlPointPosition fused away), the
+// finalize taking the step (value, acceptance, next length, WHILE condition), and the store of
+// an accepted trial position into best.
+nrb_status F3dRegistration::CaptureLineStep(cudaStream_t cs, cudaGraphConditionalHandle line) {
+    nrb_workspace *ws = ws_.h;
+    int n_be = 0;
+    if (be_w_ > 0) {
+        NRB_TRY(fork_side(ws, cs));
+        NRB_TRY(launch_be_value(ws, &g_, best_.p, ws->side, grad_.p, dstate_));
+        n_be = be_partial_count(&g_);
+    }
+    NRB_TRY(launch_fused_objective(ws, nmi_.h, &g_, ref_.p, flo_.p, nullptr, best_.p, pad_, cs, grad_.p, dstate_));
+    if (be_w_ > 0) NRB_TRY(join_side(ws, cs));
+    NRB_TRY(launch_nmi_finalize(nmi_.h, ws->be_partials, n_be, 3 * nvox(g_.cpp_dim), sim_w_, be_w_, obj_, cs,
+                                dstate_, line));
+    const long long n = 3 * nc_;
+    k_accept<<<elementwise_grid(n), 256, 0, cs>>>(n, best_.p, grad_.p, dstate_);
+    NRB_LAUNCHED("k_accept");
+    return NRB_OK;
 }
 
 // One level of reg_base::Run as one CUDA graph:
@@ -438,8 +417,7 @@ nrb_status F3dRegistration::RunLevelGraph(float max_step, float smallest_size, f
         if (s == NRB_OK) s = capture_while(cap_st_, h_inner, &inner_body);
         if (s == NRB_OK) {
             k_ctl_line_end<<<1, 1, 0, cap_st_>>>(dstate_, h_outer);
-            k_copy_dof<<<elementwise_grid(n), 256, 0, cap_st_>>>(n, cur_.p, best_.p, nullptr);  // RestoreBestDof
-            g_launch_count.fetch_add(2);
+            g_launch_count.fetch_add(1);
             if (cudaGetLastError() != cudaSuccess) s = fail(NRB_ERR_CUDA, "registration: line end launch");
         }
         if (s != NRB_OK) return abort_capture(s);
@@ -449,16 +427,7 @@ nrb_status F3dRegistration::RunLevelGraph(float max_step, float smallest_size, f
     // one line-search step
     NRB_CUDA(cudaStreamBeginCaptureToGraph(cap_st_, inner_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     {
-        k_update_from_state<<<elementwise_grid(n), 256, 0, cap_st_>>>(n, cur_.p, best_.p, grad_.p, dstate_);
-        g_launch_count.fetch_add(1);
-        nrb_status s = cudaGetLastError() == cudaSuccess ? NRB_OK : fail(NRB_ERR_CUDA, "registration: update launch");
-        if (s == NRB_OK) s = CaptureObjective(cap_st_);
-        if (s == NRB_OK) {
-            k_ctl_line_step<<<1, 1, 0, cap_st_>>>(dstate_, obj_, sim_w_, be_w_, h_inner);
-            k_copy_dof<<<elementwise_grid(n), 256, 0, cap_st_>>>(n, best_.p, cur_.p, dstate_);  // StoreCurrentDof
-            g_launch_count.fetch_add(2);
-            if (cudaGetLastError() != cudaSuccess) s = fail(NRB_ERR_CUDA, "registration: line step launch");
-        }
+        nrb_status s = CaptureLineStep(cap_st_, h_inner);
         if (s != NRB_OK) return abort_capture(s);
     }
     NRB_CUDA(cudaStreamEndCapture(cap_st_, &inner_body));
@@ -467,6 +436,8 @@ nrb_status F3dRegistration::RunLevelGraph(float max_step, float smallest_size, f
 
     NRB_CUDA(cudaGraphInstantiate(&top.exec, top.g, 0));
     NRB_CUDA(cudaGraphLaunch(top.exec, st_));
+    // RestoreBestDof of the last line search: the current position is the best one
+    NRB_CUDA(cudaMemcpyAsync(cur_.p, best_.p, n * sizeof(float), cudaMemcpyDeviceToDevice, st_));
     OptState out;
     NRB_CUDA(cudaMemcpyAsync(&out, dstate_, sizeof(OptState), cudaMemcpyDeviceToHost, st_));
     NRB_CUDA(cudaStreamSynchronize(st_));
@@ -677,11 +648,35 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const int32_
 
 }  // namespace
 
+int64_t registration_footprint(const int32_t dim[3], const float pixdim[3], const nrb_f3d_params *p);
+
+// Raises the release threshold of the device's default memory pool to at least `bytes`: the
+// buffers a registration frees stay in the pool for the next one instead of being unmapped at
+// every synchronisation and mapped again (a measurable share of a registration's time).
+// Never lowers a threshold set by the caller or by a server.
+static void keep_pool(int64_t bytes) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    uint64_t cur = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur < (uint64_t)bytes) {
+        uint64_t v = (uint64_t)bytes;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &v);
+    }
+    cudaGetLastError();
+}
+
 // One registration of host or device images on `st` (the entry point of the batch and serving
 // drivers, which run several of these concurrently on their own streams).
 nrb_status register_on_stream(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3],
                               const nrb_f3d_params *p, float *cpp_out, int64_t cap, nrb_f3d_result *res,
                               cudaStream_t st) {
+    if (st) keep_pool(registration_footprint(dim, pixdim, p));
     F3dRegistration reg(*p, st);
     reg.UseGraphs(p->host_loop == 0);
     return reg.Run(ref, flo, dim, pixdim, cpp_out, cap, res);

@@ -64,10 +64,12 @@ __device__ double block_sum_d(double v, double *red) {
 // interior node the 6 second derivatives of each component from 27-point stencils of the
 // positions, summed squares (cross terms doubled) accumulated in double. The stencil sums use
 // the reference's order without contraction: each node's terms are bit-identical to the CPU's.
+// grad/step (optional): the positions are the line search's trial values cpp - cur_len * grad
 __global__ void __launch_bounds__(NRB_RED_THREADS)
 k_be_value(int cx, int cy, int cz, const float *__restrict__ cpp, BeBasis B,
-           double *__restrict__ partials) {
+           double *__restrict__ partials, const float *__restrict__ grad, const OptState *__restrict__ step) {
     __shared__ double red[NRB_RED_THREADS];
+    const float scale = grad ? -step->cur_len : 0.f;
     const long long nc = (long long)cx * cy * cz;
     const int ix = cx - 2, iy = cy - 2, iz = cz - 2;
     const long long ni = (ix > 0 && iy > 0 && iz > 0) ? (long long)ix * iy * iz : 0;
@@ -89,7 +91,7 @@ k_be_value(int cx, int cy, int cz, const float *__restrict__ cpp, BeBasis B,
                     const long long idx = ((long long)(z + c) * cy + y + b) * cx + x + a;
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
-                        const float v = __ldg(&cpp[k * nc + idx]);
+                        const float v = trial_cp(cpp, grad, scale, k * nc + idx);
 #pragma unroll
                         for (int t = 0; t < 6; ++t) d[k][t] = __fadd_rn(d[k][t], __fmul_rn(B.v[t][i], v));
                     }
@@ -832,11 +834,12 @@ static int be_grid(const nrb_geometry *g) {
     return (int)std::max<long long>(1, std::min<long long>((ni + NRB_RED_THREADS - 1) / NRB_RED_THREADS, NRB_RED_BLOCKS));
 }
 
-nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float *cpp, cudaStream_t st) {
+nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float *cpp, cudaStream_t st,
+                           const float *grad, const OptState *step) {
     const int grid = be_grid(g);
     KernelTimer timer(TK_BE_VALUE, 12.0 * (double)nvox(g->cpp_dim), st);
     k_be_value<<<grid, NRB_RED_THREADS, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2], cpp, be_basis(),
-                                                  ws->be_partials);
+                                                  ws->be_partials, grad, step);
     NRB_LAUNCHED("k_be_value");
     return NRB_OK;
 }

@@ -22,6 +22,55 @@ constexpr int COL_X = 32;
 constexpr int TY_OBJECTIVE = 16, TY_GRADIENT = 4, TY_DEFORMATION = 4;
 constexpr int HIST_CLUSTER = 8;  // blocks whose shared-memory histograms merge through DSMEM
 
+// State of the device-resident optimiser (ConjugateGradient::Optimise and the level loop of
+// reg_base::Run) that the control kernels of a level's CUDA graph advance.
+struct OptState {
+    double best_obj, best_w_measure, best_w_be, best_nmi, best_be;
+    long long it, max_it, n_obj, n_grad;
+    float current_size, max_step, small_step;
+    float cur_len;   // step length of the next line-search evaluation
+    float step_len;  // step length of the last evaluation (applied to `best` when accepted)
+    float added_len;
+    int line_iter, first_call, just_restarted, accepted;
+};
+
+// One line-search step of Optimiser::Optimise (reg-lib/Optimiser.cpp:140-168) after its
+// objective evaluation: accept (best values, added length, length x 1.1 capped at max_step) or
+// halve the length; the objective is the weighted difference of reg_f3d::GetObjectiveFunctionValue
+// (reg-lib/_reg_f3d.cpp:443-462). Returns whether the line search goes on.
+__device__ __forceinline__ bool line_step(OptState *s, double nmi, double be, double sim_w, double be_w) {
+    const double wm = sim_w > 0 ? sim_w * nmi : 0.0;
+    const double wb = be_w > 0 ? be_w * be : 0.0;
+    const double value = __dsub_rn(wm, wb);
+    s->n_obj += 1;
+    s->step_len = s->cur_len;
+    if (value > s->best_obj) {
+        s->best_w_measure = wm;
+        s->best_w_be = wb;
+        s->best_nmi = nmi;
+        s->best_be = be;
+        s->best_obj = value;
+        s->added_len = __fadd_rn(s->added_len, s->cur_len);
+        const float c = __fmul_rn(s->cur_len, 1.1f);
+        s->cur_len = s->max_step < c ? s->max_step : c;
+        s->accepted = 1;
+    } else {
+        s->cur_len = __fmul_rn(s->cur_len, 0.5f);
+        s->accepted = 0;
+    }
+    s->it += 1;
+    s->line_iter += 1;
+    return s->cur_len > s->small_step && s->line_iter < 12 && s->it < s->max_it;
+}
+
+// Trial control-point value of the line search, best + (-len) * grad, with the float operations
+// of UpdateControlPointPosition (reg-lib/Compute.cpp:91-127); without grad, the stored value.
+__device__ __forceinline__ float trial_cp(const float *__restrict__ cpp, const float *__restrict__ grad, float scale,
+                                          long long i) {
+    const float b = __ldg(cpp + i);
+    return grad ? __fadd_rn(b, __fmul_rn(scale, __ldg(grad + i))) : b;
+}
+
 struct WalkPlan {
     int ty = 0;  // warps per block = voxel rows per item
     int tiles_x = 0, tiles_y = 0, zchunk = 0, nchunks = 0, nitems = 0;
@@ -92,21 +141,27 @@ void workspace_free(nrb_workspace *ws);
 nrb_status validate_geometry(const nrb_geometry *g);
 
 // launchers shared between translation units
+// ctl (optional, inside a level graph): the finalize also takes the line-search step and sets
+// the line search's WHILE condition `line`
 nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be_partials,
                                int64_t cpp_nvox3, double sim_weight, double be_weight,
-                               nrb_objective *obj, cudaStream_t st);
+                               nrb_objective *obj, cudaStream_t st, OptState *ctl = nullptr,
+                               cudaGraphConditionalHandle line = 0);
+// grad/step (optional): evaluate at the line search's trial position cpp - step->cur_len * grad
 nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                   const float *ref, const float *flo, const int32_t *mask,
-                                  const float *cpp, float padding, cudaStream_t st);
+                                  const float *cpp, float padding, cudaStream_t st,
+                                  const float *grad = nullptr, const OptState *step = nullptr);
 nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                  const float *ref, const float *flo, const int32_t *mask,
                                  const float *cpp, float padding, double weight, float *vgrad,
                                  cudaStream_t st);
 nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float *cpp,
-                           cudaStream_t st);
+                           cudaStream_t st, const float *grad = nullptr, const OptState *step = nullptr);
 nrb_status launch_be_derivatives(nrb_workspace *ws, const nrb_geometry *g, const float *cpp, cudaStream_t st);
 nrb_status launch_be_accumulate(nrb_workspace *ws, const nrb_geometry *g, float weight, float *node_grad,
                                 cudaStream_t st);
+int be_partial_count(const nrb_geometry *g);
 // side stream of `ws` starts after the work queued so far on st / st waits for the side stream
 nrb_status fork_side(nrb_workspace *ws, cudaStream_t st);
 nrb_status join_side(nrb_workspace *ws, cudaStream_t st);

@@ -59,9 +59,13 @@ struct Item {
 
 // Stages the control points of `item` relative to the item's first node (which keeps the
 // partial sums small) into cp[3][sc][sb][sa], and the z basis of each slice into the tables.
-// Called by every thread of the block.
+// With kTrial the control points are the line search's trial values best + scale * grad
+// (`cpp` = best), formed here instead of in a separate update pass. Called by every thread of
+// the block.
+template <bool kTrial = false>
 __device__ __forceinline__ void stage_item(const WalkParams& P, const float *__restrict__ cpp, int item,
-                                           float *cp, float *zb, int *zk, Item& I) {
+                                           float *cp, float *zb, int *zk, Item& I,
+                                           const float *__restrict__ grad = nullptr, float scale = 0.f) {
     const int tx = item % P.tiles_x;
     const int rest = item / P.tiles_x;
     const int ty = rest % P.tiles_y;
@@ -78,7 +82,7 @@ __device__ __forceinline__ void stage_item(const WalkParams& P, const float *__r
     const int nc = pre_of(I.z1 - 1, P.gsz) + 4 - I.zc0;
     const int first = (I.zc0 * P.cy + I.yb0) * P.cx + I.xa0;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) I.off[c] = __ldg(&cpp[c * P.cnv + first]);
+    for (int c = 0; c < 3; ++c) I.off[c] = trial_cp(cpp, kTrial ? grad : nullptr, scale, c * P.cnv + first);
     const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
     __syncthreads();  // the previous item's readers are done
     // one pass: the node planes of one (component, row, column) are independent loads, batched
@@ -88,18 +92,21 @@ __device__ __forceinline__ void stage_item(const WalkParams& P, const float *__r
     for (int c = 0; c < 3; ++c)
         for (int jb = ly; jb < nb; jb += P.ty)
             for (int ia = lx; ia < na; ia += 32) {
-                const float *src = cpp + c * P.cnv + (I.zc0 * P.cy + I.yb0 + jb) * P.cx + I.xa0 + ia;
+                const int src = c * P.cnv + (I.zc0 * P.cy + I.yb0 + jb) * P.cx + I.xa0 + ia;
                 float *dst = cp + (c * P.sc * P.sb + jb) * P.sa + ia;
+                const float *g = kTrial ? grad : nullptr;
                 int kc = 0;
                 for (; kc + 4 <= nc; kc += 4) {
-                    const float v0 = __ldg(src + kc * gplane), v1 = __ldg(src + (kc + 1) * gplane);
-                    const float v2 = __ldg(src + (kc + 2) * gplane), v3 = __ldg(src + (kc + 3) * gplane);
+                    const float v0 = trial_cp(cpp, g, scale, src + kc * gplane);
+                    const float v1 = trial_cp(cpp, g, scale, src + (kc + 1) * gplane);
+                    const float v2 = trial_cp(cpp, g, scale, src + (kc + 2) * gplane);
+                    const float v3 = trial_cp(cpp, g, scale, src + (kc + 3) * gplane);
                     dst[kc * splane] = v0 - I.off[c];
                     dst[(kc + 1) * splane] = v1 - I.off[c];
                     dst[(kc + 2) * splane] = v2 - I.off[c];
                     dst[(kc + 3) * splane] = v3 - I.off[c];
                 }
-                for (; kc < nc; ++kc) dst[kc * splane] = __ldg(src + kc * gplane) - I.off[c];
+                for (; kc < nc; ++kc) dst[kc * splane] = trial_cp(cpp, g, scale, src + kc * gplane) - I.off[c];
             }
     for (int zi = threadIdx.x; zi < I.z1 - I.z0; zi += blockDim.x) {
         const int z = I.z0 + zi;
@@ -173,13 +180,13 @@ __device__ __forceinline__ void column_position(const WalkParams& P, const Item&
         }
         C.win = pz;
     }
-    const float *bz = zb + 4 * zi;
+    const float4 bz = reinterpret_cast<const float4 *>(zb)[zi];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        float s = bz[0] * C.S[0][c];
-        s = fmaf(bz[1], C.S[1][c], s);
-        s = fmaf(bz[2], C.S[2][c], s);
-        s = fmaf(bz[3], C.S[3][c], s);
+        float s = bz.x * C.S[0][c];
+        s = fmaf(bz.y, C.S[1][c], s);
+        s = fmaf(bz.z, C.S[2][c], s);
+        s = fmaf(bz.w, C.S[3][c], s);
         pos[c] = I.off[c] + s;
     }
 }
@@ -203,28 +210,16 @@ __device__ __forceinline__ void to_floating_voxel(const Mat34& M, int diag, floa
     fz = (float)((double)M.m[8] * dx + (double)M.m[9] * dy + (double)M.m[10] * dz + (double)M.m[11]);
 }
 
-// floor(v) as float and as int without the XU pipe: adding 1.5 * 2^23 rounds v to the nearest
-// integer in the FMA pipe, one compare fixes the rounding direction. v is clamped to +-2^21
-// first; every position that far out lies outside any volume this library accepts.
+// floor(v) as float and as int. v is clamped to +-2^21 first: every position that far out lies
+// outside any volume this library accepts, and the clamp keeps px + 1 from overflowing.
 __device__ __forceinline__ int floor_split(float v, float& fl) {
-    const float magic = 12582912.0f;  // 1.5 * 2^23
     v = fminf(fmaxf(v, -2097152.0f), 2097152.0f);
-    const float t = __fadd_rn(v, magic);
-    int n = __float_as_int(t) - 0x4B400000;
-    float r = __fsub_rn(t, magic);
-    if (r > v) {
-        r = __fsub_rn(r, 1.0f);
-        n -= 1;
-    }
-    fl = r;
-    return n;
+    fl = floorf(v);
+    return __float2int_rd(v);
 }
 
-// (int)v for 0 <= v < 2^22 (truncation == floor there), again without the XU pipe
-__device__ __forceinline__ int trunc_nonneg(float v) {
-    float fl;
-    return floor_split(v, fl);
-}
+// (int)v for 0 <= v (truncation == floor there)
+__device__ __forceinline__ int trunc_nonneg(float v) { return __float2int_rz(v); }
 
 // Trilinear sample of the floating image at world position (x, y, z) with the padding rule of
 // ResampleImage3D (an out-of-volume tap contributes padding * weight, so NaN padding poisons a
@@ -306,7 +301,7 @@ struct WalkSmem {
 __device__ __forceinline__ WalkSmem walk_smem(const WalkParams& P, void *base) {
     WalkSmem s;
     s.cp = reinterpret_cast<float *>(base);
-    s.zb = s.cp + 3 * P.sc * P.sb * P.sa;
+    s.zb = s.cp + ((3 * P.sc * P.sb * P.sa + 3) & ~3);  // 16-byte aligned rows of 4 basis values
     s.zk = reinterpret_cast<int *>(s.zb + 4 * P.zchunk);
     s.tail = reinterpret_cast<char *>(s.zk + P.zchunk);
     // 16-byte alignment of the tail
@@ -315,18 +310,20 @@ __device__ __forceinline__ WalkSmem walk_smem(const WalkParams& P, void *base) {
 }
 
 __host__ inline size_t walk_smem_bytes(const WalkPlan& W) {
-    return ((size_t)W.cp_floats + (size_t)walk_table_floats(W.zchunk)) * 4 + 16;
+    return ((size_t)W.cp_floats + 4 + (size_t)walk_table_floats(W.zchunk)) * 4 + 16;
 }
 
 // ---------------------------------------------------------------------------------------------
 // fused objective: deformation + warp + joint histogram
 // ---------------------------------------------------------------------------------------------
+template <bool kTrial>
 __global__ void __launch_bounds__(32 * TY_OBJECTIVE, 2)
 k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
             const int32_t *__restrict__ mask, const float *__restrict__ cpp,
-            uint32_t *__restrict__ ghist) {
+            uint32_t *__restrict__ ghist, const float *__restrict__ grad, const OptState *__restrict__ step) {
     extern __shared__ float4 sm4[];
     const WalkSmem S = walk_smem(P, sm4);
+    const float scale = kTrial ? -step->cur_len : 0.f;
     uint32_t *h = reinterpret_cast<uint32_t *>(S.tail);
     const int nbins = P.rb * P.fb;
     for (int i = threadIdx.x; i < nbins; i += blockDim.x) h[i] = 0u;
@@ -334,7 +331,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
     const float frb = (float)P.rb, ffb = (float)P.fb;
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
         Item I;
-        stage_item(P, cpp, item, S.cp, S.zb, S.zk, I);
+        stage_item<kTrial>(P, cpp, item, S.cp, S.zb, S.zk, I, grad, scale);
         Column C;
         column_init(P, I, S.cp, C);
         const int nzi = I.z1 - I.z0;
@@ -603,21 +600,22 @@ __device__ __forceinline__ void block_sum3w(double& a, double& b, double& c, dou
 
 // _reg_nmi.cpp:249-346 with the histogram as integer counts: 3-tap [1/6, float(2/3), 1/6]
 // smoothing along the reference axis then the floating axis (each entry bit-identical to the
-// reference's), normalisation by the total, marginals summed in the reference's sequential
-// order, entropies and the log table. The bending-energy partials of the same evaluation are
-// summed here too.
+// reference's), normalisation by the total, marginals, entropies and the log table. The
+// bending-energy partials of the same evaluation are summed here too.
 //
 // One cluster of FIN_CLUSTER blocks: block c owns the floating-bin rows [c*rpc, (c+1)*rpc) of
 // the joint table (rows are reference-bin contiguous). It smooths its rows (reading one halo row
-// of counts on each side), and the blocks exchange partial sums and the normalised rows through
-// distributed shared memory. Shared memory per block: T = own rows, U = own rows + 2 halo rows.
+// of counts on each side) and the blocks exchange partial sums (mass, reference marginal,
+// entropies) through distributed shared memory, always combined in block order. Shared memory
+// per block: T = own rows, U = own rows + 2 halo rows (later the partial reference marginal).
 constexpr int FIN_CLUSTER = 8, FIN_CTA_THREADS = 256, FIN_WARPS = FIN_CTA_THREADS / 32;
 
 __global__ void __cluster_dims__(FIN_CLUSTER, 1, 1) __launch_bounds__(FIN_CTA_THREADS)
 k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *__restrict__ pro,
                double *__restrict__ logt, nrb_objective *__restrict__ last,
                const double *__restrict__ be_partials, int n_be, double be_norm,
-               double sim_weight, double be_weight, nrb_objective *__restrict__ obj) {
+               double sim_weight, double be_weight, nrb_objective *__restrict__ obj,
+               OptState *__restrict__ ctl, cudaGraphConditionalHandle line) {
     cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ double sm[];
     __shared__ double red[3 * 32];
@@ -669,6 +667,13 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *__restrict__
         logt[(size_t)f0 * rb + i] = l;
     }
     __syncthreads();
+    // partial reference marginal over the own rows (U is free now), in floating-bin order
+    double *R = U;
+    for (int r = tid; r < rb; r += FIN_CTA_THREADS) {
+        double sum = 0.0;
+        for (int k = 0; k < nrow; ++k) sum += T[k * rb + r];
+        R[r] = sum;
+    }
     // floating marginal of the own rows, summed over the reference bins in order
     double hw = 0.0;
     for (int k = tid; k < nrow; k += FIN_CTA_THREADS) {
@@ -682,16 +687,13 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *__restrict__
         pro[nj + rb + f0 + k] = sum;
         logt[nj + rb + f0 + k] = l;
     }
-    cluster.sync();  // normalised rows of every block visible
-    // reference marginal: bin r summed over the floating bins in order, across the blocks
+    cluster.sync();  // partial reference marginals of every block visible
+    // reference marginal: the blocks' partial sums added in block order (a fixed order, so the
+    // result repeats bit for bit; it differs from a sequential sum only in the last bits)
     double hr = 0.0;
     for (int r = c + FIN_CLUSTER * tid; r < rb; r += FIN_CLUSTER * FIN_CTA_THREADS) {
         double sum = 0.0;
-        for (int q = 0; q < FIN_CLUSTER; ++q) {
-            const int qa = min(fb, q * rpc), qb = min(fb, qa + rpc);
-            const double *Tq = cluster.map_shared_rank(T, q);
-            for (int f = qa; f < qb; ++f) sum += Tq[(f - qa) * rb + r];
-        }
+        for (int q = 0; q < FIN_CLUSTER; ++q) sum += cluster.map_shared_rank(R, q)[r];
         double l = 0.0;
         if (sum > 0) {
             l = log(sum);
@@ -732,6 +734,7 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *__restrict__
             o.max_grad_len = last->max_grad_len;
             *last = o;
             if (obj) *obj = o;
+            if (ctl) cudaGraphSetConditional(line, line_step(ctl, o.nmi, o.be, sim_weight, be_weight) ? 1u : 0u);
         }
     }
     cluster.sync();  // every block's shared memory stays alive until block 0 has read it
@@ -854,12 +857,15 @@ static nrb_status persistent_grid(K kernel, int threads, size_t smem, int nitems
 
 nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                   const float *ref, const float *flo, const int32_t *mask,
-                                  const float *cpp, float padding, cudaStream_t st) {
+                                  const float *cpp, float padding, cudaStream_t st,
+                                  const float *grad, const OptState *step) {
     const WalkParams P = make_params(ws->walk_obj, g, padding, nmi->rb, nmi->fb);
     const size_t smem = walk_smem_bytes(ws->walk_obj) + (size_t)nmi->rb * nmi->fb * 4;
     const int threads = 32 * ws->walk_obj.ty;
+    const bool trial = grad != nullptr;
+    auto kernel = trial ? k_objective<true> : k_objective<false>;
     int grid = 0;
-    NRB_TRY(persistent_grid(k_objective, threads, smem, P.nitems, grid));
+    NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid));
     grid = ((grid + HIST_CLUSTER - 1) / HIST_CLUSTER) * HIST_CLUSTER;  // whole clusters
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
@@ -879,7 +885,7 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
     cudaError_t e;
     {
         KernelTimer timer(TK_OBJECTIVE, bytes, st);
-        e = cudaLaunchKernelEx(&cfg, k_objective, P, ref, flo, mask, cpp, nmi->hist);
+        e = cudaLaunchKernelEx(&cfg, kernel, P, ref, flo, mask, cpp, nmi->hist, grad, step);
     }
     NRB_CUDA(e);
     NRB_LAUNCHED("k_objective");
@@ -913,14 +919,16 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
 
 nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be_partials,
                                int64_t cpp_nvox3, double sim_weight, double be_weight,
-                               nrb_objective *obj, cudaStream_t st) {
+                               nrb_objective *obj, cudaStream_t st, OptState *ctl,
+                               cudaGraphConditionalHandle line) {
     const int rpc = (nmi->fb + FIN_CLUSTER - 1) / FIN_CLUSTER;
     const size_t smem = (size_t)(2 * rpc + 2) * nmi->rb * sizeof(double);
     NRB_CUDA(cudaFuncSetAttribute(k_nmi_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     KernelTimer timer(TK_FINALIZE, (double)nmi->rb * nmi->fb * 8 + (double)nmi->total * 16, st);
     k_nmi_finalize<<<FIN_CLUSTER, FIN_CTA_THREADS, smem, st>>>(nmi->rb, nmi->fb, nmi->hist, nmi->pro, nmi->logt,
                                                                nmi->last, be_partials, n_be_partials,
-                                                               (double)cpp_nvox3, sim_weight, be_weight, obj);
+                                                               (double)cpp_nvox3, sim_weight, be_weight, obj,
+                                                               ctl, line);
     NRB_LAUNCHED("k_nmi_finalize");
     return NRB_OK;
 }
