@@ -186,14 +186,18 @@ nrb_status nmi_create_on(int ref_bins, int flo_bins, cudaStream_t st, nrb_nmi **
     cudaGetDevice(&n->device);
     const size_t hb = (size_t)ref_bins * flo_bins * 4, tb = (size_t)n->total * 8;
     bool ok = dev_alloc(&n->hist, hb, st) == cudaSuccess && dev_alloc(&n->pro, tb, st) == cudaSuccess &&
-              dev_alloc(&n->logt, tb, st) == cudaSuccess && dev_alloc(&n->last, sizeof(nrb_objective), st) == cudaSuccess;
+              dev_alloc(&n->logt, tb, st) == cudaSuccess && dev_alloc(&n->last, sizeof(nrb_objective), st) == cudaSuccess &&
+              dev_alloc(&n->pro2, tb, st) == cudaSuccess && dev_alloc(&n->logt2, tb, st) == cudaSuccess &&
+              dev_alloc(&n->last2, sizeof(nrb_objective), st) == cudaSuccess;
     if (ok && st) {
         ok = cudaMemsetAsync(n->hist, 0, hb, st) == cudaSuccess && cudaMemsetAsync(n->pro, 0, tb, st) == cudaSuccess &&
              cudaMemsetAsync(n->logt, 0, tb, st) == cudaSuccess &&
-             cudaMemsetAsync(n->last, 0, sizeof(nrb_objective), st) == cudaSuccess;
+             cudaMemsetAsync(n->last, 0, sizeof(nrb_objective), st) == cudaSuccess &&
+             cudaMemsetAsync(n->last2, 0, sizeof(nrb_objective), st) == cudaSuccess;
     } else if (ok) {
         ok = cudaMemset(n->hist, 0, hb) == cudaSuccess && cudaMemset(n->pro, 0, tb) == cudaSuccess &&
-             cudaMemset(n->logt, 0, tb) == cudaSuccess && cudaMemset(n->last, 0, sizeof(nrb_objective)) == cudaSuccess;
+             cudaMemset(n->logt, 0, tb) == cudaSuccess && cudaMemset(n->last, 0, sizeof(nrb_objective)) == cudaSuccess &&
+             cudaMemset(n->last2, 0, sizeof(nrb_objective)) == cudaSuccess;
     }
     if (!ok) {
         cudaGetLastError();
@@ -215,6 +219,9 @@ extern "C" void nrb_nmi_destroy(nrb_nmi *nmi) {
     dev_free(nmi->pro, nmi->st);
     dev_free(nmi->logt, nmi->st);
     dev_free(nmi->last, nmi->st);
+    dev_free(nmi->pro2, nmi->st);
+    dev_free(nmi->logt2, nmi->st);
+    dev_free(nmi->last2, nmi->st);
     delete nmi;
 }
 

@@ -322,12 +322,25 @@ public:
     void UseGraphs(bool on) { graph_ok_ = on; }
 };
 
-// GetObjectiveFunctionGradient as captured launches: fused gradient, then NormaliseGradient. In
-// the graph the current position is never materialised: after every line search it equals the
-// best one (RestoreBestDof), which the gradient reads directly.
+// GetObjectiveFunctionGradient as captured launches: the fused gradient (nrb_f3d_gradient's
+// sequence), then NormaliseGradient. In the graph the current position is never materialised:
+// after every line search it equals the best one (RestoreBestDof), which the gradient reads
+// directly. The reference recomputes the joint histogram at that position first
+// (_reg_nmi.cpp:625); here the NMI tables of the best position are still resident (the table
+// sets alternate between evaluations), and they are the same numbers.
 nrb_status F3dRegistration::CaptureGradient(cudaStream_t cs) {
-    NRB_TRY(nrb_f3d_gradient(ws_.h, nmi_.h, &g_, ref_.p, flo_.p, nullptr, best_.p, pad_, sim_w_, be_w_, vgrad_.p,
-                             grad_.p, cs));
+    nrb_workspace *ws = ws_.h;
+    const bool be = be_w_ > 0;
+    if (be) {
+        NRB_TRY(fork_side(ws, cs));
+        NRB_TRY(launch_be_derivatives(ws, &g_, best_.p, ws->side));
+    }
+    NRB_TRY(launch_fused_gradient(ws, nmi_.h, &g_, ref_.p, flo_.p, nullptr, best_.p, pad_, 1.0, vgrad_.p, cs, dstate_));
+    NRB_TRY(launch_convolve_to_nodes(ws, &g_, vgrad_.p, sim_w_, grad_.p, cs));
+    if (be) {
+        NRB_TRY(join_side(ws, cs));
+        NRB_TRY(launch_be_accumulate(ws, &g_, be_w_, grad_.p, cs));
+    }
     NRB_TRY(max_and_normalise(ws_.h, grad_.p, nc_, obj_, cs));
     k_ctl_gradient_done<<<1, 1, 0, cs>>>(dstate_);
     NRB_LAUNCHED("k_ctl_gradient_done");
@@ -379,6 +392,7 @@ nrb_status F3dRegistration::RunLevelGraph(float max_step, float smallest_size, f
     init.max_step = max_step;
     init.small_step = smallest_size;
     init.first_call = first_call_ ? 1 : 0;
+    init.best_buf = 0;  // the level's initial evaluation wrote the first table set
 
     GraphHolder top;
     cudaGraph_t outer_body = nullptr, inner_body = nullptr;

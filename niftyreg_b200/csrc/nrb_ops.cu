@@ -221,23 +221,33 @@ __device__ __forceinline__ float conv_at(int s, int n, int R, const float *__res
     return num / den;
 }
 
-// pass along x: one block per (y, z) row, the row staged in shared memory
-__global__ void k_conv_x(int nx, int ny, int nz, const float *__restrict__ vg,
-                         const int *__restrict__ samples, int ns, const float *__restrict__ K,
-                         int R, float *__restrict__ out) {
-    extern __shared__ float row[];
+// pass along x: a block stages CONV_X_ROWS consecutive (y, z) rows of each component in shared
+// memory (for a component those rows are one contiguous run of the volume, so the loads
+// coalesce and many are in flight per thread), then evaluates the sampled outputs of all of them
+constexpr int CONV_X_ROWS = 8, CONV_X_THREADS = 256;
+
+__global__ void __launch_bounds__(CONV_X_THREADS)
+k_conv_x(int nx, int ny, int nz, const float *__restrict__ vg, const int *__restrict__ samples, int ns,
+         const float *__restrict__ K, int R, float *__restrict__ out) {
+    extern __shared__ float rows[];  // [3][CONV_X_ROWS][nx]
     const long long nv = (long long)nx * ny * nz;
-    const long long rowi = blockIdx.x;  // y + ny * z
-    for (int i = threadIdx.x; i < 3 * nx; i += blockDim.x) {
-        const int c = i / nx, x = i % nx;
-        row[i] = vg[c * nv + rowi * nx + x];
+    const long long nrow = (long long)ny * nz;
+    const long long r0 = (long long)blockIdx.x * CONV_X_ROWS;
+    const int nr = (int)min((long long)CONV_X_ROWS, nrow - r0);
+    const int run = nr * nx;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float *src = vg + c * nv + r0 * nx;
+        float *dst = rows + c * CONV_X_ROWS * nx;
+        for (int i = threadIdx.x; i < run; i += CONV_X_THREADS) dst[i] = __ldg(src + i);
     }
     __syncthreads();
-    const long long nrow = (long long)ny * nz;
-    for (int i = threadIdx.x; i < 3 * ns; i += blockDim.x) {
-        const int c = i / ns, j = i % ns;
-        const float *r = row + c * nx;
-        out[(c * nrow + rowi) * ns + j] = conv_at(samples[j], nx, R, K, [&](int k) { return r[k]; });
+    const int per_c = nr * ns;
+    for (int i = threadIdx.x; i < 3 * per_c; i += CONV_X_THREADS) {
+        const int c = i / per_c, rem = i - c * per_c;
+        const int r = rem / ns, j = rem - r * ns;
+        const float *row = rows + (c * CONV_X_ROWS + r) * nx;
+        out[(c * nrow + r0 + r) * ns + j] = conv_at(samples[j], nx, R, K, [&](int k) { return row[k]; });
     }
 }
 
@@ -853,8 +863,10 @@ nrb_status launch_convolve_to_nodes(nrb_workspace *ws, const nrb_geometry *g, co
     // compulsory traffic of the whole voxel->node step: the voxel gradient once, the nodes once
     KernelTimer timer(TK_CONV, 12.0 * (double)nx * ny * nz + 12.0 * (double)nvox(g->cpp_dim), st);
     // x pass: one block per row
-    const size_t smem = (size_t)3 * nx * 4;
-    k_conv_x<<<ny * nz, 128, smem, st>>>(nx, ny, nz, vgrad, ws->d_samples[0], nsx, ws->d_kernel[0],
+    const size_t smem = (size_t)3 * CONV_X_ROWS * nx * 4;  // <= 196 KB for nx <= 2048
+    if (smem > 48 * 1024) NRB_CUDA(cudaFuncSetAttribute(k_conv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int xblocks = (int)(((long long)ny * nz + CONV_X_ROWS - 1) / CONV_X_ROWS);
+    k_conv_x<<<xblocks, CONV_X_THREADS, smem, st>>>(nx, ny, nz, vgrad, ws->d_samples[0], nsx, ws->d_kernel[0],
                                          ws->ax[0].radius, ws->conv1);
     NRB_LAUNCHED("k_conv_x");
     // y pass: [3][nz][ny][nsx] -> [3][nz][nsy][nsx]

@@ -32,6 +32,7 @@ struct OptState {
     float step_len;  // step length of the last evaluation (applied to `best` when accepted)
     float added_len;
     int line_iter, first_call, just_restarted, accepted;
+    int best_buf;    // NMI table set (0: pro/logt/last, 1: pro2/logt2/last2) of the best position
 };
 
 // One line-search step of Optimiser::Optimise (reg-lib/Optimiser.cpp:140-168) after its
@@ -54,6 +55,7 @@ __device__ __forceinline__ bool line_step(OptState *s, double nmi, double be, do
         const float c = __fmul_rn(s->cur_len, 1.1f);
         s->cur_len = s->max_step < c ? s->max_step : c;
         s->accepted = 1;
+        s->best_buf ^= 1;  // the evaluation wrote the other table set
     } else {
         s->cur_len = __fmul_rn(s->cur_len, 0.5f);
         s->accepted = 0;
@@ -89,6 +91,10 @@ struct nrb_nmi {
     double *pro = nullptr;         // total: smoothed, normalised joint | ref marginal | flo marginal
     double *logt = nullptr;        // total: log of pro (0 where pro == 0)
     nrb_objective *last = nullptr; // entropies / NMI of the last evaluation
+    // second set of tables: inside a level graph the evaluations alternate between the two so
+    // that the tables of the best position survive rejected line-search steps
+    double *pro2 = nullptr, *logt2 = nullptr;
+    nrb_objective *last2 = nullptr;
     int device = 0;
     cudaStream_t st = nullptr;     // owner's stream for stream-ordered allocation (or none)
 };
@@ -141,8 +147,8 @@ void workspace_free(nrb_workspace *ws);
 nrb_status validate_geometry(const nrb_geometry *g);
 
 // launchers shared between translation units
-// ctl (optional, inside a level graph): the finalize also takes the line-search step and sets
-// the line search's WHILE condition `line`
+// ctl (optional, inside a level graph): the finalize writes the table set that does not hold the
+// best position, takes the line-search step and sets the line search's WHILE condition `line`
 nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be_partials,
                                int64_t cpp_nvox3, double sim_weight, double be_weight,
                                nrb_objective *obj, cudaStream_t st, OptState *ctl = nullptr,
@@ -152,10 +158,11 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
                                   const float *ref, const float *flo, const int32_t *mask,
                                   const float *cpp, float padding, cudaStream_t st,
                                   const float *grad = nullptr, const OptState *step = nullptr);
+// sel (optional, inside a level graph): read the NMI table set sel->best_buf
 nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                  const float *ref, const float *flo, const int32_t *mask,
                                  const float *cpp, float padding, double weight, float *vgrad,
-                                 cudaStream_t st);
+                                 cudaStream_t st, const OptState *sel = nullptr);
 nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float *cpp,
                            cudaStream_t st, const float *grad = nullptr, const OptState *step = nullptr);
 nrb_status launch_be_derivatives(nrb_workspace *ws, const nrb_geometry *g, const float *cpp, cudaStream_t st);

@@ -468,11 +468,14 @@ template <bool kF32>
 __global__ void __launch_bounds__(32 * TY_GRADIENT, kF32 ? 6 : 4)
 k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
            const int32_t *__restrict__ mask, const float *__restrict__ cpp,
-           const double *__restrict__ logt_g, const nrb_objective *__restrict__ last,
-           double weight, float *__restrict__ vgrad) {
+           const double *logt0, const nrb_objective *last0, const double *logt1, const nrb_objective *last1,
+           const OptState *__restrict__ sel, double weight, float *__restrict__ vgrad) {
     extern __shared__ float4 sm4[];
     const WalkSmem S = walk_smem(P, sm4);
     const int nv = P.nx * P.ny * P.nz;
+    const bool second = sel && sel->best_buf == 1;
+    const double *__restrict__ logt_g = second ? logt1 : logt0;
+    const nrb_objective *__restrict__ last = second ? last1 : last0;
     const double nmi = last->nmi;
     const double scale = weight / (last->entropy[2] * last->entropy[3]);
     const float nmi_f = (float)nmi, scale_f = (float)scale;
@@ -611,12 +614,18 @@ __device__ __forceinline__ void block_sum3w(double& a, double& b, double& c, dou
 constexpr int FIN_CLUSTER = 8, FIN_CTA_THREADS = 256, FIN_WARPS = FIN_CTA_THREADS / 32;
 
 __global__ void __cluster_dims__(FIN_CLUSTER, 1, 1) __launch_bounds__(FIN_CTA_THREADS)
-k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *__restrict__ pro,
-               double *__restrict__ logt, nrb_objective *__restrict__ last,
+k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double *logt0, nrb_objective *last0,
+               double *pro1, double *logt1, nrb_objective *last1,
                const double *__restrict__ be_partials, int n_be, double be_norm,
                double sim_weight, double be_weight, nrb_objective *__restrict__ obj,
                OptState *__restrict__ ctl, cudaGraphConditionalHandle line) {
     cg::cluster_group cluster = cg::this_cluster();
+    // output table set: the one not holding the best position (read before thread 0 of block 0
+    // updates the state at the very end)
+    const bool second = ctl && ctl->best_buf == 0;
+    double *__restrict__ pro = second ? pro1 : pro0;
+    double *__restrict__ logt = second ? logt1 : logt0;
+    nrb_objective *__restrict__ last = second ? last1 : last0;
     extern __shared__ double sm[];
     __shared__ double red[3 * 32];
     __shared__ double part[4];  // this block's partial mass, H_ref, H_war, H_joint
@@ -895,7 +904,7 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
 nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                  const float *ref, const float *flo, const int32_t *mask,
                                  const float *cpp, float padding, double weight, float *vgrad,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, const OptState *sel) {
     WalkParams P = make_params(ws->walk_grad, g, padding, nmi->rb, nmi->fb);
     // an FP32 copy of the log table rides in shared memory when it fits (64 bins: 19 KB,
     // 128 bins: 70 KB); larger tables use the FP64 window on the global table
@@ -911,7 +920,8 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
     const double bytes = nv * (mask ? 24.0 : 20.0) + 12.0 * (double)P.cnv;
     {
         KernelTimer timer(TK_GRADIENT, bytes, st);
-        kernel<<<grid, threads, smem, st>>>(P, ref, flo, mask, cpp, nmi->logt, nmi->last, weight, vgrad);
+        kernel<<<grid, threads, smem, st>>>(P, ref, flo, mask, cpp, nmi->logt, nmi->last, nmi->logt2, nmi->last2, sel,
+                                            weight, vgrad);
     }
     NRB_LAUNCHED("k_gradient");
     return NRB_OK;
@@ -926,7 +936,8 @@ nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be
     NRB_CUDA(cudaFuncSetAttribute(k_nmi_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     KernelTimer timer(TK_FINALIZE, (double)nmi->rb * nmi->fb * 8 + (double)nmi->total * 16, st);
     k_nmi_finalize<<<FIN_CLUSTER, FIN_CTA_THREADS, smem, st>>>(nmi->rb, nmi->fb, nmi->hist, nmi->pro, nmi->logt,
-                                                               nmi->last, be_partials, n_be_partials,
+                                                               nmi->last, nmi->pro2, nmi->logt2, nmi->last2,
+                                                               be_partials, n_be_partials,
                                                                (double)cpp_nvox3, sim_weight, be_weight, obj,
                                                                ctl, line);
     NRB_LAUNCHED("k_nmi_finalize");
