@@ -628,15 +628,30 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const int32_
         float current_size = max_step;
         const float smallest_size = max_step / 100.0f;
         UpdateBestObjFunctionValue();
-        if (p_.verbose)
+        if (p_.verbose) {
             printf("[nrb] level %d/%d grid %dx%dx%d, initial objective %.6f = (wSIM)%.6f - (wBE)%.6g\n", level + 1,
                    levels_, grid_.dim[0], grid_.dim[1], grid_.dim[2], best_obj_, best_w_measure_, best_w_be_);
+            const WalkPlan& wo = ws_.h->walk_obj;
+            const WalkPlan& wg = ws_.h->walk_grad;
+            printf("[nrb]   walk: objective %d items (z-chunk %d, %lld resident blocks), gradient %d items "
+                   "(z-chunk %d, %lld resident blocks)\n", wo.nitems, wo.zchunk,
+                   objective_slots(walk_smem_bytes(wo) + (size_t)nmi_.h->rb * nmi_.h->fb * 4), wg.nitems, wg.zchunk,
+                   gradient_slots(walk_smem_bytes(wg) + (size_t)nmi_.h->total * 4));
+        }
         // the graph path needs a non-zero similarity weight (its gradient has no memset branch)
         // and no per-launch timing; both loops take the same steps
+        const auto tl = std::chrono::steady_clock::now();
+        const int64_t obj0 = n_obj_, grad0 = n_grad_;
         if (graph_ok_ && sim_w_ > 0 && !timing_enabled()) {
             NRB_TRY(RunLevelGraph(max_step, smallest_size, current_size));
         } else {
             NRB_TRY(RunLevelHost(max_step, smallest_size, current_size));
+        }
+        if (p_.verbose) {
+            NRB_CUDA(cudaStreamSynchronize(st_));
+            printf("[nrb] level %d: %lld objective + %lld gradient evaluations in %.2f ms\n", level + 1,
+                   (long long)(n_obj_ - obj0), (long long)(n_grad_ - grad0),
+                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl).count());
         }
         max_it_ /= 2;
     }

@@ -5,6 +5,7 @@
 // order, so each result is identical from run to run whatever the device's SM count.
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -229,25 +230,48 @@ constexpr int CONV_X_ROWS = 8, CONV_X_THREADS = 256;
 __global__ void __launch_bounds__(CONV_X_THREADS)
 k_conv_x(int nx, int ny, int nz, const float *__restrict__ vg, const int *__restrict__ samples, int ns,
          const float *__restrict__ K, int R, float *__restrict__ out) {
-    extern __shared__ float rows[];  // [3][CONV_X_ROWS][nx]
+    extern __shared__ float rows[];  // [3][CONV_X_ROWS][nx] | kernel taps [2R + 1]
+    float *Ks = rows + 3 * CONV_X_ROWS * nx;
     const long long nv = (long long)nx * ny * nz;
     const long long nrow = (long long)ny * nz;
     const long long r0 = (long long)blockIdx.x * CONV_X_ROWS;
     const int nr = (int)min((long long)CONV_X_ROWS, nrow - r0);
     const int run = nr * nx;
+    int nan = 0;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const float *src = vg + c * nv + r0 * nx;
         float *dst = rows + c * CONV_X_ROWS * nx;
-        for (int i = threadIdx.x; i < run; i += CONV_X_THREADS) dst[i] = __ldg(src + i);
+        for (int i = threadIdx.x; i < run; i += CONV_X_THREADS) {
+            const float v = __ldg(src + i);
+            nan |= v != v;
+            dst[i] = v;
+        }
     }
-    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * R + 1; i += CONV_X_THREADS) Ks[i] = K[i];
+    // rows without NaN (the fused gradient never writes one) take the check-free sum: the
+    // same operations in the same order as conv_at when every tap counts
+    const bool any_nan = __syncthreads_or(nan) != 0;
     const int per_c = nr * ns;
     for (int i = threadIdx.x; i < 3 * per_c; i += CONV_X_THREADS) {
         const int c = i / per_c, rem = i - c * per_c;
         const int r = rem / ns, j = rem - r * ns;
         const float *row = rows + (c * CONV_X_ROWS + r) * nx;
-        out[(c * nrow + r0 + r) * ns + j] = conv_at(samples[j], nx, R, K, [&](int k) { return row[k]; });
+        const int sj = samples[j];
+        float v;
+        if (any_nan) {
+            v = conv_at(sj, nx, R, Ks, [&](int k) { return row[k]; });
+        } else {
+            float num = 0.f, den = 0.f;
+            const int k0 = max(0, sj - R), k1 = min(nx - 1, sj + R);
+            const float *w = Ks - sj + R;
+            for (int k = k0; k <= k1; ++k) {
+                num = fmaf(w[k], row[k], num);
+                den += w[k];
+            }
+            v = num / den;
+        }
+        out[(c * nrow + r0 + r) * ns + j] = v;
     }
 }
 
@@ -740,9 +764,12 @@ static nrb_status upload(T *&dst, const std::vector<T>& src, size_t& bytes, cuda
     return NRB_OK;
 }
 
-// Items of the voxel walk: enough z-chunks that the persistent blocks get several items each
-// (load balance), but chunks of at least 8 slices so the staged control points are reused.
-WalkPlan plan_walk(const nrb_geometry *g, int ty) {
+// Items of the voxel walk. The persistent grid holds slots_for(shared bytes) co-resident blocks
+// and every block walks ceil(items / slots) items, so the z-chunk count is chosen to minimise a
+// block's walk: rounds x (slices per chunk + a staging overhead of about four slices), over
+// chunk counts that keep chunks at least 8 slices long (the staged control points are reused
+// along z).
+WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t smem), size_t extra_smem) {
     WalkPlan p;
     p.ty = ty;
     const int nx = g->ref_dim[0], ny = g->ref_dim[1], nz = g->ref_dim[2];
@@ -751,23 +778,34 @@ WalkPlan plan_walk(const nrb_geometry *g, int ty) {
     p.tiles_x = (nx + COL_X - 1) / COL_X;
     p.tiles_y = (ny + ty - 1) / ty;
     const long long xy = (long long)p.tiles_x * p.tiles_y;
-    const long long want = (48LL / ty) * sm_count();
-    int chunks = (int)std::max<long long>(1, (want + xy - 1) / xy);
-    chunks = std::min(chunks, std::max(1, nz / 8));
-    p.zchunk = (nz + chunks - 1) / chunks;
-    p.nchunks = (nz + p.zchunk - 1) / p.zchunk;
-    p.nitems = (int)(xy * p.nchunks);
     p.sa = tile_span(nx, COL_X, gs[0]);
     p.sb = tile_span(ny, ty, gs[1]);
-    p.sc = tile_span(nz, p.zchunk, gs[2]);
-    p.cp_floats = 3 * p.sa * p.sb * p.sc;
-    return p;
+    long long best_cost = LLONG_MAX;
+    WalkPlan best = p;
+    for (int c = 1; c <= std::max(1, nz / 8); ++c) {
+        WalkPlan q = p;
+        q.zchunk = (nz + c - 1) / c;
+        q.nchunks = (nz + q.zchunk - 1) / q.zchunk;
+        q.nitems = (int)(xy * q.nchunks);
+        q.sc = tile_span(nz, q.zchunk, gs[2]);
+        q.cp_floats = 3 * q.sa * q.sb * q.sc;
+        const long long slots = std::max(1LL, slots_for(walk_smem_bytes(q) + extra_smem));
+        const long long rounds = (q.nitems + slots - 1) / slots;
+        const long long cost = rounds * (q.zchunk + 4);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = q;
+        }
+    }
+    return best;
 }
 
 nrb_status workspace_init(nrb_workspace *ws, const nrb_geometry *g) {
     ws->g = *g;
-    ws->walk_obj = plan_walk(g, TY_OBJECTIVE);
-    ws->walk_grad = plan_walk(g, TY_GRADIENT);
+    // shared memory beyond the walk: the 64-bin joint histogram / FP32 log table (the plan is
+    // made before the bin count is known; other bin counts shift occupancy little)
+    ws->walk_obj = plan_walk(g, TY_OBJECTIVE, objective_slots, (size_t)68 * 68 * 4);
+    ws->walk_grad = plan_walk(g, TY_GRADIENT, gradient_slots, (size_t)(68 * 68 + 136) * 4);
     return NRB_OK;
 }
 
@@ -863,7 +901,8 @@ nrb_status launch_convolve_to_nodes(nrb_workspace *ws, const nrb_geometry *g, co
     // compulsory traffic of the whole voxel->node step: the voxel gradient once, the nodes once
     KernelTimer timer(TK_CONV, 12.0 * (double)nx * ny * nz + 12.0 * (double)nvox(g->cpp_dim), st);
     // x pass: one block per row
-    const size_t smem = (size_t)3 * CONV_X_ROWS * nx * 4;  // <= 196 KB for nx <= 2048
+    const size_t smem = ((size_t)3 * CONV_X_ROWS * nx + 2 * ws->ax[0].radius + 1) * 4;  // nx <= 2048: <= 197 KB
+    if (smem > 227 * 1024) return fail(NRB_ERR_UNSUPPORTED, "convolution: rows and kernel exceed shared memory");
     if (smem > 48 * 1024) NRB_CUDA(cudaFuncSetAttribute(k_conv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int xblocks = (int)(((long long)ny * nz + CONV_X_ROWS - 1) / CONV_X_ROWS);
     k_conv_x<<<xblocks, CONV_X_THREADS, smem, st>>>(nx, ny, nz, vgrad, ws->d_samples[0], nsx, ws->d_kernel[0],

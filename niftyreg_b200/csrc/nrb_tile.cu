@@ -20,6 +20,8 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <map>
+#include <mutex>
 
 #include "nrb_state.cuh"
 
@@ -309,7 +311,7 @@ __device__ __forceinline__ WalkSmem walk_smem(const WalkParams& P, void *base) {
     return s;
 }
 
-__host__ inline size_t walk_smem_bytes(const WalkPlan& W) {
+size_t walk_smem_bytes(const WalkPlan& W) {
     return ((size_t)W.cp_floats + 4 + (size_t)walk_table_floats(W.zchunk)) * 4 + 16;
 }
 
@@ -375,10 +377,13 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
     cg::cluster_group cluster = cg::this_cluster();
     cluster.sync();
     const int rank = (int)cluster.block_rank();
-    const int nblk = (int)cluster.num_blocks();
-    for (int i = rank + nblk * threadIdx.x; i < nbins; i += nblk * blockDim.x) {
+    for (int i = rank + HIST_CLUSTER * threadIdx.x; i < nbins; i += HIST_CLUSTER * blockDim.x) {
+        uint32_t part[HIST_CLUSTER];
+#pragma unroll
+        for (int q = 0; q < HIST_CLUSTER; ++q) part[q] = cluster.map_shared_rank(h, q)[i];  // loads in flight together
         uint32_t s = 0;
-        for (int q = 0; q < nblk; ++q) s += cluster.map_shared_rank(h, q)[i];
+#pragma unroll
+        for (int q = 0; q < HIST_CLUSTER; ++q) s += part[q];
         if (s) atomicAdd(&ghist[i], s);
     }
     cluster.sync();  // no block leaves while another still reads its shared memory
@@ -851,18 +856,81 @@ static WalkParams make_params(const WalkPlan& W, const nrb_geometry *g, float pa
 }
 
 template <typename K>
-static nrb_status persistent_grid(K kernel, int threads, size_t smem, int nitems, int& grid) {
+static nrb_status persistent_grid(K kernel, int threads, size_t smem, int nitems, int& grid, int resident = 0) {
     NRB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    int per_sm = 0;
-    NRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
-    if (per_sm < 1) return fail(NRB_ERR_UNSUPPORTED, "voxel walk does not fit in shared memory");
+    if (resident <= 0) {
+        int per_sm = 0;
+        NRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+        resident = per_sm * sm_count();
+    }
+    if (resident < 1) return fail(NRB_ERR_UNSUPPORTED, "voxel walk does not fit in shared memory");
     // every block gets the same number of items: as many rounds as the resident blocks need,
     // then the smallest grid that covers the items in that many rounds
-    const int resident = per_sm * sm_count();
     const int rounds = (nitems + resident - 1) / resident;
     grid = (nitems + rounds - 1) / rounds;
     return NRB_OK;
 }
+
+// co-resident blocks of the objective pass: whole clusters of HIST_CLUSTER blocks, as many as
+// the GPU can hold at once (fewer than blocks-per-SM x SMs would suggest: a cluster lives on one
+// GPC)
+static long long objective_slots_query(size_t smem);
+
+long long objective_slots(size_t smem) {
+    // cached per (device, shared bytes): the launch path asks on every evaluation
+    static std::mutex mu;
+    static std::map<std::pair<int, size_t>, long long> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find({ dev, smem });
+        if (it != cache.end()) return it->second;
+    }
+    const long long v = objective_slots_query(smem);
+    std::lock_guard<std::mutex> lock(mu);
+    cache[{ dev, smem }] = v;
+    return v;
+}
+
+static long long objective_slots_query(size_t smem) {
+    auto kernel = k_objective<true>;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(HIST_CLUSTER * 64);
+    cfg.blockDim = dim3(32 * TY_OBJECTIVE);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = HIST_CLUSTER;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, (void *)kernel, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return (long long)clusters * HIST_CLUSTER;
+}
+
+template <typename K>
+static long long blocks_resident(K kernel, int threads, size_t smem) {
+    int per_sm = 0;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return (long long)per_sm * sm_count();
+}
+
+long long gradient_slots(size_t smem) { return blocks_resident(k_gradient<true>, 32 * TY_GRADIENT, smem); }
+long long deformation_slots(size_t smem) { return blocks_resident(k_deformation, 32 * TY_DEFORMATION, smem); }
 
 nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                   const float *ref, const float *flo, const int32_t *mask,
@@ -874,7 +942,7 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
     const bool trial = grad != nullptr;
     auto kernel = trial ? k_objective<true> : k_objective<false>;
     int grid = 0;
-    NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid));
+    NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid, (int)objective_slots(smem)));
     grid = ((grid + HIST_CLUSTER - 1) / HIST_CLUSTER) * HIST_CLUSTER;  // whole clusters
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
@@ -952,7 +1020,7 @@ extern "C" nrb_status nrb_get_deformation_field(const nrb_geometry *g, const flo
                                                 const int32_t *mask, float *def, void *stream) {
     if (!g || !cpp || !def) return fail(NRB_ERR_INVALID, "nrb_get_deformation_field: null pointer");
     NRB_TRY(validate_geometry(g));
-    const WalkPlan W = plan_walk(g, TY_DEFORMATION);
+    const WalkPlan W = plan_walk(g, TY_DEFORMATION, deformation_slots, 0);
     const WalkParams P = make_params(W, g, 0.f, 0, 0);
     const size_t smem = walk_smem_bytes(W);
     int grid = 0;
