@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--concurrency", type=int, default=16, help="batched/served: concurrent registrations")
     ap.add_argument("--requests", type=int, default=300, help="served: requests per arrival rate")
     ap.add_argument("--rates", default="5,20,50", help="served: Poisson arrival rates (requests/s)")
+    ap.add_argument("--shape", default=None, help="kernel-only mode: nz,ny,nx of the volume (default: the workload's)")
     ap.add_argument("--kernel", choices=["objective", "gradient"], default=None,
                     help="profiling mode: run only `--steps` fused evaluations at the finest level "
                          "of the workload (for ncu captures); prints per-launch device times")
@@ -70,8 +71,9 @@ def run_kernel_only(args):
 
     torch.cuda.set_device(0)
     nrb.build()
-    pair = phantom.brain_pair(SHAPE, seed=args.seed)
-    nz, ny, nx = SHAPE
+    shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else SHAPE
+    pair = phantom.brain_pair(shape, seed=args.seed)
+    nz, ny, nx = shape
     dim, pix = (nx, ny, nz), (1.0, 1.0, 1.0)
     cdim, cpix, cxyz = nrb.control_grid_header(dim, pix, (5.0, 5.0, 5.0))
     rng = np.random.default_rng(args.seed)

@@ -378,12 +378,8 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
     cluster.sync();
     const int rank = (int)cluster.block_rank();
     for (int i = rank + HIST_CLUSTER * threadIdx.x; i < nbins; i += HIST_CLUSTER * blockDim.x) {
-        uint32_t part[HIST_CLUSTER];
-#pragma unroll
-        for (int q = 0; q < HIST_CLUSTER; ++q) part[q] = cluster.map_shared_rank(h, q)[i];  // loads in flight together
         uint32_t s = 0;
-#pragma unroll
-        for (int q = 0; q < HIST_CLUSTER; ++q) s += part[q];
+        for (int q = 0; q < HIST_CLUSTER; ++q) s += cluster.map_shared_rank(h, q)[i];
         if (s) atomicAdd(&ghist[i], s);
     }
     cluster.sync();  // no block leaves while another still reads its shared memory
@@ -666,7 +662,13 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
     cluster.sync();  // every block has read its halo counts; partial masses visible
     for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) hist[(size_t)f0 * rb + i] = 0u;  // next evaluation
     double total = 0.0;
-    for (int q = 0; q < FIN_CLUSTER; ++q) total += cluster.map_shared_rank(part, q)[0];
+    {
+        double pq[FIN_CLUSTER];
+#pragma unroll
+        for (int q = 0; q < FIN_CLUSTER; ++q) pq[q] = cluster.map_shared_rank(part, q)[0];  // in flight together
+#pragma unroll
+        for (int q = 0; q < FIN_CLUSTER; ++q) total += pq[q];
+    }
     // normalised own rows, their logs and the joint entropy
     double hj = 0.0;
     for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) {
@@ -688,26 +690,42 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
         for (int k = 0; k < nrow; ++k) sum += T[k * rb + r];
         R[r] = sum;
     }
-    // floating marginal of the own rows, summed over the reference bins in order
+    // floating marginal of the own rows: eight lanes per row, each summing a strided share of the
+    // reference bins, combined by shuffles in a fixed order
     double hw = 0.0;
-    for (int k = tid; k < nrow; k += FIN_CTA_THREADS) {
-        double sum = 0.0;
-        for (int r = 0; r < rb; ++r) sum += T[k * rb + r];
-        double l = 0.0;
-        if (sum > 0) {
-            l = log(sum);
-            hw -= sum * l;
+    {
+        const int sub = tid & 7;
+        // the trip count is the same for every thread, so all lanes reach the shuffles
+        for (int k0 = 0; k0 < rpc; k0 += FIN_CTA_THREADS / 8) {
+            const int k = k0 + (tid >> 3);
+            double sum = 0.0;
+            if (k < nrow)
+                for (int r = sub; r < rb; r += 8) sum += T[k * rb + r];
+            sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+            sum += __shfl_xor_sync(0xffffffffu, sum, 4);
+            if (sub == 0 && k < nrow) {
+                double l = 0.0;
+                if (sum > 0) {
+                    l = log(sum);
+                    hw -= sum * l;
+                }
+                pro[nj + rb + f0 + k] = sum;
+                logt[nj + rb + f0 + k] = l;
+            }
         }
-        pro[nj + rb + f0 + k] = sum;
-        logt[nj + rb + f0 + k] = l;
     }
     cluster.sync();  // partial reference marginals of every block visible
     // reference marginal: the blocks' partial sums added in block order (a fixed order, so the
     // result repeats bit for bit; it differs from a sequential sum only in the last bits)
     double hr = 0.0;
     for (int r = c + FIN_CLUSTER * tid; r < rb; r += FIN_CLUSTER * FIN_CTA_THREADS) {
+        double rq[FIN_CLUSTER];
+#pragma unroll
+        for (int q = 0; q < FIN_CLUSTER; ++q) rq[q] = cluster.map_shared_rank(R, q)[r];
         double sum = 0.0;
-        for (int q = 0; q < FIN_CLUSTER; ++q) sum += cluster.map_shared_rank(R, q)[r];
+#pragma unroll
+        for (int q = 0; q < FIN_CLUSTER; ++q) sum += rq[q];
         double l = 0.0;
         if (sum > 0) {
             l = log(sum);
@@ -728,12 +746,20 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
         for (int i = tid; i < n_be; i += FIN_CTA_THREADS) be += be_partials[i];
         block_sum3w<FIN_WARPS>(be, d1, d2, red);
         if (tid == 0) {
-            double h[3] = { 0.0, 0.0, 0.0 };
+            double hq[FIN_CLUSTER][3];
+#pragma unroll
             for (int q = 0; q < FIN_CLUSTER; ++q) {
                 const double *pq = cluster.map_shared_rank(part, q);
-                h[0] += pq[1];
-                h[1] += pq[2];
-                h[2] += pq[3];
+                hq[q][0] = pq[1];
+                hq[q][1] = pq[2];
+                hq[q][2] = pq[3];
+            }
+            double h[3] = { 0.0, 0.0, 0.0 };
+#pragma unroll
+            for (int q = 0; q < FIN_CLUSTER; ++q) {
+                h[0] += hq[q][0];
+                h[1] += hq[q][1];
+                h[2] += hq[q][2];
             }
             nrb_objective o;
             // with a zero similarity weight the reference never evaluates the measure
