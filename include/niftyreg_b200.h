@@ -300,10 +300,12 @@ nrb_status nrb_f3d_footprint(const int32_t dim[3], const float pixdim[3], const 
                              int64_t *bytes);
 
 /* A registration server on the current device: `slots` workers, each with its own stream, take
- * requests in arrival order as soon as a worker is free and the request's footprint fits in
- * what is left of hbm_budget_bytes (<= 0: 80% of the free device memory). Admitted requests run
- * concurrently and their kernels overlap; each result is the one nrb_f3d_register_host gives
- * for the same request alone. */
+ * requests in arrival order as soon as a worker is free, the request's footprint fits in what is
+ * left of hbm_budget_bytes (<= 0: 80% of the free device memory) and the running registrations
+ * do not already keep the device busy (a registration counts as min(1, voxels / 2^21) of the
+ * device; at most 2 devices' worth run at once). Admitted requests run concurrently and their
+ * kernels overlap; each result is the one nrb_f3d_register_host gives for the same request
+ * alone. */
 typedef struct nrb_server nrb_server;
 nrb_status nrb_server_create(int slots, int64_t hbm_budget_bytes, nrb_server **out);
 nrb_status nrb_server_submit(nrb_server *s, const nrb_pair *req, const nrb_f3d_params *p,

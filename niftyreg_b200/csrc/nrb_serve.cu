@@ -1,14 +1,16 @@
 // Batched and served F3D registrations on one device.
 //
 // A server owns `slots` worker threads, each with its own CUDA stream. Requests queue in
-// arrival order; the head of the queue is admitted when a worker is free and its device
-// footprint fits in what the HBM budget has left, so requests that arrive while others run are
+// arrival order; the head of the queue is admitted when a worker is free, its device footprint
+// fits in what the HBM budget has left and the device is not already kept busy by the running
+// registrations (load below, in whole devices), so requests that arrive while others run are
 // taken up as soon as a slot and memory free up, and their kernels overlap on the device with
 // the running ones. Each registration is the same sequence of launches as a plain
 // nrb_f3d_register_host call (deterministic kernels, no state shared between registrations), so
 // its result does not depend on what else runs.
 //
 // The batch entry point is a server sized to the batch that takes every pair at once.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -31,11 +33,18 @@ using Clock = std::chrono::steady_clock;
 
 namespace {
 
+// Share of the device one registration keeps busy on its own: its voxel passes are persistent
+// grids that fill every SM once the finest level has a few million voxels; smaller volumes leave
+// most of the device idle (latency-bound launches), so several of them overlap well.
+constexpr double kFillVoxels = 2.0 * 1024 * 1024;
+constexpr double kLoadCap = 2.0;  // admitted load, in whole devices
+
 struct Job {
     int64_t ticket = 0;
     nrb_pair pair{};
     nrb_f3d_params params{};
     int64_t footprint = 0;
+    double load = 0;
     Clock::time_point submitted, started, finished;
     bool done = false;
     nrb_status status = NRB_OK;
@@ -55,7 +64,14 @@ struct nrb_server {
     std::vector<std::thread> workers;
     int64_t next_ticket = 1, used = 0, peak_used = 0;
     int active = 0, peak_active = 0;
+    double load = 0;
     bool stop = false;
+
+    // the head of the queue fits: memory, and device load (always admitted when nothing runs)
+    bool head_fits() const {
+        const Job *j = queue.front();
+        return used + j->footprint <= budget && (active == 0 || load + j->load <= kLoadCap);
+    }
 
     void worker() {
         cudaSetDevice(device);
@@ -66,13 +82,12 @@ struct nrb_server {
             {
                 std::unique_lock<std::mutex> lock(mu);
                 // FIFO admission: the head waits for memory rather than being overtaken
-                cv.wait(lock, [&] {
-                    return (stop && queue.empty()) || (!queue.empty() && used + queue.front()->footprint <= budget);
-                });
+                cv.wait(lock, [&] { return (stop && queue.empty()) || (!queue.empty() && head_fits()); });
                 if (queue.empty()) break;  // stopping and drained
                 job = queue.front();
                 queue.pop_front();
                 used += job->footprint;
+                load += job->load;
                 ++active;
                 peak_used = std::max(peak_used, used);
                 peak_active = std::max(peak_active, active);
@@ -90,6 +105,7 @@ struct nrb_server {
                 job->error = err;
                 job->done = true;
                 used -= job->footprint;
+                load -= job->load;
                 --active;
             }
             cv.notify_all();
@@ -138,6 +154,7 @@ extern "C" nrb_status nrb_server_submit(nrb_server *s, const nrb_pair *req, cons
     job->pair = *req;
     job->params = *p;
     job->footprint = registration_footprint(req->dim, req->pixdim, p);
+    job->load = std::min(1.0, (double)req->dim[0] * req->dim[1] * req->dim[2] / kFillVoxels);
     if (job->footprint > s->budget) {
         delete job;
         return fail(NRB_ERR_OOM, "nrb_server_submit: request larger than the server's HBM budget");
