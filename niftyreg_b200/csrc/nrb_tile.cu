@@ -433,33 +433,36 @@ __device__ __forceinline__ float nmi_window_f(float rv, float wv, const float *l
     const float *wlog = rlog + rb;
     const int r0 = (int)(rv - 1.f), r1 = (int)(rv + 3.f);
     const int w0 = (int)(wv - 1.f), w1 = (int)(wv + 3.f);
-    float dw[4], wl[4];
-    bool wok[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int w = w0 + u;
-        wok[u] = w < w1 && -1 < w && w < fb;
-        dw[u] = wok[u] ? parzen_derivf(wv - (float)w) : 0.f;
-        wl[u] = wok[u] ? wlog[w] : 0.f;
-    }
-    float sr = 0.f, sw = 0.f, sj = 0.f;
+    // taps outside the window or the table get weight 0 and a clamped (valid) table index, so
+    // the sums need no branches; the marginal terms factor out of the double sum:
+    //   sum_tu br_t dw_u rlog_t = (sum_t br_t rlog_t)(sum_u dw_u), and likewise for wlog
+    float br[4], dw[4], rl[4], wl[4];
+    int ri[4], wi[4];
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
-        const int r = r0 + t;
-        if (!(r < r1 && -1 < r && r < rb)) continue;
-        const float br = parzenf(rv - (float)r);
-        const float rl = rlog[r];
-        const float *jrow = logt + r;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            if (!wok[u]) continue;
-            const float c = br * dw[u];
-            sr = fmaf(c, rl, sr);
-            sw = fmaf(c, wl[u], sw);
-            sj = fmaf(c, jrow[(w0 + u) * rb], sj);
-        }
+        const int r = r0 + t, w = w0 + t;
+        const bool rok = r < r1 && -1 < r && r < rb;
+        const bool wok = w < w1 && -1 < w && w < fb;
+        ri[t] = min(max(r, 0), rb - 1);
+        wi[t] = min(max(w, 0), fb - 1) * rb;
+        br[t] = rok ? parzenf(rv - (float)r) : 0.f;
+        dw[t] = wok ? parzen_derivf(wv - (float)w) : 0.f;
+        rl[t] = rlog[ri[t]];
+        wl[t] = wlog[min(max(w, 0), fb - 1)];
     }
-    return sr + sw - nmi * sj;
+    float sbr = 0.f, sdw = 0.f, sr = 0.f, sw = 0.f, sj = 0.f;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        sbr += br[t];
+        sdw += dw[t];
+        sr = fmaf(br[t], rl[t], sr);
+        sw = fmaf(dw[t], wl[t], sw);
+        float row = 0.f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) row = fmaf(dw[u], logt[ri[t] + wi[u]], row);
+        sj = fmaf(br[t], row, sj);
+    }
+    return fmaf(sr, sdw, sbr * sw) - nmi * sj;
 }
 
 // ---------------------------------------------------------------------------------------------
