@@ -375,6 +375,7 @@ nrb_status F3dRegistration::CaptureLineStep(cudaStream_t cs, cudaGraphConditiona
 //                                     line end + restart rule, restore best }
 // launched once; the host reads the optimiser state back when it ends.
 nrb_status F3dRegistration::RunLevelGraph(float max_step, float smallest_size, float current_size) {
+    const auto t_enter = std::chrono::steady_clock::now();
     if (!cap_st_) NRB_CUDA(cudaStreamCreateWithFlags(&cap_st_, cudaStreamNonBlocking));
     if (!dstate_) NRB_CUDA(dev_alloc(&dstate_, sizeof(OptState), st_));
     const long long n = 3 * nc_;
@@ -448,13 +449,21 @@ nrb_status F3dRegistration::RunLevelGraph(float max_step, float smallest_size, f
     const long long c_inner = g_launch_count.load() - c0 - c_top - c_outer;
     g_launch_count.fetch_sub(c_top + c_outer + c_inner);  // counted again below, per execution
 
+    const auto t_captured = std::chrono::steady_clock::now();
     NRB_CUDA(cudaGraphInstantiate(&top.exec, top.g, 0));
+    const auto t_instantiated = std::chrono::steady_clock::now();
     NRB_CUDA(cudaGraphLaunch(top.exec, st_));
     // RestoreBestDof of the last line search: the current position is the best one
     NRB_CUDA(cudaMemcpyAsync(cur_.p, best_.p, n * sizeof(float), cudaMemcpyDeviceToDevice, st_));
     OptState out;
     NRB_CUDA(cudaMemcpyAsync(&out, dstate_, sizeof(OptState), cudaMemcpyDeviceToHost, st_));
     NRB_CUDA(cudaStreamSynchronize(st_));
+    if (p_.verbose) {
+        const auto t_ran = std::chrono::steady_clock::now();
+        auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+        printf("[nrb]   graph: capture %.3f ms, instantiate %.3f ms, run %.3f ms\n", ms(t_enter, t_captured),
+               ms(t_captured, t_instantiated), ms(t_instantiated, t_ran));
+    }
     const long long iters = out.n_grad - n_grad_, steps = out.n_obj - n_obj_;
     g_launch_count.fetch_add(c_top + iters * c_outer + steps * c_inner);
     best_obj_ = out.best_obj;
@@ -618,13 +627,23 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const int32_
     }
     NRB_CUDA(cudaMallocAsync(&obj_, sizeof(nrb_objective), st_));
     NRB_CUDA(cudaMemsetAsync(obj_, 0, sizeof(nrb_objective), st_));
+    const auto tp = std::chrono::steady_clock::now();
     NRB_TRY(BuildPyramid(ref, flo, dim, pixdim));
     NRB_TRY(CreateGrid());
+    if (p_.verbose) {
+        NRB_CUDA(cudaStreamSynchronize(st_));
+        printf("[nrb] pyramid and grid %.3f ms\n",
+               std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp).count());
+    }
     max_it_ = (size_t)p_.max_iterations;
     max_it_ *= (size_t)std::pow(2, levels_ - 1);
     for (int level = 0; level < levels_; ++level) {
         float max_step = 0;
+        const auto ti = std::chrono::steady_clock::now();
         NRB_TRY(InitLevel(level, max_step));
+        if (p_.verbose)
+            printf("[nrb] level %d set-up (grid, workspace, rescale, initial objective) %.3f ms\n", level + 1,
+                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ti).count());
         float current_size = max_step;
         const float smallest_size = max_step / 100.0f;
         UpdateBestObjFunctionValue();

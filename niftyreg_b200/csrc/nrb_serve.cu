@@ -136,6 +136,10 @@ extern "C" nrb_status nrb_server_create(int slots, int64_t hbm_budget_bytes, nrb
     if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
         uint64_t thr = (uint64_t)s->budget;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        // no reuse across streams through inserted dependencies: a registration must never wait
+        // for another one's stream because the pool handed it memory that stream freed
+        int no = 0;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
     }
     cudaGetLastError();
     for (int i = 0; i < slots; ++i) s->workers.emplace_back([s] { s->worker(); });
