@@ -20,7 +20,6 @@ namespace nrb {
 // threads carry more registers, uses 4 warps.
 constexpr int COL_X = 32;
 constexpr int TY_OBJECTIVE = 16, TY_GRADIENT = 4, TY_DEFORMATION = 4;
-constexpr int HIST_CLUSTER = 8;  // blocks whose shared-memory histograms merge through DSMEM
 
 // State of the device-resident optimiser (ConjugateGradient::Optimise and the level loop of
 // reg_base::Run) that the control kernels of a level's CUDA graph advance.

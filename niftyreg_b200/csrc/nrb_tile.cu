@@ -1,7 +1,7 @@
 // Voxel-pass kernels of the F3D objective and gradient.
 //
-// Work item: a column of 32 (x) by 4 (y) reference voxels over a chunk of z slices. The block
-// stages the control points the item depends on in shared memory once (asynchronous copies),
+// Work item: a column of 32 (x) by ty (y) reference voxels over a chunk of z slices. The block
+// stages the control points the item depends on in shared memory once (batched loads),
 // together with the z basis of every slice of the chunk; then every thread walks its own voxel
 // column along z. The cubic B-spline sum sum_{a,b,c} Bx_a By_b Bz_c CP is evaluated
 // separably: for each node plane k the thread contracts the 4x4 (a, b) neighbourhood with its
@@ -11,9 +11,8 @@
 //
 // The deformation field never leaves the SM in the fused kernels: it is consumed at once by the
 // trilinear warp and then by the joint histogram (objective) or by the spatial gradient and the
-// NMI voxel gradient (gradient). Blocks are persistent; in the objective kernel they run in
-// clusters of 8 that merge their shared-memory histograms through distributed shared memory
-// before one flush per cluster.
+// NMI voxel gradient (gradient). Blocks are persistent; in the objective kernel each keeps a
+// shared-memory joint histogram and flushes it with one atomic per non-zero bin.
 #include <cooperative_groups.h>
 #include <cuda_pipeline.h>
 
@@ -56,11 +55,11 @@ __host__ __device__ inline int walk_table_floats(int zchunk) { return 5 * zchunk
 
 struct Item {
     int x0, y0, z0, z1, xa0, yb0, zc0;
-    float off[3];
 };
 
-// Stages the control points of `item` relative to the item's first node (which keeps the
-// partial sums small) into cp[3][sc][sb][sa], and the z basis of each slice into the tables.
+// Stages the control points of `item` into cp[3][sc][sb][sa] and the z basis of each slice into
+// the tables. The values are staged as they are (not relative to the item), so a voxel's
+// position is the same float whatever the item decomposition, and so are the results.
 // With kTrial the control points are the line search's trial values best + scale * grad
 // (`cpp` = best), formed here instead of in a separate update pass. Called by every thread of
 // the block.
@@ -82,9 +81,6 @@ __device__ __forceinline__ void stage_item(const WalkParams& P, const float *__r
     const int na = pre_of(min(I.x0 + COL_X - 1, P.nx - 1), P.gsx) + 4 - I.xa0;
     const int nb = pre_of(min(I.y0 + P.ty - 1, P.ny - 1), P.gsy) + 4 - I.yb0;
     const int nc = pre_of(I.z1 - 1, P.gsz) + 4 - I.zc0;
-    const int first = (I.zc0 * P.cy + I.yb0) * P.cx + I.xa0;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) I.off[c] = trial_cp(cpp, kTrial ? grad : nullptr, scale, c * P.cnv + first);
     const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
     __syncthreads();  // the previous item's readers are done
     // one pass: the node planes of one (component, row, column) are independent loads, batched
@@ -103,12 +99,12 @@ __device__ __forceinline__ void stage_item(const WalkParams& P, const float *__r
                     const float v1 = trial_cp(cpp, g, scale, src + (kc + 1) * gplane);
                     const float v2 = trial_cp(cpp, g, scale, src + (kc + 2) * gplane);
                     const float v3 = trial_cp(cpp, g, scale, src + (kc + 3) * gplane);
-                    dst[kc * splane] = v0 - I.off[c];
-                    dst[(kc + 1) * splane] = v1 - I.off[c];
-                    dst[(kc + 2) * splane] = v2 - I.off[c];
-                    dst[(kc + 3) * splane] = v3 - I.off[c];
+                    dst[kc * splane] = v0;
+                    dst[(kc + 1) * splane] = v1;
+                    dst[(kc + 2) * splane] = v2;
+                    dst[(kc + 3) * splane] = v3;
                 }
-                for (; kc < nc; ++kc) dst[kc * splane] = trial_cp(cpp, g, scale, src + kc * gplane) - I.off[c];
+                for (; kc < nc; ++kc) dst[kc * splane] = trial_cp(cpp, g, scale, src + kc * gplane);
             }
     for (int zi = threadIdx.x; zi < I.z1 - I.z0; zi += blockDim.x) {
         const int z = I.z0 + zi;
@@ -189,7 +185,7 @@ __device__ __forceinline__ void column_position(const WalkParams& P, const Item&
         s = fmaf(bz.y, C.S[1][c], s);
         s = fmaf(bz.z, C.S[2][c], s);
         s = fmaf(bz.w, C.S[3][c], s);
-        pos[c] = I.off[c] + s;
+        pos[c] = s;
     }
 }
 
@@ -372,17 +368,13 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
             }
         }
     }
-    // merge the cluster's histograms through distributed shared memory: block r of the cluster
-    // owns bins r, r + 8, r + 16, ... and flushes their sums with one atomic each
-    cg::cluster_group cluster = cg::this_cluster();
-    cluster.sync();
-    const int rank = (int)cluster.block_rank();
-    for (int i = rank + HIST_CLUSTER * threadIdx.x; i < nbins; i += HIST_CLUSTER * blockDim.x) {
-        uint32_t s = 0;
-        for (int q = 0; q < HIST_CLUSTER; ++q) s += cluster.map_shared_rank(h, q)[i];
-        if (s) atomicAdd(&ghist[i], s);
+    // one atomic per non-zero bin of the block (merging the blocks of a cluster through
+    // distributed shared memory first was measured slower at every volume size)
+    __syncthreads();
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
+        const uint32_t c = h[i];
+        if (c) atomicAdd(&ghist[i], c);
     }
-    cluster.sync();  // no block leaves while another still reads its shared memory
 }
 
 // Sum over the 4x4 Parzen window of reg_getVoxelBasedNmiGradient3d (_reg_nmi.cpp:548-571):
@@ -900,53 +892,6 @@ static nrb_status persistent_grid(K kernel, int threads, size_t smem, int nitems
     return NRB_OK;
 }
 
-// co-resident blocks of the objective pass: whole clusters of HIST_CLUSTER blocks, as many as
-// the GPU can hold at once (fewer than blocks-per-SM x SMs would suggest: a cluster lives on one
-// GPC)
-static long long objective_slots_query(size_t smem);
-
-long long objective_slots(size_t smem) {
-    // cached per (device, shared bytes): the launch path asks on every evaluation
-    static std::mutex mu;
-    static std::map<std::pair<int, size_t>, long long> cache;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        auto it = cache.find({ dev, smem });
-        if (it != cache.end()) return it->second;
-    }
-    const long long v = objective_slots_query(smem);
-    std::lock_guard<std::mutex> lock(mu);
-    cache[{ dev, smem }] = v;
-    return v;
-}
-
-static long long objective_slots_query(size_t smem) {
-    auto kernel = k_objective<true>;
-    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(HIST_CLUSTER * 64);
-    cfg.blockDim = dim3(32 * TY_OBJECTIVE);
-    cfg.dynamicSmemBytes = smem;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = HIST_CLUSTER;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, (void *)kernel, &cfg) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    return (long long)clusters * HIST_CLUSTER;
-}
-
 template <typename K>
 static long long blocks_resident(K kernel, int threads, size_t smem) {
     int per_sm = 0;
@@ -958,6 +903,7 @@ static long long blocks_resident(K kernel, int threads, size_t smem) {
     return (long long)per_sm * sm_count();
 }
 
+long long objective_slots(size_t smem) { return blocks_resident(k_objective<true>, 32 * TY_OBJECTIVE, smem); }
 long long gradient_slots(size_t smem) { return blocks_resident(k_gradient<true>, 32 * TY_GRADIENT, smem); }
 long long deformation_slots(size_t smem) { return blocks_resident(k_deformation, 32 * TY_DEFORMATION, smem); }
 
@@ -971,29 +917,14 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
     const bool trial = grad != nullptr;
     auto kernel = trial ? k_objective<true> : k_objective<false>;
     int grid = 0;
-    NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid, (int)objective_slots(smem)));
-    grid = ((grid + HIST_CLUSTER - 1) / HIST_CLUSTER) * HIST_CLUSTER;  // whole clusters
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = HIST_CLUSTER;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid));
     // algorithmic bytes: reference + floating (+ mask) per voxel, the grid once
     const double nv = (double)P.nx * P.ny * P.nz;
     const double bytes = nv * (mask ? 12.0 : 8.0) + 12.0 * (double)P.cnv;
-    cudaError_t e;
     {
         KernelTimer timer(TK_OBJECTIVE, bytes, st);
-        e = cudaLaunchKernelEx(&cfg, kernel, P, ref, flo, mask, cpp, nmi->hist, grad, step);
+        kernel<<<grid, threads, smem, st>>>(P, ref, flo, mask, cpp, nmi->hist, grad, step);
     }
-    NRB_CUDA(e);
     NRB_LAUNCHED("k_objective");
     return NRB_OK;
 }
