@@ -41,6 +41,7 @@ struct WalkParams {
     int rb, fb;              // internal bin counts
     int cnv;                 // control points per component
     int log_in_smem;         // gradient: an FP32 copy of the log table is staged in shared memory
+    int xs;                  // objective: x-contracted rows of the item staged in shared memory
 };
 
 __device__ __forceinline__ int pre_of(int v, float gs) { return (int)((float)v / gs); }
@@ -121,6 +122,7 @@ struct Column {
     int x, y;
     bool inside;     // the column lies inside the reference volume
     float bx[4], by[4];
+    int xoff, yrow;  // first node of the column relative to the staged block (x, y)
     const float *base;
     int win;         // relative z node index of S[0]
     float S[4][3];
@@ -135,7 +137,9 @@ __device__ __forceinline__ void column_init(const WalkParams& P, const Item& I, 
     const int px = pre_of(xc, P.gsx), py = pre_of(yc, P.gsy);
     bspline_basis(frac_of(xc, P.gsx, px), C.bx);
     bspline_basis(frac_of(yc, P.gsy, py), C.by);
-    C.base = cp + (py - I.yb0) * P.sa + (px - I.xa0);
+    C.xoff = px - I.xa0;
+    C.yrow = py - I.yb0;
+    C.base = cp + C.yrow * P.sa + C.xoff;
     C.win = INT_MIN;
 }
 
@@ -160,10 +164,43 @@ __device__ __forceinline__ void column_plane(const WalkParams& P, const Column& 
     }
 }
 
+// The x contraction of every (component, node plane, node row) of the item for the 32 columns
+// of its x tile, X[c][k][b][lane] = sum_a bx_lane[a] cp[c][k][b][px_lane - xa0 + a], built once
+// per item by the whole block (same operations, same order as column_plane's inner sum). Walks
+// then contract only over the 4 rows: 4 shared loads and 4 FMAs per component and plane instead
+// of 16 + 16. Called by every thread after stage_item; ends with a barrier.
+__device__ __forceinline__ void build_xrows(const WalkParams& P, const Column& C, const float *cp, float *X) {
+    const int lx = threadIdx.x & 31, ly = threadIdx.x >> 5;
+    const int rows = 3 * P.sc * P.sb;  // (c, k, b) rows of the staged block, b fastest
+    for (int e = ly; e < rows; e += P.ty) {
+        const float *r = cp + e * P.sa + C.xoff;
+        float t = C.bx[0] * r[0];
+        t = fmaf(C.bx[1], r[1], t);
+        t = fmaf(C.bx[2], r[2], t);
+        t = fmaf(C.bx[3], r[3], t);
+        X[e * 32 + lx] = t;
+    }
+    __syncthreads();
+}
+
+// S for relative node plane k from the x-contracted rows
+__device__ __forceinline__ void column_plane_x(const WalkParams& P, const Column& C, const float *X, int k,
+                                               float out[3]) {
+    const int lx = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float *q = X + ((c * P.sc + k) * P.sb + C.yrow) * 32 + lx;
+        float s = 0.f;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) s = fmaf(C.by[b], q[b * 32], s);
+        out[c] = s;
+    }
+}
+
 // World position (mm) of slice index zi (relative to the item) of the thread's column; zi must
-// not decrease between calls.
+// not decrease between calls. X: the item's x-contracted rows, or null.
 __device__ __forceinline__ void column_position(const WalkParams& P, const Item& I, Column& C, const float *zb,
-                                                const int *zk, int zi, float pos[3]) {
+                                                const int *zk, int zi, float pos[3], const float *X = nullptr) {
     const int pz = zk[zi];
     if (pz != C.win) {
         if (pz == C.win + 1) {
@@ -171,10 +208,14 @@ __device__ __forceinline__ void column_position(const WalkParams& P, const Item&
             for (int t = 0; t < 3; ++t)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) C.S[t][c] = C.S[t + 1][c];
-            column_plane(P, C, pz + 3, C.S[3]);
+            if (X) column_plane_x(P, C, X, pz + 3, C.S[3]);
+            else column_plane(P, C, pz + 3, C.S[3]);
         } else {
 #pragma unroll
-            for (int t = 0; t < 4; ++t) column_plane(P, C, pz + t, C.S[t]);
+            for (int t = 0; t < 4; ++t) {
+                if (X) column_plane_x(P, C, X, pz + t, C.S[t]);
+                else column_plane(P, C, pz + t, C.S[t]);
+            }
         }
         C.win = pz;
     }
@@ -324,6 +365,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
     const float scale = kTrial ? -step->cur_len : 0.f;
     uint32_t *h = reinterpret_cast<uint32_t *>(S.tail);
     const int nbins = P.rb * P.fb;
+    float *X = reinterpret_cast<float *>(h + ((nbins + 3) & ~3));  // x-contracted rows (P.xs)
     for (int i = threadIdx.x; i < nbins; i += blockDim.x) h[i] = 0u;
     const int lane = threadIdx.x & 31;
     const float frb = (float)P.rb, ffb = (float)P.fb;
@@ -332,6 +374,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
         stage_item<kTrial>(P, cpp, item, S.cp, S.zb, S.zk, I, grad, scale);
         Column C;
         column_init(P, I, S.cp, C);
+        if (P.xs) build_xrows(P, C, S.cp, X);
         const int nzi = I.z1 - I.z0;
         int idx = (I.z0 * P.ny + C.y) * P.nx + C.x;
         const int zstride = P.nx * P.ny;
@@ -341,7 +384,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
             for (int u = 0; u < WALK_GROUP; ++u) {
                 const int zu = min(zi + u, nzi - 1);
                 float pos[3];
-                column_position(P, I, C, S.zb, S.zk, zu, pos);
+                column_position(P, I, C, S.zb, S.zk, zu, pos, P.xs ? X : nullptr);
                 bin[u] = -1;
                 if (C.inside && zi + u < nzi) {
                     const int vi = idx + u * zstride;
@@ -873,6 +916,7 @@ static WalkParams make_params(const WalkPlan& W, const nrb_geometry *g, float pa
     const float *m = g->flo_ijk;
     P.flo_diag = m[1] == 0.f && m[2] == 0.f && m[4] == 0.f && m[6] == 0.f && m[8] == 0.f && m[9] == 0.f;
     P.log_in_smem = 0;
+    P.xs = 0;
     return P;
 }
 
@@ -911,8 +955,12 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
                                   const float *ref, const float *flo, const int32_t *mask,
                                   const float *cpp, float padding, cudaStream_t st,
                                   const float *grad, const OptState *step) {
-    const WalkParams P = make_params(ws->walk_obj, g, padding, nmi->rb, nmi->fb);
-    const size_t smem = walk_smem_bytes(ws->walk_obj) + (size_t)nmi->rb * nmi->fb * 4;
+    WalkParams P = make_params(ws->walk_obj, g, padding, nmi->rb, nmi->fb);
+    const size_t base_smem = walk_smem_bytes(ws->walk_obj) + (size_t)((nmi->rb * nmi->fb + 3) & ~3) * 4;
+    const size_t xs_bytes = (size_t)3 * P.sc * P.sb * 32 * 4;
+    // the x-contracted rows when two blocks per SM still fit
+    P.xs = base_smem + xs_bytes <= 100 * 1024;
+    const size_t smem = base_smem + (P.xs ? xs_bytes : 0);
     const int threads = 32 * ws->walk_obj.ty;
     const bool trial = grad != nullptr;
     auto kernel = trial ? k_objective<true> : k_objective<false>;
