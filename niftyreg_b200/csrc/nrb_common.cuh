@@ -1,6 +1,8 @@
 // Internal helpers shared by the niftyreg_b200 CUDA sources (not part of the public ABI).
 #pragma once
 
+#include <utility>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -40,6 +42,28 @@ extern std::atomic<long long> g_launch_count;
     } while (0)
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization may
+// start while its predecessor's last blocks are still running; it must wait here before it reads
+// anything the predecessor writes. Without that launch attribute the wait returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// cudaLaunchKernelEx with programmatic stream serialization when `pdl` is set.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t st, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Device allocation tied to an owner's stream: stream-ordered (no device-wide synchronisation,
 // so registrations on other streams keep running) when `st` is set, plain otherwise.

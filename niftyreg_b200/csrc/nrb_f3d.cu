@@ -77,6 +77,7 @@ __global__ void k_ctl_line_end(OptState *s, cudaGraphConditionalHandle outer) {
 // objective kernel formed on the fly (same float operations)
 __global__ void k_accept(long long n, float *__restrict__ best, const float *__restrict__ grad,
                          const OptState *__restrict__ s) {
+    pdl_wait();  // the decision comes from the finalize
     if (!s->accepted) return;
     const float scale = -s->step_len;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -364,7 +365,8 @@ nrb_status F3dRegistration::CaptureLineStep(cudaStream_t cs, cudaGraphConditiona
     NRB_TRY(launch_nmi_finalize(nmi_.h, ws->be_partials, n_be, 3 * nvox(g_.cpp_dim), sim_w_, be_w_, obj_, cs,
                                 dstate_, line));
     const long long n = 3 * nc_;
-    k_accept<<<elementwise_grid(n), 256, 0, cs>>>(n, best_.p, grad_.p, dstate_);
+    NRB_CUDA(launch_pdl(true, k_accept, dim3(elementwise_grid(n)), dim3(256), 0, cs, n, best_.p, grad_.p,
+                        (const OptState *)dstate_));
     NRB_LAUNCHED("k_accept");
     return NRB_OK;
 }

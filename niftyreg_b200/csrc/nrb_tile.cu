@@ -362,11 +362,12 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
             uint32_t *__restrict__ ghist, const float *__restrict__ grad, const OptState *__restrict__ step) {
     extern __shared__ float4 sm4[];
     const WalkSmem S = walk_smem(P, sm4);
-    const float scale = kTrial ? -step->cur_len : 0.f;
     uint32_t *h = reinterpret_cast<uint32_t *>(S.tail);
     const int nbins = P.rb * P.fb;
     float *X = reinterpret_cast<float *>(h + ((nbins + 3) & ~3));  // x-contracted rows (P.xs)
     for (int i = threadIdx.x; i < nbins; i += blockDim.x) h[i] = 0u;
+    if (kTrial) pdl_wait();  // the trial position and step length come from the previous launch
+    const float scale = kTrial ? -step->cur_len : 0.f;
     const int lane = threadIdx.x & 31;
     const float frb = (float)P.rb, ffb = (float)P.fb;
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
@@ -658,6 +659,7 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
                const double *__restrict__ be_partials, int n_be, double be_norm,
                double sim_weight, double be_weight, nrb_objective *__restrict__ obj,
                OptState *__restrict__ ctl, cudaGraphConditionalHandle line) {
+    pdl_wait();  // the counts come from the objective pass
     cg::cluster_group cluster = cg::this_cluster();
     // output table set: the one not holding the best position (read before thread 0 of block 0
     // updates the state at the very end)
@@ -969,10 +971,13 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
     // algorithmic bytes: reference + floating (+ mask) per voxel, the grid once
     const double nv = (double)P.nx * P.ny * P.nz;
     const double bytes = nv * (mask ? 12.0 : 8.0) + 12.0 * (double)P.cnv;
+    cudaError_t e;
     {
         KernelTimer timer(TK_OBJECTIVE, bytes, st);
-        kernel<<<grid, threads, smem, st>>>(P, ref, flo, mask, cpp, nmi->hist, grad, step);
+        e = launch_pdl(trial, kernel, dim3(grid), dim3(threads), smem, st, P, ref, flo, mask, cpp, nmi->hist, grad,
+                       step);
     }
+    NRB_CUDA(e);
     NRB_LAUNCHED("k_objective");
     return NRB_OK;
 }
@@ -1011,11 +1016,9 @@ nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be
     const size_t smem = (size_t)(2 * rpc + 2) * nmi->rb * sizeof(double);
     NRB_CUDA(cudaFuncSetAttribute(k_nmi_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     KernelTimer timer(TK_FINALIZE, (double)nmi->rb * nmi->fb * 8 + (double)nmi->total * 16, st);
-    k_nmi_finalize<<<FIN_CLUSTER, FIN_CTA_THREADS, smem, st>>>(nmi->rb, nmi->fb, nmi->hist, nmi->pro, nmi->logt,
-                                                               nmi->last, nmi->pro2, nmi->logt2, nmi->last2,
-                                                               be_partials, n_be_partials,
-                                                               (double)cpp_nvox3, sim_weight, be_weight, obj,
-                                                               ctl, line);
+    NRB_CUDA(launch_pdl(ctl != nullptr, k_nmi_finalize, dim3(FIN_CLUSTER), dim3(FIN_CTA_THREADS), smem, st, nmi->rb,
+                        nmi->fb, nmi->hist, nmi->pro, nmi->logt, nmi->last, nmi->pro2, nmi->logt2, nmi->last2,
+                        be_partials, n_be_partials, (double)cpp_nvox3, sim_weight, be_weight, obj, ctl, line));
     NRB_LAUNCHED("k_nmi_finalize");
     return NRB_OK;
 }
