@@ -2,6 +2,8 @@
 // conjugate-gradient line search of reg_f3d<float>::Run, with every image, grid and optimiser
 // array resident in HBM. Each objective evaluation returns one packed struct to the host, which
 // takes the line-search branch exactly as Optimiser::Optimise does.
+#include <cooperative_groups.h>
+
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -11,6 +13,8 @@
 #include <vector>
 
 #include "nrb_state.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace nrb {
 
@@ -71,6 +75,130 @@ __global__ void k_ctl_line_end(OptState *s, cudaGraphConditionalHandle outer) {
         s->just_restarted = 0;
     }
     cudaGraphSetConditional(outer, outer_continues(*s) ? 1u : 0u);
+}
+
+// The node-grid tail of a gradient evaluation in one launch (one cluster of TAIL_CTAS blocks):
+// GetMaximalLength + NormaliseGradient (reg-lib/Compute.cpp:140-176), the iteration count and
+// min(current_size, max_step), ConjugateGradient::UpdateGradientValues (reg-lib/Optimiser.cpp:
+// 231-317) and the start of Optimise. Every value is computed with the operations, and every
+// FP64 dot product with the partition and summation order, of the separate kernels the host loop
+// launches (k_maxlen/k_maxlen_finish, k_normalise, k_cg_dots/k_cg_update), so both loops stay
+// bit-identical. n = 3 * nnode; partials: 2 * NRB_RED_BLOCKS doubles.
+constexpr int TAIL_CTAS = 8, TAIL_THREADS = 1024;
+constexpr long long kNodeTailMaxNodes = 16384;  // above it the passes are bandwidth-bound on 8 SMs
+
+__global__ void __cluster_dims__(TAIL_CTAS, 1, 1) __launch_bounds__(TAIL_THREADS)
+k_node_tail(long long nnode, float *__restrict__ g, float *__restrict__ g1, float *__restrict__ g2,
+            double *__restrict__ partials, nrb_objective *__restrict__ obj, OptState *__restrict__ s,
+            cudaGraphConditionalHandle line) {
+    cg::cluster_group cluster = cg::this_cluster();
+    __shared__ float fmx[TAIL_THREADS / 32];
+    __shared__ double red[TAIL_THREADS];
+    __shared__ double gam_s;
+    const int rank = (int)cluster.block_rank(), tid = threadIdx.x;
+    const long long gtid = (long long)rank * TAIL_THREADS + tid, gstride = (long long)TAIL_CTAS * TAIL_THREADS;
+    const long long n = 3 * nnode;
+    const bool first = s->first_call != 0;  // read before block 0 changes the state at the end
+    // largest node-gradient length (a max: exact in any order)
+    float mx = 0.f;
+    for (long long i = gtid; i < nnode; i += gstride) {
+        const float x = g[i], y = g[nnode + i], z = g[2 * nnode + i];
+        mx = fmaxf(mx, sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z))));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((tid & 31) == 0) fmx[tid >> 5] = mx;
+    __syncthreads();
+    if (tid == 0) {
+        float m = 0.f;
+        for (int w = 0; w < TAIL_THREADS / 32; ++w) m = fmaxf(m, fmx[w]);
+        fmx[0] = m;
+    }
+    cluster.sync();
+    float m = 0.f;
+#pragma unroll
+    for (int q = 0; q < TAIL_CTAS; ++q) m = fmaxf(m, cluster.map_shared_rank(fmx, q)[0]);
+    const double len = (double)m;
+    const bool scale = len != 0;
+    const double inv = scale ? 1.0 / len : 1.0;
+    auto normalised = [&](long long i) { return scale ? (float)((double)g[i] * inv) : g[i]; };
+    if (first) {
+        for (long long i = gtid; i < n; i += gstride) {
+            const float v = normalised(i);
+            g[i] = v;
+            g1[i] = -v;
+            g2[i] = -v;
+        }
+    } else {
+        // the FP64 dots of k_cg_dots: virtual blocks of NRB_RED_THREADS threads, grid-stride over
+        // np virtual blocks, tree-summed per virtual block
+        const long long nb = (n + NRB_RED_THREADS - 1) / NRB_RED_THREADS;
+        const int np = (int)(nb < 1 ? 1 : (nb > NRB_RED_BLOCKS ? NRB_RED_BLOCKS : nb));
+        constexpr int VPB = TAIL_THREADS / NRB_RED_THREADS;  // virtual blocks per block at a time
+        const int vsub = tid / NRB_RED_THREADS, t = tid % NRB_RED_THREADS;
+        double *r = red + vsub * NRB_RED_THREADS;
+        for (int v0 = rank * VPB; v0 < np; v0 += TAIL_CTAS * VPB) {  // same trip count in the block
+            const int v = v0 + vsub;
+            double gg = 0, dgg = 0;
+            if (v < np)
+                for (long long i = (long long)v * NRB_RED_THREADS + t; i < n; i += (long long)np * NRB_RED_THREADS) {
+                    const float gi = normalised(i);
+                    gg += (double)__fmul_rn(g2[i], g1[i]);
+                    dgg += (double)__fmul_rn(__fadd_rn(gi, g1[i]), gi);
+                }
+            // block_sum_d's tree, once for gg and once for dgg
+            r[t] = gg;
+            __syncthreads();
+            for (int k = NRB_RED_THREADS / 2; k > 0; k >>= 1) {
+                if (t < k) r[t] += r[t + k];
+                __syncthreads();
+            }
+            const double a = r[0];
+            __syncthreads();
+            r[t] = dgg;
+            __syncthreads();
+            for (int k = NRB_RED_THREADS / 2; k > 0; k >>= 1) {
+                if (t < k) r[t] += r[t + k];
+                __syncthreads();
+            }
+            if (t == 0 && v < np) {
+                partials[2 * v] = a;
+                partials[2 * v + 1] = r[0];
+            }
+            __syncthreads();
+        }
+        cluster.sync();  // every partial written
+        if (rank == 0 && tid == 0) {
+            double gg = 0, dgg = 0;
+            for (int i = 0; i < np; ++i) {
+                gg += partials[2 * i];
+                dgg += partials[2 * i + 1];
+            }
+            gam_s = dgg / gg;
+        }
+        cluster.sync();
+        const double gm = *cluster.map_shared_rank(&gam_s, 0);
+        for (long long i = gtid; i < n; i += gstride) {
+            const float a1 = -normalised(i);
+            const float a2 = (float)((double)a1 + gm * (double)g2[i]);
+            g1[i] = a1;
+            g2[i] = a2;
+            g[i] = -a2;
+        }
+    }
+    if (rank == 0 && tid == 0) {
+        obj->max_grad_len = len;
+        // iteration counted, current_size = min(current_size, max_step), then Optimise starts
+        s->it += 1;
+        s->n_grad += 1;
+        s->current_size = s->max_step < s->current_size ? s->max_step : s->current_size;
+        s->first_call = 0;
+        s->line_iter = 0;
+        s->added_len = 0.f;
+        s->cur_len = s->current_size;
+        cudaGraphSetConditional(line, line_continues(*s) ? 1u : 0u);
+    }
+    cluster.sync();  // block 0's shared values stay readable until every block has read them
 }
 
 // StoreCurrentDof after an accepted step: best = best + (-len) * grad, the trial position the
@@ -342,10 +470,7 @@ nrb_status F3dRegistration::CaptureGradient(cudaStream_t cs) {
         NRB_TRY(join_side(ws, cs));
         NRB_TRY(launch_be_accumulate(ws, &g_, be_w_, grad_.p, cs));
     }
-    NRB_TRY(max_and_normalise(ws_.h, grad_.p, nc_, obj_, cs));
-    k_ctl_gradient_done<<<1, 1, 0, cs>>>(dstate_);
-    NRB_LAUNCHED("k_ctl_gradient_done");
-    return NRB_OK;
+    return NRB_OK;  // the node-grid tail follows as one launch (k_node_tail)
 }
 
 // One line-search step as captured launches: the objective at the trial position
@@ -425,11 +550,29 @@ nrb_status F3dRegistration::RunLevelGraph(float max_step, float smallest_size, f
     NRB_CUDA(cudaStreamBeginCaptureToGraph(cap_st_, outer_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     {
         nrb_status s = CaptureGradient(cap_st_);
-        if (s == NRB_OK) s = cg_update_flagged(ws_.h, grad_.p, g1_.p, g2_.p, n, &dstate_->first_call, cap_st_);
-        if (s == NRB_OK) {
-            k_ctl_line_start<<<1, 1, 0, cap_st_>>>(dstate_, h_inner);
-            g_launch_count.fetch_add(1);
-            if (cudaGetLastError() != cudaSuccess) s = fail(NRB_ERR_CUDA, "registration: line start launch");
+        if (nc_ <= kNodeTailMaxNodes) {
+            // small grids: the node-grid tail is a chain of latency-bound launches; one cluster
+            // does all of it
+            if (s == NRB_OK) {
+                k_node_tail<<<TAIL_CTAS, TAIL_THREADS, 0, cap_st_>>>(nc_, grad_.p, g1_.p, g2_.p, ws_.h->red, obj_,
+                                                                     dstate_, h_inner);
+                g_launch_count.fetch_add(1);
+                if (cudaGetLastError() != cudaSuccess) s = fail(NRB_ERR_CUDA, "registration: node tail launch");
+            }
+        } else {
+            // large grids: the separate kernels spread the passes over the whole device
+            if (s == NRB_OK) s = max_and_normalise(ws_.h, grad_.p, nc_, obj_, cap_st_);
+            if (s == NRB_OK) {
+                k_ctl_gradient_done<<<1, 1, 0, cap_st_>>>(dstate_);
+                g_launch_count.fetch_add(1);
+                if (cudaGetLastError() != cudaSuccess) s = fail(NRB_ERR_CUDA, "registration: gradient count launch");
+            }
+            if (s == NRB_OK) s = cg_update_flagged(ws_.h, grad_.p, g1_.p, g2_.p, n, &dstate_->first_call, cap_st_);
+            if (s == NRB_OK) {
+                k_ctl_line_start<<<1, 1, 0, cap_st_>>>(dstate_, h_inner);
+                g_launch_count.fetch_add(1);
+                if (cudaGetLastError() != cudaSuccess) s = fail(NRB_ERR_CUDA, "registration: line start launch");
+            }
         }
         if (s == NRB_OK) s = capture_while(cap_st_, h_inner, &inner_body);
         if (s == NRB_OK) {
