@@ -487,9 +487,13 @@ nrb_status F3dRegistration::CaptureLineStep(cudaStream_t cs, cudaGraphConditiona
     }
     NRB_TRY(launch_fused_objective(ws, nmi_.h, &g_, ref_.p, flo_.p, nullptr, best_.p, pad_, cs, grad_.p, dstate_));
     if (be_w_ > 0) NRB_TRY(join_side(ws, cs));
-    NRB_TRY(launch_nmi_finalize(nmi_.h, ws->be_partials, n_be, 3 * nvox(g_.cpp_dim), sim_w_, be_w_, obj_, cs,
-                                dstate_, line));
     const long long n = 3 * nc_;
+    // small grids: the finalize also stores an accepted trial position (one launch fewer per
+    // step); large grids: a whole-device pass does it
+    const bool fold = nc_ <= kNodeTailMaxNodes;
+    NRB_TRY(launch_nmi_finalize(nmi_.h, ws->be_partials, n_be, 3 * nvox(g_.cpp_dim), sim_w_, be_w_, obj_, cs,
+                                dstate_, line, fold ? best_.p : nullptr, grad_.p, fold ? n : 0));
+    if (fold) return NRB_OK;
     NRB_CUDA(launch_pdl(true, k_accept, dim3(elementwise_grid(n)), dim3(256), 0, cs, n, best_.p, grad_.p,
                         (const OptState *)dstate_));
     NRB_LAUNCHED("k_accept");

@@ -152,11 +152,13 @@ nrb_status validate_geometry(const nrb_geometry *g);
 
 // launchers shared between translation units
 // ctl (optional, inside a level graph): the finalize writes the table set that does not hold the
-// best position, takes the line-search step and sets the line search's WHILE condition `line`
+// best position, takes the line-search step and sets the line search's WHILE condition `line`;
+// with acc_n > 0 it also stores an accepted trial position: acc_best += -step_len * acc_grad
 nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be_partials,
                                int64_t cpp_nvox3, double sim_weight, double be_weight,
                                nrb_objective *obj, cudaStream_t st, OptState *ctl = nullptr,
-                               cudaGraphConditionalHandle line = 0);
+                               cudaGraphConditionalHandle line = 0, float *acc_best = nullptr,
+                               const float *acc_grad = nullptr, long long acc_n = 0);
 // grad/step (optional): evaluate at the line search's trial position cpp - step->cur_len * grad
 nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                   const float *ref, const float *flo, const int32_t *mask,

@@ -658,7 +658,8 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
                double *pro1, double *logt1, nrb_objective *last1,
                const double *__restrict__ be_partials, int n_be, double be_norm,
                double sim_weight, double be_weight, nrb_objective *__restrict__ obj,
-               OptState *__restrict__ ctl, cudaGraphConditionalHandle line) {
+               OptState *__restrict__ ctl, cudaGraphConditionalHandle line, float *__restrict__ acc_best,
+               const float *__restrict__ acc_grad, long long acc_n) {
     pdl_wait();  // the counts come from the objective pass
     cg::cluster_group cluster = cg::this_cluster();
     // output table set: the one not holding the best position (read before thread 0 of block 0
@@ -818,6 +819,13 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
         }
     }
     cluster.sync();  // every block's shared memory stays alive until block 0 has read it
+    // small grids: the store of an accepted trial position (k_accept's operations) in the same
+    // launch; the decision written by block 0 above is visible to the cluster after the barrier
+    if (acc_n > 0 && ctl->accepted) {
+        const float scale = -ctl->step_len;
+        for (long long i = (long long)c * FIN_CTA_THREADS + tid; i < acc_n; i += (long long)FIN_CLUSTER * FIN_CTA_THREADS)
+            acc_best[i] = __fadd_rn(acc_best[i], __fmul_rn(scale, acc_grad[i]));
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1011,14 +1019,16 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
 nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be_partials,
                                int64_t cpp_nvox3, double sim_weight, double be_weight,
                                nrb_objective *obj, cudaStream_t st, OptState *ctl,
-                               cudaGraphConditionalHandle line) {
+                               cudaGraphConditionalHandle line, float *acc_best, const float *acc_grad,
+                               long long acc_n) {
     const int rpc = (nmi->fb + FIN_CLUSTER - 1) / FIN_CLUSTER;
     const size_t smem = (size_t)(2 * rpc + 2) * nmi->rb * sizeof(double);
     NRB_CUDA(cudaFuncSetAttribute(k_nmi_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     KernelTimer timer(TK_FINALIZE, (double)nmi->rb * nmi->fb * 8 + (double)nmi->total * 16, st);
     NRB_CUDA(launch_pdl(ctl != nullptr, k_nmi_finalize, dim3(FIN_CLUSTER), dim3(FIN_CTA_THREADS), smem, st, nmi->rb,
                         nmi->fb, nmi->hist, nmi->pro, nmi->logt, nmi->last, nmi->pro2, nmi->logt2, nmi->last2,
-                        be_partials, n_be_partials, (double)cpp_nvox3, sim_weight, be_weight, obj, ctl, line));
+                        be_partials, n_be_partials, (double)cpp_nvox3, sim_weight, be_weight, obj, ctl, line,
+                        acc_best, acc_grad, acc_n));
     NRB_LAUNCHED("k_nmi_finalize");
     return NRB_OK;
 }
