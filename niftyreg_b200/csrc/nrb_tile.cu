@@ -19,8 +19,6 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
-#include <map>
-#include <mutex>
 
 #include "nrb_state.cuh"
 
