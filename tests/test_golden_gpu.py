@@ -1,7 +1,7 @@
 """The CUDA path, through the C ABI, against the golden fixtures that NiftyReg's own CPU code
 produced (tests/golden/make_golden.py). Each step is fed the reference's inputs for that step.
 
-Tolerances: deformation field within 1e-4 voxel (north-star bar); warped intensities and
+Tolerances: deformation field within 1e-4 voxel; warped intensities and
 spatial gradients within 1e-4 on [2, bins-3]-scaled images with identical NaN patterns; NMI
 within 1e-10 relative and tables within 1e-10 relative (integer counts, FP64 tables); voxel
 gradient within 1e-5 of its largest magnitude; one-axis convolutions within 1e-5 of the largest
