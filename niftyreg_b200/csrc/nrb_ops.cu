@@ -766,10 +766,12 @@ static nrb_status upload(T *&dst, const std::vector<T>& src, size_t& bytes, cuda
 
 // Items of the voxel walk. The persistent grid holds slots_for(shared bytes) co-resident blocks
 // and every block walks ceil(items / slots) items, so the z-chunk count is chosen to minimise a
-// block's walk: rounds x (slices per chunk + a staging overhead of about four slices), over
-// chunk counts that keep chunks at least 8 slices long (the staged control points are reused
-// along z).
-WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t smem), size_t extra_smem) {
+// block's walk: rounds x (slices per chunk + the item's fixed cost, `overhead` slices: staging,
+// the x rows, the column set-up), over chunk counts that keep chunks at least `min_chunk`
+// slices long (the staged control points are reused along z). Small volumes, whose few long
+// items would leave most blocks idle, get shorter chunks spread over more blocks.
+WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t smem), size_t extra_smem,
+                   int min_chunk, int overhead) {
     WalkPlan p;
     p.ty = ty;
     const int nx = g->ref_dim[0], ny = g->ref_dim[1], nz = g->ref_dim[2];
@@ -782,7 +784,7 @@ WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t 
     p.sb = tile_span(ny, ty, gs[1]);
     long long best_cost = LLONG_MAX;
     WalkPlan best = p;
-    for (int c = 1; c <= std::max(1, nz / 8); ++c) {
+    for (int c = 1; c <= std::max(1, nz / min_chunk); ++c) {
         WalkPlan q = p;
         q.zchunk = (nz + c - 1) / c;
         q.nchunks = (nz + q.zchunk - 1) / q.zchunk;
@@ -791,7 +793,7 @@ WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t 
         q.cp_floats = 3 * q.sa * q.sb * q.sc;
         const long long slots = std::max(1LL, slots_for(walk_smem_bytes(q) + extra_smem));
         const long long rounds = (q.nitems + slots - 1) / slots;
-        const long long cost = rounds * (q.zchunk + 4);
+        const long long cost = rounds * (q.zchunk + overhead);
         if (cost < best_cost) {
             best_cost = cost;
             best = q;
@@ -804,8 +806,8 @@ nrb_status workspace_init(nrb_workspace *ws, const nrb_geometry *g) {
     ws->g = *g;
     // shared memory beyond the walk: the 64-bin joint histogram / FP32 log table (the plan is
     // made before the bin count is known; other bin counts shift occupancy little)
-    ws->walk_obj = plan_walk(g, TY_OBJECTIVE, objective_slots, (size_t)68 * 68 * 4);
-    ws->walk_grad = plan_walk(g, TY_GRADIENT, gradient_slots, (size_t)(68 * 68 + 136) * 4);
+    ws->walk_obj = plan_walk(g, TY_OBJECTIVE, objective_slots, (size_t)68 * 68 * 4, 4, 6);
+    ws->walk_grad = plan_walk(g, TY_GRADIENT, gradient_slots, (size_t)(68 * 68 + 136) * 4, 4, 4);
     return NRB_OK;
 }
 

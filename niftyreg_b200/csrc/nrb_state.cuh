@@ -78,7 +78,8 @@ struct WalkPlan {
     int sa = 0, sb = 0, sc = 0;  // max control-point span of an item along x, y, z
     int cp_floats = 0;           // shared floats of the staged control-point block
 };
-WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t smem), size_t extra_smem);
+WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t smem), size_t extra_smem,
+                   int min_chunk = 8, int overhead = 4);
 size_t walk_smem_bytes(const WalkPlan& W);
 // co-resident blocks of the persistent voxel passes for a given dynamic shared-memory size
 long long objective_slots(size_t smem);
