@@ -660,16 +660,21 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
                const float *__restrict__ acc_grad, long long acc_n) {
     pdl_wait();  // the counts come from the objective pass
     cg::cluster_group cluster = cg::this_cluster();
-    // output table set: the one not holding the best position (read before thread 0 of block 0
-    // updates the state at the very end)
-    const bool second = ctl && ctl->best_buf == 0;
-    double *__restrict__ pro = second ? pro1 : pro0;
-    double *__restrict__ logt = second ? logt1 : logt0;
-    nrb_objective *__restrict__ last = second ? last1 : last0;
     extern __shared__ double sm[];
     __shared__ double red[3 * 32];
     __shared__ double part[4];  // this block's partial mass, H_ref, H_war, H_joint
+    __shared__ OptState sctl;   // this block's copy of the optimiser state
+    __shared__ double s_mgl[2];
     const int tid = threadIdx.x, c = (int)cluster.block_rank();
+    // everything the end of the kernel needs from global memory is read now, beside the counts:
+    // the optimiser state, the gradient lengths of both table sets, the bending-energy partials
+    if (tid == 0) {
+        if (ctl) sctl = *ctl;
+        s_mgl[0] = last0->max_grad_len;
+        s_mgl[1] = last1->max_grad_len;
+    }
+    double be = 0.0;
+    for (int i = tid; i < n_be; i += FIN_CTA_THREADS) be += be_partials[i];
     const int nj = rb * fb;
     const int rpc = (fb + FIN_CLUSTER - 1) / FIN_CLUSTER;
     const int f0 = min(fb, c * rpc), f1 = min(fb, f0 + rpc), nrow = f1 - f0;
@@ -687,8 +692,13 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
         U[(f - f0 + 1) * rb + r] = smooth3(r > 0, l, m, r + 1 < rb, rr, k0, k1);
     }
     __syncthreads();
+    // output table set: the one not holding the best position
+    const bool second = ctl && sctl.best_buf == 0;
+    double *__restrict__ pro = second ? pro1 : pro0;
+    double *__restrict__ logt = second ? logt1 : logt0;
+    nrb_objective *__restrict__ last = second ? last1 : last0;
     // smoothing along the floating axis of the own rows
-    double mass = 0.0, z1 = 0.0, z2 = 0.0;
+    double mass = 0.0, z2 = 0.0;
     for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) {
         const int f = f0 + i / rb;
         const double *u = U + (i / rb + 1) * rb + i % rb;
@@ -696,7 +706,8 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
         T[i] = v;
         mass += v;
     }
-    block_sum3w<FIN_WARPS>(mass, z1, z2, red);
+    // the bending-energy sum: the same partition and tree in every block, so the same value
+    block_sum3w<FIN_WARPS>(mass, be, z2, red);
     if (tid == 0) part[0] = mass;
     cluster.sync();  // every block has read its halo counts; partial masses visible
     for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) hist[(size_t)f0 * rb + i] = 0u;  // next evaluation
@@ -780,50 +791,55 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
         part[3] = hj;
     }
     cluster.sync();
-    if (c == 0) {
-        double be = 0.0, d1 = 0.0, d2 = 0.0;
-        for (int i = tid; i < n_be; i += FIN_CTA_THREADS) be += be_partials[i];
-        block_sum3w<FIN_WARPS>(be, d1, d2, red);
-        if (tid == 0) {
-            double hq[FIN_CLUSTER][3];
+    if (tid == 0) {
+        double hq[FIN_CLUSTER][3];
 #pragma unroll
-            for (int q = 0; q < FIN_CLUSTER; ++q) {
-                const double *pq = cluster.map_shared_rank(part, q);
-                hq[q][0] = pq[1];
-                hq[q][1] = pq[2];
-                hq[q][2] = pq[3];
-            }
-            double h[3] = { 0.0, 0.0, 0.0 };
+        for (int q = 0; q < FIN_CLUSTER; ++q) {
+            const double *pq = cluster.map_shared_rank(part, q);
+            hq[q][0] = pq[1];
+            hq[q][1] = pq[2];
+            hq[q][2] = pq[3];
+        }
+        double h[3] = { 0.0, 0.0, 0.0 };
 #pragma unroll
-            for (int q = 0; q < FIN_CLUSTER; ++q) {
-                h[0] += hq[q][0];
-                h[1] += hq[q][1];
-                h[2] += hq[q][2];
-            }
-            nrb_objective o;
-            // with a zero similarity weight the reference never evaluates the measure
-            // (_reg_f3d.cpp:450-454): its weighted term is 0, not 0 * NaN
-            o.nmi = sim_weight > 0 ? (h[0] + h[1]) / h[2] : 0.0;
-            o.entropy[0] = h[0];
-            o.entropy[1] = h[1];
-            o.entropy[2] = h[2];
-            o.entropy[3] = total;
-            o.be = n_be > 0 ? be / be_norm : 0.0;
-            o.objective = (sim_weight > 0 ? sim_weight * o.nmi : 0.0) - (be_weight > 0 ? be_weight * o.be : 0.0);
-            o.max_grad_len = last->max_grad_len;
+        for (int q = 0; q < FIN_CLUSTER; ++q) {
+            h[0] += hq[q][0];
+            h[1] += hq[q][1];
+            h[2] += hq[q][2];
+        }
+        nrb_objective o;
+        // with a zero similarity weight the reference never evaluates the measure
+        // (_reg_f3d.cpp:450-454): its weighted term is 0, not 0 * NaN
+        o.nmi = sim_weight > 0 ? (h[0] + h[1]) / h[2] : 0.0;
+        o.entropy[0] = h[0];
+        o.entropy[1] = h[1];
+        o.entropy[2] = h[2];
+        o.entropy[3] = total;
+        o.be = n_be > 0 ? be / be_norm : 0.0;
+        o.objective = (sim_weight > 0 ? sim_weight * o.nmi : 0.0) - (be_weight > 0 ? be_weight * o.be : 0.0);
+        o.max_grad_len = s_mgl[second ? 1 : 0];
+        // every block takes the same step on its own copy of the state; block 0 publishes it
+        const bool more = ctl ? line_step(&sctl, o.nmi, o.be, sim_weight, be_weight) : false;
+        if (c == 0) {
             *last = o;
             if (obj) *obj = o;
-            if (ctl) cudaGraphSetConditional(line, line_step(ctl, o.nmi, o.be, sim_weight, be_weight) ? 1u : 0u);
+            if (ctl) {
+                *ctl = sctl;
+                cudaGraphSetConditional(line, more ? 1u : 0u);
+            }
         }
     }
-    cluster.sync();  // every block's shared memory stays alive until block 0 has read it
+    // this block has read the others' shared memory: they may exit once every block arrived
+    auto token = cluster.barrier_arrive();
+    __syncthreads();  // the decision in sctl
     // small grids: the store of an accepted trial position (k_accept's operations) in the same
-    // launch; the decision written by block 0 above is visible to the cluster after the barrier
-    if (acc_n > 0 && ctl->accepted) {
-        const float scale = -ctl->step_len;
+    // launch
+    if (ctl && acc_n > 0 && sctl.accepted) {
+        const float scale = -sctl.step_len;
         for (long long i = (long long)c * FIN_CTA_THREADS + tid; i < acc_n; i += (long long)FIN_CLUSTER * FIN_CTA_THREADS)
             acc_best[i] = __fadd_rn(acc_best[i], __fmul_rn(scale, acc_grad[i]));
     }
+    cluster.barrier_wait(std::move(token));
 }
 
 // ---------------------------------------------------------------------------------------------
