@@ -248,6 +248,11 @@ typedef struct nrb_f3d_params {
                                * with the optimiser state on the device; 1: the host takes every
                                * line-search branch (one synchronising read per evaluation).
                                * Both take the same steps. Per-kernel timing forces 1. */
+    int32_t floating_margin;  /* voxels of the padding value laid around each level's floating
+                               * image in a padded device copy (default 8, at most 64; 0: no
+                               * copy). Samples that reach into the margin take the kernels'
+                               * plain load path instead of the clamped one; the results are the
+                               * same bit for bit. */
 } nrb_f3d_params;
 
 typedef struct nrb_f3d_result {

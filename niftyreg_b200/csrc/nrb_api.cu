@@ -246,13 +246,12 @@ static nrb_status check_fused_args(nrb_workspace *ws, nrb_nmi *nmi, const nrb_ge
     return NRB_OK;
 }
 
-extern "C" nrb_status nrb_f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
-                                        const float *ref, const float *flo, const int32_t *mask,
-                                        const float *cpp, float padding, double sim_weight,
-                                        double be_weight, nrb_objective *obj, nrb_objective *obj_host,
-                                        void *stream) {
-    NRB_TRY(check_fused_args(ws, nmi, g, ref, flo, cpp));
-    cudaStream_t st = as_stream(stream);
+namespace nrb {
+
+nrb_status f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g, const float *ref,
+                         const float *flo, int flo_margin, const int32_t *mask, const float *cpp, float padding,
+                         double sim_weight, double be_weight, nrb_objective *obj, nrb_objective *obj_host,
+                         cudaStream_t st) {
     int n_be = 0;
     const bool overlap = be_weight > 0 && sim_weight > 0;
     if (be_weight > 0) {
@@ -261,7 +260,8 @@ extern "C" nrb_status nrb_f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const n
         NRB_TRY(launch_be_value(ws, g, cpp, overlap ? ws->side : st));
         n_be = be_partial_count(g);
     }
-    if (sim_weight > 0) NRB_TRY(launch_fused_objective(ws, nmi, g, ref, flo, mask, cpp, padding, st));
+    if (sim_weight > 0)
+        NRB_TRY(launch_fused_objective(ws, nmi, g, ref, flo, mask, cpp, padding, st, nullptr, nullptr, flo_margin));
     if (overlap) NRB_TRY(join_side(ws, st));
     NRB_TRY(launch_nmi_finalize(nmi, ws->be_partials, n_be, 3 * nvox(g->cpp_dim), sim_weight, be_weight, obj, st));
     if (obj_host) {
@@ -271,13 +271,9 @@ extern "C" nrb_status nrb_f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const n
     return NRB_OK;
 }
 
-extern "C" nrb_status nrb_f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
-                                       const float *ref, const float *flo, const int32_t *mask,
-                                       const float *cpp, float padding, double sim_weight,
-                                       double be_weight, float *vgrad, float *node_grad, void *stream) {
-    NRB_TRY(check_fused_args(ws, nmi, g, ref, flo, cpp));
-    if (!vgrad || !node_grad) return fail(NRB_ERR_INVALID, "nrb_f3d_gradient: null buffer");
-    cudaStream_t st = as_stream(stream);
+nrb_status f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g, const float *ref,
+                        const float *flo, int flo_margin, const int32_t *mask, const float *cpp, float padding,
+                        double sim_weight, double be_weight, float *vgrad, float *node_grad, cudaStream_t st) {
     const bool overlap = be_weight > 0 && sim_weight > 0;
     if (overlap) {
         // the bending-energy derivatives read only the grid: they run beside the voxel passes
@@ -286,9 +282,9 @@ extern "C" nrb_status nrb_f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nr
     }
     if (sim_weight > 0) {
         // the histogram of the current position feeds the log table of the voxel gradient
-        NRB_TRY(launch_fused_objective(ws, nmi, g, ref, flo, mask, cpp, padding, st));
+        NRB_TRY(launch_fused_objective(ws, nmi, g, ref, flo, mask, cpp, padding, st, nullptr, nullptr, flo_margin));
         NRB_TRY(launch_nmi_finalize(nmi, nullptr, 0, 3 * nvox(g->cpp_dim), sim_weight, 0.0, nullptr, st));
-        NRB_TRY(launch_fused_gradient(ws, nmi, g, ref, flo, mask, cpp, padding, 1.0, vgrad, st));
+        NRB_TRY(launch_fused_gradient(ws, nmi, g, ref, flo, mask, cpp, padding, 1.0, vgrad, st, nullptr, flo_margin));
         NRB_TRY(launch_convolve_to_nodes(ws, g, vgrad, (float)sim_weight, node_grad, st));
     } else {
         NRB_CUDA(cudaMemsetAsync(node_grad, 0, 3 * nvox(g->cpp_dim) * sizeof(float), st));
@@ -299,4 +295,26 @@ extern "C" nrb_status nrb_f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nr
         NRB_TRY(launch_be_accumulate(ws, g, (float)be_weight, node_grad, st));
     }
     return NRB_OK;
+}
+
+}  // namespace nrb
+
+extern "C" nrb_status nrb_f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
+                                        const float *ref, const float *flo, const int32_t *mask,
+                                        const float *cpp, float padding, double sim_weight,
+                                        double be_weight, nrb_objective *obj, nrb_objective *obj_host,
+                                        void *stream) {
+    NRB_TRY(check_fused_args(ws, nmi, g, ref, flo, cpp));
+    return f3d_objective(ws, nmi, g, ref, flo, 0, mask, cpp, padding, sim_weight, be_weight, obj, obj_host,
+                         as_stream(stream));
+}
+
+extern "C" nrb_status nrb_f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
+                                       const float *ref, const float *flo, const int32_t *mask,
+                                       const float *cpp, float padding, double sim_weight,
+                                       double be_weight, float *vgrad, float *node_grad, void *stream) {
+    NRB_TRY(check_fused_args(ws, nmi, g, ref, flo, cpp));
+    if (!vgrad || !node_grad) return fail(NRB_ERR_INVALID, "nrb_f3d_gradient: null buffer");
+    return f3d_gradient(ws, nmi, g, ref, flo, 0, mask, cpp, padding, sim_weight, be_weight, vgrad, node_grad,
+                        as_stream(stream));
 }

@@ -217,6 +217,32 @@ int elementwise_grid(long long n) {
     return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 4LL * 148));
 }
 
+// dst = the dense [nz][ny][nx] volume src in the middle of a [nz+2m][ny+2m][nx+2m] one whose
+// margin holds `value`
+__global__ void k_pad_volume(const float *__restrict__ src, int nx, int ny, int nz, int m, float value,
+                             float *__restrict__ dst) {
+    const int px = nx + 2 * m, py = ny + 2 * m;
+    const long long n = (long long)px * py * (nz + 2 * m);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % px) - m;
+        const long long r = i / px;
+        const int y = (int)(r % py) - m;
+        const int z = (int)(r / py) - m;
+        const bool in = x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz;
+        dst[i] = in ? src[((long long)z * ny + y) * nx + x] : value;
+    }
+}
+
+nrb_status pad_volume(const float *src, const int32_t dim[3], int margin, float value, float *dst,
+                      const float **origin, cudaStream_t st) {
+    k_pad_volume<<<elementwise_grid(padded_voxels(dim, margin)), 256, 0, st>>>(src, dim[0], dim[1], dim[2], margin,
+                                                                              value, dst);
+    NRB_LAUNCHED("k_pad_volume");
+    *origin = dst + ((long long)margin * (dim[1] + 2 * margin) + margin) * (dim[0] + 2 * margin) + margin;
+    return NRB_OK;
+}
+
 struct GraphHolder {
     cudaGraph_t g = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -321,8 +347,8 @@ private:
     // reg_f3d::GetObjectiveFunctionValue (_reg_f3d.cpp:443-462)
     nrb_status GetObjectiveFunctionValue(double& value) {
         nrb_objective o;
-        NRB_TRY(nrb_f3d_objective(ws_.h, nmi_.h, &g_, ref_.p, flo_.p, nullptr, cur_.p, pad_, sim_w_, be_w_,
-                                  obj_, &o, st_));
+        NRB_TRY(f3d_objective(ws_.h, nmi_.h, &g_, ref_.p, flo_org_, margin_, nullptr, cur_.p, pad_, sim_w_, be_w_,
+                              obj_, &o, st_));
         cur_w_measure_ = sim_w_ > 0 ? (double)sim_w_ * o.nmi : 0.0;
         cur_w_be_ = be_w_ > 0 ? (double)be_w_ * o.be : 0.0;
         cur_nmi_ = o.nmi;
@@ -333,8 +359,8 @@ private:
     }
     // reg_f3d::GetObjectiveFunctionGradient (_reg_f3d.cpp:553-576) + NormaliseGradient (:395-410)
     nrb_status GetObjectiveFunctionGradient() {
-        NRB_TRY(nrb_f3d_gradient(ws_.h, nmi_.h, &g_, ref_.p, flo_.p, nullptr, cur_.p, pad_, sim_w_, be_w_, vgrad_.p,
-                                 grad_.p, st_));
+        NRB_TRY(f3d_gradient(ws_.h, nmi_.h, &g_, ref_.p, flo_org_, margin_, nullptr, cur_.p, pad_, sim_w_, be_w_,
+                             vgrad_.p, grad_.p, st_));
         ++it_;
         ++n_grad_;
         return max_and_normalise(ws_.h, grad_.p, nc_, obj_, st_);
@@ -422,6 +448,11 @@ private:
     // current level
     nrb_geometry g_{};
     DevBuf ref_, flo_, vgrad_, grad_, best_, g1_, g2_, cur_;
+    // the floating image as the voxel passes read it: flo_org_ is its voxel (0, 0, 0), inside
+    // flo_pad_ (a copy with margin_ voxels of padding values on every side) or flo_ (margin 0)
+    DevBuf flo_pad_;
+    const float *flo_org_ = nullptr;
+    int margin_ = 0;
     NmiHandle nmi_;
     WsHandle ws_;
     nrb_objective *obj_ = nullptr;
@@ -464,7 +495,8 @@ nrb_status F3dRegistration::CaptureGradient(cudaStream_t cs) {
         NRB_TRY(fork_side(ws, cs));
         NRB_TRY(launch_be_derivatives(ws, &g_, best_.p, ws->side));
     }
-    NRB_TRY(launch_fused_gradient(ws, nmi_.h, &g_, ref_.p, flo_.p, nullptr, best_.p, pad_, 1.0, vgrad_.p, cs, dstate_));
+    NRB_TRY(launch_fused_gradient(ws, nmi_.h, &g_, ref_.p, flo_org_, nullptr, best_.p, pad_, 1.0, vgrad_.p, cs, dstate_,
+                                  margin_));
     NRB_TRY(launch_convolve_to_nodes(ws, &g_, vgrad_.p, sim_w_, grad_.p, cs));
     if (be) {
         NRB_TRY(join_side(ws, cs));
@@ -485,7 +517,8 @@ nrb_status F3dRegistration::CaptureLineStep(cudaStream_t cs, cudaGraphConditiona
         NRB_TRY(launch_be_value(ws, &g_, best_.p, ws->side, grad_.p, dstate_));
         n_be = be_partial_count(&g_);
     }
-    NRB_TRY(launch_fused_objective(ws, nmi_.h, &g_, ref_.p, flo_.p, nullptr, best_.p, pad_, cs, grad_.p, dstate_));
+    NRB_TRY(launch_fused_objective(ws, nmi_.h, &g_, ref_.p, flo_org_, nullptr, best_.p, pad_, cs, grad_.p, dstate_,
+                                   margin_));
     if (be_w_ > 0) NRB_TRY(join_side(ws, cs));
     const long long n = 3 * nc_;
     // small grids: the finalize also stores an accepted trial position (one launch fewer per
@@ -748,6 +781,17 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
     // reg_nmi::InitialiseMeasure: rescale both images to [2, bins - 3]
     NRB_TRY(rescale_with(ref_.p, r.n(), 2.f, (float)(p_.ref_bins + 4) - 3.f, ws_.h->fred, st_));
     NRB_TRY(rescale_with(flo_.p, r.n(), 2.f, (float)(p_.flo_bins + 4) - 3.f, ws_.h->fred, st_));
+    // the floating image with a margin of padding values, which the voxel passes sample without
+    // clamping; the dense copy is released
+    margin_ = p_.floating_margin;
+    if (margin_ > 0) {
+        NRB_TRY(flo_pad_.alloc(padded_voxels(r.dim, margin_), st_));
+        NRB_TRY(pad_volume(flo_.p, r.dim, margin_, pad_, flo_pad_.p, &flo_org_, st_));
+        dev_free(flo_.p, flo_.st);
+        flo_.p = nullptr;
+    } else {
+        flo_org_ = flo_.p;
+    }
     // ConjugateGradient::Initialise: best = current, objective at the starting point
     it_ = 0;
     first_call_ = true;
@@ -764,6 +808,8 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const int32_
     levels_ = p_.levels;
     if (levels_ < 1) return fail(NRB_ERR_INVALID, "registration: levels must be >= 1");
     if (p_.ref_bins < 1 || p_.flo_bins < 1) return fail(NRB_ERR_INVALID, "registration: bins must be >= 1");
+    if (p_.floating_margin < 0 || p_.floating_margin > 64)
+        return fail(NRB_ERR_INVALID, "registration: floating_margin must be in [0, 64]");
     pad_ = p_.padding;
     // reg_f3d::CheckParameters (_reg_f3d.cpp:142-158): weights normalised by the penalty sum
     be_w_ = p_.bending_energy;
@@ -899,7 +945,8 @@ int64_t registration_footprint(const int32_t dim[3], const float pixdim[3], cons
         nodes *= (int64_t)ceil_ref((float)dim[i] * pixdim[i] / mm + 3.f);
     }
     const int64_t build = 16 * fine;
-    const int64_t level = 12 * fine + 24 * fine + (6 * 12 + 72) * nodes;
+    const int margin = std::min(64, std::max(0, (int)p->floating_margin));
+    const int64_t level = 12 * fine + 24 * fine + (6 * 12 + 72) * nodes + 4 * padded_voxels(dim, margin);
     return pyramid + std::max(build, level) + (4 << 20);
 }
 }  // namespace nrb
@@ -919,6 +966,7 @@ extern "C" void nrb_f3d_default_params(nrb_f3d_params *p) {
     p->padding = std::numeric_limits<float>::quiet_NaN();
     p->verbose = 0;
     p->host_loop = 0;
+    p->floating_margin = 8;
 }
 
 extern "C" nrb_status nrb_f3d_grid_dims(const int32_t ref_dim[3], const float ref_pixdim[3], const nrb_f3d_params *p,

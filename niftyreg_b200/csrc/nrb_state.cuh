@@ -161,15 +161,33 @@ nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be
                                cudaGraphConditionalHandle line = 0, float *acc_best = nullptr,
                                const float *acc_grad = nullptr, long long acc_n = 0);
 // grad/step (optional): evaluate at the line search's trial position cpp - step->cur_len * grad
+// flo_margin > 0: `flo` is the voxel (0, 0, 0) of a copy made by pad_volume with that margin
 nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                   const float *ref, const float *flo, const int32_t *mask,
                                   const float *cpp, float padding, cudaStream_t st,
-                                  const float *grad = nullptr, const OptState *step = nullptr);
+                                  const float *grad = nullptr, const OptState *step = nullptr,
+                                  int flo_margin = 0);
 // sel (optional, inside a level graph): read the NMI table set sel->best_buf
 nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                  const float *ref, const float *flo, const int32_t *mask,
                                  const float *cpp, float padding, double weight, float *vgrad,
-                                 cudaStream_t st, const OptState *sel = nullptr);
+                                 cudaStream_t st, const OptState *sel = nullptr, int flo_margin = 0);
+// Copy of a dense [nz][ny][nx] volume with `margin` voxels of `value` added on every side
+// (dst: (nx + 2m) (ny + 2m) (nz + 2m) floats); returns in *origin the copy's voxel (0, 0, 0).
+nrb_status pad_volume(const float *src, const int32_t dim[3], int margin, float value, float *dst,
+                      const float **origin, cudaStream_t st);
+inline long long padded_voxels(const int32_t dim[3], int margin) {
+    return (long long)(dim[0] + 2 * margin) * (dim[1] + 2 * margin) * (dim[2] + 2 * margin);
+}
+// the fused evaluations of nrb_f3d_objective / nrb_f3d_gradient on a floating image laid out
+// with `flo_margin` (0: the dense volume of the public entry points)
+nrb_status f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g, const float *ref,
+                         const float *flo, int flo_margin, const int32_t *mask, const float *cpp, float padding,
+                         double sim_weight, double be_weight, nrb_objective *obj, nrb_objective *obj_host,
+                         cudaStream_t st);
+nrb_status f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g, const float *ref,
+                        const float *flo, int flo_margin, const int32_t *mask, const float *cpp, float padding,
+                        double sim_weight, double be_weight, float *vgrad, float *node_grad, cudaStream_t st);
 nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float *cpp,
                            cudaStream_t st, const float *grad = nullptr, const OptState *step = nullptr);
 nrb_status launch_be_derivatives(nrb_workspace *ws, const nrb_geometry *g, const float *cpp, cudaStream_t st);

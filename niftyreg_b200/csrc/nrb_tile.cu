@@ -33,6 +33,7 @@ struct WalkParams {
     int ty, tiles_x, tiles_y, zchunk, nitems;
     int sa, sb, sc;          // shared strides of the staged block (max spans)
     int fnx, fny, fnz;       // floating dims
+    int fsy, fsz, fmargin;   // floating layout: row and slice strides, margin (sample_floating)
     Mat34 flo_ijk;           // mm -> floating voxel
     int flo_diag;            // flo_ijk has no off-diagonal terms
     float pad;               // padding value of out-of-volume taps
@@ -261,13 +262,20 @@ __device__ __forceinline__ int trunc_nonneg(float v) { return __float2int_rz(v);
 // Trilinear sample of the floating image at world position (x, y, z) with the padding rule of
 // ResampleImage3D (an out-of-volume tap contributes padding * weight, so NaN padding poisons a
 // border voxel even through a zero weight) and, when kGrad, the spatial derivative of
-// TrilinearImageGradient (NaN components -> 0). Warps whose 32 samples are all interior take
-// the plain 8-load path; otherwise every lane reads clamped in-bounds addresses and selects the
-// padding value for out-of-volume taps, with no divergence.
+// TrilinearImageGradient (NaN components -> 0).
+//
+// Layout: `flo` points at voxel (0, 0, 0), rows are `sy` and slices `sz` floats apart, and
+// `margin` voxels holding the padding value surround the volume on every side (0: a dense
+// volume). Warps whose 32 samples have all eight taps inside the volume or its margin take the
+// plain 8-load path: a tap in the margin reads the padding value from memory, the very value
+// the clamped path substitutes, so the two paths give the same numbers. Other warps read
+// clamped in-volume addresses and select the padding value for out-of-volume taps, with no
+// divergence.
 template <bool kGrad>
 __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, int fnx, int fny,
-                                                int fnz, const Mat34& M, int diag, float pad, float x,
-                                                float y, float z, float& val, float g[3]) {
+                                                int fnz, int sy, int sz, int margin, const Mat34& M,
+                                                int diag, float pad, float x, float y, float z,
+                                                float& val, float g[3]) {
     float fx, fy, fz;
     to_floating_voxel(M, diag, x, y, z, fx, fy, fz);
     float flx, fly, flz;
@@ -275,10 +283,12 @@ __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, i
     const float rx = fx - flx, ry = fy - fly, rz = fz - flz;
     const float bx0 = 1.f - rx, by0 = 1.f - ry, bz0 = 1.f - rz;
     float v[2][2][2];
-    const bool interior = px >= 0 && py >= 0 && pz >= 0 && px + 1 < fnx && py + 1 < fny && pz + 1 < fnz;
-    const int sy = fnx, sz = fnx * fny;
-    if (__all_sync(__activemask(), interior)) {
-        const float *p = flo + (pz * fny + py) * fnx + px;
+    // -margin <= p and p + 1 <= n - 1 + margin on every axis (|p| <= 2^21: no overflow)
+    const bool plain = (unsigned)(px + margin) < (unsigned)(fnx + 2 * margin - 1) &&
+                       (unsigned)(py + margin) < (unsigned)(fny + 2 * margin - 1) &&
+                       (unsigned)(pz + margin) < (unsigned)(fnz + 2 * margin - 1);
+    if (__all_sync(__activemask(), plain)) {
+        const float *p = flo + (pz * sz + py * sy + px);
         v[0][0][0] = __ldg(p);
         v[0][0][1] = __ldg(p + 1);
         v[0][1][0] = __ldg(p + sy);
@@ -389,8 +399,8 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
                     const int vi = idx + u * zstride;
                     if (mask == nullptr || __ldg(&mask[vi]) > -1) {
                         float w, g[3];
-                        sample_floating<false>(flo, P.fnx, P.fny, P.fnz, P.flo_ijk, P.flo_diag, P.pad, pos[0], pos[1],
-                                               pos[2], w, g);
+                        sample_floating<false>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin, P.flo_ijk,
+                                               P.flo_diag, P.pad, pos[0], pos[1], pos[2], w, g);
                         const float rv = __ldg(&ref[vi]);
                         if (rv == rv && w == w && 0.f <= rv && rv < frb && 0.f <= w && w < ffb)
                             bin[u] = trunc_nonneg(rv) + trunc_nonneg(w) * P.rb;
@@ -539,8 +549,8 @@ k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict_
             float out[3] = { 0.f, 0.f, 0.f };
             if (mask == nullptr || __ldg(&mask[idx]) > -1) {
                 float w, g[3];
-                sample_floating<true>(flo, P.fnx, P.fny, P.fnz, P.flo_ijk, P.flo_diag, P.pad, pos[0], pos[1], pos[2],
-                                      w, g);
+                sample_floating<true>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin, P.flo_ijk, P.flo_diag,
+                                      P.pad, pos[0], pos[1], pos[2], w, g);
                 const float rv = __ldg(&ref[idx]);
                 if (rv == rv && w == w) {
                     if (kF32) {
@@ -855,7 +865,8 @@ __global__ void k_resample(long long nv, int fnx, int fny, int fnz, Mat34 M, int
         if (!kGrad && !active) continue;
         float w = 0.f, g[3] = { 0.f, 0.f, 0.f };
         if (active)
-            sample_floating<kGrad>(flo, fnx, fny, fnz, M, diag, pad, def[i], def[nv + i], def[2 * nv + i], w, g);
+            sample_floating<kGrad>(flo, fnx, fny, fnz, fnx, fnx * fny, 0, M, diag, pad, def[i], def[nv + i],
+                                   def[2 * nv + i], w, g);
         if (kGrad) {
             out[i] = g[0];
             out[nv + i] = g[1];
@@ -932,6 +943,9 @@ static WalkParams make_params(const WalkPlan& W, const nrb_geometry *g, float pa
     P.fnx = g->flo_dim[0];
     P.fny = g->flo_dim[1];
     P.fnz = g->flo_dim[2];
+    P.fsy = P.fnx;
+    P.fsz = P.fnx * P.fny;
+    P.fmargin = 0;
     P.flo_ijk = to_mat34(g->flo_ijk);
     P.pad = pad;
     P.rb = rb;
@@ -942,6 +956,14 @@ static WalkParams make_params(const WalkPlan& W, const nrb_geometry *g, float pa
     P.log_in_smem = 0;
     P.xs = 0;
     return P;
+}
+
+// a floating image laid out by pad_volume with `margin` voxels on every side, passed as the
+// pointer to its voxel (0, 0, 0)
+static void set_floating_margin(WalkParams& P, int margin) {
+    P.fmargin = margin;
+    P.fsy = P.fnx + 2 * margin;
+    P.fsz = P.fsy * (P.fny + 2 * margin);
 }
 
 template <typename K>
@@ -978,8 +1000,9 @@ long long deformation_slots(size_t smem) { return blocks_resident(k_deformation,
 nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                   const float *ref, const float *flo, const int32_t *mask,
                                   const float *cpp, float padding, cudaStream_t st,
-                                  const float *grad, const OptState *step) {
+                                  const float *grad, const OptState *step, int flo_margin) {
     WalkParams P = make_params(ws->walk_obj, g, padding, nmi->rb, nmi->fb);
+    set_floating_margin(P, flo_margin);
     const size_t base_smem = walk_smem_bytes(ws->walk_obj) + (size_t)((nmi->rb * nmi->fb + 3) & ~3) * 4;
     const size_t xs_bytes = (size_t)3 * P.sc * P.sb * 32 * 4;
     // the x-contracted rows when two blocks per SM still fit
@@ -1007,8 +1030,9 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
 nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                  const float *ref, const float *flo, const int32_t *mask,
                                  const float *cpp, float padding, double weight, float *vgrad,
-                                 cudaStream_t st, const OptState *sel) {
+                                 cudaStream_t st, const OptState *sel, int flo_margin) {
     WalkParams P = make_params(ws->walk_grad, g, padding, nmi->rb, nmi->fb);
+    set_floating_margin(P, flo_margin);
     // an FP32 copy of the log table rides in shared memory when it fits (64 bins: 19 KB,
     // 128 bins: 70 KB); larger tables use the FP64 window on the global table
     const size_t log_bytes = (size_t)nmi->total * sizeof(float);

@@ -65,3 +65,9 @@ def test_footprint_is_host_only_and_monotone():
     for d, f in zip(sizes, fps):
         n = d[0] * d[1] * d[2]
         assert 8 * n < f < 80 * n + (8 << 20)
+    # the padded floating copy (4 bytes per voxel of the volume grown by the margin) is part of
+    # a level's working set
+    assert p.floating_margin == 8
+    d = (64, 64, 64)
+    p0 = nrb.default_params(levels=2, spacing=(-5.0,), floating_margin=0)
+    assert 0 < nrb.footprint(d, (1.0, 1.0, 1.0), p) - nrb.footprint(d, (1.0, 1.0, 1.0), p0) <= 4 * 80 ** 3

@@ -39,6 +39,21 @@ def test_graph_loop_takes_the_host_loop_steps(pair):
     assert np.array_equal(c_graph, c_host)
 
 
+@pytest.mark.parametrize("padding", [float("nan"), 0.0])
+def test_floating_margin_changes_nothing(pair, padding):
+    """The padded floating copy (samples in its margin take the plain load path) gives the same
+    registration, bit for bit, as the dense image with clamped border samples; a margin of 2
+    voxels mixes both paths inside one level."""
+    runs = [nrb.register_host(pair.reference, pair.floating, pair.pixdim,
+                              _params(floating_margin=m, padding=padding, host_loop=h))
+            for m, h in ((0, 1), (8, 0), (2, 0), (8, 1))]
+    c0, r0 = runs[0]
+    for c, r in runs[1:]:
+        assert r.objective_evaluations == r0.objective_evaluations
+        assert r.final_nmi == r0.final_nmi
+        assert np.array_equal(c, c0)
+
+
 def test_registration_repeatable(pair):
     a, ra = nrb.register_host(pair.reference, pair.floating, pair.pixdim, _params())
     b, rb = nrb.register_host(pair.reference, pair.floating, pair.pixdim, _params())
