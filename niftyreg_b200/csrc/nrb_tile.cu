@@ -482,17 +482,45 @@ __device__ __forceinline__ float nmi_window_f(float rv, float wv, const float *l
     //   sum_tu br_t dw_u rlog_t = (sum_t br_t rlog_t)(sum_u dw_u), and likewise for wlog
     float br[4], dw[4], rl[4], wl[4];
     int ri[4], wi[4];
+    if (rv >= 1.f && wv >= 1.f) {
+        // r0 + 1 = floor(rv): the four taps sit at rv - r = f + 1, f, f - 1, f - 2 (all exact)
+        // with f the fractional part, each inside one known piece of the kernel. The pieces
+        // parzenf / parzen_derivf would select are written out with their operations in their
+        // order (sign changes are exact), so every value is the same float; only |x| = 1 at
+        // f = 0 falls in the other piece and is given its value (1/6) explicitly.
+        const float f = rv - (float)(r0 + 1), mf = 1.f - f;
+        br[0] = mf * mf * mf * (1.f / 6.f);
+        br[1] = (2.0f / 3.0f) + (0.5f * f - 1.f) * f * f;
+        br[2] = mf < 1.f ? (2.0f / 3.0f) + (0.5f * mf - 1.f) * mf * mf : (1.f / 6.f);
+        br[3] = f * f * f * (1.f / 6.f);
+        const float g = wv - (float)(w0 + 1), mg = 1.f - g;
+        dw[0] = -0.5f * mg * mg;
+        dw[1] = (1.5f * g - 2.f) * g;
+        dw[2] = (1.5f * mg - 2.f) * -mg;
+        dw[3] = 0.5f * g * g;
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const int r = r0 + t, w = w0 + t;
-        const bool rok = r < r1 && -1 < r && r < rb;
-        const bool wok = w < w1 && -1 < w && w < fb;
-        ri[t] = min(max(r, 0), rb - 1);
-        wi[t] = min(max(w, 0), fb - 1) * rb;
-        br[t] = rok ? parzenf(rv - (float)r) : 0.f;
-        dw[t] = wok ? parzen_derivf(wv - (float)w) : 0.f;
-        rl[t] = rlog[ri[t]];
-        wl[t] = wlog[min(max(w, 0), fb - 1)];
+        for (int t = 0; t < 4; ++t) {
+            const int r = r0 + t, w = w0 + t;
+            if (!(r < rb)) br[t] = 0.f;
+            if (!(w < fb)) dw[t] = 0.f;
+            ri[t] = min(r, rb - 1);
+            wi[t] = min(w, fb - 1) * rb;
+            rl[t] = rlog[ri[t]];
+            wl[t] = wlog[min(w, fb - 1)];
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int r = r0 + t, w = w0 + t;
+            const bool rok = r < r1 && -1 < r && r < rb;
+            const bool wok = w < w1 && -1 < w && w < fb;
+            ri[t] = min(max(r, 0), rb - 1);
+            wi[t] = min(max(w, 0), fb - 1) * rb;
+            br[t] = rok ? parzenf(rv - (float)r) : 0.f;
+            dw[t] = wok ? parzen_derivf(wv - (float)w) : 0.f;
+            rl[t] = rlog[ri[t]];
+            wl[t] = wlog[min(max(w, 0), fb - 1)];
+        }
     }
     float sbr = 0.f, sdw = 0.f, sr = 0.f, sw = 0.f, sj = 0.f;
 #pragma unroll

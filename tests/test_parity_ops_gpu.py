@@ -183,6 +183,29 @@ def test_convolve_to_nodes(O, case):
     assert np.abs(host(node) - ref).max() <= 1e-5 * scale
 
 
+def test_convolve_to_nodes_nan_free_path_is_exact():
+    """The x pass sums NaN-free rows with a check-free loop and takes the per-tap path (conv_at)
+    for rows holding a NaN; both must give the same bits. A NaN at voxel (0, 3, 0) sends the
+    first block of rows (z = 0, y = 0..7) down the per-tap path; nodes beyond the kernel radius of
+    that voxel along x read those rows' x outputs through the y and z passes, so they must equal
+    the NaN-free run bit for bit."""
+    c = make_case(shape=(24, 24, 48), seed=31)
+    g = c.geometry()
+    rng = np.random.default_rng(31)
+    vgrad = rng.normal(0, 1e-3, 3 * c.nvox).astype(np.float32)
+    ws = nrb.Workspace(g)
+    a = torch.empty(3 * c.ncp, dtype=torch.float32, device="cuda")
+    b = torch.empty(3 * c.ncp, dtype=torch.float32, device="cuda")
+    nrb.convolve_voxel_based_gradient(ws, dev(vgrad), a, 0.995)
+    v2 = vgrad.copy()
+    v2[3 * 48] = np.nan  # component 0, z = 0, y = 3, x = 0
+    nrb.convolve_voxel_based_gradient(ws, dev(v2), b, 0.995)
+    cx, cy, cz = c.cdim
+    na, nb = host(a).reshape(3, cz, cy, cx), host(b).reshape(3, cz, cy, cx)
+    assert not np.array_equal(na[0, :, :, :3], nb[0, :, :, :3])  # the NaN changed the nodes near it
+    assert np.array_equal(na[..., 5:], nb[..., 5:])
+
+
 def test_bending_energy(O, case):
     c = case
     g = c.geometry()
