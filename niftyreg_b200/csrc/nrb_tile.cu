@@ -373,7 +373,8 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
     uint32_t *h = reinterpret_cast<uint32_t *>(S.tail);
     const int nbins = P.rb * P.fb;
     float *X = reinterpret_cast<float *>(h + ((nbins + 3) & ~3));  // x-contracted rows (P.xs)
-    for (int i = threadIdx.x; i < nbins; i += blockDim.x) h[i] = 0u;
+    // the histogram starts at 16 bytes (walk_smem): zeroed four bins at a time
+    for (int i = threadIdx.x; i < (nbins + 3) / 4; i += blockDim.x) reinterpret_cast<uint4 *>(h)[i] = make_uint4(0, 0, 0, 0);
     if (kTrial) pdl_wait();  // the trial position and step length come from the previous launch
     const float scale = kTrial ? -step->cur_len : 0.f;
     const int lane = threadIdx.x & 31;
@@ -423,7 +424,14 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
     // one atomic per non-zero bin of the block (merging the blocks of a cluster through
     // distributed shared memory first was measured slower at every volume size)
     __syncthreads();
-    for (int i = threadIdx.x; i < nbins; i += blockDim.x) {
+    for (int i = threadIdx.x; i < nbins / 4; i += blockDim.x) {
+        const uint4 c = reinterpret_cast<const uint4 *>(h)[i];
+        if (c.x) atomicAdd(&ghist[4 * i], c.x);
+        if (c.y) atomicAdd(&ghist[4 * i + 1], c.y);
+        if (c.z) atomicAdd(&ghist[4 * i + 2], c.z);
+        if (c.w) atomicAdd(&ghist[4 * i + 3], c.w);
+    }
+    for (int i = (nbins & ~3) + (int)threadIdx.x; i < nbins; i += blockDim.x) {
         const uint32_t c = h[i];
         if (c) atomicAdd(&ghist[i], c);
     }
