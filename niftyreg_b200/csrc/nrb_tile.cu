@@ -336,7 +336,7 @@ __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, i
     }
 }
 
-constexpr int WALK_GROUP = 2;  // slices per step of the walk: their gathers are in flight together
+constexpr int WALK_GROUP = 1;  // slices per step of the walk (two in flight measured 2% slower)
 
 // shared-memory layout of a walk block: cp block | z basis | z node index | kernel-specific
 struct WalkSmem {
@@ -363,7 +363,9 @@ size_t walk_smem_bytes(const WalkPlan& W) {
 // ---------------------------------------------------------------------------------------------
 // fused objective: deformation + warp + joint histogram
 // ---------------------------------------------------------------------------------------------
-template <bool kTrial>
+// kXs: the item's x-contracted node rows are staged in shared memory (a launch-time choice
+// made a template parameter, so the walk carries no test for it)
+template <bool kTrial, bool kXs>
 __global__ void __launch_bounds__(32 * TY_OBJECTIVE, 2)
 k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
             const int32_t *__restrict__ mask, const float *__restrict__ cpp,
@@ -384,7 +386,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
         stage_item<kTrial>(P, cpp, item, S.cp, S.zb, S.zk, I, grad, scale);
         Column C;
         column_init(P, I, S.cp, C);
-        if (P.xs) build_xrows(P, C, S.cp, X);
+        if (kXs) build_xrows(P, C, S.cp, X);
         const int nzi = I.z1 - I.z0;
         int idx = (I.z0 * P.ny + C.y) * P.nx + C.x;
         const int zstride = P.nx * P.ny;
@@ -394,7 +396,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
             for (int u = 0; u < WALK_GROUP; ++u) {
                 const int zu = min(zi + u, nzi - 1);
                 float pos[3];
-                column_position(P, I, C, S.zb, S.zk, zu, pos, P.xs ? X : nullptr);
+                column_position(P, I, C, S.zb, S.zk, zu, pos, kXs ? X : nullptr);
                 bin[u] = -1;
                 if (C.inside && zi + u < nzi) {
                     const int vi = idx + u * zstride;
@@ -490,7 +492,7 @@ __device__ __forceinline__ float nmi_window_f(float rv, float wv, const float *l
     //   sum_tu br_t dw_u rlog_t = (sum_t br_t rlog_t)(sum_u dw_u), and likewise for wlog
     float br[4], dw[4], rl[4], wl[4];
     int ri[4], wi[4];
-    if (rv >= 1.f && wv >= 1.f) {
+    if (rv >= 1.f && wv >= 1.f && rv < (float)(rb - 2) && wv < (float)(fb - 2)) {
         // r0 + 1 = floor(rv): the four taps sit at rv - r = f + 1, f, f - 1, f - 2 (all exact)
         // with f the fractional part, each inside one known piece of the kernel. The pieces
         // parzenf / parzen_derivf would select are written out with their operations in their
@@ -506,15 +508,14 @@ __device__ __forceinline__ float nmi_window_f(float rv, float wv, const float *l
         dw[1] = (1.5f * g - 2.f) * g;
         dw[2] = (1.5f * mg - 2.f) * -mg;
         dw[3] = 0.5f * g * g;
+        // 1 <= rv < rb - 2: the taps r0 .. r0 + 3 = floor(rv) - 1 .. floor(rv) + 2 all lie in the
+        // table (and likewise for wv), so none is masked or clamped
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
-            const int r = r0 + t, w = w0 + t;
-            if (!(r < rb)) br[t] = 0.f;
-            if (!(w < fb)) dw[t] = 0.f;
-            ri[t] = min(r, rb - 1);
-            wi[t] = min(w, fb - 1) * rb;
-            rl[t] = rlog[ri[t]];
-            wl[t] = wlog[min(w, fb - 1)];
+            ri[t] = r0 + t;
+            wi[t] = (w0 + t) * rb;
+            rl[t] = rlog[r0 + t];
+            wl[t] = wlog[w0 + t];
         }
     } else {
 #pragma unroll
@@ -1029,7 +1030,7 @@ static long long blocks_resident(K kernel, int threads, size_t smem) {
     return (long long)per_sm * sm_count();
 }
 
-long long objective_slots(size_t smem) { return blocks_resident(k_objective<true>, 32 * TY_OBJECTIVE, smem); }
+long long objective_slots(size_t smem) { return blocks_resident(k_objective<true, true>, 32 * TY_OBJECTIVE, smem); }
 long long gradient_slots(size_t smem) { return blocks_resident(k_gradient<true>, 32 * TY_GRADIENT, smem); }
 long long deformation_slots(size_t smem) { return blocks_resident(k_deformation, 32 * TY_DEFORMATION, smem); }
 
@@ -1046,7 +1047,8 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
     const size_t smem = base_smem + (P.xs ? xs_bytes : 0);
     const int threads = 32 * ws->walk_obj.ty;
     const bool trial = grad != nullptr;
-    auto kernel = trial ? k_objective<true> : k_objective<false>;
+    auto kernel = trial ? (P.xs ? k_objective<true, true> : k_objective<true, false>)
+                        : (P.xs ? k_objective<false, true> : k_objective<false, false>);
     int grid = 0;
     NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid));
     // algorithmic bytes: reference + floating (+ mask) per voxel, the grid once
