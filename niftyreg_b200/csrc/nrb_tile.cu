@@ -234,9 +234,11 @@ __device__ __forceinline__ void column_position(const WalkParams& P, const Item&
 // off-diagonal terms the single-precision FMA rounds the same exact value once instead of twice
 // (the two agree except when the exact value falls within 2^-53 of a float rounding boundary)
 // and keeps the conversions off the XU pipe.
+// kDiag: 1 = M has no off-diagonal terms, 0 = general M, -1 = decided by `diag` at run time
+template <int kDiag>
 __device__ __forceinline__ void to_floating_voxel(const Mat34& M, int diag, float x, float y, float z,
                                                   float& fx, float& fy, float& fz) {
-    if (diag) {
+    if (kDiag == 1 || (kDiag < 0 && diag)) {
         fx = __fmaf_rn(M.m[0], x, M.m[3]);
         fy = __fmaf_rn(M.m[5], y, M.m[7]);
         fz = __fmaf_rn(M.m[10], z, M.m[11]);
@@ -271,13 +273,13 @@ __device__ __forceinline__ int trunc_nonneg(float v) { return __float2int_rz(v);
 // the clamped path substitutes, so the two paths give the same numbers. Other warps read
 // clamped in-volume addresses and select the padding value for out-of-volume taps, with no
 // divergence.
-template <bool kGrad>
+template <bool kGrad, int kDiag = -1>
 __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, int fnx, int fny,
                                                 int fnz, int sy, int sz, int margin, const Mat34& M,
                                                 int diag, float pad, float x, float y, float z,
                                                 float& val, float g[3]) {
     float fx, fy, fz;
-    to_floating_voxel(M, diag, x, y, z, fx, fy, fz);
+    to_floating_voxel<kDiag>(M, diag, x, y, z, fx, fy, fz);
     float flx, fly, flz;
     const int px = floor_split(fx, flx), py = floor_split(fy, fly), pz = floor_split(fz, flz);
     const float rx = fx - flx, ry = fy - fly, rz = fz - flz;
@@ -363,9 +365,10 @@ size_t walk_smem_bytes(const WalkPlan& W) {
 // ---------------------------------------------------------------------------------------------
 // fused objective: deformation + warp + joint histogram
 // ---------------------------------------------------------------------------------------------
-// kXs: the item's x-contracted node rows are staged in shared memory (a launch-time choice
-// made a template parameter, so the walk carries no test for it)
-template <bool kTrial, bool kXs>
+// kXs: the item's x-contracted node rows are staged in shared memory; kDiag: the floating
+// image's mm -> voxel matrix has no off-diagonal terms (launch-time choices made template
+// parameters, so the walk carries no test for them)
+template <bool kTrial, bool kXs, bool kDiag>
 __global__ void __launch_bounds__(32 * TY_OBJECTIVE, 2)
 k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
             const int32_t *__restrict__ mask, const float *__restrict__ cpp,
@@ -402,10 +405,11 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
                     const int vi = idx + u * zstride;
                     if (mask == nullptr || __ldg(&mask[vi]) > -1) {
                         float w, g[3];
-                        sample_floating<false>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin, P.flo_ijk,
-                                               P.flo_diag, P.pad, pos[0], pos[1], pos[2], w, g);
+                        sample_floating<false, kDiag ? 1 : 0>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin,
+                                                              P.flo_ijk, P.flo_diag, P.pad, pos[0], pos[1], pos[2],
+                                                              w, g);
                         const float rv = __ldg(&ref[vi]);
-                        if (rv == rv && w == w && 0.f <= rv && rv < frb && 0.f <= w && w < ffb)
+                        if (0.f <= rv && rv < frb && 0.f <= w && w < ffb)  // false for NaN
                             bin[u] = trunc_nonneg(rv) + trunc_nonneg(w) * P.rb;
                     }
                 }
@@ -549,7 +553,7 @@ __device__ __forceinline__ float nmi_window_f(float rv, float wv, const float *l
 // ---------------------------------------------------------------------------------------------
 // fused gradient: deformation + warp + spatial gradient + NMI voxel gradient
 // ---------------------------------------------------------------------------------------------
-template <bool kF32>
+template <bool kF32, bool kDiag>
 __global__ void __launch_bounds__(32 * TY_GRADIENT, kF32 ? 6 : 4)
 k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
            const int32_t *__restrict__ mask, const float *__restrict__ cpp,
@@ -586,7 +590,7 @@ k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict_
             float out[3] = { 0.f, 0.f, 0.f };
             if (mask == nullptr || __ldg(&mask[idx]) > -1) {
                 float w, g[3];
-                sample_floating<true>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin, P.flo_ijk, P.flo_diag,
+                sample_floating<true, kDiag ? 1 : 0>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin, P.flo_ijk, P.flo_diag,
                                       P.pad, pos[0], pos[1], pos[2], w, g);
                 const float rv = __ldg(&ref[idx]);
                 if (rv == rv && w == w) {
@@ -1030,8 +1034,8 @@ static long long blocks_resident(K kernel, int threads, size_t smem) {
     return (long long)per_sm * sm_count();
 }
 
-long long objective_slots(size_t smem) { return blocks_resident(k_objective<true, true>, 32 * TY_OBJECTIVE, smem); }
-long long gradient_slots(size_t smem) { return blocks_resident(k_gradient<true>, 32 * TY_GRADIENT, smem); }
+long long objective_slots(size_t smem) { return blocks_resident(k_objective<true, true, true>, 32 * TY_OBJECTIVE, smem); }
+long long gradient_slots(size_t smem) { return blocks_resident(k_gradient<true, true>, 32 * TY_GRADIENT, smem); }
 long long deformation_slots(size_t smem) { return blocks_resident(k_deformation, 32 * TY_DEFORMATION, smem); }
 
 nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
@@ -1047,8 +1051,10 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
     const size_t smem = base_smem + (P.xs ? xs_bytes : 0);
     const int threads = 32 * ws->walk_obj.ty;
     const bool trial = grad != nullptr;
-    auto kernel = trial ? (P.xs ? k_objective<true, true> : k_objective<true, false>)
-                        : (P.xs ? k_objective<false, true> : k_objective<false, false>);
+    auto kernel = P.flo_diag ? (trial ? (P.xs ? k_objective<true, true, true> : k_objective<true, false, true>)
+                                      : (P.xs ? k_objective<false, true, true> : k_objective<false, false, true>))
+                             : (trial ? (P.xs ? k_objective<true, true, false> : k_objective<true, false, false>)
+                                      : (P.xs ? k_objective<false, true, false> : k_objective<false, false, false>));
     int grid = 0;
     NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid));
     // algorithmic bytes: reference + floating (+ mask) per voxel, the grid once
@@ -1078,7 +1084,8 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
     const size_t smem = walk_smem_bytes(ws->walk_grad) + (P.log_in_smem ? log_bytes : 0);
     const int threads = 32 * ws->walk_grad.ty;
     int grid = 0;
-    auto kernel = P.log_in_smem ? k_gradient<true> : k_gradient<false>;
+    auto kernel = P.flo_diag ? (P.log_in_smem ? k_gradient<true, true> : k_gradient<false, true>)
+                             : (P.log_in_smem ? k_gradient<true, false> : k_gradient<false, false>);
     NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid));
     // algorithmic bytes: reference + floating (+ mask) read, voxel gradient written, grid once
     const double nv = (double)P.nx * P.ny * P.nz;
