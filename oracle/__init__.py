@@ -103,6 +103,15 @@ class Ref:
                               _i(_i3(mask)) if mask is not None else None, ctypes.c_float(pad), _f(w))
         return w
 
+    def resample_order(self, flo, fdim, fpix, fxyz, dfield, rdim, rpix, rxyz, order, mask=None, pad=np.nan,
+                       warped_init=None):
+        w = np.zeros(int(np.prod(rdim)), np.float32) if warped_init is None else _f3(warped_init).copy()
+        self.lib.ref_resample_order(_f(_f3(flo)), _i(_i3(fdim)), _f(_f3(fpix)), _f(_m(fxyz)),
+                                    _f(_f3(dfield)), _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)),
+                                    _i(_i3(mask)) if mask is not None else None, ctypes.c_float(pad),
+                                    int(order), _f(w))
+        return w
+
     def image_gradient(self, flo, fdim, fpix, fxyz, dfield, rdim, rpix, rxyz, mask=None, pad=np.nan):
         g = np.zeros(3 * int(np.prod(rdim)), np.float32)
         self.lib.ref_image_gradient(_f(_f3(flo)), _i(_i3(fdim)), _f(_f3(fpix)), _f(_m(fxyz)),
@@ -215,6 +224,15 @@ class Restated:
         self.lib.orc_resample_linear(_f(_f3(flo)), _i(_i3(fdim)), _f(_m(flo_ijk)), _f(_f3(dfield)),
                                      _i(_i3(rdim)), _i(_i3(mask)) if mask is not None else None,
                                      ctypes.c_float(pad), _f(w))
+        return w
+
+    def resample_order(self, flo, fdim, flo_ijk, dfield, rdim, order, mask=None, pad=np.nan, warped_init=None):
+        w = np.zeros(int(np.prod(rdim)), np.float32) if warped_init is None else _f3(warped_init).copy()
+        rc = self.lib.orc_resample_order(_f(_f3(flo)), _i(_i3(fdim)), _f(_m(flo_ijk)), _f(_f3(dfield)),
+                                         _i(_i3(rdim)), _i(_i3(mask)) if mask is not None else None,
+                                         ctypes.c_float(pad), int(order), _f(w))
+        if rc != 0:
+            raise ValueError("orc_resample_order: order must be 0, 1 or 3")
         return w
 
     def image_gradient(self, flo, fdim, flo_ijk, dfield, rdim, mask=None, pad=np.nan):

@@ -129,6 +129,80 @@ int orc_resample_linear(const float *flo, const int fdim[3], const float flo_ijk
     return 0;
 }
 
+/* The resampling kernels of reg-lib/cpu/_reg_resampling.cpp:60-97, in float with each product
+ * and sum rounded on its own (the reference's CPU build has no contraction; this file is ISO C,
+ * where gcc contracts nothing either). order 0: nearest (2 taps), 1: linear (2 taps), 3: cubic
+ * spline (4 taps starting one voxel before floor(position)). */
+static int resample_taps(int order, float rel, float w[4]) {
+    if (rel < 0) rel = 0; /* rounding guard of every kernel */
+    if (order == 0) {
+        w[0] = rel >= 0.5f ? 0.f : 1.f;
+        w[1] = rel >= 0.5f ? 1.f : 0.f;
+        return 2;
+    }
+    if (order == 1) {
+        w[1] = rel;
+        w[0] = 1.f - rel;
+        return 2;
+    }
+    {
+        const float sq = rel * rel;
+        const float a0 = (2.f - rel) * rel;
+        w[0] = (rel * (a0 - 1.f)) / 2.f;
+        const float a1 = 3.f * rel - 5.f;
+        w[1] = (sq * a1 + 2.f) / 2.f;
+        const float a2 = (4.f - 3.f * rel) * rel;
+        w[2] = (rel * (a2 + 1.f)) / 2.f;
+        w[3] = (rel - 1.f) * sq / 2.f;
+        return 4;
+    }
+}
+
+/* ResampleImage3D with kernel `order` (reg-lib/cpu/_reg_resampling.cpp:316-464): the window of
+ * 2 or 4 taps per axis starts at floor(position) - offset; when the whole window lies inside
+ * the volume the taps are summed directly, otherwise every out-of-volume tap contributes
+ * padding * weight (so NaN padding poisons the voxel even through a zero weight). Sums run x,
+ * then y, then z, in float. Masked voxels keep their value. */
+int orc_resample_order(const float *flo, const int fdim[3], const float flo_ijk[16], const float *def,
+                       const int rdim[3], const int *mask, float pad, int order, float *warped) {
+    if (order != 0 && order != 1 && order != 3) return -1;
+    const size_t nr = nvox3(rdim);
+    const int offset = order == 3 ? 1 : 0;
+    for (size_t i = 0; i < nr; ++i) {
+        if (mask && mask[i] <= -1) continue;
+        const float world[3] = { def[i], def[nr + i], def[2 * nr + i] };
+        float pos[3], w[3][4];
+        mat44_apply(flo_ijk, world, pos);
+        int first[3], n = 0;
+        for (int d = 0; d < 3; ++d) {
+            const int fl = (int)floorf(pos[d]);
+            n = resample_taps(order, pos[d] - (float)fl, w[d]);
+            first[d] = fl - offset;
+        }
+        const int inside = first[0] > -1 && first[0] + n - 1 < fdim[0] && first[1] > -1 &&
+                           first[1] + n - 1 < fdim[1] && first[2] > -1 && first[2] + n - 1 < fdim[2];
+        float intensity = 0;
+        for (int c = 0; c < n; ++c) {
+            const int Z = first[2] + c;
+            float yv = 0;
+            for (int b = 0; b < n; ++b) {
+                const int Y = first[1] + b;
+                float xv = 0;
+                for (int a = 0; a < n; ++a) {
+                    const int X = first[0] + a;
+                    const int in = inside || (X > -1 && X < fdim[0] && Y > -1 && Y < fdim[1] && Z > -1 && Z < fdim[2]);
+                    const float v = in ? flo[((size_t)Z * fdim[1] + Y) * fdim[0] + X] : pad;
+                    xv += v * w[0][a];
+                }
+                yv += xv * w[1][b];
+            }
+            intensity += yv * w[2][c];
+        }
+        warped[i] = intensity;
+    }
+    return 0;
+}
+
 /* Spatial gradient of the trilinearly warped floating image in floating-voxel units:
  * TrilinearImageGradient, reg-lib/cpu/_reg_resampling.cpp:1797-1915 (derivative kernel [-1, 1],
  * out-of-volume taps read the padding value, NaN components set to 0, masked voxels get 0). */

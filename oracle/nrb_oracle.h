@@ -14,6 +14,8 @@ int orc_deformation_field(const float *cpp, const int cdim[3], const float cpix[
 int orc_resample_linear(const float *flo, const int fdim[3], const float flo_ijk[16],
                         const float *def, const int rdim[3], const int *mask, float pad,
                         float *warped);
+int orc_resample_order(const float *flo, const int fdim[3], const float flo_ijk[16], const float *def,
+                       const int rdim[3], const int *mask, float pad, int order, float *warped);
 int orc_image_gradient_linear(const float *flo, const int fdim[3], const float flo_ijk[16],
                               const float *def, const int rdim[3], const int *mask, float pad,
                               float *grad);

@@ -155,6 +155,21 @@ int ref_resample(const float *flo, const int *fdim, const float *fpix, const flo
     return 0;
 }
 
+// _reg_resampling.cpp:638-692 with the interpolation order (0 nearest, 1 linear, 3 cubic spline)
+int ref_resample_order(const float *flo, const int *fdim, const float *fpix, const float *fxyz,
+                       const float *def, const int *rdim, const float *rpix, const float *rxyz,
+                       const int *mask, float pad, int order, float *warped_inout) {
+    NiftiImage fimg = MakeImage(fdim, fpix, fxyz);
+    memcpy(fimg->data, flo, Nvox(fdim) * sizeof(float));
+    NiftiImage dimg = MakeImage(rdim, rpix, rxyz, 3);
+    memcpy(dimg->data, def, 3 * Nvox(rdim) * sizeof(float));
+    NiftiImage wimg = MakeImage(rdim, rpix, rxyz);
+    memcpy(wimg->data, warped_inout, Nvox(rdim) * sizeof(float));
+    reg_resampleImage(fimg, wimg, dimg, mask, order, pad);
+    memcpy(warped_inout, wimg->data, Nvox(rdim) * sizeof(float));
+    return 0;
+}
+
 // _reg_resampling.cpp:2328-2384
 int ref_image_gradient(const float *flo, const int *fdim, const float *fpix, const float *fxyz,
                        const float *def, const int *rdim, const float *rpix, const float *rxyz,

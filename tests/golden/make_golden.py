@@ -9,6 +9,8 @@ Each case file `<name>.npz` holds the inputs (images, grid, geometry) and the re
 for every step of the F3D objective/gradient path:
   def        reg_spline_getDeformationField (cubic B-spline, positions in mm)
   warped     reg_resampleImage, linear, NaN padding
+  warped_nn, warped_cubic, warped_cubic_pad0
+             reg_resampleImage, nearest / cubic spline (NaN padding) and cubic with padding 0
   wgrad      reg_getImageGradient, linear
   nmi, pro, logt, ent
              reg_nmi value, smoothed joint/marginal tables, log tables, entropies
@@ -43,6 +45,9 @@ def generate(name, kw):
     R.set_threads(1)
     d = R.deformation_field(c.cpp, c.cdim, c.cpix, c.cxyz, c.rdim, c.rpix, c.rxyz)
     w = R.resample(c.flo, c.fdim, c.fpix, c.fxyz, d, c.rdim, c.rpix, c.rxyz)
+    w_nn = R.resample_order(c.flo, c.fdim, c.fpix, c.fxyz, d, c.rdim, c.rpix, c.rxyz, 0)
+    w_cubic = R.resample_order(c.flo, c.fdim, c.fpix, c.fxyz, d, c.rdim, c.rpix, c.rxyz, 3)
+    w_cubic0 = R.resample_order(c.flo, c.fdim, c.fpix, c.fxyz, d, c.rdim, c.rpix, c.rxyz, 3, pad=0.0)
     g = R.image_gradient(c.flo, c.fdim, c.fpix, c.fxyz, d, c.rdim, c.rpix, c.rxyz)
     nmi, pro, logt, ent = R.nmi_value(c.ref, w, c.rdim, c.bins, c.bins)
     vg = R.nmi_voxel_gradient(c.ref, w, g, c.rdim, c.bins, c.bins, 1.0)
@@ -58,7 +63,7 @@ def generate(name, kw):
         fdim=np.array(c.fdim, np.int32), fpix=np.array(c.fpix, np.float32), fxyz=c.fxyz.astype(np.float32),
         cdim=np.array(c.cdim, np.int32), cpix=np.array(c.cpix, np.float32), cxyz=c.cxyz.astype(np.float32),
         bins=np.int32(c.bins), ref=c.ref, flo=c.flo, cpp=c.cpp,
-        **{"def": d}, warped=w, wgrad=g, nmi=np.float64(nmi), pro=pro, logt=logt, ent=ent, vgrad=vg,
+        **{"def": d}, warped=w, warped_nn=w_nn, warped_cubic=w_cubic, warped_cubic_pad0=w_cubic0, wgrad=g, nmi=np.float64(nmi), pro=pro, logt=logt, ent=ent, vgrad=vg,
         node=node, be=np.float64(be), be_grad=be_grad, **conv)
     print(f"{name}: {c.rdim} grid {c.cdim} bins {c.bins} NMI {nmi:.10f} BE {be:.6g}")
 

@@ -49,6 +49,17 @@ def test_resample_and_gradient(O, gold):
     assert np.abs(gr - g["wgrad"]).max() <= 1e-5
 
 
+def test_resample_nearest_and_cubic_bit_exact(O, gold):
+    """ResampleImage3D with the nearest and cubic-spline kernels (the final warp of
+    reg_f3d::GetWarpedImage uses the cubic one): the restatement repeats the reference's float
+    operations, so every voxel, NaN padding included, is the same float."""
+    g = gold
+    ijk = _ijk(g["fxyz"])
+    for order, key, pad in ((0, "warped_nn", np.nan), (3, "warped_cubic", np.nan), (3, "warped_cubic_pad0", 0.0)):
+        w = O.resample_order(g["flo"], g["fdim"], ijk, g["def"], g["rdim"], order, pad=pad)
+        assert np.array_equal(w, g[key], equal_nan=True), key
+
+
 def test_nmi_tables_bit_exact(O, gold):
     g = gold
     b = int(g["bins"])
