@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", choices=["plain", "batched", "served"], default="plain")
+    ap.add_argument("--mode", choices=["plain", "batched", "served", "warp"], default="plain")
     ap.add_argument("--pairs", type=int, default=64, help="batched: number of pairs")
     ap.add_argument("--concurrency", type=int, default=16, help="batched/served: concurrent registrations")
     ap.add_argument("--requests", type=int, default=300, help="served: requests per arrival rate")
@@ -550,6 +550,97 @@ def run_served(args):
     return 0
 
 
+def run_warp(args):
+    """The final warped image of a registration of the workload's volume (reg_f3d::GetWarpedImage:
+    deformation field of the grid, cubic-spline resample of the floating image), on the device
+    with inputs resident (CUDA events, L2 flushed between steps) and end to end from host
+    buffers (copies included), against the reference's own CPU path (oracle/_ref:
+    reg_spline_getDeformationField + reg_resampleImage order 3, all host threads)."""
+    import torch
+    import niftyreg_b200 as nrb
+    from niftyreg_b200 import phantom
+
+    torch.cuda.set_device(0)
+    nrb.build()
+    pair = phantom.brain_pair(SHAPE, seed=args.seed)
+    nz, ny, nx = SHAPE
+    dim, pix = (nx, ny, nz), (1.0, 1.0, 1.0)
+    cdim, cpix, cxyz = nrb.control_grid_header(dim, pix, (5.0, 5.0, 5.0))
+    rng = np.random.default_rng(args.seed)
+    cx, cy, cz = cdim
+    zz, yy, xx = np.meshgrid(np.arange(cz), np.arange(cy), np.arange(cx), indexing="ij")
+    ident = np.concatenate([(5.0 * v - 5.0).ravel() for v in (xx, yy, zz)]).astype(np.float32)
+    cpp = ident + rng.normal(0, 2.0, ident.size).astype(np.float32)
+    g = nrb.make_geometry(dim, pix, nrb.identity_header(pix), dim, pix, nrb.identity_header(pix), cdim, cpix, cxyz)
+    n = nx * ny * nz
+    flo_h = torch.from_numpy(pair.floating.ravel().copy()).pin_memory()
+    cpp_h = torch.from_numpy(cpp).pin_memory()
+    out_h = torch.empty(n, dtype=torch.float32).pin_memory()
+    flo_d, cpp_d = flo_h.cuda(), cpp_h.cuda()
+    out_d = torch.empty(n, dtype=torch.float32, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        nrb.f3d_warped_image(g, flo_d, cpp_d, out_d, order=3, padding=0.0, stream=stream)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        nrb.f3d_warped_image(g, flo_d, cpp_d, out_d, order=3, padding=0.0, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    e2e = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            flo_d.copy_(flo_h, non_blocking=True)
+            cpp_d.copy_(cpp_h, non_blocking=True)
+            nrb.f3d_warped_image(g, flo_d, cpp_d, out_d, order=3, padding=0.0, stream=stream)
+            out_h.copy_(out_d, non_blocking=True)
+        stream.synchronize()
+        e2e.append(time.perf_counter() - t0)
+    warped = out_h.numpy().copy()
+    t = sum(ms) / len(ms) / 1e3
+    peak, peak_kind = peaks()
+    alg = 8.0 * n + 12.0 * ident.size  # floating read + warped written + grid read
+    line = {"mode": "warp", "metric": "final warped image (reg_f3d::GetWarpedImage, cubic spline) per second",
+            "value": 1.0 / t, "unit": "warps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "182x218x182 float32 brain-MR-like floating image, 5 mm grid with N(0, 2 mm) "
+                                   "control-point displacements, cubic spline, padding 0",
+                       "l2": f"{L2_FLUSH_BYTES >> 20} MiB buffer written between timed steps"},
+            "roofline": {"bound": "hbm", "achieved": alg / t / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / t / 1e9 / peak, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": alg},
+            "e2e": {"value": len(e2e) / sum(e2e), "unit": "warps/s", "h2d_bytes_per_step": 4 * (n + ident.size),
+                    "d2h_bytes_per_step": 4 * n},
+            "clocks": clocks}
+    if not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            R = oracle.Ref()
+            cores = R.set_threads(os.cpu_count() or 1)
+            eye = nrb.identity_header(pix)
+            t0 = time.perf_counter()
+            d = R.deformation_field(cpp, cdim, cpix, cxyz, dim, pix, eye)
+            ref = R.resample_order(pair.floating.ravel(), dim, pix, eye, d, dim, pix, eye, 3, pad=0.0)
+            wall = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": 1.0 / wall, "unit": "warps/s", "cores": int(cores), "kind": "reference",
+                                    "sample": "reference reg_spline_getDeformationField + reg_resampleImage order 3 "
+                                              f"(oracle/_ref, OpenMP) on the same volume and grid, {wall:.2f} s"}
+            ok = np.isfinite(ref)
+            line["max_abs_diff_vs_reference"] = float(np.abs(warped[ok] - ref[ok]).max())
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -560,6 +651,8 @@ def main():
         return run_batched(args)
     if args.mode == "served":
         return run_served(args)
+    if args.mode == "warp":
+        return run_warp(args)
     return run_b200(args)
 
 

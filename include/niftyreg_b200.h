@@ -88,6 +88,16 @@ nrb_status nrb_get_deformation_field(const nrb_geometry *g, const float *cpp, co
 nrb_status nrb_resample_image(const nrb_geometry *g, const float *flo, const float *def,
                               const int32_t *mask, float padding, float *warped, void *stream);
 
+/* Warp of the floating image by a deformation field with interpolation `order`: 0 nearest,
+ * 1 linear, 3 cubic spline; any other order returns NRB_ERR_UNSUPPORTED. The reference's float
+ * operations are kept unfused, so the result is bit-identical to the reference's. Replaces
+ * Compute::ResampleImage(order, padding) (reg-lib/Compute.cpp:8-15) -> ResampleImage3D
+ * (reg-lib/cpu/_reg_resampling.cpp:316-464) with interpNearestNeighKernel / interpLinearKernel /
+ * interpCubicSplineKernel (:60-97). Masked voxels are untouched. */
+nrb_status nrb_resample_image_order(const nrb_geometry *g, const float *flo, const float *def,
+                                    const int32_t *mask, int order, float padding, float *warped,
+                                    void *stream);
+
 /* Spatial gradient (floating voxel units) of the trilinearly warped floating image, NaN -> 0.
  * Replaces Compute::GetImageGradient(1, padding, 0) (reg-lib/Compute.cpp:129-138) ->
  * TrilinearImageGradient (reg-lib/cpu/_reg_resampling.cpp:1797-1915). grad: 3 * nvox(ref). */
@@ -286,6 +296,18 @@ nrb_status nrb_f3d_register_device(const float *ref, const float *flo, const int
                                    const float pixdim[3], const nrb_f3d_params *p,
                                    float *cpp_out, int64_t cpp_capacity, nrb_f3d_result *result,
                                    void *stream);
+
+/* The final warped image of a registration, on the device: the deformation field of the
+ * control-point grid `cpp` over the reference geometry of `g` (nrb_get_deformation_field), then
+ * the floating image `flo` (device, original intensities) resampled with interpolation `order`
+ * and `padding` (nrb_resample_image_order). Replaces reg_f3d<T>::GetWarpedImage
+ * (reg-lib/_reg_f3d.cpp:503-515), which the reference runs on the CPU with order 3 (cubic
+ * spline). For a grid from nrb_f3d_register_*, `g` holds the grid of nrb_f3d_grid_dims with the
+ * spacing the registration used. One pass: the positions are computed as nrb_get_deformation_field
+ * computes them and resampled at once (no deformation field in memory, no allocation).
+ * warped: nvox(ref) floats. */
+nrb_status nrb_f3d_warped_image(const nrb_geometry *g, const float *flo, const float *cpp, int order,
+                                float padding, float *warped, void *stream);
 
 /* ---- batched and served registrations (no counterpart in the reference) -------------------- */
 

@@ -218,6 +218,20 @@ def resample_image(g, flo, deformation, warped, padding=math.nan, mask=None, str
                                    _p(warped), _s(stream)))
 
 
+def resample_image_order(g, flo, deformation, warped, order, padding=math.nan, mask=None, stream=None):
+    """Warp with interpolation `order` (0 nearest, 1 linear, 3 cubic spline), bit-identical to the
+    reference's ResampleImage3D."""
+    check(lib().nrb_resample_image_order(ctypes.byref(g), _p(flo), _p(deformation), _p(mask), int(order),
+                                         ctypes.c_float(padding), _p(warped), _s(stream)))
+
+
+def f3d_warped_image(g, flo, cpp, warped, order=3, padding=math.nan, stream=None):
+    """reg_f3d::GetWarpedImage on the device: deformation field of `cpp` over the reference
+    geometry of `g`, then the floating image resampled with `order` (cubic spline by default)."""
+    check(lib().nrb_f3d_warped_image(ctypes.byref(g), _p(flo), _p(cpp), int(order), ctypes.c_float(padding),
+                                     _p(warped), _s(stream)))
+
+
 def get_image_gradient(g, flo, deformation, grad, padding=math.nan, mask=None, stream=None):
     check(lib().nrb_get_image_gradient(ctypes.byref(g), _p(flo), _p(deformation), _p(mask), ctypes.c_float(padding),
                                        _p(grad), _s(stream)))

@@ -638,6 +638,7 @@ k_deformation(WalkParams P, const int32_t *__restrict__ mask, const float *__res
     }
 }
 
+
 // ---------------------------------------------------------------------------------------------
 // histogram -> smoothed probabilities, FP64 entropies, log table (one cluster, tables in smem)
 // ---------------------------------------------------------------------------------------------
@@ -918,6 +919,111 @@ __global__ void k_resample(long long nv, int fnx, int fny, int fnz, Mat34 M, int
     }
 }
 
+// Weights of the resampling kernels of order 0 (nearest), 1 (linear) and 3 (cubic spline), as
+// interpNearestNeighKernel / interpLinearKernel / interpCubicSplineKernel compute them
+// (reg-lib/cpu/_reg_resampling.cpp:60-97): float, every product and sum rounded on its own.
+template <int kOrder>
+__device__ __forceinline__ void order_weights(float rel, float w[4]) {
+    if (rel < 0.f) rel = 0.f;  // the kernels' rounding guard
+    if (kOrder == 0) {
+        w[0] = rel >= 0.5f ? 0.f : 1.f;
+        w[1] = rel >= 0.5f ? 1.f : 0.f;
+    } else if (kOrder == 1) {
+        w[1] = rel;
+        w[0] = __fsub_rn(1.f, rel);
+    } else {
+        const float sq = __fmul_rn(rel, rel);
+        w[0] = __fmul_rn(__fmul_rn(rel, __fsub_rn(__fmul_rn(__fsub_rn(2.f, rel), rel), 1.f)), 0.5f);
+        w[1] = __fmul_rn(__fadd_rn(__fmul_rn(sq, __fsub_rn(__fmul_rn(3.f, rel), 5.f)), 2.f), 0.5f);
+        w[2] = __fmul_rn(__fmul_rn(rel, __fadd_rn(__fmul_rn(__fsub_rn(4.f, __fmul_rn(3.f, rel)), rel), 1.f)), 0.5f);
+        w[3] = __fmul_rn(__fmul_rn(__fsub_rn(rel, 1.f), sq), 0.5f);
+    }
+}
+
+// ResampleImage3D with the kernel of order kOrder (reg-lib/cpu/_reg_resampling.cpp:316-464) at
+// world position (x, y, z), with the reference's operations: mm -> voxel as Mat44Mul (products of
+// two floats are exact in double), a window of 2 (orders 0, 1) or 4 (order 3, starting one voxel
+// before floor) taps per axis, sums in float along x, then y, then z, and padding * weight for
+// every out-of-volume tap when the window leaves the volume. Bit-identical to the reference.
+template <int kOrder>
+__device__ __forceinline__ float sample_order(const float *__restrict__ flo, int fnx, int fny, int fnz,
+                                              const Mat34& M, float pad, float x, float y, float z) {
+    constexpr int kTaps = kOrder == 3 ? 4 : 2, kOffset = kOrder == 3 ? 1 : 0;
+    float fx, fy, fz;
+    to_floating_voxel<0>(M, 0, x, y, z, fx, fy, fz);
+    const float fp[3] = { fx, fy, fz };
+    float w[3][4];
+    int first[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float fl = floorf(fp[d]);
+        order_weights<kOrder>(__fsub_rn(fp[d], fl), w[d]);
+        first[d] = (int)fl - kOffset;
+    }
+    // tap indices in unsigned arithmetic: a window far outside (a saturated floor) wraps to
+    // indices that fail the range tests instead of overflowing
+    const unsigned ux = (unsigned)first[0], uy = (unsigned)first[1], uz = (unsigned)first[2];
+    const bool inside = first[0] > -1 && ux + (kTaps - 1) < (unsigned)fnx && first[1] > -1 &&
+                        uy + (kTaps - 1) < (unsigned)fny && first[2] > -1 && uz + (kTaps - 1) < (unsigned)fnz;
+    float intensity = 0.f;
+#pragma unroll
+    for (int c = 0; c < kTaps; ++c) {
+        const unsigned Z = uz + c;
+        float yv = 0.f;
+#pragma unroll
+        for (int b = 0; b < kTaps; ++b) {
+            const unsigned Y = uy + b;
+            float xv = 0.f;
+#pragma unroll
+            for (int a = 0; a < kTaps; ++a) {
+                const unsigned X = ux + a;
+                const bool in = inside || (X < (unsigned)fnx && Y < (unsigned)fny && Z < (unsigned)fnz);
+                const float v = in ? __ldg(flo + ((long long)Z * fny + Y) * fnx + X) : pad;
+                xv = __fadd_rn(xv, __fmul_rn(v, w[0][a]));
+            }
+            yv = __fadd_rn(yv, __fmul_rn(xv, w[1][b]));
+        }
+        intensity = __fadd_rn(intensity, __fmul_rn(yv, w[2][c]));
+    }
+    return intensity;
+}
+
+// sample_order at the positions of a deformation field, one voxel per thread; masked voxels keep
+// their value
+template <int kOrder>
+__global__ void k_resample_order(long long nv, int fnx, int fny, int fnz, Mat34 M, float pad,
+                                 const float *__restrict__ flo, const float *__restrict__ def,
+                                 const int32_t *__restrict__ mask, float *__restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (mask != nullptr && mask[i] <= -1) continue;
+        out[i] = sample_order<kOrder>(flo, fnx, fny, fnz, M, pad, def[i], def[nv + i], def[2 * nv + i]);
+    }
+}
+
+// The final warp in one pass: k_deformation's positions (the same column walk, so the same
+// floats) consumed at once by sample_order; the deformation field never reaches memory.
+template <int kOrder>
+__global__ void __launch_bounds__(32 * TY_DEFORMATION)
+k_warp_order(WalkParams P, const float *__restrict__ cpp, const float *__restrict__ flo, float *__restrict__ warped) {
+    extern __shared__ float4 sm4[];
+    const WalkSmem S = walk_smem(P, sm4);
+    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
+        Item I;
+        stage_item(P, cpp, item, S.cp, S.zb, S.zk, I);
+        Column C;
+        column_init(P, I, S.cp, C);
+        const int nzi = I.z1 - I.z0;
+        for (int zi = 0; zi < nzi; ++zi) {
+            float pos[3];
+            column_position(P, I, C, S.zb, S.zk, zi, pos);
+            if (!C.inside) continue;
+            const int idx = ((I.z0 + zi) * P.ny + C.y) * P.nx + C.x;
+            warped[idx] = sample_order<kOrder>(flo, P.fnx, P.fny, P.fnz, P.flo_ijk, P.pad, pos[0], pos[1], pos[2]);
+        }
+    }
+}
+
 __global__ void k_histogram(long long nv, int rb, int fb, const float *__restrict__ ref,
                             const float *__restrict__ war, const int32_t *__restrict__ mask,
                             uint32_t *__restrict__ ghist) {
@@ -1159,6 +1265,52 @@ extern "C" nrb_status nrb_resample_image(const nrb_geometry *g, const float *flo
                                          const int32_t *mask, float padding, float *warped,
                                          void *stream) {
     return resample_common(g, flo, def, mask, padding, warped, false, stream);
+}
+
+namespace nrb {
+nrb_status resample_order(const nrb_geometry *g, const float *flo, const float *def, const int32_t *mask,
+                          int order, float padding, float *warped, cudaStream_t st) {
+    if (!g || !flo || !def || !warped) return fail(NRB_ERR_INVALID, "resample: null pointer");
+    if (order != 0 && order != 1 && order != 3)
+        return fail(NRB_ERR_UNSUPPORTED, "resample: interpolation order must be 0 (nearest), 1 (linear) or 3 (cubic spline)");
+    const long long nv = nvox(g->ref_dim);
+    if (nv <= 0) return fail(NRB_ERR_INVALID, "resample: empty reference");
+    const int threads = 256;
+    const int grid = (int)std::min<long long>((nv + threads - 1) / threads, 64LL * sm_count());
+    const Mat34 M = to_mat34(g->flo_ijk);
+    const int fx = g->flo_dim[0], fy = g->flo_dim[1], fz = g->flo_dim[2];
+    if (order == 0)
+        k_resample_order<0><<<grid, threads, 0, st>>>(nv, fx, fy, fz, M, padding, flo, def, mask, warped);
+    else if (order == 1)
+        k_resample_order<1><<<grid, threads, 0, st>>>(nv, fx, fy, fz, M, padding, flo, def, mask, warped);
+    else
+        k_resample_order<3><<<grid, threads, 0, st>>>(nv, fx, fy, fz, M, padding, flo, def, mask, warped);
+    NRB_LAUNCHED("k_resample_order");
+    return NRB_OK;
+}
+}  // namespace nrb
+
+extern "C" nrb_status nrb_resample_image_order(const nrb_geometry *g, const float *flo, const float *def,
+                                               const int32_t *mask, int order, float padding, float *warped,
+                                               void *stream) {
+    return resample_order(g, flo, def, mask, order, padding, warped, as_stream(stream));
+}
+
+extern "C" nrb_status nrb_f3d_warped_image(const nrb_geometry *g, const float *flo, const float *cpp, int order,
+                                           float padding, float *warped, void *stream) {
+    if (!g || !flo || !cpp || !warped) return fail(NRB_ERR_INVALID, "nrb_f3d_warped_image: null pointer");
+    NRB_TRY(validate_geometry(g));
+    if (order != 0 && order != 1 && order != 3)
+        return fail(NRB_ERR_UNSUPPORTED, "nrb_f3d_warped_image: interpolation order must be 0, 1 or 3");
+    const WalkPlan W = plan_walk(g, TY_DEFORMATION, deformation_slots, 0);
+    const WalkParams P = make_params(W, g, padding, 0, 0);
+    const size_t smem = walk_smem_bytes(W);
+    auto kernel = order == 0 ? k_warp_order<0> : order == 1 ? k_warp_order<1> : k_warp_order<3>;
+    int grid = 0;
+    NRB_TRY(persistent_grid(kernel, 32 * W.ty, smem, P.nitems, grid));
+    kernel<<<grid, 32 * W.ty, smem, as_stream(stream)>>>(P, cpp, flo, warped);
+    NRB_LAUNCHED("k_warp_order");
+    return NRB_OK;
 }
 
 extern "C" nrb_status nrb_get_image_gradient(const nrb_geometry *g, const float *flo, const float *def,

@@ -51,6 +51,14 @@ def test_invalid_arguments_are_reported():
     assert lib.nrb_nmi_create(2, 68, ctypes.byref(out)) == 1  # NRB_ERR_INVALID
     assert b"bins" in lib.nrb_last_error()
     assert lib.nrb_get_deformation_field(None, None, None, None, None) == 1
+    # interpolation orders other than 0, 1 and 3 are refused before any device work
+    g = nrb.make_geometry((8, 8, 8), (1.0, 1.0, 1.0), nrb.identity_header((1.0, 1.0, 1.0)), (8, 8, 8), (1.0, 1.0, 1.0),
+                          nrb.identity_header((1.0, 1.0, 1.0)), (5, 5, 5), (5.0, 5.0, 5.0),
+                          nrb.identity_header((5.0, 5.0, 5.0), (-5.0, -5.0, -5.0)))
+    fake = ctypes.c_void_p(16)  # never dereferenced: the order check comes first
+    assert lib.nrb_resample_image_order(ctypes.byref(g), fake, fake, None, 2, ctypes.c_float(0.0), fake, None) == 2
+    assert b"order" in lib.nrb_last_error()
+    assert lib.nrb_f3d_warped_image(ctypes.byref(g), fake, fake, 4, ctypes.c_float(0.0), fake, None) == 2
 
 
 def test_footprint_is_host_only_and_monotone():
