@@ -309,6 +309,38 @@ nrb_status nrb_f3d_register_device(const float *ref, const float *flo, const int
 nrb_status nrb_f3d_warped_image(const nrb_geometry *g, const float *flo, const float *cpp, int order,
                                 float padding, float *warped, void *stream);
 
+/* ---- NIfTI-1 images (reg-io/_reg_ReadWriteImage.cpp, reg-io/niftilib) ----------------------- */
+
+/* A host image as the request path of a registration carries it. */
+typedef struct nrb_image {
+    int32_t dim[3];         /* nx, ny, nz (absent axes 1) */
+    int32_t nvol;           /* volumes: product of dims 4..7 (1: scalar image, 3: vector image) */
+    float pixdim[3];        /* spacing in mm */
+    float xyz[16];          /* voxel -> mm: the sform when sform_code > 0, else the qform, else the
+                             * spacings on the diagonal (Content::GetXYZMatrix's choice) */
+    float ijk[16];          /* mm -> voxel */
+    int32_t xform_code;     /* code of the form xyz came from (0: spacings only) */
+    int32_t intent_code;    /* NIfTI intent (1007: vector) */
+    float intent_p1;        /* NiftyReg transformation type for a grid (2: cubic B-spline grid) */
+    char intent_name[16];   /* "NREG_TRANS" for NiftyReg transformations */
+    float *data;            /* host float32, nvol * nx * ny * nz, x fastest; owned by the library
+                             * after nrb_image_read (free with nrb_image_free), by the caller when
+                             * passed to nrb_image_write */
+} nrb_image;
+
+/* Reads a single-file NIfTI-1 image (.nii or .nii.gz) as reg_io_ReadImageFile does
+ * (reg-io/_reg_ReadWriteImage.cpp:51-81, with reg_checkAndCorrectDimension,
+ * reg-lib/cpu/_reg_tools.cpp:13-71): any integer or real datatype converted to float and scaled
+ * by scl_slope / scl_inter (slope 0 = 1); micron and metre spacings converted to mm. */
+nrb_status nrb_image_read(const char *path, nrb_image *out);
+/* Frees the data of an image from nrb_image_read. */
+void nrb_image_free(nrb_image *img);
+/* Writes a float32 single-file NIfTI-1 image (.nii, or .nii.gz compressed): xyz as the sform
+ * (code xform_code, or 1 when 0), no qform, nvol > 1 as the 5th axis with the intent fields, the
+ * layout NiftyReg uses for grids and deformation fields (reg_io_WriteImageFile,
+ * reg-io/_reg_ReadWriteImage.cpp:83-120). */
+nrb_status nrb_image_write(const char *path, const nrb_image *img);
+
 /* ---- batched and served registrations (no counterpart in the reference) -------------------- */
 
 /* One registration request: host images (valid until the request completes), the reference's

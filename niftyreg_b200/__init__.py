@@ -65,6 +65,14 @@ class F3dParams(ctypes.Structure):
                 ("host_loop", ctypes.c_int32), ("floating_margin", ctypes.c_int32)]
 
 
+class Image(ctypes.Structure):
+    """nrb_image: a host NIfTI image (float32 data, orientation as NiftyReg picks it)."""
+    _fields_ = [("dim", _I3), ("nvol", ctypes.c_int32), ("pixdim", _F3), ("xyz", ctypes.c_float * 16),
+                ("ijk", ctypes.c_float * 16), ("xform_code", ctypes.c_int32), ("intent_code", ctypes.c_int32),
+                ("intent_p1", ctypes.c_float), ("intent_name", ctypes.c_char * 16),
+                ("data", ctypes.POINTER(ctypes.c_float))]
+
+
 class F3dResult(ctypes.Structure):
     _fields_ = [("cpp_dim", _I3), ("final_nmi", ctypes.c_double), ("final_be", ctypes.c_double),
                 ("final_objective", ctypes.c_double), ("objective_evaluations", ctypes.c_int64),
@@ -216,6 +224,39 @@ def get_deformation_field(g, cpp, deformation, mask=None, stream=None):
 def resample_image(g, flo, deformation, warped, padding=math.nan, mask=None, stream=None):
     check(lib().nrb_resample_image(ctypes.byref(g), _p(flo), _p(deformation), _p(mask), ctypes.c_float(padding),
                                    _p(warped), _s(stream)))
+
+
+def read_image(path):
+    """A NIfTI-1 file (.nii, .nii.gz) as (data [nvol, nz, ny, nx] float32, pixdim, xyz 4x4), read as
+    NiftyReg reads it."""
+    img = Image()
+    check(lib().nrb_image_read(str(path).encode(), ctypes.byref(img)))
+    try:
+        nx, ny, nz = list(img.dim)
+        n = nx * ny * nz * img.nvol
+        data = np.ctypeslib.as_array(img.data, shape=(n,)).copy().reshape(img.nvol, nz, ny, nx)
+        return data, tuple(float(v) for v in img.pixdim), np.array(img.xyz, np.float32).reshape(4, 4)
+    finally:
+        lib().nrb_image_free(ctypes.byref(img))
+
+
+def write_image(path, data, pixdim, xyz, intent_code=0, intent_p1=0.0, intent_name=b""):
+    """Writes data [nvol, nz, ny, nx] (or [nz, ny, nx]) as a float32 NIfTI-1 file with xyz as the sform."""
+    a = np.ascontiguousarray(data, np.float32)
+    if a.ndim == 3:
+        a = a[None]
+    nvol, nz, ny, nx = a.shape
+    img = Image()
+    img.dim[:] = [nx, ny, nz]
+    img.nvol = nvol
+    img.pixdim[:] = [float(v) for v in pixdim]
+    img.xyz[:] = [float(v) for v in np.asarray(xyz, np.float32).reshape(16)]
+    img.xform_code = 1
+    img.intent_code = int(intent_code)
+    img.intent_p1 = float(intent_p1)
+    img.intent_name = intent_name
+    img.data = a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    check(lib().nrb_image_write(str(path).encode(), ctypes.byref(img)))
 
 
 def resample_image_order(g, flo, deformation, warped, order, padding=math.nan, mask=None, stream=None):

@@ -103,6 +103,16 @@ class Ref:
                               _i(_i3(mask)) if mask is not None else None, ctypes.c_float(pad), _f(w))
         return w
 
+    def image_read(self, path):
+        """(dim, nvol, pixdim, xyz, data) of a single-file NIfTI image as the reference reads it."""
+        dim, nvol, pix, xyz = np.zeros(3, np.int32), ctypes.c_int(0), np.zeros(3, np.float32), np.zeros(16, np.float32)
+        p = str(path).encode()
+        if self.lib.ref_image_read(p, _i(dim), ctypes.byref(nvol), _f(pix), _f(xyz), None) != 0:
+            raise OSError(f"reference reader failed on {path}")
+        data = np.zeros(int(np.prod(dim)) * nvol.value, np.float32)
+        self.lib.ref_image_read(p, _i(dim), ctypes.byref(nvol), _f(pix), _f(xyz), _f(data))
+        return dim, nvol.value, pix, xyz.reshape(4, 4), data
+
     def resample_order(self, flo, fdim, fpix, fxyz, dfield, rdim, rpix, rxyz, order, mask=None, pad=np.nan,
                        warped_init=None):
         w = np.zeros(int(np.prod(rdim)), np.float32) if warped_init is None else _f3(warped_init).copy()

@@ -155,6 +155,36 @@ int ref_resample(const float *flo, const int *fdim, const float *fpix, const flo
     return 0;
 }
 
+// reg_io_ReadImageFile's reading of a single-file NIfTI image (reg-io/_reg_ReadWriteImage.cpp:
+// 51-81): niftilib, then reg_checkAndCorrectDimension; the voxel -> mm matrix Content picks (the
+// sform when sform_code > 0, else the qform); data converted to float (reg_tools_changeDatatype)
+// and scaled by scl_slope / scl_inter as the intensity rescale does. With data == nullptr only the
+// sizes are returned.
+int ref_image_read(const char *path, int *dim, int *nvol, float *pixdim, float *xyz, float *data) {
+    nifti_image *im = nifti_image_read(path, data != nullptr);
+    if (!im) return -1;
+    reg_checkAndCorrectDimension(im);
+    for (int i = 0; i < 3; ++i) {
+        dim[i] = im->dim[i + 1];
+        pixdim[i] = im->pixdim[i + 1];
+    }
+    long long nv = 1;
+    for (int i = 4; i <= 7; ++i) nv *= im->dim[i] > 0 ? im->dim[i] : 1;
+    *nvol = (int)nv;
+    const mat44& m = im->sform_code > 0 ? im->sto_xyz : im->qto_xyz;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) xyz[4 * i + j] = m.m[i][j];
+    if (data) {
+        reg_tools_changeDatatype<float>(im);
+        const float slope = im->scl_slope == 0 ? 1.f : im->scl_slope, inter = im->scl_inter;
+        const float *src = static_cast<float *>(im->data);
+        for (size_t i = 0; i < im->nvox; ++i)
+            data[i] = (slope == 1.f && inter == 0.f) ? src[i] : (float)((double)src[i] * slope + inter);
+    }
+    nifti_image_free(im);
+    return 0;
+}
+
 // _reg_resampling.cpp:638-692 with the interpolation order (0 nearest, 1 linear, 3 cubic spline)
 int ref_resample_order(const float *flo, const int *fdim, const float *fpix, const float *fxyz,
                        const float *def, const int *rdim, const float *rpix, const float *rxyz,
