@@ -319,7 +319,8 @@ typedef struct nrb_image {
     float xyz[16];          /* voxel -> mm: the sform when sform_code > 0, else the qform, else the
                              * spacings on the diagonal (Content::GetXYZMatrix's choice) */
     float ijk[16];          /* mm -> voxel */
-    int32_t xform_code;     /* code of the form xyz came from (0: spacings only) */
+    int32_t sform_code;     /* as read (xyz is the sform when > 0) */
+    int32_t qform_code;     /* as read (xyz is the qform when > 0 and sform_code is 0) */
     int32_t intent_code;    /* NIfTI intent (1007: vector) */
     float intent_p1;        /* NiftyReg transformation type for a grid (2: cubic B-spline grid) */
     char intent_name[16];   /* "NREG_TRANS" for NiftyReg transformations */
@@ -336,10 +337,29 @@ nrb_status nrb_image_read(const char *path, nrb_image *out);
 /* Frees the data of an image from nrb_image_read. */
 void nrb_image_free(nrb_image *img);
 /* Writes a float32 single-file NIfTI-1 image (.nii, or .nii.gz compressed): xyz as the sform
- * (code xform_code, or 1 when 0), no qform, nvol > 1 as the 5th axis with the intent fields, the
+ * (code sform_code, else qform_code, else 1), no qform, nvol > 1 as the 5th axis with the intent fields, the
  * layout NiftyReg uses for grids and deformation fields (reg_io_WriteImageFile,
  * reg-io/_reg_ReadWriteImage.cpp:83-120). */
 nrb_status nrb_image_write(const char *path, const nrb_image *img);
+
+/* reg_f3d<float>::Run on two host images with their own dims, spacings and orientations (from
+ * nrb_image_read, or filled by the caller: xyz is used as given, as an sform when sform_code > 0),
+ * each pyramid built along its own axes, the grid oriented like the reference
+ * (reg_createControlPointGrid, reg-lib/cpu/_reg_localTrans.cpp:21-128). Results, allocated by the
+ * library (free with nrb_image_free): cpp_out (required) the final control-point grid, a vector
+ * image of 3 planes tagged as NiftyReg tags grids (intent 1007, "NREG_TRANS", p1 = 2);
+ * warped_out (optional, may be NULL) the input floating image warped by it with cubic-spline
+ * interpolation on the reference geometry (reg_f3d::GetWarpedImage). Replaces reg_f3d::Run +
+ * GetControlPointPositionImage + GetWarpedImage (reg-lib/_reg_f3d.cpp:503-523). */
+nrb_status nrb_f3d_register_images(const nrb_image *ref, const nrb_image *flo, const nrb_f3d_params *p,
+                                   nrb_image *cpp_out, nrb_image *warped_out, nrb_f3d_result *result);
+
+/* A registration request on files, the way reg_f3d -ref -flo -cpp -res runs it
+ * (reg-apps/reg_f3d.cpp): both images read with nrb_image_read, nrb_f3d_register_images, the grid
+ * written to cpp_path and, when res_path is not NULL, the warped image to res_path (NIfTI-1,
+ * .nii or .nii.gz). */
+nrb_status nrb_f3d_register_files(const char *ref_path, const char *flo_path, const nrb_f3d_params *p,
+                                  const char *cpp_path, const char *res_path, nrb_f3d_result *result);
 
 /* ---- batched and served registrations (no counterpart in the reference) -------------------- */
 

@@ -68,7 +68,8 @@ class F3dParams(ctypes.Structure):
 class Image(ctypes.Structure):
     """nrb_image: a host NIfTI image (float32 data, orientation as NiftyReg picks it)."""
     _fields_ = [("dim", _I3), ("nvol", ctypes.c_int32), ("pixdim", _F3), ("xyz", ctypes.c_float * 16),
-                ("ijk", ctypes.c_float * 16), ("xform_code", ctypes.c_int32), ("intent_code", ctypes.c_int32),
+                ("ijk", ctypes.c_float * 16), ("sform_code", ctypes.c_int32), ("qform_code", ctypes.c_int32),
+                ("intent_code", ctypes.c_int32),
                 ("intent_p1", ctypes.c_float), ("intent_name", ctypes.c_char * 16),
                 ("data", ctypes.POINTER(ctypes.c_float))]
 
@@ -251,12 +252,59 @@ def write_image(path, data, pixdim, xyz, intent_code=0, intent_p1=0.0, intent_na
     img.nvol = nvol
     img.pixdim[:] = [float(v) for v in pixdim]
     img.xyz[:] = [float(v) for v in np.asarray(xyz, np.float32).reshape(16)]
-    img.xform_code = 1
+    img.sform_code = 1
     img.intent_code = int(intent_code)
     img.intent_p1 = float(intent_p1)
     img.intent_name = intent_name
     img.data = a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
     check(lib().nrb_image_write(str(path).encode(), ctypes.byref(img)))
+
+
+def _image_of(data, pixdim, xyz, sform_code=1):
+    a = np.ascontiguousarray(data, np.float32)
+    nz, ny, nx = a.shape
+    img = Image()
+    img.dim[:] = [nx, ny, nz]
+    img.nvol = 1
+    img.pixdim[:] = [float(v) for v in pixdim]
+    m = np.asarray(xyz, np.float32).reshape(4, 4)
+    img.xyz[:] = [float(v) for v in m.ravel()]
+    img.ijk[:] = [float(v) for v in _inv(m).ravel()]
+    img.sform_code = int(sform_code)
+    img.data = a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    return img, a
+
+
+def register_images(ref, ref_pixdim, ref_xyz, flo, flo_pixdim, flo_xyz, params, warped=True, sform_code=1):
+    """reg_f3d on two host volumes ([nz, ny, nx]) with their own spacings and voxel->mm matrices.
+    Returns (cpp [3, cz, cy, cx], grid voxel->mm 4x4, warped image or None, result)."""
+    r, keep_r = _image_of(ref, ref_pixdim, ref_xyz, sform_code)
+    f, keep_f = _image_of(flo, flo_pixdim, flo_xyz, sform_code)
+    cpp, w, res = Image(), Image(), F3dResult()
+    check(lib().nrb_f3d_register_images(ctypes.byref(r), ctypes.byref(f), ctypes.byref(params), ctypes.byref(cpp),
+                                        ctypes.byref(w) if warped else None, ctypes.byref(res)))
+    try:
+        cx, cy, cz = list(cpp.dim)
+        grid = np.ctypeslib.as_array(cpp.data, shape=(3 * cx * cy * cz,)).copy().reshape(3, cz, cy, cx)
+        gxyz = np.array(cpp.xyz, np.float32).reshape(4, 4)
+        out = None
+        if warped:
+            nz, ny, nx = np.shape(ref)
+            out = np.ctypeslib.as_array(w.data, shape=(nx * ny * nz,)).copy().reshape(nz, ny, nx)
+        return grid, gxyz, out, res
+    finally:
+        lib().nrb_image_free(ctypes.byref(cpp))
+        if warped:
+            lib().nrb_image_free(ctypes.byref(w))
+
+
+def register_files(ref_path, flo_path, params, cpp_path, res_path=None):
+    """A registration request on NIfTI files (reg_f3d -ref -flo -cpp [-res])."""
+    res = F3dResult()
+    check(lib().nrb_f3d_register_files(str(ref_path).encode(), str(flo_path).encode(), ctypes.byref(params),
+                                       str(cpp_path).encode(), str(res_path).encode() if res_path else None,
+                                       ctypes.byref(res)))
+    return res
 
 
 def resample_image_order(g, flo, deformation, warped, order, padding=math.nan, mask=None, stream=None):

@@ -284,11 +284,56 @@ int ceil_ref(float x) {
 // Voxel <-> mm of an image with identity orientation and origin `origin` (qform code 1, no
 // sform): qto_xyz = diag(pixdim) + origin, qto_ijk its inverse (nifti_mat44_inverse rounds the
 // double-precision inverse to float).
+// inverse of an affine voxel <-> mm matrix, in double (nifti_mat44_inverse's role)
+static bool affine_inverse(const float m[16], float out[16]) {
+    double a[3][3], t[3];
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) a[i][j] = m[4 * i + j];
+        t[i] = m[4 * i + 3];
+    }
+    const double det = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) -
+                       a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                       a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+    if (det == 0.0 || !std::isfinite(det)) return false;
+    double inv[3][3];
+    inv[0][0] = (a[1][1] * a[2][2] - a[1][2] * a[2][1]) / det;
+    inv[0][1] = (a[0][2] * a[2][1] - a[0][1] * a[2][2]) / det;
+    inv[0][2] = (a[0][1] * a[1][2] - a[0][2] * a[1][1]) / det;
+    inv[1][0] = (a[1][2] * a[2][0] - a[1][0] * a[2][2]) / det;
+    inv[1][1] = (a[0][0] * a[2][2] - a[0][2] * a[2][0]) / det;
+    inv[1][2] = (a[0][2] * a[1][0] - a[0][0] * a[1][2]) / det;
+    inv[2][0] = (a[1][0] * a[2][1] - a[1][1] * a[2][0]) / det;
+    inv[2][1] = (a[0][1] * a[2][0] - a[0][0] * a[2][1]) / det;
+    inv[2][2] = (a[0][0] * a[1][1] - a[0][1] * a[1][0]) / det;
+    for (int i = 0; i < 3; ++i) {
+        double s = 0.0;
+        for (int j = 0; j < 3; ++j) {
+            out[4 * i + j] = (float)inv[i][j];
+            s += inv[i][j] * t[j];
+        }
+        out[4 * i + 3] = (float)-s;
+    }
+    out[12] = out[13] = out[14] = 0.f;
+    out[15] = 1.f;
+    return true;
+}
+
+// Geometry of one image of the registration. An image whose voxel -> mm matrix is the spacing
+// on the diagonal keeps that form (the arithmetic of an identity orientation with an origin);
+// any other orientation is held in full in `m`. `sform`: the matrix came from an sform, whose
+// columns reg_createControlPointGrid scales for the grid (the qform's are rebuilt instead).
 struct Header {
     int32_t dim[3];
     float pixdim[3];
     float origin[3];
-    void xyz(float m[16]) const {
+    bool full = false, sform = false;
+    float m[16];
+    void xyz(float out[16]) const {
+        if (full) {
+            memcpy(out, m, 16 * sizeof(float));
+            return;
+        }
+        float *m = out;
         memset(m, 0, 16 * sizeof(float));
         for (int i = 0; i < 3; ++i) {
             m[5 * i] = pixdim[i];
@@ -296,7 +341,12 @@ struct Header {
         }
         m[15] = 1.f;
     }
-    void ijk(float m[16]) const {
+    void ijk(float out[16]) const {
+        if (full) {
+            affine_inverse(m, out);
+            return;
+        }
+        float *m = out;
         memset(m, 0, 16 * sizeof(float));
         for (int i = 0; i < 3; ++i) {
             const double inv = 1.0 / (double)pixdim[i];
@@ -307,6 +357,89 @@ struct Header {
     }
     int64_t n() const { return (int64_t)dim[0] * dim[1] * dim[2]; }
 };
+
+// An input image's geometry: dims, spacings and, when given, its voxel -> mm matrix (from an
+// sform when `sform`). Without a matrix the image has the identity orientation at origin 0.
+struct ImageDesc {
+    int32_t dim[3];
+    float pixdim[3];
+    const float *xyz = nullptr;
+    bool sform = false;
+};
+
+static Header header_of(const ImageDesc& d) {
+    Header h{};
+    for (int i = 0; i < 3; ++i) {
+        h.dim[i] = d.dim[i];
+        h.pixdim[i] = d.pixdim[i];
+        h.origin[i] = 0.f;
+    }
+    if (d.xyz) {
+        const float *m = d.xyz;
+        const bool plain = m[1] == 0.f && m[2] == 0.f && m[4] == 0.f && m[6] == 0.f && m[8] == 0.f && m[9] == 0.f &&
+                           m[0] == d.pixdim[0] && m[5] == d.pixdim[1] && m[10] == d.pixdim[2];
+        if (plain) {
+            h.origin[0] = m[3];
+            h.origin[1] = m[7];
+            h.origin[2] = m[11];
+        } else {
+            h.full = true;
+            memcpy(h.m, m, 12 * sizeof(float));
+            h.m[12] = h.m[13] = h.m[14] = 0.f;
+            h.m[15] = 1.f;
+        }
+        h.sform = d.sform;
+    }
+    return h;
+}
+
+// reg_downsampleImage's header (reg-lib/cpu/_reg_tools.cpp:1344-1417): every axis whose size / 2
+// is at least 32 halves (ceil) and doubles its spacing and its matrix column (exact in float);
+// the origin stays
+static Header halve(const Header& src) {
+    Header dst = src;
+    for (int i = 0; i < 3; ++i) {
+        const bool down = src.dim[i] / 2 >= 32;
+        dst.dim[i] = down && src.dim[i] > 1 ? ceil_ref((float)(src.dim[i] / 2.0)) : src.dim[i];
+        dst.pixdim[i] = down ? src.pixdim[i] * 2.0f : src.pixdim[i];
+        if (down && src.full)
+            for (int r = 0; r < 3; ++r) dst.m[4 * r + i] = src.m[4 * r + i] * 2.0f;
+    }
+    return dst;
+}
+
+// The control-point grid of reg_createControlPointGrid / reg_spline_refineControlPointGrid
+// (reg-lib/cpu/_reg_localTrans.cpp:21-128, 1860-1925) over reference `r` with spacing `s` mm:
+// ceil(n * d / s + 3) nodes per axis, the reference's orientation (an sform's columns scaled by
+// the float ratio s / d; a qform's rebuilt with spacing s), the origin shifted by one node
+// (Mat44Mul of (-1, -1, -1), in double).
+static Header grid_header(const Header& r, const float s[3]) {
+    Header g{};
+    for (int i = 0; i < 3; ++i) {
+        g.dim[i] = ceil_ref((float)r.dim[i] * r.pixdim[i] / s[i] + 3.f);
+        g.pixdim[i] = s[i];
+        g.origin[i] = (float)((double)s[i] * -1.0 + (double)r.origin[i]);
+    }
+    if (!r.full && !r.sform) return g;
+    float rm[16];
+    r.xyz(rm);
+    g.full = true;
+    g.sform = r.sform;
+    for (int j = 0; j < 3; ++j) {
+        if (r.sform) {
+            const float ratio = s[j] / r.pixdim[j];
+            for (int i = 0; i < 3; ++i) g.m[4 * i + j] = rm[4 * i + j] * ratio;
+        } else {
+            for (int i = 0; i < 3; ++i) g.m[4 * i + j] = (float)((double)rm[4 * i + j] / r.pixdim[j] * s[j]);
+        }
+    }
+    for (int i = 0; i < 3; ++i)
+        g.m[4 * i + 3] = (float)((double)g.m[4 * i] * -1.0 + (double)g.m[4 * i + 1] * -1.0 +
+                                 (double)g.m[4 * i + 2] * -1.0 + (double)rm[4 * i + 3]);
+    g.m[12] = g.m[13] = g.m[14] = 0.f;
+    g.m[15] = 1.f;
+    return g;
+}
 
 // Every buffer of a registration is allocated and freed in the order of the registration's
 // stream, so concurrent registrations on other streams never wait for each other's frees.
@@ -340,8 +473,11 @@ class F3dRegistration {
 public:
     F3dRegistration(const nrb_f3d_params& p, cudaStream_t st): p_(p), st_(st) {}
 
-    nrb_status Run(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3],
-                   float *cpp_out, int64_t cap, nrb_f3d_result *res);
+    // warped_out (optional, host or device): the floating image warped by the final grid with
+    // cubic-spline interpolation (reg_f3d::GetWarpedImage), reference-sized
+    nrb_status Run(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd, float *cpp_out,
+                   int64_t cap, nrb_f3d_result *res, float *warped_out = nullptr);
+    const Header& grid() const { return grid_; }
 
 private:
     // reg_f3d::GetObjectiveFunctionValue (_reg_f3d.cpp:443-462)
@@ -436,14 +572,14 @@ private:
     nrb_status CaptureGradient(cudaStream_t cs);
     nrb_status CaptureLineStep(cudaStream_t cs, cudaGraphConditionalHandle line);
 
-    nrb_status BuildPyramid(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3]);
+    nrb_status BuildPyramid(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd);
     nrb_status CreateGrid();
     nrb_status InitLevel(int level, float& max_step);
 
     nrb_f3d_params p_;
     cudaStream_t st_;
     int levels_ = 0;
-    std::vector<Header> hdr_;
+    std::vector<Header> hdr_, fhdr_;  // reference and floating pyramids
     std::vector<DevBuf> ref_pyr_, flo_pyr_;
     // current level
     nrb_geometry g_{};
@@ -666,40 +802,38 @@ nrb_status F3dRegistration::RunLevelGraph(float max_step, float smallest_size, f
 // reg_createImagePyramid (reg-lib/cpu/_reg_tools.cpp:1705-1733): the finest level is the input,
 // each coarser level halves (ceil) every axis whose current size / 2 is at least 32, after a
 // Gaussian smoothing.
-nrb_status F3dRegistration::BuildPyramid(const float *ref, const float *flo, const int32_t dim[3],
-                                         const float pixdim[3]) {
+nrb_status F3dRegistration::BuildPyramid(const float *ref, const float *flo, const ImageDesc& rd,
+                                         const ImageDesc& fd) {
     hdr_.assign(levels_, Header{});
+    fhdr_.assign(levels_, Header{});
     ref_pyr_ = std::vector<DevBuf>(levels_);
     flo_pyr_ = std::vector<DevBuf>(levels_);
-    Header& fine = hdr_[levels_ - 1];
-    for (int i = 0; i < 3; ++i) {
-        fine.dim[i] = dim[i];
-        fine.pixdim[i] = pixdim[i];
-        fine.origin[i] = 0.f;
-    }
-    NRB_TRY(ref_pyr_[levels_ - 1].alloc(fine.n(), st_));
-    NRB_TRY(flo_pyr_[levels_ - 1].alloc(fine.n(), st_));
-    NRB_CUDA(cudaMemcpyAsync(ref_pyr_[levels_ - 1].p, ref, fine.n() * 4, cudaMemcpyDefault, st_));
-    NRB_CUDA(cudaMemcpyAsync(flo_pyr_[levels_ - 1].p, flo, fine.n() * 4, cudaMemcpyDefault, st_));
+    hdr_[levels_ - 1] = header_of(rd);
+    fhdr_[levels_ - 1] = header_of(fd);
+    const Header& rf = hdr_[levels_ - 1];
+    const Header& ff = fhdr_[levels_ - 1];
+    NRB_TRY(ref_pyr_[levels_ - 1].alloc(rf.n(), st_));
+    NRB_TRY(flo_pyr_[levels_ - 1].alloc(ff.n(), st_));
+    NRB_CUDA(cudaMemcpyAsync(ref_pyr_[levels_ - 1].p, ref, rf.n() * 4, cudaMemcpyDefault, st_));
+    NRB_CUDA(cudaMemcpyAsync(flo_pyr_[levels_ - 1].p, flo, ff.n() * 4, cudaMemcpyDefault, st_));
     if (levels_ == 1) return NRB_OK;
     DevBuf tmp;
-    NRB_TRY(tmp.alloc(4 * fine.n(), st_));
+    NRB_TRY(tmp.alloc(4 * std::max(rf.n(), ff.n()), st_));
     for (int l = levels_ - 2; l >= 0; --l) {
-        const Header& src = hdr_[l + 1];
-        Header& dst = hdr_[l];
-        for (int i = 0; i < 3; ++i) {
-            const bool down = src.dim[i] / 2 >= 32;
-            dst.dim[i] = down && src.dim[i] > 1 ? ceil_ref((float)(src.dim[i] / 2.0)) : src.dim[i];
-            dst.pixdim[i] = down ? src.pixdim[i] * 2.0f : src.pixdim[i];
-            dst.origin[i] = src.origin[i];
-        }
+        // each image halves along its own axes
+        hdr_[l] = halve(hdr_[l + 1]);
+        fhdr_[l] = halve(fhdr_[l + 1]);
         float nxyz[16], oijk[16];
-        dst.xyz(nxyz);
-        src.ijk(oijk);
-        NRB_TRY(ref_pyr_[l].alloc(dst.n(), st_));
-        NRB_TRY(flo_pyr_[l].alloc(dst.n(), st_));
-        NRB_TRY(smooth_and_downsample(ref_pyr_[l + 1].p, src.dim, ref_pyr_[l].p, dst.dim, nxyz, oijk, tmp.p, st_));
-        NRB_TRY(smooth_and_downsample(flo_pyr_[l + 1].p, src.dim, flo_pyr_[l].p, dst.dim, nxyz, oijk, tmp.p, st_));
+        NRB_TRY(ref_pyr_[l].alloc(hdr_[l].n(), st_));
+        hdr_[l].xyz(nxyz);
+        hdr_[l + 1].ijk(oijk);
+        NRB_TRY(smooth_and_downsample(ref_pyr_[l + 1].p, hdr_[l + 1].dim, ref_pyr_[l].p, hdr_[l].dim, nxyz, oijk, tmp.p,
+                                      st_));
+        NRB_TRY(flo_pyr_[l].alloc(fhdr_[l].n(), st_));
+        fhdr_[l].xyz(nxyz);
+        fhdr_[l + 1].ijk(oijk);
+        NRB_TRY(smooth_and_downsample(flo_pyr_[l + 1].p, fhdr_[l + 1].dim, flo_pyr_[l].p, fhdr_[l].dim, nxyz, oijk,
+                                      tmp.p, st_));
     }
     return NRB_OK;  // tmp is freed in stream order
 }
@@ -715,12 +849,7 @@ nrb_status F3dRegistration::CreateGrid() {
         spacing_mm_[i] = s < 0 ? s * -hdr_[levels_ - 1].pixdim[i] : s;
         spacing[i] = spacing_mm_[i] * powf(2.f, (float)(levels_ - 1));
     }
-    for (int i = 0; i < 3; ++i) {
-        grid_.dim[i] = ceil_ref((float)r.dim[i] * r.pixdim[i] / spacing[i] + 3.f);
-        grid_.pixdim[i] = spacing[i];
-        // the origin shifted by one node: Mat44Mul(qto_xyz, (-1,-1,-1)) in double
-        grid_.origin[i] = (float)((double)spacing[i] * -1.0 + (double)r.origin[i]);
-    }
+    grid_ = grid_header(r, spacing);
     float cxyz[16];
     grid_.xyz(cxyz);
     NRB_TRY(cur_.alloc(3 * grid_.n(), st_));
@@ -730,6 +859,7 @@ nrb_status F3dRegistration::CreateGrid() {
 // reg_f3d::InitCurrentLevel (_reg_f3d.cpp:92-132) + InitialiseSimilarity + SetOptimiser
 nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
     const Header& r = hdr_[level];
+    const Header& fh = fhdr_[level];
     max_step = r.pixdim[0] > r.pixdim[1] ? r.pixdim[0] : r.pixdim[1];
     max_step = r.pixdim[2] > max_step ? r.pixdim[2] : max_step;
     if (level == 0) {
@@ -737,12 +867,8 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
     } else {
         be_w_ = be_w_ * 16.f;
         // reg_spline_refineControlPointGrid onto this level's reference
-        Header ng;
-        for (int i = 0; i < 3; ++i) {
-            ng.pixdim[i] = grid_.pixdim[i] / 2.0f;
-            ng.dim[i] = ceil_ref((float)r.dim[i] * r.pixdim[i] / ng.pixdim[i] + 3.f);
-            ng.origin[i] = (float)((double)ng.pixdim[i] * -1.0 + (double)r.origin[i]);
-        }
+        const float half[3] = { grid_.pixdim[0] / 2.0f, grid_.pixdim[1] / 2.0f, grid_.pixdim[2] / 2.0f };
+        const Header ng = grid_header(r, half);
         DevBuf refined;
         NRB_TRY(refined.alloc(3 * ng.n(), st_));
         NRB_TRY(grid_refine(grid_.dim, cur_.p, ng.dim, refined.p, st_));
@@ -754,15 +880,15 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
     for (int i = 0; i < 3; ++i) {
         g.ref_dim[i] = r.dim[i];
         g.ref_pixdim[i] = r.pixdim[i];
-        g.flo_dim[i] = r.dim[i];
-        g.flo_pixdim[i] = r.pixdim[i];
+        g.flo_dim[i] = fh.dim[i];
+        g.flo_pixdim[i] = fh.pixdim[i];
         g.cpp_dim[i] = grid_.dim[i];
         g.cpp_pixdim[i] = grid_.pixdim[i];
     }
     r.xyz(g.ref_xyz);
     r.ijk(g.ref_ijk);
-    r.xyz(g.flo_xyz);
-    r.ijk(g.flo_ijk);
+    fh.xyz(g.flo_xyz);
+    fh.ijk(g.flo_ijk);
     grid_.xyz(g.cpp_xyz);
     grid_.ijk(g.cpp_ijk);
     nc_ = grid_.n();
@@ -780,13 +906,13 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
     if (!nmi_.h) NRB_TRY(nmi_create_on(p_.ref_bins + 4, p_.flo_bins + 4, st_, &nmi_.h));
     // reg_nmi::InitialiseMeasure: rescale both images to [2, bins - 3]
     NRB_TRY(rescale_with(ref_.p, r.n(), 2.f, (float)(p_.ref_bins + 4) - 3.f, ws_.h->fred, st_));
-    NRB_TRY(rescale_with(flo_.p, r.n(), 2.f, (float)(p_.flo_bins + 4) - 3.f, ws_.h->fred, st_));
+    NRB_TRY(rescale_with(flo_.p, fh.n(), 2.f, (float)(p_.flo_bins + 4) - 3.f, ws_.h->fred, st_));
     // the floating image with a margin of padding values, which the voxel passes sample without
     // clamping; the dense copy is released
     margin_ = p_.floating_margin;
     if (margin_ > 0) {
-        NRB_TRY(flo_pad_.alloc(padded_voxels(r.dim, margin_), st_));
-        NRB_TRY(pad_volume(flo_.p, r.dim, margin_, pad_, flo_pad_.p, &flo_org_, st_));
+        NRB_TRY(flo_pad_.alloc(padded_voxels(fh.dim, margin_), st_));
+        NRB_TRY(pad_volume(flo_.p, fh.dim, margin_, pad_, flo_pad_.p, &flo_org_, st_));
         dev_free(flo_.p, flo_.st);
         flo_.p = nullptr;
     } else {
@@ -802,8 +928,8 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
     return NRB_OK;
 }
 
-nrb_status F3dRegistration::Run(const float *ref, const float *flo, const int32_t dim[3], const float pixdim[3],
-                                float *cpp_out, int64_t cap, nrb_f3d_result *res) {
+nrb_status F3dRegistration::Run(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd,
+                                float *cpp_out, int64_t cap, nrb_f3d_result *res, float *warped_out) {
     const auto t0 = std::chrono::steady_clock::now();
     levels_ = p_.levels;
     if (levels_ < 1) return fail(NRB_ERR_INVALID, "registration: levels must be >= 1");
@@ -823,7 +949,7 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const int32_
     NRB_CUDA(cudaMallocAsync(&obj_, sizeof(nrb_objective), st_));
     NRB_CUDA(cudaMemsetAsync(obj_, 0, sizeof(nrb_objective), st_));
     const auto tp = std::chrono::steady_clock::now();
-    NRB_TRY(BuildPyramid(ref, flo, dim, pixdim));
+    NRB_TRY(BuildPyramid(ref, flo, rd, fd));
     NRB_TRY(CreateGrid());
     if (p_.verbose) {
         NRB_CUDA(cudaStreamSynchronize(st_));
@@ -874,6 +1000,33 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const int32_
         if (cap < n) return fail(NRB_ERR_INVALID, "registration: cpp_out capacity too small");
         NRB_CUDA(cudaMemcpyAsync(cpp_out, cur_.p, n * sizeof(float), cudaMemcpyDefault, st_));
     }
+    if (warped_out) {
+        // reg_f3d::GetWarpedImage: the input floating image (not rescaled) through the final grid
+        const Header& rf = hdr_[levels_ - 1];
+        const Header& ff = fhdr_[levels_ - 1];
+        nrb_geometry wg{};
+        for (int i = 0; i < 3; ++i) {
+            wg.ref_dim[i] = rf.dim[i];
+            wg.ref_pixdim[i] = rf.pixdim[i];
+            wg.flo_dim[i] = ff.dim[i];
+            wg.flo_pixdim[i] = ff.pixdim[i];
+            wg.cpp_dim[i] = grid_.dim[i];
+            wg.cpp_pixdim[i] = grid_.pixdim[i];
+        }
+        rf.xyz(wg.ref_xyz);
+        rf.ijk(wg.ref_ijk);
+        ff.xyz(wg.flo_xyz);
+        ff.ijk(wg.flo_ijk);
+        grid_.xyz(wg.cpp_xyz);
+        grid_.ijk(wg.cpp_ijk);
+        DevBuf fin, wout;
+        NRB_TRY(fin.alloc(ff.n(), st_));
+        NRB_TRY(wout.alloc(rf.n(), st_));
+        NRB_CUDA(cudaMemcpyAsync(fin.p, flo, ff.n() * sizeof(float), cudaMemcpyDefault, st_));
+        NRB_TRY(nrb_f3d_warped_image(&wg, fin.p, cur_.p, 3, pad_, wout.p, st_));
+        NRB_CUDA(cudaMemcpyAsync(warped_out, wout.p, rf.n() * sizeof(float), cudaMemcpyDefault, st_));
+        NRB_CUDA(cudaStreamSynchronize(st_));
+    }
     NRB_CUDA(cudaFreeAsync(obj_, st_));
     obj_ = nullptr;
     NRB_CUDA(cudaStreamSynchronize(st_));
@@ -922,7 +1075,12 @@ nrb_status register_on_stream(const float *ref, const float *flo, const int32_t 
     if (st) keep_pool(registration_footprint(dim, pixdim, p));
     F3dRegistration reg(*p, st);
     reg.UseGraphs(p->host_loop == 0);
-    return reg.Run(ref, flo, dim, pixdim, cpp_out, cap, res);
+    ImageDesc d;
+    for (int i = 0; i < 3; ++i) {
+        d.dim[i] = dim[i];
+        d.pixdim[i] = pixdim[i];
+    }
+    return reg.Run(ref, flo, d, d, cpp_out, cap, res);
 }
 
 // Peak device bytes of one registration: the resident pyramid plus the larger of the pyramid
@@ -994,6 +1152,115 @@ extern "C" nrb_status nrb_f3d_register_device(const float *ref, const float *flo
                                               int64_t cpp_capacity, nrb_f3d_result *result, void *stream) {
     NRB_TRY(check_register_args(ref, flo, dim, pixdim, p));
     return register_on_stream(ref, flo, dim, pixdim, p, cpp_out, cpp_capacity, result, as_stream(stream));
+}
+
+static nrb_status check_image(const nrb_image *img, const char *what) {
+    if (!img || !img->data) return fail(NRB_ERR_INVALID, std::string("registration: null ") + what + " image");
+    if (img->nvol != 1) return fail(NRB_ERR_INVALID, std::string("registration: the ") + what + " image must be scalar");
+    for (int i = 0; i < 3; ++i)
+        if (img->dim[i] < 2 || !(img->pixdim[i] > 0))
+            return fail(NRB_ERR_INVALID, std::string("registration: the ") + what +
+                                             " image must be 3D with positive voxel sizes");
+    return NRB_OK;
+}
+
+extern "C" nrb_status nrb_f3d_register_images(const nrb_image *ref, const nrb_image *flo, const nrb_f3d_params *p,
+                                              nrb_image *cpp_out, nrb_image *warped_out, nrb_f3d_result *result) {
+    NRB_TRY(check_image(ref, "reference"));
+    NRB_TRY(check_image(flo, "floating"));
+    if (!p || !cpp_out) return fail(NRB_ERR_INVALID, "nrb_f3d_register_images: null pointer");
+    memset(cpp_out, 0, sizeof(*cpp_out));
+    if (warped_out) memset(warped_out, 0, sizeof(*warped_out));
+    ImageDesc rd, fd;
+    for (int i = 0; i < 3; ++i) {
+        rd.dim[i] = ref->dim[i];
+        rd.pixdim[i] = ref->pixdim[i];
+        fd.dim[i] = flo->dim[i];
+        fd.pixdim[i] = flo->pixdim[i];
+    }
+    rd.xyz = ref->xyz;
+    rd.sform = ref->sform_code > 0;
+    fd.xyz = flo->xyz;
+    fd.sform = flo->sform_code > 0;
+    int32_t cdim[3];
+    NRB_TRY(nrb_f3d_grid_dims(ref->dim, ref->pixdim, p, cdim));
+    const int64_t ncpp = 3LL * cdim[0] * cdim[1] * cdim[2];
+    const int64_t nref = (int64_t)ref->dim[0] * ref->dim[1] * ref->dim[2];
+    float *cpp = (float *)malloc((size_t)ncpp * sizeof(float));
+    float *warped = warped_out ? (float *)malloc((size_t)nref * sizeof(float)) : nullptr;
+    if (!cpp || (warped_out && !warped)) {
+        free(cpp);
+        free(warped);
+        return fail(NRB_ERR_OOM, "nrb_f3d_register_images: host allocation failed");
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+        free(cpp);
+        free(warped);
+        return fail(NRB_ERR_CUDA, "nrb_f3d_register_images: stream creation failed");
+    }
+    const int32_t *big = (int64_t)flo->dim[0] * flo->dim[1] * flo->dim[2] > nref ? flo->dim : ref->dim;
+    keep_pool(registration_footprint(big, ref->pixdim, p));
+    nrb_status s;
+    Header g{};
+    {
+        F3dRegistration reg(*p, st);
+        reg.UseGraphs(p->host_loop == 0);
+        s = reg.Run(ref->data, flo->data, rd, fd, cpp, ncpp, result, warped);
+        g = reg.grid();
+    }
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (s != NRB_OK) {
+        free(cpp);
+        free(warped);
+        return s;
+    }
+    for (int i = 0; i < 3; ++i) {
+        cpp_out->dim[i] = g.dim[i];
+        cpp_out->pixdim[i] = g.pixdim[i];
+    }
+    cpp_out->nvol = 3;
+    g.xyz(cpp_out->xyz);
+    g.ijk(cpp_out->ijk);
+    // the grid carries the reference's form codes (a qform when the reference has none)
+    cpp_out->sform_code = ref->sform_code;
+    cpp_out->qform_code = ref->sform_code + ref->qform_code > 0 ? ref->qform_code : 1;
+    cpp_out->intent_code = 1007;  // NIFTI_INTENT_VECTOR
+    cpp_out->intent_p1 = 2.f;     // CUB_SPLINE_GRID
+    strncpy(cpp_out->intent_name, "NREG_TRANS", sizeof(cpp_out->intent_name) - 1);
+    cpp_out->data = cpp;
+    if (warped_out) {
+        for (int i = 0; i < 3; ++i) {
+            warped_out->dim[i] = ref->dim[i];
+            warped_out->pixdim[i] = ref->pixdim[i];
+        }
+        warped_out->nvol = 1;
+        memcpy(warped_out->xyz, ref->xyz, sizeof(ref->xyz));
+        memcpy(warped_out->ijk, ref->ijk, sizeof(ref->ijk));
+        warped_out->sform_code = ref->sform_code;
+        warped_out->qform_code = ref->qform_code;
+        warped_out->data = warped;
+    }
+    if (result) result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return NRB_OK;
+}
+
+extern "C" nrb_status nrb_f3d_register_files(const char *ref_path, const char *flo_path, const nrb_f3d_params *p,
+                                             const char *cpp_path, const char *res_path, nrb_f3d_result *result) {
+    if (!ref_path || !flo_path || !p || !cpp_path) return fail(NRB_ERR_INVALID, "nrb_f3d_register_files: null pointer");
+    nrb_image ref{}, flo{}, cpp{}, warped{};
+    nrb_status s = nrb_image_read(ref_path, &ref);
+    if (s == NRB_OK) s = nrb_image_read(flo_path, &flo);
+    if (s == NRB_OK) s = nrb_f3d_register_images(&ref, &flo, p, &cpp, res_path ? &warped : nullptr, result);
+    if (s == NRB_OK) s = nrb_image_write(cpp_path, &cpp);
+    if (s == NRB_OK && res_path) s = nrb_image_write(res_path, &warped);
+    nrb_image_free(&ref);
+    nrb_image_free(&flo);
+    nrb_image_free(&cpp);
+    nrb_image_free(&warped);
+    return s;
 }
 
 extern "C" nrb_status nrb_f3d_register_host(const float *ref_host, const float *flo_host, const int32_t dim[3],

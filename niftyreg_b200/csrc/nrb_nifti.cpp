@@ -189,17 +189,14 @@ extern "C" nrb_status nrb_image_read(const char *path, nrb_image *out) {
 
     // orientation: sform, else qform, else the spacings (with the spacings as read)
     float xyz[16];
-    int code = 0;
     if (sform_code > 0) {
         for (int i = 0; i < 12; ++i) xyz[i] = h.get<float>(kOffSrow + 4 * i);
         xyz[12] = xyz[13] = xyz[14] = 0.f;
         xyz[15] = 1.f;
-        code = sform_code;
     } else if (qform_code > 0) {
         quaternion_matrix(h.get<float>(kOffQuatern), h.get<float>(kOffQuatern + 4), h.get<float>(kOffQuatern + 8),
                           h.get<float>(kOffQuatern + 12), h.get<float>(kOffQuatern + 16),
                           h.get<float>(kOffQuatern + 20), pix[1], pix[2], pix[3], pix[0] < 0 ? -1.0 : 1.0, xyz);
-        code = qform_code;
     } else {
         quaternion_matrix(0, 0, 0, 0, 0, 0, pix[1], pix[2], pix[3], 1.0, xyz);
     }
@@ -253,7 +250,8 @@ extern "C" nrb_status nrb_image_read(const char *path, nrb_image *out) {
         free(data);
         return fail(NRB_ERR_INVALID, "nrb_image_read: singular voxel-to-mm matrix");
     }
-    out->xform_code = code;
+    out->sform_code = sform_code > 0 ? sform_code : 0;
+    out->qform_code = qform_code > 0 ? qform_code : 0;
     out->intent_code = h.get<int16_t>(kOffIntentCode);
     out->intent_p1 = h.get<float>(kOffIntentP1);
     memcpy(out->intent_name, h.b.data() + kOffIntentName, 16);
@@ -303,7 +301,8 @@ extern "C" nrb_status nrb_image_write(const char *path, const nrb_image *img) {
     hdr[kOffXyztUnits] = 2;  // mm
     const char descrip[] = "niftyreg_b200";
     put(kOffDescrip, descrip, sizeof descrip);
-    const int16_t qcode = 0, scode = (int16_t)(img->xform_code > 0 ? img->xform_code : 1);
+    const int16_t qcode = 0,
+                  scode = (int16_t)(img->sform_code > 0 ? img->sform_code : img->qform_code > 0 ? img->qform_code : 1);
     put(kOffQformCode, &qcode, 2);
     put(kOffSformCode, &scode, 2);
     put(kOffSrow, img->xyz, 12 * sizeof(float));

@@ -192,6 +192,20 @@ class Ref:
             raise RuntimeError("ref_refine_grid: capacity")
         return out[:3 * int(np.prod(cdo))].copy(), cdo, cpo, cxo.reshape(4, 4)
 
+    def f3d_register2(self, ref, rdim, rpix, rxyz, flo, fdim, fpix, fxyz, levels, maxit, be, le, bins, spacing):
+        """reg_f3d<float> on a reference and a floating image with their own geometry: (cpp, cdim,
+        grid voxel->mm, [final NMI, final weighted BE, objective calls, gradient calls])."""
+        params = np.array([levels, maxit, be, le, bins, spacing, 0], np.float64)
+        cap = 3 * int(np.prod([int(np.ceil(n * p / abs(spacing * (p if spacing < 0 else 1))) + 4)
+                               for n, p in zip(rdim, rpix)])) + 64
+        cpp, cdim, cxyz, stats = np.zeros(cap, np.float32), np.zeros(3, np.int32), np.zeros(16, np.float32), np.zeros(4)
+        rc = self.lib.ref_f3d_register2(_f(_f3(ref)), _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)), _f(_f3(flo)),
+                                        _i(_i3(fdim)), _f(_f3(fpix)), _f(_m(fxyz)), _d(params), _i(cdim), _f(cpp),
+                                        ctypes.c_size_t(cap), _f(cxyz), _d(stats))
+        if rc != 0:
+            raise RuntimeError("ref_f3d_register2 failed")
+        return cpp[:3 * int(np.prod(cdim))].copy(), cdim, cxyz.reshape(4, 4), stats
+
     def f3d_register(self, ref, flo, dim, pix, xyz, levels, maxit, be, le, bins, spacing,
                      verbose=False):
         params = np.array([levels, maxit, be, le, bins, spacing, 1 if verbose else 0], np.float64)

@@ -382,4 +382,39 @@ int ref_f3d_register(const float *ref, const float *flo, const int *dim, const f
     return 0;
 }
 
+// the same registration with a reference and a floating image of their own dims, spacings and
+// voxel -> mm matrices (both sform images); also returns the final grid's voxel -> mm matrix
+int ref_f3d_register2(const float *ref, const int *rdim, const float *rpix, const float *rxyz, const float *flo,
+                      const int *fdim, const float *fpix, const float *fxyz, const double *params, int *cdim_out,
+                      float *cpp_out, size_t cap, float *cxyz_out, double *stats) {
+    NiftiImage r = MakeImage(rdim, rpix, rxyz), f = MakeImage(fdim, fpix, fxyz);
+    memcpy(r->data, ref, Nvox(rdim) * sizeof(float));
+    memcpy(f->data, flo, Nvox(fdim) * sizeof(float));
+    ShimF3d reg;
+    reg.SetReferenceImage(r);
+    reg.SetFloatingImage(f);
+    reg.SetLevelNumber(unsigned(params[0]));
+    reg.SetLevelToPerform(unsigned(params[0]));
+    reg.SetMaximalIterationNumber(unsigned(params[1]));
+    reg.SetBendingEnergyWeight(float(params[2]));
+    reg.SetLinearEnergyWeight(float(params[3]));
+    reg.UseNMISetReferenceBinNumber(0, int(params[4]));
+    reg.UseNMISetFloatingBinNumber(0, int(params[4]));
+    reg.SetSpacing(0, float(params[5]));
+    if (params[6] == 0) reg.DoNotPrintOutInformation();
+    reg.Run();
+    NiftiImage grid = reg.GetControlPointPositionImage();
+    cdim_out[0] = grid->nx; cdim_out[1] = grid->ny; cdim_out[2] = grid->nz;
+    if (cap < grid->nvox) return -1;
+    memcpy(cpp_out, grid->data, grid->nvox * sizeof(float));
+    const mat44& m = grid->sform_code > 0 ? grid->sto_xyz : grid->qto_xyz;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) cxyz_out[4 * i + j] = m.m[i][j];
+    stats[0] = reg.SimilarityWeight() > 0 ? reg.FinalWMeasure() / reg.SimilarityWeight() : 0;
+    stats[1] = reg.FinalWBE();
+    stats[2] = double(reg.objCalls);
+    stats[3] = double(reg.gradCalls);
+    return 0;
+}
+
 }  // extern "C"
