@@ -323,6 +323,7 @@ typedef struct nrb_image {
     int32_t qform_code;     /* as read (xyz is the qform when > 0 and sform_code is 0) */
     int32_t intent_code;    /* NIfTI intent (1007: vector) */
     float intent_p1;        /* NiftyReg transformation type for a grid (2: cubic B-spline grid) */
+    float intent_p2;        /* squaring number of a velocity grid (NiftyReg's use), else 0 */
     char intent_name[16];   /* "NREG_TRANS" for NiftyReg transformations */
     float *data;            /* host float32, nvol * nx * ny * nz, x fastest; owned by the library
                              * after nrb_image_read (free with nrb_image_free), by the caller when
@@ -360,6 +361,54 @@ nrb_status nrb_f3d_register_images(const nrb_image *ref, const nrb_image *flo, c
  * .nii or .nii.gz). */
 nrb_status nrb_f3d_register_files(const char *ref_path, const char *flo_path, const nrb_f3d_params *p,
                                   const char *cpp_path, const char *res_path, nrb_f3d_result *result);
+
+/* ---- F3D2: symmetric registration with stationary velocity fields (reg_f3d2) --------------- */
+
+/* Deformation field (positions in mm) on the reference grid of g (g->ref_*) from the cubic
+ * B-spline velocity grid vel on g->cpp_*: the flow at every voxel, divided by 2^N, squared N times
+ * by composition. *steps is N (the grid's intent_p2); with update_step_number (or *steps == 0)
+ * it is first set to the smallest N >= 6 with max |flow| / 2^N < 0.28 mm. Replaces
+ * Compute::GetDefFieldFromVelocityGrid (reg-lib/Compute.cpp:223-228) ->
+ * reg_spline_getDefFieldFromVelocityGrid (reg-lib/cpu/_reg_localTrans.cpp:3583-3613).
+ * def: 3 * nvox(ref) floats. Synchronises the stream when it updates N. */
+nrb_status nrb_get_def_field_from_velocity_grid(const nrb_geometry *g, const float *vel,
+                                                int update_step_number, int32_t *steps, float *def,
+                                                void *stream);
+
+/* update(x) <- apply(update(x)): trilinear in the voxel space of apply (dim, xyz voxel -> mm,
+ * ijk mm -> voxel), positions outside extrapolated linearly from the border. apply and update
+ * are distinct 3 * nvox buffers. Replaces Compute::DefFieldCompose (reg-lib/Compute.cpp:394-397)
+ * -> reg_defField_compose (reg-lib/cpu/_reg_localTrans.cpp:2334-2480). */
+nrb_status nrb_def_field_compose(const int32_t dim[3], const float xyz[16], const float ijk[16],
+                                 const float *apply, float *update, void *stream);
+
+/* The voxel-based gradient vgrad (3 * nvox(ref), on g->ref_*) transported along the opposite
+ * transformation, whose velocity grid vel_other lies on g->cpp_*: with its intermediate fields
+ * phi_0..phi_{N-1} (N = steps), vgrad <- vgrad + J(phi_i) * vgrad(phi_i) for i = 0..N-1, then
+ * vgrad / 2^N. Replaces Compute::ExponentiateGradient (reg-lib/Compute.cpp:288-330). */
+nrb_status nrb_exponentiate_gradient(const nrb_geometry *g, const float *vel_other, int32_t steps,
+                                     float *vgrad, void *stream);
+
+/* Forward and backward velocity grids (same dims; matrices g_fw->cpp_xyz and g_bw->cpp_xyz) made
+ * opposite: as displacements, fw <- (fw - bw) / 2 and bw <- (bw - fw) / 2. Replaces
+ * Compute::SymmetriseVelocityFields (reg-lib/Compute.cpp:356-392). */
+nrb_status nrb_symmetrise_velocity_fields(const nrb_geometry *g_fw, float *fw,
+                                          const nrb_geometry *g_bw, float *bw, void *stream);
+
+/* reg_f3d2<float>::Run (reg-lib/_reg_f3d2.cpp, the -vel and -sym variant of reg_f3d) on two host
+ * images: forward and backward velocity grids over the union of both fields of view
+ * (reg_createSymmetricControlPointGrids, reg-lib/cpu/_reg_localTrans.cpp:133-357), symmetric NMI
+ * (forward + backward) minus the bending energy of both grids, gradients exponentiated along the
+ * opposite transformation, grids symmetrised after every update. The images must be axis-aligned
+ * (diagonal voxel -> mm matrices, any origin); the velocity grids are not oriented like them.
+ * Results allocated by the library (free with nrb_image_free): cpp_fw_out and cpp_bw_out
+ * (required) the final velocity grids, intent_p1 = 6 (SPLINE_VEL_GRID), intent_p2 the squaring
+ * number; warped_fw_out / warped_bw_out (optional) the floating image on the reference grid and
+ * the reference image on the floating grid, cubic spline (reg_f3d2::GetWarpedImage). The result's
+ * final_nmi is the symmetric NMI (forward + backward); final_be the sum of both grids' energies. */
+nrb_status nrb_f3d2_register_images(const nrb_image *ref, const nrb_image *flo, const nrb_f3d_params *p,
+                                    nrb_image *cpp_fw_out, nrb_image *cpp_bw_out, nrb_image *warped_fw_out,
+                                    nrb_image *warped_bw_out, nrb_f3d_result *result);
 
 /* ---- batched and served registrations (no counterpart in the reference) -------------------- */
 

@@ -70,7 +70,7 @@ class Image(ctypes.Structure):
     _fields_ = [("dim", _I3), ("nvol", ctypes.c_int32), ("pixdim", _F3), ("xyz", ctypes.c_float * 16),
                 ("ijk", ctypes.c_float * 16), ("sform_code", ctypes.c_int32), ("qform_code", ctypes.c_int32),
                 ("intent_code", ctypes.c_int32),
-                ("intent_p1", ctypes.c_float), ("intent_name", ctypes.c_char * 16),
+                ("intent_p1", ctypes.c_float), ("intent_p2", ctypes.c_float), ("intent_name", ctypes.c_char * 16),
                 ("data", ctypes.POINTER(ctypes.c_float))]
 
 
@@ -258,6 +258,64 @@ def write_image(path, data, pixdim, xyz, intent_code=0, intent_p1=0.0, intent_na
     img.intent_name = intent_name
     img.data = a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
     check(lib().nrb_image_write(str(path).encode(), ctypes.byref(img)))
+
+
+# ---- F3D2 (reg_f3d2): symmetric registration with velocity fields ----------------------------
+def get_def_field_from_velocity_grid(g, vel, steps, deformation, update=False, stream=None):
+    """Compute::GetDefFieldFromVelocityGrid: deformation field on g's reference grid from the
+    velocity grid `vel` (g's grid); returns the squaring number used."""
+    n = ctypes.c_int32(int(steps))
+    check(lib().nrb_get_def_field_from_velocity_grid(ctypes.byref(g), _p(vel), int(bool(update)), ctypes.byref(n),
+                                                     _p(deformation), _s(stream)))
+    return n.value
+
+
+def def_field_compose(dim, xyz, apply, update, stream=None):
+    """reg_defField_compose: update(x) <- apply(update(x)) on a field of dims `dim`, voxel->mm `xyz`."""
+    m = np.asarray(xyz, np.float32).reshape(16)
+    x16, i16 = (ctypes.c_float * 16)(*[float(v) for v in m]), (ctypes.c_float * 16)(*[float(v) for v in _inv(m).ravel()])
+    check(lib().nrb_def_field_compose(_I3(*[int(v) for v in dim]), x16, i16, _p(apply), _p(update), _s(stream)))
+
+
+def exponentiate_gradient(g, vel_other, steps, vgrad, stream=None):
+    """Compute::ExponentiateGradient: vgrad (on g's reference grid) along the velocity grid
+    `vel_other` (g's grid), in place."""
+    check(lib().nrb_exponentiate_gradient(ctypes.byref(g), _p(vel_other), int(steps), _p(vgrad), _s(stream)))
+
+
+def symmetrise_velocity_fields(g_fw, fw, g_bw, bw, stream=None):
+    """Compute::SymmetriseVelocityFields on the two grids, in place."""
+    check(lib().nrb_symmetrise_velocity_fields(ctypes.byref(g_fw), _p(fw), ctypes.byref(g_bw), _p(bw), _s(stream)))
+
+
+def f3d2_register_images(ref, ref_pixdim, ref_xyz, flo, flo_pixdim, flo_xyz, params, warped=True):
+    """reg_f3d2 (-vel) on two host volumes ([nz, ny, nx]) with axis-aligned voxel->mm matrices.
+    Returns (fw grid [3, cz, cy, cx], bw grid, grid voxel->mm 4x4 (fw, bw), squaring number,
+    warped floating on the reference grid or None, warped reference on the floating grid or None,
+    result)."""
+    r, keep_r = _image_of(ref, ref_pixdim, ref_xyz)
+    f, keep_f = _image_of(flo, flo_pixdim, flo_xyz)
+    cf, cb, wf, wb, res = Image(), Image(), Image(), Image(), F3dResult()
+    check(lib().nrb_f3d2_register_images(ctypes.byref(r), ctypes.byref(f), ctypes.byref(params), ctypes.byref(cf),
+                                         ctypes.byref(cb), ctypes.byref(wf) if warped else None,
+                                         ctypes.byref(wb) if warped else None, ctypes.byref(res)))
+    try:
+        def grid(img):
+            cx, cy, cz = list(img.dim)
+            return (np.ctypeslib.as_array(img.data, shape=(3 * cx * cy * cz,)).copy().reshape(3, cz, cy, cx),
+                    np.array(img.xyz, np.float32).reshape(4, 4))
+
+        gf, xf = grid(cf)
+        gb, xb = grid(cb)
+        outs = [None, None]
+        if warped:
+            for k, (img, like) in enumerate(((wf, ref), (wb, flo))):
+                nz, ny, nx = np.shape(like)
+                outs[k] = np.ctypeslib.as_array(img.data, shape=(nx * ny * nz,)).copy().reshape(nz, ny, nx)
+        return gf, gb, (xf, xb), int(cf.intent_p2), outs[0], outs[1], res
+    finally:
+        for img in (cf, cb) + ((wf, wb) if warped else ()):
+            lib().nrb_image_free(ctypes.byref(img))
 
 
 def _image_of(data, pixdim, xyz, sform_code=1):

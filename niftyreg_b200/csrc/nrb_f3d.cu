@@ -468,6 +468,11 @@ struct WsHandle {
     ~WsHandle() { nrb_workspace_destroy(h); }
 };
 
+// reg_createImagePyramid for both images (definition below the registration class)
+nrb_status build_pyramids(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd, int levels,
+                          cudaStream_t st, std::vector<Header>& hdr, std::vector<Header>& fhdr,
+                          std::vector<DevBuf>& ref_pyr, std::vector<DevBuf>& flo_pyr);
+
 // reg_f3d<float> with the NMI measure and the bending-energy penalty on the B200 platform.
 class F3dRegistration {
 public:
@@ -802,40 +807,46 @@ nrb_status F3dRegistration::RunLevelGraph(float max_step, float smallest_size, f
 // reg_createImagePyramid (reg-lib/cpu/_reg_tools.cpp:1705-1733): the finest level is the input,
 // each coarser level halves (ceil) every axis whose current size / 2 is at least 32, after a
 // Gaussian smoothing.
-nrb_status F3dRegistration::BuildPyramid(const float *ref, const float *flo, const ImageDesc& rd,
-                                         const ImageDesc& fd) {
-    hdr_.assign(levels_, Header{});
-    fhdr_.assign(levels_, Header{});
-    ref_pyr_ = std::vector<DevBuf>(levels_);
-    flo_pyr_ = std::vector<DevBuf>(levels_);
-    hdr_[levels_ - 1] = header_of(rd);
-    fhdr_[levels_ - 1] = header_of(fd);
-    const Header& rf = hdr_[levels_ - 1];
-    const Header& ff = fhdr_[levels_ - 1];
-    NRB_TRY(ref_pyr_[levels_ - 1].alloc(rf.n(), st_));
-    NRB_TRY(flo_pyr_[levels_ - 1].alloc(ff.n(), st_));
-    NRB_CUDA(cudaMemcpyAsync(ref_pyr_[levels_ - 1].p, ref, rf.n() * 4, cudaMemcpyDefault, st_));
-    NRB_CUDA(cudaMemcpyAsync(flo_pyr_[levels_ - 1].p, flo, ff.n() * 4, cudaMemcpyDefault, st_));
-    if (levels_ == 1) return NRB_OK;
+nrb_status build_pyramids(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd, int levels,
+                          cudaStream_t st, std::vector<Header>& hdr, std::vector<Header>& fhdr,
+                          std::vector<DevBuf>& ref_pyr, std::vector<DevBuf>& flo_pyr) {
+    hdr.assign(levels, Header{});
+    fhdr.assign(levels, Header{});
+    ref_pyr = std::vector<DevBuf>(levels);
+    flo_pyr = std::vector<DevBuf>(levels);
+    hdr[levels - 1] = header_of(rd);
+    fhdr[levels - 1] = header_of(fd);
+    const Header& rf = hdr[levels - 1];
+    const Header& ff = fhdr[levels - 1];
+    NRB_TRY(ref_pyr[levels - 1].alloc(rf.n(), st));
+    NRB_TRY(flo_pyr[levels - 1].alloc(ff.n(), st));
+    NRB_CUDA(cudaMemcpyAsync(ref_pyr[levels - 1].p, ref, rf.n() * 4, cudaMemcpyDefault, st));
+    NRB_CUDA(cudaMemcpyAsync(flo_pyr[levels - 1].p, flo, ff.n() * 4, cudaMemcpyDefault, st));
+    if (levels == 1) return NRB_OK;
     DevBuf tmp;
-    NRB_TRY(tmp.alloc(4 * std::max(rf.n(), ff.n()), st_));
-    for (int l = levels_ - 2; l >= 0; --l) {
+    NRB_TRY(tmp.alloc(4 * std::max(rf.n(), ff.n()), st));
+    for (int l = levels - 2; l >= 0; --l) {
         // each image halves along its own axes
-        hdr_[l] = halve(hdr_[l + 1]);
-        fhdr_[l] = halve(fhdr_[l + 1]);
+        hdr[l] = halve(hdr[l + 1]);
+        fhdr[l] = halve(fhdr[l + 1]);
         float nxyz[16], oijk[16];
-        NRB_TRY(ref_pyr_[l].alloc(hdr_[l].n(), st_));
-        hdr_[l].xyz(nxyz);
-        hdr_[l + 1].ijk(oijk);
-        NRB_TRY(smooth_and_downsample(ref_pyr_[l + 1].p, hdr_[l + 1].dim, ref_pyr_[l].p, hdr_[l].dim, nxyz, oijk, tmp.p,
-                                      st_));
-        NRB_TRY(flo_pyr_[l].alloc(fhdr_[l].n(), st_));
-        fhdr_[l].xyz(nxyz);
-        fhdr_[l + 1].ijk(oijk);
-        NRB_TRY(smooth_and_downsample(flo_pyr_[l + 1].p, fhdr_[l + 1].dim, flo_pyr_[l].p, fhdr_[l].dim, nxyz, oijk,
-                                      tmp.p, st_));
+        NRB_TRY(ref_pyr[l].alloc(hdr[l].n(), st));
+        hdr[l].xyz(nxyz);
+        hdr[l + 1].ijk(oijk);
+        NRB_TRY(smooth_and_downsample(ref_pyr[l + 1].p, hdr[l + 1].dim, ref_pyr[l].p, hdr[l].dim, nxyz, oijk, tmp.p,
+                                      st));
+        NRB_TRY(flo_pyr[l].alloc(fhdr[l].n(), st));
+        fhdr[l].xyz(nxyz);
+        fhdr[l + 1].ijk(oijk);
+        NRB_TRY(smooth_and_downsample(flo_pyr[l + 1].p, fhdr[l + 1].dim, flo_pyr[l].p, fhdr[l].dim, nxyz, oijk,
+                                      tmp.p, st));
     }
     return NRB_OK;  // tmp is freed in stream order
+}
+
+nrb_status F3dRegistration::BuildPyramid(const float *ref, const float *flo, const ImageDesc& rd,
+                                         const ImageDesc& fd) {
+    return build_pyramids(ref, flo, rd, fd, levels_, st_, hdr_, fhdr_, ref_pyr_, flo_pyr_);
 }
 
 // reg_f3d::Initialise (_reg_f3d.cpp:161-200) -> reg_createControlPointGrid
@@ -1278,4 +1289,593 @@ extern "C" nrb_status nrb_f3d_register_host(const float *ref_host, const float *
     if (s == NRB_OK && result)
         result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// F3D2: symmetric registration with stationary velocity fields (reg_f3d2<float>)
+// ---------------------------------------------------------------------------------------------
+namespace nrb {
+
+nrb_status velocity_to_deformation(const nrb_geometry *g, const float *vel, bool update, int *steps, float *def,
+                                   float *fields, float *scratch, unsigned *minmax, cudaStream_t st);
+nrb_status exponentiate_gradient(const nrb_geometry *g, const float *vel_other, int steps, float *vgrad,
+                                 float *fields, float *scratch, unsigned *minmax, cudaStream_t st);
+nrb_status symmetrise_velocity(const int32_t cdim[3], const float fw_xyz[16], float *fw, const float bw_xyz[16],
+                               float *bw, cudaStream_t st);
+
+namespace {
+
+// Mat44Mul (reg-lib/cpu/Maths.hpp:271-286): in double, rounded to float
+void mat44_mul_f(const float m[16], const float in[3], float out[3]) {
+    for (int r = 0; r < 3; ++r)
+        out[r] = (float)((double)m[4 * r] * (double)in[0] + (double)m[4 * r + 1] * (double)in[1] +
+                         (double)m[4 * r + 2] * (double)in[2] + (double)m[4 * r + 3]);
+}
+
+// reg_createSymmetricControlPointGrids (reg-lib/cpu/_reg_localTrans.cpp:133-357) without an
+// affine: an axis-aligned grid (sform, identity orientation) over the union of the two images'
+// fields of view (corners at voxel 0 and n along each axis), its node 0 one spacing below the
+// lowest corner; ceil(extent / spacing + 3) nodes per axis.
+Header symmetric_grid_header(const Header& r, const Header& f, const float s[3]) {
+    float rm[16], fm[16];
+    r.xyz(rm);
+    f.xyz(fm);
+    float lo[3], hi[3];
+    for (int c = 0; c < 8; ++c) {
+        const float rc[3] = { (c & 1) ? (float)r.dim[0] : 0.f, (c & 2) ? (float)r.dim[1] : 0.f,
+                              (c & 4) ? (float)r.dim[2] : 0.f };
+        const float fc[3] = { (c & 1) ? (float)f.dim[0] : 0.f, (c & 2) ? (float)f.dim[1] : 0.f,
+                              (c & 4) ? (float)f.dim[2] : 0.f };
+        float ro[3], fo[3];
+        mat44_mul_f(rm, rc, ro);
+        mat44_mul_f(fm, fc, fo);
+        for (int i = 0; i < 3; ++i) {
+            const float a = std::min(ro[i], fo[i]), b = std::max(ro[i], fo[i]);
+            lo[i] = c == 0 ? a : std::min(lo[i], a);
+            hi[i] = c == 0 ? b : std::max(hi[i], b);
+        }
+    }
+    Header g{};
+    g.full = true;
+    g.sform = true;
+    memset(g.m, 0, sizeof(g.m));
+    for (int i = 0; i < 3; ++i) {
+        g.dim[i] = ceil_ref((hi[i] - lo[i]) / s[i] + 3.f);
+        g.pixdim[i] = s[i];
+        g.m[5 * i] = s[i];
+        g.m[4 * i + 3] = lo[i] - s[i];
+        g.origin[i] = g.m[4 * i + 3];
+    }
+    g.m[15] = 1.f;
+    return g;
+}
+
+// reg_spline_refineControlPointGrid3D without a reference image (_reg_localTrans.cpp:1809-1830,
+// 2212-2229): (n - 3) * 2 + 3 nodes, spacing and matrix columns halved, the origin moved to
+// node (1, 1, 1) of the halved matrix
+Header refine_header(const Header& g) {
+    Header n = g;
+    float m[16];
+    g.xyz(m);
+    for (int i = 0; i < 3; ++i) {
+        n.dim[i] = (g.dim[i] - 3) * 2 + 3;
+        n.pixdim[i] = g.pixdim[i] / 2.0f;
+        for (int r = 0; r < 3; ++r) m[4 * r + i] /= 2.f;
+    }
+    const float one[3] = { 1.f, 1.f, 1.f };
+    float o[3];
+    mat44_mul_f(m, one, o);
+    for (int r = 0; r < 3; ++r) m[4 * r + 3] = o[r];
+    n.full = true;
+    memcpy(n.m, m, sizeof(m));
+    for (int i = 0; i < 3; ++i) n.origin[i] = o[i];
+    return n;
+}
+
+void fill_geometry(nrb_geometry& g, const Header& r, const Header& f, const Header& c) {
+    for (int i = 0; i < 3; ++i) {
+        g.ref_dim[i] = r.dim[i];
+        g.ref_pixdim[i] = r.pixdim[i];
+        g.flo_dim[i] = f.dim[i];
+        g.flo_pixdim[i] = f.pixdim[i];
+        g.cpp_dim[i] = c.dim[i];
+        g.cpp_pixdim[i] = c.pixdim[i];
+    }
+    r.xyz(g.ref_xyz);
+    r.ijk(g.ref_ijk);
+    f.xyz(g.flo_xyz);
+    f.ijk(g.flo_ijk);
+    c.xyz(g.cpp_xyz);
+    c.ijk(g.cpp_ijk);
+}
+
+// reg_f3d2<float> with the symmetric NMI measure and the bending-energy penalty: forward
+// (reference -> floating) and backward velocity grids optimised together by one conjugate
+// gradient over both, with the step loop of reg_base::Run on the host.
+class F3d2Registration {
+public:
+    F3d2Registration(const nrb_f3d_params& p, cudaStream_t st): p_(p), st_(st) {}
+    nrb_status Run(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd, float *fw_out,
+                   float *bw_out, float *warped_fw, float *warped_bw, nrb_f3d_result *res);
+    const Header& grid_fw() const { return gf_; }
+    const Header& grid_bw() const { return gb_; }
+    int steps() const { return steps_; }
+
+private:
+    float *fw(DevBuf& b) { return b.p; }
+    float *bw(DevBuf& b) { return b.p + 3 * nc_; }
+
+    nrb_status Fields(int64_t nvox_max) {
+        const int64_t need = (int64_t)steps_ * 3 * nvox_max;
+        if (need > fields_n_) {
+            NRB_TRY(fields_.alloc(need, st_));
+            fields_n_ = need;
+        }
+        return NRB_OK;
+    }
+    // reg_f3d2::GetDeformationField + WarpFloatingImage (_reg_f3d2.cpp:144-181): the forward
+    // field (squaring number updated when the optimiser runs), the backward one with the same
+    // number, both images warped (trilinear)
+    nrb_status Warp(bool update) {
+        NRB_TRY(velocity_to_deformation(&gfw_, fw(cur_), update, &steps_, def_fw_.p, nullptr, scr_r_.p, mm_, st_));
+        NRB_TRY(velocity_to_deformation(&gbw_, bw(cur_), false, &steps_, def_bw_.p, nullptr, scr_f_.p, mm_, st_));
+        NRB_TRY(nrb_resample_image(&gfw_, flo_.p, def_fw_.p, nullptr, pad_, war_fw_.p, st_));
+        NRB_TRY(nrb_resample_image(&gbw_, ref_.p, def_bw_.p, nullptr, pad_, war_bw_.p, st_));
+        return NRB_OK;
+    }
+    nrb_status Similarity(double& nmi_fw, double& nmi_bw) {
+        NRB_TRY(nrb_nmi_value(nmi_fw_.h, &gfw_, ref_.p, war_fw_.p, nullptr, nullptr, &nmi_fw, st_));
+        NRB_TRY(nrb_nmi_value(nmi_bw_.h, &gbw_, flo_.p, war_bw_.p, nullptr, nullptr, &nmi_bw, st_));
+        return NRB_OK;
+    }
+    // reg_f3d2::GetObjectiveFunctionValue (_reg_f3d2.cpp:465-485)
+    nrb_status GetObjectiveFunctionValue(bool update, double& value) {
+        double be_f = 0, be_b = 0;
+        if (be_w_ > 0) {
+            NRB_TRY(nrb_approx_bending_energy(ws_fw_.h, &gfw_, fw(cur_), nullptr, &be_f, st_));
+            NRB_TRY(nrb_approx_bending_energy(ws_bw_.h, &gbw_, bw(cur_), nullptr, &be_b, st_));
+        }
+        cur_w_be_ = be_w_ > 0 ? (double)be_w_ * be_f + (double)be_w_ * be_b : 0.0;
+        cur_be_ = be_f + be_b;
+        double nf = 0, nb = 0;
+        if (sim_w_ > 0) {
+            NRB_TRY(Warp(update));
+            NRB_TRY(Similarity(nf, nb));
+        }
+        cur_nmi_ = nf + nb;
+        cur_w_measure_ = sim_w_ > 0 ? (double)sim_w_ * (nf + nb) : 0.0;
+        ++n_obj_;
+        value = cur_w_measure_ - cur_w_be_;
+        return NRB_OK;
+    }
+    // reg_f3d2::GetObjectiveFunctionGradient (_reg_f3d2.cpp:393-418) with GetVoxelBasedGradient
+    // (:244-305), ExponentiateGradient (:637-650) and NormaliseGradient (:369-391)
+    nrb_status GetObjectiveFunctionGradient() {
+        const int64_t nr = nvox(gfw_.ref_dim), nf = nvox(gbw_.ref_dim);
+        if (sim_w_ > 0) {
+            NRB_TRY(Warp(true));
+            NRB_CUDA(cudaMemsetAsync(vg_fw_.p, 0, 3 * nr * sizeof(float), st_));
+            NRB_CUDA(cudaMemsetAsync(vg_bw_.p, 0, 3 * nf * sizeof(float), st_));
+            NRB_TRY(nrb_get_image_gradient(&gfw_, flo_.p, def_fw_.p, nullptr, pad_, wg_fw_.p, st_));
+            NRB_TRY(nrb_get_image_gradient(&gbw_, ref_.p, def_bw_.p, nullptr, pad_, wg_bw_.p, st_));
+            double a, b;
+            NRB_TRY(Similarity(a, b));  // reg_nmi::GetVoxelBasedSimilarityMeasureGradientFw recomputes both
+            NRB_TRY(nrb_nmi_voxel_gradient(nmi_fw_.h, &gfw_, ref_.p, war_fw_.p, wg_fw_.p, nullptr, 1.0, vg_fw_.p, st_));
+            NRB_TRY(nrb_nmi_voxel_gradient(nmi_bw_.h, &gbw_, flo_.p, war_bw_.p, wg_bw_.p, nullptr, 1.0, vg_bw_.p, st_));
+            // forward gradient along the backward transformation on the reference grid, and back
+            NRB_TRY(Fields(std::max(nr, nf)));
+            nrb_geometry gx = gfw_;
+            for (int i = 0; i < 3; ++i) gx.cpp_dim[i] = gbw_.cpp_dim[i], gx.cpp_pixdim[i] = gbw_.cpp_pixdim[i];
+            memcpy(gx.cpp_xyz, gbw_.cpp_xyz, sizeof(gx.cpp_xyz));
+            memcpy(gx.cpp_ijk, gbw_.cpp_ijk, sizeof(gx.cpp_ijk));
+            NRB_TRY(exponentiate_gradient(&gx, bw(cur_), steps_, vg_fw_.p, fields_.p, scr_r_.p, mm_, st_));
+            gx = gbw_;
+            for (int i = 0; i < 3; ++i) gx.cpp_dim[i] = gfw_.cpp_dim[i], gx.cpp_pixdim[i] = gfw_.cpp_pixdim[i];
+            memcpy(gx.cpp_xyz, gfw_.cpp_xyz, sizeof(gx.cpp_xyz));
+            memcpy(gx.cpp_ijk, gfw_.cpp_ijk, sizeof(gx.cpp_ijk));
+            NRB_TRY(exponentiate_gradient(&gx, fw(cur_), steps_, vg_bw_.p, fields_.p, scr_f_.p, mm_, st_));
+            NRB_TRY(nrb_convolve_voxel_based_gradient(ws_fw_.h, &gfw_, vg_fw_.p, sim_w_, fw(grad_), st_));
+            NRB_TRY(nrb_convolve_voxel_based_gradient(ws_bw_.h, &gbw_, vg_bw_.p, sim_w_, bw(grad_), st_));
+        } else {
+            NRB_CUDA(cudaMemsetAsync(grad_.p, 0, 6 * nc_ * sizeof(float), st_));
+        }
+        ++it_;
+        ++n_grad_;
+        if (be_w_ > 0) {
+            NRB_TRY(nrb_approx_bending_energy_gradient(ws_fw_.h, &gfw_, fw(cur_), be_w_, fw(grad_), st_));
+            NRB_TRY(nrb_approx_bending_energy_gradient(ws_bw_.h, &gbw_, bw(cur_), be_w_, bw(grad_), st_));
+        }
+        double mf = 0, mb = 0;
+        NRB_TRY(nrb_get_maximal_length(fw(grad_), nc_, nullptr, &mf, st_));
+        NRB_TRY(nrb_get_maximal_length(bw(grad_), nc_, nullptr, &mb, st_));
+        const float mx = std::max((float)mb, (float)mf);
+        NRB_TRY(nrb_normalise_gradient(fw(grad_), nc_, (double)mx, nullptr, st_));
+        NRB_TRY(nrb_normalise_gradient(bw(grad_), nc_, (double)mx, nullptr, st_));
+        return NRB_OK;
+    }
+    void UpdateBestObjFunctionValue() {
+        best_w_measure_ = cur_w_measure_;
+        best_w_be_ = cur_w_be_;
+        best_nmi_ = cur_nmi_;
+        best_be_ = cur_be_;
+    }
+    nrb_status StoreCurrentDof() {
+        NRB_CUDA(cudaMemcpyAsync(best_.p, cur_.p, 6 * nc_ * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+        return NRB_OK;
+    }
+    nrb_status RestoreBestDof() {
+        NRB_CUDA(cudaMemcpyAsync(cur_.p, best_.p, 6 * nc_ * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+        return NRB_OK;
+    }
+    // reg_f3d2::UpdateParameters (_reg_f3d2.cpp:652-684): best + scale * gradient for both grids
+    // (UpdateVelocityField), then SymmetriseVelocityFields
+    nrb_status UpdateParameters(float scale) {
+        NRB_TRY(nrb_update_control_point_position(cur_.p, best_.p, grad_.p, scale, 6 * nc_, st_));
+        return symmetrise_velocity(gf_.dim, gfw_.cpp_xyz, fw(cur_), gbw_.cpp_xyz, bw(cur_), st_);
+    }
+    // ConjugateGradient::Optimise over both grids (reg-lib/Optimiser.cpp:231-323, :129-173)
+    nrb_status Optimise(float max_length, float small_length, float& start_length) {
+        NRB_TRY(nrb_conjugate_gradient(ws_fw_.h, grad_.p, g1_.p, g2_.p, 6 * nc_, first_call_ ? 1 : 0, st_));
+        first_call_ = false;
+        size_t line_iteration = 0;
+        float added_length = 0;
+        float current_length = start_length;
+        while (current_length > small_length && line_iteration < 12 && it_ < max_it_) {
+            NRB_TRY(UpdateParameters(-current_length));
+            double value = 0;
+            NRB_TRY(GetObjectiveFunctionValue(true, value));
+            if (value > best_obj_) {
+                UpdateBestObjFunctionValue();
+                best_obj_ = value;
+                added_length += current_length;
+                current_length *= 1.1f;
+                current_length = std::min(current_length, max_length);
+                NRB_TRY(StoreCurrentDof());
+            } else {
+                current_length *= 0.5;
+            }
+            ++it_;
+            ++line_iteration;
+        }
+        start_length = added_length;
+        return RestoreBestDof();
+    }
+    nrb_status InitLevel(int level, float& max_step);
+
+    nrb_f3d_params p_;
+    cudaStream_t st_;
+    int levels_ = 0;
+    std::vector<Header> hdr_, fhdr_;
+    std::vector<DevBuf> ref_pyr_, flo_pyr_;
+    Header gf_{}, gb_{};          // forward and backward velocity grids (same dims)
+    nrb_geometry gfw_{}, gbw_{};  // reference / floating / forward grid, and swapped / backward grid
+    int64_t nc_ = 0;
+    int steps_ = 6;               // squaring number (the grids' intent_p2)
+    DevBuf ref_, flo_, cur_, best_, grad_, g1_, g2_;  // dof arrays: [forward | backward]
+    DevBuf def_fw_, def_bw_, war_fw_, war_bw_, wg_fw_, wg_bw_, vg_fw_, vg_bw_, scr_r_, scr_f_, fields_;
+    int64_t fields_n_ = 0;
+    unsigned *mm_ = nullptr;
+    NmiHandle nmi_fw_, nmi_bw_;
+    WsHandle ws_fw_, ws_bw_;
+    float pad_ = std::numeric_limits<float>::quiet_NaN();
+    float sim_w_ = 1, be_w_ = 0;
+    size_t it_ = 0, max_it_ = 0;
+    bool first_call_ = true;
+    double best_obj_ = 0;
+    double cur_w_measure_ = 0, cur_w_be_ = 0, best_w_measure_ = 0, best_w_be_ = 0;
+    double cur_nmi_ = 0, cur_be_ = 0, best_nmi_ = 0, best_be_ = 0;
+    int64_t n_obj_ = 0, n_grad_ = 0;
+
+public:
+    ~F3d2Registration() { dev_free(mm_, st_); }
+};
+
+// reg_f3d2::InitCurrentLevel (_reg_f3d2.cpp:52-102) + InitialiseSimilarity + SetOptimiser
+nrb_status F3d2Registration::InitLevel(int level, float& max_step) {
+    const Header& r = hdr_[level];
+    const Header& f = fhdr_[level];
+    max_step = std::max(std::max(std::max(r.pixdim[0], r.pixdim[1]), std::max(f.pixdim[0], f.pixdim[1])),
+                        std::max(r.pixdim[2], f.pixdim[2]));
+    if (level == 0) {
+        be_w_ = be_w_ / powf(16.f, (float)(levels_ - 1));
+    } else {
+        be_w_ = be_w_ * 16.f;
+        const Header nf = refine_header(gf_), nb = refine_header(gb_);
+        DevBuf refined;
+        NRB_TRY(refined.alloc(6 * nf.n(), st_));
+        NRB_TRY(grid_refine(gf_.dim, fw(cur_), nf.dim, refined.p, st_));
+        NRB_TRY(grid_refine(gb_.dim, bw(cur_), nb.dim, refined.p + 3 * nf.n(), st_));
+        std::swap(cur_.p, refined.p);
+        gf_ = nf;
+        gb_ = nb;
+    }
+    nc_ = gf_.n();
+    fill_geometry(gfw_, r, f, gf_);
+    fill_geometry(gbw_, f, r, gb_);
+    std::swap(ref_.p, ref_pyr_[level].p);
+    std::swap(flo_.p, flo_pyr_[level].p);
+    ref_.st = flo_.st = st_;
+    const int64_t nr = r.n(), nfv = f.n();
+    NRB_TRY(best_.alloc(6 * nc_, st_));
+    NRB_TRY(grad_.alloc(6 * nc_, st_));
+    NRB_TRY(g1_.alloc(6 * nc_, st_));
+    NRB_TRY(g2_.alloc(6 * nc_, st_));
+    NRB_TRY(def_fw_.alloc(3 * nr, st_));
+    NRB_TRY(war_fw_.alloc(nr, st_));
+    NRB_TRY(wg_fw_.alloc(3 * nr, st_));
+    NRB_TRY(vg_fw_.alloc(3 * nr, st_));
+    NRB_TRY(scr_r_.alloc(3 * nr, st_));
+    NRB_TRY(def_bw_.alloc(3 * nfv, st_));
+    NRB_TRY(war_bw_.alloc(nfv, st_));
+    NRB_TRY(wg_bw_.alloc(3 * nfv, st_));
+    NRB_TRY(vg_bw_.alloc(3 * nfv, st_));
+    NRB_TRY(scr_f_.alloc(3 * nfv, st_));
+    fields_n_ = 0;
+    for (WsHandle *w : { &ws_fw_, &ws_bw_ }) {
+        nrb_workspace_destroy(w->h);
+        w->h = nullptr;
+    }
+    NRB_TRY(workspace_create_on(&gfw_, st_, &ws_fw_.h));
+    NRB_TRY(workspace_create_on(&gbw_, st_, &ws_bw_.h));
+    if (!nmi_fw_.h) NRB_TRY(nmi_create_on(p_.ref_bins + 4, p_.flo_bins + 4, st_, &nmi_fw_.h));
+    if (!nmi_bw_.h) NRB_TRY(nmi_create_on(p_.flo_bins + 4, p_.ref_bins + 4, st_, &nmi_bw_.h));
+    // reg_nmi::InitialiseMeasure: both images rescaled to [2, bins - 3]
+    NRB_TRY(rescale_with(ref_.p, nr, 2.f, (float)(p_.ref_bins + 4) - 3.f, ws_fw_.h->fred, st_));
+    NRB_TRY(rescale_with(flo_.p, nfv, 2.f, (float)(p_.flo_bins + 4) - 3.f, ws_fw_.h->fred, st_));
+    // Optimiser::Initialise: best = current, objective at the start (no optimiser yet, so the
+    // squaring number is not updated: _reg_f3d2.cpp:146-148)
+    it_ = 0;
+    first_call_ = true;
+    NRB_TRY(StoreCurrentDof());
+    double v = 0;
+    NRB_TRY(GetObjectiveFunctionValue(false, v));
+    best_obj_ = v;
+    return NRB_OK;
+}
+
+nrb_status F3d2Registration::Run(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd,
+                                 float *fw_out, float *bw_out, float *warped_fw, float *warped_bw,
+                                 nrb_f3d_result *res) {
+    const auto t0 = std::chrono::steady_clock::now();
+    levels_ = p_.levels;
+    if (levels_ < 1) return fail(NRB_ERR_INVALID, "registration: levels must be >= 1");
+    if (p_.ref_bins < 1 || p_.flo_bins < 1) return fail(NRB_ERR_INVALID, "registration: bins must be >= 1");
+    pad_ = p_.padding;
+    // reg_f3d2::CheckParameters (_reg_f3d2.cpp:119-141): weights normalised by the penalty sum
+    be_w_ = p_.bending_energy;
+    const float penalty = be_w_;
+    if (penalty >= 1) {
+        sim_w_ = 0;
+        be_w_ /= penalty;
+    } else {
+        sim_w_ = 1 - penalty;
+    }
+    NRB_CUDA(dev_alloc(&mm_, 2 * sizeof(unsigned), st_));
+    NRB_TRY(build_pyramids(ref, flo, rd, fd, levels_, st_, hdr_, fhdr_, ref_pyr_, flo_pyr_));
+    // reg_f3d2::Initialise (_reg_f3d2.cpp:539-610): spacing in voxels of the mean of both images'
+    // input spacings, times 2^(levels - 1), grids over the coarsest images
+    const Header& rin = hdr_[levels_ - 1];
+    const Header& fin = fhdr_[levels_ - 1];
+    float spacing[3];
+    for (int i = 0; i < 3; ++i) {
+        float s = p_.spacing[i];
+        if (s != s) s = p_.spacing[0];
+        if (s < 0) s *= -(rin.pixdim[i] + fin.pixdim[i]) / 2.f;
+        spacing[i] = s * powf(2.f, (float)(levels_ - 1));
+    }
+    gf_ = symmetric_grid_header(hdr_[0], fhdr_[0], spacing);
+    gb_ = gf_;
+    nc_ = gf_.n();
+    NRB_TRY(cur_.alloc(6 * nc_, st_));
+    float cxyz[16];
+    gf_.xyz(cxyz);
+    NRB_TRY(grid_identity(gf_.dim, cxyz, fw(cur_), st_));
+    NRB_TRY(grid_identity(gb_.dim, cxyz, bw(cur_), st_));
+    steps_ = 6;
+    max_it_ = (size_t)p_.max_iterations;
+    max_it_ *= (size_t)std::pow(2, levels_ - 1);
+    for (int level = 0; level < levels_; ++level) {
+        float max_step = 0;
+        NRB_TRY(InitLevel(level, max_step));
+        float current_size = max_step;
+        const float smallest_size = max_step / 100.0f;
+        UpdateBestObjFunctionValue();
+        if (p_.verbose)
+            printf("[nrb] f3d2 level %d/%d grid %dx%dx%d, initial objective %.6f = (wSIM)%.6f - (wBE)%.6g\n",
+                   level + 1, levels_, gf_.dim[0], gf_.dim[1], gf_.dim[2], best_obj_, best_w_measure_, best_w_be_);
+        bool just_restarted = false;
+        while (current_size) {
+            if (it_ >= max_it_) break;
+            NRB_TRY(GetObjectiveFunctionGradient());
+            current_size = std::min(current_size, max_step);
+            NRB_TRY(Optimise(max_step, smallest_size, current_size));
+            if (p_.verbose)
+                printf("[nrb] [%zu] objective %.6f = (wSIM)%.6f - (wBE)%.6g [+ %g mm], N = %d\n", it_, best_obj_,
+                       best_w_measure_, best_w_be_, current_size, steps_);
+            if (current_size == 0) {
+                if (!just_restarted && it_ < max_it_) {
+                    first_call_ = true;
+                    current_size = max_step;
+                    just_restarted = true;
+                }
+            } else {
+                just_restarted = false;
+            }
+        }
+        max_it_ /= 2;
+    }
+    const int64_t n = 3 * nc_;
+    if (fw_out) NRB_CUDA(cudaMemcpyAsync(fw_out, fw(cur_), n * sizeof(float), cudaMemcpyDefault, st_));
+    if (bw_out) NRB_CUDA(cudaMemcpyAsync(bw_out, bw(cur_), n * sizeof(float), cudaMemcpyDefault, st_));
+    if (warped_fw || warped_bw) {
+        // reg_f3d2::GetWarpedImage (_reg_f3d2.cpp:686-700): the input images through both
+        // transformations at full resolution, cubic spline, squaring number as it stands
+        const Header& rf = hdr_[levels_ - 1];
+        const Header& ff = fhdr_[levels_ - 1];
+        nrb_geometry wf{}, wb{};
+        fill_geometry(wf, rf, ff, gf_);
+        fill_geometry(wb, ff, rf, gb_);
+        DevBuf rimg, fimg, def, scr, out;
+        NRB_TRY(rimg.alloc(rf.n(), st_));
+        NRB_TRY(fimg.alloc(ff.n(), st_));
+        NRB_TRY(def.alloc(3 * std::max(rf.n(), ff.n()), st_));
+        NRB_TRY(scr.alloc(3 * std::max(rf.n(), ff.n()), st_));
+        NRB_TRY(out.alloc(std::max(rf.n(), ff.n()), st_));
+        NRB_CUDA(cudaMemcpyAsync(rimg.p, ref, rf.n() * sizeof(float), cudaMemcpyDefault, st_));
+        NRB_CUDA(cudaMemcpyAsync(fimg.p, flo, ff.n() * sizeof(float), cudaMemcpyDefault, st_));
+        int N = steps_;
+        if (warped_fw) {
+            NRB_TRY(velocity_to_deformation(&wf, fw(cur_), false, &N, def.p, nullptr, scr.p, mm_, st_));
+            NRB_TRY(nrb_resample_image_order(&wf, fimg.p, def.p, nullptr, 3, pad_, out.p, st_));
+            NRB_CUDA(cudaMemcpyAsync(warped_fw, out.p, rf.n() * sizeof(float), cudaMemcpyDefault, st_));
+        }
+        if (warped_bw) {
+            NRB_TRY(velocity_to_deformation(&wb, bw(cur_), false, &N, def.p, nullptr, scr.p, mm_, st_));
+            NRB_TRY(nrb_resample_image_order(&wb, rimg.p, def.p, nullptr, 3, pad_, out.p, st_));
+            NRB_CUDA(cudaMemcpyAsync(warped_bw, out.p, ff.n() * sizeof(float), cudaMemcpyDefault, st_));
+        }
+        NRB_CUDA(cudaStreamSynchronize(st_));
+    }
+    NRB_CUDA(cudaStreamSynchronize(st_));
+    if (res) {
+        for (int i = 0; i < 3; ++i) res->cpp_dim[i] = gf_.dim[i];
+        res->final_nmi = best_nmi_;
+        res->final_be = best_be_;
+        res->final_objective = best_obj_;
+        res->objective_evaluations = n_obj_;
+        res->gradient_evaluations = n_grad_;
+        res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return NRB_OK;
+}
+
+}  // namespace
+}  // namespace nrb
+
+// a velocity grid as NiftyReg tags one (reg_f3d2::Initialise, _reg_f3d2.cpp:596-599)
+static void velocity_grid_image(const Header& g, int steps, float *data, nrb_image *out) {
+    for (int i = 0; i < 3; ++i) {
+        out->dim[i] = g.dim[i];
+        out->pixdim[i] = g.pixdim[i];
+    }
+    out->nvol = 3;
+    g.xyz(out->xyz);
+    g.ijk(out->ijk);
+    out->sform_code = 1;
+    out->qform_code = 0;
+    out->intent_code = 1007;  // NIFTI_INTENT_VECTOR
+    out->intent_p1 = 6.f;     // SPLINE_VEL_GRID
+    out->intent_p2 = (float)steps;
+    strncpy(out->intent_name, "NREG_TRANS", sizeof(out->intent_name) - 1);
+    out->data = data;
+}
+
+static bool axis_aligned(const nrb_image *img) {
+    const float *m = img->xyz;
+    return m[1] == 0.f && m[2] == 0.f && m[4] == 0.f && m[6] == 0.f && m[8] == 0.f && m[9] == 0.f && m[0] > 0.f &&
+           m[5] > 0.f && m[10] > 0.f;
+}
+
+extern "C" nrb_status nrb_f3d2_register_images(const nrb_image *ref, const nrb_image *flo, const nrb_f3d_params *p,
+                                               nrb_image *cpp_fw_out, nrb_image *cpp_bw_out, nrb_image *warped_fw_out,
+                                               nrb_image *warped_bw_out, nrb_f3d_result *result) {
+    NRB_TRY(check_image(ref, "reference"));
+    NRB_TRY(check_image(flo, "floating"));
+    if (!p || !cpp_fw_out || !cpp_bw_out) return fail(NRB_ERR_INVALID, "nrb_f3d2_register_images: null pointer");
+    if (!axis_aligned(ref) || !axis_aligned(flo))
+        return fail(NRB_ERR_UNSUPPORTED,
+                    "nrb_f3d2_register_images: images with axis-aligned voxel -> mm matrices (positive diagonal) only");
+    for (nrb_image *o : { cpp_fw_out, cpp_bw_out, warped_fw_out, warped_bw_out })
+        if (o) memset(o, 0, sizeof(*o));
+    ImageDesc rd, fd;
+    for (int i = 0; i < 3; ++i) {
+        rd.dim[i] = ref->dim[i];
+        rd.pixdim[i] = ref->pixdim[i];
+        fd.dim[i] = flo->dim[i];
+        fd.pixdim[i] = flo->pixdim[i];
+    }
+    rd.xyz = ref->xyz;
+    rd.sform = ref->sform_code > 0;
+    fd.xyz = flo->xyz;
+    fd.sform = flo->sform_code > 0;
+    const int64_t nref = (int64_t)ref->dim[0] * ref->dim[1] * ref->dim[2];
+    const int64_t nflo = (int64_t)flo->dim[0] * flo->dim[1] * flo->dim[2];
+    const auto t0 = std::chrono::steady_clock::now();
+    cudaStream_t st = nullptr;
+    NRB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    nrb_status s = NRB_OK;
+    float *fw = nullptr, *bw = nullptr, *wf = nullptr, *wb = nullptr;
+    {
+        F3d2Registration reg(*p, st);
+        // the final grid's size from the headers alone (the registration builds the same), so
+        // that the results go straight into host buffers
+        std::vector<Header> hdr, fhdr;
+        const int levels = std::max(1, (int)p->levels);
+        hdr.assign(levels, Header{});
+        fhdr.assign(levels, Header{});
+        hdr[levels - 1] = header_of(rd);
+        fhdr[levels - 1] = header_of(fd);
+        for (int l = levels - 2; l >= 0; --l) {
+            hdr[l] = halve(hdr[l + 1]);
+            fhdr[l] = halve(fhdr[l + 1]);
+        }
+        float spacing[3];
+        for (int i = 0; i < 3; ++i) {
+            float sp = p->spacing[i];
+            if (sp != sp) sp = p->spacing[0];
+            if (sp < 0) sp *= -(hdr[levels - 1].pixdim[i] + fhdr[levels - 1].pixdim[i]) / 2.f;
+            spacing[i] = sp * powf(2.f, (float)(levels - 1));
+        }
+        Header g = symmetric_grid_header(hdr[0], fhdr[0], spacing);
+        for (int l = 1; l < levels; ++l) g = refine_header(g);
+        const int64_t ncpp = 3 * g.n();
+        fw = (float *)malloc((size_t)ncpp * sizeof(float));
+        bw = (float *)malloc((size_t)ncpp * sizeof(float));
+        wf = warped_fw_out ? (float *)malloc((size_t)nref * sizeof(float)) : nullptr;
+        wb = warped_bw_out ? (float *)malloc((size_t)nflo * sizeof(float)) : nullptr;
+        if (!fw || !bw || (warped_fw_out && !wf) || (warped_bw_out && !wb)) {
+            s = fail(NRB_ERR_OOM, "nrb_f3d2_register_images: host allocation failed");
+        } else {
+            s = reg.Run(ref->data, flo->data, rd, fd, fw, bw, wf, wb, result);
+        }
+        if (s == NRB_OK) {
+            velocity_grid_image(reg.grid_fw(), reg.steps(), fw, cpp_fw_out);
+            velocity_grid_image(reg.grid_bw(), reg.steps(), bw, cpp_bw_out);
+        }
+    }
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (s != NRB_OK) {
+        free(fw);
+        free(bw);
+        free(wf);
+        free(wb);
+        return s;
+    }
+    if (warped_fw_out) {
+        for (int i = 0; i < 3; ++i) {
+            warped_fw_out->dim[i] = ref->dim[i];
+            warped_fw_out->pixdim[i] = ref->pixdim[i];
+        }
+        warped_fw_out->nvol = 1;
+        memcpy(warped_fw_out->xyz, ref->xyz, sizeof(ref->xyz));
+        memcpy(warped_fw_out->ijk, ref->ijk, sizeof(ref->ijk));
+        warped_fw_out->sform_code = ref->sform_code;
+        warped_fw_out->qform_code = ref->qform_code;
+        warped_fw_out->data = wf;
+    }
+    if (warped_bw_out) {
+        for (int i = 0; i < 3; ++i) {
+            warped_bw_out->dim[i] = flo->dim[i];
+            warped_bw_out->pixdim[i] = flo->pixdim[i];
+        }
+        warped_bw_out->nvol = 1;
+        memcpy(warped_bw_out->xyz, flo->xyz, sizeof(flo->xyz));
+        memcpy(warped_bw_out->ijk, flo->ijk, sizeof(flo->ijk));
+        warped_bw_out->sform_code = flo->sform_code;
+        warped_bw_out->qform_code = flo->qform_code;
+        warped_bw_out->data = wb;
+    }
+    if (result) result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return NRB_OK;
 }

@@ -254,6 +254,7 @@ extern "C" nrb_status nrb_image_read(const char *path, nrb_image *out) {
     out->qform_code = qform_code > 0 ? qform_code : 0;
     out->intent_code = h.get<int16_t>(kOffIntentCode);
     out->intent_p1 = h.get<float>(kOffIntentP1);
+    out->intent_p2 = h.get<float>(kOffIntentP1 + 4);
     memcpy(out->intent_name, h.b.data() + kOffIntentName, 16);
     out->intent_name[15] = 0;
     out->data = data;
@@ -289,6 +290,7 @@ extern "C" nrb_status nrb_image_write(const char *path, const nrb_image *img) {
     }
     put(kOffDim, dim, sizeof dim);
     put(kOffIntentP1, &img->intent_p1, 4);
+    put(kOffIntentP1 + 4, &img->intent_p2, 4);
     const int16_t intent = (int16_t)img->intent_code, datatype = 16, bitpix = 32;
     put(kOffIntentCode, &intent, 2);
     put(kOffDatatype, &datatype, 2);

@@ -192,6 +192,65 @@ class Ref:
             raise RuntimeError("ref_refine_grid: capacity")
         return out[:3 * int(np.prod(cdo))].copy(), cdo, cpo, cxo.reshape(4, 4)
 
+    # ---- F3D2 (reg_f3d2): velocity fields --------------------------------------------------
+    def velocity_def_field(self, vel, gdim, gpix, gxyz, steps, update, fdim, fpix, fxyz):
+        """reg_spline_getDefFieldFromVelocityGrid: (deformation field, squaring number)."""
+        out = np.zeros(3 * int(np.prod(fdim)), np.float32)
+        n = ctypes.c_int(0)
+        self.lib.ref_velocity_def_field(_f(_f3(vel)), _i(_i3(gdim)), _f(_f3(gpix)), _f(_m(gxyz)), int(steps),
+                                        int(bool(update)), _i(_i3(fdim)), _f(_f3(fpix)), _f(_m(fxyz)), _f(out),
+                                        ctypes.byref(n))
+        return out, n.value
+
+    def def_compose(self, dim, pix, xyz, apply, update):
+        """reg_defField_compose: update(x) <- apply(update(x))."""
+        u = _f3(update).copy()
+        self.lib.ref_def_compose(_i(_i3(dim)), _f(_f3(pix)), _f(_m(xyz)), _f(_f3(apply)), _f(u))
+        return u
+
+    def exponentiate_gradient(self, fdim, fpix, fxyz, vel, gdim, gpix, gxyz, steps, vgrad):
+        """Compute::ExponentiateGradient with the reference's functions."""
+        g = _f3(vgrad).copy()
+        self.lib.ref_exponentiate_gradient(_i(_i3(fdim)), _f(_f3(fpix)), _f(_m(fxyz)), _f(_f3(vel)), _i(_i3(gdim)),
+                                           _f(_f3(gpix)), _f(_m(gxyz)), int(steps), _f(g))
+        return g
+
+    def symmetrise(self, gdim, gpix, fw_xyz, bw_xyz, fw, bw):
+        """Compute::SymmetriseVelocityFields."""
+        a, b = _f3(fw).copy(), _f3(bw).copy()
+        self.lib.ref_symmetrise(_i(_i3(gdim)), _f(_f3(gpix)), _f(_m(fw_xyz)), _f(_m(bw_xyz)), _f(a), _f(b))
+        return a, b
+
+    def symmetric_grids(self, rdim, rpix, rxyz, fdim, fpix, fxyz, spacing):
+        """reg_createSymmetricControlPointGrids: (dims, voxel->mm 4x4, identity positions)."""
+        gdim, gxyz = np.zeros(3, np.int32), np.zeros(16, np.float32)
+        self.lib.ref_symmetric_grids(_i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)), _i(_i3(fdim)), _f(_f3(fpix)),
+                                     _f(_m(fxyz)), _f(_f3(spacing)), _i(gdim), _f(gxyz), None, ctypes.c_size_t(0))
+        cap = 3 * int(np.prod(gdim))
+        cpp = np.zeros(cap, np.float32)
+        self.lib.ref_symmetric_grids(_i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)), _i(_i3(fdim)), _f(_f3(fpix)),
+                                     _f(_m(fxyz)), _f(_f3(spacing)), _i(gdim), _f(gxyz), _f(cpp),
+                                     ctypes.c_size_t(cap))
+        return gdim, gxyz.reshape(4, 4), cpp
+
+    def f3d2_register(self, ref, rdim, rpix, rxyz, flo, fdim, fpix, fxyz, levels, maxit, be, le, bins, spacing):
+        """reg_f3d2<float>: (fw grid, bw grid, cdim, grid voxel->mm, squaring number,
+        [final symmetric NMI, final weighted BE, objective calls, gradient calls])."""
+        params = np.array([levels, maxit, be, le, bins, spacing, 0], np.float64)
+        ext = [n * p for n, p in zip(rdim, rpix)] + [n * p for n, p in zip(fdim, fpix)]
+        s = abs(spacing) * (min(list(rpix) + list(fpix)) if spacing < 0 else 1)
+        cap = 3 * int(np.prod([np.ceil(2 * max(ext) / s) + 8] * 3)) + 64
+        fw, bw = np.zeros(cap, np.float32), np.zeros(cap, np.float32)
+        cdim, cxyz, stats = np.zeros(3, np.int32), np.zeros(16, np.float32), np.zeros(4)
+        steps = ctypes.c_int(0)
+        rc = self.lib.ref_f3d2_register(_f(_f3(ref)), _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)), _f(_f3(flo)),
+                                        _i(_i3(fdim)), _f(_f3(fpix)), _f(_m(fxyz)), _d(params), _i(cdim), _f(fw),
+                                        _f(bw), ctypes.c_size_t(cap), _f(cxyz), ctypes.byref(steps), _d(stats))
+        if rc != 0:
+            raise RuntimeError("ref_f3d2_register failed")
+        n = 3 * int(np.prod(cdim))
+        return fw[:n].copy(), bw[:n].copy(), cdim, cxyz.reshape(4, 4), steps.value, stats
+
     def f3d_register2(self, ref, rdim, rpix, rxyz, flo, fdim, fpix, fxyz, levels, maxit, be, le, bins, spacing):
         """reg_f3d<float> on a reference and a floating image with their own geometry: (cpp, cdim,
         grid voxel->mm, [final NMI, final weighted BE, objective calls, gradient calls])."""

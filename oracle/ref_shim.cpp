@@ -12,6 +12,7 @@
 #include <memory>
 #include <vector>
 #include "_reg_f3d.h"
+#include "_reg_f3d2.h"
 #include "_reg_localTrans.h"
 #include "_reg_localTrans_regul.h"
 #include "_reg_nmi.h"
@@ -100,6 +101,27 @@ public:
     std::vector<Mark> marks;
     long objCalls = 0, gradCalls = 0;
 };
+
+class ShimF3d2: public reg_f3d2<float> {
+public:
+    ShimF3d2(): reg_f3d2<float>(1, 1) {}
+    double GetObjectiveFunctionValue() override { ++objCalls; return reg_f3d2<float>::GetObjectiveFunctionValue(); }
+    void GetObjectiveFunctionGradient() override { ++gradCalls; reg_f3d2<float>::GetObjectiveFunctionGradient(); }
+    double FinalWMeasure() const { return this->bestWMeasure; }
+    double FinalWBE() const { return this->bestWBE; }
+    double SimilarityWeight() const { return this->similarityWeight; }
+    long objCalls = 0, gradCalls = 0;
+};
+
+// a cubic B-spline velocity grid as reg_f3d2 tags it
+NiftiImage MakeVelocityGrid(const int *gdim, const float *gpix, const float *gxyz, const float *vel, int steps) {
+    NiftiImage grid = MakeImage(gdim, gpix, gxyz, 3);
+    memcpy(grid->data, vel, grid->nvox * sizeof(float));
+    grid->intent_code = NIFTI_INTENT_VECTOR;
+    grid->intent_p1 = SPLINE_VEL_GRID;
+    grid->intent_p2 = float(steps);
+    return grid;
+}
 
 }  // namespace
 
@@ -410,6 +432,125 @@ int ref_f3d_register2(const float *ref, const int *rdim, const float *rpix, cons
     const mat44& m = grid->sform_code > 0 ? grid->sto_xyz : grid->qto_xyz;
     for (int i = 0; i < 4; ++i)
         for (int j = 0; j < 4; ++j) cxyz_out[4 * i + j] = m.m[i][j];
+    stats[0] = reg.SimilarityWeight() > 0 ? reg.FinalWMeasure() / reg.SimilarityWeight() : 0;
+    stats[1] = reg.FinalWBE();
+    stats[2] = double(reg.objCalls);
+    stats[3] = double(reg.gradCalls);
+    return 0;
+}
+
+// reg_spline_getDefFieldFromVelocityGrid on a deformation field of the given geometry
+int ref_velocity_def_field(const float *vel, const int *gdim, const float *gpix, const float *gxyz, int steps,
+                           int update, const int *fdim, const float *fpix, const float *fxyz, float *def_out,
+                           int *steps_out) {
+    NiftiImage grid = MakeVelocityGrid(gdim, gpix, gxyz, vel, steps);
+    NiftiImage field = MakeImage(fdim, fpix, fxyz, 3);
+    reg_spline_getDefFieldFromVelocityGrid(grid, field, update != 0);
+    memcpy(def_out, field->data, field->nvox * sizeof(float));
+    *steps_out = int(grid->intent_p2);
+    return 0;
+}
+
+// reg_defField_compose: update <- apply(update)
+int ref_def_compose(const int *dim, const float *pix, const float *xyz, const float *apply, float *update) {
+    NiftiImage a = MakeImage(dim, pix, xyz, 3), u = MakeImage(dim, pix, xyz, 3);
+    memcpy(a->data, apply, a->nvox * sizeof(float));
+    memcpy(u->data, update, u->nvox * sizeof(float));
+    reg_defField_compose(a, u, nullptr);
+    memcpy(update, u->data, u->nvox * sizeof(float));
+    return 0;
+}
+
+// Compute::ExponentiateGradient (reg-lib/Compute.cpp:288-330, no affine) with the reference's
+// own functions, in its order, on a gradient image of the given geometry
+int ref_exponentiate_gradient(const int *fdim, const float *fpix, const float *fxyz, const float *vel,
+                              const int *gdim, const float *gpix, const float *gxyz, int steps, float *vgrad) {
+    NiftiImage grid = MakeVelocityGrid(gdim, gpix, gxyz, vel, steps);
+    NiftiImage field = MakeImage(fdim, fpix, fxyz, 3);
+    NiftiImage grad = MakeImage(fdim, fpix, fxyz, 3);
+    memcpy(grad->data, vgrad, grad->nvox * sizeof(float));
+    const size_t compNum = size_t(fabs(grid->intent_p2));
+    NiftiImage tempGrad(grad, NiftiImage::Copy::ImageInfoAndAllocData);
+    std::unique_ptr<NiftiImage[]> tempDef(new NiftiImage[compNum + 1]);
+    for (size_t i = 0; i <= compNum; ++i) tempDef[i] = NiftiImage(field, NiftiImage::Copy::ImageInfoAndAllocData);
+    reg_spline_getIntermediateDefFieldFromVelGrid(grid, tempDef.get());
+    for (size_t i = 0; i < compNum; ++i) {
+        reg_resampleGradient(grad, tempGrad, tempDef[i], 1, 0);
+        reg_tools_addImageToImage(tempGrad, grad, grad);
+    }
+    reg_tools_divideValueToImage(grad, grad, pow(2, compNum));
+    memcpy(vgrad, grad->data, grad->nvox * sizeof(float));
+    return 0;
+}
+
+// Compute::SymmetriseVelocityFields (reg-lib/Compute.cpp:356-392) with the reference's functions
+int ref_symmetrise(const int *gdim, const float *gpix, const float *fw_xyz, const float *bw_xyz, float *fw,
+                   float *bw) {
+    NiftiImage g = MakeImage(gdim, gpix, fw_xyz, 3), gb = MakeImage(gdim, gpix, bw_xyz, 3);
+    memcpy(g->data, fw, g->nvox * sizeof(float));
+    memcpy(gb->data, bw, gb->nvox * sizeof(float));
+    NiftiImage warpedTrans(gb, NiftiImage::Copy::ImageInfoAndAllocData);
+    NiftiImage warpedTransBw(g, NiftiImage::Copy::ImageInfoAndAllocData);
+    reg_getDisplacementFromDeformation(g);
+    reg_getDisplacementFromDeformation(gb);
+    warpedTrans.copyData(g);
+    warpedTransBw.copyData(gb);
+    reg_tools_subtractImageFromImage(gb, warpedTrans, gb);
+    reg_tools_subtractImageFromImage(g, warpedTransBw, g);
+    reg_tools_multiplyValueToImage(gb, gb, 0.5f);
+    reg_tools_multiplyValueToImage(g, g, 0.5f);
+    reg_getDeformationFromDisplacement(g);
+    reg_getDeformationFromDisplacement(gb);
+    memcpy(fw, g->data, g->nvox * sizeof(float));
+    memcpy(bw, gb->data, gb->nvox * sizeof(float));
+    return 0;
+}
+
+// reg_createSymmetricControlPointGrids (no affine): dims and voxel -> mm of the grids, and the
+// forward grid's identity positions
+int ref_symmetric_grids(const int *rdim, const float *rpix, const float *rxyz, const int *fdim, const float *fpix,
+                        const float *fxyz, const float *spacing, int *gdim, float *gxyz, float *cpp_out,
+                        size_t cap) {
+    NiftiImage r = MakeImage(rdim, rpix, rxyz), f = MakeImage(fdim, fpix, fxyz);
+    NiftiImage fw, bw;
+    reg_createSymmetricControlPointGrids<float>(fw, bw, r, f, nullptr, spacing);
+    gdim[0] = fw->nx; gdim[1] = fw->ny; gdim[2] = fw->nz;
+    for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) gxyz[4 * i + j] = fw->sto_xyz.m[i][j];
+    if (cpp_out) {
+        if (cap < fw->nvox) return -1;
+        memcpy(cpp_out, fw->data, fw->nvox * sizeof(float));
+    }
+    return 0;
+}
+
+// reg_f3d2<float> (the -vel / -sym registration): final grids, the forward grid's voxel -> mm,
+// the squaring number and [final symmetric NMI, final weighted BE, objective calls, gradient calls]
+int ref_f3d2_register(const float *ref, const int *rdim, const float *rpix, const float *rxyz, const float *flo,
+                      const int *fdim, const float *fpix, const float *fxyz, const double *params, int *cdim_out,
+                      float *fw_out, float *bw_out, size_t cap, float *cxyz_out, int *steps_out, double *stats) {
+    NiftiImage r = MakeImage(rdim, rpix, rxyz), f = MakeImage(fdim, fpix, fxyz);
+    memcpy(r->data, ref, Nvox(rdim) * sizeof(float));
+    memcpy(f->data, flo, Nvox(fdim) * sizeof(float));
+    ShimF3d2 reg;
+    reg.SetReferenceImage(r);
+    reg.SetFloatingImage(f);
+    reg.SetLevelNumber(unsigned(params[0]));
+    reg.SetLevelToPerform(unsigned(params[0]));
+    reg.SetMaximalIterationNumber(unsigned(params[1]));
+    reg.SetBendingEnergyWeight(float(params[2]));
+    reg.SetLinearEnergyWeight(float(params[3]));
+    reg.UseNMISetReferenceBinNumber(0, int(params[4]));
+    reg.UseNMISetFloatingBinNumber(0, int(params[4]));
+    reg.SetSpacing(0, float(params[5]));
+    if (params[6] == 0) reg.DoNotPrintOutInformation();
+    reg.Run();
+    NiftiImage fw = reg.GetControlPointPositionImage(), bw = reg.GetBackwardControlPointPositionImage();
+    cdim_out[0] = fw->nx; cdim_out[1] = fw->ny; cdim_out[2] = fw->nz;
+    if (cap < fw->nvox || cap < bw->nvox) return -1;
+    memcpy(fw_out, fw->data, fw->nvox * sizeof(float));
+    memcpy(bw_out, bw->data, bw->nvox * sizeof(float));
+    for (int i = 0; i < 4; ++i) for (int j = 0; j < 4; ++j) cxyz_out[4 * i + j] = fw->sto_xyz.m[i][j];
+    *steps_out = int(fw->intent_p2);
     stats[0] = reg.SimilarityWeight() > 0 ? reg.FinalWMeasure() / reg.SimilarityWeight() : 0;
     stats[1] = reg.FinalWBE();
     stats[2] = double(reg.objCalls);
