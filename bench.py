@@ -50,16 +50,56 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--mode", choices=["plain", "batched", "served", "warp"], default="plain")
+    ap.add_argument("--mode", choices=["plain", "batched", "served", "warp", "f3d2"], default="plain")
     ap.add_argument("--pairs", type=int, default=64, help="batched: number of pairs")
     ap.add_argument("--concurrency", type=int, default=16, help="batched/served: concurrent registrations")
     ap.add_argument("--requests", type=int, default=300, help="served: requests per arrival rate")
     ap.add_argument("--rates", default="5,20,50", help="served: Poisson arrival rates (requests/s)")
     ap.add_argument("--shape", default=None, help="kernel-only mode: nz,ny,nx of the volume (default: the workload's)")
-    ap.add_argument("--kernel", choices=["objective", "gradient"], default=None,
+    ap.add_argument("--kernel", choices=["objective", "gradient", "velocity", "compose"], default=None,
                     help="profiling mode: run only `--steps` fused evaluations at the finest level "
                          "of the workload (for ncu captures); prints per-launch device times")
     return ap.parse_args()
+
+
+def run_velocity_only(args, shape):
+    """`--steps` exponentiations of a velocity grid (F3D2: flow, scaling, 6 squarings) or
+    `--steps` single compositions, on a field of the workload's shape: a 5 mm velocity grid with
+    N(0, 3 mm) node displacements over the volume (one node of margin). Per-launch device times."""
+    import torch
+    import niftyreg_b200 as nrb
+
+    nz, ny, nx = shape
+    dim, pix = (nx, ny, nz), (1.0, 1.0, 1.0)
+    eye = nrb.identity_header(pix)
+    cdim = [int(np.ceil(v / 5.0 + 3)) + 1 for v in dim]
+    cxyz = nrb.identity_header((5.0, 5.0, 5.0), (-5.5, -5.5, -5.5))
+    rng = np.random.default_rng(args.seed)
+    cx, cy, cz = cdim
+    zz, yy, xx = np.meshgrid(np.arange(cz), np.arange(cy), np.arange(cx), indexing="ij")
+    ident = np.concatenate([(5.0 * v - 5.5).ravel() for v in (xx, yy, zz)]).astype(np.float32)
+    vel = torch.from_numpy(ident + rng.normal(0, 3.0, ident.size).astype(np.float32)).cuda()
+    g = nrb.make_geometry(dim, pix, eye, dim, pix, eye, cdim, (5.0, 5.0, 5.0), cxyz)
+    n = nx * ny * nz
+    d = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    nrb.get_def_field_from_velocity_grid(g, vel, 6, d)
+    torch.cuda.synchronize()
+    pos = d.clone()
+    nrb.timing_enable(True)
+    for _ in range(args.steps):
+        if args.kernel == "velocity":
+            nrb.get_def_field_from_velocity_grid(g, vel, 6, d)
+        else:
+            pos.copy_(d)
+            nrb.def_field_compose(dim, eye, d, pos)
+    torch.cuda.synchronize()
+    out = {k: nrb.timing_read(k) for k in ("f3d2_velocity", "f3d2_compose")}
+    nrb.timing_enable(False)
+    print(json.dumps({"mode": f"kernel-only {args.kernel}", "voxels": n, "nodes": int(np.prod(cdim)),
+                      "timing": {k: {"launches": v[0], "avg_us": (v[1] / v[0] * 1e3) if v[0] else None,
+                                     "GBps": (v[2] / (v[1] / 1e3) / 1e9) if v[1] and v[2] else None}
+                                 for k, v in out.items()}}))
+    return 0
 
 
 def run_kernel_only(args):
@@ -72,6 +112,8 @@ def run_kernel_only(args):
     torch.cuda.set_device(0)
     nrb.build()
     shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else SHAPE
+    if args.kernel in ("velocity", "compose"):
+        return run_velocity_only(args, shape)
     pair = phantom.brain_pair(shape, seed=args.seed)
     nz, ny, nx = shape
     dim, pix = (nx, ny, nz), (1.0, 1.0, 1.0)
@@ -641,6 +683,120 @@ def run_warp(args):
     return 0
 
 
+def run_f3d2(args):
+    """The symmetric registration (reg_f3d2, the -vel / -sym variant) of the workload's pair with
+    the workload's schedule, through nrb_f3d2_register_images (host images in, both grids and the
+    warped images out: copies included), against the reference's reg_f3d2<float> on the box's
+    host cores (a 1/10 iteration budget, extrapolated x10). Also the roofline of the composition
+    kernel (the squaring step, the most launched F3D2 kernel) timed alone on a full-size field."""
+    import torch
+    import niftyreg_b200 as nrb
+    from niftyreg_b200 import phantom
+
+    torch.cuda.set_device(0)
+    nrb.build()
+    pair = phantom.brain_pair(SHAPE, seed=args.seed)
+    pix = tuple(float(p) for p in pair.pixdim)
+    eye = nrb.identity_header(pix)
+    params = nrb.default_params(levels=LEVELS, max_iterations=MAXIT, bending_energy=BE, spacing=(SPACING,),
+                                ref_bins=BINS, flo_bins=BINS)
+    for _ in range(args.warmup):
+        nrb.f3d2_register_images(pair.reference, pix, eye, pair.floating, pix, eye, params)
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    secs, res = [], None
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        gf, gb, _, steps, wf, wb, res = nrb.f3d2_register_images(pair.reference, pix, eye, pair.floating, pix, eye,
+                                                                 params)
+        secs.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    t = float(np.mean(secs))
+    # one more registration with every F3D2 stage bracketed by CUDA events: where the time goes,
+    # and the composition kernel's launches inside a real registration
+    stages = ("f3d2_velocity", "f3d2_gradient_exp", "f3d2_warp", "f3d2_nmi", "f3d2_voxel_gradient", "f3d2_nodes",
+              "f3d2_be", "f3d2_update")
+    nrb.timing_enable(True)
+    t0 = time.perf_counter()
+    nrb.f3d2_register_images(pair.reference, pix, eye, pair.floating, pix, eye, params, warped=False)
+    t_timed = time.perf_counter() - t0
+    timed = {k: nrb.timing_read(k) for k in stages + ("f3d2_compose",)}
+    nrb.timing_enable(False)
+    stage_ms = {k: timed[k][1] for k in stages}
+    comp_n, comp_ms, comp_bytes = timed["f3d2_compose"]
+    # composition kernel alone: one squaring of a full-size smooth field (a few mm of displacement,
+    # as the fields of a registration are smooth)
+    nz, ny, nx = SHAPE
+    n = nx * ny * nz
+    k, j, i = np.meshgrid(np.arange(nz, dtype=np.float32), np.arange(ny, dtype=np.float32),
+                          np.arange(nx, dtype=np.float32), indexing="ij")
+    disp = 2.0 * np.sin(2 * np.pi * i / 61.0) * np.cos(2 * np.pi * j / 47.0) * np.sin(2 * np.pi * k / 53.0)
+    field = np.concatenate([(i + disp).ravel(), (j - disp).ravel(), (k + 0.5 * disp).ravel()])
+    apply_d = torch.from_numpy(field.astype(np.float32)).cuda()
+    pos_d = apply_d.clone()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    for _ in range(3):
+        nrb.def_field_compose((nx, ny, nz), eye, apply_d, pos_d, stream=stream)
+    ms = []
+    for _ in range(10):
+        with torch.cuda.stream(stream):
+            pos_d.copy_(apply_d)
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        nrb.def_field_compose((nx, ny, nz), eye, apply_d, pos_d, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    tc = float(np.mean(ms)) / 1e3
+    alg = 36.0 * n  # positions read, the applied field read once, the result written (3 x 4 B each)
+    peak, peak_kind = peaks()
+    line = {"mode": "f3d2", "metric": "symmetric F3D2 registrations/s (reg_f3d2, velocity grids)",
+            "value": 1.0 / t, "unit": "registrations/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD.replace("single-pair F3D", "single-pair F3D2 (symmetric, velocity grids)"),
+                       "api": "nrb_f3d2_register_images, host images in and out (copies inside the timed region)"},
+            "registration": {"final_symmetric_nmi": res.final_nmi, "objective_evaluations": res.objective_evaluations,
+                             "gradient_evaluations": res.gradient_evaluations, "squaring_steps": steps,
+                             "seconds": secs},
+            "roofline": {"kernel": "k_compose", "bound": "hbm",
+                         "achieved": comp_bytes / (comp_ms / 1e3) / 1e9 if comp_ms else None, "peak": peak,
+                         "unit": "GB/s", "frac": comp_bytes / (comp_ms / 1e3) / 1e9 / peak if comp_ms else None,
+                         "peak_source": peak_kind, "launches": comp_n,
+                         "avg_launch_us": comp_ms / max(comp_n, 1) * 1e3,
+                         "algorithmic_bytes_per_launch": comp_bytes / max(comp_n, 1),
+                         "alone_full_size": {"achieved": alg / tc / 1e9, "frac": alg / tc / 1e9 / peak,
+                                             "avg_launch_us": tc * 1e6, "algorithmic_bytes_per_launch": alg,
+                                             "field": "182x218x182, smooth displacement up to 2 mm, L2 flushed"}},
+            "stage_ms": {k: round(v, 3) for k, v in stage_ms.items()},
+            "stage_share_of_wall": {k: round(v / 1e3 / t_timed, 4) for k, v in stage_ms.items()},
+            "e2e": {"value": 1.0 / t, "unit": "registrations/s",
+                    "h2d_bytes_per_step": int(pair.reference.nbytes + pair.floating.nbytes),
+                    "d2h_bytes_per_step": int(gf.nbytes + gb.nbytes + wf.nbytes + wb.nbytes)},
+            "clocks": clocks}
+    if not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            R = oracle.Ref()
+            cores = R.set_threads(os.cpu_count() or 1)
+            dim = pair.dim
+            t0 = time.perf_counter()
+            _, _, _, _, _, st = R.f3d2_register(pair.reference.ravel(), dim, pix, eye, pair.floating.ravel(), dim,
+                                                pix, eye, LEVELS, REF_SAMPLE_MAXIT, BE, 0.0, BINS, SPACING)
+            wall = time.perf_counter() - t0
+            est = wall * MAXIT / REF_SAMPLE_MAXIT
+            line["cpu_baseline"] = {"value": 1.0 / est, "unit": "registrations/s", "cores": int(cores),
+                                    "kind": "reference",
+                                    "sample": f"reference reg_f3d2<float> (oracle/_ref, OpenMP) on the same pair with "
+                                              f"a 1/10 iteration budget ({REF_SAMPLE_MAXIT} at the finest level): "
+                                              f"{wall:.1f} s, x10 = {est:.1f} s per registration",
+                                    "sample_final_symmetric_nmi": float(st[0])}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -651,6 +807,8 @@ def main():
         return run_batched(args)
     if args.mode == "served":
         return run_served(args)
+    if args.mode == "f3d2":
+        return run_f3d2(args)
     if args.mode == "warp":
         return run_warp(args)
     return run_b200(args)

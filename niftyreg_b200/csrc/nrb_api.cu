@@ -53,7 +53,9 @@ std::vector<Pending> g_pending;
 std::vector<cudaEvent_t> g_pool;
 long long g_tlaunch[TK_COUNT] = {};
 double g_tms[TK_COUNT] = {}, g_tbytes[TK_COUNT] = {};
-const char *g_tnames[TK_COUNT] = { "objective", "gradient", "finalize", "conv", "be_value", "be_gradient" };
+const char *g_tnames[TK_COUNT] = { "objective", "gradient", "finalize", "conv", "be_value", "be_gradient",
+                                   "f3d2_velocity", "f3d2_compose", "f3d2_gradient_exp", "f3d2_warp", "f3d2_nmi",
+                                   "f3d2_voxel_gradient", "f3d2_nodes", "f3d2_be", "f3d2_update" };
 
 cudaEvent_t pooled_event() {
     if (!g_pool.empty()) {

@@ -79,7 +79,12 @@ inline void dev_free(void *p, cudaStream_t st) {
 
 // Optional per-kernel CUDA-event timing (nrb_timing_enable). A KernelTimer brackets one launch
 // with events on its stream and records the algorithmic bytes that launch must move.
-enum TimedKernel { TK_OBJECTIVE = 0, TK_GRADIENT, TK_FINALIZE, TK_CONV, TK_BE_VALUE, TK_BE_GRADIENT, TK_COUNT };
+enum TimedKernel {
+    TK_OBJECTIVE = 0, TK_GRADIENT, TK_FINALIZE, TK_CONV, TK_BE_VALUE, TK_BE_GRADIENT,
+    // F3D2 stages (a stage brackets all launches it makes on its stream) and kernels
+    TK_F2_VELOCITY, TK_F2_COMPOSE, TK_F2_GRADIENT_EXP, TK_F2_WARP, TK_F2_NMI, TK_F2_VOXEL_GRADIENT, TK_F2_NODES,
+    TK_F2_BE, TK_F2_UPDATE, TK_COUNT
+};
 class KernelTimer {
 public:
     KernelTimer(TimedKernel k, double bytes, cudaStream_t st);

@@ -1419,29 +1419,36 @@ private:
     nrb_status Warp(bool update) {
         NRB_TRY(velocity_to_deformation(&gfw_, fw(cur_), update, &steps_, def_fw_.p, nullptr, scr_r_.p, mm_, st_));
         NRB_TRY(velocity_to_deformation(&gbw_, bw(cur_), false, &steps_, def_bw_.p, nullptr, scr_f_.p, mm_, st_));
+        KernelTimer kt(TK_F2_WARP, 0.0, st_);
         NRB_TRY(nrb_resample_image(&gfw_, flo_.p, def_fw_.p, nullptr, pad_, war_fw_.p, st_));
         NRB_TRY(nrb_resample_image(&gbw_, ref_.p, def_bw_.p, nullptr, pad_, war_bw_.p, st_));
         return NRB_OK;
     }
-    nrb_status Similarity(double& nmi_fw, double& nmi_bw) {
-        NRB_TRY(nrb_nmi_value(nmi_fw_.h, &gfw_, ref_.p, war_fw_.p, nullptr, nullptr, &nmi_fw, st_));
-        NRB_TRY(nrb_nmi_value(nmi_bw_.h, &gbw_, flo_.p, war_bw_.p, nullptr, nullptr, &nmi_bw, st_));
+    // both NMI values into the device scalars (obj_[2], obj_[3]); no host read
+    nrb_status Similarity() {
+        KernelTimer kt(TK_F2_NMI, 0.0, st_);
+        NRB_TRY(nrb_nmi_value(nmi_fw_.h, &gfw_, ref_.p, war_fw_.p, nullptr, obj_ + 2, nullptr, st_));
+        NRB_TRY(nrb_nmi_value(nmi_bw_.h, &gbw_, flo_.p, war_bw_.p, nullptr, obj_ + 3, nullptr, st_));
         return NRB_OK;
     }
-    // reg_f3d2::GetObjectiveFunctionValue (_reg_f3d2.cpp:465-485)
+    // reg_f3d2::GetObjectiveFunctionValue (_reg_f3d2.cpp:465-485): both energies and both NMI
+    // values land in device scalars and come back in one read
     nrb_status GetObjectiveFunctionValue(bool update, double& value) {
-        double be_f = 0, be_b = 0;
         if (be_w_ > 0) {
-            NRB_TRY(nrb_approx_bending_energy(ws_fw_.h, &gfw_, fw(cur_), nullptr, &be_f, st_));
-            NRB_TRY(nrb_approx_bending_energy(ws_bw_.h, &gbw_, bw(cur_), nullptr, &be_b, st_));
+            KernelTimer kt(TK_F2_BE, 0.0, st_);
+            NRB_TRY(nrb_approx_bending_energy(ws_fw_.h, &gfw_, fw(cur_), obj_, nullptr, st_));
+            NRB_TRY(nrb_approx_bending_energy(ws_bw_.h, &gbw_, bw(cur_), obj_ + 1, nullptr, st_));
         }
-        cur_w_be_ = be_w_ > 0 ? (double)be_w_ * be_f + (double)be_w_ * be_b : 0.0;
-        cur_be_ = be_f + be_b;
-        double nf = 0, nb = 0;
         if (sim_w_ > 0) {
             NRB_TRY(Warp(update));
-            NRB_TRY(Similarity(nf, nb));
+            NRB_TRY(Similarity());
         }
+        NRB_CUDA(cudaMemcpyAsync(obj_h_, obj_, 4 * sizeof(nrb_objective), cudaMemcpyDeviceToHost, st_));
+        NRB_CUDA(cudaStreamSynchronize(st_));
+        const double be_f = be_w_ > 0 ? obj_h_[0].be : 0.0, be_b = be_w_ > 0 ? obj_h_[1].be : 0.0;
+        const double nf = sim_w_ > 0 ? obj_h_[2].nmi : 0.0, nb = sim_w_ > 0 ? obj_h_[3].nmi : 0.0;
+        cur_w_be_ = be_w_ > 0 ? (double)be_w_ * be_f + (double)be_w_ * be_b : 0.0;
+        cur_be_ = be_f + be_b;
         cur_nmi_ = nf + nb;
         cur_w_measure_ = sim_w_ > 0 ? (double)sim_w_ * (nf + nb) : 0.0;
         ++n_obj_;
@@ -1454,14 +1461,18 @@ private:
         const int64_t nr = nvox(gfw_.ref_dim), nf = nvox(gbw_.ref_dim);
         if (sim_w_ > 0) {
             NRB_TRY(Warp(true));
-            NRB_CUDA(cudaMemsetAsync(vg_fw_.p, 0, 3 * nr * sizeof(float), st_));
-            NRB_CUDA(cudaMemsetAsync(vg_bw_.p, 0, 3 * nf * sizeof(float), st_));
-            NRB_TRY(nrb_get_image_gradient(&gfw_, flo_.p, def_fw_.p, nullptr, pad_, wg_fw_.p, st_));
-            NRB_TRY(nrb_get_image_gradient(&gbw_, ref_.p, def_bw_.p, nullptr, pad_, wg_bw_.p, st_));
-            double a, b;
-            NRB_TRY(Similarity(a, b));  // reg_nmi::GetVoxelBasedSimilarityMeasureGradientFw recomputes both
-            NRB_TRY(nrb_nmi_voxel_gradient(nmi_fw_.h, &gfw_, ref_.p, war_fw_.p, wg_fw_.p, nullptr, 1.0, vg_fw_.p, st_));
-            NRB_TRY(nrb_nmi_voxel_gradient(nmi_bw_.h, &gbw_, flo_.p, war_bw_.p, wg_bw_.p, nullptr, 1.0, vg_bw_.p, st_));
+            NRB_TRY(Similarity());  // reg_nmi::GetVoxelBasedSimilarityMeasureGradientFw recomputes both
+            {
+                KernelTimer kt(TK_F2_VOXEL_GRADIENT, 0.0, st_);
+                NRB_CUDA(cudaMemsetAsync(vg_fw_.p, 0, 3 * nr * sizeof(float), st_));
+                NRB_CUDA(cudaMemsetAsync(vg_bw_.p, 0, 3 * nf * sizeof(float), st_));
+                NRB_TRY(nrb_get_image_gradient(&gfw_, flo_.p, def_fw_.p, nullptr, pad_, wg_fw_.p, st_));
+                NRB_TRY(nrb_get_image_gradient(&gbw_, ref_.p, def_bw_.p, nullptr, pad_, wg_bw_.p, st_));
+                NRB_TRY(nrb_nmi_voxel_gradient(nmi_fw_.h, &gfw_, ref_.p, war_fw_.p, wg_fw_.p, nullptr, 1.0, vg_fw_.p,
+                                               st_));
+                NRB_TRY(nrb_nmi_voxel_gradient(nmi_bw_.h, &gbw_, flo_.p, war_bw_.p, wg_bw_.p, nullptr, 1.0, vg_bw_.p,
+                                               st_));
+            }
             // forward gradient along the backward transformation on the reference grid, and back
             NRB_TRY(Fields(std::max(nr, nf)));
             nrb_geometry gx = gfw_;
@@ -1474,6 +1485,7 @@ private:
             memcpy(gx.cpp_xyz, gfw_.cpp_xyz, sizeof(gx.cpp_xyz));
             memcpy(gx.cpp_ijk, gfw_.cpp_ijk, sizeof(gx.cpp_ijk));
             NRB_TRY(exponentiate_gradient(&gx, fw(cur_), steps_, vg_bw_.p, fields_.p, scr_f_.p, mm_, st_));
+            KernelTimer kt(TK_F2_NODES, 0.0, st_);
             NRB_TRY(nrb_convolve_voxel_based_gradient(ws_fw_.h, &gfw_, vg_fw_.p, sim_w_, fw(grad_), st_));
             NRB_TRY(nrb_convolve_voxel_based_gradient(ws_bw_.h, &gbw_, vg_bw_.p, sim_w_, bw(grad_), st_));
         } else {
@@ -1510,6 +1522,7 @@ private:
     // reg_f3d2::UpdateParameters (_reg_f3d2.cpp:652-684): best + scale * gradient for both grids
     // (UpdateVelocityField), then SymmetriseVelocityFields
     nrb_status UpdateParameters(float scale) {
+        KernelTimer kt(TK_F2_UPDATE, 0.0, st_);
         NRB_TRY(nrb_update_control_point_position(cur_.p, best_.p, grad_.p, scale, 6 * nc_, st_));
         return symmetrise_velocity(gf_.dim, gfw_.cpp_xyz, fw(cur_), gbw_.cpp_xyz, bw(cur_), st_);
     }
@@ -1555,6 +1568,8 @@ private:
     DevBuf def_fw_, def_bw_, war_fw_, war_bw_, wg_fw_, wg_bw_, vg_fw_, vg_bw_, scr_r_, scr_f_, fields_;
     int64_t fields_n_ = 0;
     unsigned *mm_ = nullptr;
+    nrb_objective *obj_ = nullptr;    // device: BE forward, BE backward, NMI forward, NMI backward
+    nrb_objective *obj_h_ = nullptr;  // pinned host copy
     NmiHandle nmi_fw_, nmi_bw_;
     WsHandle ws_fw_, ws_bw_;
     float pad_ = std::numeric_limits<float>::quiet_NaN();
@@ -1567,7 +1582,11 @@ private:
     int64_t n_obj_ = 0, n_grad_ = 0;
 
 public:
-    ~F3d2Registration() { dev_free(mm_, st_); }
+    ~F3d2Registration() {
+        dev_free(mm_, st_);
+        dev_free(obj_, st_);
+        if (obj_h_) cudaFreeHost(obj_h_);
+    }
 };
 
 // reg_f3d2::InitCurrentLevel (_reg_f3d2.cpp:52-102) + InitialiseSimilarity + SetOptimiser
@@ -1651,6 +1670,9 @@ nrb_status F3d2Registration::Run(const float *ref, const float *flo, const Image
         sim_w_ = 1 - penalty;
     }
     NRB_CUDA(dev_alloc(&mm_, 2 * sizeof(unsigned), st_));
+    NRB_CUDA(dev_alloc(&obj_, 4 * sizeof(nrb_objective), st_));
+    NRB_CUDA(cudaMemsetAsync(obj_, 0, 4 * sizeof(nrb_objective), st_));
+    NRB_CUDA(cudaMallocHost(&obj_h_, 4 * sizeof(nrb_objective)));
     NRB_TRY(build_pyramids(ref, flo, rd, fd, levels_, st_, hdr_, fhdr_, ref_pyr_, flo_pyr_));
     // reg_f3d2::Initialise (_reg_f3d2.cpp:539-610): spacing in voxels of the mean of both images'
     // input spacings, times 2^(levels - 1), grids over the coarsest images
@@ -1803,6 +1825,12 @@ extern "C" nrb_status nrb_f3d2_register_images(const nrb_image *ref, const nrb_i
     const auto t0 = std::chrono::steady_clock::now();
     cudaStream_t st = nullptr;
     NRB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    // the buffers a level frees stay in the pool for the next (the F3D footprint of the larger
+    // image, doubled for the second direction)
+    {
+        const int32_t *big = nflo > nref ? flo->dim : ref->dim;
+        keep_pool(2 * registration_footprint(big, ref->pixdim, p));
+    }
     nrb_status s = NRB_OK;
     float *fw = nullptr, *bw = nullptr, *wf = nullptr, *wb = nullptr;
     {

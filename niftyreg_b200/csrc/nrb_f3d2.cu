@@ -101,50 +101,115 @@ float fkey_inv(unsigned k) {
 // of every voxel, minus that position. The 64 taps are summed as the SSE build sums them: four
 // x-lanes accumulated over (z, y), then the lanes added in order. Also the extrema of all three
 // components (the squaring-number rule, :3514-3521).
-__global__ void __launch_bounds__(256) k_velocity_flow(const float *__restrict__ vel, int gx, int gy, int gz,
-                                                      Mat34 gxyz, Mat34 gijk, FieldGeom f, float *__restrict__ disp,
+// One axis of the flow's sampling when the field's voxel -> mm and the grid's mm -> voxel
+// matrices are both diagonal: then the identity coordinate, the grid coordinate and so the node
+// index and the four basis values along an axis depend on that axis's voxel index alone (every
+// off-diagonal product is an exact zero and adds nothing), and are the same floats as the
+// per-voxel evaluation gives.
+struct AxisEntry {
+    float w[4];
+    float r;  // identity coordinate (mm)
+    int pre;  // first node
+};
+
+__global__ void k_axis_table(int axis, int n, FieldGeom f, Mat34 gijk, AxisEntry *__restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float fx = axis == 0 ? (float)t : 0.f, fy = axis == 1 ? (float)t : 0.f, fz = axis == 2 ? (float)t : 0.f;
+    const float rx = row(f.xyz.m, fx, fy, fz), ry = row(f.xyz.m + 4, fx, fy, fz), rz = row(f.xyz.m + 8, fx, fy, fz);
+    const float v = row(gijk.m + 4 * axis, rx, ry, rz);
+    const int p = floor_int(v);
+    const float b = v - (float)p;
+    AxisEntry e;
+    bspline_basis_f64(b < 0 ? 0.f : b, e.w);
+    e.r = axis == 0 ? rx : (axis == 1 ? ry : rz);
+    e.pre = p - 1;
+    out[t] = e;
+}
+
+// at most 85 registers: three blocks of 256 threads per SM hide the tap loads' latency
+template <bool kTable>
+__global__ void __launch_bounds__(256, 3) k_velocity_flow(const float *__restrict__ vel, int gx, int gy, int gz,
+                                                      Mat34 gxyz, Mat34 gijk, FieldGeom f,
+                                                      const AxisEntry *__restrict__ tab, float *__restrict__ disp,
                                                       unsigned *__restrict__ minmax) {
     const long long n = (long long)f.nx * f.ny * f.nz;
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     float lo = INFINITY, hi = -INFINITY;
     if (i < n) {
         const int x = (int)(i % f.nx), y = (int)((i / f.nx) % f.ny), z = (int)(i / ((long long)f.nx * f.ny));
-        const float fx = (float)x, fy = (float)y, fz = (float)z;
-        const float rx = row(f.xyz.m, fx, fy, fz), ry = row(f.xyz.m + 4, fx, fy, fz), rz = row(f.xyz.m + 8, fx, fy, fz);
-        const float vx = row(gijk.m, rx, ry, rz), vy = row(gijk.m + 4, rx, ry, rz), vz = row(gijk.m + 8, rx, ry, rz);
-        int xp = floor_int(vx), yp = floor_int(vy), zp = floor_int(vz);
-        float b = vx - (float)xp;
-        float xb[4], yb[4], zb[4];
-        bspline_basis_f64(b < 0 ? 0.f : b, xb);
-        b = vy - (float)yp;
-        bspline_basis_f64(b < 0 ? 0.f : b, yb);
-        b = vz - (float)zp;
-        bspline_basis_f64(b < 0 ? 0.f : b, zb);
-        --xp;
-        --yp;
-        --zp;
+        float rx, ry, rz, xb[4], yb[4], zb[4];
+        int xp, yp, zp;
+        if (kTable) {
+            const AxisEntry ex = tab[x], ey = tab[f.nx + y], ez = tab[f.nx + f.ny + z];
+            rx = ex.r;
+            ry = ey.r;
+            rz = ez.r;
+            xp = ex.pre;
+            yp = ey.pre;
+            zp = ez.pre;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                xb[k] = ex.w[k];
+                yb[k] = ey.w[k];
+                zb[k] = ez.w[k];
+            }
+        } else {
+            const float fx = (float)x, fy = (float)y, fz = (float)z;
+            rx = row(f.xyz.m, fx, fy, fz);
+            ry = row(f.xyz.m + 4, fx, fy, fz);
+            rz = row(f.xyz.m + 8, fx, fy, fz);
+            const float vx = row(gijk.m, rx, ry, rz), vy = row(gijk.m + 4, rx, ry, rz), vz = row(gijk.m + 8, rx, ry, rz);
+            xp = floor_int(vx);
+            yp = floor_int(vy);
+            zp = floor_int(vz);
+            float b = vx - (float)xp;
+            bspline_basis_f64(b < 0 ? 0.f : b, xb);
+            b = vy - (float)yp;
+            bspline_basis_f64(b < 0 ? 0.f : b, yb);
+            b = vz - (float)zp;
+            bspline_basis_f64(b < 0 ? 0.f : b, zb);
+            --xp;
+            --yp;
+            --zp;
+        }
         const long long gn = (long long)gx * gy * gz;
         const float *cx = vel, *cy = vel + gn, *cz = vel + 2 * gn;
-        const bool inside = xp >= 0 && xp + 3 < gx && yp >= 0 && yp + 3 < gy && zp >= 0 && zp + 3 < gz;
         float tx[4] = { 0.f, 0.f, 0.f, 0.f }, ty[4] = { 0.f, 0.f, 0.f, 0.f }, tz[4] = { 0.f, 0.f, 0.f, 0.f };
-        for (int c = 0; c < 4; ++c) {
-            for (int bb = 0; bb < 4; ++bb) {
-                const float yz = yb[bb] * zb[c];
+        if (xp >= 0 && xp + 3 < gx && yp >= 0 && yp + 3 < gy && zp >= 0 && zp + 3 < gz) {
+            // every tap inside the grid: one row pointer per (z, y), the taps in the same order
+            const float *p0 = cx + ((long long)zp * gy + yp) * gx + xp;
+#pragma unroll 1
+            for (int c = 0; c < 4; ++c) {
+#pragma unroll 1
+                for (int bb = 0; bb < 4; ++bb) {
+                    const float *q = p0 + (c * gy + bb) * gx;
+                    const float yz = yb[bb] * zb[c];
 #pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    const float w = yz * xb[a];
-                    float px, py, pz;
-                    if (inside) {
-                        const long long j = ((long long)(zp + c) * gy + (yp + bb)) * gx + (xp + a);
-                        px = __ldg(cx + j);
-                        py = __ldg(cy + j);
-                        pz = __ldg(cz + j);
-                    } else {
-                        slided(cx, cy, cz, xp + a, yp + bb, zp + c, gx, gy, gz, gxyz, px, py, pz);
+                    for (int a = 0; a < 4; ++a) {
+                        const float w = yz * xb[a];
+                        tx[a] = w * __ldg(q + a) + tx[a];
+                        ty[a] = w * __ldg(q + gn + a) + ty[a];
+                        tz[a] = w * __ldg(q + 2 * gn + a) + tz[a];
                     }
-                    tx[a] = w * px + tx[a];
-                    ty[a] = w * py + ty[a];
-                    tz[a] = w * pz + tz[a];
+                }
+            }
+        } else {
+            // a border voxel: sliding values, the taps in the same order
+#pragma unroll 1
+            for (int c = 0; c < 4; ++c) {
+#pragma unroll 1
+                for (int bb = 0; bb < 4; ++bb) {
+                    const float yz = yb[bb] * zb[c];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        const float w = yz * xb[a];
+                        float px, py, pz;
+                        slided(cx, cy, cz, xp + a, yp + bb, zp + c, gx, gy, gz, gxyz, px, py, pz);
+                        tx[a] = w * px + tx[a];
+                        ty[a] = w * py + ty[a];
+                        tz[a] = w * pz + tz[a];
+                    }
                 }
             }
         }
@@ -169,6 +234,11 @@ __global__ void __launch_bounds__(256) k_velocity_flow(const float *__restrict__
     }
 }
 
+__global__ void k_minmax_init(unsigned *minmax) {
+    minmax[0] = 0xffffffffu;
+    minmax[1] = 0u;
+}
+
 // displacement / 2^N back to a deformation (reg_defField_getDeformationFieldFromFlowField,
 // :3537-3547): scale is 2^-N, exact, as the reference's double division by 2^N is
 __global__ void __launch_bounds__(256) k_flow_scale(float *__restrict__ d, float scale, FieldGeom f) {
@@ -185,51 +255,88 @@ __global__ void __launch_bounds__(256) k_flow_scale(float *__restrict__ d, float
 // reg_defField_compose3D (reg-lib/cpu/_reg_localTrans.cpp:2334-2458): out(x) = apply(pos(x)),
 // trilinear in the apply field's voxel space, sliding (linear extrapolation of the positions)
 // outside it. out may alias pos (each voxel reads only its own position), never apply.
-__global__ void __launch_bounds__(256) k_compose(const float *__restrict__ apply, const float *pos, float *out,
+constexpr int kComposeVox = 2;  // voxels per thread: their position loads and gathers overlap
+
+__global__ void __launch_bounds__(256, 4) k_compose(const float *__restrict__ apply, const float *pos, float *out,
                                                 FieldGeom f) {
     const long long n = (long long)f.nx * f.ny * f.nz;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float px = pos[i], py = pos[n + i], pz = pos[2 * n + i];
-    const float vx = row(f.ijk.m, px, py, pz), vy = row(f.ijk.m + 4, px, py, pz), vz = row(f.ijk.m + 8, px, py, pz);
-    const int x0 = floor_int(vx), y0 = floor_int(vy), z0 = floor_int(vz);
-    float rx[2], ry[2], rz[2];
-    rx[1] = vx - (float)x0;
-    rx[0] = 1.f - rx[1];
-    ry[1] = vy - (float)y0;
-    ry[0] = 1.f - ry[1];
-    rz[1] = vz - (float)z0;
-    rz[0] = 1.f - rz[1];
+    const long long base = (long long)blockIdx.x * blockDim.x * kComposeVox + threadIdx.x;
     const float *ax = apply, *ay = apply + n, *az = apply + 2 * n;
-    float ox = 0.f, oy = 0.f, oz = 0.f;
-    for (int c = 0; c < 2; ++c) {
-        const int z = z0 + c;
-        const bool inz = z > -1 && z < f.nz;
-        for (int b = 0; b < 2; ++b) {
-            const int y = y0 + b;
-            const float tb = ry[b] * rz[c];
-            const bool iny = y > -1 && y < f.ny;
-            for (int a = 0; a < 2; ++a) {
-                const int x = x0 + a;
-                float dx, dy, dz;
-                if (x > -1 && x < f.nx && iny && inz) {
-                    const long long j = ((long long)z * f.ny + y) * f.nx + x;
-                    dx = __ldg(ax + j);
-                    dy = __ldg(ay + j);
-                    dz = __ldg(az + j);
-                } else {
-                    slided(ax, ay, az, x, y, z, f.nx, f.ny, f.nz, f.xyz, dx, dy, dz);
-                }
-                const float w = rx[a] * tb;
-                ox = ox + dx * w;
-                oy = oy + dy * w;
-                oz = oz + dz * w;
-            }
+    float px[kComposeVox], py[kComposeVox], pz[kComposeVox];
+#pragma unroll
+    for (int v = 0; v < kComposeVox; ++v) {
+        const long long i = base + (long long)v * blockDim.x;
+        if (i < n) {
+            px[v] = pos[i];
+            py[v] = pos[n + i];
+            pz[v] = pos[2 * n + i];
         }
     }
-    out[i] = ox;
-    out[n + i] = oy;
-    out[2 * n + i] = oz;
+#pragma unroll
+    for (int v = 0; v < kComposeVox; ++v) {
+        const long long i = base + (long long)v * blockDim.x;
+        if (i >= n) continue;
+        const float vx = row(f.ijk.m, px[v], py[v], pz[v]), vy = row(f.ijk.m + 4, px[v], py[v], pz[v]),
+                    vz = row(f.ijk.m + 8, px[v], py[v], pz[v]);
+        const int x0 = floor_int(vx), y0 = floor_int(vy), z0 = floor_int(vz);
+        float rx[2], ry[2], rz[2];
+        rx[1] = vx - (float)x0;
+        rx[0] = 1.f - rx[1];
+        ry[1] = vy - (float)y0;
+        ry[0] = 1.f - ry[1];
+        rz[1] = vz - (float)z0;
+        rz[0] = 1.f - rz[1];
+        float ox = 0.f, oy = 0.f, oz = 0.f;
+        if (x0 >= 0 && x0 + 1 < f.nx && y0 >= 0 && y0 + 1 < f.ny && z0 >= 0 && z0 + 1 < f.nz) {
+            // every tap inside the field: offsets from one base, the taps in the same order
+            const long long j0 = ((long long)z0 * f.ny + y0) * f.nx + x0;
+            const long long sy = f.nx, sz = (long long)f.nx * f.ny;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    const long long j = j0 + c * sz + b * sy;
+                    const float tb = ry[b] * rz[c];
+#pragma unroll
+                    for (int a = 0; a < 2; ++a) {
+                        const float w = rx[a] * tb;
+                        ox = ox + __ldg(ax + j + a) * w;
+                        oy = oy + __ldg(ay + j + a) * w;
+                        oz = oz + __ldg(az + j + a) * w;
+                    }
+                }
+            }
+        } else {
+            for (int c = 0; c < 2; ++c) {
+                const int z = z0 + c;
+                const bool inz = z > -1 && z < f.nz;
+                for (int b = 0; b < 2; ++b) {
+                    const int y = y0 + b;
+                    const float tb = ry[b] * rz[c];
+                    const bool iny = y > -1 && y < f.ny;
+                    for (int a = 0; a < 2; ++a) {
+                        const int x = x0 + a;
+                        float dx, dy, dz;
+                        if (x > -1 && x < f.nx && iny && inz) {
+                            const long long j = ((long long)z * f.ny + y) * f.nx + x;
+                            dx = __ldg(ax + j);
+                            dy = __ldg(ay + j);
+                            dz = __ldg(az + j);
+                        } else {
+                            slided(ax, ay, az, x, y, z, f.nx, f.ny, f.nz, f.xyz, dx, dy, dz);
+                        }
+                        const float w = rx[a] * tb;
+                        ox = ox + dx * w;
+                        oy = oy + dy * w;
+                        oz = oz + dz * w;
+                    }
+                }
+            }
+        }
+        out[i] = ox;
+        out[n + i] = oy;
+        out[2 * n + i] = oz;
+    }
 }
 
 struct Mat33f {
@@ -343,6 +450,11 @@ __global__ void __launch_bounds__(256) k_symmetrise(float *__restrict__ fw, floa
 }
 
 inline unsigned blocks_for(long long n) { return (unsigned)((n + 255) / 256); }
+inline unsigned compose_blocks(long long n) { return (unsigned)((n + 256LL * kComposeVox - 1) / (256LL * kComposeVox)); }
+
+// algorithmic bytes of one composition per voxel: its position read, the applied field read once
+// and the result written, 3 x 4 bytes each
+constexpr double kComposeBytes = 36.0;
 
 }  // namespace
 
@@ -366,20 +478,42 @@ nrb_status velocity_to_deformation(const nrb_geometry *g, const float *vel, bool
     const FieldGeom f = field_geom(g->ref_dim, g->ref_xyz, g->ref_ijk);
     const long long n = nvox(g->ref_dim);
     if (!def && !fields) return fail(NRB_ERR_INVALID, "velocity exponentiation: no output");
+    KernelTimer stage(TK_F2_VELOCITY, 0.0, st);
     int N = *steps;
     // the flow (displacement) lands where the squarings start: the first intermediate field, or
     // the buffer from which N ping-pong squarings end in def
     float *first = fields ? fields : (N % 2 == 0 ? def : scratch);
     if (update) {
-        const unsigned init[2] = { 0xffffffffu, 0u };
-        NRB_CUDA(cudaMemcpyAsync(minmax, init, sizeof(init), cudaMemcpyHostToDevice, st));
+        k_minmax_init<<<1, 1, 0, st>>>(minmax);
+        NRB_LAUNCHED("k_minmax_init");
     }
-    k_velocity_flow<<<blocks_for(n), 256, 0, st>>>(vel, g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2],
-                                                   to_mat34(g->cpp_xyz), to_mat34(g->cpp_ijk), f, first, minmax);
+    auto diagonal = [](const float *m) {
+        return m[1] == 0.f && m[2] == 0.f && m[4] == 0.f && m[6] == 0.f && m[8] == 0.f && m[9] == 0.f;
+    };
+    if (diagonal(g->ref_xyz) && diagonal(g->cpp_ijk)) {
+        const int nt = f.nx + f.ny + f.nz;
+        AxisEntry *tab = nullptr;
+        NRB_CUDA(dev_alloc(&tab, nt * sizeof(AxisEntry), st));
+        const int off[3] = { 0, f.nx, f.nx + f.ny }, len[3] = { f.nx, f.ny, f.nz };
+        for (int a = 0; a < 3; ++a) {
+            k_axis_table<<<(len[a] + 127) / 128, 128, 0, st>>>(a, len[a], f, to_mat34(g->cpp_ijk), tab + off[a]);
+            NRB_LAUNCHED("k_axis_table");
+        }
+        k_velocity_flow<true><<<blocks_for(n), 256, 0, st>>>(vel, g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2],
+                                                             to_mat34(g->cpp_xyz), to_mat34(g->cpp_ijk), f, tab,
+                                                             first, minmax);
+        dev_free(tab, st);
+    } else {
+        k_velocity_flow<false><<<blocks_for(n), 256, 0, st>>>(vel, g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2],
+                                                              to_mat34(g->cpp_xyz), to_mat34(g->cpp_ijk), f, nullptr,
+                                                              first, minmax);
+    }
     NRB_LAUNCHED("k_velocity_flow");
     if (update) {
-        unsigned mm[2];
-        NRB_CUDA(cudaMemcpyAsync(mm, minmax, sizeof(mm), cudaMemcpyDeviceToHost, st));
+        // the extrema land in pinned host memory (a pageable copy would stage through the driver)
+        static thread_local unsigned *mm = nullptr;
+        if (!mm) NRB_CUDA(cudaMallocHost(&mm, 2 * sizeof(unsigned)));
+        NRB_CUDA(cudaMemcpyAsync(mm, minmax, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         NRB_CUDA(cudaStreamSynchronize(st));
         N = velocity_squaring_steps(fkey_inv(mm[0]), fkey_inv(mm[1]));
         *steps = N;
@@ -395,19 +529,22 @@ nrb_status velocity_to_deformation(const nrb_geometry *g, const float *vel, bool
     if (fields) {
         // keep every intermediate field; the last squaring only when def is wanted
         for (int k = 1; k < N; ++k) {
-            k_compose<<<blocks_for(n), 256, 0, st>>>(fields + (k - 1) * 3 * n, fields + (k - 1) * 3 * n,
+            KernelTimer kt(TK_F2_COMPOSE, kComposeBytes * n, st);
+            k_compose<<<compose_blocks(n), 256, 0, st>>>(fields + (k - 1) * 3 * n, fields + (k - 1) * 3 * n,
                                                      fields + k * 3 * n, f);
             NRB_LAUNCHED("k_compose");
         }
         if (def) {
-            k_compose<<<blocks_for(n), 256, 0, st>>>(fields + (N - 1) * 3 * n, fields + (N - 1) * 3 * n, def, f);
+            KernelTimer kt(TK_F2_COMPOSE, kComposeBytes * n, st);
+            k_compose<<<compose_blocks(n), 256, 0, st>>>(fields + (N - 1) * 3 * n, fields + (N - 1) * 3 * n, def, f);
             NRB_LAUNCHED("k_compose");
         }
         return NRB_OK;
     }
     float *a = first, *b = first == def ? scratch : def;
     for (int k = 0; k < N; ++k) {
-        k_compose<<<blocks_for(n), 256, 0, st>>>(a, a, b, f);
+        KernelTimer kt(TK_F2_COMPOSE, kComposeBytes * n, st);
+        k_compose<<<compose_blocks(n), 256, 0, st>>>(a, a, b, f);
         NRB_LAUNCHED("k_compose");
         std::swap(a, b);
     }
@@ -417,7 +554,8 @@ nrb_status velocity_to_deformation(const nrb_geometry *g, const float *vel, bool
 nrb_status compose_fields(const int32_t dim[3], const float xyz[16], const float ijk[16], const float *apply,
                           float *update, cudaStream_t st) {
     const FieldGeom f = field_geom(dim, xyz, ijk);
-    k_compose<<<blocks_for(nvox(dim)), 256, 0, st>>>(apply, update, update, f);
+    KernelTimer kt(TK_F2_COMPOSE, kComposeBytes * nvox(dim), st);
+    k_compose<<<compose_blocks(nvox(dim)), 256, 0, st>>>(apply, update, update, f);
     NRB_LAUNCHED("k_compose");
     return NRB_OK;
 }
@@ -481,6 +619,7 @@ static void real_spacing(const float xyz[16], float sp[3]) {
 nrb_status exponentiate_gradient(const nrb_geometry *g, const float *vel_other, int steps, float *vgrad,
                                  float *fields, float *scratch, unsigned *minmax, cudaStream_t st) {
     if (steps < 1) return fail(NRB_ERR_INVALID, "gradient exponentiation: the squaring number must be >= 1");
+    KernelTimer stage(TK_F2_GRADIENT_EXP, 0.0, st);
     int N = steps;
     NRB_TRY(velocity_to_deformation(g, vel_other, false, &N, nullptr, fields, scratch, minmax, st));
     const FieldGeom f = field_geom(g->ref_dim, g->ref_xyz, g->ref_ijk);
