@@ -751,6 +751,7 @@ def run_f3d2(args):
         ms.append(e0.elapsed_time(e1))
     tc = float(np.mean(ms)) / 1e3
     alg = 36.0 * n  # positions read, the applied field read once, the result written (3 x 4 B each)
+    # (inside the registration every composition is a squaring: the field applied to itself, 24 B)
     peak, peak_kind = peaks()
     line = {"mode": "f3d2", "metric": "symmetric F3D2 registrations/s (reg_f3d2, velocity grids)",
             "value": 1.0 / t, "unit": "registrations/s", "n_gpus": 1, "steps": args.steps,

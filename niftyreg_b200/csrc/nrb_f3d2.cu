@@ -255,9 +255,9 @@ __global__ void __launch_bounds__(256) k_flow_scale(float *__restrict__ d, float
 // reg_defField_compose3D (reg-lib/cpu/_reg_localTrans.cpp:2334-2458): out(x) = apply(pos(x)),
 // trilinear in the apply field's voxel space, sliding (linear extrapolation of the positions)
 // outside it. out may alias pos (each voxel reads only its own position), never apply.
-constexpr int kComposeVox = 2;  // voxels per thread: their position loads and gathers overlap
+constexpr int kComposeVox = 4;  // voxels per thread: their position loads and gathers overlap
 
-__global__ void __launch_bounds__(256, 4) k_compose(const float *__restrict__ apply, const float *pos, float *out,
+__global__ void __launch_bounds__(256, 3) k_compose(const float *__restrict__ apply, const float *pos, float *out,
                                                 FieldGeom f) {
     const long long n = (long long)f.nx * f.ny * f.nz;
     const long long base = (long long)blockIdx.x * blockDim.x * kComposeVox + threadIdx.x;
@@ -453,8 +453,9 @@ inline unsigned blocks_for(long long n) { return (unsigned)((n + 255) / 256); }
 inline unsigned compose_blocks(long long n) { return (unsigned)((n + 256LL * kComposeVox - 1) / (256LL * kComposeVox)); }
 
 // algorithmic bytes of one composition per voxel: its position read, the applied field read once
-// and the result written, 3 x 4 bytes each
-constexpr double kComposeBytes = 36.0;
+// and the result written, 3 x 4 bytes each; a squaring step applies the field to itself, so the
+// positions and the applied field are one read
+constexpr double kComposeBytes = 36.0, kSquaringBytes = 24.0;
 
 }  // namespace
 
@@ -529,13 +530,13 @@ nrb_status velocity_to_deformation(const nrb_geometry *g, const float *vel, bool
     if (fields) {
         // keep every intermediate field; the last squaring only when def is wanted
         for (int k = 1; k < N; ++k) {
-            KernelTimer kt(TK_F2_COMPOSE, kComposeBytes * n, st);
+            KernelTimer kt(TK_F2_COMPOSE, kSquaringBytes * n, st);
             k_compose<<<compose_blocks(n), 256, 0, st>>>(fields + (k - 1) * 3 * n, fields + (k - 1) * 3 * n,
                                                      fields + k * 3 * n, f);
             NRB_LAUNCHED("k_compose");
         }
         if (def) {
-            KernelTimer kt(TK_F2_COMPOSE, kComposeBytes * n, st);
+            KernelTimer kt(TK_F2_COMPOSE, kSquaringBytes * n, st);
             k_compose<<<compose_blocks(n), 256, 0, st>>>(fields + (N - 1) * 3 * n, fields + (N - 1) * 3 * n, def, f);
             NRB_LAUNCHED("k_compose");
         }
@@ -543,7 +544,7 @@ nrb_status velocity_to_deformation(const nrb_geometry *g, const float *vel, bool
     }
     float *a = first, *b = first == def ? scratch : def;
     for (int k = 0; k < N; ++k) {
-        KernelTimer kt(TK_F2_COMPOSE, kComposeBytes * n, st);
+        KernelTimer kt(TK_F2_COMPOSE, kSquaringBytes * n, st);
         k_compose<<<compose_blocks(n), 256, 0, st>>>(a, a, b, f);
         NRB_LAUNCHED("k_compose");
         std::swap(a, b);
