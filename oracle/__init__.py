@@ -293,6 +293,34 @@ class Restated:
         for name in ("orc_nmi_value", "orc_be_value", "orc_max_length"):
             getattr(self.lib, name).restype = ctypes.c_double
 
+    # ---- F3D2 (reg_f3d2): velocity fields ----------------------------------------------------
+    def velocity_def_field(self, vel, gdim, gxyz, steps, update, fdim, fxyz):
+        out = np.zeros(3 * int(np.prod(fdim)), np.float32)
+        n = ctypes.c_int(0)
+        rc = self.lib.orc_velocity_def_field(_f(_f3(vel)), _i(_i3(gdim)), _f(_m(gxyz)), int(steps), int(bool(update)),
+                                             _i(_i3(fdim)), _f(_m(fxyz)), _f(out), ctypes.byref(n))
+        if rc != 0:
+            raise MemoryError("orc_velocity_def_field")
+        return out, n.value
+
+    def def_compose(self, dim, xyz, apply, update):
+        u = _f3(update).copy()
+        self.lib.orc_def_compose(_i(_i3(dim)), _f(_m(xyz)), _f(_f3(apply)), _f(u))
+        return u
+
+    def exponentiate_gradient(self, fdim, fxyz, vel, gdim, gxyz, steps, vgrad):
+        g = _f3(vgrad).copy()
+        rc = self.lib.orc_exponentiate_gradient(_i(_i3(fdim)), _f(_m(fxyz)), _f(_f3(vel)), _i(_i3(gdim)),
+                                                _f(_m(gxyz)), int(steps), _f(g))
+        if rc != 0:
+            raise MemoryError("orc_exponentiate_gradient")
+        return g
+
+    def symmetrise(self, gdim, fw_xyz, bw_xyz, fw, bw):
+        a, b = _f3(fw).copy(), _f3(bw).copy()
+        self.lib.orc_symmetrise(_i(_i3(gdim)), _f(_m(fw_xyz)), _f(_m(bw_xyz)), _f(a), _f(b))
+        return a, b
+
     def deformation_field(self, cpp, cdim, cpix, rdim, rpix, mask=None):
         out = np.zeros(3 * int(np.prod(rdim)), np.float32)
         rc = self.lib.orc_deformation_field(_f(_f3(cpp)), _i(_i3(cdim)), _f(_f3(cpix)), _i(_i3(rdim)),

@@ -741,3 +741,435 @@ void orc_cg_update(float *grad, float *g1, float *g2, size_t nvox, int first_cal
         grad[i] = -g2[i];
     }
 }
+
+/* ------------------------------------------------------------------------------------------
+ * F3D2 (reg_f3d2): velocity fields
+ * ------------------------------------------------------------------------------------------ */
+
+/* the affine inverse of nifti_mat44_inverse (reg-io/niftilib): the 3x3 block by cofactors over
+ * the determinant in double, the translation as -inverse * t, rounded to float */
+static void mat44_inverse(const float m[16], float out[16]) {
+    const double r11 = m[0], r12 = m[1], r13 = m[2], r21 = m[4], r22 = m[5], r23 = m[6];
+    const double r31 = m[8], r32 = m[9], r33 = m[10], v1 = m[3], v2 = m[7], v3 = m[11];
+    double deti = r11 * r22 * r33 - r11 * r32 * r23 - r21 * r12 * r33 + r21 * r32 * r13 + r31 * r12 * r23 -
+                  r31 * r22 * r13;
+    if (deti != 0.0) deti = 1.0 / deti;
+    out[0] = (float)(deti * (r22 * r33 - r32 * r23));
+    out[1] = (float)(deti * (-r12 * r33 + r32 * r13));
+    out[2] = (float)(deti * (r12 * r23 - r22 * r13));
+    out[3] = (float)(deti * (-r12 * r23 * v3 + r12 * v2 * r33 + r22 * r13 * v3 - r22 * v1 * r33 - r32 * r13 * v2 +
+                             r32 * v1 * r23));
+    out[4] = (float)(deti * (-r21 * r33 + r31 * r23));
+    out[5] = (float)(deti * (r11 * r33 - r31 * r13));
+    out[6] = (float)(deti * (-r11 * r23 + r21 * r13));
+    out[7] = (float)(deti * (r11 * r23 * v3 - r11 * v2 * r33 - r21 * r13 * v3 + r21 * v1 * r33 + r31 * r13 * v2 -
+                             r31 * v1 * r23));
+    out[8] = (float)(deti * (r21 * r32 - r31 * r22));
+    out[9] = (float)(deti * (-r11 * r32 + r31 * r12));
+    out[10] = (float)(deti * (r11 * r22 - r21 * r12));
+    out[11] = (float)(deti * (-r11 * r22 * v3 + r11 * r32 * v2 + r21 * r12 * v3 - r21 * r32 * v1 - r31 * r12 * v2 +
+                              r31 * r22 * v1));
+    out[12] = out[13] = out[14] = 0.f;
+    out[15] = (float)(deti != 0.0 ? 1.0 : 0.0);
+}
+
+/* m[r][0] * x + m[r][1] * y + m[r][2] * z + m[r][3] in float, left to right: the conversions of
+ * reg_getDeformationFromDisplacement_3D (reg-lib/cpu/_reg_tools.cpp:2107-2150) and of the
+ * composition paths (reg-lib/cpu/_reg_localTrans.cpp:925-940, 2380-2395) */
+static float row_f(const float *m, float x, float y, float z) {
+    float v = m[0] * x;
+    v = v + m[1] * y;
+    v = v + m[2] * z;
+    return v + m[3];
+}
+
+/* get_SlidedValues for positions (reg-lib/cpu/_reg_splineBasis.cpp:497-550) */
+static void slided3(const float *px, const float *py, const float *pz, int x, int y, int z, const int d[3],
+                    const float xyz[16], float *vx, float *vy, float *vz) {
+    const int nx = x < 0 ? 0 : (x >= d[0] ? d[0] - 1 : x);
+    const int ny = y < 0 ? 0 : (y >= d[1] ? d[1] - 1 : y);
+    const int nz = z < 0 ? 0 : (z >= d[2] ? d[2] - 1 : z);
+    const int sx = x - nx, sy = y - ny, sz = z - nz;
+    const float shx = (float)sx * xyz[0] + (float)sy * xyz[1] + (float)sz * xyz[2];
+    const float shy = (float)sx * xyz[4] + (float)sy * xyz[5] + (float)sz * xyz[6];
+    const float shz = (float)sx * xyz[8] + (float)sy * xyz[9] + (float)sz * xyz[10];
+    const size_t i = ((size_t)nz * d[1] + ny) * d[0] + nx;
+    *vx = px[i] + shx;
+    *vy = py[i] + shy;
+    *vz = pz[i] + shz;
+}
+
+/* the flow of a velocity grid at every voxel of a field, as a displacement (mm): the identity
+ * positions of reg_spline_getFlowFieldFromVelocityGrid (:3465-3491) through the composition
+ * branch of reg_cubic_spline_getDeformationField3D with the SSE build's sums (:903-1079: four
+ * x-lanes accumulated over (z, y), then added in lane order; the grid values of get_GridValues,
+ * reg-lib/cpu/_reg_splineBasis.cpp:603-663, whose rows after an outside one take the sliding
+ * path), then reg_getDisplacementFromDeformation. Also the extrema of all components. */
+static void velocity_flow(const float *vel, const int gdim[3], const float gxyz[16], const float gijk[16],
+                          const int fdim[3], const float fxyz[16], float *disp, float *lo, float *hi) {
+    const size_t n = nvox3(fdim), gn = nvox3(gdim);
+    const float *cx = vel, *cy = vel + gn, *cz = vel + 2 * gn;
+    *lo = FLT_MAX;
+    *hi = -FLT_MAX;
+    for (int z = 0; z < fdim[2]; ++z)
+        for (int y = 0; y < fdim[1]; ++y)
+            for (int x = 0; x < fdim[0]; ++x) {
+                const size_t i = ((size_t)z * fdim[1] + y) * fdim[0] + x;
+                const float rx = row_f(fxyz, (float)x, (float)y, (float)z);
+                const float ry = row_f(fxyz + 4, (float)x, (float)y, (float)z);
+                const float rz = row_f(fxyz + 8, (float)x, (float)y, (float)z);
+                const float v[3] = { row_f(gijk, rx, ry, rz), row_f(gijk + 4, rx, ry, rz), row_f(gijk + 8, rx, ry, rz) };
+                int pre[3];
+                float bas[3][4];
+                for (int k = 0; k < 3; ++k) {
+                    pre[k] = (int)floorf(v[k]);
+                    float b = v[k] - (float)pre[k];
+                    pre[k] -= 1;
+                    if (b < 0) b = 0;
+                    orc_bspline_basis(b, bas[k]);
+                }
+                float gx[64], gy[64], gz[64];
+                int coord = 0;
+                for (int Z = pre[2]; Z < pre[2] + 4; ++Z) {
+                    int out = !(Z > -1 && Z < gdim[2]);
+                    for (int Y = pre[1]; Y < pre[1] + 4; ++Y) {
+                        if (!(Y > -1 && Y < gdim[1])) out = 1;
+                        for (int X = pre[0]; X < pre[0] + 4; ++X, ++coord) {
+                            if (X > -1 && X < gdim[0] && !out) {
+                                const size_t j = ((size_t)Z * gdim[1] + Y) * gdim[0] + X;
+                                gx[coord] = cx[j];
+                                gy[coord] = cy[j];
+                                gz[coord] = cz[j];
+                            } else {
+                                slided3(cx, cy, cz, X, Y, Z, gdim, gxyz, &gx[coord], &gy[coord], &gz[coord]);
+                            }
+                        }
+                    }
+                }
+                float tx[4] = { 0, 0, 0, 0 }, ty[4] = { 0, 0, 0, 0 }, tz[4] = { 0, 0, 0, 0 };
+                for (int c = 0; c < 4; ++c)
+                    for (int b = 0; b < 4; ++b) {
+                        const float yz = bas[1][b] * bas[2][c];
+                        for (int a = 0; a < 4; ++a) {
+                            const float w = yz * bas[0][a];
+                            tx[a] = w * gx[c * 16 + b * 4 + a] + tx[a];
+                            ty[a] = w * gy[c * 16 + b * 4 + a] + ty[a];
+                            tz[a] = w * gz[c * 16 + b * 4 + a] + tz[a];
+                        }
+                    }
+                const float d[3] = { tx[0] + tx[1] + tx[2] + tx[3] - rx, ty[0] + ty[1] + ty[2] + ty[3] - ry,
+                                     tz[0] + tz[1] + tz[2] + tz[3] - rz };
+                for (int k = 0; k < 3; ++k) {
+                    disp[k * n + i] = d[k];
+                    if (d[k] < *lo) *lo = d[k];
+                    if (d[k] > *hi) *hi = d[k];
+                }
+            }
+}
+
+/* reg_defField_compose3D (reg-lib/cpu/_reg_localTrans.cpp:2334-2458): upd(x) <- app(upd(x)) */
+static void compose3(const float *app, float *upd, const int dim[3], const float xyz[16], const float ijk[16]) {
+    const size_t n = nvox3(dim);
+    const float *ax = app, *ay = app + n, *az = app + 2 * n;
+    for (size_t i = 0; i < n; ++i) {
+        const float p0 = upd[i], p1 = upd[n + i], p2 = upd[2 * n + i];
+        const float v[3] = { row_f(ijk, p0, p1, p2), row_f(ijk + 4, p0, p1, p2), row_f(ijk + 8, p0, p1, p2) };
+        int pre[3];
+        float rel[3][2];
+        for (int k = 0; k < 3; ++k) {
+            pre[k] = (int)floorf(v[k]);
+            rel[k][1] = v[k] - (float)pre[k];
+            rel[k][0] = 1.f - rel[k][1];
+        }
+        float r0 = 0, r1 = 0, r2 = 0;
+        for (int c = 0; c < 2; ++c) {
+            const int Z = pre[2] + c;
+            const int inZ = Z > -1 && Z < dim[2];
+            for (int b = 0; b < 2; ++b) {
+                const int Y = pre[1] + b;
+                const float tb = rel[1][b] * rel[2][c];
+                const int inY = Y > -1 && Y < dim[1];
+                for (int a = 0; a < 2; ++a) {
+                    const int X = pre[0] + a;
+                    float dx, dy, dz;
+                    if (X > -1 && X < dim[0] && inY && inZ) {
+                        const size_t j = ((size_t)Z * dim[1] + Y) * dim[0] + X;
+                        dx = ax[j];
+                        dy = ay[j];
+                        dz = az[j];
+                    } else {
+                        slided3(ax, ay, az, X, Y, Z, dim, xyz, &dx, &dy, &dz);
+                    }
+                    const float w = rel[0][a] * tb;
+                    r0 += dx * w;
+                    r1 += dy * w;
+                    r2 += dz * w;
+                }
+            }
+        }
+        upd[i] = r0;
+        upd[n + i] = r1;
+        upd[2 * n + i] = r2;
+    }
+}
+
+int orc_velocity_squaring_steps(float lo, float hi) {
+    float extrema = fabsf(lo) > hi ? fabsf(lo) : hi;
+    int steps = 1;
+    while (extrema / (float)pow(2, steps) >= 0.28f) ++steps;
+    return steps > 6 ? steps : 6;
+}
+
+/* the flow divided by 2^N (reg_tools_divideValueToImage: in double, rounded to float) and turned
+ * back into positions */
+static void flow_scale(float *d, const int dim[3], const float xyz[16], int steps) {
+    const size_t n = nvox3(dim);
+    const double s = (double)(float)pow(2, steps);
+    for (int z = 0; z < dim[2]; ++z)
+        for (int y = 0; y < dim[1]; ++y)
+            for (int x = 0; x < dim[0]; ++x) {
+                const size_t i = ((size_t)z * dim[1] + y) * dim[0] + x;
+                for (int k = 0; k < 3; ++k)
+                    d[k * n + i] = (float)((double)d[k * n + i] / s) + row_f(xyz + 4 * k, (float)x, (float)y, (float)z);
+            }
+}
+
+/* reg_spline_getDefFieldFromVelocityGrid (reg-lib/cpu/_reg_localTrans.cpp:3583-3613) with
+ * reg_defField_getDeformationFieldFromFlowField (:3494-3580), no affine: N = steps, recomputed
+ * from the flow's extrema when update (or steps == 0); the scaled flow squared N times. */
+int orc_velocity_def_field(const float *vel, const int gdim[3], const float gxyz[16], int steps, int update,
+                           const int fdim[3], const float fxyz[16], float *def, int *steps_out) {
+    const size_t n = nvox3(fdim);
+    float gijk[16], fijk[16], lo, hi;
+    mat44_inverse(gxyz, gijk);
+    mat44_inverse(fxyz, fijk);
+    velocity_flow(vel, gdim, gxyz, gijk, fdim, fxyz, def, &lo, &hi);
+    if (update || steps == 0) steps = orc_velocity_squaring_steps(lo, hi);
+    flow_scale(def, fdim, fxyz, steps);
+    float *tmp = (float *)malloc(3 * n * sizeof(float));
+    if (!tmp) return -1;
+    for (int k = 0; k < steps; ++k) {
+        memcpy(tmp, def, 3 * n * sizeof(float));
+        compose3(tmp, def, fdim, fxyz, fijk);
+    }
+    free(tmp);
+    *steps_out = steps;
+    return 0;
+}
+
+void orc_def_compose(const int dim[3], const float xyz[16], const float *apply, float *update) {
+    float ijk[16];
+    mat44_inverse(xyz, ijk);
+    compose3(apply, update, dim, xyz, ijk);
+}
+
+/* the orthogonal factor of a 3x3 matrix (nifti_mat33_polar's role), scaled Newton iteration in
+ * double; exactly the identity for a diagonal matrix with positive entries */
+static void polar3(const double A[3][3], double Q[3][3]) {
+    double X[3][3];
+    memcpy(X, A, sizeof(X));
+    for (int it = 0; it < 100; ++it) {
+        const double det = X[0][0] * (X[1][1] * X[2][2] - X[1][2] * X[2][1]) -
+                           X[0][1] * (X[1][0] * X[2][2] - X[1][2] * X[2][0]) +
+                           X[0][2] * (X[1][0] * X[2][1] - X[1][1] * X[2][0]);
+        if (det == 0.0) break;
+        double Y[3][3];
+        Y[0][0] = (X[1][1] * X[2][2] - X[1][2] * X[2][1]) / det;
+        Y[0][1] = (X[1][2] * X[2][0] - X[1][0] * X[2][2]) / det;
+        Y[0][2] = (X[1][0] * X[2][1] - X[1][1] * X[2][0]) / det;
+        Y[1][0] = (X[0][2] * X[2][1] - X[0][1] * X[2][2]) / det;
+        Y[1][1] = (X[0][0] * X[2][2] - X[0][2] * X[2][0]) / det;
+        Y[1][2] = (X[0][1] * X[2][0] - X[0][0] * X[2][1]) / det;
+        Y[2][0] = (X[0][1] * X[1][2] - X[0][2] * X[1][1]) / det;
+        Y[2][1] = (X[0][2] * X[1][0] - X[0][0] * X[1][2]) / det;
+        Y[2][2] = (X[0][0] * X[1][1] - X[0][1] * X[1][0]) / det;
+        double nx = 0, ny = 0, dif = 0;
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                nx += X[r][c] * X[r][c];
+                ny += Y[r][c] * Y[r][c];
+            }
+        const double g = sqrt(sqrt(ny / nx));
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                const double v = 0.5 * (g * X[r][c] + Y[r][c] / g);
+                dif += fabs(v - X[r][c]);
+                X[r][c] = v;
+            }
+        if (dif < 1e-15) break;
+    }
+    memcpy(Q, X, sizeof(X));
+}
+
+/* reg_trilinearResampleGradient (reg-lib/cpu/_reg_resampling.cpp:1537-1766) with padding 0, the
+ * gradient image and the field on one grid (dim, xyz, ijk): trilinear sample of g at def(x),
+ * times the finite-difference Jacobian of def (the reference's 8-term weight loop, backward at
+ * the last index) premultiplied by `reorient` and divided by the real spacing per column */
+static void resample_gradient(const float *g, float *out, const float *def, const int dim[3], const float ijk[16],
+                              const float R[9], const float sp[3]) {
+    const size_t n = nvox3(dim);
+    const float *gx = g, *gy = g + n, *gz = g + 2 * n;
+    const float *dx = def, *dy = def + n, *dz = def + 2 * n;
+    const float basis[2] = { 1.f, 0.f }, deriv[2] = { -1.f, 1.f };
+    for (int z = 0; z < dim[2]; ++z)
+        for (int y = 0; y < dim[1]; ++y)
+            for (int x = 0; x < dim[0]; ++x) {
+                const size_t i = ((size_t)z * dim[1] + y) * dim[0] + x;
+                const float D0 = dx[i], D1 = dy[i], D2 = dz[i];
+                const float c[3] = { row_f(ijk, D0, D1, D2), row_f(ijk + 4, D0, D1, D2), row_f(ijk + 8, D0, D1, D2) };
+                int lo[3][2];
+                float bw[3][2];
+                for (int k = 0; k < 3; ++k) {
+                    lo[k][0] = (int)floorf(c[k]);
+                    lo[k][1] = (int)ceilf(c[k]);
+                    bw[k][1] = fabsf(c[k] - (float)lo[k][0]);
+                    bw[k][0] = 1.f - bw[k][1];
+                }
+                float vx = 0, vy = 0, vz = 0;
+                for (int cc = 0; cc < 2; ++cc) {
+                    if (lo[2][cc] > -1 && lo[2][cc] < dim[2]) {
+                        for (int b = 0; b < 2; ++b) {
+                            if (lo[1][b] > -1 && lo[1][b] < dim[1]) {
+                                for (int a = 0; a < 2; ++a) {
+                                    const float w = bw[0][a] * bw[1][b] * bw[2][cc];
+                                    if (lo[0][a] > -1 && lo[0][a] < dim[0]) {
+                                        const size_t j = ((size_t)lo[2][cc] * dim[1] + lo[1][b]) * dim[0] + lo[0][a];
+                                        vx += gx[j] * w;
+                                        vy += gy[j] * w;
+                                        vz += gz[j] * w;
+                                    } else {
+                                        vx += 0.f * w;
+                                        vy += 0.f * w;
+                                        vz += 0.f * w;
+                                    }
+                                }
+                            } else {
+                                vx += 0.f * bw[1][b] * bw[2][cc];
+                                vy += 0.f * bw[1][b] * bw[2][cc];
+                                vz += 0.f * bw[1][b] * bw[2][cc];
+                            }
+                        }
+                    } else {
+                        vx += 0.f * bw[2][cc];
+                        vy += 0.f * bw[2][cc];
+                        vz += 0.f * bw[2][cc];
+                    }
+                }
+                float J[3][3] = { { 0, 0, 0 }, { 0, 0, 0 }, { 0, 0, 0 } };
+                for (int cc = 0; cc < 2; ++cc) {
+                    int Z = z + cc;
+                    float bz0 = basis[cc], bz1 = deriv[cc];
+                    if (z == dim[2] - 1) {
+                        if (cc == 1) Z -= 2;
+                        bz0 = fabsf(bz0 - 1);
+                        bz1 *= -1;
+                    }
+                    for (int b = 0; b < 2; ++b) {
+                        int Y = y + b;
+                        float by0 = basis[b], by1 = deriv[b];
+                        if (y == dim[1] - 1) {
+                            if (b == 1) Y -= 2;
+                            by0 = fabsf(by0 - 1);
+                            by1 *= -1;
+                        }
+                        for (int a = 0; a < 2; ++a) {
+                            int X = x + a;
+                            float bx0 = basis[a], bx1 = deriv[a];
+                            if (x == dim[0] - 1) {
+                                if (a == 1) X -= 2;
+                                bx0 = fabsf(bx0 - 1);
+                                bx1 *= -1;
+                            }
+                            const float w0 = bx1 * by0 * bz0, w1 = bx0 * by1 * bz0, w2 = bx0 * by0 * bz1;
+                            const size_t j = ((size_t)Z * dim[1] + Y) * dim[0] + X;
+                            const float e[3] = { dx[j], dy[j], dz[j] };
+                            for (int r = 0; r < 3; ++r) {
+                                J[r][0] += w0 * e[r];
+                                J[r][1] += w1 * e[r];
+                                J[r][2] += w2 * e[r];
+                            }
+                        }
+                    }
+                }
+                float M[3][3];
+                for (int r = 0; r < 3; ++r)
+                    for (int col = 0; col < 3; ++col)
+                        M[r][col] = R[3 * r] * J[0][col] + R[3 * r + 1] * J[1][col] + R[3 * r + 2] * J[2][col];
+                for (int r = 0; r < 3; ++r)
+                    for (int col = 0; col < 3; ++col) M[r][col] /= sp[col];
+                out[i] = M[0][0] * vx + M[0][1] * vy + M[0][2] * vz;
+                out[n + i] = M[1][0] * vx + M[1][1] * vy + M[1][2] * vz;
+                out[2 * n + i] = M[2][0] * vx + M[2][1] * vy + M[2][2] * vz;
+            }
+}
+
+/* Compute::ExponentiateGradient (reg-lib/Compute.cpp:288-330, no affine): the opposite velocity
+ * grid's intermediate fields on the gradient's grid (reg_spline_getIntermediateDefFieldFromVelGrid,
+ * reg-lib/cpu/_reg_localTrans.cpp:3616-3681), then for each of them the gradient resampled
+ * (reg_resampleGradient, linear, padding 0) and added, then the division by 2^N */
+int orc_exponentiate_gradient(const int fdim[3], const float fxyz[16], const float *vel, const int gdim[3],
+                              const float gxyz[16], int steps, float *vgrad) {
+    const size_t n = nvox3(fdim);
+    float gijk[16], fijk[16], lo, hi;
+    mat44_inverse(gxyz, gijk);
+    mat44_inverse(fxyz, fijk);
+    float *fields = (float *)malloc((size_t)steps * 3 * n * sizeof(float));
+    float *tmp = (float *)malloc(3 * n * sizeof(float));
+    if (!fields || !tmp) {
+        free(fields);
+        free(tmp);
+        return -1;
+    }
+    velocity_flow(vel, gdim, gxyz, gijk, fdim, fxyz, fields, &lo, &hi);
+    flow_scale(fields, fdim, fxyz, steps);
+    for (int k = 1; k < steps; ++k) {
+        memcpy(fields + (size_t)k * 3 * n, fields + (size_t)(k - 1) * 3 * n, 3 * n * sizeof(float));
+        compose3(fields + (size_t)(k - 1) * 3 * n, fields + (size_t)k * 3 * n, fdim, fxyz, fijk);
+    }
+    double A[3][3], Q[3][3];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) A[r][c] = fxyz[4 * r + c];
+    polar3(A, Q);
+    float R[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) R[3 * r + c] = (float)Q[c][r];
+    float sp[3];
+    {
+        const float o[3] = { 0, 0, 0 };
+        float p0[3];
+        mat44_apply(fxyz, o, p0);
+        for (int c = 0; c < 3; ++c) {
+            float e[3] = { 0, 0, 0 }, p1[3];
+            e[c] = 1;
+            mat44_apply(fxyz, e, p1);
+            const float a = p0[0] - p1[0], b = p0[1] - p1[1], d = p0[2] - p1[2];
+            sp[c] = sqrtf(a * a + b * b + d * d);
+        }
+    }
+    for (int k = 0; k < steps; ++k) {
+        resample_gradient(vgrad, tmp, fields + (size_t)k * 3 * n, fdim, fijk, R, sp);
+        for (size_t i = 0; i < 3 * n; ++i) vgrad[i] = (float)((double)tmp[i] + (double)vgrad[i]);
+    }
+    const double s = pow(2, steps);
+    for (size_t i = 0; i < 3 * n; ++i) vgrad[i] = (float)((double)vgrad[i] / s);
+    free(fields);
+    free(tmp);
+    return 0;
+}
+
+/* Compute::SymmetriseVelocityFields (reg-lib/Compute.cpp:356-392) */
+void orc_symmetrise(const int gdim[3], const float fw_xyz[16], const float bw_xyz[16], float *fw, float *bw) {
+    const size_t n = nvox3(gdim);
+    for (int z = 0; z < gdim[2]; ++z)
+        for (int y = 0; y < gdim[1]; ++y)
+            for (int x = 0; x < gdim[0]; ++x) {
+                const size_t i = ((size_t)z * gdim[1] + y) * gdim[0] + x;
+                for (int k = 0; k < 3; ++k) {
+                    const float idf = row_f(fw_xyz + 4 * k, (float)x, (float)y, (float)z);
+                    const float idb = row_f(bw_xyz + 4 * k, (float)x, (float)y, (float)z);
+                    const float df = fw[k * n + i] - idf, db = bw[k * n + i] - idb;
+                    fw[k * n + i] = (float)((double)(df - db) * 0.5) + idf;
+                    bw[k * n + i] = (float)((double)(db - df) * 0.5) + idb;
+                }
+            }
+}

@@ -44,4 +44,13 @@ void orc_update_control_points(float *cur, const float *best, const float *grad,
                                size_t nvox);
 void orc_cg_update(float *grad, float *g1, float *g2, size_t nvox, int first_call);
 
+/* F3D2 (reg_f3d2): velocity fields */
+int orc_velocity_squaring_steps(float lo, float hi);
+int orc_velocity_def_field(const float *vel, const int gdim[3], const float gxyz[16], int steps, int update,
+                           const int fdim[3], const float fxyz[16], float *def, int *steps_out);
+void orc_def_compose(const int dim[3], const float xyz[16], const float *apply, float *update);
+int orc_exponentiate_gradient(const int fdim[3], const float fxyz[16], const float *vel, const int gdim[3],
+                              const float gxyz[16], int steps, float *vgrad);
+void orc_symmetrise(const int gdim[3], const float fw_xyz[16], const float bw_xyz[16], float *fw, float *bw);
+
 #endif

@@ -179,3 +179,32 @@ def test_f3d2_refuses_rotated_images():
     with pytest.raises(nrb.NrbError):
         x = torch.zeros(3 * 8, dtype=torch.float32, device="cuda")
         nrb.def_field_compose((2, 2, 2), np.eye(4, dtype=np.float32), x, x)
+
+
+@pytest.mark.parametrize("update,amp,margin", [(True, 2.0, 1), (True, 25.0, 1), (False, 2.0, -2)])
+def test_velocity_deformation_matches_the_restatement(update, amp, margin):
+    """Against the C restatement (oracle/nrb_oracle.c): a grid that does not reach the whole
+    field (margin -2) runs the border path of the flow kernel."""
+    from tests.test_oracle_f3d2 import case
+    ensure_built()
+    O = oracle.Restated()
+    fdim, fpix, fxyz, gdim, gpix, gxyz, vel = case(61, amp=amp, margin=margin)
+    ref, rs = O.velocity_def_field(vel, gdim, gxyz, 6, update, fdim, fxyz)
+    g = nrb.make_geometry(fdim, fpix, fxyz, fdim, fpix, fxyz, gdim, gpix, gxyz)
+    d = torch.empty(3 * int(np.prod(fdim)), dtype=torch.float32, device="cuda")
+    steps = nrb.get_def_field_from_velocity_grid(g, dev(vel), 6, d, update=update)
+    assert steps == rs
+    assert np.array_equal(host(d), ref)
+
+
+def test_gradient_exponentiation_matches_the_restatement():
+    from tests.test_oracle_f3d2 import case
+    ensure_built()
+    O = oracle.Restated()
+    fdim, fpix, fxyz, gdim, gpix, gxyz, vel = case(63, amp=1.5)
+    vg = np.random.default_rng(63).normal(0, 1, 3 * int(np.prod(fdim))).astype(np.float32)
+    ref = O.exponentiate_gradient(fdim, fxyz, vel, gdim, gxyz, 7, vg)
+    g = nrb.make_geometry(fdim, fpix, fxyz, fdim, fpix, fxyz, gdim, gpix, gxyz)
+    t = dev(vg)
+    nrb.exponentiate_gradient(g, dev(vel), 7, t)
+    assert np.array_equal(host(t), ref)

@@ -1,0 +1,93 @@
+"""The F3D2 restatement (oracle/nrb_oracle.c: velocity flow and squarings, composition, gradient
+exponentiation, symmetrisation) pinned to the reference's own functions (oracle/_ref) on the
+CPU. Tolerance: none, every value must be the same float.
+
+The cases are small (a 20x18x16 field, anisotropic spacing, non-zero origin) and cover a grid
+that does not reach the whole field, so the sliding extrapolation runs for the flow too.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import ensure_built, identity_grid
+
+import niftyreg_b200 as nrb
+
+
+@pytest.fixture(scope="module")
+def both():
+    ensure_built()
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref (the reference build) is not present")
+    r = oracle.Ref()
+    r.set_threads(4)
+    return r, oracle.Restated()
+
+
+def case(seed, fdim=(20, 18, 16), fpix=(1.0, 1.1, 0.9), spacing=4.0, amp=2.0, margin=1):
+    rng = np.random.default_rng(seed)
+    origin = (-3.0, 2.0, 1.5)
+    fxyz = nrb.identity_header(fpix, origin)
+    gdim = [int(np.ceil(n * p / spacing + 3)) + margin for n, p in zip(fdim, fpix)]
+    gxyz = nrb.identity_header((spacing,) * 3, [o - spacing - 0.5 for o in origin])
+    ident = identity_grid(gdim, gxyz)
+    vel = (ident + rng.normal(0, amp, ident.size)).astype(np.float32)
+    return fdim, fpix, fxyz, gdim, (spacing,) * 3, gxyz, vel
+
+
+@pytest.mark.parametrize("update,amp,margin", [(False, 2.0, 1), (True, 2.0, 1), (True, 25.0, 1), (False, 2.0, -2)])
+def test_velocity_deformation_is_the_reference(both, update, amp, margin):
+    R, O = both
+    fdim, fpix, fxyz, gdim, gpix, gxyz, vel = case(61, amp=amp, margin=margin)
+    ref, rs = R.velocity_def_field(vel, gdim, gpix, gxyz, 6, update, fdim, fpix, fxyz)
+    out, os_ = O.velocity_def_field(vel, gdim, gxyz, 6, update, fdim, fxyz)
+    assert os_ == rs
+    assert np.array_equal(out, ref)
+
+
+def test_composition_is_the_reference(both):
+    R, O = both
+    fdim, fpix, fxyz, *_ = case(62)
+    rng = np.random.default_rng(62)
+    n = int(np.prod(fdim))
+    k, j, i = np.meshgrid(*[np.arange(v) for v in fdim[::-1]], indexing="ij")
+    vox = np.stack([i.ravel(), j.ravel(), k.ravel(), np.ones(n)])
+    ident = (fxyz.astype(np.float64) @ vox)[:3].astype(np.float32).ravel()
+    apply = (ident + rng.normal(0, 1.0, ident.size)).astype(np.float32)
+    pos = (ident + rng.uniform(-5, 5, ident.size)).astype(np.float32)
+    assert np.array_equal(O.def_compose(fdim, fxyz, apply, pos), R.def_compose(fdim, fpix, fxyz, apply, pos))
+
+
+@pytest.mark.parametrize("steps", [6, 7])
+def test_gradient_exponentiation_is_the_reference(both, steps):
+    R, O = both
+    fdim, fpix, fxyz, gdim, gpix, gxyz, vel = case(63, amp=1.5)
+    g = np.random.default_rng(63).normal(0, 1, 3 * int(np.prod(fdim))).astype(np.float32)
+    ref = R.exponentiate_gradient(fdim, fpix, fxyz, vel, gdim, gpix, gxyz, steps, g)
+    out = O.exponentiate_gradient(fdim, fxyz, vel, gdim, gxyz, steps, g)
+    assert np.array_equal(out, ref)
+
+
+def test_symmetrisation_is_the_reference(both):
+    R, O = both
+    fdim, fpix, fxyz, gdim, gpix, gxyz, vel = case(64)
+    rng = np.random.default_rng(64)
+    bxyz = gxyz.copy()
+    bxyz[:3, 3] += np.float32(0.75)
+    fw = (identity_grid(gdim, gxyz) + rng.normal(0, 2, vel.size)).astype(np.float32)
+    bw = (identity_grid(gdim, bxyz) + rng.normal(0, 2, vel.size)).astype(np.float32)
+    rf, rb = R.symmetrise(gdim, gpix, gxyz, bxyz, fw, bw)
+    of, ob = O.symmetrise(gdim, gxyz, bxyz, fw, bw)
+    assert np.array_equal(of, rf) and np.array_equal(ob, rb)
+
+
+def test_squaring_number_rule(both):
+    _, O = both
+    assert O.lib.orc_velocity_squaring_steps(ctypes_float(-1.0), ctypes_float(2.0)) == 6
+    # 0.28 * 2^7 = 35.84: an extremum of 36 mm needs 8 squarings
+    assert O.lib.orc_velocity_squaring_steps(ctypes_float(-36.0), ctypes_float(1.0)) == 8
+
+
+def ctypes_float(v):
+    import ctypes
+    return ctypes.c_float(v)
