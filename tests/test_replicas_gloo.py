@@ -35,7 +35,7 @@ def _rank(rank, world, port, out):
 
 def test_two_replicas_take_the_slowest_rank():
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.start_processes(_rank, args=(2, port, out), nprocs=2, start_method="spawn")
         res = dict(out)
