@@ -399,8 +399,8 @@ nrb_status nrb_symmetrise_velocity_fields(const nrb_geometry *g_fw, float *fw,
  * images: forward and backward velocity grids over the union of both fields of view
  * (reg_createSymmetricControlPointGrids, reg-lib/cpu/_reg_localTrans.cpp:133-357), symmetric NMI
  * (forward + backward) minus the bending energy of both grids, gradients exponentiated along the
- * opposite transformation, grids symmetrised after every update. The images must be axis-aligned
- * (diagonal voxel -> mm matrices, any origin); the velocity grids are not oriented like them.
+ * opposite transformation, grids symmetrised after every update. Images in any orientation; the
+ * velocity grids are axis-aligned in the world.
  * Results allocated by the library (free with nrb_image_free): cpp_fw_out and cpp_bw_out
  * (required) the final velocity grids, intent_p1 = 6 (SPLINE_VEL_GRID), intent_p2 the squaring
  * number; warped_fw_out / warped_bw_out (optional) the floating image on the reference grid and

@@ -289,7 +289,7 @@ def symmetrise_velocity_fields(g_fw, fw, g_bw, bw, stream=None):
 
 
 def f3d2_register_images(ref, ref_pixdim, ref_xyz, flo, flo_pixdim, flo_xyz, params, warped=True):
-    """reg_f3d2 (-vel) on two host volumes ([nz, ny, nx]) with axis-aligned voxel->mm matrices.
+    """reg_f3d2 (-vel) on two host volumes ([nz, ny, nx]) with their own voxel->mm matrices.
     Returns (fw grid [3, cz, cy, cx], bw grid, grid voxel->mm 4x4 (fw, bw), squaring number,
     warped floating on the reference grid or None, warped reference on the floating grid or None,
     result)."""

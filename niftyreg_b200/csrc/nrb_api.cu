@@ -254,6 +254,8 @@ nrb_status f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                          const float *flo, int flo_margin, const int32_t *mask, const float *cpp, float padding,
                          double sim_weight, double be_weight, nrb_objective *obj, nrb_objective *obj_host,
                          cudaStream_t st) {
+    if (ws->general)
+        return fail(NRB_ERR_UNSUPPORTED, "fused evaluation: the grid must be aligned with the reference");
     int n_be = 0;
     const bool overlap = be_weight > 0 && sim_weight > 0;
     if (be_weight > 0) {
@@ -276,6 +278,8 @@ nrb_status f3d_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
 nrb_status f3d_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g, const float *ref,
                         const float *flo, int flo_margin, const int32_t *mask, const float *cpp, float padding,
                         double sim_weight, double be_weight, float *vgrad, float *node_grad, cudaStream_t st) {
+    if (ws->general)
+        return fail(NRB_ERR_UNSUPPORTED, "fused evaluation: the grid must be aligned with the reference");
     const bool overlap = be_weight > 0 && sim_weight > 0;
     if (overlap) {
         // the bending-energy derivatives read only the grid: they run beside the voxel passes

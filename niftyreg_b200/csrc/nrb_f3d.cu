@@ -1792,21 +1792,12 @@ static void velocity_grid_image(const Header& g, int steps, float *data, nrb_ima
     out->data = data;
 }
 
-static bool axis_aligned(const nrb_image *img) {
-    const float *m = img->xyz;
-    return m[1] == 0.f && m[2] == 0.f && m[4] == 0.f && m[6] == 0.f && m[8] == 0.f && m[9] == 0.f && m[0] > 0.f &&
-           m[5] > 0.f && m[10] > 0.f;
-}
-
 extern "C" nrb_status nrb_f3d2_register_images(const nrb_image *ref, const nrb_image *flo, const nrb_f3d_params *p,
                                                nrb_image *cpp_fw_out, nrb_image *cpp_bw_out, nrb_image *warped_fw_out,
                                                nrb_image *warped_bw_out, nrb_f3d_result *result) {
     NRB_TRY(check_image(ref, "reference"));
     NRB_TRY(check_image(flo, "floating"));
     if (!p || !cpp_fw_out || !cpp_bw_out) return fail(NRB_ERR_INVALID, "nrb_f3d2_register_images: null pointer");
-    if (!axis_aligned(ref) || !axis_aligned(flo))
-        return fail(NRB_ERR_UNSUPPORTED,
-                    "nrb_f3d2_register_images: images with axis-aligned voxel -> mm matrices (positive diagonal) only");
     for (nrb_image *o : { cpp_fw_out, cpp_bw_out, warped_fw_out, warped_bw_out })
         if (o) memset(o, 0, sizeof(*o));
     ImageDesc rd, fd;

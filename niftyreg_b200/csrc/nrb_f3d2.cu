@@ -449,6 +449,55 @@ __global__ void __launch_bounds__(256) k_symmetrise(float *__restrict__ fw, floa
     }
 }
 
+// reg_voxelCentricToNodeCentric (reg-lib/cpu/_reg_localTrans.cpp:1540-1685) for a grid in any
+// orientation relative to the image: each node mapped into the image's voxels (T = image ijk x
+// grid xyz, Mat44Mul in double), the convolved voxel gradient sampled trilinearly (0 outside),
+// reoriented by the transpose of R and scaled by the weight. One thread per node.
+__global__ void k_voxel_to_node_general(const float *__restrict__ vox, int nx, int ny, int nz, Mat34 T, Mat33f R,
+                                        float weight, int cx, int cy, int cz, float *__restrict__ node) {
+    const long long nc = (long long)cx * cy * cz, nv = (long long)nx * ny * nz;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nc) return;
+    const double gx = (double)(i % cx), gy = (double)((i / cx) % cy), gz = (double)(i / ((long long)cx * cy));
+    float v[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+        v[r] = (float)((double)T.m[4 * r] * gx + (double)T.m[4 * r + 1] * gy + (double)T.m[4 * r + 2] * gz +
+                       (double)T.m[4 * r + 3]);
+    int pre[3];
+    float b[3][2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        pre[k] = floor_int(v[k]);
+        b[k][1] = v[k] - (float)pre[k];
+        b[k][0] = 1.f - b[k][1];
+    }
+    float iv0 = 0.f, iv1 = 0.f, iv2 = 0.f;
+    for (int c = 0; c < 2; ++c) {
+        const int Z = pre[2] + c;
+        if (Z <= -1 || Z >= nz) continue;
+        for (int bb = 0; bb < 2; ++bb) {
+            const int Y = pre[1] + bb;
+            if (Y <= -1 || Y >= ny) continue;
+            for (int a = 0; a < 2; ++a) {
+                const int X = pre[0] + a;
+                if (X <= -1 || X >= nx) continue;
+                const long long j = ((long long)Z * ny + Y) * nx + X;
+                float lw = b[0][a] * b[1][bb];
+                lw = lw * b[2][c];
+                iv0 = iv0 + lw * __ldg(vox + j);
+                iv1 = iv1 + lw * __ldg(vox + nv + j);
+                iv2 = iv2 + lw * __ldg(vox + 2 * nv + j);
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float ro = R.m[d] * iv0 + R.m[3 + d] * iv1 + R.m[6 + d] * iv2;
+        node[d * nc + i] = ro * weight;
+    }
+}
+
 inline unsigned blocks_for(long long n) { return (unsigned)((n + 255) / 256); }
 inline unsigned compose_blocks(long long n) { return (unsigned)((n + 256LL * kComposeVox - 1) / (256LL * kComposeVox)); }
 
@@ -644,6 +693,34 @@ nrb_status exponentiate_gradient(const nrb_geometry *g, const float *vel_other, 
         std::swap(a, b);
     }
     if (a != vgrad) NRB_CUDA(cudaMemcpyAsync(vgrad, a, 3 * n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    return NRB_OK;
+}
+
+// The voxel -> node step for a grid not aligned with the image (the F3D2 grids of rotated
+// images): `vox` holds the voxel gradient already convolved along the image axes.
+nrb_status voxel_to_node_general(const float *vox, const nrb_geometry *g, float weight, float *node,
+                                 cudaStream_t st) {
+    float T[16];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            double acc = 0;
+            for (int k = 0; k < 4; ++k) acc += (double)g->ref_ijk[4 * r + k] * (double)g->cpp_xyz[4 * k + c];
+            T[4 * r + c] = (float)acc;  // mat44 product, each entry rounded to float
+        }
+    for (int r = 0; r < 3; ++r) {
+        const float a = g->cpp_xyz[4 * r], b = g->cpp_xyz[4 * r + 1], c = g->cpp_xyz[4 * r + 2];
+        float ratio = std::sqrt(a * a + b * b + c * c);
+        ratio = ratio / g->ref_pixdim[r];
+        weight = weight * ratio;
+    }
+    Mat33f R;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) R.m[3 * r + c] = g->flo_ijk[4 * r + c];
+    const long long nc = nvox(g->cpp_dim);
+    k_voxel_to_node_general<<<blocks_for(nc), 256, 0, st>>>(vox, g->ref_dim[0], g->ref_dim[1], g->ref_dim[2],
+                                                           to_mat34(T), R, weight, g->cpp_dim[0], g->cpp_dim[1],
+                                                           g->cpp_dim[2], node);
+    NRB_LAUNCHED("k_voxel_to_node_general");
     return NRB_OK;
 }
 

@@ -673,6 +673,26 @@ static std::vector<float> cubic_kernel(float spacing_mm, float pixdim, int& radi
     return k;
 }
 
+// ref_ijk * cpp_xyz (mat44 product, entries rounded to float): the grid's node -> reference
+// voxel map; aligned when its 3x3 part is diagonal (to 1e-6 relative), as every grid built by
+// reg_createControlPointGrid / refinement is for its reference
+static void node_to_voxel(const nrb_geometry *g, double T[3][4]) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 4; ++j) {
+            double s = 0;
+            for (int k = 0; k < 4; ++k) s += (double)g->ref_ijk[4 * i + k] * (double)g->cpp_xyz[4 * k + j];
+            T[i][j] = (float)s;
+        }
+}
+static bool grid_aligned(const nrb_geometry *g) {
+    double T[3][4];
+    node_to_voxel(g, T);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            if (i != j && std::fabs(T[i][j]) > 1e-6 * std::fabs(T[i][i])) return false;
+    return true;
+}
+
 nrb_status validate_geometry(const nrb_geometry *g) {
     // voxel and node indices are 32-bit in the kernels
     if (nvox(g->ref_dim) >= (1LL << 31) / 3 || nvox(g->flo_dim) >= (1LL << 31) || nvox(g->cpp_dim) >= (1LL << 31) / 3)
@@ -686,7 +706,9 @@ nrb_status validate_geometry(const nrb_geometry *g) {
         const float gs = g->cpp_pixdim[d] / g->ref_pixdim[d];
         if (gs < 1.f) return fail(NRB_ERR_UNSUPPORTED, "geometry: control spacing below one voxel");
         const int last = (int)((float)(g->ref_dim[d] - 1) / gs);
-        if (last + 3 >= g->cpp_dim[d])
+        // the aligned passes address nodes from voxel indices; an unaligned grid is sampled
+        // through its full matrix (0 outside), so only an aligned grid must cover the reference
+        if (last + 3 >= g->cpp_dim[d] && grid_aligned(g))
             return fail(NRB_ERR_UNSUPPORTED, "geometry: control-point grid does not cover the reference");
     }
     return NRB_OK;
@@ -706,12 +728,7 @@ static int tile_span(int n, int tile, float gs) {
 // for every grid built by reg_createControlPointGrid / refinement.
 static nrb_status make_sampling(const nrb_geometry *g, AxisSampling ax[3]) {
     double T[3][4];
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 4; ++j) {
-            double s = 0;
-            for (int k = 0; k < 4; ++k) s += (double)g->ref_ijk[4 * i + k] * (double)g->cpp_xyz[4 * k + j];
-            T[i][j] = (float)s;  // mat44 operator* rounds each entry to float
-        }
+    node_to_voxel(g, T);  // mat44 operator* rounds each entry to float
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j)
             if (i != j && std::fabs(T[i][j]) > 1e-6 * std::fabs(T[i][i]))
@@ -814,8 +831,24 @@ nrb_status workspace_init(nrb_workspace *ws, const nrb_geometry *g) {
 static nrb_status workspace_alloc(nrb_workspace *ws) {
     const nrb_geometry *g = &ws->g;
     NRB_CUDA(cudaGetDevice(&ws->device));
-    NRB_TRY(make_sampling(g, ws->ax));
     size_t bytes = 0;
+    if (!grid_aligned(g)) {
+        // the whole-volume convolution and per-node sampling replace the separable passes
+        ws->general = true;
+        const size_t vb = (size_t)3 * nvox(g->ref_dim) * 4;
+        if (dev_alloc(&ws->general_vox, vb, ws->st) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(NRB_ERR_OOM, "workspace allocation failed");
+        }
+        bytes += vb;
+        for (int d = 0; d < 3; ++d) {
+            ws->ax[d] = AxisSampling{};
+            ws->ax[d].samples.assign(1, 0);
+            ws->ax[d].nsamples = 1;
+        }
+    } else {
+        NRB_TRY(make_sampling(g, ws->ax));
+    }
     for (int d = 0; d < 3; ++d) {
         NRB_TRY(upload(ws->d_samples[d], ws->ax[d].samples, bytes, ws->st));
         NRB_TRY(upload(ws->d_tap_slot[d], ws->ax[d].tap_slot, bytes, ws->st));
@@ -868,6 +901,7 @@ void workspace_free(nrb_workspace *ws) {
     }
     dev_free(ws->conv1, st);
     dev_free(ws->conv2, st);
+    dev_free(ws->general_vox, st);
     dev_free(ws->be_deriv, st);
     dev_free(ws->red, st);
     dev_free(ws->be_partials, st);
@@ -896,8 +930,23 @@ nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float
 
 int be_partial_count(const nrb_geometry *g) { return be_grid(g); }
 
+nrb_status voxel_to_node_general(const float *vox, const nrb_geometry *g, float weight, float *node,
+                                 cudaStream_t st);
+
 nrb_status launch_convolve_to_nodes(nrb_workspace *ws, const nrb_geometry *g, const float *vgrad,
                                     float weight, float *node, cudaStream_t st) {
+    if (ws->general) {
+        // Compute::ConvolveVoxelBasedMeasureGradient (reg-lib/Compute.cpp:230-281) as written:
+        // the whole gradient convolved along the image axes with the grid spacings, then every
+        // node sampled through the full node -> voxel matrix
+        KernelTimer timer(TK_CONV, 0.0, st);
+        const long long nv = nvox(g->ref_dim);
+        NRB_CUDA(cudaMemcpyAsync(ws->general_vox, vgrad, 3 * nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        for (int axis = 0; axis < 3; ++axis)
+            NRB_TRY(nrb_kernel_convolution_cubic(ws->general_vox, 3, g->ref_dim, g->ref_pixdim, g->cpp_pixdim[axis],
+                                                 axis, st));
+        return voxel_to_node_general(ws->general_vox, g, weight, node, st);
+    }
     const int nx = g->ref_dim[0], ny = g->ref_dim[1], nz = g->ref_dim[2];
     const int nsx = ws->ax[0].nsamples, nsy = ws->ax[1].nsamples, nsz = ws->ax[2].nsamples;
     // compulsory traffic of the whole voxel->node step: the voxel gradient once, the nodes once

@@ -134,6 +134,10 @@ struct nrb_workspace {
     float *d_kernel[3] = { nullptr, nullptr, nullptr };
     float *conv1 = nullptr;         // [3][nz][ny][nsx]
     float *conv2 = nullptr;         // [3][nz][nsy][nsx]
+    // a grid not aligned with the reference (F3D2 grids of rotated images): the voxel gradient is
+    // convolved whole in `general_vox` ([3][nz][ny][nx]) and sampled node by node
+    bool general = false;
+    float *general_vox = nullptr;
     size_t bytes = 0;
     cudaStream_t st = nullptr;      // owner's stream for stream-ordered allocation (or none)
     // the node-grid kernels (bending energy) run on a side stream, overlapped with the voxel
