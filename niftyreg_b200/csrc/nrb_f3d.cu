@@ -1460,7 +1460,19 @@ private:
     nrb_status GetObjectiveFunctionGradient() {
         const int64_t nr = nvox(gfw_.ref_dim), nf = nvox(gbw_.ref_dim);
         if (sim_w_ > 0) {
-            NRB_TRY(Warp(true));
+            // the fields and warped images at the best position: those of the accepted trial when
+            // it recomputed the squaring number (the same flow gives the same number, so they are
+            // what Warp(true) would compute); else computed here
+            if (best_fields_) {
+                std::swap(def_fw_.p, bdef_fw_.p);
+                std::swap(def_bw_.p, bdef_bw_.p);
+                std::swap(war_fw_.p, bwar_fw_.p);
+                std::swap(war_bw_.p, bwar_bw_.p);
+                steps_ = best_steps_;
+                best_fields_ = false;  // the best buffers now hold scratch
+            } else {
+                NRB_TRY(Warp(true));
+            }
             NRB_TRY(Similarity());  // reg_nmi::GetVoxelBasedSimilarityMeasureGradientFw recomputes both
             {
                 KernelTimer kt(TK_F2_VOXEL_GRADIENT, 0.0, st_);
@@ -1540,6 +1552,7 @@ private:
             if (value > best_obj_) {
                 UpdateBestObjFunctionValue();
                 best_obj_ = value;
+                KeepBestFields();
                 added_length += current_length;
                 current_length *= 1.1f;
                 current_length = std::min(current_length, max_length);
@@ -1552,6 +1565,16 @@ private:
         }
         start_length = added_length;
         return RestoreBestDof();
+    }
+    // the fields of an accepted trial become the best position's (pointer swaps)
+    void KeepBestFields() {
+        if (sim_w_ <= 0) return;
+        std::swap(def_fw_.p, bdef_fw_.p);
+        std::swap(def_bw_.p, bdef_bw_.p);
+        std::swap(war_fw_.p, bwar_fw_.p);
+        std::swap(war_bw_.p, bwar_bw_.p);
+        best_steps_ = steps_;
+        best_fields_ = true;
     }
     nrb_status InitLevel(int level, float& max_step);
 
@@ -1566,6 +1589,10 @@ private:
     int steps_ = 6;               // squaring number (the grids' intent_p2)
     DevBuf ref_, flo_, cur_, best_, grad_, g1_, g2_;  // dof arrays: [forward | backward]
     DevBuf def_fw_, def_bw_, war_fw_, war_bw_, wg_fw_, wg_bw_, vg_fw_, vg_bw_, scr_r_, scr_f_, fields_;
+    // the deformation fields and warped images of the best position, when best_fields_
+    DevBuf bdef_fw_, bdef_bw_, bwar_fw_, bwar_bw_;
+    bool best_fields_ = false;
+    int best_steps_ = 6;
     int64_t fields_n_ = 0;
     unsigned *mm_ = nullptr;
     nrb_objective *obj_ = nullptr;    // device: BE forward, BE backward, NMI forward, NMI backward
@@ -1621,6 +1648,11 @@ nrb_status F3d2Registration::InitLevel(int level, float& max_step) {
     NRB_TRY(g2_.alloc(6 * nc_, st_));
     NRB_TRY(def_fw_.alloc(3 * nr, st_));
     NRB_TRY(war_fw_.alloc(nr, st_));
+    NRB_TRY(bdef_fw_.alloc(3 * nr, st_));
+    NRB_TRY(bwar_fw_.alloc(nr, st_));
+    NRB_TRY(bdef_bw_.alloc(3 * nfv, st_));
+    NRB_TRY(bwar_bw_.alloc(nfv, st_));
+    best_fields_ = false;  // the level's initial objective keeps the previous squaring number
     NRB_TRY(wg_fw_.alloc(3 * nr, st_));
     NRB_TRY(vg_fw_.alloc(3 * nr, st_));
     NRB_TRY(scr_r_.alloc(3 * nr, st_));
@@ -1816,11 +1848,13 @@ extern "C" nrb_status nrb_f3d2_register_images(const nrb_image *ref, const nrb_i
     const auto t0 = std::chrono::steady_clock::now();
     cudaStream_t st = nullptr;
     NRB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    // the buffers a level frees stay in the pool for the next (the F3D footprint of the larger
-    // image, doubled for the second direction)
+    // the buffers a level or an evaluation frees stay in the pool for the next. Per voxel of
+    // the larger image at the finest level, both directions: deformation, warped, image and voxel
+    // gradients, scratch (52 B), the best position's deformation and warped image (16 B), the
+    // intermediate fields (12 B per squaring, up to 16 kept here), the pyramids, and slack.
     {
-        const int32_t *big = nflo > nref ? flo->dim : ref->dim;
-        keep_pool(2 * registration_footprint(big, ref->pixdim, p));
+        const int64_t big = std::max(nref, nflo);
+        keep_pool(big * (2 * 52 + 2 * 16 + 16 * 12 + 2 * 8 * 2) + (256LL << 20));
     }
     nrb_status s = NRB_OK;
     float *fw = nullptr, *bw = nullptr, *wf = nullptr, *wb = nullptr;
