@@ -410,6 +410,14 @@ nrb_status nrb_f3d2_register_images(const nrb_image *ref, const nrb_image *flo, 
                                     nrb_image *cpp_fw_out, nrb_image *cpp_bw_out, nrb_image *warped_fw_out,
                                     nrb_image *warped_bw_out, nrb_f3d_result *result);
 
+/* A reg_f3d -vel request on files (reg-apps/reg_f3d.cpp:647-705): both images read with
+ * nrb_image_read, nrb_f3d2_register_images, the forward velocity grid written to cpp_path and the
+ * backward one beside it with "_backward" before the extension (a.nii.gz -> a_backward.nii.gz);
+ * when res_path is not NULL the warped floating image to res_path and the warped reference to its
+ * "_backward" name. */
+nrb_status nrb_f3d2_register_files(const char *ref_path, const char *flo_path, const nrb_f3d_params *p,
+                                   const char *cpp_path, const char *res_path, nrb_f3d_result *result);
+
 /* ---- batched and served registrations (no counterpart in the reference) -------------------- */
 
 /* One registration request: host images (valid until the request completes), the reference's

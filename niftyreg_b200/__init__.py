@@ -318,6 +318,16 @@ def f3d2_register_images(ref, ref_pixdim, ref_xyz, flo, flo_pixdim, flo_xyz, par
             lib().nrb_image_free(ctypes.byref(img))
 
 
+def f3d2_register_files(ref_path, flo_path, params, cpp_path, res_path=None):
+    """A reg_f3d -vel request on NIfTI files: the backward grid (and warped reference) are written
+    beside the forward ones with "_backward" before the extension."""
+    res = F3dResult()
+    check(lib().nrb_f3d2_register_files(str(ref_path).encode(), str(flo_path).encode(), ctypes.byref(params),
+                                        str(cpp_path).encode(), str(res_path).encode() if res_path else None,
+                                        ctypes.byref(res)))
+    return res
+
+
 def _image_of(data, pixdim, xyz, sform_code=1):
     a = np.ascontiguousarray(data, np.float32)
     nz, ny, nx = a.shape

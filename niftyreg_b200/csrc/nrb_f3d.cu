@@ -1932,3 +1932,30 @@ extern "C" nrb_status nrb_f3d2_register_images(const nrb_image *ref, const nrb_i
     if (result) result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     return NRB_OK;
 }
+
+// reg-apps/reg_f3d.cpp:652-700: the backward result's name inserts "_backward" before the
+// .nii.gz / .nii extension (else appends "_backward.nii")
+static std::string backward_name(const std::string& f) {
+    for (const char *ext : { ".nii.gz", ".nii" }) {
+        const size_t at = f.find(ext);
+        if (at != std::string::npos) return f.substr(0, at) + "_backward" + ext + f.substr(at + strlen(ext));
+    }
+    return f + "_backward.nii";
+}
+
+extern "C" nrb_status nrb_f3d2_register_files(const char *ref_path, const char *flo_path, const nrb_f3d_params *p,
+                                              const char *cpp_path, const char *res_path, nrb_f3d_result *result) {
+    if (!ref_path || !flo_path || !p || !cpp_path) return fail(NRB_ERR_INVALID, "nrb_f3d2_register_files: null pointer");
+    nrb_image ref{}, flo{}, cf{}, cb{}, wf{}, wb{};
+    nrb_status s = nrb_image_read(ref_path, &ref);
+    if (s == NRB_OK) s = nrb_image_read(flo_path, &flo);
+    if (s == NRB_OK)
+        s = nrb_f3d2_register_images(&ref, &flo, p, &cf, &cb, res_path ? &wf : nullptr, res_path ? &wb : nullptr,
+                                     result);
+    if (s == NRB_OK) s = nrb_image_write(cpp_path, &cf);
+    if (s == NRB_OK) s = nrb_image_write(backward_name(cpp_path).c_str(), &cb);
+    if (s == NRB_OK && res_path) s = nrb_image_write(res_path, &wf);
+    if (s == NRB_OK && res_path) s = nrb_image_write(backward_name(res_path).c_str(), &wb);
+    for (nrb_image *img : { &ref, &flo, &cf, &cb, &wf, &wb }) nrb_image_free(img);
+    return s;
+}

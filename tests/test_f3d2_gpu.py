@@ -250,3 +250,23 @@ def test_gradient_exponentiation_matches_the_restatement():
     t = dev(vg)
     nrb.exponentiate_gradient(g, dev(vel), 7, t)
     assert np.array_equal(host(t), ref)
+
+
+def test_f3d2_file_request_writes_both_directions(tmp_path):
+    """reg_f3d -vel on files: forward and backward grids and warped images, named as the
+    reference's application names them, read back as the in-memory results."""
+    ensure_built()
+    ref, rdim, rpix, rxyz, flo, fdim, fpix, fxyz = _pair()
+    params = nrb.default_params(levels=1, max_iterations=10, bending_energy=0.005, spacing=(-5.0,))
+    nrb.write_image(tmp_path / "ref.nii.gz", ref, rpix, rxyz)
+    nrb.write_image(tmp_path / "flo.nii", flo, fpix, fxyz)
+    res = nrb.f3d2_register_files(tmp_path / "ref.nii.gz", tmp_path / "flo.nii", params, tmp_path / "cpp.nii.gz",
+                                  tmp_path / "res.nii")
+    gf, gb, (xf, xb), steps, wf, wb, r = nrb.f3d2_register_images(ref, rpix, rxyz, flo, fpix, fxyz, params)
+    assert res.final_nmi == r.final_nmi and res.objective_evaluations == r.objective_evaluations
+    c, _, cx = nrb.read_image(tmp_path / "cpp.nii.gz")
+    cb, _, _ = nrb.read_image(tmp_path / "cpp_backward.nii.gz")
+    assert np.array_equal(c, gf) and np.array_equal(cb, gb) and np.array_equal(cx, xf)
+    w, _, _ = nrb.read_image(tmp_path / "res.nii")
+    wbk, _, _ = nrb.read_image(tmp_path / "res_backward.nii")
+    assert np.array_equal(w[0], wf, equal_nan=True) and np.array_equal(wbk[0], wb, equal_nan=True)
