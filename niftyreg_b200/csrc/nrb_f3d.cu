@@ -1395,8 +1395,9 @@ void fill_geometry(nrb_geometry& g, const Header& r, const Header& f, const Head
 class F3d2Registration {
 public:
     F3d2Registration(const nrb_f3d_params& p, cudaStream_t st): p_(p), st_(st) {}
+    // fw_out / bw_out hold cap floats each (3 x the final grid's nodes)
     nrb_status Run(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd, float *fw_out,
-                   float *bw_out, float *warped_fw, float *warped_bw, nrb_f3d_result *res);
+                   float *bw_out, int64_t cap, float *warped_fw, float *warped_bw, nrb_f3d_result *res);
     const Header& grid_fw() const { return gf_; }
     const Header& grid_bw() const { return gb_; }
     int steps() const { return steps_; }
@@ -1685,7 +1686,7 @@ nrb_status F3d2Registration::InitLevel(int level, float& max_step) {
 }
 
 nrb_status F3d2Registration::Run(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd,
-                                 float *fw_out, float *bw_out, float *warped_fw, float *warped_bw,
+                                 float *fw_out, float *bw_out, int64_t cap, float *warped_fw, float *warped_bw,
                                  nrb_f3d_result *res) {
     const auto t0 = std::chrono::steady_clock::now();
     levels_ = p_.levels;
@@ -1759,6 +1760,7 @@ nrb_status F3d2Registration::Run(const float *ref, const float *flo, const Image
         max_it_ /= 2;
     }
     const int64_t n = 3 * nc_;
+    if ((fw_out || bw_out) && cap < n) return fail(NRB_ERR_INVALID, "registration: grid output capacity too small");
     if (fw_out) NRB_CUDA(cudaMemcpyAsync(fw_out, fw(cur_), n * sizeof(float), cudaMemcpyDefault, st_));
     if (bw_out) NRB_CUDA(cudaMemcpyAsync(bw_out, bw(cur_), n * sizeof(float), cudaMemcpyDefault, st_));
     if (warped_fw || warped_bw) {
@@ -1889,7 +1891,7 @@ extern "C" nrb_status nrb_f3d2_register_images(const nrb_image *ref, const nrb_i
         if (!fw || !bw || (warped_fw_out && !wf) || (warped_bw_out && !wb)) {
             s = fail(NRB_ERR_OOM, "nrb_f3d2_register_images: host allocation failed");
         } else {
-            s = reg.Run(ref->data, flo->data, rd, fd, fw, bw, wf, wb, result);
+            s = reg.Run(ref->data, flo->data, rd, fd, fw, bw, ncpp, wf, wb, result);
         }
         if (s == NRB_OK) {
             velocity_grid_image(reg.grid_fw(), reg.steps(), fw, cpp_fw_out);

@@ -560,9 +560,10 @@ nrb_status velocity_to_deformation(const nrb_geometry *g, const float *vel, bool
     }
     NRB_LAUNCHED("k_velocity_flow");
     if (update) {
-        // the extrema land in pinned host memory (a pageable copy would stage through the driver)
+        // the extrema land in pinned host memory (a pageable copy would stage through the driver):
+        // 8 bytes per host thread, portable across devices, kept for the thread's lifetime
         static thread_local unsigned *mm = nullptr;
-        if (!mm) NRB_CUDA(cudaMallocHost(&mm, 2 * sizeof(unsigned)));
+        if (!mm) NRB_CUDA(cudaHostAlloc((void **)&mm, 2 * sizeof(unsigned), cudaHostAllocPortable));
         NRB_CUDA(cudaMemcpyAsync(mm, minmax, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         NRB_CUDA(cudaStreamSynchronize(st));
         N = velocity_squaring_steps(fkey_inv(mm[0]), fkey_inv(mm[1]));
