@@ -61,6 +61,39 @@ def test_invalid_arguments_are_reported():
     assert lib.nrb_f3d_warped_image(ctypes.byref(g), fake, fake, 4, ctypes.c_float(0.0), fake, None) == 2
 
 
+def test_f3d2_refusals_before_any_device_work(tmp_path):
+    """The velocity-field entry points check their arguments before touching the device."""
+    ensure_built()
+    lib = nrb.lib()
+    fake = ctypes.c_void_p(16)  # never dereferenced: every check below comes first
+    eye = nrb.identity_header((1.0, 1.0, 1.0))
+    x16 = (ctypes.c_float * 16)(*[float(v) for v in eye.ravel()])
+    dim = (ctypes.c_int32 * 3)(4, 4, 4)
+    # composition in place over the applied field itself
+    assert lib.nrb_def_field_compose(dim, x16, x16, fake, fake, None) == 1
+    assert b"alias" in lib.nrb_last_error()
+    flat = nrb.make_geometry((8, 8, 1), (1.0, 1.0, 1.0), eye, (8, 8, 1), (1.0, 1.0, 1.0), eye, (5, 5, 4),
+                             (5.0, 5.0, 5.0), nrb.identity_header((5.0, 5.0, 5.0), (-5.0, -5.0, -5.0)))
+    # the Jacobian's finite differences need two voxels per axis
+    assert lib.nrb_exponentiate_gradient(ctypes.byref(flat), fake, 6, fake, None) == 1
+    g = nrb.make_geometry((8, 8, 8), (1.0, 1.0, 1.0), eye, (8, 8, 8), (1.0, 1.0, 1.0), eye, (5, 5, 5),
+                          (5.0, 5.0, 5.0), nrb.identity_header((5.0, 5.0, 5.0), (-5.0, -5.0, -5.0)))
+    assert lib.nrb_exponentiate_gradient(ctypes.byref(g), fake, 0, fake, None) == 1
+    steps = ctypes.c_int32(-1)
+    assert lib.nrb_get_def_field_from_velocity_grid(ctypes.byref(g), fake, 0, ctypes.byref(steps), fake, None) == 1
+    other = nrb.make_geometry((8, 8, 8), (1.0, 1.0, 1.0), eye, (8, 8, 8), (1.0, 1.0, 1.0), eye, (6, 5, 5),
+                              (5.0, 5.0, 5.0), nrb.identity_header((5.0, 5.0, 5.0), (-5.0, -5.0, -5.0)))
+    assert lib.nrb_symmetrise_velocity_fields(ctypes.byref(g), fake, ctypes.byref(other), ctypes.c_void_p(32),
+                                              None) == 1
+    assert lib.nrb_symmetrise_velocity_fields(ctypes.byref(g), fake, ctypes.byref(g), fake, None) == 1
+    # images and files: checked on the host
+    params = nrb.default_params(levels=1, max_iterations=2)
+    assert lib.nrb_f3d2_register_images(None, None, ctypes.byref(params), None, None, None, None, None) == 1
+    missing = str(tmp_path / "missing.nii").encode()
+    assert lib.nrb_f3d2_register_files(missing, missing, ctypes.byref(params), str(tmp_path / "c.nii").encode(),
+                                       None, None) != 0
+
+
 def test_footprint_is_host_only_and_monotone():
     """Admission unit of the server: computed on the host, grows with the volume, and covers at
     least the resident pyramid (2 images x 4 bytes x the finest level)."""
