@@ -91,3 +91,23 @@ def test_squaring_number_rule(both):
 def ctypes_float(v):
     import ctypes
     return ctypes.c_float(v)
+
+
+def test_restatement_matches_the_committed_reference_outputs():
+    """Against the reference's own outputs committed in tests/golden/f3d2/velocity.npz (made by
+    make_f3d2_golden.py from oracle/_ref): needs no reference build. Bitwise."""
+    import os
+    ensure_built()
+    O = oracle.Restated()
+    g = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "f3d2", "velocity.npz")))
+    fdim, fxyz, gdim, gxyz, vel = tuple(g["fdim"]), g["fxyz"], tuple(g["gdim"]), g["gxyz"], g["vel"]
+    d6, s6 = O.velocity_def_field(vel, gdim, gxyz, 6, False, fdim, fxyz)
+    assert s6 == 6 and np.array_equal(d6, g["def6"])
+    du, su = O.velocity_def_field(vel, gdim, gxyz, 6, True, fdim, fxyz)
+    assert su == int(g["steps_upd"]) and np.array_equal(du, g["def_upd"])
+    dt, _ = O.velocity_def_field(g["vel_tight"], tuple(g["gdim_tight"]), g["gxyz_tight"], 6, False, fdim, fxyz)
+    assert np.array_equal(dt, g["def_tight"])
+    assert np.array_equal(O.def_compose(fdim, fxyz, g["apply"], g["pos"]), g["composed"])
+    assert np.array_equal(O.exponentiate_gradient(fdim, fxyz, vel, gdim, gxyz, 7, g["vgrad"]), g["expgrad7"])
+    sf, sb = O.symmetrise(gdim, gxyz, g["bxyz"], g["fw"], g["bw"])
+    assert np.array_equal(sf, g["sym_fw"]) and np.array_equal(sb, g["sym_bw"])
