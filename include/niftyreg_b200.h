@@ -410,6 +410,14 @@ nrb_status nrb_f3d2_register_images(const nrb_image *ref, const nrb_image *flo, 
                                     nrb_image *cpp_fw_out, nrb_image *cpp_bw_out, nrb_image *warped_fw_out,
                                     nrb_image *warped_bw_out, nrb_f3d_result *result);
 
+/* Dims, spacing and voxel -> mm matrix of the final (finest-level) velocity grids that
+ * nrb_f3d2_register_images returns for these images and parameters, from the headers alone (host
+ * only, no device work): reg_createSymmetricControlPointGrids over the coarsest pyramid images
+ * (reg-lib/cpu/_reg_localTrans.cpp:133-357), refined once per finer level
+ * (reg_spline_refineControlPointGrid without a reference, :1809-2229). Data is not read. */
+nrb_status nrb_f3d2_grid_header(const nrb_image *ref, const nrb_image *flo, const nrb_f3d_params *p,
+                                int32_t dim_out[3], float pixdim_out[3], float xyz_out[16]);
+
 /* A reg_f3d -vel request on files (reg-apps/reg_f3d.cpp:647-705): both images read with
  * nrb_image_read, nrb_f3d2_register_images, the forward velocity grid written to cpp_path and the
  * backward one beside it with "_backward" before the extension (a.nii.gz -> a_backward.nii.gz);

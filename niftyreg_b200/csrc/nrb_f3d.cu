@@ -1808,6 +1808,60 @@ nrb_status F3d2Registration::Run(const float *ref, const float *flo, const Image
 }  // namespace
 }  // namespace nrb
 
+// The finest level's velocity grid of a registration, from the image headers alone: the
+// symmetric grid over the coarsest pyramid images (reg_f3d2::Initialise, _reg_f3d2.cpp:539-566),
+// refined once per finer level (reg_spline_refineControlPointGrid without a reference image).
+// F3d2Registration::Run builds the same sequence on the device.
+static Header final_velocity_grid(const ImageDesc& rd, const ImageDesc& fd, const nrb_f3d_params *p) {
+    const int levels = std::max(1, (int)p->levels);
+    std::vector<Header> hdr(levels), fhdr(levels);
+    hdr[levels - 1] = header_of(rd);
+    fhdr[levels - 1] = header_of(fd);
+    for (int l = levels - 2; l >= 0; --l) {
+        hdr[l] = halve(hdr[l + 1]);
+        fhdr[l] = halve(fhdr[l + 1]);
+    }
+    float spacing[3];
+    for (int i = 0; i < 3; ++i) {
+        float sp = p->spacing[i];
+        if (sp != sp) sp = p->spacing[0];
+        if (sp < 0) sp *= -(hdr[levels - 1].pixdim[i] + fhdr[levels - 1].pixdim[i]) / 2.f;
+        spacing[i] = sp * powf(2.f, (float)(levels - 1));
+    }
+    Header g = symmetric_grid_header(hdr[0], fhdr[0], spacing);
+    for (int l = 1; l < levels; ++l) g = refine_header(g);
+    return g;
+}
+
+static void image_desc(const nrb_image *img, ImageDesc& d) {
+    for (int i = 0; i < 3; ++i) {
+        d.dim[i] = img->dim[i];
+        d.pixdim[i] = img->pixdim[i];
+    }
+    d.xyz = img->xyz;
+    d.sform = img->sform_code > 0;
+}
+
+extern "C" nrb_status nrb_f3d2_grid_header(const nrb_image *ref, const nrb_image *flo, const nrb_f3d_params *p,
+                                           int32_t dim_out[3], float pixdim_out[3], float xyz_out[16]) {
+    if (!ref || !flo || !p || !dim_out || !pixdim_out || !xyz_out)
+        return fail(NRB_ERR_INVALID, "nrb_f3d2_grid_header: null pointer");
+    for (const nrb_image *img : { ref, flo })
+        for (int i = 0; i < 3; ++i)
+            if (img->dim[i] < 2 || !(img->pixdim[i] > 0))
+                return fail(NRB_ERR_INVALID, "nrb_f3d2_grid_header: 3D images with positive voxel sizes expected");
+    ImageDesc rd, fd;
+    image_desc(ref, rd);
+    image_desc(flo, fd);
+    const Header g = final_velocity_grid(rd, fd, p);
+    for (int i = 0; i < 3; ++i) {
+        dim_out[i] = g.dim[i];
+        pixdim_out[i] = g.pixdim[i];
+    }
+    g.xyz(xyz_out);
+    return NRB_OK;
+}
+
 // a velocity grid as NiftyReg tags one (reg_f3d2::Initialise, _reg_f3d2.cpp:596-599)
 static void velocity_grid_image(const Header& g, int steps, float *data, nrb_image *out) {
     for (int i = 0; i < 3; ++i) {
@@ -1864,25 +1918,7 @@ extern "C" nrb_status nrb_f3d2_register_images(const nrb_image *ref, const nrb_i
         F3d2Registration reg(*p, st);
         // the final grid's size from the headers alone (the registration builds the same), so
         // that the results go straight into host buffers
-        std::vector<Header> hdr, fhdr;
-        const int levels = std::max(1, (int)p->levels);
-        hdr.assign(levels, Header{});
-        fhdr.assign(levels, Header{});
-        hdr[levels - 1] = header_of(rd);
-        fhdr[levels - 1] = header_of(fd);
-        for (int l = levels - 2; l >= 0; --l) {
-            hdr[l] = halve(hdr[l + 1]);
-            fhdr[l] = halve(fhdr[l + 1]);
-        }
-        float spacing[3];
-        for (int i = 0; i < 3; ++i) {
-            float sp = p->spacing[i];
-            if (sp != sp) sp = p->spacing[0];
-            if (sp < 0) sp *= -(hdr[levels - 1].pixdim[i] + fhdr[levels - 1].pixdim[i]) / 2.f;
-            spacing[i] = sp * powf(2.f, (float)(levels - 1));
-        }
-        Header g = symmetric_grid_header(hdr[0], fhdr[0], spacing);
-        for (int l = 1; l < levels; ++l) g = refine_header(g);
+        const Header g = final_velocity_grid(rd, fd, p);
         const int64_t ncpp = 3 * g.n();
         fw = (float *)malloc((size_t)ncpp * sizeof(float));
         bw = (float *)malloc((size_t)ncpp * sizeof(float));
