@@ -355,6 +355,13 @@ nrb_status nrb_image_write(const char *path, const nrb_image *img);
 nrb_status nrb_f3d_register_images(const nrb_image *ref, const nrb_image *flo, const nrb_f3d_params *p,
                                    nrb_image *cpp_out, nrb_image *warped_out, nrb_f3d_result *result);
 
+/* Dims, spacing and voxel -> mm matrix of the final (finest-level) control-point grid that
+ * nrb_f3d_register_images returns for this reference and these parameters, from the header alone
+ * (host only): reg_createControlPointGrid over the coarsest reference
+ * (reg-lib/cpu/_reg_localTrans.cpp:21-128), refined onto each finer reference (:1808-2238). */
+nrb_status nrb_f3d_grid_header(const nrb_image *ref, const nrb_f3d_params *p, int32_t dim_out[3],
+                               float pixdim_out[3], float xyz_out[16]);
+
 /* A registration request on files, the way reg_f3d -ref -flo -cpp -res runs it
  * (reg-apps/reg_f3d.cpp): both images read with nrb_image_read, nrb_f3d_register_images, the grid
  * written to cpp_path and, when res_path is not NULL, the warped image to res_path (NIfTI-1,

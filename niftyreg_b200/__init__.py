@@ -318,6 +318,25 @@ def f3d2_register_images(ref, ref_pixdim, ref_xyz, flo, flo_pixdim, flo_xyz, par
             lib().nrb_image_free(ctypes.byref(img))
 
 
+def _header_image(dim, pix, xyz):
+    i = Image()
+    i.dim[:] = [int(v) for v in dim]
+    i.nvol = 1
+    i.pixdim[:] = [float(v) for v in pix]
+    i.xyz[:] = [float(v) for v in np.asarray(xyz, np.float32).ravel()]
+    i.sform_code = 1
+    return i
+
+
+def f3d_grid_header(ref_dim, ref_pixdim, ref_xyz, params):
+    """(dims, spacing, voxel->mm 4x4) of the final control-point grid of a reg_f3d registration
+    of a reference with this header (host only)."""
+    r = _header_image(ref_dim, ref_pixdim, ref_xyz)
+    d, pix, x = _I3(), (ctypes.c_float * 3)(), (ctypes.c_float * 16)()
+    check(lib().nrb_f3d_grid_header(ctypes.byref(r), ctypes.byref(params), d, pix, x))
+    return list(d), list(pix), np.array(list(x), np.float32).reshape(4, 4)
+
+
 def f3d2_grid_header(ref_dim, ref_pixdim, ref_xyz, flo_dim, flo_pixdim, flo_xyz, params):
     """(dims, spacing, voxel->mm 4x4) of the final velocity grids of a reg_f3d2 registration of
     images with these headers (host only)."""

@@ -1862,6 +1862,47 @@ extern "C" nrb_status nrb_f3d2_grid_header(const nrb_image *ref, const nrb_image
     return NRB_OK;
 }
 
+// The finest level's control-point grid of an F3D registration from the reference's header: the
+// grid of reg_createControlPointGrid over the coarsest reference (spacing x 2^(levels - 1)), then
+// reg_spline_refineControlPointGrid onto each finer reference, as F3dRegistration::CreateGrid and
+// InitLevel build it on the device.
+static Header final_control_grid(const ImageDesc& rd, const nrb_f3d_params *p) {
+    const int levels = std::max(1, (int)p->levels);
+    std::vector<Header> hdr(levels);
+    hdr[levels - 1] = header_of(rd);
+    for (int l = levels - 2; l >= 0; --l) hdr[l] = halve(hdr[l + 1]);
+    float spacing[3];
+    for (int i = 0; i < 3; ++i) {
+        float sp = p->spacing[i];
+        if (sp != sp) sp = p->spacing[0];
+        const float mm = sp < 0 ? sp * -hdr[levels - 1].pixdim[i] : sp;
+        spacing[i] = mm * powf(2.f, (float)(levels - 1));
+    }
+    Header g = grid_header(hdr[0], spacing);
+    for (int l = 1; l < levels; ++l) {
+        const float half[3] = { g.pixdim[0] / 2.0f, g.pixdim[1] / 2.0f, g.pixdim[2] / 2.0f };
+        g = grid_header(hdr[l], half);
+    }
+    return g;
+}
+
+extern "C" nrb_status nrb_f3d_grid_header(const nrb_image *ref, const nrb_f3d_params *p, int32_t dim_out[3],
+                                          float pixdim_out[3], float xyz_out[16]) {
+    if (!ref || !p || !dim_out || !pixdim_out || !xyz_out) return fail(NRB_ERR_INVALID, "nrb_f3d_grid_header: null pointer");
+    for (int i = 0; i < 3; ++i)
+        if (ref->dim[i] < 2 || !(ref->pixdim[i] > 0))
+            return fail(NRB_ERR_INVALID, "nrb_f3d_grid_header: a 3D image with positive voxel sizes expected");
+    ImageDesc rd;
+    image_desc(ref, rd);
+    const Header g = final_control_grid(rd, p);
+    for (int i = 0; i < 3; ++i) {
+        dim_out[i] = g.dim[i];
+        pixdim_out[i] = g.pixdim[i];
+    }
+    g.xyz(xyz_out);
+    return NRB_OK;
+}
+
 // a velocity grid as NiftyReg tags one (reg_f3d2::Initialise, _reg_f3d2.cpp:596-599)
 static void velocity_grid_image(const Header& g, int steps, float *data, nrb_image *out) {
     for (int i = 0; i < 3; ++i) {
