@@ -111,3 +111,25 @@ def test_restatement_matches_the_committed_reference_outputs():
     assert np.array_equal(O.exponentiate_gradient(fdim, fxyz, vel, gdim, gxyz, 7, g["vgrad"]), g["expgrad7"])
     sf, sb = O.symmetrise(gdim, gxyz, g["bxyz"], g["fw"], g["bw"])
     assert np.array_equal(sf, g["sym_fw"]) and np.array_equal(sb, g["sym_bw"])
+
+
+def test_voxel_to_node_for_an_unaligned_grid_is_the_reference(both):
+    """Compute::ConvolveVoxelBasedMeasureGradient with a rotated reference under an axis-aligned
+    grid (the F3D2 situation): the restatement convolves the whole gradient along the image axes
+    and samples every node through the full node -> voxel matrix. Within 1e-6 of the largest
+    node value: the convolution sums run in another order than the reference's (as for an
+    aligned grid, tests/test_oracle_golden.py); the measured gap is 1.6e-7 relative."""
+    from tests.test_register_images_gpu import affine, rotation
+    R, O = both
+    rdim, rpix = (26, 22, 18), (1.0, 1.1, 0.9)
+    rxyz = affine(rotation(0.09, -0.05, 0.21), rpix, (-14.0, -12.5, -9.0))
+    fdim, fpix = (24, 20, 20), (1.1, 1.0, 1.0)
+    fxyz = affine(rotation(0.0, 0.1, -0.07), fpix, (-12.0, -11.0, -10.0))
+    cdim, cpix = (10, 9, 8), (5.0, 5.0, 5.0)
+    cxyz = nrb.identity_header(cpix, (-20.0, -18.0, -16.0))
+    vg = np.random.default_rng(3).normal(size=3 * int(np.prod(rdim))).astype(np.float32)
+    _, ref = R.convolve_to_nodes(vg, rdim, rpix, rxyz, fdim, fpix, fxyz, cdim, cpix, cxyz, 0.7)
+    ijk = np.linalg.inv(rxyz.astype(np.float64)).astype(np.float32)
+    fijk = np.linalg.inv(fxyz.astype(np.float64)).astype(np.float32)
+    _, out = O.convolve_to_nodes(vg, rdim, rpix, ijk, cdim, cpix, cxyz, fijk, 0.7)
+    assert float(np.abs(out - ref).max()) <= 1e-6 * float(np.abs(ref).max())
