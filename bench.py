@@ -38,7 +38,6 @@ WORKLOAD = ("plain single-pair F3D, 182x218x182 float32 1 mm brain-MR-like 3-cla
             "3 levels, 300 counted iterations at the finest level (600/1200 coarser), NMI 64 bins, "
             "BE 0.005, 5 mm control spacing")
 L2_FLUSH_BYTES = 256 << 20
-REF_SAMPLE_MAXIT = 30          # reference arm: 1/10 of every level's iteration budget
 
 
 def parse():
@@ -231,35 +230,49 @@ def traffic_per_launch(kernel):
     return None
 
 
-def reference_sample(pair, threads):
-    """The reference NiftyReg CPU registration (oracle/_ref, all host threads) on a bounded sample
-    of the workload: every level runs 1/10 of its counted-iteration budget; the registration time
-    is extrapolated per level by time per counted iteration x that level's full budget."""
+def reference_registration(pair, threads):
+    """One full-budget registration of the workload by the reference NiftyReg CPU library
+    (reg_f3d<float>::Run from oracle/_ref, -O3 -msse3 OpenMP, all host threads given), timed with
+    the host clock around Run (in-memory images, no file I/O, as reg-apps/reg_benchmark.cpp
+    times it). Returns None when the library is not built."""
     import oracle
     if not oracle.ref_available():
         return None
     R = oracle.Ref()
     cores = R.set_threads(threads)
     eye = np.eye(4, dtype=np.float32)
-    t0 = time.perf_counter()
     _, _, st = R.f3d_register(pair.reference.ravel(), pair.floating.ravel(), pair.dim, pair.pixdim, eye, LEVELS,
-                              REF_SAMPLE_MAXIT, BE, 0.0, BINS, SPACING)
-    wall = time.perf_counter() - t0
-    est = 0.0
-    for level in range(LEVELS):
-        n_obj, n_grad, sec = st[5 + 3 * level: 8 + 3 * level]
-        counted = n_obj - 1 + n_grad  # the initial objective of a level is not counted
-        budget = MAXIT * 2 ** (LEVELS - 1 - level)
-        est += sec / max(counted, 1) * budget
-    return {"value": 1.0 / est, "unit": "registrations/s", "cores": int(cores), "kind": "reference",
-            "sample": (f"reference reg_f3d<float> (oracle/_ref, -O3 -msse3 OpenMP) on the same pair with "
-                       f"{REF_SAMPLE_MAXIT}/{2 * REF_SAMPLE_MAXIT}/{4 * REF_SAMPLE_MAXIT} counted iterations "
-                       f"(1/10 budget, {wall:.1f} s); time per counted iteration per level x full budget "
-                       f"{MAXIT}/{2 * MAXIT}/{4 * MAXIT} = {est:.1f} s per registration"),
-            "sample_seconds": wall, "estimated_seconds_per_registration": est}
+                              MAXIT, BE, 0.0, BINS, SPACING)
+    sec = float(st[4])
+    n_obj, n_grad = int(st[2]), int(st[3])
+    return {"seconds": sec, "cores": int(cores), "final_nmi": float(st[0]), "objective_evaluations": n_obj,
+            "gradient_evaluations": n_grad, "evaluations_per_s": (n_obj + n_grad) / sec,
+            "per_level_seconds": [float(st[7 + 3 * l]) for l in range(LEVELS)]}
+
+
+def reference_baseline(pair, threads):
+    """cpu_baseline of the b200 line: one full-budget reference registration (the bounded sample
+    is one registration of the workload)."""
+    r = reference_registration(pair, threads)
+    if r is None:
+        return None
+    return {"value": 1.0 / r["seconds"], "unit": "registrations/s", "cores": r["cores"], "kind": "reference",
+            "sample": (f"one full-budget reference reg_f3d<float> registration (oracle/_ref, -O3 -msse3 OpenMP, "
+                       f"{r['cores']} threads) of the same pair: {r['seconds']:.1f} s, "
+                       f"{r['objective_evaluations']} objective + {r['gradient_evaluations']} gradient "
+                       f"evaluations, final NMI {r['final_nmi']:.7f}"),
+            "final_nmi": r["final_nmi"], "objective_evaluations": r["objective_evaluations"],
+            "gradient_evaluations": r["gradient_evaluations"], "evaluations_per_s": r["evaluations_per_s"]}
+
+
+REF_ARM_BUDGET_S = 150.0       # reference arm: registrations are timed while they fit in this
 
 
 def run_reference(args):
+    """The reference arm: whole reference registrations of the workload on the host cores, each
+    one timed (a step = one full-budget registration). At least one registration runs whatever
+    --steps is; further ones run while --steps and REF_ARM_BUDGET_S allow, and the line states
+    how many were timed. No warm-up is needed on the CPU (--warmup is recorded, not run)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
@@ -271,21 +284,34 @@ def run_reference(args):
                           "reference sources: make -C oracle ref)"}))
         return 0
     threads = os.cpu_count() or 1
-    vals = []
-    last = None
-    for i in range(args.warmup + args.steps):
-        s = reference_sample(pair, threads)
-        if i >= args.warmup:
-            vals.append(s["estimated_seconds_per_registration"])
-        last = s
-    sec = float(np.mean(vals))
+    runs = []
+    t_start = time.perf_counter()
+    while True:
+        runs.append(reference_registration(pair, threads))
+        elapsed = time.perf_counter() - t_start
+        mean = elapsed / len(runs)
+        if len(runs) >= max(1, args.steps) or elapsed + mean > REF_ARM_BUDGET_S:
+            break
+    sec = float(np.mean([r["seconds"] for r in runs]))
     v = 1.0 / sec
+    last = runs[-1]
+    evals = float(np.mean([r["evaluations_per_s"] for r in runs]))
+    sample = (f"{len(runs)} full-budget reference reg_f3d<float> registrations (oracle/_ref, -O3 -msse3 OpenMP, "
+              f"{last['cores']} threads), each timed around Run: mean {sec:.1f} s; last: "
+              f"{last['objective_evaluations']} objective + {last['gradient_evaluations']} gradient evaluations, "
+              f"final NMI {last['final_nmi']:.7f}")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "registrations/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "steps": len(runs), "requested_steps": args.steps, "warmup": 0, "requested_warmup": args.warmup,
+            "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "parallelism": "replicas", "host_threads": threads},
+            "evaluations_per_s": evals,
+            "registration": {"final_nmi": last["final_nmi"], "objective_evaluations": last["objective_evaluations"],
+                             "gradient_evaluations": last["gradient_evaluations"],
+                             "per_level_seconds": last["per_level_seconds"],
+                             "step_s": [round(r["seconds"], 3) for r in runs]},
             "cpu_baseline": {"value": v, "unit": "registrations/s", "cores": last["cores"], "kind": "reference",
-                             "sample": last["sample"]},
+                             "sample": sample},
             "e2e": {"value": v, "unit": "registrations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -424,15 +450,20 @@ def run_b200(args):
         "e2e": {"value": e2e_value, "unit": "registrations/s", "h2d_bytes_per_step": 2 * 4 * nx * ny * nz,
                 "d2h_bytes_per_step": 4 * ncpp},
         "gpu_launches": int(launches),
+        "evaluations_per_s": sum(r.objective_evaluations + r.gradient_evaluations for r in results)
+                             / (sum(step_ms) / 1e3),
         "clocks": clocks,
         "registration": {"final_nmi": results[-1].final_nmi, "objective_evaluations": results[-1].objective_evaluations,
                          "gradient_evaluations": results[-1].gradient_evaluations,
                          "step_ms": [round(s, 3) for s in step_ms]},
     }
     if world == 1 and not args.no_cpu_baseline:
-        cb = reference_sample(pair, os.cpu_count() or 1)
+        cb = reference_baseline(pair, os.cpu_count() or 1)
         if cb is not None:
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            line["reference_registration"] = {k: cb[k] for k in ("final_nmi", "objective_evaluations",
+                                                                 "gradient_evaluations", "evaluations_per_s")}
+            line["abs_dnmi_vs_reference"] = abs(results[-1].final_nmi - cb["final_nmi"])
     print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
@@ -666,6 +697,7 @@ def run_warp(args):
             "clocks": clocks}
     if not args.no_cpu_baseline:
         import oracle
+        REF_SAMPLE_MAXIT = 30  # F3D2 reference: 1/10 of the finest level's budget, extrapolated
         if oracle.ref_available():
             R = oracle.Ref()
             cores = R.set_threads(os.cpu_count() or 1)
@@ -779,6 +811,7 @@ def run_f3d2(args):
             "clocks": clocks}
     if not args.no_cpu_baseline:
         import oracle
+        REF_SAMPLE_MAXIT = 30  # F3D2 reference: 1/10 of the finest level's budget, extrapolated
         if oracle.ref_available():
             R = oracle.Ref()
             cores = R.set_threads(os.cpu_count() or 1)

@@ -355,6 +355,24 @@ nrb_status nrb_image_write(const char *path, const nrb_image *img);
 nrb_status nrb_f3d_register_images(const nrb_image *ref, const nrb_image *flo, const nrb_f3d_params *p,
                                    nrb_image *cpp_out, nrb_image *warped_out, nrb_f3d_result *result);
 
+/* The image pyramid of reg_createImagePyramid<float> (reg-lib/cpu/_reg_tools.cpp:1705-1733) for a
+ * device image with dims, spacings and voxel -> mm matrix xyz (NULL: identity orientation at
+ * origin 0): level levels-1 is the input, each coarser level is Gaussian-smoothed (sigma 0.7355
+ * voxel) and nearest-neighbour downsampled from the next finer one along every axis whose size / 2
+ * is at least 32 (reg_downsampleImage, _reg_tools.cpp:1343-1500). out receives the levels end to
+ * end, coarsest first; dims_out (3 per level), xyz_out (16 per level) and total_out (floats of
+ * out) may be NULL; with out == NULL only the headers and the total are computed (host only). */
+nrb_status nrb_image_pyramid(const float *img, const int32_t dim[3], const float pixdim[3],
+                             const float xyz[16], int levels, float *out, int64_t capacity,
+                             int32_t *dims_out, float *xyz_out, int64_t *total_out, void *stream);
+
+/* The node values of reg_spline_refineControlPointGrid3D (reg-lib/cpu/_reg_localTrans.cpp:
+ * 1809-2119): a grid of old_dim nodes (three planes) refined onto new_dim nodes at half the
+ * spacing, as the registration does between pyramid levels. new_dim comes from the finer
+ * reference (nrb_f3d_grid_header) and lies in [1, 2 * old_dim]; out must not alias old. */
+nrb_status nrb_refine_control_point_grid(const float *old, const int32_t old_dim[3], float *out,
+                                         const int32_t new_dim[3], void *stream);
+
 /* Dims, spacing and voxel -> mm matrix of the final (finest-level) control-point grid that
  * nrb_f3d_register_images returns for this reference and these parameters, from the header alone
  * (host only): reg_createControlPointGrid over the coarsest reference
@@ -456,13 +474,16 @@ nrb_status nrb_f3d_footprint(const int32_t dim[3], const float pixdim[3], const 
  * do not already keep the device busy (a registration counts as min(1, voxels / 2^21) of the
  * device; at most 2 devices' worth run at once). Admitted requests run concurrently and their
  * kernels overlap; each result is the one nrb_f3d_register_host gives for the same request
- * alone. */
+ * alone. While servers exist on a device, its default memory pool keeps freed memory up to the
+ * budget (release threshold) and does not reuse memory across streams through inserted
+ * dependencies; the pool's previous settings come back when the last server is destroyed. */
 typedef struct nrb_server nrb_server;
 nrb_status nrb_server_create(int slots, int64_t hbm_budget_bytes, nrb_server **out);
 nrb_status nrb_server_submit(nrb_server *s, const nrb_pair *req, const nrb_f3d_params *p,
                              int64_t *ticket);
 /* Blocks until the request ends; queue_seconds = submit -> admission, latency_seconds =
- * submit -> result. */
+ * submit -> result. A ticket is waited on once: a second wait on it (another thread, or after
+ * the first returned) returns NRB_ERR_INVALID. */
 nrb_status nrb_server_wait(nrb_server *s, int64_t ticket, nrb_f3d_result *result,
                            double *queue_seconds, double *latency_seconds);
 /* Peak admitted footprint and peak number of concurrent registrations so far. */

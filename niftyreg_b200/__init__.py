@@ -425,6 +425,36 @@ def f3d_warped_image(g, flo, cpp, warped, order=3, padding=math.nan, stream=None
                                      _p(warped), _s(stream)))
 
 
+def image_pyramid_headers(dim, pixdim, xyz, levels):
+    """(dims [levels x 3], xyz [levels x 4 x 4], total floats) of reg_createImagePyramid for an
+    image of these dims, spacings and voxel -> mm matrix (host only), coarsest level first."""
+    dims = np.zeros(3 * levels, np.int32)
+    mats = np.zeros(16 * levels, np.float32)
+    total = ctypes.c_int64()
+    x16 = (ctypes.c_float * 16)(*[float(v) for v in np.asarray(xyz, np.float32).ravel()]) if xyz is not None else None
+    check(lib().nrb_image_pyramid(None, _I3(*[int(v) for v in dim]), _F3(*[float(v) for v in pixdim]), x16,
+                                  int(levels), None, ctypes.c_int64(0), dims.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                  mats.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(total), None))
+    return dims.reshape(levels, 3), mats.reshape(levels, 4, 4), total.value
+
+
+def image_pyramid(img, dim, pixdim, xyz, levels, out, stream=None):
+    """reg_createImagePyramid<float> on the device: `out` (device, >= total floats) receives the
+    levels end to end, coarsest first. Returns the headers as image_pyramid_headers does."""
+    dims, mats, total = image_pyramid_headers(dim, pixdim, xyz, levels)
+    x16 = (ctypes.c_float * 16)(*[float(v) for v in np.asarray(xyz, np.float32).ravel()]) if xyz is not None else None
+    check(lib().nrb_image_pyramid(_p(img), _I3(*[int(v) for v in dim]), _F3(*[float(v) for v in pixdim]), x16,
+                                  int(levels), _p(out), ctypes.c_int64(total), None, None, None, _s(stream)))
+    return dims, mats, total
+
+
+def refine_control_point_grid(old, old_dim, out, new_dim, stream=None):
+    """reg_spline_refineControlPointGrid3D's node values: `old` (old_dim nodes, three planes)
+    refined onto new_dim nodes at half the spacing, into `out` (device)."""
+    check(lib().nrb_refine_control_point_grid(_p(old), _I3(*[int(v) for v in old_dim]), _p(out),
+                                              _I3(*[int(v) for v in new_dim]), _s(stream)))
+
+
 def get_image_gradient(g, flo, deformation, grad, padding=math.nan, mask=None, stream=None):
     check(lib().nrb_get_image_gradient(ctypes.byref(g), _p(flo), _p(deformation), _p(mask), ctypes.c_float(padding),
                                        _p(grad), _s(stream)))

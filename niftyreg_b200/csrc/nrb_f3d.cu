@@ -1903,6 +1903,64 @@ extern "C" nrb_status nrb_f3d_grid_header(const nrb_image *ref, const nrb_f3d_pa
     return NRB_OK;
 }
 
+// reg_createImagePyramid<float> (reg-lib/cpu/_reg_tools.cpp:1705-1733) of one device image: the
+// headers on the host (halve), every coarser level smoothed and downsampled on the device from
+// the next finer one, the levels laid end to end in `out`, coarsest first.
+extern "C" nrb_status nrb_image_pyramid(const float *img, const int32_t dim[3], const float pixdim[3],
+                                        const float xyz[16], int levels, float *out, int64_t capacity,
+                                        int32_t *dims_out, float *xyz_out, int64_t *total_out, void *stream) {
+    if (!dim || !pixdim || levels < 1 || levels > 16)
+        return fail(NRB_ERR_INVALID, "nrb_image_pyramid: dims, spacings and 1..16 levels expected");
+    for (int i = 0; i < 3; ++i)
+        if (dim[i] < 1 || !(pixdim[i] > 0) || !std::isfinite(pixdim[i]))
+            return fail(NRB_ERR_INVALID, "nrb_image_pyramid: positive dims and voxel sizes expected");
+    ImageDesc d;
+    for (int i = 0; i < 3; ++i) {
+        d.dim[i] = dim[i];
+        d.pixdim[i] = pixdim[i];
+    }
+    d.xyz = xyz;
+    d.sform = xyz != nullptr;
+    std::vector<Header> h(levels);
+    h[levels - 1] = header_of(d);
+    for (int l = levels - 2; l >= 0; --l) h[l] = halve(h[l + 1]);
+    std::vector<int64_t> off(levels + 1, 0);
+    for (int l = 0; l < levels; ++l) {
+        off[l + 1] = off[l] + h[l].n();
+        if (dims_out) memcpy(dims_out + 3 * l, h[l].dim, 3 * sizeof(int32_t));
+        if (xyz_out) h[l].xyz(xyz_out + 16 * l);
+    }
+    if (total_out) *total_out = off[levels];
+    if (!out) return NRB_OK;  // headers only
+    if (!img) return fail(NRB_ERR_INVALID, "nrb_image_pyramid: null image");
+    if (capacity < off[levels]) return fail(NRB_ERR_INVALID, "nrb_image_pyramid: output capacity below the total");
+    cudaStream_t st = as_stream(stream);
+    NRB_CUDA(cudaMemcpyAsync(out + off[levels - 1], img, h[levels - 1].n() * sizeof(float), cudaMemcpyDeviceToDevice,
+                             st));
+    if (levels == 1) return NRB_OK;
+    DevBuf tmp;
+    NRB_TRY(tmp.alloc(4 * h[levels - 1].n(), st));
+    for (int l = levels - 2; l >= 0; --l) {
+        float nxyz[16], oijk[16];
+        h[l].xyz(nxyz);
+        h[l + 1].ijk(oijk);
+        NRB_TRY(smooth_and_downsample(out + off[l + 1], h[l + 1].dim, out + off[l], h[l].dim, nxyz, oijk, tmp.p, st));
+    }
+    return NRB_OK;  // tmp is freed in stream order
+}
+
+// reg_spline_refineControlPointGrid3D's node values (reg-lib/cpu/_reg_localTrans.cpp:1930-2119):
+// the grid of old_dim nodes refined onto new_dim nodes at half the spacing, three planes each
+extern "C" nrb_status nrb_refine_control_point_grid(const float *old, const int32_t old_dim[3], float *out,
+                                                    const int32_t new_dim[3], void *stream) {
+    if (!old || !old_dim || !out || !new_dim) return fail(NRB_ERR_INVALID, "nrb_refine_control_point_grid: null pointer");
+    for (int i = 0; i < 3; ++i)
+        if (old_dim[i] < 1 || new_dim[i] < 1 || new_dim[i] > 2 * old_dim[i])
+            return fail(NRB_ERR_INVALID, "nrb_refine_control_point_grid: new dims must be in [1, 2 * old dims]");
+    if (old == out) return fail(NRB_ERR_INVALID, "nrb_refine_control_point_grid: the output aliases the input");
+    return grid_refine(old_dim, old, new_dim, out, as_stream(stream));
+}
+
 // a velocity grid as NiftyReg tags one (reg_f3d2::Initialise, _reg_f3d2.cpp:596-599)
 static void velocity_grid_image(const Header& g, int steps, float *data, nrb_image *out) {
     for (int i = 0; i < 3; ++i) {

@@ -209,10 +209,16 @@ extern "C" nrb_status nrb_image_read(const char *path, nrb_image *out) {
     if (units == 1)
         for (int d = 1; d <= 3; ++d) pix[d] *= 1000.f;
 
-    const size_t nvox3 = (size_t)dim[1] * dim[2] * dim[3];
-    size_t nvol = 1;
-    for (int i = 4; i < 8; ++i) nvol *= (size_t)dim[i];
-    const size_t n = nvox3 * nvol;
+    // element counts: each dim is at most 32767, so the products are checked for overflow before
+    // any size is derived from them, and bounded by the file's length below
+    size_t nvox3 = 1, nvol = 1;
+    bool overflow = false;
+    for (int i = 1; i <= 3; ++i) overflow |= __builtin_mul_overflow(nvox3, (size_t)dim[i], &nvox3);
+    for (int i = 4; i < 8; ++i) overflow |= __builtin_mul_overflow(nvol, (size_t)dim[i], &nvol);
+    size_t n = 0;
+    overflow |= __builtin_mul_overflow(nvox3, nvol, &n);
+    if (overflow) return fail(NRB_ERR_INVALID, "nrb_image_read: voxel count overflows");
+    if (nvol > (size_t)INT32_MAX) return fail(NRB_ERR_INVALID, "nrb_image_read: more than 2^31 - 1 volumes");
     int bytes = 0;
     switch (datatype) {
     case 2: case 256: bytes = 1; break;     // uint8, int8
@@ -223,8 +229,12 @@ extern "C" nrb_status nrb_image_read(const char *path, nrb_image *out) {
         return fail(NRB_ERR_UNSUPPORTED, "nrb_image_read: datatype " + std::to_string(datatype) +
                                               " (complex, RGB or unknown) is not read");
     }
+    if (!std::isfinite(vox_offset) || vox_offset >= (float)file.size())
+        return fail(NRB_ERR_INVALID, "nrb_image_read: vox_offset is not finite or lies past the end of the file");
     const size_t start = vox_offset > 0 ? (size_t)vox_offset : 352;
-    if (file.size() < start + n * bytes) return fail(NRB_ERR_INVALID, "nrb_image_read: data shorter than the header says");
+    // n <= (file length - start) / bytes bounds n * bytes and n * sizeof(float) far below 2^64
+    if (start > file.size() || n > (file.size() - start) / (size_t)bytes)
+        return fail(NRB_ERR_INVALID, "nrb_image_read: data shorter than the header says");
     float *data = (float *)malloc(std::max<size_t>(n, 1) * sizeof(float));
     if (!data) return fail(NRB_ERR_OOM, "nrb_image_read: host allocation failed");
     const unsigned char *src = file.data() + start;

@@ -657,19 +657,39 @@ static int grid_for(long long n, int threads, int max_blocks_per_sm = 16) {
     return (int)std::max<long long>(1, std::min<long long>(want, (long long)max_blocks_per_sm * sm_count()));
 }
 
-// cubic B-spline convolution kernel of reg_tools_kernelConvolution (_reg_tools.cpp:877-904)
-static std::vector<float> cubic_kernel(float spacing_mm, float pixdim, int& radius) {
-    const double temp = spacing_mm > 0 ? (double)(spacing_mm / pixdim) : std::fabs((double)spacing_mm);
+// Kernel width of reg_tools_kernelConvolution (_reg_tools.cpp:882-884): the spacing in mm over
+// the voxel size, or |spacing| voxels when the spacing is negative; radius = int(2 * width).
+// Refuses spacings and voxel sizes for which that is undefined (NaN, infinite, a voxel size that
+// is not > 0 with a spacing in mm) and radii above 2^20 voxels.
+static nrb_status cubic_extent(const char *who, float spacing_mm, float pixdim, double& temp, int& radius) {
+    if (!std::isfinite(spacing_mm) || (spacing_mm > 0 && !(std::isfinite(pixdim) && pixdim > 0.f)))
+        return fail(NRB_ERR_INVALID, std::string(who) + ": the spacing must be finite and, when given in mm, the "
+                                                        "voxel size finite and > 0");
+    temp = spacing_mm > 0 ? (double)(spacing_mm / pixdim) : std::fabs((double)spacing_mm);
+    if (!(temp * 2.0 < (double)(1 << 20)))
+        return fail(NRB_ERR_UNSUPPORTED, std::string(who) + ": kernel radius above 2^20 voxels");
     radius = (int)(temp * 2.0f);
-    std::vector<float> k(2 * radius + 1);
+    return NRB_OK;
+}
+
+// the 2 * radius + 1 cubic B-spline taps of reg_tools_kernelConvolution (_reg_tools.cpp:893-904)
+static void cubic_taps(double temp, int radius, float *out) {
     for (int i = -radius; i <= radius; ++i) {
         const double rel = std::fabs(i / temp);
         float v;
         if (rel < 1.0) v = (float)(2.0 / 3.0 - rel * rel + 0.5 * rel * rel * rel);
         else if (rel < 2.0) v = (float)(-(rel - 2.0) * (rel - 2.0) * (rel - 2.0) / 6.0);
         else v = 0.f;
-        k[i + radius] = v;
+        out[i + radius] = v;
     }
+}
+
+// cubic B-spline convolution kernel of a geometry the workspace has already validated
+static std::vector<float> cubic_kernel(float spacing_mm, float pixdim, int& radius) {
+    const double temp = spacing_mm > 0 ? (double)(spacing_mm / pixdim) : std::fabs((double)spacing_mm);
+    radius = (int)(temp * 2.0f);
+    std::vector<float> k(2 * radius + 1);
+    cubic_taps(temp, radius, k.data());
     return k;
 }
 
@@ -1038,9 +1058,12 @@ extern "C" nrb_status nrb_kernel_convolution_cubic(float *img, int nvol, const i
     if (!img || !dim || !pixdim || nvol <= 0 || axis < 0 || axis > 2)
         return fail(NRB_ERR_INVALID, "nrb_kernel_convolution_cubic: bad argument");
     cudaStream_t st = as_stream(stream);
+    double temp = 0;
     int radius = 0;
-    const std::vector<float> k = cubic_kernel(spacing_mm, pixdim[axis], radius);
+    NRB_TRY(cubic_extent("nrb_kernel_convolution_cubic", spacing_mm, pixdim[axis], temp, radius));
     if (radius <= 0 || dim[axis] <= 1) return NRB_OK;  // the reference leaves the image as is
+    std::vector<float> k(2 * radius + 1);
+    cubic_taps(temp, radius, k.data());
     const long long nv = (long long)dim[0] * dim[1] * dim[2];
     float *dk = nullptr, *tv = nullptr, *td = nullptr;
     NRB_CUDA(cudaMallocAsync(&dk, k.size() * 4, st));
@@ -1093,23 +1116,6 @@ __global__ void k_static_taps(const __grid_constant__ StaticTaps t, int n, float
     for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = t.k[i];
 }
 
-// cubic B-spline taps with the values and radius rule of cubic_kernel(), into a fixed array;
-// returns the radius, or -1 when 2 * radius + 1 taps do not fit in `cap`
-int cubic_taps_fixed(float spacing_mm, float pixdim, float *out, int cap) {
-    const double temp = spacing_mm > 0 ? (double)(spacing_mm / pixdim) : std::fabs((double)spacing_mm);
-    const int radius = (int)(temp * 2.0f);
-    if (2 * radius + 1 > cap) return -1;
-    for (int i = -radius; i <= radius; ++i) {
-        const double rel = std::fabs(i / temp);
-        float v;
-        if (rel < 1.0) v = (float)(2.0 / 3.0 - rel * rel + 0.5 * rel * rel * rel);
-        else if (rel < 2.0) v = (float)(-(rel - 2.0) * (rel - 2.0) * (rel - 2.0) / 6.0);
-        else v = 0.f;
-        out[i + radius] = v;
-    }
-    return radius;
-}
-
 // Address of this device's scratch. cudaGetSymbolAddress runs once per device, with that device
 // current (the caller's current device); later calls read the cached pointer.
 constexpr int kMaxDevices = 64;
@@ -1141,12 +1147,16 @@ extern "C" nrb_status nrb_kernel_convolution_cubic_static(float *img, int nvol, 
     if (nv > NRB_STATIC_CONV_MAX_VOXELS)
         return fail(NRB_ERR_UNSUPPORTED, "nrb_kernel_convolution_cubic_static: volume has more voxels than the "
                                          "static scratch holds (NRB_STATIC_CONV_MAX_VOXELS = 2097152)");
-    StaticTaps taps;
-    const int radius = cubic_taps_fixed(spacing_mm, pixdim[axis], taps.k, NRB_STATIC_CONV_MAX_TAPS);
-    if (radius < 0)
+    double temp = 0;
+    int radius = 0;
+    NRB_TRY(cubic_extent("nrb_kernel_convolution_cubic_static", spacing_mm, pixdim[axis], temp, radius));
+    // the same early return as the allocating entry point, before the size limit on the taps
+    if (radius <= 0 || dim[axis] <= 1) return NRB_OK;  // the reference leaves the image as is
+    if (2 * radius + 1 > NRB_STATIC_CONV_MAX_TAPS)
         return fail(NRB_ERR_UNSUPPORTED, "nrb_kernel_convolution_cubic_static: kernel wider than the static "
                                          "scratch holds (NRB_STATIC_CONV_MAX_TAPS = 511 taps)");
-    if (radius <= 0 || dim[axis] <= 1) return NRB_OK;  // the reference leaves the image as is
+    StaticTaps taps;
+    cubic_taps(temp, radius, taps.k);
     unsigned char *base = nullptr;
     NRB_TRY(static_scratch(&base));
     float *dk = reinterpret_cast<float *>(base);

@@ -47,10 +47,62 @@ struct Job {
     double load = 0;
     Clock::time_point submitted, started, finished;
     bool done = false;
+    bool claimed = false;  // a nrb_server_wait call owns this ticket
     nrb_status status = NRB_OK;
     std::string error;
     nrb_f3d_result result{};
 };
+
+// The device's default memory pool is shared with the host application. While servers exist
+// on a device, its release threshold and internal-dependency reuse are set for them; the values
+// found when the first server was created are put back when the last one is destroyed.
+struct PoolSettings {
+    int servers = 0;
+    uint64_t threshold = 0;
+    int reuse_internal = 1;
+};
+std::mutex g_pool_mu;
+std::map<int, PoolSettings> g_pool_saved;
+
+void pool_acquire(int dev, int64_t budget) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    PoolSettings& ps = g_pool_saved[dev];
+    if (ps.servers++ == 0) {
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &ps.threshold);
+        cudaMemPoolGetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &ps.reuse_internal);
+    }
+    // keep freed registration buffers in the pool up to the budget, so the next admitted request
+    // reuses them instead of mapping new memory
+    uint64_t thr = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    thr = std::max(thr, (uint64_t)budget);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    // no reuse across streams through inserted dependencies: a registration must never wait for
+    // another one's stream because the pool handed it memory that stream freed
+    int no = 0;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+    cudaGetLastError();
+}
+
+void pool_release(int dev) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    auto it = g_pool_saved.find(dev);
+    if (it == g_pool_saved.end() || --it->second.servers > 0) return;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &it->second.threshold);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &it->second.reuse_internal);
+    g_pool_saved.erase(it);
+    cudaGetLastError();
+}
 
 }  // namespace
 
@@ -130,18 +182,7 @@ extern "C" nrb_status nrb_server_create(int slots, int64_t hbm_budget_bytes, nrb
     nrb_server *s = new nrb_server();
     s->device = dev;
     s->budget = hbm_budget_bytes > 0 ? hbm_budget_bytes : (int64_t)(0.8 * (double)free_b);
-    // keep freed registration buffers in the device's default pool up to the budget, so the
-    // next admitted request reuses them instead of mapping new memory
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-        uint64_t thr = (uint64_t)s->budget;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-        // no reuse across streams through inserted dependencies: a registration must never wait
-        // for another one's stream because the pool handed it memory that stream freed
-        int no = 0;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
-    }
-    cudaGetLastError();
+    pool_acquire(dev, s->budget);
     for (int i = 0; i < slots; ++i) s->workers.emplace_back([s] { s->worker(); });
     *out = s;
     return NRB_OK;
@@ -184,8 +225,12 @@ extern "C" nrb_status nrb_server_wait(nrb_server *s, int64_t ticket, nrb_f3d_res
         auto it = s->jobs.find(ticket);
         if (it == s->jobs.end()) return fail(NRB_ERR_INVALID, "nrb_server_wait: unknown ticket");
         job = it->second;
+        // a ticket is waited on once: a second waiter (another thread) is refused instead of
+        // reading the job after the first one has released it
+        if (job->claimed) return fail(NRB_ERR_INVALID, "nrb_server_wait: ticket already being waited on");
+        job->claimed = true;
         s->cv.wait(lock, [&] { return job->done; });
-        s->jobs.erase(it);
+        s->jobs.erase(ticket);
     }
     const nrb_status st = job->status;
     const std::string err = job->error;
@@ -214,6 +259,7 @@ extern "C" void nrb_server_destroy(nrb_server *s) {
     s->cv.notify_all();
     for (auto& t : s->workers) t.join();
     for (auto& kv : s->jobs) delete kv.second;
+    pool_release(s->device);
     delete s;
 }
 

@@ -6,7 +6,11 @@ Two CPU implementations sit here, both used only as checkers (by ``tests/``,
 * ``restated`` -- ``liboracle.so`` built from ``nrb_oracle.c``, a plain-C restatement of the
   reference algorithm, each function citing the reference file:line it follows;
 * ``ref``      -- ``_ref/libnrref.so``, the reference NiftyReg CPU library itself, compiled from
-  its own sources by ``oracle/Makefile`` (target ``ref``) plus the adapter ``ref_shim.cpp``.
+  its own sources by ``oracle/Makefile`` (target ``ref``) plus the adapters ``ref_shim.cpp`` and
+  ``ref_evaluate.cpp``;
+* ``ref64``    -- ``_ref64/libnrref64.so``, the same sources built without the SSE path (target
+  ``ref64``): the FP64 oracle (``evaluate(..., fp64=True)`` runs the reference's FLOAT64
+  instantiations) and the reference's scalar single-precision build.
 
 Parity of the restatement is pinned against ``ref`` and against the reference's own
 known-answer tests (see ``tests/test_oracle_pins.py``).
@@ -22,6 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATED_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libnrref.so")
+REF64_SO = os.path.join(HERE, "_ref64", "libnrref64.so")
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -61,11 +66,16 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
 
+def ref64_available() -> bool:
+    return os.path.exists(REF64_SO)
+
+
 # ----------------------------------------------------------------------------------------------
 # the reference library (oracle/_ref)
 # ----------------------------------------------------------------------------------------------
 class Ref:
-    """ctypes view of oracle/_ref/libnrref.so (the reference CPU implementation)."""
+    """ctypes view of oracle/_ref/libnrref.so (the reference CPU implementation), or of
+    oracle/_ref64/libnrref64.so (``Ref(REF64_SO)``: its build without the SSE path)."""
 
     def __init__(self, path: str = REF_SO):
         self.lib = ctypes.CDLL(path)
@@ -74,6 +84,32 @@ class Ref:
 
     def set_threads(self, n: int) -> int:
         return self.lib.ref_set_threads(int(n))
+
+    def evaluate(self, ref, rdim, rpix, rxyz, flo, fdim, fpix, fxyz, cpp, cdim, cpix, cxyz, bins,
+                 sim_weight, be_weight, pad=np.nan, fp64=False, want_def=False, want_warped=False):
+        """One F3D objective-and-gradient evaluation through the reference's own functions
+        (ref_evaluate.cpp): FLOAT32 images, or FLOAT64 ones with fp64=True (the FP64 oracle; only
+        the ref64 build runs it through double arithmetic everywhere). Returns a dict with
+        nmi, be, objective, entropies (H_ref, H_war, H_joint, total), node (3C, float64) and
+        optionally def (3N) and warped (N), all float64 arrays."""
+        nv, nc = int(np.prod(rdim)), int(np.prod(cdim))
+        node = np.zeros(3 * nc, np.float64)
+        vals = np.zeros(7, np.float64)
+        d = np.zeros(3 * nv, np.float64) if want_def else None
+        w = np.zeros(nv, np.float64) if want_warped else None
+        fn = self.lib.ref64_evaluate if fp64 else self.lib.ref32_evaluate
+        rc = fn(_f(_f3(ref)), _i(_i3(rdim)), _f(_f3(rpix)), _f(_m(rxyz)), _f(_f3(flo)), _i(_i3(fdim)),
+                _f(_f3(fpix)), _f(_m(fxyz)), _f(_f3(cpp)), _i(_i3(cdim)), _f(_f3(cpix)), _f(_m(cxyz)),
+                int(bins), int(bins), ctypes.c_double(sim_weight), ctypes.c_double(be_weight),
+                ctypes.c_float(pad), _d(d), _d(w), _d(node), _d(vals))
+        if rc != 0:
+            raise RuntimeError("reference evaluation failed")
+        out = dict(nmi=vals[0], be=vals[1], objective=vals[2], entropies=vals[3:7].copy(), node=node)
+        if want_def:
+            out["def"] = d
+        if want_warped:
+            out["warped"] = w
+        return out
 
     def create_control_point_grid(self, rdim, rpix, rxyz, spacing):
         cdim = np.zeros(3, np.int32)
@@ -178,6 +214,25 @@ class Ref:
         self.lib.ref_be_gradient(_f(_f3(cpp)), _i(_i3(cdim)), _f(_f3(cpix)), _f(_m(cxyz)),
                                  ctypes.c_float(weight), _f(g))
         return g
+
+    def image_pyramid(self, img, dim, pix, xyz, levels):
+        """reg_createImagePyramid<float>: list of (data [nz, ny, nx], dim, sform 4x4), coarsest first."""
+        self.lib.ref_image_pyramid.restype = ctypes.c_longlong
+        dims = np.zeros(3 * levels, np.int32)
+        mats = np.zeros(16 * levels, np.float32)
+        total = self.lib.ref_image_pyramid(_f(_f3(img)), _i(_i3(dim)), _f(_f3(pix)), _f(_m(xyz)), int(levels), None,
+                                           ctypes.c_size_t(0), _i(dims), _f(mats))
+        out = np.zeros(int(total), np.float32)
+        self.lib.ref_image_pyramid(_f(_f3(img)), _i(_i3(dim)), _f(_f3(pix)), _f(_m(xyz)), int(levels), _f(out),
+                                   ctypes.c_size_t(out.size), _i(dims), _f(mats))
+        res, off = [], 0
+        for l in range(levels):
+            d = dims[3 * l: 3 * l + 3]
+            n = int(np.prod(d))
+            res.append((out[off:off + n].reshape(d[2], d[1], d[0]), tuple(int(v) for v in d),
+                        mats[16 * l: 16 * l + 16].reshape(4, 4)))
+            off += n
+        return res
 
     def refine_grid(self, cpp, cdim, cpix, cxyz, rdim, rpix, rxyz):
         cap = 3 * int(np.prod([(int(c) - 3) * 2 + 8 for c in cdim]))

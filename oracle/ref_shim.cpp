@@ -339,6 +339,34 @@ int ref_be_gradient(const float *cpp, const int *cdim, const float *cpix, const 
     return 0;
 }
 
+// reg_createImagePyramid<float> (_reg_tools.cpp:1705-1733) with `levels` levels, all performed:
+// the levels end to end in out (coarsest first), their dims and sform matrices; out may be null
+// to query the total. Returns the total float count, or -1 when cap is too small.
+long long ref_image_pyramid(const float *img, const int *dim, const float *pix, const float *xyz, int levels,
+                            float *out, size_t cap, int *dims_out, float *xyz_out) {
+    NiftiImage im = MakeImage(dim, pix, xyz);
+    memcpy(im->data, img, Nvox(dim) * sizeof(float));
+    std::vector<NiftiImage> pyr(levels);
+    reg_createImagePyramid<float>(im, pyr, unsigned(levels), unsigned(levels));
+    size_t total = 0;
+    for (int l = 0; l < levels; ++l) {
+        dims_out[3 * l] = pyr[l]->nx;
+        dims_out[3 * l + 1] = pyr[l]->ny;
+        dims_out[3 * l + 2] = pyr[l]->nz;
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) xyz_out[16 * l + 4 * i + j] = pyr[l]->sto_xyz.m[i][j];
+        total += pyr[l]->nvox;
+    }
+    if (!out) return (long long)total;
+    if (cap < total) return -1;
+    size_t off = 0;
+    for (int l = 0; l < levels; ++l) {
+        memcpy(out + off, pyr[l]->data, pyr[l]->nvox * sizeof(float));
+        off += pyr[l]->nvox;
+    }
+    return (long long)total;
+}
+
 // _reg_localTrans.cpp:2121-2170 (grid refinement onto the reference image)
 int ref_refine_grid(const float *cpp, const int *cdim, const float *cpix, const float *cxyz,
                     const int *rdim, const float *rpix, const float *rxyz,

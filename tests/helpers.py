@@ -20,6 +20,35 @@ def ensure_built():
         subprocess.check_call(["make", "-C", oracle_dir, "liboracle.so"], stdout=subprocess.DEVNULL)
 
 
+class ArgBuffers:
+    """Real buffers for the tests that check an entry point refuses bad arguments before any
+    device work. With a CUDA device they are device allocations, so an entry point that launched
+    a kernel before its checks would read valid memory and fail the test's assertion, never
+    fault the device; without one no kernel can launch at all, and host buffers stand in."""
+
+    def __init__(self, count=2, nbytes=1 << 16):
+        import ctypes
+        self._keep = []
+        self.ptrs = []
+        try:
+            import torch
+            cuda = torch.cuda.is_available()
+        except Exception:
+            cuda = False
+        for _ in range(count):
+            if cuda:
+                t = torch.zeros(nbytes // 4, dtype=torch.float32, device="cuda")
+                self._keep.append(t)
+                self.ptrs.append(ctypes.c_void_p(t.data_ptr()))
+            else:
+                b = (ctypes.c_char * nbytes)()
+                self._keep.append(b)
+                self.ptrs.append(ctypes.c_void_p(ctypes.addressof(b)))
+
+    def __getitem__(self, i):
+        return self.ptrs[i]
+
+
 @dataclasses.dataclass
 class Case:
     rdim: tuple        # (nx, ny, nz)

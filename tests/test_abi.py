@@ -7,7 +7,7 @@ import re
 import numpy as np
 
 import niftyreg_b200 as nrb
-from tests.helpers import ROOT, ensure_built
+from tests.helpers import ROOT, ArgBuffers, ensure_built
 
 
 def declared_functions():
@@ -55,7 +55,7 @@ def test_invalid_arguments_are_reported():
     g = nrb.make_geometry((8, 8, 8), (1.0, 1.0, 1.0), nrb.identity_header((1.0, 1.0, 1.0)), (8, 8, 8), (1.0, 1.0, 1.0),
                           nrb.identity_header((1.0, 1.0, 1.0)), (5, 5, 5), (5.0, 5.0, 5.0),
                           nrb.identity_header((5.0, 5.0, 5.0), (-5.0, -5.0, -5.0)))
-    fake = ctypes.c_void_p(16)  # never dereferenced: the order check comes first
+    fake = ArgBuffers(1)[0]  # a real buffer: the order check comes first
     assert lib.nrb_resample_image_order(ctypes.byref(g), fake, fake, None, 2, ctypes.c_float(0.0), fake, None) == 2
     assert b"order" in lib.nrb_last_error()
     assert lib.nrb_f3d_warped_image(ctypes.byref(g), fake, fake, 4, ctypes.c_float(0.0), fake, None) == 2
@@ -65,7 +65,8 @@ def test_f3d2_refusals_before_any_device_work(tmp_path):
     """The velocity-field entry points check their arguments before touching the device."""
     ensure_built()
     lib = nrb.lib()
-    fake = ctypes.c_void_p(16)  # never dereferenced: every check below comes first
+    bufs = ArgBuffers(2)  # real buffers: every check below comes first
+    fake = bufs[0]
     eye = nrb.identity_header((1.0, 1.0, 1.0))
     x16 = (ctypes.c_float * 16)(*[float(v) for v in eye.ravel()])
     dim = (ctypes.c_int32 * 3)(4, 4, 4)
@@ -83,7 +84,7 @@ def test_f3d2_refusals_before_any_device_work(tmp_path):
     assert lib.nrb_get_def_field_from_velocity_grid(ctypes.byref(g), fake, 0, ctypes.byref(steps), fake, None) == 1
     other = nrb.make_geometry((8, 8, 8), (1.0, 1.0, 1.0), eye, (8, 8, 8), (1.0, 1.0, 1.0), eye, (6, 5, 5),
                               (5.0, 5.0, 5.0), nrb.identity_header((5.0, 5.0, 5.0), (-5.0, -5.0, -5.0)))
-    assert lib.nrb_symmetrise_velocity_fields(ctypes.byref(g), fake, ctypes.byref(other), ctypes.c_void_p(32),
+    assert lib.nrb_symmetrise_velocity_fields(ctypes.byref(g), fake, ctypes.byref(other), bufs[1],
                                               None) == 1
     assert lib.nrb_symmetrise_velocity_fields(ctypes.byref(g), fake, ctypes.byref(g), fake, None) == 1
     # images and files: checked on the host

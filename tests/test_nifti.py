@@ -154,3 +154,36 @@ def test_refusals(tmp_path):
     (tmp_path / "complex.nii").write_bytes(bytes(raw))
     with pytest.raises(nrb.NrbError):
         nrb.read_image(tmp_path / "complex.nii")
+
+
+def test_headers_whose_sizes_overflow_or_point_past_the_file_are_refused(tmp_path):
+    """Crafted headers: element counts whose byte size wraps 64 bits, a vox_offset that is NaN or
+    past the end of the file, and data shorter than the dims say are all refused before any
+    allocation sized from them."""
+    ensure_built()
+    data = np.zeros((2, 2, 2), np.float32)
+    base = bytearray(nifti_bytes(data, 16))
+
+    def refused(name, raw):
+        (tmp_path / name).write_bytes(bytes(raw))
+        with pytest.raises(nrb.NrbError):
+            nrb.read_image(tmp_path / name)
+
+    # 16384^4 * 64 voxels = 2^62: times 4 bytes wraps to 0 in 64-bit arithmetic
+    wrap = bytearray(base)
+    struct.pack_into("<8h", wrap, 40, 5, 16384, 16384, 16384, 16384, 64, 1, 1)
+    refused("wrap.nii", wrap)
+    # every dim at its maximum: the element count itself overflows
+    huge = bytearray(base)
+    struct.pack_into("<8h", huge, 40, 7, 32767, 32767, 32767, 32767, 32767, 32767, 32767)
+    refused("huge.nii", huge)
+    for off in (float("nan"), float("inf"), 1.0e9):
+        raw = bytearray(base)
+        struct.pack_into("<f", raw, 108, off)
+        refused(f"offset_{off}.nii", raw)
+    short = bytearray(base)
+    struct.pack_into("<8h", short, 40, 3, 2, 2, 3, 1, 1, 1, 1)  # 12 voxels, the file holds 8
+    refused("short.nii", short)
+    # the unmodified file still reads
+    (tmp_path / "ok.nii").write_bytes(bytes(base))
+    nrb.read_image(tmp_path / "ok.nii")
