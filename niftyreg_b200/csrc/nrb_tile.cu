@@ -41,6 +41,9 @@ struct WalkParams {
     int cnv;                 // control points per component
     int log_in_smem;         // gradient: an FP32 copy of the log table is staged in shared memory
     int xs;                  // objective: x-contracted rows of the item staged in shared memory
+    // identity split of the positions (grid matrix without off-diagonal terms; zero otherwise):
+    // node k of axis c sits at io[c] + is[c] * k mm when the transformation is the identity
+    float io[3], is[3];
 };
 
 __device__ __forceinline__ int pre_of(int v, float gs) { return (int)((float)v / gs); }
@@ -50,8 +53,34 @@ __device__ __forceinline__ float frac_of(int v, float gs, int pre) {
     return t < 0.f ? 0.f : t;
 }
 
-// shared floats of the per-item tables: z basis [zchunk][4] and z node index [zchunk]
-__host__ __device__ inline int walk_table_floats(int zchunk) { return 5 * zchunk; }
+// shared floats of the per-item tables: z basis [zchunk][4], z node index [zchunk] and the
+// identity z position of each slice as a (hi, lo) float pair [zchunk][2]
+__host__ __device__ inline int walk_table_floats(int zchunk) { return 7 * zchunk; }
+
+// Positions as identity + displacement. With the grid's voxel -> mm matrix free of off-diagonal
+// terms, the identity position of node k along axis c is io[c] + is[c] * k, and the cubic
+// B-spline reproduces linear functions exactly, so for a voxel at grid coordinate pre + t
+// (pre = node index, t = basis fraction)
+//     sum_k B_k(t) CP_k = io + is * (pre + 1 + t) + sum_k B_k(t) (CP_k - io - is * k).
+// The walk sums the displacements CP_k - (io + is * k) in float (magnitudes of a few mm, so their
+// rounding errors are ~1e-7 mm) and adds the identity part, evaluated in double and held as a
+// (hi, lo) float pair, at the end: the position is then within about one float ulp of the FP64
+// evaluation of the same sum, where summing absolute positions (hundreds of mm) in float drifts
+// by several ulps. With a general grid matrix io = is = 0 and the sum is the absolute one.
+__device__ __forceinline__ double identity_coord(float io, float is, int pre, double t) {
+    return (double)io + (double)is * ((double)(pre + 1) + t);
+}
+
+__device__ __forceinline__ void split_hi_lo(double v, float& hi, float& lo) {
+    hi = (float)v;
+    lo = (float)(v - (double)hi);
+}
+
+// basis fraction of voxel v in double (the FP64 evaluation's t), clamped as frac_of clamps
+__device__ __forceinline__ double frac_of_d(int v, float gs, int pre) {
+    const double t = (double)v / (double)gs - (double)pre;
+    return t < 0.0 ? 0.0 : t;
+}
 
 struct Item {
     int x0, y0, z0, z1, xa0, yb0, zc0;
@@ -65,7 +94,7 @@ struct Item {
 // the block.
 template <bool kTrial = false>
 __device__ __forceinline__ void stage_item(const WalkParams& P, const float *__restrict__ cpp, int item,
-                                           float *cp, float *zb, int *zk, Item& I,
+                                           float *cp, float *zb, int *zk, float2 *zid, Item& I,
                                            const float *__restrict__ grad = nullptr, float scale = 0.f) {
     const int tx = item % P.tiles_x;
     const int rest = item / P.tiles_x;
@@ -93,24 +122,33 @@ __device__ __forceinline__ void stage_item(const WalkParams& P, const float *__r
                 const int src = c * P.cnv + (I.zc0 * P.cy + I.yb0 + jb) * P.cx + I.xa0 + ia;
                 float *dst = cp + (c * P.sc * P.sb + jb) * P.sa + ia;
                 const float *g = kTrial ? grad : nullptr;
+                // the identity position of this node row (component c varies along axis c only)
+                const double io = (double)P.io[c], is = (double)P.is[c];
+                const double rowid = c == 0 ? io + is * (double)(I.xa0 + ia)
+                                   : c == 1 ? io + is * (double)(I.yb0 + jb) : io + is * (double)I.zc0;
+                const double kstep = c == 2 ? is : 0.0;
                 int kc = 0;
                 for (; kc + 4 <= nc; kc += 4) {
                     const float v0 = trial_cp(cpp, g, scale, src + kc * gplane);
                     const float v1 = trial_cp(cpp, g, scale, src + (kc + 1) * gplane);
                     const float v2 = trial_cp(cpp, g, scale, src + (kc + 2) * gplane);
                     const float v3 = trial_cp(cpp, g, scale, src + (kc + 3) * gplane);
-                    dst[kc * splane] = v0;
-                    dst[(kc + 1) * splane] = v1;
-                    dst[(kc + 2) * splane] = v2;
-                    dst[(kc + 3) * splane] = v3;
+                    dst[kc * splane] = (float)((double)v0 - (rowid + kstep * kc));
+                    dst[(kc + 1) * splane] = (float)((double)v1 - (rowid + kstep * (kc + 1)));
+                    dst[(kc + 2) * splane] = (float)((double)v2 - (rowid + kstep * (kc + 2)));
+                    dst[(kc + 3) * splane] = (float)((double)v3 - (rowid + kstep * (kc + 3)));
                 }
-                for (; kc < nc; ++kc) dst[kc * splane] = trial_cp(cpp, g, scale, src + kc * gplane);
+                for (; kc < nc; ++kc)
+                    dst[kc * splane] = (float)((double)trial_cp(cpp, g, scale, src + kc * gplane) - (rowid + kstep * kc));
             }
     for (int zi = threadIdx.x; zi < I.z1 - I.z0; zi += blockDim.x) {
         const int z = I.z0 + zi;
         const int pz = pre_of(z, P.gsz);
         zk[zi] = pz - I.zc0;
         bspline_basis(frac_of(z, P.gsz, pz), zb + 4 * zi);
+        float2 h;
+        split_hi_lo(identity_coord(P.io[2], P.is[2], pz, frac_of_d(z, P.gsz, pz)), h.x, h.y);
+        zid[zi] = h;
     }
     __syncthreads();
 }
@@ -125,6 +163,7 @@ struct Column {
     const float *base;
     int win;         // relative z node index of S[0]
     float S[4][3];
+    float hx, lx, hy, ly;  // identity x and y positions of the column as (hi, lo) float pairs
 };
 
 __device__ __forceinline__ void column_init(const WalkParams& P, const Item& I, const float *cp, Column& C) {
@@ -136,6 +175,8 @@ __device__ __forceinline__ void column_init(const WalkParams& P, const Item& I, 
     const int px = pre_of(xc, P.gsx), py = pre_of(yc, P.gsy);
     bspline_basis(frac_of(xc, P.gsx, px), C.bx);
     bspline_basis(frac_of(yc, P.gsy, py), C.by);
+    split_hi_lo(identity_coord(P.io[0], P.is[0], px, frac_of_d(xc, P.gsx, px)), C.hx, C.lx);
+    split_hi_lo(identity_coord(P.io[1], P.is[1], py, frac_of_d(yc, P.gsy, py)), C.hy, C.ly);
     C.xoff = px - I.xa0;
     C.yrow = py - I.yb0;
     C.base = cp + C.yrow * P.sa + C.xoff;
@@ -199,7 +240,8 @@ __device__ __forceinline__ void column_plane_x(const WalkParams& P, const Column
 // World position (mm) of slice index zi (relative to the item) of the thread's column; zi must
 // not decrease between calls. X: the item's x-contracted rows, or null.
 __device__ __forceinline__ void column_position(const WalkParams& P, const Item& I, Column& C, const float *zb,
-                                                const int *zk, int zi, float pos[3], const float *X = nullptr) {
+                                                const int *zk, const float2 *zid, int zi, float pos[3],
+                                                const float *X = nullptr) {
     const int pz = zk[zi];
     if (pz != C.win) {
         if (pz == C.win + 1) {
@@ -227,6 +269,11 @@ __device__ __forceinline__ void column_position(const WalkParams& P, const Item&
         s = fmaf(bz.w, C.S[3][c], s);
         pos[c] = s;
     }
+    // identity part: hi + (lo + displacement), two roundings on values far below an ulp of hi
+    const float2 hz = zid[zi];
+    pos[0] = __fadd_rn(C.hx, __fadd_rn(C.lx, pos[0]));
+    pos[1] = __fadd_rn(C.hy, __fadd_rn(C.ly, pos[1]));
+    pos[2] = __fadd_rn(hz.x, __fadd_rn(hz.y, pos[2]));
 }
 
 // mm -> floating voxel as Mat44Mul does it (reg-lib/cpu/Maths.hpp:272-286): the products of
@@ -344,6 +391,7 @@ constexpr int WALK_GROUP = 1;  // slices per step of the walk (two in flight mea
 struct WalkSmem {
     float *cp, *zb;
     int *zk;
+    float2 *zid;
     char *tail;
 };
 
@@ -351,7 +399,8 @@ __device__ __forceinline__ WalkSmem walk_smem(const WalkParams& P, void *base) {
     WalkSmem s;
     s.cp = reinterpret_cast<float *>(base);
     s.zb = s.cp + ((3 * P.sc * P.sb * P.sa + 3) & ~3);  // 16-byte aligned rows of 4 basis values
-    s.zk = reinterpret_cast<int *>(s.zb + 4 * P.zchunk);
+    s.zid = reinterpret_cast<float2 *>(s.zb + 4 * P.zchunk);  // 8-byte aligned pairs
+    s.zk = reinterpret_cast<int *>(s.zid + P.zchunk);
     s.tail = reinterpret_cast<char *>(s.zk + P.zchunk);
     // 16-byte alignment of the tail
     s.tail = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(s.tail) + 15) & ~uintptr_t(15));
@@ -386,7 +435,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
     const float frb = (float)P.rb, ffb = (float)P.fb;
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
         Item I;
-        stage_item<kTrial>(P, cpp, item, S.cp, S.zb, S.zk, I, grad, scale);
+        stage_item<kTrial>(P, cpp, item, S.cp, S.zb, S.zk, S.zid, I, grad, scale);
         Column C;
         column_init(P, I, S.cp, C);
         if (kXs) build_xrows(P, C, S.cp, X);
@@ -399,7 +448,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
             for (int u = 0; u < WALK_GROUP; ++u) {
                 const int zu = min(zi + u, nzi - 1);
                 float pos[3];
-                column_position(P, I, C, S.zb, S.zk, zu, pos, kXs ? X : nullptr);
+                column_position(P, I, C, S.zb, S.zk, S.zid, zu, pos, kXs ? X : nullptr);
                 bin[u] = -1;
                 if (C.inside && zi + u < nzi) {
                     const int vi = idx + u * zstride;
@@ -577,7 +626,7 @@ k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict_
     }
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
         Item I;
-        stage_item(P, cpp, item, S.cp, S.zb, S.zk, I);
+        stage_item(P, cpp, item, S.cp, S.zb, S.zk, S.zid, I);
         Column C;
         column_init(P, I, S.cp, C);
         const int nzi = I.z1 - I.z0;
@@ -585,7 +634,7 @@ k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict_
         int idx = (I.z0 * P.ny + C.y) * P.nx + C.x;
         for (int zi = 0; zi < nzi; ++zi, idx += zstride) {
             float pos[3];
-            column_position(P, I, C, S.zb, S.zk, zi, pos);
+            column_position(P, I, C, S.zb, S.zk, S.zid, zi, pos);
             if (!C.inside) continue;
             float out[3] = { 0.f, 0.f, 0.f };
             if (mask == nullptr || __ldg(&mask[idx]) > -1) {
@@ -621,13 +670,13 @@ k_deformation(WalkParams P, const int32_t *__restrict__ mask, const float *__res
     const int nv = P.nx * P.ny * P.nz;
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
         Item I;
-        stage_item(P, cpp, item, S.cp, S.zb, S.zk, I);
+        stage_item(P, cpp, item, S.cp, S.zb, S.zk, S.zid, I);
         Column C;
         column_init(P, I, S.cp, C);
         const int nzi = I.z1 - I.z0;
         for (int zi = 0; zi < nzi; ++zi) {
             float pos[3];
-            column_position(P, I, C, S.zb, S.zk, zi, pos);
+            column_position(P, I, C, S.zb, S.zk, S.zid, zi, pos);
             if (!C.inside) continue;
             const int idx = ((I.z0 + zi) * P.ny + C.y) * P.nx + C.x;
             if (mask != nullptr && __ldg(&mask[idx]) <= -1) pos[0] = pos[1] = pos[2] = 0.f;
@@ -1010,13 +1059,13 @@ k_warp_order(WalkParams P, const float *__restrict__ cpp, const float *__restric
     const WalkSmem S = walk_smem(P, sm4);
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
         Item I;
-        stage_item(P, cpp, item, S.cp, S.zb, S.zk, I);
+        stage_item(P, cpp, item, S.cp, S.zb, S.zk, S.zid, I);
         Column C;
         column_init(P, I, S.cp, C);
         const int nzi = I.z1 - I.z0;
         for (int zi = 0; zi < nzi; ++zi) {
             float pos[3];
-            column_position(P, I, C, S.zb, S.zk, zi, pos);
+            column_position(P, I, C, S.zb, S.zk, S.zid, zi, pos);
             if (!C.inside) continue;
             const int idx = ((I.z0 + zi) * P.ny + C.y) * P.nx + C.x;
             warped[idx] = sample_order<kOrder>(flo, P.fnx, P.fny, P.fnz, P.flo_ijk, P.pad, pos[0], pos[1], pos[2]);
@@ -1102,6 +1151,13 @@ static WalkParams make_params(const WalkPlan& W, const nrb_geometry *g, float pa
     P.flo_diag = m[1] == 0.f && m[2] == 0.f && m[4] == 0.f && m[6] == 0.f && m[8] == 0.f && m[9] == 0.f;
     P.log_in_smem = 0;
     P.xs = 0;
+    // identity split when the grid's voxel -> mm matrix has no off-diagonal terms
+    const float *c = g->cpp_xyz;
+    const bool cdiag = c[1] == 0.f && c[2] == 0.f && c[4] == 0.f && c[6] == 0.f && c[8] == 0.f && c[9] == 0.f;
+    for (int d = 0; d < 3; ++d) {
+        P.io[d] = cdiag ? c[4 * d + 3] : 0.f;
+        P.is[d] = cdiag ? c[5 * d] : 0.f;
+    }
     return P;
 }
 

@@ -1,24 +1,19 @@
-"""The fused F3D evaluations against the oracle pipeline, plus determinism and full-size
-properties.
+"""The fused F3D evaluations against the oracle pipeline, plus determinism properties.
 
-Tolerances: NMI within 1e-5 relative; bending energy within 1e-6 relative; node gradient
-within NODE_L2 in relative L2 norm, and no component off by more than NODE_MAX of the largest
-magnitude (a gross-error cap). The node-gradient bounds are set by the reference itself: the
-spatial gradient of a trilinear interpolant jumps at voxel faces, so a 1e-5 mm change of a
-warped position can move one voxel's contribution across the jump. The reference's own SSE
-build and its scalar arithmetic (the oracle) differ by 2.5e-5..9e-5 (L2) and 3e-5..1.3e-4
-(max) on the small cases and by 1.2e-4 (L2) / 1.7e-3 (max) on the 182x218x182 case. Repeated
-evaluations must be bit-identical (integer histograms, fixed-order FP64 reductions).
+Tolerances: NMI within 1e-5 relative and bending energy within 1e-6 relative of the C
+restatement (oracle/liboracle.so); node gradient within 1e-4 relative L2
+of the reference's own CPU evaluation (oracle/_ref, its default SSE build, through
+ref_evaluate.cpp), with no separate cap on single components: on these small volumes the whole
+gradient meets the bar. The full-size cases, where single precision itself sets the floor, are
+in test_parity_reference_gpu.py together with the FP64 oracle. Repeated evaluations must be
+bit-identical (integer histograms, fixed-order FP64 reductions).
 """
-import math
-
 import numpy as np
 import pytest
 
 import niftyreg_b200 as nrb
 import oracle
-from niftyreg_b200 import phantom
-from tests.helpers import ensure_built, identity_grid, make_case, rescale
+from tests.helpers import ensure_built, make_case
 
 pytestmark = pytest.mark.gpu
 
@@ -32,7 +27,7 @@ CASES = {
     "bins132": dict(seed=5, bins=132),
 }
 SIM_W, BE_W = 0.995, 0.005
-NODE_L2, NODE_MAX = 3e-4, 5e-2
+NODE_L2 = 1e-4
 
 
 @pytest.fixture(scope="module")
@@ -84,18 +79,18 @@ def test_fused_objective(O, case):
 
 def test_fused_gradient(O, case):
     c = case
+    if not oracle.ref_available():
+        pytest.skip("reference library (oracle/_ref) not built")
     g = c.geometry()
     ws, nmi = nrb.Workspace(g), nrb.Nmi(c.bins, c.bins)
     vg = torch.empty(3 * c.nvox, dtype=torch.float32, device="cuda")
     node = torch.full((3 * c.ncp,), 7.0, dtype=torch.float32, device="cuda")
     nrb.f3d_gradient(ws, nmi, dev(c.ref), dev(c.flo), dev(c.cpp), vg, node, SIM_W, BE_W)
-    ref = oracle_gradient(O, c)
-    out = host(node)
-    scale = np.abs(ref).max()
-    err = np.abs(out - ref).max()
+    ref = oracle.Ref().evaluate(c.ref, c.rdim, c.rpix, c.rxyz, c.flo, c.fdim, c.fpix, c.fxyz, c.cpp, c.cdim,
+                                c.cpix, c.cxyz, c.bins, SIM_W, BE_W)["node"]
+    out = host(node).astype(np.float64)
     l2 = np.linalg.norm(out - ref) / np.linalg.norm(ref)
     assert l2 <= NODE_L2, f"node gradient L2 error {l2:.3g}"
-    assert err <= NODE_MAX * scale, f"node gradient error {err / scale:.3g} of max"
 
 
 def test_repeatable_bitwise():
@@ -141,37 +136,3 @@ def test_zero_similarity_weight():
     ws, nmi = nrb.Workspace(c.geometry()), nrb.Nmi(c.bins, c.bins)
     o = nrb.f3d_objective(ws, nmi, dev(c.ref), dev(c.flo), dev(c.cpp), 0.0, 1.0)
     assert o.nmi == 0.0 and o.objective == -o.be
-
-
-def test_full_size_against_oracle(O):
-    """The brain-MR-sized workload (182x218x182, 1 mm, 5 mm grid, N(0,3 mm) control
-    displacements): fused objective and gradient against the full oracle pipeline, and
-    bit-identical repeats."""
-    shape = (182, 218, 182)
-    pair = phantom.brain_pair(shape, seed=3)
-    nz, ny, nx = shape
-    rdim, rpix = (nx, ny, nz), (1.0, 1.0, 1.0)
-    rxyz = nrb.identity_header(rpix)
-    cdim, cpix, cxyz = nrb.control_grid_header(rdim, rpix, (5.0, 5.0, 5.0))
-    rng = np.random.default_rng(3)
-    cpp = identity_grid(cdim, cxyz) + rng.normal(0, 3.0, 3 * int(np.prod(cdim))).astype(np.float32)
-    ref = rescale(pair.reference, 2, 65).ravel()
-    flo = rescale(pair.floating, 2, 65).ravel()
-    from tests.helpers import Case
-    c = Case(rdim, rpix, rxyz, rdim, rpix, rxyz, tuple(cdim), tuple(cpix), cxyz, ref, flo, cpp, 68)
-    g = c.geometry()
-    ws, nmi = nrb.Workspace(g), nrb.Nmi(68, 68)
-    rt, ft, ct = dev(ref), dev(flo), dev(cpp)
-    a = nrb.f3d_objective(ws, nmi, rt, ft, ct, SIM_W, BE_W)
-    b = nrb.f3d_objective(ws, nmi, rt, ft, ct, SIM_W, BE_W)
-    assert a.nmi == b.nmi and a.be == b.be
-    v, be, *_ = oracle_objective(O, c)
-    assert abs(a.nmi - v) <= 1e-5 * v
-    assert abs(a.be - be) <= 1e-6 * be
-    vg = torch.empty(3 * c.nvox, dtype=torch.float32, device="cuda")
-    node = torch.empty(3 * c.ncp, dtype=torch.float32, device="cuda")
-    nrb.f3d_gradient(ws, nmi, rt, ft, ct, vg, node, SIM_W, BE_W)
-    ref_node = oracle_gradient(O, c)
-    out = host(node)
-    assert np.linalg.norm(out - ref_node) <= NODE_L2 * np.linalg.norm(ref_node)
-    assert np.abs(out - ref_node).max() <= NODE_MAX * np.abs(ref_node).max()
