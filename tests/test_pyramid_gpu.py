@@ -110,7 +110,9 @@ def test_grid_refinement_matches_reference(name):
     nrb.refine_control_point_grid(torch.from_numpy(cpp).cuda(), cdim, out, ndim)
     got = out.cpu().numpy()
     diff = np.abs(got - want)
-    ulps = diff / np.spacing(np.abs(want))
+    # ulps at the scale of the summed node values: a node near the origin is a sum of terms of
+    # the order of the grid spacing, whose rounding does not shrink with the result
+    ulps = diff / np.spacing(np.maximum(np.abs(want), np.float32(spacing)))
     print(f"[refine] {name}: {tuple(int(v) for v in cdim)} -> {tuple(int(v) for v in ndim)} nodes, "
           f"max |diff| {diff.max():.3g} ({ulps.max():.1f} ulp), {np.mean(got == want):.4f} bit-identical")
     assert ulps.max() <= 2.0
