@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--mode", choices=["plain", "batched", "served", "warp", "f3d2"], default="plain")
     ap.add_argument("--pairs", type=int, default=64, help="batched: number of pairs")
     ap.add_argument("--concurrency", type=int, default=16, help="batched/served: concurrent registrations")
+    ap.add_argument("--grad-percent", type=int, default=50,
+                    help="batched: run a level's gradient stage once this share of the active pairs waits for it")
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--batch-only", action="store_true", help="batched: skip the one-by-one run (profiling)")
     ap.add_argument("--requests", type=int, default=300, help="served: requests per arrival rate")
     ap.add_argument("--rates", default="5,20,50", help="served: Poisson arrival rates (requests/s)")
     ap.add_argument("--shape", default=None, help="kernel-only mode: nz,ny,nx of the volume (default: the workload's)")
@@ -516,12 +520,18 @@ def run_batched(args):
     sampler = _gpu_clock_sampler()
     sampler.start()
     t0 = time.perf_counter()
-    plain = [nrb.register_host(p.reference, p.floating, p.pixdim, params) for p in pairs]
+    plain = [] if args.batch_only else [nrb.register_host(p.reference, p.floating, p.pixdim, params) for p in pairs]
     t_plain = time.perf_counter() - t0
+    bparams = nrb.default_params(levels=BATCH_LEVELS, max_iterations=BATCH_MAXIT, bending_energy=BE,
+                                 spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS,
+                                 batch_gradient_percent=args.grad_percent, verbose=int(args.verbose))
     t0 = time.perf_counter()
-    batched = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], params, args.concurrency)
+    batched = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], bparams, args.concurrency)
     t_batch = time.perf_counter() - t0
     clocks = sampler.stop()
+    if args.batch_only:
+        print(json.dumps({"mode": "batched", "batch_only": True, "value": args.pairs / t_batch, "seconds": t_batch}))
+        return 0
     dnmi = max(abs(a[1].final_nmi - b[1].final_nmi) for a, b in zip(plain, batched))
     identical = all(np.array_equal(a[0], b[0]) for a, b in zip(plain, batched))
     line = {"mode": "batched", "metric": METRIC, "value": args.pairs / t_batch, "unit": "registrations/s",

@@ -263,6 +263,10 @@ typedef struct nrb_f3d_params {
                                * copy). Samples that reach into the margin take the kernels'
                                * plain load path instead of the clamped one; the results are the
                                * same bit for bit. */
+    int32_t batch_gradient_percent; /* nrb_f3d_register_batch: a level's gradient stage runs
+                               * once this share (%) of the pairs still active waits for a
+                               * gradient, or when no pair has a line-search step left (default
+                               * 50; 1..100). Scheduling only: results do not depend on it. */
 } nrb_f3d_params;
 
 typedef struct nrb_f3d_result {
@@ -491,7 +495,15 @@ nrb_status nrb_server_stats(nrb_server *s, int64_t *peak_bytes, int32_t *peak_ac
 /* Finishes the queued requests, then stops the workers. */
 void nrb_server_destroy(nrb_server *s);
 
-/* n registrations, up to `concurrency` at once under hbm_budget_bytes (<= 0: 80% of free). */
+/* n registrations advanced together (no counterpart in the reference, which registers one pair
+ * per reg_f3d run). The pairs are taken in order in groups of at most `concurrency` (<= 128)
+ * whose summed footprints fit in hbm_budget_bytes (<= 0: 80% of the free device memory); a group
+ * runs level by level, each level as one CUDA graph in which every stage -- the line-search
+ * objective, its finalize, the gradient, the node convolution, the conjugate-gradient direction
+ * -- is one launch over all the pairs that need it. Each pair's arithmetic is that of its plain
+ * registration, so results[i] and pairs[i].cpp_out_host equal nrb_f3d_register_host's for pair i
+ * alone, bit for bit. The pairs of a group share the parameters, so they share the bin counts;
+ * they may differ in size and spacing. */
 nrb_status nrb_f3d_register_batch(const nrb_pair *pairs, int n, const nrb_f3d_params *p,
                                   int concurrency, int64_t hbm_budget_bytes,
                                   nrb_f3d_result *results);

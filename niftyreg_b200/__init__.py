@@ -62,7 +62,8 @@ class F3dParams(ctypes.Structure):
     _fields_ = [("levels", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
                 ("bending_energy", ctypes.c_float), ("spacing", _F3), ("ref_bins", ctypes.c_int32),
                 ("flo_bins", ctypes.c_int32), ("padding", ctypes.c_float), ("verbose", ctypes.c_int32),
-                ("host_loop", ctypes.c_int32), ("floating_margin", ctypes.c_int32)]
+                ("host_loop", ctypes.c_int32), ("floating_margin", ctypes.c_int32),
+                ("batch_gradient_percent", ctypes.c_int32)]
 
 
 class Image(ctypes.Structure):

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -36,10 +37,6 @@ nrb_status cg_update_flagged(nrb_workspace *ws, float *grad, float *g1, float *g
 // kernels set. The arithmetic on the step lengths and objective values is the host loop's,
 // operation for operation.
 // ---------------------------------------------------------------------------------------------
-__device__ __forceinline__ bool outer_continues(const OptState& s) { return s.current_size != 0.f && s.it < s.max_it; }
-__device__ __forceinline__ bool line_continues(const OptState& s) {
-    return s.cur_len > s.small_step && s.line_iter < 12 && s.it < s.max_it;
-}
 
 __global__ void k_ctl_level(OptState *s, OptState init, cudaGraphConditionalHandle outer) {
     *s = init;
@@ -64,17 +61,7 @@ __global__ void k_ctl_line_start(OptState *s, cudaGraphConditionalHandle inner) 
 
 // end of Optimise (start length = added length) and the restart rule of _reg_base.cpp:784-793
 __global__ void k_ctl_line_end(OptState *s, cudaGraphConditionalHandle outer) {
-    s->current_size = s->added_len;
-    if (s->current_size == 0.f) {
-        if (!s->just_restarted && s->it < s->max_it) {
-            s->first_call = 1;
-            s->current_size = s->max_step;
-            s->just_restarted = 1;
-        }
-    } else {
-        s->just_restarted = 0;
-    }
-    cudaGraphSetConditional(outer, outer_continues(*s) ? 1u : 0u);
+    cudaGraphSetConditional(outer, line_end(s) ? 1u : 0u);
 }
 
 // The node-grid tail of a gradient evaluation in one launch (one cluster of TAIL_CTAS blocks):
@@ -87,11 +74,11 @@ __global__ void k_ctl_line_end(OptState *s, cudaGraphConditionalHandle outer) {
 constexpr int TAIL_CTAS = 8, TAIL_THREADS = 1024;
 constexpr long long kNodeTailMaxNodes = 16384;  // above it the passes are bandwidth-bound on 8 SMs
 
-__global__ void __cluster_dims__(TAIL_CTAS, 1, 1) __launch_bounds__(TAIL_THREADS)
-k_node_tail(long long nnode, float *__restrict__ g, float *__restrict__ g1, float *__restrict__ g2,
-            double *__restrict__ partials, nrb_objective *__restrict__ obj, OptState *__restrict__ s,
-            cudaGraphConditionalHandle line) {
-    cg::cluster_group cluster = cg::this_cluster();
+// The cluster's work: returns the largest node-gradient length; the optimiser state is only read
+// (first_call) and the caller publishes the rest.
+__device__ __forceinline__ double node_tail_cluster(cg::cluster_group& cluster, long long nnode, float *__restrict__ g,
+                                                    float *__restrict__ g1, float *__restrict__ g2,
+                                                    double *__restrict__ partials, const OptState *__restrict__ s) {
     __shared__ float fmx[TAIL_THREADS / 32];
     __shared__ double red[TAIL_THREADS];
     __shared__ double gam_s;
@@ -186,19 +173,47 @@ k_node_tail(long long nnode, float *__restrict__ g, float *__restrict__ g1, floa
             g[i] = -a2;
         }
     }
-    if (rank == 0 && tid == 0) {
+    return len;
+}
+
+__global__ void __cluster_dims__(TAIL_CTAS, 1, 1) __launch_bounds__(TAIL_THREADS)
+k_node_tail(long long nnode, float *__restrict__ g, float *__restrict__ g1, float *__restrict__ g2,
+            double *__restrict__ partials, nrb_objective *__restrict__ obj, OptState *__restrict__ s,
+            cudaGraphConditionalHandle line) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const double len = node_tail_cluster(cluster, nnode, g, g1, g2, partials, s);
+    if (cluster.block_rank() == 0 && threadIdx.x == 0) {
         obj->max_grad_len = len;
         // iteration counted, current_size = min(current_size, max_step), then Optimise starts
-        s->it += 1;
-        s->n_grad += 1;
-        s->current_size = s->max_step < s->current_size ? s->max_step : s->current_size;
-        s->first_call = 0;
-        s->line_iter = 0;
-        s->added_len = 0.f;
-        s->cur_len = s->current_size;
-        cudaGraphSetConditional(line, line_continues(*s) ? 1u : 0u);
+        cudaGraphSetConditional(line, gradient_done_line_start(s) ? 1u : 0u);
     }
     cluster.sync();  // block 0's shared values stay readable until every block has read them
+}
+
+// One node-tail cluster per pair (cluster q = pair q) for the pairs in GRAD: the same work, then
+// the pair's line search starts (LINE), or ends at once when it has no step to take (GRAD again
+// after a restart, or DONE); the last cluster sets whether the level goes on.
+__global__ void __cluster_dims__(TAIL_CTAS, 1, 1) __launch_bounds__(TAIL_THREADS)
+k_b_node_tail(const BatchPair *__restrict__ pairs, OptState *__restrict__ states, int npairs,
+              BatchCtl *__restrict__ bctl, cudaGraphConditionalHandle outer) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int p = blockIdx.x / TAIL_CTAS;
+    if (states[p].phase == PH_GRAD) {
+        const BatchPair& B = pairs[p];
+        OptState *s = &states[p];
+        const double len = node_tail_cluster(cluster, B.nnode, B.grad, B.g1, B.g2, B.red, s);
+        if (cluster.block_rank() == 0 && threadIdx.x == 0) {
+            B.obj->max_grad_len = len;
+            const bool line = gradient_done_line_start(s);
+            s->phase = line ? PH_LINE : (line_end(s) ? PH_GRAD : PH_DONE);
+        }
+        cluster.sync();
+    }
+    if (cluster.block_rank() != 0) return;
+    if (!batch_last_cluster(&bctl->ticket_tail, gridDim.x / TAIL_CTAS)) return;
+    int nline, ngrad;
+    batch_counts(states, npairs, nline, ngrad);
+    if (threadIdx.x == 0) cudaGraphSetConditional(outer, nline + ngrad > 0 ? 1u : 0u);
 }
 
 // StoreCurrentDof after an accepted step: best = best + (-len) * grad, the trial position the
@@ -265,6 +280,26 @@ nrb_status capture_while(cudaStream_t st, cudaGraphConditionalHandle h, cudaGrap
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = h;
     cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    NRB_CUDA(cudaGraphAddNode(&node, capg, deps, nd, &cp));
+    *body = cp.conditional.phGraph_out[0];
+    NRB_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return NRB_OK;
+}
+
+// Appends an IF node driven by `h` (body runs when the handle is non-zero), like capture_while.
+nrb_status capture_if(cudaStream_t st, cudaGraphConditionalHandle h, cudaGraph_t *body) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t capg = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    NRB_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &capg, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return fail(NRB_ERR_CUDA, "registration: stream capture not active");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
     cp.conditional.size = 1;
     cudaGraphNode_t node;
     NRB_CUDA(cudaGraphAddNode(&node, capg, deps, nd, &cp));
@@ -484,6 +519,20 @@ public:
                    int64_t cap, nrb_f3d_result *res, float *warped_out = nullptr);
     const Header& grid() const { return grid_; }
 
+    // The pieces of Run a batched driver calls for every pair: Begin (pyramid, grid, budget);
+    // per level PrepareLevel (InitLevel without the initial objective), Describe (the pair's
+    // BatchPair and starting optimiser state), Absorb (the optimiser state the batched level
+    // ended with), EndLevel; then Finish.
+    nrb_status Begin(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd);
+    nrb_status PrepareLevel(int level, float& max_step) {
+        batched_ = true;
+        return InitLevel(level, max_step);
+    }
+    nrb_status Describe(float max_step, BatchPair& b, OptState& init);
+    nrb_status Absorb(const OptState& out);
+    void EndLevel() { max_it_ /= 2; }
+    nrb_status Finish(const float *flo, float *cpp_out, int64_t cap, nrb_f3d_result *res, float *warped_out = nullptr);
+
 private:
     // reg_f3d::GetObjectiveFunctionValue (_reg_f3d.cpp:443-462)
     nrb_status GetObjectiveFunctionValue(double& value) {
@@ -610,6 +659,8 @@ private:
     double cur_w_measure_ = 0, cur_w_be_ = 0, best_w_measure_ = 0, best_w_be_ = 0;
     double cur_nmi_ = 0, cur_be_ = 0, best_nmi_ = 0, best_be_ = 0;
     int64_t n_obj_ = 0, n_grad_ = 0;
+    std::chrono::steady_clock::time_point t0_;
+    bool batched_ = false;  // levels driven by a batched graph (the initial objective is its first stage)
     // device-resident optimiser
     bool graph_ok_ = true;
     OptState *dstate_ = nullptr;
@@ -844,6 +895,64 @@ nrb_status build_pyramids(const float *ref, const float *flo, const ImageDesc& r
     return NRB_OK;  // tmp is freed in stream order
 }
 
+// The pair's description for a batched level (its walks, buffers, NMI tables, node stage) and
+// the optimiser state its level starts from (RunLevelGraph's init, the initial objective still
+// to be evaluated: phase INIT).
+nrb_status F3dRegistration::Describe(float max_step, BatchPair& b, OptState& init) {
+    if (!(sim_w_ > 0)) return fail(NRB_ERR_UNSUPPORTED, "batched registration: the similarity weight must be > 0");
+    memset(&b, 0, sizeof(b));
+    NRB_TRY(batch_walks(ws_.h, nmi_.h, &g_, pad_, margin_, b.wo, b.wg));
+    b.ref = ref_.p;
+    b.flo = flo_org_;
+    b.best = best_.p;
+    b.grad = grad_.p;
+    b.g1 = g1_.p;
+    b.g2 = g2_.p;
+    b.vgrad = vgrad_.p;
+    b.hist = nmi_.h->hist;
+    b.pro0 = nmi_.h->pro;
+    b.logt0 = nmi_.h->logt;
+    b.last0 = nmi_.h->last;
+    b.pro1 = nmi_.h->pro2;
+    b.logt1 = nmi_.h->logt2;
+    b.last1 = nmi_.h->last2;
+    b.obj = obj_;
+    b.rb = nmi_.h->rb;
+    b.fb = nmi_.h->fb;
+    NRB_TRY(batch_node_stage(ws_.h, &g_, sim_w_, be_w_, b));
+    b.sim_w = sim_w_;
+    b.be_w = be_w_;
+    b.obj_items = b.wo.nitems;
+    b.grad_items = b.wg.nitems;
+    init = OptState{};
+    init.it = (long long)it_;
+    init.max_it = (long long)max_it_;
+    init.n_obj = n_obj_;
+    init.n_grad = n_grad_;
+    init.current_size = max_step;
+    init.max_step = max_step;
+    init.small_step = max_step / 100.0f;
+    init.first_call = 1;
+    init.best_buf = 0;
+    init.phase = PH_INIT;
+    return NRB_OK;
+}
+
+// the optimiser state a batched level ended with; RestoreBestDof (current = best)
+nrb_status F3dRegistration::Absorb(const OptState& out) {
+    best_obj_ = out.best_obj;
+    best_w_measure_ = out.best_w_measure;
+    best_w_be_ = out.best_w_be;
+    best_nmi_ = out.best_nmi;
+    best_be_ = out.best_be;
+    it_ = (size_t)out.it;
+    n_obj_ = out.n_obj;
+    n_grad_ = out.n_grad;
+    first_call_ = out.first_call != 0;
+    NRB_CUDA(cudaMemcpyAsync(cur_.p, best_.p, 3 * nc_ * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+    return NRB_OK;
+}
+
 nrb_status F3dRegistration::BuildPyramid(const float *ref, const float *flo, const ImageDesc& rd,
                                          const ImageDesc& fd) {
     return build_pyramids(ref, flo, rd, fd, levels_, st_, hdr_, fhdr_, ref_pyr_, flo_pyr_);
@@ -929,19 +1038,21 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
     } else {
         flo_org_ = flo_.p;
     }
-    // ConjugateGradient::Initialise: best = current, objective at the starting point
+    // ConjugateGradient::Initialise: best = current, objective at the starting point (in a
+    // batched level the first stage of the level's graph evaluates it)
     it_ = 0;
     first_call_ = true;
     NRB_TRY(StoreCurrentDof());
+    if (batched_) return NRB_OK;
     double v = 0;
     NRB_TRY(GetObjectiveFunctionValue(v));
     best_obj_ = v;
     return NRB_OK;
 }
 
-nrb_status F3dRegistration::Run(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd,
-                                float *cpp_out, int64_t cap, nrb_f3d_result *res, float *warped_out) {
-    const auto t0 = std::chrono::steady_clock::now();
+// reg_f3d::Run up to the level loop: weights, pyramid, grid, iteration budget
+nrb_status F3dRegistration::Begin(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd) {
+    t0_ = std::chrono::steady_clock::now();
     levels_ = p_.levels;
     if (levels_ < 1) return fail(NRB_ERR_INVALID, "registration: levels must be >= 1");
     if (p_.ref_bins < 1 || p_.flo_bins < 1) return fail(NRB_ERR_INVALID, "registration: bins must be >= 1");
@@ -969,6 +1080,12 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const ImageD
     }
     max_it_ = (size_t)p_.max_iterations;
     max_it_ *= (size_t)std::pow(2, levels_ - 1);
+    return NRB_OK;
+}
+
+nrb_status F3dRegistration::Run(const float *ref, const float *flo, const ImageDesc& rd, const ImageDesc& fd,
+                                float *cpp_out, int64_t cap, nrb_f3d_result *res, float *warped_out) {
+    NRB_TRY(Begin(ref, flo, rd, fd));
     for (int level = 0; level < levels_; ++level) {
         float max_step = 0;
         const auto ti = std::chrono::steady_clock::now();
@@ -1006,6 +1123,12 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const ImageD
         }
         max_it_ /= 2;
     }
+    return Finish(flo, cpp_out, cap, res, warped_out);
+}
+
+// reg_f3d::Run after the level loop: the final grid (and warped image) out, the result record
+nrb_status F3dRegistration::Finish(const float *flo, float *cpp_out, int64_t cap, nrb_f3d_result *res,
+                                   float *warped_out) {
     const int64_t n = 3 * nc_;
     if (cpp_out) {
         if (cap < n) return fail(NRB_ERR_INVALID, "registration: cpp_out capacity too small");
@@ -1048,7 +1171,7 @@ nrb_status F3dRegistration::Run(const float *ref, const float *flo, const ImageD
         res->final_objective = best_obj_;
         res->objective_evaluations = n_obj_;
         res->gradient_evaluations = n_grad_;
-        res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
     }
     return NRB_OK;
 }
@@ -1136,6 +1259,7 @@ extern "C" void nrb_f3d_default_params(nrb_f3d_params *p) {
     p->verbose = 0;
     p->host_loop = 0;
     p->floating_margin = 8;
+    p->batch_gradient_percent = 50;
 }
 
 extern "C" nrb_status nrb_f3d_grid_dims(const int32_t ref_dim[3], const float ref_pixdim[3], const nrb_f3d_params *p,
@@ -1272,6 +1396,217 @@ extern "C" nrb_status nrb_f3d_register_files(const char *ref_path, const char *f
     nrb_image_free(&cpp);
     nrb_image_free(&warped);
     return s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched registrations: one graph per pyramid level for every pair of the batch
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+nrb_status batch_gradient_voxels(const BatchPair *d, const OptState *states, cudaStream_t st, void *arg) {
+    return launch_batch_gradient(d, states, *static_cast<const BatchLaunch *>(arg), st);
+}
+
+// One level of reg_base::Run for every pair, as one CUDA graph:
+//   WHILE(any pair active) {
+//       [bending-energy value || objective] of the pairs in INIT / LINE, one launch each;
+//       finalize, one cluster per pair (tables, NMI, line-search step, accepted step stored,
+//       phase moved on; sets the two conditions);
+//       IF(enough pairs wait for a gradient, or none has a line-search step left) {
+//           [bending-energy derivatives || voxel gradient -> node convolution (4 launches)] ->
+//           bending-energy gradient -> node tail, one cluster per pair (CG direction, line
+//           search started) } }
+// Each launch covers every pair that needs that stage; every pair's arithmetic is its plain
+// registration's (same walks, same reductions in the same order), so its result does not depend
+// on the rest of the batch. The host syncs once per level.
+struct BatchLevelRunner {
+    cudaStream_t st = nullptr, cap = nullptr, side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int grad_percent = 50;
+    BatchCtl stats{};  // of the last level run
+    double graph_ms[2] = { 0, 0 };  // instantiation, execution
+    ~BatchLevelRunner() {
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (cap) cudaStreamDestroy(cap);
+        if (side) cudaStreamDestroy(side);
+    }
+    nrb_status init(cudaStream_t s) {
+        st = s;
+        NRB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        NRB_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        NRB_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        NRB_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        return NRB_OK;
+    }
+
+    nrb_status run(std::vector<BatchPair>& hp, const std::vector<OptState>& init, std::vector<OptState>& out,
+                   int64_t *launches) {
+        const int np = (int)hp.size();
+        BatchLaunch L;
+        NRB_TRY(batch_plan(hp, L));
+        BatchPair *d_pairs = nullptr;
+        OptState *d_states = nullptr;
+        BatchCtl *d_ctl = nullptr;
+        NRB_CUDA(dev_alloc(&d_pairs, np * sizeof(BatchPair), st));
+        NRB_CUDA(dev_alloc(&d_states, np * sizeof(OptState), st));
+        NRB_CUDA(dev_alloc(&d_ctl, sizeof(BatchCtl), st));
+        BatchCtl ctl{};
+        ctl.grad_percent = grad_percent;
+        NRB_CUDA(cudaMemcpyAsync(d_pairs, hp.data(), np * sizeof(BatchPair), cudaMemcpyHostToDevice, st));
+        NRB_CUDA(cudaMemcpyAsync(d_states, init.data(), np * sizeof(OptState), cudaMemcpyHostToDevice, st));
+        NRB_CUDA(cudaMemcpyAsync(d_ctl, &ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, st));
+        nrb_status s = capture_and_run(hp, L, d_pairs, d_states, d_ctl, launches);
+        out.resize(np);
+        if (s == NRB_OK)
+            s = cudaMemcpyAsync(out.data(), d_states, np * sizeof(OptState), cudaMemcpyDeviceToHost, st) == cudaSuccess
+                    ? NRB_OK : fail(NRB_ERR_CUDA, "batched level: state read");
+        if (s == NRB_OK)
+            s = cudaMemcpyAsync(&stats, d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, st) == cudaSuccess
+                    ? NRB_OK : fail(NRB_ERR_CUDA, "batched level: statistics read");
+        dev_free(d_pairs, st);
+        dev_free(d_states, st);
+        dev_free(d_ctl, st);
+        if (s == NRB_OK) NRB_CUDA(cudaStreamSynchronize(st));
+        return s;
+    }
+
+    nrb_status capture_and_run(std::vector<BatchPair>& hp, const BatchLaunch& L, const BatchPair *d_pairs,
+                               OptState *d_states, BatchCtl *d_ctl, int64_t *launches) {
+        GraphHolder top;
+        cudaGraph_t while_body = nullptr, if_body = nullptr;
+        cudaGraphConditionalHandle h_outer, h_grad;
+        NRB_CUDA(cudaGraphCreate(&top.g, 0));
+        NRB_CUDA(cudaGraphConditionalHandleCreate(&h_outer, top.g, 1, cudaGraphCondAssignDefault));
+        auto abort_capture = [&](nrb_status e) {
+            cudaGraph_t dummy = nullptr;
+            cudaStreamEndCapture(cap, &dummy);
+            if (dummy && dummy != top.g && dummy != while_body && dummy != if_body) cudaGraphDestroy(dummy);
+            cudaGetLastError();
+            return e;
+        };
+        const long long c0 = g_launch_count.load();
+        NRB_CUDA(cudaStreamBeginCaptureToGraph(cap, top.g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        {
+            nrb_status e = capture_while(cap, h_outer, &while_body);
+            if (e != NRB_OK) return abort_capture(e);
+        }
+        NRB_CUDA(cudaStreamEndCapture(cap, &top.g));
+        NRB_CUDA(cudaGraphConditionalHandleCreate(&h_grad, while_body, 0, cudaGraphCondAssignDefault));
+        // the line-search stage
+        NRB_CUDA(cudaStreamBeginCaptureToGraph(cap, while_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        {
+            nrb_status e = NRB_OK;
+            const bool be = hp[0].be_w > 0;
+            if (be) {
+                if (cudaEventRecord(ev_fork, cap) != cudaSuccess || cudaStreamWaitEvent(side, ev_fork, 0) != cudaSuccess)
+                    e = fail(NRB_ERR_CUDA, "batched level: fork");
+                if (e == NRB_OK) e = launch_batch_be_value(hp, d_pairs, d_states, side);
+                if (e == NRB_OK && cudaEventRecord(ev_join, side) != cudaSuccess)
+                    e = fail(NRB_ERR_CUDA, "batched level: join");
+            }
+            if (e == NRB_OK) e = launch_batch_objective(d_pairs, d_states, L, cap);
+            if (e == NRB_OK && be && cudaStreamWaitEvent(cap, ev_join, 0) != cudaSuccess)
+                e = fail(NRB_ERR_CUDA, "batched level: join");
+            if (e == NRB_OK) e = launch_batch_finalize(d_pairs, d_states, d_ctl, L, h_grad, h_outer, cap);
+            if (e == NRB_OK) e = capture_if(cap, h_grad, &if_body);
+            if (e != NRB_OK) return abort_capture(e);
+        }
+        NRB_CUDA(cudaStreamEndCapture(cap, &while_body));
+        const long long c_line = g_launch_count.load() - c0;
+        // the gradient stage
+        NRB_CUDA(cudaStreamBeginCaptureToGraph(cap, if_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        {
+            nrb_status e = launch_batch_node_stage(hp, d_pairs, d_states, cap, side, ev_fork, ev_join,
+                                                   batch_gradient_voxels, const_cast<BatchLaunch *>(&L));
+            if (e == NRB_OK) {
+                k_b_node_tail<<<TAIL_CTAS * L.npairs, TAIL_THREADS, 0, cap>>>(d_pairs, d_states, L.npairs, d_ctl,
+                                                                            h_outer);
+                g_launch_count.fetch_add(1);
+                if (cudaGetLastError() != cudaSuccess) e = fail(NRB_ERR_CUDA, "batched level: node tail launch");
+            }
+            if (e != NRB_OK) return abort_capture(e);
+        }
+        NRB_CUDA(cudaStreamEndCapture(cap, &if_body));
+        const long long c_grad = g_launch_count.load() - c0 - c_line;
+        g_launch_count.fetch_sub(c_line + c_grad);  // counted per execution below
+        const auto t_inst = std::chrono::steady_clock::now();
+        NRB_CUDA(cudaGraphInstantiate(&top.exec, top.g, 0));
+        const auto t_run = std::chrono::steady_clock::now();
+        NRB_CUDA(cudaGraphLaunch(top.exec, st));
+        NRB_CUDA(cudaStreamSynchronize(st));
+        graph_ms[0] = std::chrono::duration<double, std::milli>(t_run - t_inst).count();
+        graph_ms[1] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_run).count();
+        if (launches) *launches = c_line + c_grad;
+        return NRB_OK;
+    }
+};
+
+}  // namespace
+
+// Registrations of `n` pairs advanced together, level by level, every stage one launch over the
+// pairs that need it. results[i] / cpp_out of pair i equal nrb_f3d_register_host's for pair i
+// alone, bit for bit.
+nrb_status nrb::register_batch_fused(const nrb_pair *pairs, int n, const nrb_f3d_params *p, nrb_f3d_result *results,
+                                cudaStream_t st, int grad_percent) {
+    using Clock = std::chrono::steady_clock;
+    auto ms_since = [](Clock::time_point t) { return std::chrono::duration<double, std::milli>(Clock::now() - t).count(); };
+    const auto t_begin = Clock::now();
+    std::vector<std::unique_ptr<F3dRegistration>> regs;
+    regs.reserve(n);
+    for (int i = 0; i < n; ++i) {
+        regs.emplace_back(new F3dRegistration(*p, st));
+        ImageDesc d;
+        for (int k = 0; k < 3; ++k) {
+            d.dim[k] = pairs[i].dim[k];
+            d.pixdim[k] = pairs[i].pixdim[k];
+        }
+        NRB_TRY(regs[i]->Begin(pairs[i].ref_host, pairs[i].flo_host, d, d));
+    }
+    BatchLevelRunner runner;
+    runner.grad_percent = grad_percent;
+    NRB_TRY(runner.init(st));
+    if (p->verbose) {
+        NRB_CUDA(cudaStreamSynchronize(st));
+        printf("[nrb] batch of %d: pyramids and grids %.2f ms\n", n, ms_since(t_begin));
+    }
+    for (int level = 0; level < p->levels; ++level) {
+        std::vector<BatchPair> hp(n);
+        std::vector<OptState> init(n), out;
+        const auto t_prep = Clock::now();
+        for (int i = 0; i < n; ++i) {
+            float max_step = 0;
+            NRB_TRY(regs[i]->PrepareLevel(level, max_step));
+            NRB_TRY(regs[i]->Describe(max_step, hp[i], init[i]));
+        }
+        if (p->verbose) {
+            NRB_CUDA(cudaStreamSynchronize(st));
+            printf("[nrb] batched level %d set-up %.2f ms\n", level + 1, ms_since(t_prep));
+        }
+        int64_t per_iteration = 0;
+        const auto t_level = std::chrono::steady_clock::now();
+        NRB_TRY(runner.run(hp, init, out, &per_iteration));
+        if (p->verbose) {
+            long long evals = 0;
+            for (int i = 0; i < n; ++i) evals += out[i].n_obj - init[i].n_obj + out[i].n_grad - init[i].n_grad;
+            printf("[nrb] batched level %d: %d pairs, %lld graph iterations, %lld gradient stages, %lld evaluations, "
+                   "%.2f ms (graph instantiation %.2f ms, execution %.2f ms)\n", level + 1, n, runner.stats.iterations,
+                   runner.stats.grad_stages, evals, ms_since(t_level), runner.graph_ms[0], runner.graph_ms[1]);
+        }
+        long long iters = 0;
+        for (int i = 0; i < n; ++i) {
+            iters = std::max(iters, (long long)(out[i].n_obj - init[i].n_obj));
+            NRB_TRY(regs[i]->Absorb(out[i]));
+            regs[i]->EndLevel();
+        }
+        g_launch_count.fetch_add(iters * per_iteration);  // an upper bound: the IF stage may be skipped
+    }
+    const auto t_fin = Clock::now();
+    for (int i = 0; i < n; ++i)
+        NRB_TRY(regs[i]->Finish(pairs[i].flo_host, pairs[i].cpp_out_host, pairs[i].cpp_capacity,
+                                results ? &results[i] : nullptr));
+    if (p->verbose) printf("[nrb] batch of %d: results out %.2f ms, total %.2f ms\n", n, ms_since(t_fin), ms_since(t_begin));
+    return NRB_OK;
 }
 
 extern "C" nrb_status nrb_f3d_register_host(const float *ref_host, const float *flo_host, const int32_t dim[3],

@@ -61,22 +61,12 @@ __device__ double block_sum_d(double v, double *red) {
     return red[0];
 }
 
-// reg_spline_approxBendingEnergyValue3D (reg-lib/cpu/_reg_localTrans_regul.cpp:72-153): per
-// interior node the 6 second derivatives of each component from 27-point stencils of the
-// positions, summed squares (cross terms doubled) accumulated in double. The stencil sums use
-// the reference's order without contraction: each node's terms are bit-identical to the CPU's.
-// grad/step (optional): the positions are the line search's trial values cpp - cur_len * grad
-__global__ void __launch_bounds__(NRB_RED_THREADS)
-k_be_value(int cx, int cy, int cz, const float *__restrict__ cpp, BeBasis B,
-           double *__restrict__ partials, const float *__restrict__ grad, const OptState *__restrict__ step) {
-    __shared__ double red[NRB_RED_THREADS];
-    const float scale = grad ? -step->cur_len : 0.f;
+// the bending-energy value term of interior node n (of ix * iy * iz interior nodes)
+__device__ __forceinline__ double be_node_value(int cx, int cy, int cz, int ix, int iy, const float *__restrict__ cpp,
+                                                const BeBasis& B, const float *__restrict__ grad, float scale,
+                                                long long n) {
     const long long nc = (long long)cx * cy * cz;
-    const int ix = cx - 2, iy = cy - 2, iz = cz - 2;
-    const long long ni = (ix > 0 && iy > 0 && iz > 0) ? (long long)ix * iy * iz : 0;
-    double acc = 0;
-    for (long long n = blockIdx.x * (long long)NRB_RED_THREADS + threadIdx.x; n < ni;
-         n += (long long)gridDim.x * NRB_RED_THREADS) {
+    {
         const int x = 1 + (int)(n % ix);
         const int y = 1 + (int)((n / ix) % iy);
         const int z = 1 + (int)(n / ((long long)ix * iy));
@@ -109,8 +99,26 @@ k_be_value(int cx, int cy, int cz, const float *__restrict__ cpp, BeBasis B,
             s = __dadd_rn(s, (double)sq(d[k][2]));
             s = __dadd_rn(s, __dmul_rn(2.0, (double)sum3(k, 3)));
         }
-        acc += s;
+        return s;
     }
+}
+
+// reg_spline_approxBendingEnergyValue3D (reg-lib/cpu/_reg_localTrans_regul.cpp:72-153): per
+// interior node the 6 second derivatives of each component from 27-point stencils of the
+// positions, summed squares (cross terms doubled) accumulated in double. The stencil sums use
+// the reference's order without contraction: each node's terms are bit-identical to the CPU's.
+// grad/step (optional): the positions are the line search's trial values cpp - cur_len * grad
+__global__ void __launch_bounds__(NRB_RED_THREADS)
+k_be_value(int cx, int cy, int cz, const float *__restrict__ cpp, BeBasis B,
+           double *__restrict__ partials, const float *__restrict__ grad, const OptState *__restrict__ step) {
+    __shared__ double red[NRB_RED_THREADS];
+    const float scale = grad ? -step->cur_len : 0.f;
+    const int ix = cx - 2, iy = cy - 2, iz = cz - 2;
+    const long long ni = (ix > 0 && iy > 0 && iz > 0) ? (long long)ix * iy * iz : 0;
+    double acc = 0;
+    for (long long n = blockIdx.x * (long long)NRB_RED_THREADS + threadIdx.x; n < ni;
+         n += (long long)gridDim.x * NRB_RED_THREADS)
+        acc += be_node_value(cx, cy, cz, ix, iy, cpp, B, grad, scale, n);
     const double tot = block_sum_d(acc, red);
     if (threadIdx.x == 0) partials[blockIdx.x] = tot;
 }
@@ -135,11 +143,10 @@ __device__ __forceinline__ float identity_pos(const Mat34& M, int k, int x, int 
 // reg_spline_approxBendingEnergyGradient3D (reg-lib/cpu/_reg_localTrans_regul.cpp:286-451),
 // first half: the 18 derivative values of every node from zero-padded stencils of the
 // displacements, cross terms doubled. Layout der[(3 * t + k) * nc + node].
-__global__ void k_be_derivatives(int cx, int cy, int cz, Mat34 M, const float *__restrict__ cpp,
-                                 BeBasis B, float *__restrict__ der) {
+__device__ __forceinline__ void be_node_derivatives(int cx, int cy, int cz, const Mat34& M, const float *__restrict__ cpp,
+                                                    const BeBasis& B, float *__restrict__ der, long long n) {
     const long long nc = (long long)cx * cy * cz;
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nc;
-         n += (long long)gridDim.x * blockDim.x) {
+    {
         const int x = (int)(n % cx);
         const int y = (int)((n / cx) % cy);
         const int z = (int)(n / ((long long)cx * cy));
@@ -173,13 +180,20 @@ __global__ void k_be_derivatives(int cx, int cy, int cz, Mat34 M, const float *_
     }
 }
 
-// second half: the same stencils applied to the derivative values of the 27 neighbours,
-// grad += weight / #nodes * sum.
-__global__ void k_be_accumulate(int cx, int cy, int cz, const float *__restrict__ der, BeBasis B,
-                                float ratio, float *__restrict__ grad) {
+__global__ void k_be_derivatives(int cx, int cy, int cz, Mat34 M, const float *__restrict__ cpp,
+                                 BeBasis B, float *__restrict__ der) {
     const long long nc = (long long)cx * cy * cz;
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nc;
-         n += (long long)gridDim.x * blockDim.x) {
+         n += (long long)gridDim.x * blockDim.x)
+        be_node_derivatives(cx, cy, cz, M, cpp, B, der, n);
+}
+
+// second half: the same stencils applied to the derivative values of the 27 neighbours,
+// grad += weight / #nodes * sum.
+__device__ __forceinline__ void be_node_accumulate(int cx, int cy, int cz, const float *__restrict__ der, const BeBasis& B,
+                                                   float ratio, float *__restrict__ grad, long long n) {
+    const long long nc = (long long)cx * cy * cz;
+    {
         const int x = (int)(n % cx);
         const int y = (int)((n / cx) % cy);
         const int z = (int)(n / ((long long)cx * cy));
@@ -198,6 +212,14 @@ __global__ void k_be_accumulate(int cx, int cy, int cz, const float *__restrict_
 #pragma unroll
         for (int k = 0; k < 3; ++k) grad[k * nc + n] = __fadd_rn(grad[k * nc + n], __fmul_rn(ratio, g[k]));
     }
+}
+
+__global__ void k_be_accumulate(int cx, int cy, int cz, const float *__restrict__ der, BeBasis B,
+                                float ratio, float *__restrict__ grad) {
+    const long long nc = (long long)cx * cy * cz;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nc;
+         n += (long long)gridDim.x * blockDim.x)
+        be_node_accumulate(cx, cy, cz, der, B, ratio, grad, n);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -227,14 +249,15 @@ __device__ __forceinline__ float conv_at(int s, int n, int R, const float *__res
 // coalesce and many are in flight per thread), then evaluates the sampled outputs of all of them
 constexpr int CONV_X_ROWS = 8, CONV_X_THREADS = 256;
 
-__global__ void __launch_bounds__(CONV_X_THREADS)
-k_conv_x(int nx, int ny, int nz, const float *__restrict__ vg, const int *__restrict__ samples, int ns,
-         const float *__restrict__ K, int R, float *__restrict__ out) {
-    extern __shared__ float rows[];  // [3][CONV_X_ROWS][nx] | kernel taps [2R + 1]
+// rows [rb * CONV_X_ROWS, ...) of the x pass; `rows` is the block's shared memory
+// ([3][CONV_X_ROWS][nx] | kernel taps [2R + 1]); ends with every output of those rows written
+__device__ __forceinline__ void conv_x_rows(int nx, int ny, int nz, const float *__restrict__ vg,
+                                            const int *__restrict__ samples, int ns, const float *__restrict__ K,
+                                            int R, float *__restrict__ out, long long rb, float *rows) {
     float *Ks = rows + 3 * CONV_X_ROWS * nx;
     const long long nv = (long long)nx * ny * nz;
     const long long nrow = (long long)ny * nz;
-    const long long r0 = (long long)blockIdx.x * CONV_X_ROWS;
+    const long long r0 = rb * CONV_X_ROWS;
     const int nr = (int)min((long long)CONV_X_ROWS, nrow - r0);
     const int run = nr * nx;
     int nan = 0;
@@ -275,14 +298,19 @@ k_conv_x(int nx, int ny, int nz, const float *__restrict__ vg, const int *__rest
     }
 }
 
+__global__ void __launch_bounds__(CONV_X_THREADS)
+k_conv_x(int nx, int ny, int nz, const float *__restrict__ vg, const int *__restrict__ samples, int ns,
+         const float *__restrict__ K, int R, float *__restrict__ out) {
+    extern __shared__ float rows[];
+    conv_x_rows(nx, ny, nz, vg, samples, ns, K, R, out, blockIdx.x, rows);
+}
+
 // pass along an outer axis of a [3][outer][len][inner] array at sampled positions of `len`:
 // out[3][outer][ns][inner]
-__global__ void k_conv_strided(int outer, int len, int inner, const float *__restrict__ in,
-                               const int *__restrict__ samples, int ns, const float *__restrict__ K,
-                               int R, float *__restrict__ out) {
-    const long long total = 3LL * outer * ns * inner;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
+__device__ __forceinline__ void conv_strided_at(int outer, int len, int inner, const float *__restrict__ in,
+                                                const int *__restrict__ samples, int ns, const float *__restrict__ K,
+                                                int R, float *__restrict__ out, long long i) {
+    {
         const int ii = (int)(i % inner);
         long long rest = i / inner;
         const int j = (int)(rest % ns);
@@ -294,19 +322,27 @@ __global__ void k_conv_strided(int outer, int len, int inner, const float *__res
     }
 }
 
+__global__ void k_conv_strided(int outer, int len, int inner, const float *__restrict__ in,
+                               const int *__restrict__ samples, int ns, const float *__restrict__ K,
+                               int R, float *__restrict__ out) {
+    const long long total = 3LL * outer * ns * inner;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x)
+        conv_strided_at(outer, len, inner, in, samples, ns, K, R, out, i);
+}
+
 // reg_voxelCentricToNodeCentric (reg-lib/cpu/_reg_localTrans.cpp:1616-1683): trilinear sample
 // of the convolved gradient (taps outside the volume skipped), reorientation by the transpose
 // of the floating ijk 3x3, weighting; overwrites the node gradient.
-__global__ void k_nodes(int cx, int cy, int cz, int nsx, int nsy, int nsz,
-                        const float *__restrict__ conv, const int *__restrict__ tsx,
-                        const float *__restrict__ wsx, const int *__restrict__ tsy,
-                        const float *__restrict__ wsy, const int *__restrict__ tsz,
-                        const float *__restrict__ wsz, Mat34 R, float weight,
-                        float *__restrict__ node) {
+__device__ __forceinline__ void node_at(int cx, int cy, int cz, int nsx, int nsy, int nsz,
+                                        const float *__restrict__ conv, const int *__restrict__ tsx,
+                                        const float *__restrict__ wsx, const int *__restrict__ tsy,
+                                        const float *__restrict__ wsy, const int *__restrict__ tsz,
+                                        const float *__restrict__ wsz, const Mat34& R, float weight,
+                                        float *__restrict__ node, long long n) {
     const long long nc = (long long)cx * cy * cz;
     const long long cs = (long long)nsz * nsy * nsx;
-    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nc;
-         n += (long long)gridDim.x * blockDim.x) {
+    {
         const int x = (int)(n % cx);
         const int y = (int)((n / cx) % cy);
         const int z = (int)(n / ((long long)cx * cy));
@@ -336,6 +372,146 @@ __global__ void k_nodes(int cx, int cy, int cz, int nsx, int nsy, int nsz,
             node[d * nc + n] = ro * weight;
         }
     }
+}
+
+__global__ void k_nodes(int cx, int cy, int cz, int nsx, int nsy, int nsz,
+                        const float *__restrict__ conv, const int *__restrict__ tsx,
+                        const float *__restrict__ wsx, const int *__restrict__ tsy,
+                        const float *__restrict__ wsy, const int *__restrict__ tsz,
+                        const float *__restrict__ wsz, Mat34 R, float weight,
+                        float *__restrict__ node) {
+    const long long nc = (long long)cx * cy * cz;
+    for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nc;
+         n += (long long)gridDim.x * blockDim.x)
+        node_at(cx, cy, cz, nsx, nsy, nsz, conv, tsx, wsx, tsy, wsy, tsz, wsz, R, weight, node, n);
+}
+
+// ---------------------------------------------------------------------------------------------
+// batched levels: the node-grid and node-convolution stages of every pair that needs them, with
+// each pair's elements computed exactly as the plain kernels compute them
+// ---------------------------------------------------------------------------------------------
+// bending-energy value partials of every pair in INIT or LINE: work unit = one block of the plain
+// k_be_value (same node range, same shared-memory tree), persistent blocks of NRB_RED_THREADS
+__global__ void __launch_bounds__(NRB_RED_THREADS)
+k_b_be_value(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs, BeBasis B) {
+    __shared__ BatchList L;
+    __shared__ double red[NRB_RED_THREADS];
+    batch_list_build(pairs, states, npairs, (1u << PH_INIT) | (1u << PH_LINE),
+                     [](const BatchPair& b, int& u, int& w) {
+                         u = b.be_w > 0 ? b.n_be : 0;
+                         w = 1;
+                     }, L);
+    int k = 0;
+    for (long long u = blockIdx.x; u < L.total; u += gridDim.x) {
+        while (L.pref[k + 1] <= u) ++k;
+        const int p = L.pair[k], v = (int)(u - L.pref[k]);
+        const BatchPair& P = pairs[p];
+        const bool line = states[p].phase == PH_LINE;
+        const float *grad = line ? P.grad : nullptr;
+        const float scale = line ? -states[p].cur_len : 0.f;
+        const int cx = P.cdim[0], cy = P.cdim[1], cz = P.cdim[2];
+        const int ix = cx - 2, iy = cy - 2, iz = cz - 2;
+        const long long ni = (ix > 0 && iy > 0 && iz > 0) ? (long long)ix * iy * iz : 0;
+        double acc = 0;
+        for (long long n = (long long)v * NRB_RED_THREADS + threadIdx.x; n < ni; n += (long long)P.n_be * NRB_RED_THREADS)
+            acc += be_node_value(cx, cy, cz, ix, iy, P.best, B, grad, scale, n);
+        const double tot = block_sum_d(acc, red);
+        if (threadIdx.x == 0) P.be_partials[v] = tot;
+        __syncthreads();  // red is reused by the next unit
+    }
+}
+
+__global__ void k_b_be_derivatives(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states,
+                                   int npairs, BeBasis B) {
+    __shared__ BatchList L;
+    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
+                     [](const BatchPair& b, int& u, int& w) {
+                         u = b.be_w > 0 ? (int)b.nnode : 0;
+                         w = 1;
+                     }, L);
+    batch_elements(L, [&](int p, long long n) {
+        const BatchPair& P = pairs[p];
+        be_node_derivatives(P.cdim[0], P.cdim[1], P.cdim[2], P.grid_xyz, P.best, B, P.be_der, n);
+    });
+}
+
+__global__ void k_b_be_accumulate(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states,
+                                  int npairs, BeBasis B) {
+    __shared__ BatchList L;
+    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
+                     [](const BatchPair& b, int& u, int& w) {
+                         u = b.be_w > 0 ? (int)b.nnode : 0;
+                         w = 1;
+                     }, L);
+    batch_elements(L, [&](int p, long long n) {
+        const BatchPair& P = pairs[p];
+        be_node_accumulate(P.cdim[0], P.cdim[1], P.cdim[2], P.be_der, B, P.be_ratio, P.grad, n);
+    });
+}
+
+// x pass of the node convolution: work unit = one block of the plain k_conv_x
+__global__ void __launch_bounds__(CONV_X_THREADS)
+k_b_conv_x(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
+    extern __shared__ float rows[];
+    __shared__ BatchList L;
+    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
+                     [](const BatchPair& b, int& u, int& w) {
+                         u = b.xblocks;
+                         w = 1;
+                     }, L);
+    int k = 0;
+    for (long long u = blockIdx.x; u < L.total; u += gridDim.x) {
+        while (L.pref[k + 1] <= u) ++k;
+        const BatchPair& P = pairs[L.pair[k]];
+        conv_x_rows(P.rdim[0], P.rdim[1], P.rdim[2], P.vgrad, P.samples[0], P.ns[0], P.kernel[0], P.radius[0], P.conv1,
+                    u - L.pref[k], rows);
+        __syncthreads();  // rows are reused by the next unit
+    }
+}
+
+// y pass ([3][nz][ny][nsx] -> [3][nz][nsy][nsx]) and z pass ([3][nz][nsy * nsx] ->
+// [3][nsz][nsy * nsx]) of the node convolution, element-wise
+__global__ void k_b_conv_y(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
+    __shared__ BatchList L;
+    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
+                     [](const BatchPair& b, int& u, int& w) {
+                         u = 3 * b.rdim[2] * b.ns[1] * b.ns[0];
+                         w = 1;
+                     }, L);
+    batch_elements(L, [&](int p, long long i) {
+        const BatchPair& P = pairs[p];
+        conv_strided_at(P.rdim[2], P.rdim[1], P.ns[0], P.conv1, P.samples[1], P.ns[1], P.kernel[1], P.radius[1],
+                        P.conv2, i);
+    });
+}
+
+__global__ void k_b_conv_z(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
+    __shared__ BatchList L;
+    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
+                     [](const BatchPair& b, int& u, int& w) {
+                         u = 3 * b.ns[2] * b.ns[1] * b.ns[0];
+                         w = 1;
+                     }, L);
+    batch_elements(L, [&](int p, long long i) {
+        const BatchPair& P = pairs[p];
+        conv_strided_at(1, P.rdim[2], P.ns[1] * P.ns[0], P.conv2, P.samples[2], P.ns[2], P.kernel[2], P.radius[2],
+                        P.conv1, i);
+    });
+}
+
+// node sampling, reorientation and weighting (overwrites the node gradient)
+__global__ void k_b_nodes(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
+    __shared__ BatchList L;
+    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
+                     [](const BatchPair& b, int& u, int& w) {
+                         u = (int)b.nnode;
+                         w = 1;
+                     }, L);
+    batch_elements(L, [&](int p, long long n) {
+        const BatchPair& P = pairs[p];
+        node_at(P.cdim[0], P.cdim[1], P.cdim[2], P.ns[0], P.ns[1], P.ns[2], P.conv1, P.tap_slot[0], P.tap_weight[0],
+                P.tap_slot[1], P.tap_weight[1], P.tap_slot[2], P.tap_weight[2], P.flo_ijk, P.node_weight, P.grad, n);
+    });
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1218,6 +1394,114 @@ nrb_status launch_be_accumulate(nrb_workspace *ws, const nrb_geometry *g, float 
     k_be_accumulate<<<grid_for(nc, 128), 128, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2], ws->be_deriv,
                                                        be_basis(), ratio, node_grad);
     NRB_LAUNCHED("k_be_accumulate");
+    return NRB_OK;
+}
+
+// ---- batched levels -------------------------------------------------------------------------
+// A pair's node-stage description: its workspace's convolution sampling and bending-energy
+// buffers, as launch_convolve_to_nodes / launch_be_* use them for its geometry.
+nrb_status batch_node_stage(const nrb_workspace *ws, const nrb_geometry *g, float sim_weight, float be_weight,
+                            BatchPair& b) {
+    if (ws->general) return fail(NRB_ERR_UNSUPPORTED, "batched level: the grid must be aligned with the reference");
+    for (int i = 0; i < 3; ++i) {
+        b.rdim[i] = g->ref_dim[i];
+        b.cdim[i] = g->cpp_dim[i];
+        b.ns[i] = ws->ax[i].nsamples;
+        b.radius[i] = ws->ax[i].radius;
+        b.samples[i] = ws->d_samples[i];
+        b.tap_slot[i] = ws->d_tap_slot[i];
+        b.tap_weight[i] = ws->d_tap_weight[i];
+        b.kernel[i] = ws->d_kernel[i];
+    }
+    b.nnode = nvox(g->cpp_dim);
+    b.conv1 = ws->conv1;
+    b.conv2 = ws->conv2;
+    float w = sim_weight;
+    for (int i = 0; i < 3; ++i) w *= g->cpp_pixdim[i] / g->ref_pixdim[i];
+    b.node_weight = w;
+    b.flo_ijk = to_mat34(g->flo_ijk);
+    b.grid_xyz = to_mat34(g->cpp_xyz);
+    b.be_partials = ws->be_partials;
+    b.n_be = be_grid(g);
+    b.be_norm = 3.0 * (double)b.nnode;
+    b.be_der = ws->be_deriv;
+    b.be_ratio = be_weight / (float)b.nnode;
+    b.red = ws->red;
+    b.xblocks = (int)(((long long)g->ref_dim[1] * g->ref_dim[2] + CONV_X_ROWS - 1) / CONV_X_ROWS);
+    return NRB_OK;
+}
+
+static int batch_grid(const std::vector<BatchPair>& pairs, long long (*units)(const BatchPair&), int threads,
+                      int max_per_sm) {
+    long long total = 0;
+    for (const BatchPair& b : pairs) total += units(b);
+    return grid_for(std::max(1LL, total), threads, max_per_sm);
+}
+
+nrb_status launch_batch_be_value(const std::vector<BatchPair>& hp, const BatchPair *d, const OptState *states,
+                                 cudaStream_t st) {
+    long long units = 0;
+    for (const BatchPair& b : hp) units += b.n_be;
+    const int grid = (int)std::max(1LL, std::min(units, 8LL * sm_count()));
+    k_b_be_value<<<grid, NRB_RED_THREADS, 0, st>>>(d, states, (int)hp.size(), be_basis());
+    NRB_CUDA(cudaGetLastError());
+    NRB_LAUNCHED("k_b_be_value");
+    return NRB_OK;
+}
+
+nrb_status launch_batch_node_stage(const std::vector<BatchPair>& hp, const BatchPair *d, const OptState *states,
+                                   cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join,
+                                   nrb_status (*gradient)(const BatchPair *, const OptState *, cudaStream_t, void *),
+                                   void *gradient_arg) {
+    const int np = (int)hp.size();
+    const bool be = hp[0].be_w > 0;
+    // bending-energy derivatives on the side branch, beside the voxel passes (they read best only)
+    if (be) {
+        NRB_CUDA(cudaEventRecord(fork, st));
+        NRB_CUDA(cudaStreamWaitEvent(side, fork, 0));
+        const int g = batch_grid(hp, [](const BatchPair& b) { return b.nnode; }, 128, 16);
+        k_b_be_derivatives<<<g, 128, 0, side>>>(d, states, np, be_basis());
+        NRB_CUDA(cudaGetLastError());
+        NRB_LAUNCHED("k_b_be_derivatives");
+    }
+    NRB_TRY(gradient(d, states, st, gradient_arg));
+    // x pass: shared rows for the widest reference
+    int nx = 0, R = 0;
+    long long xb = 0;
+    for (const BatchPair& b : hp) {
+        nx = std::max(nx, b.rdim[0]);
+        R = std::max(R, b.radius[0]);
+        xb += b.xblocks;
+    }
+    const size_t smem = ((size_t)3 * CONV_X_ROWS * nx + 2 * R + 1) * 4;
+    if (smem > 227 * 1024) return fail(NRB_ERR_UNSUPPORTED, "convolution: rows and kernel exceed shared memory");
+    NRB_CUDA(cudaFuncSetAttribute(k_b_conv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per = 0;
+    NRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_b_conv_x, CONV_X_THREADS, smem));
+    const int xg = (int)std::max(1LL, std::min(xb, (long long)std::max(1, per) * sm_count()));
+    k_b_conv_x<<<xg, CONV_X_THREADS, smem, st>>>(d, states, np);
+    NRB_CUDA(cudaGetLastError());
+    NRB_LAUNCHED("k_b_conv_x");
+    const int gy = batch_grid(hp, [](const BatchPair& b) { return 3LL * b.rdim[2] * b.ns[1] * b.ns[0]; }, 256, 16);
+    k_b_conv_y<<<gy, 256, 0, st>>>(d, states, np);
+    NRB_CUDA(cudaGetLastError());
+    NRB_LAUNCHED("k_b_conv_y");
+    const int gz = batch_grid(hp, [](const BatchPair& b) { return 3LL * b.ns[2] * b.ns[1] * b.ns[0]; }, 256, 16);
+    k_b_conv_z<<<gz, 256, 0, st>>>(d, states, np);
+    NRB_CUDA(cudaGetLastError());
+    NRB_LAUNCHED("k_b_conv_z");
+    const int gn = batch_grid(hp, [](const BatchPair& b) { return b.nnode; }, 256, 16);
+    k_b_nodes<<<gn, 256, 0, st>>>(d, states, np);
+    NRB_CUDA(cudaGetLastError());
+    NRB_LAUNCHED("k_b_nodes");
+    if (be) {
+        NRB_CUDA(cudaEventRecord(join, side));
+        NRB_CUDA(cudaStreamWaitEvent(st, join, 0));
+        const int g = batch_grid(hp, [](const BatchPair& b) { return b.nnode; }, 128, 16);
+        k_b_be_accumulate<<<g, 128, 0, st>>>(d, states, np, be_basis());
+        NRB_CUDA(cudaGetLastError());
+        NRB_LAUNCHED("k_b_be_accumulate");
+    }
     return NRB_OK;
 }
 }  // namespace nrb

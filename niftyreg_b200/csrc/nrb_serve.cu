@@ -267,27 +267,43 @@ extern "C" nrb_status nrb_f3d_register_batch(const nrb_pair *pairs, int n, const
                                              int64_t hbm_budget_bytes, nrb_f3d_result *results) {
     if (!pairs || n < 0 || !p) return fail(NRB_ERR_INVALID, "nrb_f3d_register_batch: bad argument");
     if (n == 0) return NRB_OK;
-    nrb_server *s = nullptr;
-    NRB_TRY(nrb_server_create(std::max(1, std::min(concurrency, n)), hbm_budget_bytes, &s));
-    std::vector<int64_t> tickets(n, 0);
-    nrb_status first = NRB_OK;
-    std::string first_err;
     for (int i = 0; i < n; ++i) {
-        const nrb_status st = nrb_server_submit(s, &pairs[i], p, &tickets[i]);
-        if (st != NRB_OK && first == NRB_OK) {
-            first = st;
-            first_err = nrb_last_error();
-        }
+        if (!pairs[i].ref_host || !pairs[i].flo_host) return fail(NRB_ERR_INVALID, "nrb_f3d_register_batch: null image");
+        for (int k = 0; k < 3; ++k)
+            if (pairs[i].dim[k] < 2 || !(pairs[i].pixdim[k] > 0))
+                return fail(NRB_ERR_INVALID, "nrb_f3d_register_batch: 3D volumes with positive voxel size expected");
     }
-    for (int i = 0; i < n; ++i) {
-        if (!tickets[i]) continue;
-        const nrb_status st = nrb_server_wait(s, tickets[i], results ? &results[i] : nullptr, nullptr, nullptr);
-        if (st != NRB_OK && first == NRB_OK) {
-            first = st;
-            first_err = nrb_last_error();
-        }
+    const int pct = p->batch_gradient_percent;
+    if (pct < 1 || pct > 100) return fail(NRB_ERR_INVALID, "nrb_f3d_register_batch: batch_gradient_percent in [1, 100]");
+    const int group_max = std::max(1, std::min(concurrency > 0 ? concurrency : BATCH_MAX_PAIRS, BATCH_MAX_PAIRS));
+    int64_t budget = hbm_budget_bytes;
+    if (budget <= 0) {
+        size_t free_b = 0, total_b = 0;
+        NRB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        budget = (int64_t)(0.8 * (double)free_b);
     }
-    nrb_server_destroy(s);
-    if (first != NRB_OK) return fail(first, first_err.c_str());
-    return NRB_OK;
+    cudaStream_t st = nullptr;
+    NRB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    nrb_status s = NRB_OK;
+    for (int i0 = 0; i0 < n && s == NRB_OK;) {
+        // the next group: pairs in order while they fit in the budget (a pair larger than the
+        // budget alone is refused)
+        int64_t used = 0;
+        int i1 = i0;
+        while (i1 < n && i1 - i0 < group_max) {
+            const int64_t f = registration_footprint(pairs[i1].dim, pairs[i1].pixdim, p);
+            if (used + f > budget) break;
+            used += f;
+            ++i1;
+        }
+        if (i1 == i0) {
+            s = fail(NRB_ERR_OOM, "nrb_f3d_register_batch: a pair is larger than the HBM budget");
+            break;
+        }
+        s = register_batch_fused(pairs + i0, i1 - i0, p, results ? results + i0 : nullptr, st, pct);
+        i0 = i1;
+    }
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    return s;
 }

@@ -21,6 +21,28 @@ namespace nrb {
 constexpr int COL_X = 32;
 constexpr int TY_OBJECTIVE = 16, TY_GRADIENT = 4, TY_DEFORMATION = 4;
 
+// Launch-time description of one voxel walk (a pair's reference volume, grid and floating image,
+// and the walk plan's item decomposition).
+struct WalkParams {
+    int nx, ny, nz;          // reference / deformation-field dims
+    int cx, cy, cz;          // control-point grid dims
+    float gsx, gsy, gsz;     // grid spacing in reference voxels (grid pixdim / ref pixdim)
+    int ty, tiles_x, tiles_y, zchunk, nitems;
+    int sa, sb, sc;          // shared strides of the staged block (max spans)
+    int fnx, fny, fnz;       // floating dims
+    int fsy, fsz, fmargin;   // floating layout: row and slice strides, margin (sample_floating)
+    Mat34 flo_ijk;           // mm -> floating voxel
+    int flo_diag;            // flo_ijk has no off-diagonal terms
+    float pad;               // padding value of out-of-volume taps
+    int rb, fb;              // internal bin counts
+    int cnv;                 // control points per component
+    int log_in_smem;         // gradient: an FP32 copy of the log table is staged in shared memory
+    int xs;                  // objective: x-contracted rows of the item staged in shared memory
+    // identity split of the positions (grid matrix without off-diagonal terms; zero otherwise):
+    // node k of axis c sits at io[c] + is[c] * k mm when the transformation is the identity
+    float io[3], is[3];
+};
+
 // State of the device-resident optimiser (ConjugateGradient::Optimise and the level loop of
 // reg_base::Run) that the control kernels of a level's CUDA graph advance.
 struct OptState {
@@ -32,6 +54,216 @@ struct OptState {
     float added_len;
     int line_iter, first_call, just_restarted, accepted;
     int best_buf;    // NMI table set (0: pro/logt/last, 1: pro2/logt2/last2) of the best position
+    int phase;       // batched levels: what the pair needs next (BatchPhase)
+};
+
+// Loop conditions of reg_base::Run's level loop and Optimiser::Optimise's line search
+// (reg-lib/_reg_base.cpp:760-794, reg-lib/Optimiser.cpp:140-168).
+__device__ __forceinline__ bool outer_continues(const OptState& s) { return s.current_size != 0.f && s.it < s.max_it; }
+__device__ __forceinline__ bool line_continues(const OptState& s) {
+    return s.cur_len > s.small_step && s.line_iter < 12 && s.it < s.max_it;
+}
+
+// End of Optimise (start length = added length) and the restart rule of _reg_base.cpp:784-793;
+// returns whether the level goes on
+__device__ __forceinline__ bool line_end(OptState *s) {
+    s->current_size = s->added_len;
+    if (s->current_size == 0.f) {
+        if (!s->just_restarted && s->it < s->max_it) {
+            s->first_call = 1;
+            s->current_size = s->max_step;
+            s->just_restarted = 1;
+        }
+    } else {
+        s->just_restarted = 0;
+    }
+    return outer_continues(*s);
+}
+
+// Start of Optimise after a gradient evaluation: iteration counted, current_size =
+// min(current_size, max_step), first_call consumed, line search set up; returns whether the line
+// search runs at all
+__device__ __forceinline__ bool gradient_done_line_start(OptState *s) {
+    s->it += 1;
+    s->n_grad += 1;
+    s->current_size = s->max_step < s->current_size ? s->max_step : s->current_size;
+    s->first_call = 0;
+    s->line_iter = 0;
+    s->added_len = 0.f;
+    s->cur_len = s->current_size;
+    return line_continues(*s);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched levels: many registrations advanced together, one launch per stage over every pair
+// that needs that stage. A pair's phase says what it needs next.
+// ---------------------------------------------------------------------------------------------
+enum BatchPhase : int {
+    PH_DONE = 0,  // the level is over for this pair
+    PH_INIT = 1,  // the objective at the level's starting point (ConjugateGradient::Initialise)
+    PH_LINE = 2,  // a line-search step: the objective at best - cur_len * grad
+    PH_GRAD = 3,  // a gradient evaluation at best, then the conjugate-gradient direction
+};
+
+// Everything the batched kernels need of one pair at the current level (device array, one per
+// pair). Pointers are the pair's own buffers; walks and tables are those its plain
+// registration would use, so each pair's arithmetic is the same whatever else is in the batch.
+struct BatchPair {
+    WalkParams wo, wg;               // objective and gradient walks
+    const float *ref, *flo;          // rescaled reference; floating voxel (0, 0, 0) (margin in wo/wg)
+    float *best, *grad, *g1, *g2, *vgrad;
+    uint32_t *hist;                  // joint counts (zero between evaluations)
+    double *pro0, *logt0, *pro1, *logt1;
+    nrb_objective *last0, *last1, *obj;
+    int rb, fb;
+    double *be_partials;
+    int n_be;                        // bending-energy partials (blocks of the plain k_be_value)
+    double be_norm;                  // 3 * nodes
+    float *be_der;                   // 18 derivative values per node
+    float be_ratio;                  // bending-energy weight / nodes
+    Mat34 grid_xyz;                  // node -> mm (identity positions of k_be_derivatives)
+    int rdim[3], cdim[3];
+    long long nnode;
+    double *red;                     // node-tail partials (2 * NRB_RED_BLOCKS doubles)
+    // convolution to the nodes (the aligned-grid passes of launch_convolve_to_nodes)
+    int ns[3], radius[3];
+    const int *samples[3], *tap_slot[3];
+    const float *tap_weight[3], *kernel[3];
+    float *conv1, *conv2;
+    float node_weight;               // similarity weight x grid/voxel spacing ratios
+    Mat34 flo_ijk;                   // reorientation of the node gradient
+    double sim_w, be_w;
+    OptState *st;
+    int obj_items, grad_items, xblocks;
+};
+
+constexpr int BATCH_MAX_PAIRS = 128;
+
+// Launch shapes of a batched level, derived on the host from every pair (shared memory for the
+// largest walk, template choices every pair allows).
+struct BatchLaunch {
+    int npairs = 0;
+    bool obj_xs = false, obj_diag = false, grad_f32 = false, grad_diag = false;
+    size_t obj_smem = 0, grad_smem = 0, fin_smem = 0;
+    int obj_grid = 0, grad_grid = 0;
+};
+
+// The pairs a batched stage serves (their phase is in `mask`) with the cost of their work units,
+// built by warp 0 of every block from the pairs' device state (each block builds the same list)
+// and laid out as cost prefix sums. A block then takes the units whose start cost falls in its
+// equal share of the total, in pair order, so each block touches few pairs and the shares are
+// balanced when units of different pairs cost differently.
+struct BatchList {
+    int n;                           // pairs served
+    long long total;                 // their summed cost
+    int pair[BATCH_MAX_PAIRS];       // pair index
+    int units[BATCH_MAX_PAIRS];      // work units of the pair
+    int w[BATCH_MAX_PAIRS];          // cost of one unit
+    long long pref[BATCH_MAX_PAIRS + 1];
+};
+
+template <typename F>
+__device__ __forceinline__ void batch_list_build(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states,
+                                                 int npairs, unsigned mask, F units_of, BatchList& L) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int n = 0;
+        long long total = 0;
+        for (int base = 0; base < npairs; base += 32) {
+            const int p = base + lane;
+            int u = 0, w = 0;
+            if (p < npairs && ((mask >> states[p].phase) & 1u)) units_of(pairs[p], u, w);
+            const long long c = (long long)u * w;
+            long long inc = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long v = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += v;
+            }
+            const unsigned act = __ballot_sync(0xffffffffu, u > 0);
+            if (u > 0) {
+                const int slot = n + __popc(act & ((1u << lane) - 1u));
+                L.pair[slot] = p;
+                L.units[slot] = u;
+                L.w[slot] = w;
+                L.pref[slot] = total + inc - c;
+            }
+            total += __shfl_sync(0xffffffffu, inc, 31);
+            n += __popc(act);
+        }
+        if (lane == 0) {
+            L.n = n;
+            L.total = total;
+            L.pref[n] = total;
+        }
+    }
+    __syncthreads();
+}
+
+// units [j0, j1) of active pair k that start in the cost range [c0, c1)
+__device__ __forceinline__ bool batch_units(const BatchList& L, int k, long long c0, long long c1, int& j0, int& j1) {
+    const long long a = L.pref[k], b = L.pref[k + 1], w = L.w[k];
+    if (b <= c0 || a >= c1) return false;
+    j0 = c0 > a ? (int)((c0 - a + w - 1) / w) : 0;
+    j1 = (int)min((long long)L.units[k], (c1 - a + w - 1) / w);
+    return j0 < j1;
+}
+
+__device__ __forceinline__ void copy_words(void *dst, const void *src, int bytes) {
+    for (int i = threadIdx.x; i < bytes / 4; i += blockDim.x)
+        static_cast<int *>(dst)[i] = static_cast<const int *>(src)[i];
+}
+
+// The same list walked element-wise: every element of every served pair, grid-stride per pair
+template <typename F>
+__device__ __forceinline__ void batch_elements(const BatchList& L, F work) {
+    const long long gtid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long gs = (long long)gridDim.x * blockDim.x;
+    for (int k = 0; k < L.n; ++k)
+        for (long long i = gtid; i < L.units[k]; i += gs) work(L.pair[k], i);
+}
+
+// Counts of the pairs' phases, by the block that took the last ticket of a per-pair cluster
+// launch; that block sets the graph's conditions for the rest of the iteration.
+__device__ __forceinline__ void batch_counts(const OptState *states, int npairs, int& nline, int& ngrad) {
+    __shared__ int s_line, s_grad;
+    if (threadIdx.x == 0) s_line = s_grad = 0;
+    __syncthreads();
+    int l = 0, g = 0;
+    for (int q = threadIdx.x; q < npairs; q += blockDim.x) {
+        const int ph = *reinterpret_cast<const volatile int *>(&states[q].phase);
+        l += ph == PH_LINE || ph == PH_INIT;
+        g += ph == PH_GRAD;
+    }
+    if (l) atomicAdd(&s_line, l);
+    if (g) atomicAdd(&s_grad, g);
+    __syncthreads();
+    nline = s_line;
+    ngrad = s_grad;
+}
+
+// Takes the cluster's ticket (block rank 0 of each cluster, every thread of that block); true
+// in the block that took the last one, after which every pair's state is visible.
+__device__ __forceinline__ bool batch_last_cluster(unsigned int *ticket, unsigned int nclusters) {
+    __shared__ unsigned int s_last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(ticket, 1u) == nclusters - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        if (threadIdx.x == 0) *ticket = 0u;
+    }
+    return s_last != 0;
+}
+
+// Tickets of the per-pair cluster kernels: the last cluster to finish sets the graph's
+// conditions from every pair's phase.
+struct BatchCtl {
+    unsigned int ticket_fin, ticket_tail;
+    int grad_percent;                // run the gradient stage once this share (%) of the active pairs waits for it
+    long long iterations, grad_stages;  // graph iterations and gradient stages run (statistics)
 };
 
 // One line-search step of Optimiser::Optimise (reg-lib/Optimiser.cpp:140-168) after its
@@ -198,6 +430,32 @@ nrb_status launch_be_derivatives(nrb_workspace *ws, const nrb_geometry *g, const
 nrb_status launch_be_accumulate(nrb_workspace *ws, const nrb_geometry *g, float weight, float *node_grad,
                                 cudaStream_t st);
 int be_partial_count(const nrb_geometry *g);
+// batched levels (csrc/nrb_tile.cu): a pair's walks as its plain registration would launch them
+nrb_status batch_walks(nrb_workspace *ws, const nrb_nmi *nmi, const nrb_geometry *g, float padding, int flo_margin,
+                       WalkParams& wo, WalkParams& wg);
+nrb_status batch_plan(std::vector<BatchPair>& pairs, BatchLaunch& L);
+nrb_status launch_batch_objective(const BatchPair *d_pairs, const OptState *states, const BatchLaunch& L,
+                                  cudaStream_t st);
+nrb_status launch_batch_gradient(const BatchPair *d_pairs, const OptState *states, const BatchLaunch& L,
+                                 cudaStream_t st);
+nrb_status launch_batch_finalize(const BatchPair *d_pairs, OptState *states, BatchCtl *bctl, const BatchLaunch& L,
+                                 cudaGraphConditionalHandle grad_if, cudaGraphConditionalHandle outer,
+                                 cudaStream_t st);
+// batched levels (csrc/nrb_ops.cu): a pair's node-stage description from its workspace, the
+// bending-energy value partials of the pairs in INIT / LINE, and the gradient stage of the pairs in
+// GRAD around the voxel pass `gradient` (bending-energy derivatives on `side`, the node
+// convolution, the bending-energy gradient)
+nrb_status batch_node_stage(const nrb_workspace *ws, const nrb_geometry *g, float sim_weight, float be_weight,
+                            BatchPair& b);
+nrb_status launch_batch_be_value(const std::vector<BatchPair>& hp, const BatchPair *d, const OptState *states,
+                                 cudaStream_t st);
+nrb_status launch_batch_node_stage(const std::vector<BatchPair>& hp, const BatchPair *d, const OptState *states,
+                                   cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join,
+                                   nrb_status (*gradient)(const BatchPair *, const OptState *, cudaStream_t, void *),
+                                   void *gradient_arg);
+// batched registrations (csrc/nrb_f3d.cu): n pairs advanced together level by level on `st`
+nrb_status register_batch_fused(const nrb_pair *pairs, int n, const nrb_f3d_params *p, nrb_f3d_result *results,
+                                cudaStream_t st, int grad_percent);
 // side stream of `ws` starts after the work queued so far on st / st waits for the side stream
 nrb_status fork_side(nrb_workspace *ws, cudaStream_t st);
 nrb_status join_side(nrb_workspace *ws, cudaStream_t st);

@@ -26,26 +26,6 @@ namespace cg = cooperative_groups;
 
 namespace nrb {
 
-struct WalkParams {
-    int nx, ny, nz;          // reference / deformation-field dims
-    int cx, cy, cz;          // control-point grid dims
-    float gsx, gsy, gsz;     // grid spacing in reference voxels (grid pixdim / ref pixdim)
-    int ty, tiles_x, tiles_y, zchunk, nitems;
-    int sa, sb, sc;          // shared strides of the staged block (max spans)
-    int fnx, fny, fnz;       // floating dims
-    int fsy, fsz, fmargin;   // floating layout: row and slice strides, margin (sample_floating)
-    Mat34 flo_ijk;           // mm -> floating voxel
-    int flo_diag;            // flo_ijk has no off-diagonal terms
-    float pad;               // padding value of out-of-volume taps
-    int rb, fb;              // internal bin counts
-    int cnv;                 // control points per component
-    int log_in_smem;         // gradient: an FP32 copy of the log table is staged in shared memory
-    int xs;                  // objective: x-contracted rows of the item staged in shared memory
-    // identity split of the positions (grid matrix without off-diagonal terms; zero otherwise):
-    // node k of axis c sits at io[c] + is[c] * k mm when the transformation is the identity
-    float io[3], is[3];
-};
-
 __device__ __forceinline__ int pre_of(int v, float gs) { return (int)((float)v / gs); }
 
 __device__ __forceinline__ float frac_of(int v, float gs, int pre) {
@@ -414,70 +394,15 @@ size_t walk_smem_bytes(const WalkPlan& W) {
 // ---------------------------------------------------------------------------------------------
 // fused objective: deformation + warp + joint histogram
 // ---------------------------------------------------------------------------------------------
-// kXs: the item's x-contracted node rows are staged in shared memory; kDiag: the floating
-// image's mm -> voxel matrix has no off-diagonal terms (launch-time choices made template
-// parameters, so the walk carries no test for them)
-template <bool kTrial, bool kXs, bool kDiag>
-__global__ void __launch_bounds__(32 * TY_OBJECTIVE, 2)
-k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
-            const int32_t *__restrict__ mask, const float *__restrict__ cpp,
-            uint32_t *__restrict__ ghist, const float *__restrict__ grad, const OptState *__restrict__ step) {
-    extern __shared__ float4 sm4[];
-    const WalkSmem S = walk_smem(P, sm4);
-    uint32_t *h = reinterpret_cast<uint32_t *>(S.tail);
-    const int nbins = P.rb * P.fb;
-    float *X = reinterpret_cast<float *>(h + ((nbins + 3) & ~3));  // x-contracted rows (P.xs)
-    // the histogram starts at 16 bytes (walk_smem): zeroed four bins at a time
+// Shared histogram of a walk block: zeroed four bins at a time (it starts 16-byte aligned) and
+// flushed with one global atomic per non-zero bin (merging the blocks of a cluster through
+// distributed shared memory first was measured slower at every volume size). flush_hist starts
+// with a barrier (every count of the block is in).
+__device__ __forceinline__ void zero_hist(uint32_t *h, int nbins) {
     for (int i = threadIdx.x; i < (nbins + 3) / 4; i += blockDim.x) reinterpret_cast<uint4 *>(h)[i] = make_uint4(0, 0, 0, 0);
-    if (kTrial) pdl_wait();  // the trial position and step length come from the previous launch
-    const float scale = kTrial ? -step->cur_len : 0.f;
-    const int lane = threadIdx.x & 31;
-    const float frb = (float)P.rb, ffb = (float)P.fb;
-    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
-        Item I;
-        stage_item<kTrial>(P, cpp, item, S.cp, S.zb, S.zk, S.zid, I, grad, scale);
-        Column C;
-        column_init(P, I, S.cp, C);
-        if (kXs) build_xrows(P, C, S.cp, X);
-        const int nzi = I.z1 - I.z0;
-        int idx = (I.z0 * P.ny + C.y) * P.nx + C.x;
-        const int zstride = P.nx * P.ny;
-        for (int zi = 0; zi < nzi; zi += WALK_GROUP) {
-            int bin[WALK_GROUP];
-#pragma unroll
-            for (int u = 0; u < WALK_GROUP; ++u) {
-                const int zu = min(zi + u, nzi - 1);
-                float pos[3];
-                column_position(P, I, C, S.zb, S.zk, S.zid, zu, pos, kXs ? X : nullptr);
-                bin[u] = -1;
-                if (C.inside && zi + u < nzi) {
-                    const int vi = idx + u * zstride;
-                    if (mask == nullptr || __ldg(&mask[vi]) > -1) {
-                        float w, g[3];
-                        sample_floating<false, kDiag ? 1 : 0>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin,
-                                                              P.flo_ijk, P.flo_diag, P.pad, pos[0], pos[1], pos[2],
-                                                              w, g);
-                        const float rv = __ldg(&ref[vi]);
-                        if (0.f <= rv && rv < frb && 0.f <= w && w < ffb)  // false for NaN
-                            bin[u] = trunc_nonneg(rv) + trunc_nonneg(w) * P.rb;
-                    }
-                }
-            }
-            idx += WALK_GROUP * zstride;
-#pragma unroll
-            for (int u = 0; u < WALK_GROUP; ++u) {
-                // a warp whose 32 voxels share one bin (background) adds 32 with one atomic
-                const int b0 = __shfl_sync(0xffffffffu, bin[u], 0);
-                if (__all_sync(0xffffffffu, bin[u] == b0)) {
-                    if (lane == 0 && b0 >= 0) atomicAdd(&h[b0], 32u);
-                } else if (bin[u] >= 0) {
-                    atomicAdd(&h[bin[u]], 1u);
-                }
-            }
-        }
-    }
-    // one atomic per non-zero bin of the block (merging the blocks of a cluster through
-    // distributed shared memory first was measured slower at every volume size)
+}
+
+__device__ __forceinline__ void flush_hist(const uint32_t *h, int nbins, uint32_t *__restrict__ ghist) {
     __syncthreads();
     for (int i = threadIdx.x; i < nbins / 4; i += blockDim.x) {
         const uint4 c = reinterpret_cast<const uint4 *>(h)[i];
@@ -490,6 +415,92 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
         const uint32_t c = h[i];
         if (c) atomicAdd(&ghist[i], c);
     }
+}
+
+// One item of the fused objective (deformation + warp + joint histogram): stage the item's
+// control points (the trial values best - len * grad when grad is given), walk its columns and
+// count every active voxel's (reference, warped) bin pair into the block's histogram h. Called
+// by every thread of the block.
+template <bool kXs, bool kDiag>
+__device__ __forceinline__ void objective_item(const WalkParams& P, const WalkSmem& S, uint32_t *h, float *X,
+                                               int item, const float *__restrict__ ref,
+                                               const float *__restrict__ flo, const int32_t *__restrict__ mask,
+                                               const float *__restrict__ cpp, const float *__restrict__ grad,
+                                               float scale) {
+    const int lane = threadIdx.x & 31;
+    const float frb = (float)P.rb, ffb = (float)P.fb;
+    Item I;
+    stage_item<true>(P, cpp, item, S.cp, S.zb, S.zk, S.zid, I, grad, scale);
+    Column C;
+    column_init(P, I, S.cp, C);
+    if (kXs) build_xrows(P, C, S.cp, X);
+    const int nzi = I.z1 - I.z0;
+    int idx = (I.z0 * P.ny + C.y) * P.nx + C.x;
+    const int zstride = P.nx * P.ny;
+    for (int zi = 0; zi < nzi; zi += WALK_GROUP) {
+        int bin[WALK_GROUP];
+#pragma unroll
+        for (int u = 0; u < WALK_GROUP; ++u) {
+            const int zu = min(zi + u, nzi - 1);
+            float pos[3];
+            column_position(P, I, C, S.zb, S.zk, S.zid, zu, pos, kXs ? X : nullptr);
+            bin[u] = -1;
+            if (C.inside && zi + u < nzi) {
+                const int vi = idx + u * zstride;
+                if (mask == nullptr || __ldg(&mask[vi]) > -1) {
+                    float w, g[3];
+                    sample_floating<false, kDiag ? 1 : 0>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin,
+                                                          P.flo_ijk, P.flo_diag, P.pad, pos[0], pos[1], pos[2], w, g);
+                    const float rv = __ldg(&ref[vi]);
+                    if (0.f <= rv && rv < frb && 0.f <= w && w < ffb)  // false for NaN
+                        bin[u] = trunc_nonneg(rv) + trunc_nonneg(w) * P.rb;
+                }
+            }
+        }
+        idx += WALK_GROUP * zstride;
+#pragma unroll
+        for (int u = 0; u < WALK_GROUP; ++u) {
+            // a warp whose 32 voxels share one bin (background) adds 32 with one atomic
+            const int b0 = __shfl_sync(0xffffffffu, bin[u], 0);
+            if (__all_sync(0xffffffffu, bin[u] == b0)) {
+                if (lane == 0 && b0 >= 0) atomicAdd(&h[b0], 32u);
+            } else if (bin[u] >= 0) {
+                atomicAdd(&h[bin[u]], 1u);
+            }
+        }
+    }
+}
+
+// shared layout of an objective block: walk | histogram | x-contracted rows (P.xs)
+__device__ __forceinline__ void objective_smem(const WalkParams& P, void *base, WalkSmem& S, uint32_t *&h, float *&X) {
+    S = walk_smem(P, base);
+    h = reinterpret_cast<uint32_t *>(S.tail);
+    X = reinterpret_cast<float *>(h + ((P.rb * P.fb + 3) & ~3));
+}
+
+// ---------------------------------------------------------------------------------------------
+// fused objective: deformation + warp + joint histogram
+// ---------------------------------------------------------------------------------------------
+// kXs: the item's x-contracted node rows are staged in shared memory; kDiag: the floating
+// image's mm -> voxel matrix has no off-diagonal terms (launch-time choices made template
+// parameters, so the walk carries no test for them)
+template <bool kTrial, bool kXs, bool kDiag>
+__global__ void __launch_bounds__(32 * TY_OBJECTIVE, 2)
+k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
+            const int32_t *__restrict__ mask, const float *__restrict__ cpp,
+            uint32_t *__restrict__ ghist, const float *__restrict__ grad, const OptState *__restrict__ step) {
+    extern __shared__ float4 sm4[];
+    WalkSmem S;
+    uint32_t *h;
+    float *X;
+    objective_smem(P, sm4, S, h, X);
+    const int nbins = P.rb * P.fb;
+    zero_hist(h, nbins);
+    if (kTrial) pdl_wait();  // the trial position and step length come from the previous launch
+    const float scale = kTrial ? -step->cur_len : 0.f;
+    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x)
+        objective_item<kXs, kDiag>(P, S, h, X, item, ref, flo, mask, cpp, kTrial ? grad : nullptr, scale);
+    flush_hist(h, nbins, ghist);
 }
 
 // Sum over the 4x4 Parzen window of reg_getVoxelBasedNmiGradient3d (_reg_nmi.cpp:548-571):
@@ -602,6 +613,77 @@ __device__ __forceinline__ float nmi_window_f(float rv, float wv, const float *l
 // ---------------------------------------------------------------------------------------------
 // fused gradient: deformation + warp + spatial gradient + NMI voxel gradient
 // ---------------------------------------------------------------------------------------------
+// The NMI quantities one gradient evaluation reads: the log table of the best position's table
+// set, its NMI and the normalisation weight / (H_joint * total).
+struct GradientTables {
+    const double *logt;
+    double nmi, scale;
+    float nmi_f, scale_f;
+};
+
+__device__ __forceinline__ GradientTables gradient_tables(const double *logt0, const nrb_objective *last0,
+                                                          const double *logt1, const nrb_objective *last1,
+                                                          bool second, double weight) {
+    GradientTables T;
+    T.logt = second ? logt1 : logt0;
+    const nrb_objective *last = second ? last1 : last0;
+    T.nmi = last->nmi;
+    T.scale = weight / (last->entropy[2] * last->entropy[3]);
+    T.nmi_f = (float)T.nmi;
+    T.scale_f = (float)T.scale;
+    return T;
+}
+
+// FP32 copy of the log table in shared memory for the FP32 window (visible after the next
+// stage_item barrier)
+__device__ __forceinline__ void stage_log_table(const WalkParams& P, const double *logt, float *logf) {
+    const int total = P.rb * P.fb + P.rb + P.fb;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) logf[i] = (float)logt[i];
+}
+
+// One item of the fused gradient: stage the item's control points, walk its columns and write
+// every voxel's NMI gradient (zero where masked or NaN). Called by every thread of the block.
+template <bool kF32, bool kDiag>
+__device__ __forceinline__ void gradient_item(const WalkParams& P, const WalkSmem& S, const float *logf,
+                                              const GradientTables& T, int item, const float *__restrict__ ref,
+                                              const float *__restrict__ flo, const int32_t *__restrict__ mask,
+                                              const float *__restrict__ cpp, float *__restrict__ vgrad) {
+    const int nv = P.nx * P.ny * P.nz;
+    Item I;
+    stage_item(P, cpp, item, S.cp, S.zb, S.zk, S.zid, I);
+    Column C;
+    column_init(P, I, S.cp, C);
+    const int nzi = I.z1 - I.z0;
+    const int zstride = P.nx * P.ny;
+    int idx = (I.z0 * P.ny + C.y) * P.nx + C.x;
+    for (int zi = 0; zi < nzi; ++zi, idx += zstride) {
+        float pos[3];
+        column_position(P, I, C, S.zb, S.zk, S.zid, zi, pos);
+        if (!C.inside) continue;
+        float out[3] = { 0.f, 0.f, 0.f };
+        if (mask == nullptr || __ldg(&mask[idx]) > -1) {
+            float w, g[3];
+            sample_floating<true, kDiag ? 1 : 0>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin, P.flo_ijk,
+                                                 P.flo_diag, P.pad, pos[0], pos[1], pos[2], w, g);
+            const float rv = __ldg(&ref[idx]);
+            if (rv == rv && w == w) {
+                if (kF32) {
+                    const float s = nmi_window_f(rv, w, logf, P.rb, P.fb, T.nmi_f);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) out[d] = T.scale_f * (g[d] * s);
+                } else {
+                    const double s = nmi_window(rv, w, T.logt, P.rb, P.fb, T.nmi);
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) out[d] = (float)(T.scale * ((double)g[d] * s));
+                }
+            }
+        }
+        vgrad[idx] = out[0];
+        vgrad[nv + idx] = out[1];
+        vgrad[2 * nv + idx] = out[2];
+    }
+}
+
 template <bool kF32, bool kDiag>
 __global__ void __launch_bounds__(32 * TY_GRADIENT, kF32 ? 6 : 4)
 k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict__ flo,
@@ -610,55 +692,11 @@ k_gradient(WalkParams P, const float *__restrict__ ref, const float *__restrict_
            const OptState *__restrict__ sel, double weight, float *__restrict__ vgrad) {
     extern __shared__ float4 sm4[];
     const WalkSmem S = walk_smem(P, sm4);
-    const int nv = P.nx * P.ny * P.nz;
-    const bool second = sel && sel->best_buf == 1;
-    const double *__restrict__ logt_g = second ? logt1 : logt0;
-    const nrb_objective *__restrict__ last = second ? last1 : last0;
-    const double nmi = last->nmi;
-    const double scale = weight / (last->entropy[2] * last->entropy[3]);
-    const float nmi_f = (float)nmi, scale_f = (float)scale;
-    float *logf = nullptr;
-    if (kF32) {  // FP32 copy of the log table for the FP32 window
-        logf = reinterpret_cast<float *>(S.tail);
-        const int total = P.rb * P.fb + P.rb + P.fb;
-        for (int i = threadIdx.x; i < total; i += blockDim.x) logf[i] = (float)logt_g[i];
-        // visible after the first stage_item barrier
-    }
-    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
-        Item I;
-        stage_item(P, cpp, item, S.cp, S.zb, S.zk, S.zid, I);
-        Column C;
-        column_init(P, I, S.cp, C);
-        const int nzi = I.z1 - I.z0;
-        const int zstride = P.nx * P.ny;
-        int idx = (I.z0 * P.ny + C.y) * P.nx + C.x;
-        for (int zi = 0; zi < nzi; ++zi, idx += zstride) {
-            float pos[3];
-            column_position(P, I, C, S.zb, S.zk, S.zid, zi, pos);
-            if (!C.inside) continue;
-            float out[3] = { 0.f, 0.f, 0.f };
-            if (mask == nullptr || __ldg(&mask[idx]) > -1) {
-                float w, g[3];
-                sample_floating<true, kDiag ? 1 : 0>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin, P.flo_ijk, P.flo_diag,
-                                      P.pad, pos[0], pos[1], pos[2], w, g);
-                const float rv = __ldg(&ref[idx]);
-                if (rv == rv && w == w) {
-                    if (kF32) {
-                        const float s = nmi_window_f(rv, w, logf, P.rb, P.fb, nmi_f);
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) out[d] = scale_f * (g[d] * s);
-                    } else {
-                        const double s = nmi_window(rv, w, logt_g, P.rb, P.fb, nmi);
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) out[d] = (float)(scale * ((double)g[d] * s));
-                    }
-                }
-            }
-            vgrad[idx] = out[0];
-            vgrad[nv + idx] = out[1];
-            vgrad[2 * nv + idx] = out[2];
-        }
-    }
+    const GradientTables T = gradient_tables(logt0, last0, logt1, last1, sel && sel->best_buf == 1, weight);
+    float *logf = reinterpret_cast<float *>(S.tail);
+    if (kF32) stage_log_table(P, T.logt, logf);
+    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x)
+        gradient_item<kF32, kDiag>(P, S, logf, T, item, ref, flo, mask, cpp, vgrad);
 }
 
 // standalone deformation field (Compute::GetDeformationField) with the same arithmetic
@@ -752,15 +790,41 @@ __device__ __forceinline__ void block_sum3w(double& a, double& b, double& c, dou
 // per block: T = own rows, U = own rows + 2 halo rows (later the partial reference marginal).
 constexpr int FIN_CLUSTER = 8, FIN_CTA_THREADS = 256, FIN_WARPS = FIN_CTA_THREADS / 32;
 
-__global__ void __cluster_dims__(FIN_CLUSTER, 1, 1) __launch_bounds__(FIN_CTA_THREADS)
-k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double *logt0, nrb_objective *last0,
-               double *pro1, double *logt1, nrb_objective *last1,
-               const double *__restrict__ be_partials, int n_be, double be_norm,
-               double sim_weight, double be_weight, nrb_objective *__restrict__ obj,
-               OptState *__restrict__ ctl, cudaGraphConditionalHandle line, float *__restrict__ acc_best,
-               const float *__restrict__ acc_grad, long long acc_n) {
-    pdl_wait();  // the counts come from the objective pass
-    cg::cluster_group cluster = cg::this_cluster();
+// What the finalize does besides the tables: FIN_PLAIN a standalone evaluation (table set 0, no
+// optimiser); FIN_LINE a line-search step of a level graph (line_step, the line search's WHILE
+// condition); FIN_BATCH_INIT / FIN_BATCH_LINE the same two inside a batched level, where the
+// pair's phase moves on instead of a condition being set (INIT: the starting point's values
+// become the best ones; LINE: line_step, then the end of the line search when it stops).
+enum FinMode : int { FIN_PLAIN = 0, FIN_LINE = 1, FIN_BATCH_INIT = 2, FIN_BATCH_LINE = 3 };
+
+struct FinArgs {
+    int rb, fb;
+    uint32_t *hist;
+    double *pro0, *logt0;
+    nrb_objective *last0;
+    double *pro1, *logt1;
+    nrb_objective *last1;
+    const double *be_partials;
+    int n_be;
+    double be_norm, sim_weight, be_weight;
+    nrb_objective *obj;
+    OptState *ctl;
+    float *acc_best;
+    const float *acc_grad;
+    long long acc_n;
+};
+
+template <int kMode>
+__device__ __forceinline__ void finalize_cluster(cg::cluster_group& cluster, const FinArgs& A,
+                                                 cudaGraphConditionalHandle line) {
+    const int rb = A.rb, fb = A.fb;
+    uint32_t *__restrict__ hist = A.hist;
+    const double *__restrict__ be_partials = A.be_partials;
+    const int n_be = A.n_be;
+    const double be_norm = A.be_norm, sim_weight = A.sim_weight, be_weight = A.be_weight;
+    nrb_objective *__restrict__ obj = A.obj;
+    OptState *__restrict__ ctl = A.ctl;
+    nrb_objective *last0 = A.last0, *last1 = A.last1;
     extern __shared__ double sm[];
     __shared__ double red[3 * 32];
     __shared__ double part[4];  // this block's partial mass, H_ref, H_war, H_joint
@@ -793,10 +857,11 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
         U[(f - f0 + 1) * rb + r] = smooth3(r > 0, l, m, r + 1 < rb, rr, k0, k1);
     }
     __syncthreads();
-    // output table set: the one not holding the best position
-    const bool second = ctl && sctl.best_buf == 0;
-    double *__restrict__ pro = second ? pro1 : pro0;
-    double *__restrict__ logt = second ? logt1 : logt0;
+    // output table set: the one not holding the best position (a level's starting point and a
+    // standalone evaluation write the first set)
+    const bool second = (kMode == FIN_LINE || kMode == FIN_BATCH_LINE) && sctl.best_buf == 0;
+    double *__restrict__ pro = second ? A.pro1 : A.pro0;
+    double *__restrict__ logt = second ? A.logt1 : A.logt0;
     nrb_objective *__restrict__ last = second ? last1 : last0;
     // smoothing along the floating axis of the own rows
     double mass = 0.0, z2 = 0.0;
@@ -920,27 +985,49 @@ k_nmi_finalize(int rb, int fb, uint32_t *__restrict__ hist, double *pro0, double
         o.objective = (sim_weight > 0 ? sim_weight * o.nmi : 0.0) - (be_weight > 0 ? be_weight * o.be : 0.0);
         o.max_grad_len = s_mgl[second ? 1 : 0];
         // every block takes the same step on its own copy of the state; block 0 publishes it
-        const bool more = ctl ? line_step(&sctl, o.nmi, o.be, sim_weight, be_weight) : false;
+        bool more = false;
+        if (kMode == FIN_LINE || kMode == FIN_BATCH_LINE) more = line_step(&sctl, o.nmi, o.be, sim_weight, be_weight);
+        if (kMode == FIN_BATCH_INIT) {
+            // ConjugateGradient::Initialise: the starting point is the best one so far
+            // (reg_f3d::GetObjectiveFunctionValue's weighted terms, as line_step forms them)
+            const double wm = sim_weight > 0 ? sim_weight * o.nmi : 0.0;
+            const double wb = be_weight > 0 ? be_weight * o.be : 0.0;
+            sctl.n_obj += 1;
+            sctl.best_w_measure = wm;
+            sctl.best_w_be = wb;
+            sctl.best_nmi = o.nmi;
+            sctl.best_be = o.be;
+            sctl.best_obj = __dsub_rn(wm, wb);
+            sctl.accepted = 0;
+            sctl.phase = outer_continues(sctl) ? PH_GRAD : PH_DONE;
+        }
+        if (kMode == FIN_BATCH_LINE && !more) sctl.phase = line_end(&sctl) ? PH_GRAD : PH_DONE;
         if (c == 0) {
             *last = o;
             if (obj) *obj = o;
-            if (ctl) {
-                *ctl = sctl;
-                cudaGraphSetConditional(line, more ? 1u : 0u);
-            }
+            if (kMode != FIN_PLAIN) *ctl = sctl;
+            if (kMode == FIN_LINE) cudaGraphSetConditional(line, more ? 1u : 0u);
         }
     }
     // this block has read the others' shared memory: they may exit once every block arrived
     auto token = cluster.barrier_arrive();
     __syncthreads();  // the decision in sctl
-    // small grids: the store of an accepted trial position (k_accept's operations) in the same
-    // launch
-    if (ctl && acc_n > 0 && sctl.accepted) {
+    // the store of an accepted trial position (k_accept's operations) in the same launch
+    if ((kMode == FIN_LINE || kMode == FIN_BATCH_LINE) && A.acc_n > 0 && sctl.accepted) {
         const float scale = -sctl.step_len;
-        for (long long i = (long long)c * FIN_CTA_THREADS + tid; i < acc_n; i += (long long)FIN_CLUSTER * FIN_CTA_THREADS)
-            acc_best[i] = __fadd_rn(acc_best[i], __fmul_rn(scale, acc_grad[i]));
+        for (long long i = (long long)c * FIN_CTA_THREADS + tid; i < A.acc_n;
+             i += (long long)FIN_CLUSTER * FIN_CTA_THREADS)
+            A.acc_best[i] = __fadd_rn(A.acc_best[i], __fmul_rn(scale, A.acc_grad[i]));
     }
     cluster.barrier_wait(std::move(token));
+}
+
+__global__ void __cluster_dims__(FIN_CLUSTER, 1, 1) __launch_bounds__(FIN_CTA_THREADS)
+k_nmi_finalize(FinArgs A, cudaGraphConditionalHandle line) {
+    pdl_wait();  // the counts come from the objective pass
+    cg::cluster_group cluster = cg::this_cluster();
+    if (A.ctl) finalize_cluster<FIN_LINE>(cluster, A, line);
+    else finalize_cluster<FIN_PLAIN>(cluster, A, line);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1115,6 +1202,125 @@ __global__ void k_nmi_voxel_gradient(long long nv, int rb, int fb, const float *
 }
 
 // ---------------------------------------------------------------------------------------------
+// batched levels: one launch per stage over every pair that needs it
+// ---------------------------------------------------------------------------------------------
+// The objective of every pair in INIT (at best) or LINE (at best - cur_len * grad): each block
+// walks its share of the pairs' items with the pair's own walk and histogram, exactly the
+// plain k_objective's work per item.
+template <bool kXs, bool kDiag>
+__global__ void __launch_bounds__(32 * TY_OBJECTIVE, 2)
+k_b_objective(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
+    extern __shared__ float4 sm4[];
+    __shared__ BatchList L;
+    __shared__ WalkParams sP;
+    batch_list_build(pairs, states, npairs, (1u << PH_INIT) | (1u << PH_LINE),
+                     [](const BatchPair& b, int& u, int& w) {
+                         u = b.wo.nitems;
+                         w = b.wo.zchunk + 6;
+                     }, L);
+    const long long c0 = L.total * blockIdx.x / gridDim.x, c1 = L.total * (blockIdx.x + 1) / gridDim.x;
+    for (int k = 0; k < L.n; ++k) {
+        int j0, j1;
+        if (!batch_units(L, k, c0, c1, j0, j1)) continue;
+        const int p = L.pair[k];
+        const BatchPair& B = pairs[p];
+        __syncthreads();  // the previous pair's readers of sP are done
+        copy_words(&sP, &B.wo, sizeof(WalkParams));
+        __syncthreads();
+        WalkSmem S;
+        uint32_t *h;
+        float *X;
+        objective_smem(sP, sm4, S, h, X);
+        const int nbins = sP.rb * sP.fb;
+        zero_hist(h, nbins);  // ordered before the counts by stage_item's first barrier
+        const bool line = states[p].phase == PH_LINE;
+        const float *grad = line ? B.grad : nullptr;
+        const float scale = line ? -states[p].cur_len : 0.f;
+        for (int j = j0; j < j1; ++j)
+            objective_item<kXs, kDiag>(sP, S, h, X, j, B.ref, B.flo, nullptr, B.best, grad, scale);
+        flush_hist(h, nbins, B.hist);
+    }
+}
+
+// The fused voxel gradient of every pair in GRAD, at best, with the NMI tables of its best
+// position (the plain k_gradient's work per item).
+template <bool kF32, bool kDiag>
+__global__ void __launch_bounds__(32 * TY_GRADIENT, kF32 ? 6 : 4)
+k_b_gradient(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
+    extern __shared__ float4 sm4[];
+    __shared__ BatchList L;
+    __shared__ WalkParams sP;
+    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
+                     [](const BatchPair& b, int& u, int& w) {
+                         u = b.wg.nitems;
+                         w = b.wg.zchunk + 4;
+                     }, L);
+    const long long c0 = L.total * blockIdx.x / gridDim.x, c1 = L.total * (blockIdx.x + 1) / gridDim.x;
+    for (int k = 0; k < L.n; ++k) {
+        int j0, j1;
+        if (!batch_units(L, k, c0, c1, j0, j1)) continue;
+        const int p = L.pair[k];
+        const BatchPair& B = pairs[p];
+        __syncthreads();
+        copy_words(&sP, &B.wg, sizeof(WalkParams));
+        __syncthreads();
+        const WalkSmem S = walk_smem(sP, sm4);
+        const GradientTables T = gradient_tables(B.logt0, B.last0, B.logt1, B.last1, states[p].best_buf == 1, 1.0);
+        float *logf = reinterpret_cast<float *>(S.tail);
+        if (kF32) stage_log_table(sP, T.logt, logf);  // visible after stage_item's first barrier
+        for (int j = j0; j < j1; ++j) gradient_item<kF32, kDiag>(sP, S, logf, T, j, B.ref, B.flo, nullptr, B.best, B.vgrad);
+    }
+}
+
+// One finalize cluster per pair (cluster q = pair q): the pairs in INIT or LINE finish their
+// evaluation (tables, NMI, bending energy, line-search step, accepted step stored, phase moved
+// on); the last cluster sets whether the gradient stage runs this iteration (enough pairs wait
+// for it, or no pair has a line-search step left) and whether the level goes on.
+__global__ void __cluster_dims__(FIN_CLUSTER, 1, 1) __launch_bounds__(FIN_CTA_THREADS)
+k_b_finalize(const BatchPair *__restrict__ pairs, OptState *__restrict__ states, int npairs,
+             BatchCtl *__restrict__ bctl, cudaGraphConditionalHandle grad_if, cudaGraphConditionalHandle outer) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int p = blockIdx.x / FIN_CLUSTER;
+    const int phase = states[p].phase;
+    if (phase == PH_INIT || phase == PH_LINE) {
+        const BatchPair& B = pairs[p];
+        FinArgs A;
+        A.rb = B.rb;
+        A.fb = B.fb;
+        A.hist = B.hist;
+        A.pro0 = B.pro0;
+        A.logt0 = B.logt0;
+        A.last0 = B.last0;
+        A.pro1 = B.pro1;
+        A.logt1 = B.logt1;
+        A.last1 = B.last1;
+        A.be_partials = B.be_partials;
+        A.n_be = B.be_w > 0 ? B.n_be : 0;
+        A.be_norm = B.be_norm;
+        A.sim_weight = B.sim_w;
+        A.be_weight = B.be_w;
+        A.obj = B.obj;
+        A.ctl = &states[p];
+        A.acc_best = B.best;
+        A.acc_grad = B.grad;
+        A.acc_n = 3 * B.nnode;
+        if (phase == PH_INIT) finalize_cluster<FIN_BATCH_INIT>(cluster, A, 0);
+        else finalize_cluster<FIN_BATCH_LINE>(cluster, A, 0);
+    }
+    if (cluster.block_rank() != 0) return;
+    if (!batch_last_cluster(&bctl->ticket_fin, gridDim.x / FIN_CLUSTER)) return;
+    int nline, ngrad;
+    batch_counts(states, npairs, nline, ngrad);
+    if (threadIdx.x == 0) {
+        const bool run_grad = ngrad > 0 && (100 * ngrad >= bctl->grad_percent * (nline + ngrad) || nline == 0);
+        cudaGraphSetConditional(grad_if, run_grad ? 1u : 0u);
+        bctl->iterations += 1;
+        bctl->grad_stages += run_grad ? 1 : 0;
+        cudaGraphSetConditional(outer, nline + ngrad > 0 ? 1u : 0u);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
 static WalkParams make_params(const WalkPlan& W, const nrb_geometry *g, float pad, int rb, int fb) {
@@ -1270,11 +1476,115 @@ nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be
     const size_t smem = (size_t)(2 * rpc + 2) * nmi->rb * sizeof(double);
     NRB_CUDA(cudaFuncSetAttribute(k_nmi_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     KernelTimer timer(TK_FINALIZE, (double)nmi->rb * nmi->fb * 8 + (double)nmi->total * 16, st);
-    NRB_CUDA(launch_pdl(ctl != nullptr, k_nmi_finalize, dim3(FIN_CLUSTER), dim3(FIN_CTA_THREADS), smem, st, nmi->rb,
-                        nmi->fb, nmi->hist, nmi->pro, nmi->logt, nmi->last, nmi->pro2, nmi->logt2, nmi->last2,
-                        be_partials, n_be_partials, (double)cpp_nvox3, sim_weight, be_weight, obj, ctl, line,
-                        acc_best, acc_grad, acc_n));
+    FinArgs A;
+    A.rb = nmi->rb;
+    A.fb = nmi->fb;
+    A.hist = nmi->hist;
+    A.pro0 = nmi->pro;
+    A.logt0 = nmi->logt;
+    A.last0 = nmi->last;
+    A.pro1 = nmi->pro2;
+    A.logt1 = nmi->logt2;
+    A.last1 = nmi->last2;
+    A.be_partials = be_partials;
+    A.n_be = n_be_partials;
+    A.be_norm = (double)cpp_nvox3;
+    A.sim_weight = sim_weight;
+    A.be_weight = be_weight;
+    A.obj = obj;
+    A.ctl = ctl;
+    A.acc_best = acc_best;
+    A.acc_grad = acc_grad;
+    A.acc_n = acc_n;
+    NRB_CUDA(launch_pdl(ctl != nullptr, k_nmi_finalize, dim3(FIN_CLUSTER), dim3(FIN_CTA_THREADS), smem, st, A, line));
     NRB_LAUNCHED("k_nmi_finalize");
+    return NRB_OK;
+}
+
+// ---- batched levels: walks, launch shapes, launches ----------------------------------------
+nrb_status batch_walks(nrb_workspace *ws, const nrb_nmi *nmi, const nrb_geometry *g, float padding, int flo_margin,
+                       WalkParams& wo, WalkParams& wg) {
+    wo = make_params(ws->walk_obj, g, padding, nmi->rb, nmi->fb);
+    set_floating_margin(wo, flo_margin);
+    wg = make_params(ws->walk_grad, g, padding, nmi->rb, nmi->fb);
+    set_floating_margin(wg, flo_margin);
+    wg.log_in_smem = (size_t)nmi->total * sizeof(float) <= 96 * 1024;
+    return NRB_OK;
+}
+
+nrb_status batch_plan(std::vector<BatchPair>& pairs, BatchLaunch& L) {
+    L = BatchLaunch{};
+    L.npairs = (int)pairs.size();
+    if (L.npairs < 1 || L.npairs > BATCH_MAX_PAIRS)
+        return fail(NRB_ERR_INVALID, "batched level: 1 to " + std::to_string(BATCH_MAX_PAIRS) + " pairs");
+    size_t base = 0, xs = 0, gsm = 0;
+    bool diag = true, f32 = true;
+    int rb = pairs[0].rb, fb = pairs[0].fb;
+    for (const BatchPair& b : pairs) {
+        if (b.rb != rb || b.fb != fb) return fail(NRB_ERR_INVALID, "batched level: every pair needs the same bins");
+        const size_t cp_o = (size_t)3 * b.wo.sa * b.wo.sb * b.wo.sc;
+        base = std::max(base, (cp_o + 4 + (size_t)walk_table_floats(b.wo.zchunk)) * 4 + 16 +
+                                  (size_t)((rb * fb + 3) & ~3) * 4);
+        xs = std::max(xs, (size_t)3 * b.wo.sc * b.wo.sb * 32 * 4);
+        const size_t cp_g = (size_t)3 * b.wg.sa * b.wg.sb * b.wg.sc;
+        gsm = std::max(gsm, (cp_g + 4 + (size_t)walk_table_floats(b.wg.zchunk)) * 4 + 16);
+        diag = diag && b.wo.flo_diag;
+        f32 = f32 && b.wg.log_in_smem;
+    }
+    L.obj_xs = base + xs <= 100 * 1024;
+    L.obj_diag = diag;
+    L.obj_smem = base + (L.obj_xs ? xs : 0);
+    L.grad_f32 = f32;
+    L.grad_diag = diag;
+    L.grad_smem = gsm + (f32 ? (size_t)(rb * fb + rb + fb) * sizeof(float) : 0);
+    const int rpc = (fb + FIN_CLUSTER - 1) / FIN_CLUSTER;
+    L.fin_smem = (size_t)(2 * rpc + 2) * rb * sizeof(double);
+    for (BatchPair& b : pairs) {
+        b.wo.xs = L.obj_xs;
+        b.wg.log_in_smem = f32;
+    }
+    auto ko = L.obj_diag ? (L.obj_xs ? k_b_objective<true, true> : k_b_objective<false, true>)
+                         : (L.obj_xs ? k_b_objective<true, false> : k_b_objective<false, false>);
+    auto kg = L.grad_diag ? (L.grad_f32 ? k_b_gradient<true, true> : k_b_gradient<false, true>)
+                          : (L.grad_f32 ? k_b_gradient<true, false> : k_b_gradient<false, false>);
+    int per = 0;
+    NRB_CUDA(cudaFuncSetAttribute(ko, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    NRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, ko, 32 * TY_OBJECTIVE, L.obj_smem));
+    L.obj_grid = std::max(1, per) * sm_count();
+    NRB_CUDA(cudaFuncSetAttribute(kg, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    NRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kg, 32 * TY_GRADIENT, L.grad_smem));
+    L.grad_grid = std::max(1, per) * sm_count();
+    NRB_CUDA(cudaFuncSetAttribute(k_b_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.fin_smem));
+    return NRB_OK;
+}
+
+nrb_status launch_batch_objective(const BatchPair *d_pairs, const OptState *states, const BatchLaunch& L,
+                                  cudaStream_t st) {
+    auto ko = L.obj_diag ? (L.obj_xs ? k_b_objective<true, true> : k_b_objective<false, true>)
+                         : (L.obj_xs ? k_b_objective<true, false> : k_b_objective<false, false>);
+    ko<<<L.obj_grid, 32 * TY_OBJECTIVE, L.obj_smem, st>>>(d_pairs, states, L.npairs);
+    NRB_CUDA(cudaGetLastError());
+    NRB_LAUNCHED("k_b_objective");
+    return NRB_OK;
+}
+
+nrb_status launch_batch_gradient(const BatchPair *d_pairs, const OptState *states, const BatchLaunch& L,
+                                 cudaStream_t st) {
+    auto kg = L.grad_diag ? (L.grad_f32 ? k_b_gradient<true, true> : k_b_gradient<false, true>)
+                          : (L.grad_f32 ? k_b_gradient<true, false> : k_b_gradient<false, false>);
+    kg<<<L.grad_grid, 32 * TY_GRADIENT, L.grad_smem, st>>>(d_pairs, states, L.npairs);
+    NRB_CUDA(cudaGetLastError());
+    NRB_LAUNCHED("k_b_gradient");
+    return NRB_OK;
+}
+
+nrb_status launch_batch_finalize(const BatchPair *d_pairs, OptState *states, BatchCtl *bctl, const BatchLaunch& L,
+                                 cudaGraphConditionalHandle grad_if, cudaGraphConditionalHandle outer,
+                                 cudaStream_t st) {
+    k_b_finalize<<<FIN_CLUSTER * L.npairs, FIN_CTA_THREADS, L.fin_smem, st>>>(d_pairs, states, L.npairs, bctl,
+                                                                              grad_if, outer);
+    NRB_CUDA(cudaGetLastError());
+    NRB_LAUNCHED("k_b_finalize");
     return NRB_OK;
 }
 

@@ -3,6 +3,7 @@ function include/niftyreg_b200.h declares, and host-only entry points behave."""
 import ctypes
 import os
 import re
+import subprocess
 
 import numpy as np
 
@@ -113,3 +114,13 @@ def test_footprint_is_host_only_and_monotone():
     d = (64, 64, 64)
     p0 = nrb.default_params(levels=2, spacing=(-5.0,), floating_margin=0)
     assert 0 < nrb.footprint(d, (1.0, 1.0, 1.0), p) - nrb.footprint(d, (1.0, 1.0, 1.0), p0) <= 4 * 80 ** 3
+
+
+def test_library_has_no_undefined_internal_symbols():
+    """Every function of the library's own namespace that one translation unit calls is defined
+    in another: the shared library links without them, so a missing definition would only show
+    when the first call fails to resolve."""
+    ensure_built()
+    out = subprocess.run(["nm", "-C", "-u", nrb.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    missing = [l.strip() for l in out.splitlines() if "nrb::" in l]
+    assert not missing, missing

@@ -1,5 +1,10 @@
 """Batched and served registrations: every result equals the plain single-pair result for the
-same request, bit for bit, whatever else runs beside it; admission respects the HBM budget."""
+same request, bit for bit, whatever else runs beside it; admission respects the HBM budget.
+
+The batch runs every pair of a group through one graph per level whose stages each cover all the
+pairs that need them; each pair's arithmetic (walks, reductions and their order, line-search
+control) is its plain registration's, so the grids, NMI values and evaluation counts must be
+identical, whatever the group size and the gradient-stage scheduling."""
 import numpy as np
 import pytest
 
@@ -41,6 +46,29 @@ def _same(a, b):
 def test_batch_equals_plain(pairs, plain):
     out = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], _params(), concurrency=4)
     for a, b in zip(out, plain):
+        _same(a, b)
+
+
+@pytest.mark.parametrize("percent,concurrency", [(1, 8), (100, 8), (50, 3), (50, 1)])
+def test_batch_scheduling_changes_nothing(pairs, plain, percent, concurrency):
+    """The gradient stage run as soon as one pair waits, only when all do, and groups of 3 and of
+    1 pair: the same results bit for bit (the batch holds each pair twice, so a group also mixes
+    copies of the same registration)."""
+    params = _params()
+    params.batch_gradient_percent = percent
+    out = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs * 2], params,
+                             concurrency=concurrency)
+    for i, a in enumerate(out):
+        _same(a, plain[i % len(pairs)])
+
+
+def test_batch_without_bending_energy_and_one_level(pairs):
+    """No bending-energy stages (weight 0) and a single level, against the plain path."""
+    params = nrb.default_params(levels=1, max_iterations=25, bending_energy=0.0, spacing=(-5.0,),
+                                ref_bins=32, flo_bins=32)
+    want = [nrb.register_host(p.reference, p.floating, p.pixdim, params) for p in pairs[:3]]
+    out = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs[:3]], params, concurrency=3)
+    for a, b in zip(out, want):
         _same(a, b)
 
 
