@@ -472,17 +472,21 @@ typedef struct nrb_pair {
 nrb_status nrb_f3d_footprint(const int32_t dim[3], const float pixdim[3], const nrb_f3d_params *p,
                              int64_t *bytes);
 
-/* A registration server on the current device: `slots` workers, each with its own stream, take
- * requests in arrival order as soon as a worker is free, the request's footprint fits in what is
- * left of hbm_budget_bytes (<= 0: 80% of the free device memory) and the running registrations
- * do not already keep the device busy (a registration counts as min(1, voxels / 2^21) of the
- * device; at most 2 devices' worth run at once). Admitted requests run concurrently and their
- * kernels overlap; each result is the one nrb_f3d_register_host gives for the same request
- * alone. While servers exist on a device, its default memory pool keeps freed memory up to the
- * budget (release threshold) and does not reuse memory across streams through inserted
- * dependencies; the pool's previous settings come back when the last server is destroyed. */
+/* A registration server on the current device (no counterpart in the reference: reg_f3d
+ * registers one pair per process). `slots` workers, each with its own stream, take requests in
+ * arrival order: a free worker takes the queue's head once its footprint fits in what is left of
+ * hbm_budget_bytes (<= 0: 80% of the free device memory; a request always runs when nothing else
+ * does), together with the queued requests that can share its group (the same parameters, a
+ * volume within a factor of two of the head's, up to max_group requests, within the budget), and
+ * registers the group as nrb_f3d_register_batch does. Requests that arrive while groups run wait
+ * for the next free worker and run beside them; each result is the one nrb_f3d_register_host
+ * gives for the same request alone. nrb_server_create uses max_group = 16. While servers exist
+ * on a device, its default memory pool keeps freed memory up to the budget (release threshold)
+ * and does not reuse memory across streams through inserted dependencies; the pool's previous
+ * settings come back when the last server is destroyed. */
 typedef struct nrb_server nrb_server;
 nrb_status nrb_server_create(int slots, int64_t hbm_budget_bytes, nrb_server **out);
+nrb_status nrb_server_create_grouped(int slots, int max_group, int64_t hbm_budget_bytes, nrb_server **out);
 nrb_status nrb_server_submit(nrb_server *s, const nrb_pair *req, const nrb_f3d_params *p,
                              int64_t *ticket);
 /* Blocks until the request ends; queue_seconds = submit -> admission, latency_seconds =
@@ -492,6 +496,8 @@ nrb_status nrb_server_wait(nrb_server *s, int64_t ticket, nrb_f3d_result *result
                            double *queue_seconds, double *latency_seconds);
 /* Peak admitted footprint and peak number of concurrent registrations so far. */
 nrb_status nrb_server_stats(nrb_server *s, int64_t *peak_bytes, int32_t *peak_active);
+/* Largest group registered together so far. */
+nrb_status nrb_server_peak_group(nrb_server *s, int32_t *peak_group);
 /* Finishes the queued requests, then stops the workers. */
 void nrb_server_destroy(nrb_server *s);
 

@@ -604,14 +604,16 @@ class _Request:
 
 class Server:
     """Continuous-batching registration server on the current device (nrb_server_*): `slots`
-    concurrent registrations, admitted in arrival order against an HBM budget in bytes
+    workers, each registering a group of up to `max_group` queued requests of similar size at a
+    time through the batched engine, admitted in arrival order against an HBM budget in bytes
     (0 = 80% of the free device memory)."""
 
-    def __init__(self, slots: int, budget_bytes: int = 0):
+    def __init__(self, slots: int, budget_bytes: int = 0, max_group: int = 16):
         self.h = ctypes.c_void_p()
         L = lib()
         L.nrb_server_destroy.restype = None
-        check(L.nrb_server_create(int(slots), ctypes.c_int64(budget_bytes), ctypes.byref(self.h)))
+        check(L.nrb_server_create_grouped(int(slots), int(max_group), ctypes.c_int64(budget_bytes),
+                                          ctypes.byref(self.h)))
         self._pending = {}
 
     def submit(self, ref, flo, pixdim, params: F3dParams) -> int:
@@ -636,6 +638,11 @@ class Server:
         b, a = ctypes.c_int64(), ctypes.c_int32()
         check(lib().nrb_server_stats(self.h, ctypes.byref(b), ctypes.byref(a)))
         return int(b.value), int(a.value)
+
+    def peak_group(self) -> int:
+        g = ctypes.c_int32()
+        check(lib().nrb_server_peak_group(self.h, ctypes.byref(g)))
+        return int(g.value)
 
     def close(self):
         if self.h:

@@ -1,15 +1,16 @@
 // Batched and served F3D registrations on one device.
 //
-// A server owns `slots` worker threads, each with its own CUDA stream. Requests queue in
-// arrival order; the head of the queue is admitted when a worker is free, its device footprint
-// fits in what the HBM budget has left and the device is not already kept busy by the running
-// registrations (load below, in whole devices), so requests that arrive while others run are
-// taken up as soon as a slot and memory free up, and their kernels overlap on the device with
-// the running ones. Each registration is the same sequence of launches as a plain
-// nrb_f3d_register_host call (deterministic kernels, no state shared between registrations), so
-// its result does not depend on what else runs.
+// A server owns `slots` worker threads, each with its own CUDA stream; a worker runs one group of
+// requests at a time through the batched registration (one graph per pyramid level in which every
+// stage is one launch over all the group's pairs). Requests queue in arrival order. When a worker
+// is free and the queue's head fits in what the HBM budget has left, the worker takes the head and
+// the queued requests that can share its group (the same parameters, a volume within a factor of
+// two of the head's, in arrival order, up to `max_group` requests and the budget). Requests that
+// arrive while groups run wait for the next free worker and run beside the groups already on the
+// device. Each pair's arithmetic in a group is that of its plain registration, so every result
+// equals nrb_f3d_register_host's for the same request alone, whatever it was grouped with.
 //
-// The batch entry point is a server sized to the batch that takes every pair at once.
+// The batch entry point forms groups the same way from the pairs it is given.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -33,18 +34,11 @@ using Clock = std::chrono::steady_clock;
 
 namespace {
 
-// Share of the device one registration keeps busy on its own: its voxel passes are persistent
-// grids that fill every SM once the finest level has a few million voxels; smaller volumes leave
-// most of the device idle (latency-bound launches), so several of them overlap well.
-constexpr double kFillVoxels = 2.0 * 1024 * 1024;
-constexpr double kLoadCap = 2.0;  // admitted load, in whole devices
-
 struct Job {
     int64_t ticket = 0;
     nrb_pair pair{};
     nrb_f3d_params params{};
     int64_t footprint = 0;
-    double load = 0;
     Clock::time_point submitted, started, finished;
     bool done = false;
     bool claimed = false;  // a nrb_server_wait call owns this ticket
@@ -106,23 +100,57 @@ void pool_release(int dev) {
 
 }  // namespace
 
+// parameters two requests must share to run in one group
+static bool same_params(const nrb_f3d_params& a, const nrb_f3d_params& b) {
+    auto feq = [](float x, float y) { return x == y || (x != x && y != y); };
+    for (int i = 0; i < 3; ++i)
+        if (!feq(a.spacing[i], b.spacing[i])) return false;
+    return a.levels == b.levels && a.max_iterations == b.max_iterations && feq(a.bending_energy, b.bending_energy) &&
+           a.ref_bins == b.ref_bins && a.flo_bins == b.flo_bins && feq(a.padding, b.padding) &&
+           a.floating_margin == b.floating_margin && a.batch_gradient_percent == b.batch_gradient_percent &&
+           a.verbose == b.verbose;
+}
+
+static int64_t voxels_of(const nrb_pair& p) { return (int64_t)p.dim[0] * p.dim[1] * p.dim[2]; }
+
 struct nrb_server {
     int device = 0;
     int64_t budget = 0;
+    int max_group = 16;
     std::mutex mu;
     std::condition_variable cv;
     std::deque<Job *> queue;
     std::map<int64_t, Job *> jobs;
     std::vector<std::thread> workers;
     int64_t next_ticket = 1, used = 0, peak_used = 0;
-    int active = 0, peak_active = 0;
-    double load = 0;
+    int active = 0, peak_active = 0, peak_group = 0;
     bool stop = false;
 
-    // the head of the queue fits: memory, and device load (always admitted when nothing runs)
-    bool head_fits() const {
-        const Job *j = queue.front();
-        return used + j->footprint <= budget && (active == 0 || load + j->load <= kLoadCap);
+    // the head of the queue fits in the budget (always admitted when nothing runs, so a request
+    // the size of the whole budget still runs)
+    bool head_fits() const { return active == 0 || used + queue.front()->footprint <= budget; }
+
+    // the head and the queued requests that can share its group, removed from the queue
+    std::vector<Job *> take_group() {
+        std::vector<Job *> g;
+        Job *head = queue.front();
+        queue.pop_front();
+        g.push_back(head);
+        int64_t bytes = head->footprint;
+        const int64_t hv = voxels_of(head->pair);
+        for (auto it = queue.begin(); it != queue.end() && (int)g.size() < max_group;) {
+            Job *j = *it;
+            const int64_t v = voxels_of(j->pair);
+            if (same_params(j->params, head->params) && v <= 2 * hv && hv <= 2 * v &&
+                used + bytes + j->footprint <= budget) {
+                g.push_back(j);
+                bytes += j->footprint;
+                it = queue.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        return g;
     }
 
     void worker() {
@@ -130,35 +158,44 @@ struct nrb_server {
         cudaStream_t st = nullptr;
         const bool have_stream = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
         for (;;) {
-            Job *job = nullptr;
+            std::vector<Job *> group;
             {
                 std::unique_lock<std::mutex> lock(mu);
                 // FIFO admission: the head waits for memory rather than being overtaken
                 cv.wait(lock, [&] { return (stop && queue.empty()) || (!queue.empty() && head_fits()); });
                 if (queue.empty()) break;  // stopping and drained
-                job = queue.front();
-                queue.pop_front();
-                used += job->footprint;
-                load += job->load;
-                ++active;
+                group = take_group();
+                for (Job *j : group) used += j->footprint;
+                active += (int)group.size();
                 peak_used = std::max(peak_used, used);
                 peak_active = std::max(peak_active, active);
+                peak_group = std::max(peak_group, (int)group.size());
             }
-            job->started = Clock::now();
+            const auto started = Clock::now();
+            std::vector<nrb_pair> pairs;
+            std::vector<nrb_f3d_result> results(group.size());
+            for (Job *j : group) {
+                j->started = started;
+                pairs.push_back(j->pair);
+            }
             nrb_status s = have_stream ? NRB_OK : fail(NRB_ERR_CUDA, "server: stream creation failed");
             if (s == NRB_OK)
-                s = register_on_stream(job->pair.ref_host, job->pair.flo_host, job->pair.dim, job->pair.pixdim,
-                                       &job->params, job->pair.cpp_out_host, job->pair.cpp_capacity, &job->result, st);
+                s = register_batch_fused(pairs.data(), (int)pairs.size(), &group[0]->params, results.data(), st,
+                                         group[0]->params.batch_gradient_percent);
             const std::string err = s == NRB_OK ? std::string() : std::string(nrb_last_error());
             {
                 std::lock_guard<std::mutex> lock(mu);
-                job->finished = Clock::now();
-                job->status = s;
-                job->error = err;
-                job->done = true;
-                used -= job->footprint;
-                load -= job->load;
-                --active;
+                const auto finished = Clock::now();
+                for (size_t i = 0; i < group.size(); ++i) {
+                    Job *j = group[i];
+                    j->finished = finished;
+                    j->status = s;
+                    j->error = err;
+                    j->result = results[i];
+                    j->done = true;
+                    used -= j->footprint;
+                }
+                active -= (int)group.size();
             }
             cv.notify_all();
         }
@@ -174,13 +211,20 @@ extern "C" nrb_status nrb_f3d_footprint(const int32_t dim[3], const float pixdim
 }
 
 extern "C" nrb_status nrb_server_create(int slots, int64_t hbm_budget_bytes, nrb_server **out) {
+    return nrb_server_create_grouped(slots, 16, hbm_budget_bytes, out);
+}
+
+extern "C" nrb_status nrb_server_create_grouped(int slots, int max_group, int64_t hbm_budget_bytes, nrb_server **out) {
     if (!out || slots < 1 || slots > 256) return fail(NRB_ERR_INVALID, "nrb_server_create: slots must be in [1, 256]");
+    if (max_group < 1 || max_group > BATCH_MAX_PAIRS)
+        return fail(NRB_ERR_INVALID, "nrb_server_create: max_group must be in [1, " + std::to_string(BATCH_MAX_PAIRS) + "]");
     int dev = 0;
     NRB_CUDA(cudaGetDevice(&dev));
     size_t free_b = 0, total_b = 0;
     NRB_CUDA(cudaMemGetInfo(&free_b, &total_b));
     nrb_server *s = new nrb_server();
     s->device = dev;
+    s->max_group = max_group;
     s->budget = hbm_budget_bytes > 0 ? hbm_budget_bytes : (int64_t)(0.8 * (double)free_b);
     pool_acquire(dev, s->budget);
     for (int i = 0; i < slots; ++i) s->workers.emplace_back([s] { s->worker(); });
@@ -199,7 +243,10 @@ extern "C" nrb_status nrb_server_submit(nrb_server *s, const nrb_pair *req, cons
     job->pair = *req;
     job->params = *p;
     job->footprint = registration_footprint(req->dim, req->pixdim, p);
-    job->load = std::min(1.0, (double)req->dim[0] * req->dim[1] * req->dim[2] / kFillVoxels);
+    if (p->batch_gradient_percent < 1 || p->batch_gradient_percent > 100) {
+        delete job;
+        return fail(NRB_ERR_INVALID, "nrb_server_submit: batch_gradient_percent in [1, 100]");
+    }
     if (job->footprint > s->budget) {
         delete job;
         return fail(NRB_ERR_OOM, "nrb_server_submit: request larger than the server's HBM budget");
@@ -247,6 +294,13 @@ extern "C" nrb_status nrb_server_stats(nrb_server *s, int64_t *peak_bytes, int32
     std::lock_guard<std::mutex> lock(s->mu);
     if (peak_bytes) *peak_bytes = s->peak_used;
     if (peak_active) *peak_active = s->peak_active;
+    return NRB_OK;
+}
+
+extern "C" nrb_status nrb_server_peak_group(nrb_server *s, int32_t *peak_group) {
+    if (!s || !peak_group) return fail(NRB_ERR_INVALID, "nrb_server_peak_group: null pointer");
+    std::lock_guard<std::mutex> lock(s->mu);
+    *peak_group = s->peak_group;
     return NRB_OK;
 }
 

@@ -1279,6 +1279,7 @@ k_b_gradient(const BatchPair *__restrict__ pairs, const OptState *__restrict__ s
 __global__ void __cluster_dims__(FIN_CLUSTER, 1, 1) __launch_bounds__(FIN_CTA_THREADS)
 k_b_finalize(const BatchPair *__restrict__ pairs, OptState *__restrict__ states, int npairs,
              BatchCtl *__restrict__ bctl, cudaGraphConditionalHandle grad_if, cudaGraphConditionalHandle outer) {
+    pdl_wait();  // the counts come from the objective pass
     cg::cluster_group cluster = cg::this_cluster();
     const int p = blockIdx.x / FIN_CLUSTER;
     const int phase = states[p].phase;
@@ -1581,9 +1582,8 @@ nrb_status launch_batch_gradient(const BatchPair *d_pairs, const OptState *state
 nrb_status launch_batch_finalize(const BatchPair *d_pairs, OptState *states, BatchCtl *bctl, const BatchLaunch& L,
                                  cudaGraphConditionalHandle grad_if, cudaGraphConditionalHandle outer,
                                  cudaStream_t st) {
-    k_b_finalize<<<FIN_CLUSTER * L.npairs, FIN_CTA_THREADS, L.fin_smem, st>>>(d_pairs, states, L.npairs, bctl,
-                                                                              grad_if, outer);
-    NRB_CUDA(cudaGetLastError());
+    NRB_CUDA(launch_pdl(true, k_b_finalize, dim3(FIN_CLUSTER * L.npairs), dim3(FIN_CTA_THREADS), L.fin_smem, st,
+                        d_pairs, states, L.npairs, bctl, grad_if, outer));
     NRB_LAUNCHED("k_b_finalize");
     return NRB_OK;
 }

@@ -78,7 +78,8 @@ def test_server_mix_equals_plain(pairs, plain):
         tickets = [srv.submit(p.reference, p.floating, p.pixdim, _params()) for p in pairs * 2]
         outs = [srv.wait(t) for t in tickets]
         _, peak_active = srv.stats()
-    assert peak_active >= 2
+        peak_group = srv.peak_group()
+    assert peak_active >= 2 and peak_group >= 2
     for i, (cpp, res, q, lat) in enumerate(outs):
         _same((cpp, res), plain[i % len(pairs)])
         assert lat >= q >= 0.0
