@@ -56,6 +56,8 @@ def parse():
                     help="batched: run a level's gradient stage once this share of the active pairs waits for it")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--batch-only", action="store_true", help="batched: skip the one-by-one run (profiling)")
+    ap.add_argument("--kernel-timing", action="store_true",
+                    help="batched: run the batch once more driven from the host with per-kernel CUDA events")
     ap.add_argument("--requests", type=int, default=2000,
                     help="served: requests over the whole sweep, split across the rates in proportion to "
                          "the rate (every rate runs for about the same time)")
@@ -533,8 +535,24 @@ def run_batched(args):
     batched = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], bparams, args.concurrency)
     t_batch = time.perf_counter() - t0
     clocks = sampler.stop()
+    kt = None
+    if args.kernel_timing:
+        # the same batch once more, driven from the host with every launch bracketed by events
+        nrb.timing_enable(True)
+        nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], bparams, args.concurrency)
+        torch.cuda.synchronize()
+        raw = {k: nrb.timing_read(k) for k in ("objective", "gradient", "finalize", "conv", "be_value", "be_gradient")}
+        nrb.timing_enable(False)
+        peak, _ = peaks()
+        tot = sum(v[1] for v in raw.values())
+        kt = {k: {"launches": v[0], "ms": round(v[1], 3), "share": round(v[1] / tot, 4) if tot else None,
+                  "avg_us": round(v[1] / v[0] * 1e3, 2) if v[0] else None,
+                  "GBps": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] and v[2] else None,
+                  "frac_of_measured_hbm": round(v[2] / (v[1] / 1e3) / 1e9 / peak, 4) if v[1] and v[2] else None}
+              for k, v in raw.items()}
     if args.batch_only:
-        print(json.dumps({"mode": "batched", "batch_only": True, "value": args.pairs / t_batch, "seconds": t_batch}))
+        print(json.dumps({"mode": "batched", "batch_only": True, "value": args.pairs / t_batch, "seconds": t_batch,
+                          "kernel_timing": kt}))
         return 0
     dnmi = max(abs(a[1].final_nmi - b[1].final_nmi) for a, b in zip(plain, batched))
     identical = all(np.array_equal(a[0], b[0]) for a, b in zip(plain, batched))

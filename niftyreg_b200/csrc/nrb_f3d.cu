@@ -195,7 +195,7 @@ k_node_tail(long long nnode, float *__restrict__ g, float *__restrict__ g1, floa
 // after a restart, or DONE); the last cluster sets whether the level goes on.
 __global__ void __cluster_dims__(TAIL_CTAS, 1, 1) __launch_bounds__(TAIL_THREADS)
 k_b_node_tail(const BatchPair *__restrict__ pairs, OptState *__restrict__ states, int npairs,
-              BatchCtl *__restrict__ bctl, cudaGraphConditionalHandle outer) {
+              BatchCtl *__restrict__ bctl, int in_graph, cudaGraphConditionalHandle outer) {
     cg::cluster_group cluster = cg::this_cluster();
     const int p = blockIdx.x / TAIL_CTAS;
     if (states[p].phase == PH_GRAD) {
@@ -213,7 +213,10 @@ k_b_node_tail(const BatchPair *__restrict__ pairs, OptState *__restrict__ states
     if (!batch_last_cluster(&bctl->ticket_tail, gridDim.x / TAIL_CTAS)) return;
     int nline, ngrad;
     batch_counts(states, npairs, nline, ngrad);
-    if (threadIdx.x == 0) cudaGraphSetConditional(outer, nline + ngrad > 0 ? 1u : 0u);
+    if (threadIdx.x == 0) {
+        if (in_graph) cudaGraphSetConditional(outer, nline + ngrad > 0 ? 1u : 0u);
+        bctl->go_on = nline + ngrad > 0;
+    }
 }
 
 // StoreCurrentDof after an accepted step: best = best + (-len) * grad, the trial position the
@@ -1403,10 +1406,6 @@ extern "C" nrb_status nrb_f3d_register_files(const char *ref_path, const char *f
 // ---------------------------------------------------------------------------------------------
 namespace {
 
-nrb_status batch_gradient_voxels(const BatchPair *d, const OptState *states, cudaStream_t st, void *arg) {
-    return launch_batch_gradient(d, states, *static_cast<const BatchLaunch *>(arg), st);
-}
-
 // One level of reg_base::Run for every pair, as one CUDA graph:
 //   WHILE(any pair active) {
 //       [bending-energy value || objective] of the pairs in INIT / LINE, one launch each;
@@ -1471,8 +1470,80 @@ struct BatchLevelRunner {
         return s;
     }
 
+    // the line-search stage: [bending-energy value || objective] -> finalize
+    nrb_status line_stage(std::vector<BatchPair>& hp, const BatchLaunch& L, const BatchPair *d_pairs,
+                          OptState *d_states, BatchCtl *d_ctl, cudaStream_t s, bool in_graph,
+                          cudaGraphConditionalHandle h_grad, cudaGraphConditionalHandle h_outer, double obj_bytes) {
+        const bool be = hp[0].be_w > 0;
+        if (be) {
+            NRB_CUDA(cudaEventRecord(ev_fork, s));
+            NRB_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
+            NRB_TRY(launch_batch_be_value(hp, d_pairs, d_states, side));
+            NRB_CUDA(cudaEventRecord(ev_join, side));
+        }
+        NRB_TRY(launch_batch_objective(d_pairs, d_states, L, s, obj_bytes));
+        if (be) NRB_CUDA(cudaStreamWaitEvent(s, ev_join, 0));
+        return launch_batch_finalize(d_pairs, d_states, d_ctl, L, in_graph, h_grad, h_outer, s);
+    }
+
+    // the gradient stage: [bending-energy derivatives || voxel gradient -> node convolution] ->
+    // bending-energy gradient -> node tail
+    nrb_status gradient_stage(std::vector<BatchPair>& hp, const BatchLaunch& L, const BatchPair *d_pairs,
+                              OptState *d_states, BatchCtl *d_ctl, cudaStream_t s, bool in_graph,
+                              cudaGraphConditionalHandle h_outer, double grad_bytes) {
+        struct Arg {
+            const BatchLaunch *L;
+            double bytes;
+        } arg{ &L, grad_bytes };
+        auto voxels = [](const BatchPair *d, const OptState *states, cudaStream_t st, void *a) {
+            const Arg *x = static_cast<const Arg *>(a);
+            return launch_batch_gradient(d, states, *x->L, st, x->bytes);
+        };
+        NRB_TRY(launch_batch_node_stage(hp, d_pairs, d_states, s, side, ev_fork, ev_join, voxels, &arg));
+        k_b_node_tail<<<TAIL_CTAS * L.npairs, TAIL_THREADS, 0, s>>>(d_pairs, d_states, L.npairs, d_ctl, in_graph ? 1 : 0,
+                                                                  h_outer);
+        NRB_CUDA(cudaGetLastError());
+        NRB_LAUNCHED("k_b_node_tail");
+        return NRB_OK;
+    }
+
+    // The level driven from the host, one synchronising read of the decisions per stage (per-
+    // kernel timing is on): the same kernels and the same decisions as the graph.
+    nrb_status host_driven(std::vector<BatchPair>& hp, const BatchLaunch& L, const BatchPair *d_pairs,
+                           OptState *d_states, BatchCtl *d_ctl) {
+        const int np = (int)hp.size();
+        std::vector<OptState> cur(np);
+        for (;;) {
+            NRB_CUDA(cudaMemcpyAsync(cur.data(), d_states, np * sizeof(OptState), cudaMemcpyDeviceToHost, st));
+            NRB_CUDA(cudaStreamSynchronize(st));
+            double ob = 0;
+            for (int i = 0; i < np; ++i)
+                if (cur[i].phase == PH_INIT || cur[i].phase == PH_LINE)
+                    ob += 8.0 * ((double)hp[i].rdim[0] * hp[i].rdim[1] * hp[i].rdim[2]) + 12.0 * (double)hp[i].nnode;
+            NRB_TRY(line_stage(hp, L, d_pairs, d_states, d_ctl, st, false, 0, 0, ob));
+            BatchCtl c;
+            NRB_CUDA(cudaMemcpyAsync(&c, d_ctl, sizeof(c), cudaMemcpyDeviceToHost, st));
+            NRB_CUDA(cudaMemcpyAsync(cur.data(), d_states, np * sizeof(OptState), cudaMemcpyDeviceToHost, st));
+            NRB_CUDA(cudaStreamSynchronize(st));
+            if (c.run_grad) {
+                double gb = 0;
+                for (int i = 0; i < np; ++i)
+                    if (cur[i].phase == PH_GRAD)
+                        gb += 20.0 * ((double)hp[i].rdim[0] * hp[i].rdim[1] * hp[i].rdim[2]) + 12.0 * (double)hp[i].nnode;
+                NRB_TRY(gradient_stage(hp, L, d_pairs, d_states, d_ctl, st, false, 0, gb));
+                NRB_CUDA(cudaMemcpyAsync(&c, d_ctl, sizeof(c), cudaMemcpyDeviceToHost, st));
+                NRB_CUDA(cudaStreamSynchronize(st));
+            }
+            if (!c.go_on) return NRB_OK;
+        }
+    }
+
     nrb_status capture_and_run(std::vector<BatchPair>& hp, const BatchLaunch& L, const BatchPair *d_pairs,
                                OptState *d_states, BatchCtl *d_ctl, int64_t *launches) {
+        if (timing_enabled()) {
+            if (launches) *launches = 0;
+            return host_driven(hp, L, d_pairs, d_states, d_ctl);
+        }
         GraphHolder top;
         cudaGraph_t while_body = nullptr, if_body = nullptr;
         cudaGraphConditionalHandle h_outer, h_grad;
@@ -1493,38 +1564,18 @@ struct BatchLevelRunner {
         }
         NRB_CUDA(cudaStreamEndCapture(cap, &top.g));
         NRB_CUDA(cudaGraphConditionalHandleCreate(&h_grad, while_body, 0, cudaGraphCondAssignDefault));
-        // the line-search stage
+        // the line-search stage, then the IF node of the gradient stage
         NRB_CUDA(cudaStreamBeginCaptureToGraph(cap, while_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         {
-            nrb_status e = NRB_OK;
-            const bool be = hp[0].be_w > 0;
-            if (be) {
-                if (cudaEventRecord(ev_fork, cap) != cudaSuccess || cudaStreamWaitEvent(side, ev_fork, 0) != cudaSuccess)
-                    e = fail(NRB_ERR_CUDA, "batched level: fork");
-                if (e == NRB_OK) e = launch_batch_be_value(hp, d_pairs, d_states, side);
-                if (e == NRB_OK && cudaEventRecord(ev_join, side) != cudaSuccess)
-                    e = fail(NRB_ERR_CUDA, "batched level: join");
-            }
-            if (e == NRB_OK) e = launch_batch_objective(d_pairs, d_states, L, cap);
-            if (e == NRB_OK && be && cudaStreamWaitEvent(cap, ev_join, 0) != cudaSuccess)
-                e = fail(NRB_ERR_CUDA, "batched level: join");
-            if (e == NRB_OK) e = launch_batch_finalize(d_pairs, d_states, d_ctl, L, h_grad, h_outer, cap);
+            nrb_status e = line_stage(hp, L, d_pairs, d_states, d_ctl, cap, true, h_grad, h_outer, 0.0);
             if (e == NRB_OK) e = capture_if(cap, h_grad, &if_body);
             if (e != NRB_OK) return abort_capture(e);
         }
         NRB_CUDA(cudaStreamEndCapture(cap, &while_body));
         const long long c_line = g_launch_count.load() - c0;
-        // the gradient stage
         NRB_CUDA(cudaStreamBeginCaptureToGraph(cap, if_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         {
-            nrb_status e = launch_batch_node_stage(hp, d_pairs, d_states, cap, side, ev_fork, ev_join,
-                                                   batch_gradient_voxels, const_cast<BatchLaunch *>(&L));
-            if (e == NRB_OK) {
-                k_b_node_tail<<<TAIL_CTAS * L.npairs, TAIL_THREADS, 0, cap>>>(d_pairs, d_states, L.npairs, d_ctl,
-                                                                            h_outer);
-                g_launch_count.fetch_add(1);
-                if (cudaGetLastError() != cudaSuccess) e = fail(NRB_ERR_CUDA, "batched level: node tail launch");
-            }
+            nrb_status e = gradient_stage(hp, L, d_pairs, d_states, d_ctl, cap, true, h_outer, 0.0);
             if (e != NRB_OK) return abort_capture(e);
         }
         NRB_CUDA(cudaStreamEndCapture(cap, &if_body));

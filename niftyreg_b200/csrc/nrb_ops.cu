@@ -396,8 +396,9 @@ __global__ void __launch_bounds__(NRB_RED_THREADS)
 k_b_be_value(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs, BeBasis B) {
     __shared__ BatchList L;
     __shared__ double red[NRB_RED_THREADS];
-    batch_list_build(pairs, states, npairs, (1u << PH_INIT) | (1u << PH_LINE),
-                     [](const BatchPair& b, int& u, int& w) {
+    batch_list_build(states, npairs, (1u << PH_INIT) | (1u << PH_LINE),
+                     [&](int q, int& u, int& w) {
+                         const BatchPair& b = pairs[q];
                          u = b.be_w > 0 ? b.n_be : 0;
                          w = 1;
                      }, L);
@@ -424,8 +425,9 @@ k_b_be_value(const BatchPair *__restrict__ pairs, const OptState *__restrict__ s
 __global__ void k_b_be_derivatives(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states,
                                    int npairs, BeBasis B) {
     __shared__ BatchList L;
-    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
-                     [](const BatchPair& b, int& u, int& w) {
+    batch_list_build(states, npairs, 1u << PH_GRAD,
+                     [&](int q, int& u, int& w) {
+                         const BatchPair& b = pairs[q];
                          u = b.be_w > 0 ? (int)b.nnode : 0;
                          w = 1;
                      }, L);
@@ -438,8 +440,9 @@ __global__ void k_b_be_derivatives(const BatchPair *__restrict__ pairs, const Op
 __global__ void k_b_be_accumulate(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states,
                                   int npairs, BeBasis B) {
     __shared__ BatchList L;
-    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
-                     [](const BatchPair& b, int& u, int& w) {
+    batch_list_build(states, npairs, 1u << PH_GRAD,
+                     [&](int q, int& u, int& w) {
+                         const BatchPair& b = pairs[q];
                          u = b.be_w > 0 ? (int)b.nnode : 0;
                          w = 1;
                      }, L);
@@ -454,8 +457,9 @@ __global__ void __launch_bounds__(CONV_X_THREADS)
 k_b_conv_x(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
     extern __shared__ float rows[];
     __shared__ BatchList L;
-    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
-                     [](const BatchPair& b, int& u, int& w) {
+    batch_list_build(states, npairs, 1u << PH_GRAD,
+                     [&](int q, int& u, int& w) {
+                         const BatchPair& b = pairs[q];
                          u = b.xblocks;
                          w = 1;
                      }, L);
@@ -473,8 +477,9 @@ k_b_conv_x(const BatchPair *__restrict__ pairs, const OptState *__restrict__ sta
 // [3][nsz][nsy * nsx]) of the node convolution, element-wise
 __global__ void k_b_conv_y(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
     __shared__ BatchList L;
-    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
-                     [](const BatchPair& b, int& u, int& w) {
+    batch_list_build(states, npairs, 1u << PH_GRAD,
+                     [&](int q, int& u, int& w) {
+                         const BatchPair& b = pairs[q];
                          u = 3 * b.rdim[2] * b.ns[1] * b.ns[0];
                          w = 1;
                      }, L);
@@ -487,8 +492,9 @@ __global__ void k_b_conv_y(const BatchPair *__restrict__ pairs, const OptState *
 
 __global__ void k_b_conv_z(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
     __shared__ BatchList L;
-    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
-                     [](const BatchPair& b, int& u, int& w) {
+    batch_list_build(states, npairs, 1u << PH_GRAD,
+                     [&](int q, int& u, int& w) {
+                         const BatchPair& b = pairs[q];
                          u = 3 * b.ns[2] * b.ns[1] * b.ns[0];
                          w = 1;
                      }, L);
@@ -502,8 +508,9 @@ __global__ void k_b_conv_z(const BatchPair *__restrict__ pairs, const OptState *
 // node sampling, reorientation and weighting (overwrites the node gradient)
 __global__ void k_b_nodes(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
     __shared__ BatchList L;
-    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
-                     [](const BatchPair& b, int& u, int& w) {
+    batch_list_build(states, npairs, 1u << PH_GRAD,
+                     [&](int q, int& u, int& w) {
+                         const BatchPair& b = pairs[q];
                          u = (int)b.nnode;
                          w = 1;
                      }, L);
@@ -1443,6 +1450,7 @@ nrb_status launch_batch_be_value(const std::vector<BatchPair>& hp, const BatchPa
     long long units = 0;
     for (const BatchPair& b : hp) units += b.n_be;
     const int grid = (int)std::max(1LL, std::min(units, 8LL * sm_count()));
+    KernelTimer timer(TK_BE_VALUE, 0.0, st);
     k_b_be_value<<<grid, NRB_RED_THREADS, 0, st>>>(d, states, (int)hp.size(), be_basis());
     NRB_CUDA(cudaGetLastError());
     NRB_LAUNCHED("k_b_be_value");
@@ -1460,6 +1468,7 @@ nrb_status launch_batch_node_stage(const std::vector<BatchPair>& hp, const Batch
         NRB_CUDA(cudaEventRecord(fork, st));
         NRB_CUDA(cudaStreamWaitEvent(side, fork, 0));
         const int g = batch_grid(hp, [](const BatchPair& b) { return b.nnode; }, 128, 16);
+        KernelTimer timer(TK_BE_GRADIENT, 0.0, side);
         k_b_be_derivatives<<<g, 128, 0, side>>>(d, states, np, be_basis());
         NRB_CUDA(cudaGetLastError());
         NRB_LAUNCHED("k_b_be_derivatives");
@@ -1479,6 +1488,8 @@ nrb_status launch_batch_node_stage(const std::vector<BatchPair>& hp, const Batch
     int per = 0;
     NRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_b_conv_x, CONV_X_THREADS, smem));
     const int xg = (int)std::max(1LL, std::min(xb, (long long)std::max(1, per) * sm_count()));
+    {
+    KernelTimer timer(TK_CONV, 0.0, st);
     k_b_conv_x<<<xg, CONV_X_THREADS, smem, st>>>(d, states, np);
     NRB_CUDA(cudaGetLastError());
     NRB_LAUNCHED("k_b_conv_x");
@@ -1494,10 +1505,12 @@ nrb_status launch_batch_node_stage(const std::vector<BatchPair>& hp, const Batch
     k_b_nodes<<<gn, 256, 0, st>>>(d, states, np);
     NRB_CUDA(cudaGetLastError());
     NRB_LAUNCHED("k_b_nodes");
+    }
     if (be) {
         NRB_CUDA(cudaEventRecord(join, side));
         NRB_CUDA(cudaStreamWaitEvent(st, join, 0));
         const int g = batch_grid(hp, [](const BatchPair& b) { return b.nnode; }, 128, 16);
+        KernelTimer timer2(TK_BE_GRADIENT, 0.0, st);
         k_b_be_accumulate<<<g, 128, 0, st>>>(d, states, np, be_basis());
         NRB_CUDA(cudaGetLastError());
         NRB_LAUNCHED("k_b_be_accumulate");

@@ -137,12 +137,36 @@ struct BatchPair {
     int obj_items, grad_items, xblocks;
 };
 
-constexpr int BATCH_MAX_PAIRS = 128;
+constexpr int BATCH_MAX_PAIRS = 64;
+
+// Per-pair tables of the batched voxel passes, passed whole as __grid_constant__ kernel
+// parameters: a pair's walk and pointers are then read with uniform constant-bank loads, with no
+// copy into shared memory and nothing held in registers.
+struct BatchObjEntry {
+    WalkParams P;
+    const float *ref, *flo, *best, *grad;
+    uint32_t *hist;
+};
+struct BatchObjTable {
+    BatchObjEntry e[BATCH_MAX_PAIRS];
+};
+struct BatchGradEntry {
+    WalkParams P;
+    const float *ref, *flo, *best;
+    float *vgrad;
+    const double *logt0, *logt1;
+    const nrb_objective *last0, *last1;
+};
+struct BatchGradTable {
+    BatchGradEntry e[BATCH_MAX_PAIRS];
+};
 
 // Launch shapes of a batched level, derived on the host from every pair (shared memory for the
-// largest walk, template choices every pair allows).
+// largest walk, template choices every pair allows), and the voxel passes' tables.
 struct BatchLaunch {
     int npairs = 0;
+    BatchObjTable obj_table;
+    BatchGradTable grad_table;
     bool obj_xs = false, obj_diag = false, grad_f32 = false, grad_diag = false;
     size_t obj_smem = 0, grad_smem = 0, fin_smem = 0;
     int obj_grid = 0, grad_grid = 0;
@@ -163,8 +187,8 @@ struct BatchList {
 };
 
 template <typename F>
-__device__ __forceinline__ void batch_list_build(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states,
-                                                 int npairs, unsigned mask, F units_of, BatchList& L) {
+__device__ __forceinline__ void batch_list_build(const OptState *__restrict__ states, int npairs, unsigned mask,
+                                                 F units_of, BatchList& L) {
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
         int n = 0;
@@ -172,7 +196,7 @@ __device__ __forceinline__ void batch_list_build(const BatchPair *__restrict__ p
         for (int base = 0; base < npairs; base += 32) {
             const int p = base + lane;
             int u = 0, w = 0;
-            if (p < npairs && ((mask >> states[p].phase) & 1u)) units_of(pairs[p], u, w);
+            if (p < npairs && ((mask >> states[p].phase) & 1u)) units_of(p, u, w);
             const long long c = (long long)u * w;
             long long inc = c;
 #pragma unroll
@@ -196,6 +220,34 @@ __device__ __forceinline__ void batch_list_build(const BatchPair *__restrict__ p
             L.total = total;
             L.pref[n] = total;
         }
+    }
+    __syncthreads();
+}
+
+// A block's share of a batched stage as segments (pair, first unit, end unit), in pair order,
+// computed once per block into shared memory so that none of the bookkeeping stays live across
+// the walk of a unit.
+struct BatchSegments {
+    int n;
+    int pair[BATCH_MAX_PAIRS], j0[BATCH_MAX_PAIRS], j1[BATCH_MAX_PAIRS];
+};
+
+__device__ __forceinline__ bool batch_units(const BatchList& L, int k, long long c0, long long c1, int& j0, int& j1);
+
+// the block's equal share of the list's cost (after batch_list_build; ends with a barrier)
+__device__ __forceinline__ void batch_segments(const BatchList& L, BatchSegments& G) {
+    if (threadIdx.x == 0) {
+        const long long c0 = L.total * blockIdx.x / gridDim.x, c1 = L.total * (blockIdx.x + 1) / gridDim.x;
+        int n = 0;
+        for (int k = 0; k < L.n; ++k) {
+            int j0, j1;
+            if (!batch_units(L, k, c0, c1, j0, j1)) continue;
+            G.pair[n] = L.pair[k];
+            G.j0[n] = j0;
+            G.j1[n] = j1;
+            ++n;
+        }
+        G.n = n;
     }
     __syncthreads();
 }
@@ -264,6 +316,7 @@ struct BatchCtl {
     unsigned int ticket_fin, ticket_tail;
     int grad_percent;                // run the gradient stage once this share (%) of the active pairs waits for it
     long long iterations, grad_stages;  // graph iterations and gradient stages run (statistics)
+    int run_grad, go_on;             // the last decisions (read by the host when it drives the level)
 };
 
 // One line-search step of Optimiser::Optimise (reg-lib/Optimiser.cpp:140-168) after its
@@ -434,12 +487,14 @@ int be_partial_count(const nrb_geometry *g);
 nrb_status batch_walks(nrb_workspace *ws, const nrb_nmi *nmi, const nrb_geometry *g, float padding, int flo_margin,
                        WalkParams& wo, WalkParams& wg);
 nrb_status batch_plan(std::vector<BatchPair>& pairs, BatchLaunch& L);
+// (bytes: the algorithmic bytes of the launch, for the per-kernel timers when they are on)
 nrb_status launch_batch_objective(const BatchPair *d_pairs, const OptState *states, const BatchLaunch& L,
-                                  cudaStream_t st);
+                                  cudaStream_t st, double bytes = 0.0);
 nrb_status launch_batch_gradient(const BatchPair *d_pairs, const OptState *states, const BatchLaunch& L,
-                                 cudaStream_t st);
+                                 cudaStream_t st, double bytes = 0.0);
+// in_graph: set the level graph's conditions (else the decisions are only left in bctl)
 nrb_status launch_batch_finalize(const BatchPair *d_pairs, OptState *states, BatchCtl *bctl, const BatchLaunch& L,
-                                 cudaGraphConditionalHandle grad_if, cudaGraphConditionalHandle outer,
+                                 bool in_graph, cudaGraphConditionalHandle grad_if, cudaGraphConditionalHandle outer,
                                  cudaStream_t st);
 // batched levels (csrc/nrb_ops.cu): a pair's node-stage description from its workspace, the
 // bending-energy value partials of the pairs in INIT / LINE, and the gradient stage of the pairs in

@@ -1209,36 +1209,32 @@ __global__ void k_nmi_voxel_gradient(long long nv, int rb, int fb, const float *
 // plain k_objective's work per item.
 template <bool kXs, bool kDiag>
 __global__ void __launch_bounds__(32 * TY_OBJECTIVE, 2)
-k_b_objective(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
+k_b_objective(const __grid_constant__ BatchObjTable T, const OptState *__restrict__ states, int npairs) {
     extern __shared__ float4 sm4[];
     __shared__ BatchList L;
-    __shared__ WalkParams sP;
-    batch_list_build(pairs, states, npairs, (1u << PH_INIT) | (1u << PH_LINE),
-                     [](const BatchPair& b, int& u, int& w) {
-                         u = b.wo.nitems;
-                         w = b.wo.zchunk + 6;
+    __shared__ BatchSegments G;
+    batch_list_build(states, npairs, (1u << PH_INIT) | (1u << PH_LINE),
+                     [&](int q, int& u, int& w) {
+                         u = T.e[q].P.nitems;
+                         w = T.e[q].P.zchunk + 6;
                      }, L);
-    const long long c0 = L.total * blockIdx.x / gridDim.x, c1 = L.total * (blockIdx.x + 1) / gridDim.x;
-    for (int k = 0; k < L.n; ++k) {
-        int j0, j1;
-        if (!batch_units(L, k, c0, c1, j0, j1)) continue;
-        const int p = L.pair[k];
-        const BatchPair& B = pairs[p];
-        __syncthreads();  // the previous pair's readers of sP are done
-        copy_words(&sP, &B.wo, sizeof(WalkParams));
-        __syncthreads();
+    batch_segments(L, G);
+    for (int sg = 0; sg < G.n; ++sg) {
+        const int p = G.pair[sg];
         WalkSmem S;
         uint32_t *h;
         float *X;
-        objective_smem(sP, sm4, S, h, X);
-        const int nbins = sP.rb * sP.fb;
+        objective_smem(T.e[p].P, sm4, S, h, X);
+        const int nbins = T.e[p].P.rb * T.e[p].P.fb;
+        __syncthreads();  // the previous pair's flush has read the shared histogram
         zero_hist(h, nbins);  // ordered before the counts by stage_item's first barrier
-        const bool line = states[p].phase == PH_LINE;
-        const float *grad = line ? B.grad : nullptr;
-        const float scale = line ? -states[p].cur_len : 0.f;
-        for (int j = j0; j < j1; ++j)
-            objective_item<kXs, kDiag>(sP, S, h, X, j, B.ref, B.flo, nullptr, B.best, grad, scale);
-        flush_hist(h, nbins, B.hist);
+        for (int j = G.j0[sg]; j < G.j1[sg]; ++j) {
+            const int q = G.pair[sg];
+            const bool line = states[q].phase == PH_LINE;
+            objective_item<kXs, kDiag>(T.e[q].P, S, h, X, j, T.e[q].ref, T.e[q].flo, nullptr, T.e[q].best,
+                                       line ? T.e[q].grad : nullptr, line ? -states[q].cur_len : 0.f);
+        }
+        flush_hist(h, nbins, T.e[G.pair[sg]].hist);
     }
 }
 
@@ -1246,29 +1242,26 @@ k_b_objective(const BatchPair *__restrict__ pairs, const OptState *__restrict__ 
 // position (the plain k_gradient's work per item).
 template <bool kF32, bool kDiag>
 __global__ void __launch_bounds__(32 * TY_GRADIENT, kF32 ? 6 : 4)
-k_b_gradient(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs) {
+k_b_gradient(const __grid_constant__ BatchGradTable T, const OptState *__restrict__ states, int npairs) {
     extern __shared__ float4 sm4[];
     __shared__ BatchList L;
-    __shared__ WalkParams sP;
-    batch_list_build(pairs, states, npairs, 1u << PH_GRAD,
-                     [](const BatchPair& b, int& u, int& w) {
-                         u = b.wg.nitems;
-                         w = b.wg.zchunk + 4;
+    __shared__ BatchSegments G;
+    batch_list_build(states, npairs, 1u << PH_GRAD,
+                     [&](int q, int& u, int& w) {
+                         u = T.e[q].P.nitems;
+                         w = T.e[q].P.zchunk + 4;
                      }, L);
-    const long long c0 = L.total * blockIdx.x / gridDim.x, c1 = L.total * (blockIdx.x + 1) / gridDim.x;
-    for (int k = 0; k < L.n; ++k) {
-        int j0, j1;
-        if (!batch_units(L, k, c0, c1, j0, j1)) continue;
-        const int p = L.pair[k];
-        const BatchPair& B = pairs[p];
-        __syncthreads();
-        copy_words(&sP, &B.wg, sizeof(WalkParams));
-        __syncthreads();
-        const WalkSmem S = walk_smem(sP, sm4);
-        const GradientTables T = gradient_tables(B.logt0, B.last0, B.logt1, B.last1, states[p].best_buf == 1, 1.0);
+    batch_segments(L, G);
+    for (int sg = 0; sg < G.n; ++sg) {
+        const int p = G.pair[sg];
+        const BatchGradEntry& E = T.e[p];
+        const WalkSmem S = walk_smem(E.P, sm4);
+        const GradientTables N = gradient_tables(E.logt0, E.last0, E.logt1, E.last1, states[p].best_buf == 1, 1.0);
         float *logf = reinterpret_cast<float *>(S.tail);
-        if (kF32) stage_log_table(sP, T.logt, logf);  // visible after stage_item's first barrier
-        for (int j = j0; j < j1; ++j) gradient_item<kF32, kDiag>(sP, S, logf, T, j, B.ref, B.flo, nullptr, B.best, B.vgrad);
+        __syncthreads();  // the previous pair's walk is done with the shared tables
+        if (kF32) stage_log_table(E.P, N.logt, logf);  // visible after stage_item's first barrier
+        for (int j = G.j0[sg]; j < G.j1[sg]; ++j)
+            gradient_item<kF32, kDiag>(E.P, S, logf, N, j, E.ref, E.flo, nullptr, E.best, E.vgrad);
     }
 }
 
@@ -1278,7 +1271,8 @@ k_b_gradient(const BatchPair *__restrict__ pairs, const OptState *__restrict__ s
 // for it, or no pair has a line-search step left) and whether the level goes on.
 __global__ void __cluster_dims__(FIN_CLUSTER, 1, 1) __launch_bounds__(FIN_CTA_THREADS)
 k_b_finalize(const BatchPair *__restrict__ pairs, OptState *__restrict__ states, int npairs,
-             BatchCtl *__restrict__ bctl, cudaGraphConditionalHandle grad_if, cudaGraphConditionalHandle outer) {
+             BatchCtl *__restrict__ bctl, int in_graph, cudaGraphConditionalHandle grad_if,
+             cudaGraphConditionalHandle outer) {
     pdl_wait();  // the counts come from the objective pass
     cg::cluster_group cluster = cg::this_cluster();
     const int p = blockIdx.x / FIN_CLUSTER;
@@ -1314,10 +1308,14 @@ k_b_finalize(const BatchPair *__restrict__ pairs, OptState *__restrict__ states,
     batch_counts(states, npairs, nline, ngrad);
     if (threadIdx.x == 0) {
         const bool run_grad = ngrad > 0 && (100 * ngrad >= bctl->grad_percent * (nline + ngrad) || nline == 0);
-        cudaGraphSetConditional(grad_if, run_grad ? 1u : 0u);
+        if (in_graph) {
+            cudaGraphSetConditional(grad_if, run_grad ? 1u : 0u);
+            cudaGraphSetConditional(outer, nline + ngrad > 0 ? 1u : 0u);
+        }
+        bctl->run_grad = run_grad;
+        bctl->go_on = nline + ngrad > 0;
         bctl->iterations += 1;
         bctl->grad_stages += run_grad ? 1 : 0;
-        cudaGraphSetConditional(outer, nline + ngrad > 0 ? 1u : 0u);
     }
 }
 
@@ -1540,9 +1538,27 @@ nrb_status batch_plan(std::vector<BatchPair>& pairs, BatchLaunch& L) {
     L.grad_smem = gsm + (f32 ? (size_t)(rb * fb + rb + fb) * sizeof(float) : 0);
     const int rpc = (fb + FIN_CLUSTER - 1) / FIN_CLUSTER;
     L.fin_smem = (size_t)(2 * rpc + 2) * rb * sizeof(double);
-    for (BatchPair& b : pairs) {
+    for (size_t i = 0; i < pairs.size(); ++i) {
+        BatchPair& b = pairs[i];
         b.wo.xs = L.obj_xs;
         b.wg.log_in_smem = f32;
+        BatchObjEntry& o = L.obj_table.e[i];
+        o.P = b.wo;
+        o.ref = b.ref;
+        o.flo = b.flo;
+        o.best = b.best;
+        o.grad = b.grad;
+        o.hist = b.hist;
+        BatchGradEntry& g = L.grad_table.e[i];
+        g.P = b.wg;
+        g.ref = b.ref;
+        g.flo = b.flo;
+        g.best = b.best;
+        g.vgrad = b.vgrad;
+        g.logt0 = b.logt0;
+        g.logt1 = b.logt1;
+        g.last0 = b.last0;
+        g.last1 = b.last1;
     }
     auto ko = L.obj_diag ? (L.obj_xs ? k_b_objective<true, true> : k_b_objective<false, true>)
                          : (L.obj_xs ? k_b_objective<true, false> : k_b_objective<false, false>);
@@ -1560,30 +1576,33 @@ nrb_status batch_plan(std::vector<BatchPair>& pairs, BatchLaunch& L) {
 }
 
 nrb_status launch_batch_objective(const BatchPair *d_pairs, const OptState *states, const BatchLaunch& L,
-                                  cudaStream_t st) {
+                                  cudaStream_t st, double bytes) {
+    KernelTimer timer(TK_OBJECTIVE, bytes, st);
     auto ko = L.obj_diag ? (L.obj_xs ? k_b_objective<true, true> : k_b_objective<false, true>)
                          : (L.obj_xs ? k_b_objective<true, false> : k_b_objective<false, false>);
-    ko<<<L.obj_grid, 32 * TY_OBJECTIVE, L.obj_smem, st>>>(d_pairs, states, L.npairs);
+    ko<<<L.obj_grid, 32 * TY_OBJECTIVE, L.obj_smem, st>>>(L.obj_table, states, L.npairs);
     NRB_CUDA(cudaGetLastError());
     NRB_LAUNCHED("k_b_objective");
     return NRB_OK;
 }
 
 nrb_status launch_batch_gradient(const BatchPair *d_pairs, const OptState *states, const BatchLaunch& L,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, double bytes) {
+    KernelTimer timer(TK_GRADIENT, bytes, st);
     auto kg = L.grad_diag ? (L.grad_f32 ? k_b_gradient<true, true> : k_b_gradient<false, true>)
                           : (L.grad_f32 ? k_b_gradient<true, false> : k_b_gradient<false, false>);
-    kg<<<L.grad_grid, 32 * TY_GRADIENT, L.grad_smem, st>>>(d_pairs, states, L.npairs);
+    kg<<<L.grad_grid, 32 * TY_GRADIENT, L.grad_smem, st>>>(L.grad_table, states, L.npairs);
     NRB_CUDA(cudaGetLastError());
     NRB_LAUNCHED("k_b_gradient");
     return NRB_OK;
 }
 
 nrb_status launch_batch_finalize(const BatchPair *d_pairs, OptState *states, BatchCtl *bctl, const BatchLaunch& L,
-                                 cudaGraphConditionalHandle grad_if, cudaGraphConditionalHandle outer,
+                                 bool in_graph, cudaGraphConditionalHandle grad_if, cudaGraphConditionalHandle outer,
                                  cudaStream_t st) {
-    NRB_CUDA(launch_pdl(true, k_b_finalize, dim3(FIN_CLUSTER * L.npairs), dim3(FIN_CTA_THREADS), L.fin_smem, st,
-                        d_pairs, states, L.npairs, bctl, grad_if, outer));
+    KernelTimer timer(TK_FINALIZE, 0.0, st);
+    NRB_CUDA(launch_pdl(in_graph, k_b_finalize, dim3(FIN_CLUSTER * L.npairs), dim3(FIN_CTA_THREADS), L.fin_smem, st,
+                        d_pairs, states, L.npairs, bctl, in_graph ? 1 : 0, grad_if, outer));
     NRB_LAUNCHED("k_b_finalize");
     return NRB_OK;
 }

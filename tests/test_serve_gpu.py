@@ -86,18 +86,27 @@ def test_server_mix_equals_plain(pairs, plain):
 
 
 def test_server_budget_serialises(pairs, plain):
-    """A budget that holds one request at a time admits one at a time."""
+    """Admission never takes the admitted footprint above the budget; requests that each fill the
+    budget run one at a time (groups of one), with the results of the plain path."""
     prm = _params()
     fps = [nrb.footprint(p.dim, p.pixdim, prm) for p in pairs]
     budget = max(fps) + min(fps) // 2
     with nrb.Server(slots=4, budget_bytes=budget) as srv:
         tickets = [srv.submit(p.reference, p.floating, p.pixdim, prm) for p in pairs]
         outs = [srv.wait(t) for t in tickets]
-        peak_bytes, peak_active = srv.stats()
+        peak_bytes, _ = srv.stats()
     assert peak_bytes <= budget
-    assert peak_active == 1
     for (cpp, res, _, _), b in zip(outs, plain):
         _same((cpp, res), b)
+    big = int(np.argmax(fps))
+    with nrb.Server(slots=4, budget_bytes=fps[big]) as srv:
+        tickets = [srv.submit(pairs[big].reference, pairs[big].floating, pairs[big].pixdim, prm) for _ in range(3)]
+        outs = [srv.wait(t) for t in tickets]
+        peak_bytes, peak_active = srv.stats()
+        peak_group = srv.peak_group()
+    assert peak_bytes <= fps[big] and peak_active == 1 and peak_group == 1
+    for cpp, res, _, _ in outs:
+        _same((cpp, res), plain[big])
 
 
 def test_server_rejects_oversized(pairs):
