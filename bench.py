@@ -11,6 +11,10 @@ control spacing, linear interpolation, NaN padding. A "step" is one whole regist
   python bench.py --mode batched   # many uneven pairs at once vs the same pairs one by one
   python bench.py --mode served    # open-loop Poisson requests: p50/p95/p99 latency
 
+On one GPU the default line also carries the metric's batched and served figures (a 64-pair
+--mode batched run and a two-rate --mode served run, keys "batched", "batched_speedup_vs_plain"
+and "served"; --no-extras skips them).
+
 Under torchrun every rank registers its own pair (replicas: registrations are independent) and
 rank 0 prints one JSON line with the whole-job rate and the slowest rank's device time.
 """
@@ -49,6 +53,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="plain mode: skip the shortened batched and served runs attached to the line")
     ap.add_argument("--mode", choices=["plain", "batched", "served", "warp", "f3d2"], default="plain")
     ap.add_argument("--pairs", type=int, default=64, help="batched: number of pairs")
     ap.add_argument("--concurrency", type=int, default=16, help="batched/served: concurrent registrations")
@@ -467,6 +473,25 @@ def run_b200(args):
                          "gradient_evaluations": results[-1].gradient_evaluations,
                          "step_ms": [round(s, 3) for s in step_ms]},
     }
+    if world == 1 and not args.no_extras:
+        # the metric's batched and served figures (shortened runs of --mode batched / --mode served)
+        import copy
+        ba = copy.copy(args)
+        ba.batch_only, ba.kernel_timing, ba.verbose = False, False, False
+        ba.pairs, ba.concurrency = 64, 64
+        b = run_batched(ba, emit=False)
+        line["batched"] = {k: b[k] for k in ("value", "plain_value", "speedup_vs_plain", "max_abs_dnmi_vs_plain",
+                                             "bitwise_identical_to_plain")}
+        line["batched"]["workload"] = b["config"]["workload"]
+        line["batched_speedup_vs_plain"] = b["speedup_vs_plain"]
+        sa = copy.copy(args)
+        sa.rates, sa.requests = "20,50", 350
+        sv = run_served(sa, emit=False)
+        line["served"] = {"value": sv["value"], "plain_value": sv["plain_value"],
+                          "served_vs_plain_at_saturation": sv["served_vs_plain_at_saturation"],
+                          "sweep": [{k: r[k] for k in ("rate_req_s", "requests", "achieved_req_s", "p50_ms", "p95_ms",
+                                                       "p99_ms", "peak_group")} for r in sv["sweep"]],
+                          "workload": sv["config"]["workload"]}
     if world == 1 and not args.no_cpu_baseline:
         cb = reference_baseline(pair, os.cpu_count() or 1)
         if cb is not None:
@@ -504,7 +529,7 @@ def _gpu_clock_sampler():
     return ClockSampler(torch.cuda.current_device())
 
 
-def run_batched(args):
+def run_batched(args, emit=True):
     """`--pairs` registrations with sizes drawn uniformly from BATCH_SHAPES: first one by one
     through the plain path (nrb_f3d_register_host), then all at once through
     nrb_f3d_register_batch with `--concurrency` registrations in flight. Reports both rates and
@@ -564,11 +589,13 @@ def run_batched(args):
                                    f"counted iterations at the finest level, NMI {BINS} bins, BE {BE}, 5-voxel grid",
                        "concurrency": args.concurrency, "timing": "host wall clock, host images, copies included"},
             "max_abs_dnmi_vs_plain": dnmi, "bitwise_identical_to_plain": identical, "clocks": clocks}
-    print(json.dumps(line))
-    return 0
+    if emit:
+        print(json.dumps(line))
+        return 0
+    return line
 
 
-def run_served(args):
+def run_served(args, emit=True):
     """Open-loop Poisson request streams at each rate of `--rates` (`--requests` in total, split in
     proportion to the rates): sizes drawn from SERVE_MIX, admitted by a server with `--slots`
     workers grouping up to `--max-group` similar requests under 80% of free HBM. Reports latency
@@ -658,8 +685,10 @@ def run_served(args):
                                     "requests of similar size (within 2x voxels) into one batched registration"},
             "served_vs_plain_at_saturation": best["achieved_req_s"] / plain_rate,
             "sweep": results, "clocks": clocks}
-    print(json.dumps(line))
-    return 0
+    if emit:
+        print(json.dumps(line))
+        return 0
+    return line
 
 
 def run_warp(args):

@@ -267,6 +267,10 @@ typedef struct nrb_f3d_params {
                                * once this share (%) of the pairs still active waits for a
                                * gradient, or when no pair has a line-search step left (default
                                * 50; 1..100). Scheduling only: results do not depend on it. */
+    int32_t floating_texture; /* 1 (default): each level's padded floating copy is also held as
+                               * a layered texture, and the fused passes fetch each slice's 2x2
+                               * footprint with one gather; 0: plain loads. The same values are
+                               * read either way, so the results are identical. */
 } nrb_f3d_params;
 
 typedef struct nrb_f3d_result {

@@ -63,7 +63,7 @@ class F3dParams(ctypes.Structure):
                 ("bending_energy", ctypes.c_float), ("spacing", _F3), ("ref_bins", ctypes.c_int32),
                 ("flo_bins", ctypes.c_int32), ("padding", ctypes.c_float), ("verbose", ctypes.c_int32),
                 ("host_loop", ctypes.c_int32), ("floating_margin", ctypes.c_int32),
-                ("batch_gradient_percent", ctypes.c_int32)]
+                ("batch_gradient_percent", ctypes.c_int32), ("floating_texture", ctypes.c_int32)]
 
 
 class Image(ctypes.Structure):

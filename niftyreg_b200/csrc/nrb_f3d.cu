@@ -644,6 +644,7 @@ private:
     // the floating image as the voxel passes read it: flo_org_ is its voxel (0, 0, 0), inside
     // flo_pad_ (a copy with margin_ voxels of padding values on every side) or flo_ (margin 0)
     DevBuf flo_pad_;
+    FloTexture ftex_;  // flo_pad_ as a layered texture (p_.floating_texture)
     const float *flo_org_ = nullptr;
     int margin_ = 0;
     NmiHandle nmi_;
@@ -671,6 +672,7 @@ private:
 
 public:
     ~F3dRegistration() {
+        flo_texture_release(ftex_);
         dev_free(dstate_, st_);
         if (cap_st_) cudaStreamDestroy(cap_st_);
     }
@@ -1038,6 +1040,14 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
         NRB_TRY(pad_volume(flo_.p, fh.dim, margin_, pad_, flo_pad_.p, &flo_org_, st_));
         dev_free(flo_.p, flo_.st);
         flo_.p = nullptr;
+        // the padded copy as a layered texture: the fused passes gather its 2x2 footprints
+        if (p_.floating_texture) {
+            const int w = fh.dim[0] + 2 * margin_, h = fh.dim[1] + 2 * margin_, l = fh.dim[2] + 2 * margin_;
+            flo_texture_release(ftex_);
+            NRB_TRY(flo_texture_acquire(w, h, l, ftex_));
+            NRB_TRY(flo_texture_upload(ftex_, flo_pad_.p, w, h, l, st_));
+            ws_.h->flo_tex = ftex_.tex;
+        }
     } else {
         flo_org_ = flo_.p;
     }
@@ -1263,6 +1273,7 @@ extern "C" void nrb_f3d_default_params(nrb_f3d_params *p) {
     p->host_loop = 0;
     p->floating_margin = 8;
     p->batch_gradient_percent = 50;
+    p->floating_texture = 1;
 }
 
 extern "C" nrb_status nrb_f3d_grid_dims(const int32_t ref_dim[3], const float ref_pixdim[3], const nrb_f3d_params *p,

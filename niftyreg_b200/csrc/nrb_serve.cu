@@ -108,7 +108,7 @@ static bool same_params(const nrb_f3d_params& a, const nrb_f3d_params& b) {
     return a.levels == b.levels && a.max_iterations == b.max_iterations && feq(a.bending_energy, b.bending_energy) &&
            a.ref_bins == b.ref_bins && a.flo_bins == b.flo_bins && feq(a.padding, b.padding) &&
            a.floating_margin == b.floating_margin && a.batch_gradient_percent == b.batch_gradient_percent &&
-           a.verbose == b.verbose;
+           a.floating_texture == b.floating_texture && a.verbose == b.verbose;
 }
 
 static int64_t voxels_of(const nrb_pair& p) { return (int64_t)p.dim[0] * p.dim[1] * p.dim[2]; }

@@ -21,6 +21,21 @@ namespace nrb {
 constexpr int COL_X = 32;
 constexpr int TY_OBJECTIVE = 16, TY_GRADIENT = 4, TY_DEFORMATION = 4;
 
+// A floating image (with its margin) held as a 2D layered float array, one layer per z slice,
+// and its texture object. Arrays are pooled per process and reused across registrations:
+// allocating and freeing them is not ordered on a stream, so the pool keeps that out of the
+// registrations' paths (up to a cap on the bytes it keeps unused).
+struct FloTexture {
+    cudaArray_t arr = nullptr;
+    unsigned long long tex = 0;
+    int width = 0, height = 0, layers = 0, device = -1;
+};
+nrb_status flo_texture_acquire(int width, int height, int layers, FloTexture& out);
+void flo_texture_release(FloTexture& t);
+// copies a dense [layers][height][width] volume into the array's corner, on `st`
+nrb_status flo_texture_upload(const FloTexture& t, const float *src, int width, int height, int layers,
+                              cudaStream_t st);
+
 // Launch-time description of one voxel walk (a pair's reference volume, grid and floating image,
 // and the walk plan's item decomposition).
 struct WalkParams {
@@ -31,6 +46,7 @@ struct WalkParams {
     int sa, sb, sc;          // shared strides of the staged block (max spans)
     int fnx, fny, fnz;       // floating dims
     int fsy, fsz, fmargin;   // floating layout: row and slice strides, margin (sample_floating)
+    unsigned long long ftex; // the floating image with its margin as a layered texture (0: none)
     Mat34 flo_ijk;           // mm -> floating voxel
     int flo_diag;            // flo_ijk has no off-diagonal terms
     float pad;               // padding value of out-of-volume taps
@@ -423,6 +439,9 @@ struct nrb_workspace {
     // convolved whole in `general_vox` ([3][nz][ny][nx]) and sampled node by node
     bool general = false;
     float *general_vox = nullptr;
+    // a registration's floating image with its margin as a layered texture (FloTexture), which the
+    // fused passes gather from when they sample that padded image (0: none)
+    unsigned long long flo_tex = 0;
     size_t bytes = 0;
     cudaStream_t st = nullptr;      // owner's stream for stream-ordered allocation (or none)
     // the node-grid kernels (bending energy) run on a side stream, overlapped with the voxel

@@ -19,6 +19,8 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <mutex>
+#include <vector>
 
 #include "nrb_state.cuh"
 
@@ -300,8 +302,27 @@ __device__ __forceinline__ int trunc_nonneg(float v) { return __float2int_rz(v);
 // the clamped path substitutes, so the two paths give the same numbers. Other warps read
 // clamped in-volume addresses and select the padding value for out-of-volume taps, with no
 // divergence.
+// The 2x2 footprint of layer `layer` whose lower corner is texel (x0, y0), from one texture
+// gather (tld4) of a 2D layered float array at (x0 + 1, y0 + 1): the texels come back as stored.
+// The gather returns (x0, y0 + 1), (x0 + 1, y0 + 1), (x0 + 1, y0), (x0, y0) in that order;
+// v[b][a] = texel (x0 + a, y0 + b).
+__device__ __forceinline__ void gather_footprint(unsigned long long tex, int layer, float x0p1, float y0p1,
+                                                 float v[2][2]) {
+    float r0, r1, r2, r3;
+    asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %8}];"
+        : "=f"(r0), "=f"(r1), "=f"(r2), "=f"(r3)
+        : "l"(tex), "r"(layer), "f"(x0p1), "f"(y0p1), "f"(0.f));
+    v[1][0] = r0;
+    v[1][1] = r1;
+    v[0][1] = r2;
+    v[0][0] = r3;
+}
+
+// tex (optional): the same floating image with its margin as a 2D layered float array (layer k =
+// slice k - margin, texel (i, j) = voxel (i - margin, j - margin)); warps on the plain path then
+// fetch each slice's 2x2 footprint with one gather instead of four loads.
 template <bool kGrad, int kDiag = -1>
-__device__ __forceinline__ void sample_floating(const float *__restrict__ flo, int fnx, int fny,
+__device__ __forceinline__ void sample_floating(const float *__restrict__ flo, unsigned long long tex, int fnx, int fny,
                                                 int fnz, int sy, int sz, int margin, const Mat34& M,
                                                 int diag, float pad, float x, float y, float z,
                                                 float& val, float g[3]) {
@@ -316,7 +337,11 @@ __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, i
     const bool plain = (unsigned)(px + margin) < (unsigned)(fnx + 2 * margin - 1) &&
                        (unsigned)(py + margin) < (unsigned)(fny + 2 * margin - 1) &&
                        (unsigned)(pz + margin) < (unsigned)(fnz + 2 * margin - 1);
-    if (__all_sync(__activemask(), plain)) {
+    if (__all_sync(__activemask(), plain) && tex) {
+        const float off = (float)(margin + 1);
+        gather_footprint(tex, pz + margin, flx + off, fly + off, v[0]);
+        gather_footprint(tex, pz + margin + 1, flx + off, fly + off, v[1]);
+    } else if (__all_sync(__activemask(), plain)) {
         const float *p = flo + (pz * sz + py * sy + px);
         v[0][0][0] = __ldg(p);
         v[0][0][1] = __ldg(p + 1);
@@ -449,7 +474,7 @@ __device__ __forceinline__ void objective_item(const WalkParams& P, const WalkSm
                 const int vi = idx + u * zstride;
                 if (mask == nullptr || __ldg(&mask[vi]) > -1) {
                     float w, g[3];
-                    sample_floating<false, kDiag ? 1 : 0>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin,
+                    sample_floating<false, kDiag ? 1 : 0>(flo, P.ftex, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin,
                                                           P.flo_ijk, P.flo_diag, P.pad, pos[0], pos[1], pos[2], w, g);
                     const float rv = __ldg(&ref[vi]);
                     if (0.f <= rv && rv < frb && 0.f <= w && w < ffb)  // false for NaN
@@ -663,7 +688,7 @@ __device__ __forceinline__ void gradient_item(const WalkParams& P, const WalkSme
         float out[3] = { 0.f, 0.f, 0.f };
         if (mask == nullptr || __ldg(&mask[idx]) > -1) {
             float w, g[3];
-            sample_floating<true, kDiag ? 1 : 0>(flo, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin, P.flo_ijk,
+            sample_floating<true, kDiag ? 1 : 0>(flo, P.ftex, P.fnx, P.fny, P.fnz, P.fsy, P.fsz, P.fmargin, P.flo_ijk,
                                                  P.flo_diag, P.pad, pos[0], pos[1], pos[2], w, g);
             const float rv = __ldg(&ref[idx]);
             if (rv == rv && w == w) {
@@ -1043,7 +1068,7 @@ __global__ void k_resample(long long nv, int fnx, int fny, int fnz, Mat34 M, int
         if (!kGrad && !active) continue;
         float w = 0.f, g[3] = { 0.f, 0.f, 0.f };
         if (active)
-            sample_floating<kGrad>(flo, fnx, fny, fnz, fnx, fnx * fny, 0, M, diag, pad, def[i], def[nv + i],
+            sample_floating<kGrad>(flo, 0ull, fnx, fny, fnz, fnx, fnx * fny, 0, M, diag, pad, def[i], def[nv + i],
                                    def[2 * nv + i], w, g);
         if (kGrad) {
             out[i] = g[0];
@@ -1356,6 +1381,7 @@ static WalkParams make_params(const WalkPlan& W, const nrb_geometry *g, float pa
     P.flo_diag = m[1] == 0.f && m[2] == 0.f && m[4] == 0.f && m[6] == 0.f && m[8] == 0.f && m[9] == 0.f;
     P.log_in_smem = 0;
     P.xs = 0;
+    P.ftex = 0;
     // identity split when the grid's voxel -> mm matrix has no off-diagonal terms
     const float *c = g->cpp_xyz;
     const bool cdiag = c[1] == 0.f && c[2] == 0.f && c[4] == 0.f && c[6] == 0.f && c[8] == 0.f && c[9] == 0.f;
@@ -1411,6 +1437,7 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
                                   const float *grad, const OptState *step, int flo_margin) {
     WalkParams P = make_params(ws->walk_obj, g, padding, nmi->rb, nmi->fb);
     set_floating_margin(P, flo_margin);
+    P.ftex = flo_margin > 0 ? ws->flo_tex : 0ull;
     const size_t base_smem = walk_smem_bytes(ws->walk_obj) + (size_t)((nmi->rb * nmi->fb + 3) & ~3) * 4;
     const size_t xs_bytes = (size_t)3 * P.sc * P.sb * 32 * 4;
     // the x-contracted rows when two blocks per SM still fit
@@ -1444,6 +1471,7 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
                                  cudaStream_t st, const OptState *sel, int flo_margin) {
     WalkParams P = make_params(ws->walk_grad, g, padding, nmi->rb, nmi->fb);
     set_floating_margin(P, flo_margin);
+    P.ftex = flo_margin > 0 ? ws->flo_tex : 0ull;
     // an FP32 copy of the log table rides in shared memory when it fits (64 bins: 19 KB,
     // 128 bins: 70 KB); larger tables use the FP64 window on the global table
     const size_t log_bytes = (size_t)nmi->total * sizeof(float);
@@ -1507,6 +1535,7 @@ nrb_status batch_walks(nrb_workspace *ws, const nrb_nmi *nmi, const nrb_geometry
     set_floating_margin(wo, flo_margin);
     wg = make_params(ws->walk_grad, g, padding, nmi->rb, nmi->fb);
     set_floating_margin(wg, flo_margin);
+    wo.ftex = wg.ftex = flo_margin > 0 ? ws->flo_tex : 0ull;
     wg.log_in_smem = (size_t)nmi->total * sizeof(float) <= 96 * 1024;
     return NRB_OK;
 }
@@ -1604,6 +1633,106 @@ nrb_status launch_batch_finalize(const BatchPair *d_pairs, OptState *states, Bat
     NRB_CUDA(launch_pdl(in_graph, k_b_finalize, dim3(FIN_CLUSTER * L.npairs), dim3(FIN_CTA_THREADS), L.fin_smem, st,
                         d_pairs, states, L.npairs, bctl, in_graph ? 1 : 0, grad_if, outer));
     NRB_LAUNCHED("k_b_finalize");
+    return NRB_OK;
+}
+
+// ---- floating-image textures ---------------------------------------------------------------
+namespace {
+std::mutex g_tex_mu;
+std::vector<FloTexture> g_tex_free;  // unused arrays, any device
+size_t g_tex_free_bytes = 0;
+constexpr size_t kTexPoolKeepBytes = size_t(4) << 30;
+
+size_t tex_bytes(const FloTexture& t) { return (size_t)t.width * t.height * t.layers * sizeof(float); }
+
+void tex_destroy(FloTexture& t) {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (t.device >= 0 && t.device != cur) cudaSetDevice(t.device);
+    if (t.tex) cudaDestroyTextureObject((cudaTextureObject_t)t.tex);
+    if (t.arr) cudaFreeArray(t.arr);
+    if (t.device >= 0 && t.device != cur) cudaSetDevice(cur);
+    cudaGetLastError();
+    t = FloTexture{};
+}
+}  // namespace
+
+nrb_status flo_texture_acquire(int width, int height, int layers, FloTexture& out) {
+    out = FloTexture{};
+    if (width < 1 || height < 1 || layers < 1 || width > 32768 || height > 32768 || layers > 2048)
+        return fail(NRB_ERR_UNSUPPORTED, "floating texture: extent outside a layered array's limits");
+    int dev = 0;
+    NRB_CUDA(cudaGetDevice(&dev));
+    {
+        // the smallest unused array of this device that holds the extent
+        std::lock_guard<std::mutex> lock(g_tex_mu);
+        int best = -1;
+        for (int i = 0; i < (int)g_tex_free.size(); ++i) {
+            const FloTexture& t = g_tex_free[i];
+            if (t.device == dev && t.width >= width && t.height >= height && t.layers >= layers &&
+                (best < 0 || tex_bytes(t) < tex_bytes(g_tex_free[best])))
+                best = i;
+        }
+        if (best >= 0) {
+            out = g_tex_free[best];
+            g_tex_free_bytes -= tex_bytes(out);
+            g_tex_free.erase(g_tex_free.begin() + best);
+            return NRB_OK;
+        }
+    }
+    FloTexture t;
+    t.device = dev;
+    t.width = width;
+    t.height = height;
+    t.layers = layers;
+    const cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+    NRB_CUDA(cudaMalloc3DArray(&t.arr, &cd, make_cudaExtent(width, height, layers), cudaArrayLayered));
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = t.arr;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    cudaTextureObject_t obj = 0;
+    const cudaError_t e = cudaCreateTextureObject(&obj, &rd, &td, nullptr);
+    if (e != cudaSuccess) {
+        cudaFreeArray(t.arr);
+        return check_cuda(e, "cudaCreateTextureObject");
+    }
+    t.tex = (unsigned long long)obj;
+    out = t;
+    return NRB_OK;
+}
+
+void flo_texture_release(FloTexture& t) {
+    if (!t.arr) return;
+    std::lock_guard<std::mutex> lock(g_tex_mu);
+    g_tex_free.push_back(t);
+    g_tex_free_bytes += tex_bytes(t);
+    // over the cap: free the largest unused arrays first
+    while (g_tex_free_bytes > kTexPoolKeepBytes && !g_tex_free.empty()) {
+        int big = 0;
+        for (int i = 1; i < (int)g_tex_free.size(); ++i)
+            if (tex_bytes(g_tex_free[i]) > tex_bytes(g_tex_free[big])) big = i;
+        g_tex_free_bytes -= tex_bytes(g_tex_free[big]);
+        tex_destroy(g_tex_free[big]);
+        g_tex_free.erase(g_tex_free.begin() + big);
+    }
+    t = FloTexture{};
+}
+
+nrb_status flo_texture_upload(const FloTexture& t, const float *src, int width, int height, int layers,
+                              cudaStream_t st) {
+    if (width > t.width || height > t.height || layers > t.layers)
+        return fail(NRB_ERR_INVALID, "floating texture: volume larger than the array");
+    cudaMemcpy3DParms p = {};
+    p.srcPtr = make_cudaPitchedPtr(const_cast<float *>(src), (size_t)width * sizeof(float), width, height);
+    p.dstArray = t.arr;
+    p.extent = make_cudaExtent(width, height, layers);
+    p.kind = cudaMemcpyDeviceToDevice;
+    NRB_CUDA(cudaMemcpy3DAsync(&p, st));
     return NRB_OK;
 }
 

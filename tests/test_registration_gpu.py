@@ -41,12 +41,13 @@ def test_graph_loop_takes_the_host_loop_steps(pair):
 
 @pytest.mark.parametrize("padding", [float("nan"), 0.0])
 def test_floating_margin_changes_nothing(pair, padding):
-    """The padded floating copy (samples in its margin take the plain load path) gives the same
-    registration, bit for bit, as the dense image with clamped border samples; a margin of 2
-    voxels mixes both paths inside one level."""
+    """The padded floating copy (samples in its margin take the plain path) gives the same
+    registration, bit for bit, as the dense image with clamped border samples, whether the plain
+    path gathers the copy's 2x2 footprints from its layered texture or loads them; a margin of 2
+    voxels mixes the plain and clamped paths inside one level."""
     runs = [nrb.register_host(pair.reference, pair.floating, pair.pixdim,
-                              _params(floating_margin=m, padding=padding, host_loop=h))
-            for m, h in ((0, 1), (8, 0), (2, 0), (8, 1))]
+                              _params(floating_margin=m, padding=padding, host_loop=h, floating_texture=t))
+            for m, h, t in ((0, 1, 0), (8, 0, 1), (2, 0, 1), (8, 1, 1), (8, 0, 0), (2, 1, 0))]
     c0, r0 = runs[0]
     for c, r in runs[1:]:
         assert r.objective_evaluations == r0.objective_evaluations
