@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--floating-texture", type=int, default=1,
+                    help="1: the registrations sample the floating image through its layered texture; 0: loads")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain mode: skip the shortened batched and served runs attached to the line")
     ap.add_argument("--mode", choices=["plain", "batched", "served", "warp", "f3d2"], default="plain")
@@ -371,7 +373,7 @@ def run_b200(args):
     flo_h = torch.from_numpy(pair.floating.ravel().copy()).pin_memory()
     ref_d, flo_d = ref_h.to(dev), flo_h.to(dev)
     params = nrb.default_params(levels=LEVELS, max_iterations=MAXIT, bending_energy=BE, spacing=(SPACING,),
-                                ref_bins=BINS, flo_bins=BINS)
+                                ref_bins=BINS, flo_bins=BINS, floating_texture=args.floating_texture)
     cdim = nrb.grid_dims(dim, pix, params)
     ncpp = 3 * int(np.prod(cdim))
     cpp_d = torch.empty(ncpp, dtype=torch.float32, device=dev)
@@ -543,7 +545,8 @@ def run_batched(args, emit=True):
     picks = [BATCH_SHAPES[i] for i in rng.integers(0, len(BATCH_SHAPES), args.pairs)]
     pairs = [pool[s][int(rng.integers(0, 2))] for s in picks]
     params = nrb.default_params(levels=BATCH_LEVELS, max_iterations=BATCH_MAXIT, bending_energy=BE,
-                                spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS)
+                                spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS,
+                                floating_texture=args.floating_texture)
     # warm-up: one registration of every size
     for s in BATCH_SHAPES:
         p = pool[s][0]
@@ -555,7 +558,8 @@ def run_batched(args, emit=True):
     t_plain = time.perf_counter() - t0
     bparams = nrb.default_params(levels=BATCH_LEVELS, max_iterations=BATCH_MAXIT, bending_energy=BE,
                                  spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS,
-                                 batch_gradient_percent=args.grad_percent, verbose=int(args.verbose))
+                                 batch_gradient_percent=args.grad_percent, verbose=int(args.verbose),
+                                 floating_texture=args.floating_texture)
     t0 = time.perf_counter()
     batched = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], bparams, args.concurrency)
     t_batch = time.perf_counter() - t0
@@ -612,7 +616,8 @@ def run_served(args, emit=True):
     probs = np.array([w for _, w in SERVE_MIX])
     pool = _phantom_pool(shapes, 2, args.seed)
     params = nrb.default_params(levels=SERVE_LEVELS, max_iterations=SERVE_MAXIT, bending_energy=BE,
-                                spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS)
+                                spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS,
+                                floating_texture=args.floating_texture)
     for s in shapes:
         p = pool[s][0]
         nrb.register_host(p.reference, p.floating, p.pixdim, params)
