@@ -1415,7 +1415,14 @@ extern "C" nrb_status nrb_f3d_register_files(const char *ref_path, const char *f
 // ---------------------------------------------------------------------------------------------
 // Batched registrations: one graph per pyramid level for every pair of the batch
 // ---------------------------------------------------------------------------------------------
+// first node of a batched level's graph: the level's WHILE runs (every pair starts in INIT)
+__global__ void k_b_level_start(cudaGraphConditionalHandle outer) { cudaGraphSetConditional(outer, 1u); }
+
 namespace {
+
+// Graph construction, instantiation and destruction of batched levels are serialised across
+// threads (two server workers each build a graph per level); graph execution is not.
+std::mutex g_graph_mu;
 
 // One level of reg_base::Run for every pair, as one CUDA graph:
 //   WHILE(any pair active) {
@@ -1555,11 +1562,12 @@ struct BatchLevelRunner {
             if (launches) *launches = 0;
             return host_driven(hp, L, d_pairs, d_states, d_ctl);
         }
+        std::unique_lock<std::mutex> graph_lock(g_graph_mu);
         GraphHolder top;
         cudaGraph_t while_body = nullptr, if_body = nullptr;
         cudaGraphConditionalHandle h_outer, h_grad;
         NRB_CUDA(cudaGraphCreate(&top.g, 0));
-        NRB_CUDA(cudaGraphConditionalHandleCreate(&h_outer, top.g, 1, cudaGraphCondAssignDefault));
+        NRB_CUDA(cudaGraphConditionalHandleCreate(&h_outer, top.g, 0, 0));
         auto abort_capture = [&](nrb_status e) {
             cudaGraph_t dummy = nullptr;
             cudaStreamEndCapture(cap, &dummy);
@@ -1570,11 +1578,13 @@ struct BatchLevelRunner {
         const long long c0 = g_launch_count.load();
         NRB_CUDA(cudaStreamBeginCaptureToGraph(cap, top.g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         {
-            nrb_status e = capture_while(cap, h_outer, &while_body);
+            k_b_level_start<<<1, 1, 0, cap>>>(h_outer);
+            nrb_status e = cudaGetLastError() == cudaSuccess ? NRB_OK : fail(NRB_ERR_CUDA, "batched level: start launch");
+            if (e == NRB_OK) e = capture_while(cap, h_outer, &while_body);
             if (e != NRB_OK) return abort_capture(e);
         }
         NRB_CUDA(cudaStreamEndCapture(cap, &top.g));
-        NRB_CUDA(cudaGraphConditionalHandleCreate(&h_grad, while_body, 0, cudaGraphCondAssignDefault));
+        NRB_CUDA(cudaGraphConditionalHandleCreate(&h_grad, while_body, 0, 0));
         // the line-search stage, then the IF node of the gradient stage
         NRB_CUDA(cudaStreamBeginCaptureToGraph(cap, while_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         {
@@ -1594,9 +1604,12 @@ struct BatchLevelRunner {
         g_launch_count.fetch_sub(c_line + c_grad);  // counted per execution below
         const auto t_inst = std::chrono::steady_clock::now();
         NRB_CUDA(cudaGraphInstantiate(&top.exec, top.g, 0));
+        graph_lock.unlock();
         const auto t_run = std::chrono::steady_clock::now();
-        NRB_CUDA(cudaGraphLaunch(top.exec, st));
-        NRB_CUDA(cudaStreamSynchronize(st));
+        cudaError_t e = cudaGraphLaunch(top.exec, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        graph_lock.lock();  // held while `top` is destroyed on return
+        NRB_CUDA(e);
         graph_ms[0] = std::chrono::duration<double, std::milli>(t_run - t_inst).count();
         graph_ms[1] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_run).count();
         if (launches) *launches = c_line + c_grad;
