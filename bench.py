@@ -57,7 +57,7 @@ def parse():
                     help="1: the registrations sample the floating image through its layered texture; 0: loads")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain mode: skip the shortened batched and served runs attached to the line")
-    ap.add_argument("--mode", choices=["plain", "batched", "served", "warp", "f3d2"], default="plain")
+    ap.add_argument("--mode", choices=["plain", "batched", "served", "warp", "f3d2", "ct"], default="plain")
     ap.add_argument("--pairs", type=int, default=64, help="batched: number of pairs")
     ap.add_argument("--concurrency", type=int, default=16, help="batched/served: concurrent registrations")
     ap.add_argument("--grad-percent", type=int, default=50,
@@ -696,6 +696,59 @@ def run_served(args, emit=True):
     return line
 
 
+CT_SHAPE, CT_PIX = (320, 512, 512), (0.8, 0.8, 1.5)   # (nz, ny, nx), (dx, dy, dz) mm
+CT_LEVELS, CT_MAXIT, CT_BE, CT_BINS, CT_SPACING = 3, 200, 0.001, 128, 10.0
+
+
+def run_ct(args):
+    """The large CT-like pair: 512x512x320 float32 at 0.8x0.8x1.5 mm, HU phantom, floating warped by a
+    seeded 10 mm FFD with N(0, 4 mm) displacements; 3 levels, 200 counted iterations at the finest
+    level, NMI 128 bins, BE 0.001, 10 mm grid. Four registrations (two seeded phantoms, each
+    twice) one by one through the plain path (host images in, grids out), then the same four in
+    one batch; the batch must give the plain results bit for bit."""
+    import torch
+    import niftyreg_b200 as nrb
+    from niftyreg_b200 import phantom
+
+    torch.cuda.set_device(0)
+    nrb.build()
+    two = [phantom.ct_pair(CT_SHAPE, seed=args.seed + i, pixdim=CT_PIX, spacing_mm=CT_SPACING, disp_sigma_mm=4.0)
+           for i in range(2)]
+    pairs = two + two
+    params = nrb.default_params(levels=CT_LEVELS, max_iterations=CT_MAXIT, bending_energy=CT_BE,
+                                spacing=(CT_SPACING,), ref_bins=CT_BINS, flo_bins=CT_BINS,
+                                floating_texture=args.floating_texture)
+    # warm-up: one registration
+    p0 = pairs[0]
+    nrb.register_host(p0.reference, p0.floating, p0.pixdim, params)
+    sampler = _gpu_clock_sampler()
+    sampler.start()
+    times, plain = [], []
+    for p in pairs:
+        t0 = time.perf_counter()
+        plain.append(nrb.register_host(p.reference, p.floating, p.pixdim, params))
+        times.append(time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    batched = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], params, concurrency=4)
+    t_batch = time.perf_counter() - t0
+    clocks = sampler.stop()
+    identical = all(np.array_equal(a[0], b[0]) for a, b in zip(plain, batched))
+    line = {"mode": "ct", "metric": METRIC, "value": 1.0 / float(np.mean(times)), "unit": "registrations/s",
+            "plain_seconds": [round(t, 3) for t in times], "batch_of_4_value": 4 / t_batch,
+            "batch_of_4_speedup_vs_plain": sum(times) / t_batch, "bitwise_identical_to_plain": identical,
+            "max_abs_dnmi_vs_plain": max(abs(a[1].final_nmi - b[1].final_nmi) for a, b in zip(plain, batched)),
+            "registration": [{"final_nmi": r.final_nmi, "objective_evaluations": r.objective_evaluations,
+                              "gradient_evaluations": r.gradient_evaluations} for _, r in plain],
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "512x512x320 float32 at 0.8x0.8x1.5 mm CT-like HU phantom (air, lungs, soft "
+                                   "tissue, bone ellipsoids), 10 mm FFD N(0, 4 mm); 3 levels, 200 counted iterations "
+                                   "at the finest level, NMI 128 bins, BE 0.001, 10 mm grid",
+                       "timing": "host wall clock, host images in and grids out (copies included)"},
+            "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
 def run_warp(args):
     """The final warped image of a registration of the workload's volume (reg_f3d::GetWarpedImage:
     deformation field of the grid, cubic-spline resample of the floating image), on the device
@@ -918,6 +971,8 @@ def main():
         return run_f3d2(args)
     if args.mode == "warp":
         return run_warp(args)
+    if args.mode == "ct":
+        return run_ct(args)
     return run_b200(args)
 
 
