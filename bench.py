@@ -57,7 +57,8 @@ def parse():
                     help="1: the registrations sample the floating image through its layered texture; 0: loads")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain mode: skip the shortened batched and served runs attached to the line")
-    ap.add_argument("--mode", choices=["plain", "batched", "served", "warp", "f3d2", "ct"], default="plain")
+    ap.add_argument("--mode", choices=["plain", "batched", "served", "warp", "f3d2", "ct", "refcuda"],
+                    default="plain")
     ap.add_argument("--pairs", type=int, default=64, help="batched: number of pairs")
     ap.add_argument("--concurrency", type=int, default=16, help="batched/served: concurrent registrations")
     ap.add_argument("--grad-percent", type=int, default=50,
@@ -494,6 +495,21 @@ def run_b200(args):
                           "sweep": [{k: r[k] for k in ("rate_req_s", "requests", "achieved_req_s", "p50_ms", "p95_ms",
                                                        "p99_ms", "peak_group")} for r in sv["sweep"]],
                           "workload": sv["config"]["workload"]}
+    if world == 1 and not args.no_extras and nrb.platform_available():
+        # NiftyReg's own reg_f3d<float>::Run on the B200 platform (niftyreg_b200/platform): the
+        # reference driver and optimiser with every step one C-ABI call, host images in
+        t0 = time.perf_counter()
+        _, pr = nrb.platform_register(pair.reference, pair.floating, pix, levels=LEVELS, max_iterations=MAXIT,
+                                      bending_energy=BE, spacing=SPACING, bins=BINS)
+        wall = time.perf_counter() - t0
+        ev = pr.objective_evaluations + pr.gradient_evaluations
+        line["platform_plugin"] = {
+            "value": 1.0 / wall, "unit": "registrations/s", "seconds_run": pr.seconds, "seconds_wall": wall,
+            "final_nmi": pr.final_nmi, "objective_evaluations": pr.objective_evaluations,
+            "gradient_evaluations": pr.gradient_evaluations, "evaluations_per_s": ev / pr.seconds,
+            "abs_dnmi_vs_b200": abs(pr.final_nmi - results[-1].final_nmi),
+            "what": "reg_f3d<float>::Run of the reference's own code (pyramid, CG optimiser) on the B200 Platform "
+                    "classes, host images in, grid out, host wall clock"}
     if world == 1 and not args.no_cpu_baseline:
         cb = reference_baseline(pair, os.cpu_count() or 1)
         if cb is not None:
@@ -749,6 +765,52 @@ def run_ct(args):
     return 0
 
 
+def run_refcuda(args):
+    """The reference's own CUDA platform (reg-lib/cuda built for sm_100a into oracle/_refcuda,
+    reg_f3d<float>::Run with PlatformType::Cuda) on this GPU: one registration of the 64^3
+    one-level workload (1 level, 100 counted iterations, BE 0.005, 64 bins, 5-voxel grid) and,
+    unless --shape picks another size, --steps registrations of the brain-like workload, each
+    timed with the host clock around Run (host images in, grid out: the reference's CUDA content
+    copies the images to the device at every level). The library makes its own CUDA context, so
+    this mode runs no other GPU work in the process."""
+    import oracle
+    from niftyreg_b200 import phantom
+    if not oracle.refcuda_available():
+        print(json.dumps({"mode": "refcuda", "unavailable": "oracle/_refcuda/libnrref_cuda.so not built "
+                          "(make -C oracle refcuda, needs the reference sources)"}))
+        return 0
+    eye = np.eye(4, dtype=np.float32)
+    sampler = ClockSampler(0)
+    sampler.start()
+    out = {}
+    small = phantom.blobs_pair((64, 64, 64), seed=1)
+    _, _, st = oracle.refcuda_register(small.reference.ravel(), small.floating.ravel(), small.dim, small.pixdim, eye,
+                                       1, 100, 0.005, 0.0, 64, -5.0)
+    out["blobs_64"] = {"seconds": float(st[4]), "final_nmi": float(st[0]), "objective_evaluations": int(st[2]),
+                       "gradient_evaluations": int(st[3])}
+    shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else SHAPE
+    pair = phantom.brain_pair(shape, seed=args.seed)
+    runs = []
+    for _ in range(max(1, args.steps)):
+        _, _, st = oracle.refcuda_register(pair.reference.ravel(), pair.floating.ravel(), pair.dim, pair.pixdim, eye,
+                                           LEVELS, MAXIT, BE, 0.0, BINS, SPACING)
+        n_obj, n_grad = int(st[2]), int(st[3])
+        runs.append({"seconds": float(st[4]), "final_nmi": float(st[0]), "objective_evaluations": n_obj,
+                     "gradient_evaluations": n_grad, "evaluations_per_s": (n_obj + n_grad) / float(st[4]),
+                     "per_level_seconds": [float(st[7 + 3 * l]) for l in range(LEVELS)]})
+    clocks = sampler.stop()
+    sec = float(np.mean([r["seconds"] for r in runs]))
+    line = {"mode": "refcuda", "impl": "reference-cuda", "metric": METRIC, "value": 1.0 / sec,
+            "unit": "registrations/s", "n_gpus": 1, "steps": len(runs), "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic", "evaluations_per_s": float(np.mean([r["evaluations_per_s"] for r in runs])),
+            "registrations": runs, "blobs_64": out["blobs_64"],
+            "config": {"workload": WORKLOAD if shape == SHAPE else f"brain-like phantom {shape}",
+                       "timing": "host wall clock around reg_f3d<float>::Run on the reference CUDA platform"},
+            "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
 def run_warp(args):
     """The final warped image of a registration of the workload's volume (reg_f3d::GetWarpedImage:
     deformation field of the grid, cubic-spline resample of the floating image), on the device
@@ -973,6 +1035,8 @@ def main():
         return run_warp(args)
     if args.mode == "ct":
         return run_ct(args)
+    if args.mode == "refcuda":
+        return run_refcuda(args)
     return run_b200(args)
 
 

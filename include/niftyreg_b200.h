@@ -271,6 +271,11 @@ typedef struct nrb_f3d_params {
                                * a layered texture, and the fused passes fetch each slice's 2x2
                                * footprint with one gather; 0: plain loads. The same values are
                                * read either way, so the results are identical. */
+    int32_t autotune;         /* 1 (default): the first level of each shape times the objective
+                               * and gradient walks over a candidate set (block height, z-chunk,
+                               * resident blocks) and keeps the fastest in the process's walk
+                               * table (nrb_autotune_entries); 0: the cost model's plans. The
+                               * walk plan moves no value, so results are identical either way. */
 } nrb_f3d_params;
 
 typedef struct nrb_f3d_result {
@@ -282,6 +287,24 @@ typedef struct nrb_f3d_result {
     int64_t gradient_evaluations;
     double seconds;           /* host wall time of the whole call */
 } nrb_f3d_result;
+
+/* ---- walk autotuner (no counterpart in the reference) --------------------------------------
+ * One entry per level shape registered in this process with autotune on: the fastest measured
+ * objective and gradient walks and the times of the cost model's own plans beside them. */
+typedef struct nrb_walk_entry {
+    int32_t ref_dim[3];
+    int32_t cpp_dim[3];
+    int32_t bins[2];          /* user bins (reference, floating) */
+    int32_t obj_ty, obj_zchunk, obj_resident;    /* block height (warps), z-chunk, resident blocks (0: occupancy) */
+    float obj_us, obj_model_us;                  /* device us per launch: tuned, cost model's plan */
+    int32_t grad_ty, grad_zchunk, grad_resident;
+    float grad_us, grad_model_us;
+    int32_t candidates;       /* walks timed */
+} nrb_walk_entry;
+/* Copies up to `capacity` entries into out (may be NULL) and returns the number of entries. */
+int nrb_autotune_entries(nrb_walk_entry *out, int capacity);
+/* Empties the table: the next registration of each shape tunes again. */
+void nrb_autotune_clear(void);
 
 /* Default parameters of reg_f3d<float> (reg-lib/_reg_base.cpp:17-70, _reg_f3d.cpp:18-40). */
 void nrb_f3d_default_params(nrb_f3d_params *p);

@@ -63,7 +63,17 @@ class F3dParams(ctypes.Structure):
                 ("bending_energy", ctypes.c_float), ("spacing", _F3), ("ref_bins", ctypes.c_int32),
                 ("flo_bins", ctypes.c_int32), ("padding", ctypes.c_float), ("verbose", ctypes.c_int32),
                 ("host_loop", ctypes.c_int32), ("floating_margin", ctypes.c_int32),
-                ("batch_gradient_percent", ctypes.c_int32), ("floating_texture", ctypes.c_int32)]
+                ("batch_gradient_percent", ctypes.c_int32), ("floating_texture", ctypes.c_int32),
+                ("autotune", ctypes.c_int32)]
+
+
+class WalkEntry(ctypes.Structure):
+    """nrb_walk_entry: one shape of the walk autotuner's table."""
+    _fields_ = [("ref_dim", _I3), ("cpp_dim", _I3), ("bins", ctypes.c_int32 * 2), ("obj_ty", ctypes.c_int32),
+                ("obj_zchunk", ctypes.c_int32), ("obj_resident", ctypes.c_int32), ("obj_us", ctypes.c_float),
+                ("obj_model_us", ctypes.c_float), ("grad_ty", ctypes.c_int32), ("grad_zchunk", ctypes.c_int32),
+                ("grad_resident", ctypes.c_int32), ("grad_us", ctypes.c_float), ("grad_model_us", ctypes.c_float),
+                ("candidates", ctypes.c_int32)]
 
 
 class Image(ctypes.Structure):
@@ -676,6 +686,27 @@ def register_device(ref, flo, dim, pixdim, params: F3dParams, cpp_out, capacity,
     return res
 
 
+def autotune_entries():
+    """The walk autotuner's table: a list of dicts, one per tuned level shape."""
+    n = int(lib().nrb_autotune_entries(None, 0))
+    arr = (WalkEntry * max(n, 1))()
+    n = min(n, int(lib().nrb_autotune_entries(arr, n)))
+    out = []
+    for e in arr[:n]:
+        out.append({"ref_dim": list(e.ref_dim), "cpp_dim": list(e.cpp_dim), "bins": list(e.bins),
+                    "objective": {"ty": e.obj_ty, "zchunk": e.obj_zchunk, "resident": e.obj_resident,
+                                  "us": e.obj_us, "model_us": e.obj_model_us},
+                    "gradient": {"ty": e.grad_ty, "zchunk": e.grad_zchunk, "resident": e.grad_resident,
+                                 "us": e.grad_us, "model_us": e.grad_model_us},
+                    "candidates": e.candidates})
+    return out
+
+
+def autotune_clear():
+    lib().nrb_autotune_clear.restype = None
+    lib().nrb_autotune_clear()
+
+
 def kernel_launch_count() -> int:
     return int(lib().nrb_kernel_launch_count())
 
@@ -691,3 +722,71 @@ def timing_read(kernel: str):
     n, ms, by = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
     check(lib().nrb_timing_read(kernel.encode(), ctypes.byref(n), ctypes.byref(ms), ctypes.byref(by)))
     return n.value, ms.value, by.value
+
+
+# ----------------------------------------------------------------------------------------------
+# NiftyReg's reg_f3d on the B200 platform (platform/libniftyreg_b200_platform.so,
+# include/niftyreg_b200_platform.h)
+# ----------------------------------------------------------------------------------------------
+PLATFORM_LIB_PATH = os.path.join(HERE, "platform", "libniftyreg_b200_platform.so")
+_PLATFORM_LIB = None
+PLATFORM_CPU, PLATFORM_B200 = 0, 1
+
+
+class PlatformParams(ctypes.Structure):
+    _fields_ = [("platform", ctypes.c_int32), ("gpu", ctypes.c_int32), ("levels", ctypes.c_int32),
+                ("max_iterations", ctypes.c_int32), ("bending_energy", ctypes.c_float),
+                ("linear_energy", ctypes.c_float), ("spacing", ctypes.c_float), ("bins", ctypes.c_int32),
+                ("verbose", ctypes.c_int32)]
+
+
+class PlatformResult(ctypes.Structure):
+    _fields_ = [("cpp_dim", _I3), ("final_nmi", ctypes.c_double), ("objective_evaluations", ctypes.c_int64),
+                ("gradient_evaluations", ctypes.c_int64), ("seconds", ctypes.c_double),
+                ("level_seconds", ctypes.c_double * 8)]
+
+
+def platform_available() -> bool:
+    """True when the NiftyReg library with the B200 platform has been built (it needs the
+    NiftyReg sources: make -C niftyreg_b200/platform)."""
+    return os.path.exists(PLATFORM_LIB_PATH)
+
+
+def platform_lib() -> ctypes.CDLL:
+    global _PLATFORM_LIB
+    if _PLATFORM_LIB is None:
+        if not platform_available():
+            raise RuntimeError(f"{PLATFORM_LIB_PATH} is missing: make -C niftyreg_b200/platform "
+                               "(NIFTYREG_SOURCE_DIR = the NiftyReg checkout)")
+        lib()  # the C ABI it links against, loaded from this package
+        L = ctypes.CDLL(PLATFORM_LIB_PATH)
+        L.nrb_platform_last_error.restype = ctypes.c_char_p
+        _PLATFORM_LIB = L
+    return _PLATFORM_LIB
+
+
+def platform_register(ref: np.ndarray, flo: np.ndarray, pixdim, xyz=None, platform=PLATFORM_B200, levels=1,
+                      max_iterations=100, bending_energy=0.005, linear_energy=0.0, spacing=-5.0, bins=64,
+                      gpu=-1, verbose=False):
+    """reg_f3d<float>::Run of NiftyReg's own registration code on the CPU or the B200 platform,
+    host volumes [nz, ny, nx] float32 in, (cpp [3, cz, cy, cx], PlatformResult) out."""
+    ref = np.ascontiguousarray(ref, np.float32)
+    flo = np.ascontiguousarray(flo, np.float32)
+    nz, ny, nx = ref.shape
+    if xyz is None:
+        xyz = identity_header(pixdim)
+    xyz = np.ascontiguousarray(xyz, np.float32).ravel()
+    p = PlatformParams(int(platform), int(gpu), int(levels), int(max_iterations), float(bending_energy),
+                       float(linear_energy), float(spacing), int(bins), int(bool(verbose)))
+    step = [abs(spacing) * (pixdim[a] if spacing < 0 else 1.0) for a in range(3)]
+    cap = 3 * int(np.prod([int(math.ceil(n * pixdim[a] / step[a])) + 8 for a, n in enumerate((nx, ny, nz))]))
+    cpp = np.zeros(cap, np.float32)
+    res = PlatformResult()
+    rc = platform_lib().nrb_platform_f3d_register(
+        ref.ctypes.data_as(ctypes.c_void_p), flo.ctypes.data_as(ctypes.c_void_p), _I3(nx, ny, nz),
+        _F3(*[float(v) for v in pixdim]), xyz.ctypes.data_as(ctypes.c_void_p), ctypes.byref(p),
+        cpp.ctypes.data_as(ctypes.c_void_p), ctypes.c_int64(cap), ctypes.byref(res))
+    if rc != 0:
+        raise NrbError(-1, platform_lib().nrb_platform_last_error().decode())
+    cx, cy, cz = [int(v) for v in res.cpp_dim]
+    return cpp[:3 * cx * cy * cz].reshape(3, cz, cy, cx).copy(), res

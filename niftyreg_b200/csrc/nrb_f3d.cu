@@ -1056,10 +1056,19 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
     it_ = 0;
     first_call_ = true;
     NRB_TRY(StoreCurrentDof());
-    if (batched_) return NRB_OK;
+    if (batched_) {
+        // the batched kernels take each pair's z-chunk from the walk table when its shape has
+        // been tuned (their block heights are fixed)
+        if (p_.autotune) autotune_lookup(ws_.h, nmi_.h, nullptr, margin_, true);
+        return NRB_OK;
+    }
     double v = 0;
     NRB_TRY(GetObjectiveFunctionValue(v));
     best_obj_ = v;
+    // walk plans for the level: timed once per shape (the evaluation above filled the tables
+    // the gradient pass reads); per-launch timing keeps the model's plans
+    if (p_.autotune && sim_w_ > 0 && !timing_enabled())
+        NRB_TRY(autotune_walks(ws_.h, nmi_.h, &g_, ref_.p, flo_org_, nullptr, cur_.p, pad_, margin_, vgrad_.p, st_));
     return NRB_OK;
 }
 
@@ -1274,6 +1283,7 @@ extern "C" void nrb_f3d_default_params(nrb_f3d_params *p) {
     p->floating_margin = 8;
     p->batch_gradient_percent = 50;
     p->floating_texture = 1;
+    p->autotune = 1;
 }
 
 extern "C" nrb_status nrb_f3d_grid_dims(const int32_t ref_dim[3], const float ref_pixdim[3], const nrb_f3d_params *p,

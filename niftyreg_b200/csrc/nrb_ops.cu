@@ -1022,12 +1022,45 @@ WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t 
     return best;
 }
 
+std::vector<WalkPlan> plan_walk_candidates(const nrb_geometry *g, int ty, long long (*slots_for)(size_t smem),
+                                           size_t extra_smem, int min_chunk, int overhead, int count) {
+    const int nx = g->ref_dim[0], ny = g->ref_dim[1], nz = g->ref_dim[2];
+    const float gs[3] = { g->cpp_pixdim[0] / g->ref_pixdim[0], g->cpp_pixdim[1] / g->ref_pixdim[1],
+                          g->cpp_pixdim[2] / g->ref_pixdim[2] };
+    WalkPlan p;
+    p.ty = ty;
+    p.tiles_x = (nx + COL_X - 1) / COL_X;
+    p.tiles_y = (ny + ty - 1) / ty;
+    p.sa = tile_span(nx, COL_X, gs[0]);
+    p.sb = tile_span(ny, ty, gs[1]);
+    const long long xy = (long long)p.tiles_x * p.tiles_y;
+    std::vector<std::pair<long long, WalkPlan>> all;
+    int last_chunk = -1;
+    for (int c = 1; c <= std::max(1, nz / min_chunk); ++c) {
+        WalkPlan q = p;
+        q.zchunk = (nz + c - 1) / c;
+        if (q.zchunk == last_chunk) continue;
+        last_chunk = q.zchunk;
+        q.nchunks = (nz + q.zchunk - 1) / q.zchunk;
+        q.nitems = (int)(xy * q.nchunks);
+        q.sc = tile_span(nz, q.zchunk, gs[2]);
+        q.cp_floats = 3 * q.sa * q.sb * q.sc;
+        const long long slots = std::max(1LL, slots_for(walk_smem_bytes(q) + extra_smem));
+        const long long rounds = (q.nitems + slots - 1) / slots;
+        all.emplace_back(rounds * (q.zchunk + overhead), q);
+    }
+    std::stable_sort(all.begin(), all.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    std::vector<WalkPlan> out;
+    for (size_t i = 0; i < all.size() && (int)out.size() < count; ++i) out.push_back(all[i].second);
+    return out;
+}
+
 nrb_status workspace_init(nrb_workspace *ws, const nrb_geometry *g) {
     ws->g = *g;
     // shared memory beyond the walk: the 64-bin joint histogram / FP32 log table (the plan is
     // made before the bin count is known; other bin counts shift occupancy little)
-    ws->walk_obj = plan_walk(g, TY_OBJECTIVE, objective_slots, (size_t)68 * 68 * 4, 4, 6);
-    ws->walk_grad = plan_walk(g, TY_GRADIENT, gradient_slots, (size_t)(68 * 68 + 136) * 4, 4, 4);
+    ws->walk_obj = plan_walk(g, TY_OBJECTIVE, objective_slots, OBJ_PLAN_EXTRA, 4, 6);
+    ws->walk_grad = plan_walk(g, TY_GRADIENT, gradient_slots, GRAD_PLAN_EXTRA, 4, 4);
     return NRB_OK;
 }
 

@@ -378,9 +378,15 @@ struct WalkPlan {
     int tiles_x = 0, tiles_y = 0, zchunk = 0, nchunks = 0, nitems = 0;
     int sa = 0, sb = 0, sc = 0;  // max control-point span of an item along x, y, z
     int cp_floats = 0;           // shared floats of the staged control-point block
+    int resident = 0;            // co-resident blocks of the persistent grid; 0 = occupancy limit
 };
 WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t smem), size_t extra_smem,
                    int min_chunk = 8, int overhead = 4);
+// The `count` plans of lowest modelled cost (distinct z-chunks), best first.
+std::vector<WalkPlan> plan_walk_candidates(const nrb_geometry *g, int ty, long long (*slots_for)(size_t smem),
+                                           size_t extra_smem, int min_chunk, int overhead, int count);
+// shared bytes beyond the walk that plan_walk assumes for the objective and gradient passes
+constexpr size_t OBJ_PLAN_EXTRA = (size_t)68 * 68 * 4, GRAD_PLAN_EXTRA = (size_t)(68 * 68 + 136) * 4;
 size_t walk_smem_bytes(const WalkPlan& W);
 // co-resident blocks of the persistent voxel passes for a given dynamic shared-memory size
 long long objective_slots(size_t smem);
@@ -470,6 +476,21 @@ nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be
                                const float *acc_grad = nullptr, long long acc_n = 0);
 // grad/step (optional): evaluate at the line search's trial position cpp - step->cur_len * grad
 // flo_margin > 0: `flo` is the voxel (0, 0, 0) of a copy made by pad_volume with that margin
+// Walk autotuner: the level's objective and gradient walks (items per block row ty, z-chunk,
+// resident blocks) timed on the device over a candidate set, the fastest kept in a process-wide
+// table keyed by the level's shape (reference and grid dims, grid spacing in voxels, bins, mask,
+// floating margin, texture). The walk plan changes which block visits which voxels, never a
+// value: the histogram counts are integers and every other output is per voxel or per node, so
+// results are bit-identical whatever the table holds. autotune_walks times the candidates the
+// first time a shape is seen (the tables of nmi must hold an evaluation: the gradient pass reads
+// them) and leaves the histogram counts zero; later levels of that shape reuse the entry.
+// autotune_lookup applies an entry if one exists; with `batched` it applies the best plan among
+// those with the batched kernels' block shapes (ty = TY_OBJECTIVE / TY_GRADIENT).
+nrb_status autotune_walks(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g, const float *ref, const float *flo,
+                          const int32_t *mask, const float *cpp, float padding, int flo_margin, float *vgrad,
+                          cudaStream_t st);
+bool autotune_lookup(nrb_workspace *ws, const nrb_nmi *nmi, const int32_t *mask, int flo_margin, bool batched);
+
 nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g,
                                   const float *ref, const float *flo, const int32_t *mask,
                                   const float *cpp, float padding, cudaStream_t st,

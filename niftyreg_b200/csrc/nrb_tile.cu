@@ -19,6 +19,8 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <cstring>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -1450,7 +1452,7 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
                              : (trial ? (P.xs ? k_objective<true, true, false> : k_objective<true, false, false>)
                                       : (P.xs ? k_objective<false, true, false> : k_objective<false, false, false>));
     int grid = 0;
-    NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid));
+    NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid, ws->walk_obj.resident));
     // algorithmic bytes: reference + floating (+ mask) per voxel, the grid once
     const double nv = (double)P.nx * P.ny * P.nz;
     const double bytes = nv * (mask ? 12.0 : 8.0) + 12.0 * (double)P.cnv;
@@ -1481,7 +1483,7 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
     int grid = 0;
     auto kernel = P.flo_diag ? (P.log_in_smem ? k_gradient<true, true> : k_gradient<false, true>)
                              : (P.log_in_smem ? k_gradient<true, false> : k_gradient<false, false>);
-    NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid));
+    NRB_TRY(persistent_grid(kernel, threads, smem, P.nitems, grid, ws->walk_grad.resident));
     // algorithmic bytes: reference + floating (+ mask) read, voxel gradient written, grid once
     const double nv = (double)P.nx * P.ny * P.nz;
     const double bytes = nv * (mask ? 24.0 : 20.0) + 12.0 * (double)P.cnv;
@@ -1493,6 +1495,183 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
     NRB_LAUNCHED("k_gradient");
     return NRB_OK;
 }
+
+// ---- walk autotuner ---------------------------------------------------------------------------
+namespace {
+
+struct TuneKey {
+    int rd[3], cd[3], gs[3];  // reference dims, grid dims, grid spacing in 1/1000 voxel
+    int rb, fb, mask, margin, tex;
+    bool operator<(const TuneKey& o) const {
+        return std::memcmp(this, &o, sizeof(TuneKey)) < 0;
+    }
+};
+
+struct TuneEntry {
+    WalkPlan obj, grad;              // fastest measured
+    WalkPlan obj_batch, grad_batch;  // fastest with the batched kernels' block shapes
+    float obj_us = 0, grad_us = 0, obj_model_us = 0, grad_model_us = 0;
+    int candidates = 0;
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneEntry> g_tune;
+
+TuneKey tune_key(const nrb_geometry *g, const nrb_nmi *nmi, const int32_t *mask, int margin, unsigned long long tex) {
+    TuneKey k;
+    std::memset(&k, 0, sizeof(k));
+    for (int d = 0; d < 3; ++d) {
+        k.rd[d] = g->ref_dim[d];
+        k.cd[d] = g->cpp_dim[d];
+        k.gs[d] = (int)lrintf(1000.f * g->cpp_pixdim[d] / g->ref_pixdim[d]);
+    }
+    k.rb = nmi->rb;
+    k.fb = nmi->fb;
+    k.mask = mask != nullptr;
+    k.margin = margin > 0;
+    k.tex = tex != 0;
+    return k;
+}
+
+// mean device time of `reps` launches after one untimed launch; +inf if a launch fails
+template <typename F>
+float time_launch(F launch, cudaStream_t st, int reps) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    float ms = INFINITY;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+        cudaGetLastError();
+        if (a) cudaEventDestroy(a);
+        return ms;
+    }
+    bool ok = launch() == NRB_OK && cudaEventRecord(a, st) == cudaSuccess;
+    for (int r = 0; ok && r < reps; ++r) ok = launch() == NRB_OK;
+    if (ok && cudaEventRecord(b, st) == cudaSuccess && cudaEventSynchronize(b) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, a, b) == cudaSuccess) {
+        ms = ms * 1000.f / (float)reps;
+    } else {
+        ms = INFINITY;
+        cudaGetLastError();
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+}
+
+}  // namespace
+
+bool autotune_lookup(nrb_workspace *ws, const nrb_nmi *nmi, const int32_t *mask, int flo_margin, bool batched) {
+    const TuneKey k = tune_key(&ws->g, nmi, mask, flo_margin, ws->flo_tex);
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(k);
+    if (it == g_tune.end()) return false;
+    ws->walk_obj = batched ? it->second.obj_batch : it->second.obj;
+    ws->walk_grad = batched ? it->second.grad_batch : it->second.grad;
+    return true;
+}
+
+nrb_status autotune_walks(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geometry *g, const float *ref, const float *flo,
+                          const int32_t *mask, const float *cpp, float padding, int flo_margin, float *vgrad,
+                          cudaStream_t st) {
+    if (autotune_lookup(ws, nmi, mask, flo_margin, false)) return NRB_OK;
+    const TuneKey key = tune_key(g, nmi, mask, flo_margin, ws->flo_tex);
+    const WalkPlan obj0 = ws->walk_obj, grad0 = ws->walk_grad;
+    constexpr int kChunks = 3, kReps = 3;
+    const int sms = sm_count();
+    TuneEntry e;
+    // objective: two block heights, the model's best z-chunks, the occupancy limit or one block
+    // per SM
+    float best = INFINITY, best_batch = INFINITY;
+    for (int ty : { TY_OBJECTIVE / 2, TY_OBJECTIVE }) {
+        for (const WalkPlan& c : plan_walk_candidates(g, ty, objective_slots, OBJ_PLAN_EXTRA, 4, 6, kChunks)) {
+            for (int resident : { 0, sms }) {
+                WalkPlan w = c;
+                w.resident = resident;
+                ws->walk_obj = w;
+                const float us = time_launch([&] {
+                    return launch_fused_objective(ws, nmi, g, ref, flo, mask, cpp, padding, st, nullptr, nullptr,
+                                                  flo_margin);
+                }, st, kReps);
+                ++e.candidates;
+                if (ty == obj0.ty && resident == 0 && c.zchunk == obj0.zchunk) e.obj_model_us = us;
+                if (us < best) { best = us; e.obj = w; }
+                if (ty == TY_OBJECTIVE && resident == 0 && us < best_batch) { best_batch = us; e.obj_batch = w; }
+            }
+        }
+    }
+    e.obj_us = best;
+    // the candidates' histogram counts go; the counts stay zero between evaluations
+    NRB_CUDA(cudaMemsetAsync(nmi->hist, 0, (size_t)nmi->rb * nmi->fb * sizeof(uint32_t), st));
+    best = best_batch = INFINITY;
+    for (int ty : { TY_GRADIENT / 2, TY_GRADIENT }) {
+        for (const WalkPlan& c : plan_walk_candidates(g, ty, gradient_slots, GRAD_PLAN_EXTRA, 4, 4, kChunks)) {
+            for (int resident : { 0, 2 * sms }) {
+                WalkPlan w = c;
+                w.resident = resident;
+                ws->walk_grad = w;
+                const float us = time_launch([&] {
+                    return launch_fused_gradient(ws, nmi, g, ref, flo, mask, cpp, padding, 1.0, vgrad, st, nullptr,
+                                                 flo_margin);
+                }, st, kReps);
+                ++e.candidates;
+                if (ty == grad0.ty && resident == 0 && c.zchunk == grad0.zchunk) e.grad_model_us = us;
+                if (us < best) { best = us; e.grad = w; }
+                if (ty == TY_GRADIENT && resident == 0 && us < best_batch) { best_batch = us; e.grad_batch = w; }
+            }
+        }
+    }
+    e.grad_us = best;
+    if (!std::isfinite(e.obj_us) || !std::isfinite(e.grad_us) || e.obj_batch.ty == 0 || e.grad_batch.ty == 0) {
+        ws->walk_obj = obj0;  // nothing measurable: keep the model's plans, record nothing
+        ws->walk_grad = grad0;
+        cudaGetLastError();
+        return NRB_OK;
+    }
+    ws->walk_obj = e.obj;
+    ws->walk_grad = e.grad;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune.emplace(key, e);
+    return NRB_OK;
+}
+
+}  // namespace nrb
+
+extern "C" int nrb_autotune_entries(nrb_walk_entry *out, int capacity) {
+    std::lock_guard<std::mutex> lock(nrb::g_tune_mu);
+    int i = 0;
+    for (const auto& kv : nrb::g_tune) {
+        if (out && i < capacity) {
+            nrb_walk_entry& o = out[i];
+            const nrb::TuneKey& k = kv.first;
+            const nrb::TuneEntry& e = kv.second;
+            for (int d = 0; d < 3; ++d) {
+                o.ref_dim[d] = k.rd[d];
+                o.cpp_dim[d] = k.cd[d];
+            }
+            o.bins[0] = k.rb - 4;
+            o.bins[1] = k.fb - 4;
+            o.obj_ty = e.obj.ty;
+            o.obj_zchunk = e.obj.zchunk;
+            o.obj_resident = e.obj.resident;
+            o.obj_us = e.obj_us;
+            o.obj_model_us = e.obj_model_us;
+            o.grad_ty = e.grad.ty;
+            o.grad_zchunk = e.grad.zchunk;
+            o.grad_resident = e.grad.resident;
+            o.grad_us = e.grad_us;
+            o.grad_model_us = e.grad_model_us;
+            o.candidates = e.candidates;
+        }
+        ++i;
+    }
+    return i;
+}
+
+extern "C" void nrb_autotune_clear(void) {
+    std::lock_guard<std::mutex> lock(nrb::g_tune_mu);
+    nrb::g_tune.clear();
+}
+
+namespace nrb {
 
 nrb_status launch_nmi_finalize(nrb_nmi *nmi, const double *be_partials, int n_be_partials,
                                int64_t cpp_nvox3, double sim_weight, double be_weight,

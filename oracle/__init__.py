@@ -27,6 +27,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATED_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libnrref.so")
 REF64_SO = os.path.join(HERE, "_ref64", "libnrref64.so")
+REFCUDA_SO = os.path.join(HERE, "_refcuda", "libnrref_cuda.so")
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -68,6 +69,28 @@ def ref_available() -> bool:
 
 def ref64_available() -> bool:
     return os.path.exists(REF64_SO)
+
+
+def refcuda_available() -> bool:
+    return os.path.exists(REFCUDA_SO)
+
+
+def refcuda_register(ref, flo, dim, pix, xyz, levels, maxit, be, le, bins, spacing, verbose=False):
+    """reg_f3d<float>::Run on the reference's own CUDA platform (oracle/_refcuda, its reg-lib/cuda
+    sources built for sm_100a): (cpp, cdim, stats) with stats as ``Ref.f3d_register``'s. Needs a
+    GPU; the library creates its own CUDA context on the device it picks."""
+    lib = ctypes.CDLL(REFCUDA_SO)
+    params = np.array([levels, maxit, be, le, bins, spacing, 1 if verbose else 0], np.float64)
+    cap = 3 * int(np.prod([int(np.ceil(n * p / abs(spacing * (p if spacing < 0 else 1))) + 4)
+                           for n, p in zip(dim, pix)])) + 64
+    cpp = np.zeros(cap, np.float32)
+    cdim = np.zeros(3, np.int32)
+    stats = np.zeros(5 + 3 * int(levels), np.float64)
+    rc = lib.refcuda_f3d_register(_f(_f3(ref)), _f(_f3(flo)), _i(_i3(dim)), _f(_f3(pix)), _f(_m(xyz)), _d(params),
+                                  _i(cdim), _f(cpp), ctypes.c_size_t(cap), _d(stats))
+    if rc != 0:
+        raise RuntimeError("refcuda_f3d_register failed")
+    return cpp[:3 * int(np.prod(cdim))].copy(), cdim, stats
 
 
 # ----------------------------------------------------------------------------------------------

@@ -43,6 +43,10 @@ def test_host_entry_points_without_gpu():
     assert nrb.grid_dims((182, 218, 182), (1.0, 1.0, 1.0), p) == [40, 47, 40]
     assert nrb.grid_dims((64, 64, 64), (1.0, 1.0, 1.0), p) == [16, 16, 16]
     assert nrb.grid_dims((512, 512, 320), (0.8, 0.8, 1.5), nrb.default_params(spacing=(10.0,))) == [44, 44, 51]
+    assert p.autotune == 1 and p.floating_texture == 1
+    # the walk table is host state: empty until a registration tunes a shape
+    nrb.autotune_clear()
+    assert nrb.autotune_entries() == []
 
 
 def test_invalid_arguments_are_reported():
