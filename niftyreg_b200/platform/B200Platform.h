@@ -43,10 +43,14 @@ void Check(nrb_status s, const char *what);
 // A CUDA runtime error likewise.
 void CheckCuda(cudaError_t e, const char *what);
 
-// Device copy of an NiftiImage's float data.
+// A device allocation owned by one object (freed with it).
 struct DeviceArray {
     void *ptr = nullptr;
     size_t bytes = 0;
+    DeviceArray() = default;
+    DeviceArray(const DeviceArray&) = delete;
+    DeviceArray& operator=(const DeviceArray&) = delete;
+    ~DeviceArray() { Free(); }
     void Allocate(size_t n);
     void Free();
     float *f() const { return static_cast<float*>(ptr); }

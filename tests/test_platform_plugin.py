@@ -119,6 +119,24 @@ def test_registration_matches_cpu_platform(pair):
 
 @pytest.mark.gpu
 @needs_platform
+def test_ct_like_two_levels_matches_cpu_platform():
+    """Anisotropic voxels (0.8 x 0.8 x 1.5 mm), a 10 mm grid, two levels with grid refinement
+    between them: the reference driver on both platforms, same end-point bar."""
+    ensure_built()
+    p = phantom.ct_pair((40, 72, 64), seed=2)
+    kw = dict(levels=2, max_iterations=30, bending_energy=0.001, spacing=10.0, bins=64)
+    c_b2, r_b2 = nrb.platform_register(p.reference, p.floating, p.pixdim, platform=nrb.PLATFORM_B200, **kw)
+    c_cpu, r_cpu = nrb.platform_register(p.reference, p.floating, p.pixdim, platform=nrb.PLATFORM_CPU, **kw)
+    print(f"[platform] CT-like 2 levels: NMI B200 {r_b2.final_nmi:.8f} CPU {r_cpu.final_nmi:.8f}; evaluations "
+          f"{r_b2.objective_evaluations}/{r_b2.gradient_evaluations} vs {r_cpu.objective_evaluations}/"
+          f"{r_cpu.gradient_evaluations}")
+    assert c_b2.shape == c_cpu.shape
+    assert abs(r_b2.final_nmi - r_cpu.final_nmi) <= 5e-3 * r_cpu.final_nmi
+    assert r_b2.final_nmi >= (1.0 - 1e-3) * r_cpu.final_nmi
+
+
+@pytest.mark.gpu
+@needs_platform
 def test_platform_equals_fused_path_start(pair):
     """The platform's step-by-step calls and the fused registration driver start from the same
     first evaluation."""
