@@ -29,6 +29,7 @@ typedef struct nrb_platform_params {
     float spacing;           /* control-point spacing: negative = voxels, positive = mm [-sx] */
     int32_t bins;            /* NMI bins of both images [--rbn/--fbn] */
     int32_t verbose;         /* 0: DoNotPrintOutInformation */
+    float padding;           /* warped padding value, NaN by default [-pad] */
 } nrb_platform_params;
 
 typedef struct nrb_platform_result {

@@ -737,7 +737,7 @@ class PlatformParams(ctypes.Structure):
     _fields_ = [("platform", ctypes.c_int32), ("gpu", ctypes.c_int32), ("levels", ctypes.c_int32),
                 ("max_iterations", ctypes.c_int32), ("bending_energy", ctypes.c_float),
                 ("linear_energy", ctypes.c_float), ("spacing", ctypes.c_float), ("bins", ctypes.c_int32),
-                ("verbose", ctypes.c_int32)]
+                ("verbose", ctypes.c_int32), ("padding", ctypes.c_float)]
 
 
 class PlatformResult(ctypes.Structure):
@@ -767,7 +767,7 @@ def platform_lib() -> ctypes.CDLL:
 
 def platform_register(ref: np.ndarray, flo: np.ndarray, pixdim, xyz=None, platform=PLATFORM_B200, levels=1,
                       max_iterations=100, bending_energy=0.005, linear_energy=0.0, spacing=-5.0, bins=64,
-                      gpu=-1, verbose=False):
+                      gpu=-1, verbose=False, padding=math.nan):
     """reg_f3d<float>::Run of NiftyReg's own registration code on the CPU or the B200 platform,
     host volumes [nz, ny, nx] float32 in, (cpp [3, cz, cy, cx], PlatformResult) out."""
     ref = np.ascontiguousarray(ref, np.float32)
@@ -777,7 +777,7 @@ def platform_register(ref: np.ndarray, flo: np.ndarray, pixdim, xyz=None, platfo
         xyz = identity_header(pixdim)
     xyz = np.ascontiguousarray(xyz, np.float32).ravel()
     p = PlatformParams(int(platform), int(gpu), int(levels), int(max_iterations), float(bending_energy),
-                       float(linear_energy), float(spacing), int(bins), int(bool(verbose)))
+                       float(linear_energy), float(spacing), int(bins), int(bool(verbose)), float(padding))
     step = [abs(spacing) * (pixdim[a] if spacing < 0 else 1.0) for a in range(3)]
     cap = 3 * int(np.prod([int(math.ceil(n * pixdim[a] / step[a])) + 8 for a, n in enumerate((nx, ny, nz))]))
     cpp = np.zeros(cap, np.float32)

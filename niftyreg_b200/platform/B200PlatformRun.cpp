@@ -89,6 +89,7 @@ extern "C" int nrb_platform_f3d_register(const float *ref, const float *flo, con
         reg.UseNMISetReferenceBinNumber(0, p->bins);
         reg.UseNMISetFloatingBinNumber(0, p->bins);
         reg.SetSpacing(0, p->spacing);
+        reg.SetWarpedPaddingValue(p->padding);
         if (!p->verbose) reg.DoNotPrintOutInformation();
         const auto t0 = std::chrono::steady_clock::now();
         reg.Run();
