@@ -74,6 +74,10 @@ def parse():
     ap.add_argument("--slots", type=int, default=2, help="served: workers (groups registered at once)")
     ap.add_argument("--max-group", type=int, default=16, help="served: requests registered together at most")
     ap.add_argument("--shape", default=None, help="kernel-only mode: nz,ny,nx of the volume (default: the workload's)")
+    ap.add_argument("--group-mb", type=int, default=None,
+                    help="batched/served: finest-level image MB a group of pairs may hold (default: the library's)")
+    ap.add_argument("--batch-shapes", default=None,
+                    help="batched: sizes to draw from, 'nz,ny,nx;nz,ny,nx;...' (default: config 3's four sizes)")
     ap.add_argument("--kernel", choices=["objective", "gradient", "velocity", "compose"], default=None,
                     help="profiling mode: run only `--steps` fused evaluations at the finest level "
                          "of the workload (for ncu captures); prints per-launch device times")
@@ -557,14 +561,16 @@ def run_batched(args, emit=True):
     torch.cuda.set_device(0)
     nrb.build()
     rng = np.random.default_rng(args.seed)
-    pool = _phantom_pool(BATCH_SHAPES, 2, args.seed)
-    picks = [BATCH_SHAPES[i] for i in rng.integers(0, len(BATCH_SHAPES), args.pairs)]
+    shapes = ([tuple(int(v) for v in t.split(",")) for t in args.batch_shapes.split(";")] if args.batch_shapes
+              else BATCH_SHAPES)
+    pool = _phantom_pool(shapes, 2, args.seed)
+    picks = [shapes[i] for i in rng.integers(0, len(shapes), args.pairs)]
     pairs = [pool[s][int(rng.integers(0, 2))] for s in picks]
     params = nrb.default_params(levels=BATCH_LEVELS, max_iterations=BATCH_MAXIT, bending_energy=BE,
                                 spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS,
                                 floating_texture=args.floating_texture)
     # warm-up: one registration of every size
-    for s in BATCH_SHAPES:
+    for s in shapes:
         p = pool[s][0]
         nrb.register_host(p.reference, p.floating, p.pixdim, params)
     sampler = _gpu_clock_sampler()
@@ -576,6 +582,8 @@ def run_batched(args, emit=True):
                                  spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS,
                                  batch_gradient_percent=args.grad_percent, verbose=int(args.verbose),
                                  floating_texture=args.floating_texture)
+    if args.group_mb is not None:
+        bparams.batch_group_mb = args.group_mb
     t0 = time.perf_counter()
     batched = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], bparams, args.concurrency)
     t_batch = time.perf_counter() - t0
@@ -604,7 +612,7 @@ def run_batched(args, emit=True):
     line = {"mode": "batched", "metric": METRIC, "value": args.pairs / t_batch, "unit": "registrations/s",
             "plain_value": args.pairs / t_plain, "speedup_vs_plain": t_plain / t_batch, "n_gpus": 1,
             "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.pairs} pairs, sizes uniform over {BATCH_SHAPES} (nz, ny, nx), blob "
+            "config": {"workload": f"{args.pairs} pairs, sizes uniform over {shapes} (nz, ny, nx), blob "
                                    f"phantoms (2 distinct pairs per size), {BATCH_LEVELS} levels, {BATCH_MAXIT} "
                                    f"counted iterations at the finest level, NMI {BINS} bins, BE {BE}, 5-voxel grid",
                        "concurrency": args.concurrency, "timing": "host wall clock, host images, copies included"},
@@ -634,6 +642,8 @@ def run_served(args, emit=True):
     params = nrb.default_params(levels=SERVE_LEVELS, max_iterations=SERVE_MAXIT, bending_energy=BE,
                                 spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS,
                                 floating_texture=args.floating_texture)
+    if args.group_mb is not None:
+        params.batch_group_mb = args.group_mb
     for s in shapes:
         p = pool[s][0]
         nrb.register_host(p.reference, p.floating, p.pixdim, params)

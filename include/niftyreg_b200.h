@@ -276,6 +276,12 @@ typedef struct nrb_f3d_params {
                                * resident blocks) and keeps the fastest in the process's walk
                                * table (nrb_autotune_entries); 0: the cost model's plans. The
                                * walk plan moves no value, so results are identical either way. */
+    int32_t batch_group_mb;   /* nrb_f3d_register_batch and the grouping server: a group of pairs
+                               * registered together holds at most this many MB of finest-level
+                               * images (reference + floating), so that a line-search step's
+                               * images stay in L2 between steps (default 96; a pair larger than
+                               * that is a group of its own; 0: no cap). Scheduling only: results
+                               * do not depend on it. */
 } nrb_f3d_params;
 
 typedef struct nrb_f3d_result {
@@ -529,8 +535,9 @@ nrb_status nrb_server_peak_group(nrb_server *s, int32_t *peak_group);
 void nrb_server_destroy(nrb_server *s);
 
 /* n registrations advanced together (no counterpart in the reference, which registers one pair
- * per reg_f3d run). The pairs are taken in order in groups of at most `concurrency` (<= 128)
- * whose summed footprints fit in hbm_budget_bytes (<= 0: 80% of the free device memory); a group
+ * per reg_f3d run). The pairs are taken in order of size in groups of at most `concurrency`
+ * (<= 64) whose summed footprints fit in hbm_budget_bytes (<= 0: 80% of the free device memory)
+ * and whose finest-level images fit in p->batch_group_mb; a group
  * runs level by level, each level as one CUDA graph in which every stage -- the line-search
  * objective, its finalize, the gradient, the node convolution, the conjugate-gradient direction
  * -- is one launch over all the pairs that need it. Each pair's arithmetic is that of its plain

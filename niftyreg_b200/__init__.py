@@ -64,7 +64,7 @@ class F3dParams(ctypes.Structure):
                 ("flo_bins", ctypes.c_int32), ("padding", ctypes.c_float), ("verbose", ctypes.c_int32),
                 ("host_loop", ctypes.c_int32), ("floating_margin", ctypes.c_int32),
                 ("batch_gradient_percent", ctypes.c_int32), ("floating_texture", ctypes.c_int32),
-                ("autotune", ctypes.c_int32)]
+                ("autotune", ctypes.c_int32), ("batch_group_mb", ctypes.c_int32)]
 
 
 class WalkEntry(ctypes.Structure):

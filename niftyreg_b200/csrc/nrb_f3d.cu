@@ -704,8 +704,11 @@ nrb_status F3dRegistration::CaptureGradient(cudaStream_t cs) {
 
 // One line-search step as captured launches: the objective at the trial position
 // best - cur_len * grad formed inside the kernels (UpdateControlPointPosition fused away), the
-// finalize taking the step (value, acceptance, next length, WHILE condition), and the store of
-// an accepted trial position into best.
+// bending energy of the same position beside it on the side stream, and the finalize taking the
+// step (value, acceptance, next length, WHILE condition) and storing an accepted trial position
+// into best. (One launch per step, the finalize run by the objective's last cluster to finish,
+// was measured slower: a launch of 8-block clusters holds fewer blocks at once and paid a fixed
+// cost of about 18 us per step at the coarse levels.)
 nrb_status F3dRegistration::CaptureLineStep(cudaStream_t cs, cudaGraphConditionalHandle line) {
     nrb_workspace *ws = ws_.h;
     int n_be = 0;
@@ -1284,6 +1287,7 @@ extern "C" void nrb_f3d_default_params(nrb_f3d_params *p) {
     p->batch_gradient_percent = 50;
     p->floating_texture = 1;
     p->autotune = 1;
+    p->batch_group_mb = 96;
 }
 
 extern "C" nrb_status nrb_f3d_grid_dims(const int32_t ref_dim[3], const float ref_pixdim[3], const nrb_f3d_params *p,
@@ -1637,6 +1641,11 @@ nrb_status nrb::register_batch_fused(const nrb_pair *pairs, int n, const nrb_f3d
     using Clock = std::chrono::steady_clock;
     auto ms_since = [](Clock::time_point t) { return std::chrono::duration<double, std::milli>(Clock::now() - t).count(); };
     const auto t_begin = Clock::now();
+    // the stream-ordered pool keeps the whole group's working set between batches (a pool that
+    // grows again for every batch pays for mapping the memory each time)
+    int64_t group_bytes = 0;
+    for (int i = 0; i < n; ++i) group_bytes += registration_footprint(pairs[i].dim, pairs[i].pixdim, p);
+    keep_pool(group_bytes);
     std::vector<std::unique_ptr<F3dRegistration>> regs;
     regs.reserve(n);
     for (int i = 0; i < n; ++i) {

@@ -21,10 +21,6 @@ namespace nrb {
 // set_second_order_bspline_basis_values (reg-lib/cpu/_reg_splineBasis.cpp:291-455). The
 // reference tabulates the exact values rounded to 6 decimals; the same rounding is applied
 // here to B(+-1) = 1/6, B(0) = 2/3, B'(+-1) = +-1/2, B'(0) = 0, B''(+-1) = 1, B''(0) = -2.
-struct BeBasis {
-    float v[6][27];  // xx, yy, zz, xy, yz, xz
-};
-
 static BeBasis make_be_basis() {
     const double B[3] = { 1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0 };
     const double D[3] = { -0.5, 0.0, 0.5 };
@@ -59,48 +55,6 @@ __device__ double block_sum_d(double v, double *red) {
         __syncthreads();
     }
     return red[0];
-}
-
-// the bending-energy value term of interior node n (of ix * iy * iz interior nodes)
-__device__ __forceinline__ double be_node_value(int cx, int cy, int cz, int ix, int iy, const float *__restrict__ cpp,
-                                                const BeBasis& B, const float *__restrict__ grad, float scale,
-                                                long long n) {
-    const long long nc = (long long)cx * cy * cz;
-    {
-        const int x = 1 + (int)(n % ix);
-        const int y = 1 + (int)((n / ix) % iy);
-        const int z = 1 + (int)(n / ((long long)ix * iy));
-        float d[3][6];
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-#pragma unroll
-            for (int t = 0; t < 6; ++t) d[k][t] = 0.f;
-        int i = 0;
-        for (int c = -1; c < 2; ++c)
-            for (int b = -1; b < 2; ++b)
-                for (int a = -1; a < 2; ++a, ++i) {
-                    const long long idx = ((long long)(z + c) * cy + y + b) * cx + x + a;
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const float v = trial_cp(cpp, grad, scale, k * nc + idx);
-#pragma unroll
-                        for (int t = 0; t < 6; ++t) d[k][t] = __fadd_rn(d[k][t], __fmul_rn(B.v[t][i], v));
-                    }
-                }
-        // the reference expression's order: the first three squares summed in float, every
-        // later term added in double
-        auto sq = [](float v) { return __fmul_rn(v, v); };
-        auto sum3 = [&](int k, int t) { return __fadd_rn(__fadd_rn(sq(d[k][t]), sq(d[k][t + 1])), sq(d[k][t + 2])); };
-        double s = __dadd_rn((double)sum3(0, 0), __dmul_rn(2.0, (double)sum3(0, 3)));
-#pragma unroll
-        for (int k = 1; k < 3; ++k) {
-            s = __dadd_rn(s, (double)sq(d[k][0]));
-            s = __dadd_rn(s, (double)sq(d[k][1]));
-            s = __dadd_rn(s, (double)sq(d[k][2]));
-            s = __dadd_rn(s, __dmul_rn(2.0, (double)sum3(k, 3)));
-        }
-        return s;
-    }
 }
 
 // reg_spline_approxBendingEnergyValue3D (reg-lib/cpu/_reg_localTrans_regul.cpp:72-153): per

@@ -108,10 +108,13 @@ static bool same_params(const nrb_f3d_params& a, const nrb_f3d_params& b) {
     return a.levels == b.levels && a.max_iterations == b.max_iterations && feq(a.bending_energy, b.bending_energy) &&
            a.ref_bins == b.ref_bins && a.flo_bins == b.flo_bins && feq(a.padding, b.padding) &&
            a.floating_margin == b.floating_margin && a.batch_gradient_percent == b.batch_gradient_percent &&
-           a.floating_texture == b.floating_texture && a.verbose == b.verbose;
+           a.floating_texture == b.floating_texture && a.verbose == b.verbose && a.autotune == b.autotune &&
+           a.batch_group_mb == b.batch_group_mb;
 }
 
 static int64_t voxels_of(const nrb_pair& p) { return (int64_t)p.dim[0] * p.dim[1] * p.dim[2]; }
+// finest-level reference + floating bytes of a pair (one geometry for both)
+static int64_t image_bytes(const nrb_pair& p) { return 2 * 4 * voxels_of(p); }
 
 struct nrb_server {
     int device = 0;
@@ -136,15 +139,18 @@ struct nrb_server {
         Job *head = queue.front();
         queue.pop_front();
         g.push_back(head);
-        int64_t bytes = head->footprint;
+        int64_t bytes = head->footprint, images = image_bytes(head->pair);
         const int64_t hv = voxels_of(head->pair);
+        const int64_t group_bytes = (int64_t)std::max(0, head->params.batch_group_mb) << 20;
         for (auto it = queue.begin(); it != queue.end() && (int)g.size() < max_group;) {
             Job *j = *it;
             const int64_t v = voxels_of(j->pair);
             if (same_params(j->params, head->params) && v <= 2 * hv && hv <= 2 * v &&
-                used + bytes + j->footprint <= budget) {
+                used + bytes + j->footprint <= budget &&
+                (group_bytes == 0 || images + image_bytes(j->pair) <= group_bytes)) {
                 g.push_back(j);
                 bytes += j->footprint;
+                images += image_bytes(j->pair);
                 it = queue.erase(it);
             } else {
                 ++it;
@@ -336,25 +342,42 @@ extern "C" nrb_status nrb_f3d_register_batch(const nrb_pair *pairs, int n, const
         NRB_CUDA(cudaMemGetInfo(&free_b, &total_b));
         budget = (int64_t)(0.8 * (double)free_b);
     }
+    // pairs in order of size (stable), so that a group holds pairs of similar size
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return voxels_of(pairs[a]) < voxels_of(pairs[b]); });
+    const int64_t group_bytes = (int64_t)std::max(0, p->batch_group_mb) << 20;
     cudaStream_t st = nullptr;
     NRB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     nrb_status s = NRB_OK;
+    std::vector<nrb_pair> gp;
+    std::vector<nrb_f3d_result> gr;
     for (int i0 = 0; i0 < n && s == NRB_OK;) {
-        // the next group: pairs in order while they fit in the budget (a pair larger than the
-        // budget alone is refused)
-        int64_t used = 0;
+        // the next group: pairs while they fit in the HBM budget (a pair larger than the budget
+        // alone is refused) and their finest-level images in the group cap (the first pair
+        // always joins)
+        int64_t used = 0, images = 0;
         int i1 = i0;
         while (i1 < n && i1 - i0 < group_max) {
-            const int64_t f = registration_footprint(pairs[i1].dim, pairs[i1].pixdim, p);
+            const nrb_pair& q = pairs[order[i1]];
+            const int64_t f = registration_footprint(q.dim, q.pixdim, p);
+            const int64_t img = image_bytes(q);
             if (used + f > budget) break;
+            if (i1 > i0 && group_bytes > 0 && images + img > group_bytes) break;
             used += f;
+            images += img;
             ++i1;
         }
         if (i1 == i0) {
             s = fail(NRB_ERR_OOM, "nrb_f3d_register_batch: a pair is larger than the HBM budget");
             break;
         }
-        s = register_batch_fused(pairs + i0, i1 - i0, p, results ? results + i0 : nullptr, st, pct);
+        gp.clear();
+        for (int i = i0; i < i1; ++i) gp.push_back(pairs[order[i]]);
+        gr.assign(i1 - i0, nrb_f3d_result{});
+        s = register_batch_fused(gp.data(), i1 - i0, p, gr.data(), st, pct);
+        if (s == NRB_OK && results)
+            for (int i = i0; i < i1; ++i) results[order[i]] = gr[i - i0];
         i0 = i1;
     }
     cudaStreamSynchronize(st);

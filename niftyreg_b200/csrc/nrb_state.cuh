@@ -382,6 +382,55 @@ struct WalkPlan {
 };
 WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t smem), size_t extra_smem,
                    int min_chunk = 8, int overhead = 4);
+// Second-derivative stencils of the bending energy at the nodes, in the 27-point (c, b, a) order
+// of set_second_order_bspline_basis_values (reg-lib/cpu/_reg_splineBasis.cpp:291-455), rounded to
+// 6 decimals as the reference tabulates them.
+struct BeBasis {
+    float v[6][27];  // xx, yy, zz, xy, yz, xz
+};
+// the bending-energy value term of interior node n (of ix * iy * iz interior nodes)
+__device__ __forceinline__ double be_node_value(int cx, int cy, int cz, int ix, int iy, const float *__restrict__ cpp,
+                                                const BeBasis& B, const float *__restrict__ grad, float scale,
+                                                long long n) {
+    const long long nc = (long long)cx * cy * cz;
+    const int x = 1 + (int)(n % ix);
+    const int y = 1 + (int)((n / ix) % iy);
+    const int z = 1 + (int)(n / ((long long)ix * iy));
+    auto sq = [](float v) { return __fmul_rn(v, v); };
+    // one component at a time: its 6 stencil sums over the 27 points in (c, b, a) order, then
+    // its terms in the reference expression's order (the first three squares of component 0
+    // summed in float, every later term added in double), so only 6 sums are live at once
+    double s = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < 3; ++k) {
+        float d[6];
+#pragma unroll
+        for (int t = 0; t < 6; ++t) d[t] = 0.f;
+#pragma unroll 1
+        for (int c = -1; c < 2; ++c)
+#pragma unroll
+            for (int b = -1; b < 2; ++b)
+#pragma unroll
+                for (int a = -1; a < 2; ++a) {
+                    const int i = 9 * (c + 1) + 3 * (b + 1) + (a + 1);
+                    const long long idx = ((long long)(z + c) * cy + y + b) * cx + x + a;
+                    const float v = trial_cp(cpp, grad, scale, k * nc + idx);
+#pragma unroll
+                    for (int t = 0; t < 6; ++t) d[t] = __fadd_rn(d[t], __fmul_rn(B.v[t][i], v));
+                }
+        const float cross = __fadd_rn(__fadd_rn(sq(d[3]), sq(d[4])), sq(d[5]));
+        if (k == 0) {
+            s = __dadd_rn((double)__fadd_rn(__fadd_rn(sq(d[0]), sq(d[1])), sq(d[2])), __dmul_rn(2.0, (double)cross));
+        } else {
+            s = __dadd_rn(s, (double)sq(d[0]));
+            s = __dadd_rn(s, (double)sq(d[1]));
+            s = __dadd_rn(s, (double)sq(d[2]));
+            s = __dadd_rn(s, __dmul_rn(2.0, (double)cross));
+        }
+    }
+    return s;
+}
+
 // The `count` plans of lowest modelled cost (distinct z-chunks), best first.
 std::vector<WalkPlan> plan_walk_candidates(const nrb_geometry *g, int ty, long long (*slots_for)(size_t smem),
                                            size_t extra_smem, int min_chunk, int overhead, int count);

@@ -858,15 +858,20 @@ __device__ __forceinline__ void finalize_cluster(cg::cluster_group& cluster, con
     __shared__ OptState sctl;   // this block's copy of the optimiser state
     __shared__ double s_mgl[2];
     const int tid = threadIdx.x, c = (int)cluster.block_rank();
+    // threads beyond FIN_CTA_THREADS (a caller with larger blocks) take part in the barriers only,
+    // so the work and its summation order are those of FIN_CTA_THREADS-thread blocks
+    const bool act = tid < FIN_CTA_THREADS;
     // everything the end of the kernel needs from global memory is read now, beside the counts:
     // the optimiser state, the gradient lengths of both table sets, the bending-energy partials
+    // (counts and partials through L2: other blocks of the same launch may have written them)
     if (tid == 0) {
         if (ctl) sctl = *ctl;
         s_mgl[0] = last0->max_grad_len;
         s_mgl[1] = last1->max_grad_len;
     }
     double be = 0.0;
-    for (int i = tid; i < n_be; i += FIN_CTA_THREADS) be += be_partials[i];
+    if (act)
+        for (int i = tid; i < n_be; i += FIN_CTA_THREADS) be += __ldcg(&be_partials[i]);
     const int nj = rb * fb;
     const int rpc = (fb + FIN_CLUSTER - 1) / FIN_CLUSTER;
     const int f0 = min(fb, c * rpc), f1 = min(fb, f0 + rpc), nrow = f1 - f0;
@@ -875,14 +880,15 @@ __device__ __forceinline__ void finalize_cluster(cg::cluster_group& cluster, con
     const double k0 = parzen(-1.0), k1 = parzen(0.0);
     // smoothing along the reference axis straight from the integer counts, own rows + halo
     const int ua = max(0, f0 - 1), ub = min(fb, f1 + 1);
-    for (int i = tid; i < (ub - ua) * rb; i += FIN_CTA_THREADS) {
-        const int f = ua + i / rb, r = i % rb;
-        const uint32_t *row = hist + (size_t)f * rb;
-        const double m = (double)row[r];
-        const double l = r > 0 ? (double)row[r - 1] : 0.0;
-        const double rr = r + 1 < rb ? (double)row[r + 1] : 0.0;
-        U[(f - f0 + 1) * rb + r] = smooth3(r > 0, l, m, r + 1 < rb, rr, k0, k1);
-    }
+    if (act)
+        for (int i = tid; i < (ub - ua) * rb; i += FIN_CTA_THREADS) {
+            const int f = ua + i / rb, r = i % rb;
+            const uint32_t *row = hist + (size_t)f * rb;
+            const double m = (double)__ldcg(&row[r]);
+            const double l = r > 0 ? (double)__ldcg(&row[r - 1]) : 0.0;
+            const double rr = r + 1 < rb ? (double)__ldcg(&row[r + 1]) : 0.0;
+            U[(f - f0 + 1) * rb + r] = smooth3(r > 0, l, m, r + 1 < rb, rr, k0, k1);
+        }
     __syncthreads();
     // output table set: the one not holding the best position (a level's starting point and a
     // standalone evaluation write the first set)
@@ -892,18 +898,20 @@ __device__ __forceinline__ void finalize_cluster(cg::cluster_group& cluster, con
     nrb_objective *__restrict__ last = second ? last1 : last0;
     // smoothing along the floating axis of the own rows
     double mass = 0.0, z2 = 0.0;
-    for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) {
-        const int f = f0 + i / rb;
-        const double *u = U + (i / rb + 1) * rb + i % rb;
-        const double v = smooth3(f > 0, f > 0 ? u[-rb] : 0.0, u[0], f + 1 < fb, f + 1 < fb ? u[rb] : 0.0, k0, k1);
-        T[i] = v;
-        mass += v;
-    }
+    if (act)
+        for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) {
+            const int f = f0 + i / rb;
+            const double *u = U + (i / rb + 1) * rb + i % rb;
+            const double v = smooth3(f > 0, f > 0 ? u[-rb] : 0.0, u[0], f + 1 < fb, f + 1 < fb ? u[rb] : 0.0, k0, k1);
+            T[i] = v;
+            mass += v;
+        }
     // the bending-energy sum: the same partition and tree in every block, so the same value
     block_sum3w<FIN_WARPS>(mass, be, z2, red);
     if (tid == 0) part[0] = mass;
     cluster.sync();  // every block has read its halo counts; partial masses visible
-    for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) hist[(size_t)f0 * rb + i] = 0u;  // next evaluation
+    if (act)
+        for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) hist[(size_t)f0 * rb + i] = 0u;  // next evaluation
     double total = 0.0;
     {
         double pq[FIN_CLUSTER];
@@ -914,29 +922,31 @@ __device__ __forceinline__ void finalize_cluster(cg::cluster_group& cluster, con
     }
     // normalised own rows, their logs and the joint entropy
     double hj = 0.0;
-    for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) {
-        const double p = T[i] / total;
-        T[i] = p;
-        double l = 0.0;
-        if (p > 0) {
-            l = log(p);
-            hj -= p * l;
+    if (act)
+        for (int i = tid; i < nrow * rb; i += FIN_CTA_THREADS) {
+            const double p = T[i] / total;
+            T[i] = p;
+            double l = 0.0;
+            if (p > 0) {
+                l = log(p);
+                hj -= p * l;
+            }
+            pro[(size_t)f0 * rb + i] = p;
+            logt[(size_t)f0 * rb + i] = l;
         }
-        pro[(size_t)f0 * rb + i] = p;
-        logt[(size_t)f0 * rb + i] = l;
-    }
     __syncthreads();
     // partial reference marginal over the own rows (U is free now), in floating-bin order
     double *R = U;
-    for (int r = tid; r < rb; r += FIN_CTA_THREADS) {
-        double sum = 0.0;
-        for (int k = 0; k < nrow; ++k) sum += T[k * rb + r];
-        R[r] = sum;
-    }
+    if (act)
+        for (int r = tid; r < rb; r += FIN_CTA_THREADS) {
+            double sum = 0.0;
+            for (int k = 0; k < nrow; ++k) sum += T[k * rb + r];
+            R[r] = sum;
+        }
     // floating marginal of the own rows: eight lanes per row, each summing a strided share of the
     // reference bins, combined by shuffles in a fixed order
     double hw = 0.0;
-    {
+    if (act) {  // whole warps: the shuffles below stay within active warps
         const int sub = tid & 7;
         // the trip count is the same for every thread, so all lanes reach the shuffles
         for (int k0 = 0; k0 < rpc; k0 += FIN_CTA_THREADS / 8) {
@@ -962,7 +972,7 @@ __device__ __forceinline__ void finalize_cluster(cg::cluster_group& cluster, con
     // reference marginal: the blocks' partial sums added in block order (a fixed order, so the
     // result repeats bit for bit; it differs from a sequential sum only in the last bits)
     double hr = 0.0;
-    for (int r = c + FIN_CLUSTER * tid; r < rb; r += FIN_CLUSTER * FIN_CTA_THREADS) {
+    for (int r = c + FIN_CLUSTER * tid; act && r < rb; r += FIN_CLUSTER * FIN_CTA_THREADS) {
         double rq[FIN_CLUSTER];
 #pragma unroll
         for (int q = 0; q < FIN_CLUSTER; ++q) rq[q] = cluster.map_shared_rank(R, q)[r];
@@ -1040,7 +1050,7 @@ __device__ __forceinline__ void finalize_cluster(cg::cluster_group& cluster, con
     auto token = cluster.barrier_arrive();
     __syncthreads();  // the decision in sctl
     // the store of an accepted trial position (k_accept's operations) in the same launch
-    if ((kMode == FIN_LINE || kMode == FIN_BATCH_LINE) && A.acc_n > 0 && sctl.accepted) {
+    if ((kMode == FIN_LINE || kMode == FIN_BATCH_LINE) && A.acc_n > 0 && sctl.accepted && act) {
         const float scale = -sctl.step_len;
         for (long long i = (long long)c * FIN_CTA_THREADS + tid; i < A.acc_n;
              i += (long long)FIN_CLUSTER * FIN_CTA_THREADS)

@@ -49,13 +49,16 @@ def test_batch_equals_plain(pairs, plain):
         _same(a, b)
 
 
-@pytest.mark.parametrize("percent,concurrency", [(1, 8), (100, 8), (50, 3), (50, 1)])
-def test_batch_scheduling_changes_nothing(pairs, plain, percent, concurrency):
-    """The gradient stage run as soon as one pair waits, only when all do, and groups of 3 and of
-    1 pair: the same results bit for bit (the batch holds each pair twice, so a group also mixes
-    copies of the same registration)."""
+@pytest.mark.parametrize("percent,concurrency,group_mb", [(1, 8, 96), (100, 8, 0), (50, 3, 96), (50, 1, 96),
+                                                       (50, 8, 1)])
+def test_batch_scheduling_changes_nothing(pairs, plain, percent, concurrency, group_mb):
+    """The gradient stage run as soon as one pair waits, only when all do, groups of 3 and of 1
+    pair, no image cap on a group and a cap that makes every pair a group of its own: the same
+    results bit for bit, each at its own index although the batch is grouped by size (the batch
+    holds each pair twice, so a group also mixes copies of the same registration)."""
     params = _params()
     params.batch_gradient_percent = percent
+    params.batch_group_mb = group_mb
     out = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs * 2], params,
                              concurrency=concurrency)
     for i, a in enumerate(out):
