@@ -471,7 +471,7 @@ def run_b200(args):
                      "algorithmic_bytes_per_launch": bytes_l / n_l if n_l else None,
                      "time_share": share},
         "e2e": {"value": e2e_value, "unit": "registrations/s", "h2d_bytes_per_step": 2 * 4 * nx * ny * nz,
-                "d2h_bytes_per_step": 4 * ncpp},
+                "d2h_bytes_per_step": 4 * ncpp, "step_ms": [round(1e3 * t, 2) for t in e2e_s]},
         "gpu_launches": int(launches),
         "evaluations_per_s": sum(r.objective_evaluations + r.gradient_evaluations for r in results)
                              / (sum(step_ms) / 1e3),

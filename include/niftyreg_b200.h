@@ -276,12 +276,12 @@ typedef struct nrb_f3d_params {
                                * resident blocks) and keeps the fastest in the process's walk
                                * table (nrb_autotune_entries); 0: the cost model's plans. The
                                * walk plan moves no value, so results are identical either way. */
-    int32_t batch_group_mb;   /* nrb_f3d_register_batch and the grouping server: a group of pairs
-                               * registered together holds at most this many MB of finest-level
-                               * images (reference + floating), so that a line-search step's
-                               * images stay in L2 between steps (default 96; a pair larger than
-                               * that is a group of its own; 0: no cap). Scheduling only: results
-                               * do not depend on it. */
+    int32_t batch_group_mb;   /* nrb_f3d_register_batch and the grouping server: when > 0, a
+                               * group of pairs registered together holds at most this many MB of
+                               * finest-level images (reference + floating); a pair larger than
+                               * that is a group of its own. 0 (default): no cap; larger groups
+                               * measured faster on every mix tried. Scheduling only: results do
+                               * not depend on it. */
 } nrb_f3d_params;
 
 typedef struct nrb_f3d_result {
@@ -537,8 +537,8 @@ void nrb_server_destroy(nrb_server *s);
 /* n registrations advanced together (no counterpart in the reference, which registers one pair
  * per reg_f3d run). The pairs are taken in order of size in groups of at most `concurrency`
  * (<= 64) whose summed footprints fit in hbm_budget_bytes (<= 0: 80% of the free device memory)
- * and whose finest-level images fit in p->batch_group_mb; a group
- * runs level by level, each level as one CUDA graph in which every stage -- the line-search
+ * and, when p->batch_group_mb is set, whose finest-level images fit in it; a group runs level
+ * by level, each level as one CUDA graph in which every stage -- the line-search
  * objective, its finalize, the gradient, the node convolution, the conjugate-gradient direction
  * -- is one launch over all the pairs that need it. Each pair's arithmetic is that of its plain
  * registration, so results[i] and pairs[i].cpp_out_host equal nrb_f3d_register_host's for pair i

@@ -1287,7 +1287,7 @@ extern "C" void nrb_f3d_default_params(nrb_f3d_params *p) {
     p->batch_gradient_percent = 50;
     p->floating_texture = 1;
     p->autotune = 1;
-    p->batch_group_mb = 96;
+    p->batch_group_mb = 0;
 }
 
 extern "C" nrb_status nrb_f3d_grid_dims(const int32_t ref_dim[3], const float ref_pixdim[3], const nrb_f3d_params *p,
