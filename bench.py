@@ -74,9 +74,12 @@ def parse():
                          "the rate (every rate runs for about the same time)")
     ap.add_argument("--rates", default="1,2,5,10,20,30,40,50", help="served: Poisson arrival rates (requests/s)")
     ap.add_argument("--slots", type=int, default=2, help="served: workers (groups registered at once)")
-    ap.add_argument("--max-group", type=int, default=64, help="served: requests registered together at most")
+    ap.add_argument("--max-group", type=int, default=16,
+                    help="served: requests registered together at most during the rate sweep")
     ap.add_argument("--burst", type=int, default=300,
                     help="served: requests of the capacity run, submitted at once after the rate sweep")
+    ap.add_argument("--burst-group", type=int, default=64, help="served: requests registered together at most "
+                    "in the capacity run")
     ap.add_argument("--shape", default=None, help="kernel-only mode: nz,ny,nx of the volume (default: the workload's)")
     ap.add_argument("--group-mb", type=int, default=None,
                     help="batched/served: finest-level image MB a group of pairs may hold (default: the library's)")
@@ -719,14 +722,15 @@ def run_served(args, emit=True):
     # server can take, so their achieved rate is the offered one)
     n_burst = max(1, args.burst)
     reqs = [pool[shapes[int(i)]][int(rng.integers(0, 2))] for i in rng.choice(len(shapes), n_burst, p=probs)]
-    with nrb.Server(slots=args.slots, max_group=args.max_group) as srv:
+    with nrb.Server(slots=args.slots, max_group=args.burst_group) as srv:
         t_start = time.perf_counter()
         tickets = [srv.submit(p.reference, p.floating, p.pixdim, params) for p in reqs]
         outs = [srv.wait(t) for t in tickets]
         t_end = time.perf_counter()
         peak_group = srv.peak_group()
     lat_ms = np.array([o[3] for o in outs]) * 1e3
-    capacity = {"requests": n_burst, "achieved_req_s": n_burst / (t_end - t_start), "peak_group": peak_group,
+    capacity = {"requests": n_burst, "max_group": args.burst_group,
+                "achieved_req_s": n_burst / (t_end - t_start), "peak_group": peak_group,
                 "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99))}
     capacity["vs_plain"] = capacity["achieved_req_s"] / plain_rate
     clocks = sampler.stop()
