@@ -47,6 +47,9 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 // start while its predecessor's last blocks are still running; it must wait here before it reads
 // anything the predecessor writes. Without that launch attribute the wait returns at once.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Lets the launch that depends on this one (programmatic stream serialization) be scheduled now:
+// its blocks may start and do whatever does not need this launch's results, then pdl_wait().
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
 // cudaLaunchKernelEx with programmatic stream serialization when `pdl` is set.
 template <typename... KArgs, typename... Args>

@@ -524,6 +524,7 @@ k_objective(WalkParams P, const float *__restrict__ ref, const float *__restrict
     const int nbins = P.rb * P.fb;
     zero_hist(h, nbins);
     if (kTrial) pdl_wait();  // the trial position and step length come from the previous launch
+    pdl_launch_dependents();  // the finalize may start its preamble (it waits for the counts)
     const float scale = kTrial ? -step->cur_len : 0.f;
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x)
         objective_item<kXs, kDiag>(P, S, h, X, item, ref, flo, mask, cpp, kTrial ? grad : nullptr, scale);
@@ -872,6 +873,9 @@ __device__ __forceinline__ void finalize_cluster(cg::cluster_group& cluster, con
     double be = 0.0;
     if (act)
         for (int i = tid; i < n_be; i += FIN_CTA_THREADS) be += __ldcg(&be_partials[i]);
+    // the state and the partials come from earlier launches (the bending-energy pass is a full
+    // dependency); the counts from the objective pass this launch may have started beside
+    pdl_wait();
     const int nj = rb * fb;
     const int rpc = (fb + FIN_CLUSTER - 1) / FIN_CLUSTER;
     const int f0 = min(fb, c * rpc), f1 = min(fb, f0 + rpc), nrow = f1 - f0;
@@ -1061,7 +1065,7 @@ __device__ __forceinline__ void finalize_cluster(cg::cluster_group& cluster, con
 
 __global__ void __cluster_dims__(FIN_CLUSTER, 1, 1) __launch_bounds__(FIN_CTA_THREADS)
 k_nmi_finalize(FinArgs A, cudaGraphConditionalHandle line) {
-    pdl_wait();  // the counts come from the objective pass
+    pdl_launch_dependents();  // the store of an accepted position (large grids) may queue behind it
     cg::cluster_group cluster = cg::this_cluster();
     if (A.ctl) finalize_cluster<FIN_LINE>(cluster, A, line);
     else finalize_cluster<FIN_PLAIN>(cluster, A, line);
