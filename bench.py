@@ -59,8 +59,9 @@ def parse():
                     help="1: the registrations sample the floating image through its layered texture; 0: loads")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain mode: skip the shortened batched and served runs attached to the line")
-    ap.add_argument("--mode", choices=["plain", "batched", "served", "warp", "f3d2", "ct", "refcuda"],
-                    default="plain")
+    ap.add_argument("--mode", choices=["plain", "batched", "served", "warp", "f3d2", "ct"], default="plain")
+    ap.add_argument("--reference-platform", choices=["cpu", "cuda"], default="cpu",
+                    help="--impl reference: the reference's CPU path (default) or its own CUDA platform")
     ap.add_argument("--pairs", type=int, default=64, help="batched: number of pairs")
     ap.add_argument("--concurrency", type=int, default=16, help="batched/served: concurrent registrations")
     ap.add_argument("--grad-percent", type=int, default=50,
@@ -807,19 +808,24 @@ def run_ct(args):
     return 0
 
 
-def run_refcuda(args):
-    """The reference's own CUDA platform (reg-lib/cuda built for sm_100a into oracle/_refcuda,
-    reg_f3d<float>::Run with PlatformType::Cuda) on this GPU: one registration of the 64^3
+def run_reference_cuda(args):
+    """The reference arm on the reference's own CUDA platform (--impl reference
+    --reference-platform cuda): reg-lib/cuda built for sm_100a into oracle/_refcuda,
+    reg_f3d<float>::Run with PlatformType::Cuda on this GPU. One registration of the 64^3
     one-level workload (1 level, 100 counted iterations, BE 0.005, 64 bins, 5-voxel grid) and,
     unless --shape picks another size, --steps registrations of the brain-like workload, each
     timed with the host clock around Run (host images in, grid out: the reference's CUDA content
     copies the images to the device at every level). The library makes its own CUDA context, so
-    this mode runs no other GPU work in the process."""
+    this arm runs no other GPU work in the process; under torchrun only rank 0 runs it."""
+    rank, _, _ = dist_env()
+    if rank != 0:
+        return 0
     import oracle
     from niftyreg_b200 import phantom
     if not oracle.refcuda_available():
-        print(json.dumps({"mode": "refcuda", "unavailable": "oracle/_refcuda/libnrref_cuda.so not built "
-                          "(make -C oracle refcuda, needs the reference sources)"}))
+        print(json.dumps({"impl": "reference", "reference_platform": "cuda",
+                          "unavailable": "oracle/_refcuda/libnrref_cuda.so not built (make -C oracle refcuda, "
+                                         "needs the reference sources)"}))
         return 0
     eye = np.eye(4, dtype=np.float32)
     sampler = ClockSampler(0)
@@ -842,12 +848,15 @@ def run_refcuda(args):
                      "per_level_seconds": [float(st[7 + 3 * l]) for l in range(LEVELS)]})
     clocks = sampler.stop()
     sec = float(np.mean([r["seconds"] for r in runs]))
-    line = {"mode": "refcuda", "impl": "reference-cuda", "metric": METRIC, "value": 1.0 / sec,
-            "unit": "registrations/s", "n_gpus": 1, "steps": len(runs), "higher_is_better": True, "dtype": "f32",
-            "data": "synthetic", "evaluations_per_s": float(np.mean([r["evaluations_per_s"] for r in runs])),
+    line = {"impl": "reference", "reference_platform": "cuda", "metric": METRIC, "value": 1.0 / sec,
+            "unit": "registrations/s", "n_gpus": 1, "steps": len(runs), "warmup": 0, "ms_per_step": sec * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "evaluations_per_s": float(np.mean([r["evaluations_per_s"] for r in runs])),
             "registrations": runs, "blobs_64": out["blobs_64"],
             "config": {"workload": WORKLOAD if shape == SHAPE else f"brain-like phantom {shape}",
+                       "parallelism": "replicas",
                        "timing": "host wall clock around reg_f3d<float>::Run on the reference CUDA platform"},
+            "e2e": {"value": 1.0 / sec, "unit": "registrations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "clocks": clocks}
     print(json.dumps(line))
     return 0
@@ -1064,7 +1073,7 @@ def run_f3d2(args):
 def main():
     args = parse()
     if args.impl == "reference":
-        return run_reference(args)
+        return run_reference_cuda(args) if args.reference_platform == "cuda" else run_reference(args)
     if args.kernel:
         return run_kernel_only(args)
     if args.mode == "batched":
@@ -1077,8 +1086,7 @@ def main():
         return run_warp(args)
     if args.mode == "ct":
         return run_ct(args)
-    if args.mode == "refcuda":
-        return run_refcuda(args)
+
     return run_b200(args)
 
 
