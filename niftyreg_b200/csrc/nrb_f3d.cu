@@ -1043,8 +1043,9 @@ nrb_status F3dRegistration::InitLevel(int level, float& max_step) {
         NRB_TRY(pad_volume(flo_.p, fh.dim, margin_, pad_, flo_pad_.p, &flo_org_, st_));
         dev_free(flo_.p, flo_.st);
         flo_.p = nullptr;
-        // the padded copy as a layered texture: the fused passes gather its 2x2 footprints
-        if (p_.floating_texture) {
+        // the padded copy as a layered texture: the fused passes gather its 2x2 footprints (a
+        // margin of 2 or more keeps every clamped footprint inside the padding)
+        if (p_.floating_texture && margin_ >= 2) {
             const int w = fh.dim[0] + 2 * margin_, h = fh.dim[1] + 2 * margin_, l = fh.dim[2] + 2 * margin_;
             flo_texture_release(ftex_);
             NRB_TRY(flo_texture_acquire(w, h, l, ftex_));

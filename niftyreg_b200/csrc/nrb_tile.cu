@@ -320,9 +320,10 @@ __device__ __forceinline__ void gather_footprint(unsigned long long tex, int lay
     v[0][0] = r3;
 }
 
-// tex (optional): the same floating image with its margin as a 2D layered float array (layer k =
-// slice k - margin, texel (i, j) = voxel (i - margin, j - margin)); warps on the plain path then
-// fetch each slice's 2x2 footprint with one gather instead of four loads.
+// tex (optional; needs margin >= 2): the same floating image with its margin as a 2D layered
+// float array (layer k = slice k - margin, texel (i, j) = voxel (i - margin, j - margin)); every
+// sample then fetches each slice's 2x2 footprint with one gather instead of four loads, with no
+// warp vote and no clamped path.
 template <bool kGrad, int kDiag = -1>
 __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, unsigned long long tex, int fnx, int fny,
                                                 int fnz, int sy, int sz, int margin, const Mat34& M,
@@ -339,10 +340,18 @@ __device__ __forceinline__ void sample_floating(const float *__restrict__ flo, u
     const bool plain = (unsigned)(px + margin) < (unsigned)(fnx + 2 * margin - 1) &&
                        (unsigned)(py + margin) < (unsigned)(fny + 2 * margin - 1) &&
                        (unsigned)(pz + margin) < (unsigned)(fnz + 2 * margin - 1);
-    if (__all_sync(__activemask(), plain) && tex) {
+    if (tex) {
+        // every sample, no vote: the footprint's first texel (p + margin on each axis) clamped to
+        // [0, n + 2 margin - 2]. Unclamped, that is the plain path's footprint; clamped, both taps
+        // on that axis lie outside the volume (p < -margin or p > n + margin - 2) and the clamped
+        // footprint lies in the margin (margin >= 2), so they read the padding value, as the
+        // clamped path substitutes it. Texels past the padded extent are never read.
         const float off = (float)(margin + 1);
-        gather_footprint(tex, pz + margin, flx + off, fly + off, v[0]);
-        gather_footprint(tex, pz + margin + 1, flx + off, fly + off, v[1]);
+        const float tx = fminf(fmaxf(flx + off, 1.f), (float)(fnx + 2 * margin - 1));
+        const float ty = fminf(fmaxf(fly + off, 1.f), (float)(fny + 2 * margin - 1));
+        const int layer = min(max(pz + margin, 0), fnz + 2 * margin - 2);
+        gather_footprint(tex, layer, tx, ty, v[0]);
+        gather_footprint(tex, layer + 1, tx, ty, v[1]);
     } else if (__all_sync(__activemask(), plain)) {
         const float *p = flo + (pz * sz + py * sy + px);
         v[0][0][0] = __ldg(p);
@@ -1453,7 +1462,7 @@ nrb_status launch_fused_objective(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geo
                                   const float *grad, const OptState *step, int flo_margin) {
     WalkParams P = make_params(ws->walk_obj, g, padding, nmi->rb, nmi->fb);
     set_floating_margin(P, flo_margin);
-    P.ftex = flo_margin > 0 ? ws->flo_tex : 0ull;
+    P.ftex = flo_margin >= 2 ? ws->flo_tex : 0ull;
     const size_t base_smem = walk_smem_bytes(ws->walk_obj) + (size_t)((nmi->rb * nmi->fb + 3) & ~3) * 4;
     const size_t xs_bytes = (size_t)3 * P.sc * P.sb * 32 * 4;
     // the x-contracted rows when two blocks per SM still fit
@@ -1487,7 +1496,7 @@ nrb_status launch_fused_gradient(nrb_workspace *ws, nrb_nmi *nmi, const nrb_geom
                                  cudaStream_t st, const OptState *sel, int flo_margin) {
     WalkParams P = make_params(ws->walk_grad, g, padding, nmi->rb, nmi->fb);
     set_floating_margin(P, flo_margin);
-    P.ftex = flo_margin > 0 ? ws->flo_tex : 0ull;
+    P.ftex = flo_margin >= 2 ? ws->flo_tex : 0ull;
     // an FP32 copy of the log table rides in shared memory when it fits (64 bins: 19 KB,
     // 128 bins: 70 KB); larger tables use the FP64 window on the global table
     const size_t log_bytes = (size_t)nmi->total * sizeof(float);
@@ -1728,7 +1737,7 @@ nrb_status batch_walks(nrb_workspace *ws, const nrb_nmi *nmi, const nrb_geometry
     set_floating_margin(wo, flo_margin);
     wg = make_params(ws->walk_grad, g, padding, nmi->rb, nmi->fb);
     set_floating_margin(wg, flo_margin);
-    wo.ftex = wg.ftex = flo_margin > 0 ? ws->flo_tex : 0ull;
+    wo.ftex = wg.ftex = flo_margin >= 2 ? ws->flo_tex : 0ull;
     wg.log_in_smem = (size_t)nmi->total * sizeof(float) <= 96 * 1024;
     return NRB_OK;
 }
