@@ -540,7 +540,10 @@ void nrb_server_destroy(nrb_server *s);
  * and, when p->batch_group_mb is set, whose finest-level images fit in it; a group runs level
  * by level, each level as one CUDA graph in which every stage -- the line-search
  * objective, its finalize, the gradient, the node convolution, the conjugate-gradient direction
- * -- is one launch over all the pairs that need it. Each pair's arithmetic is that of its plain
+ * -- is one launch over all the pairs that need it. When the pairs make two or more groups that
+ * each fit in half the budget, two host threads run the groups, so that one group's uploads,
+ * pyramids and level set-up overlap the other's graphs on the device; otherwise the groups run
+ * one after another with the whole budget. Each pair's arithmetic is that of its plain
  * registration, so results[i] and pairs[i].cpp_out_host equal nrb_f3d_register_host's for pair i
  * alone, bit for bit. The pairs of a group share the parameters, so they share the bin counts;
  * they may differ in size and spacing. */

@@ -10,7 +10,8 @@
 // device. Each pair's arithmetic in a group is that of its plain registration, so every result
 // equals nrb_f3d_register_host's for the same request alone, whatever it was grouped with.
 //
-// The batch entry point forms groups the same way from the pairs it is given.
+// The batch entry point forms groups the same way from the pairs it is given and runs them on
+// two such workers when they fit in half the budget each.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -347,40 +348,85 @@ extern "C" nrb_status nrb_f3d_register_batch(const nrb_pair *pairs, int n, const
     for (int i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return voxels_of(pairs[a]) < voxels_of(pairs[b]); });
     const int64_t group_bytes = (int64_t)std::max(0, p->batch_group_mb) << 20;
-    cudaStream_t st = nullptr;
-    NRB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    nrb_status s = NRB_OK;
-    std::vector<nrb_pair> gp;
-    std::vector<nrb_f3d_result> gr;
-    for (int i0 = 0; i0 < n && s == NRB_OK;) {
-        // the next group: pairs while they fit in the HBM budget (a pair larger than the budget
-        // alone is refused) and their finest-level images in the group cap (the first pair
-        // always joins)
-        int64_t used = 0, images = 0;
-        int i1 = i0;
-        while (i1 < n && i1 - i0 < group_max) {
-            const nrb_pair& q = pairs[order[i1]];
-            const int64_t f = registration_footprint(q.dim, q.pixdim, p);
-            const int64_t img = image_bytes(q);
-            if (used + f > budget) break;
-            if (i1 > i0 && group_bytes > 0 && images + img > group_bytes) break;
-            used += f;
-            images += img;
-            ++i1;
+    // the groups: pairs while they fit in the group budget (a pair larger than it alone is
+    // refused) and their finest-level images in the group cap (the first pair always joins)
+    auto plan = [&](int64_t gbudget, std::vector<std::pair<int, int>>& groups) {
+        groups.clear();
+        for (int i0 = 0; i0 < n;) {
+            int64_t used = 0, images = 0;
+            int i1 = i0;
+            while (i1 < n && i1 - i0 < group_max) {
+                const nrb_pair& q = pairs[order[i1]];
+                const int64_t f = registration_footprint(q.dim, q.pixdim, p);
+                const int64_t img = image_bytes(q);
+                if (used + f > gbudget) break;
+                if (i1 > i0 && group_bytes > 0 && images + img > group_bytes) break;
+                used += f;
+                images += img;
+                ++i1;
+            }
+            if (i1 == i0) return false;
+            groups.emplace_back(i0, i1);
+            i0 = i1;
         }
-        if (i1 == i0) {
-            s = fail(NRB_ERR_OOM, "nrb_f3d_register_batch: a pair is larger than the HBM budget");
-            break;
-        }
-        gp.clear();
-        for (int i = i0; i < i1; ++i) gp.push_back(pairs[order[i]]);
-        gr.assign(i1 - i0, nrb_f3d_result{});
-        s = register_batch_fused(gp.data(), i1 - i0, p, gr.data(), st, pct);
-        if (s == NRB_OK && results)
-            for (int i = i0; i < i1; ++i) results[order[i]] = gr[i - i0];
-        i0 = i1;
+        return true;
+    };
+    // two workers, each with half the budget, when that still makes groups and there are two or
+    // more: one group's uploads, pyramids and level set-up (host work) overlap the other's
+    // graphs on the device. Otherwise one worker with the whole budget.
+    std::vector<std::pair<int, int>> groups;
+    int workers = 2;
+    if (!plan(budget / 2, groups) || groups.size() < 2) {
+        workers = 1;
+        if (!plan(budget, groups)) return fail(NRB_ERR_OOM, "nrb_f3d_register_batch: a pair is larger than the HBM budget");
     }
-    cudaStreamSynchronize(st);
-    cudaStreamDestroy(st);
-    return s;
+    std::mutex mu;
+    size_t next = 0;
+    nrb_status first_error = NRB_OK;
+    std::string first_message;
+    auto work = [&]() {
+        cudaStream_t st = nullptr;
+        nrb_status s = NRB_OK;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            s = fail(NRB_ERR_CUDA, "nrb_f3d_register_batch: stream creation failed");
+        }
+        std::vector<nrb_pair> gp;
+        std::vector<nrb_f3d_result> gr;
+        while (s == NRB_OK) {
+            size_t g;
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                if (first_error != NRB_OK || next >= groups.size()) break;
+                g = next++;
+            }
+            const int i0 = groups[g].first, i1 = groups[g].second;
+            gp.clear();
+            for (int i = i0; i < i1; ++i) gp.push_back(pairs[order[i]]);
+            gr.assign(i1 - i0, nrb_f3d_result{});
+            s = register_batch_fused(gp.data(), i1 - i0, p, gr.data(), st, pct);
+            if (s == NRB_OK && results)
+                for (int i = i0; i < i1; ++i) results[order[i]] = gr[i - i0];
+        }
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+        if (s != NRB_OK) {
+            std::lock_guard<std::mutex> lock(mu);
+            if (first_error == NRB_OK) {
+                first_error = s;
+                first_message = nrb_last_error();
+            }
+        }
+    };
+    if (workers == 1) {
+        work();
+    } else {
+        std::thread other(work);
+        work();
+        other.join();
+    }
+    if (first_error != NRB_OK) return fail(first_error, first_message);
+    return NRB_OK;
 }

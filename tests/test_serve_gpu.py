@@ -65,6 +65,20 @@ def test_batch_scheduling_changes_nothing(pairs, plain, percent, concurrency, gr
         _same(a, plain[i % len(pairs)])
 
 
+def test_batch_budget_for_one_worker(pairs, plain):
+    """A budget that holds the largest pair but not in half: the groups run one after another
+    on one worker (two workers take half the budget each), with the same results."""
+    params = _params()
+    big = max(nrb.footprint(p.dim, p.pixdim, params) for p in pairs)
+    out = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], params, concurrency=4,
+                             budget_bytes=int(1.5 * big))
+    for a, b in zip(out, plain):
+        _same(a, b)
+    with pytest.raises(nrb.NrbError, match="larger than the HBM budget"):
+        nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], params, concurrency=4,
+                           budget_bytes=big // 2)
+
+
 def test_batch_without_bending_energy_and_one_level(pairs):
     """No bending-energy stages (weight 0) and a single level, against the plain path."""
     params = nrb.default_params(levels=1, max_iterations=25, bending_energy=0.0, spacing=(-5.0,),
