@@ -380,6 +380,8 @@ extern "C" nrb_status nrb_f3d_register_batch(const nrb_pair *pairs, int n, const
         workers = 1;
         if (!plan(budget, groups)) return fail(NRB_ERR_OOM, "nrb_f3d_register_batch: a pair is larger than the HBM budget");
     }
+    int device = 0;
+    NRB_CUDA(cudaGetDevice(&device));
     std::mutex mu;
     size_t next = 0;
     nrb_status first_error = NRB_OK;
@@ -387,7 +389,8 @@ extern "C" nrb_status nrb_f3d_register_batch(const nrb_pair *pairs, int n, const
     auto work = [&]() {
         cudaStream_t st = nullptr;
         nrb_status s = NRB_OK;
-        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+        // the caller's device (a new host thread starts on device 0)
+        if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
             cudaGetLastError();
             s = fail(NRB_ERR_CUDA, "nrb_f3d_register_batch: stream creation failed");
         }
