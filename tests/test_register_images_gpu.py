@@ -90,6 +90,26 @@ def test_identity_images_are_the_dims_and_spacing_registration():
     assert warped.shape == p.reference.shape
 
 
+@pytest.mark.parametrize("padding", [float("nan"), 0.0])
+def test_partial_overlap_margins_change_nothing(oriented, padding):
+    """A floating image covering a third of the reference's space: most samples fall far outside
+    it, beyond any margin, where the texture path clamps its footprints into the margin and the
+    dense path selects the padding value per tap; margins 0, 2 and 8, with and without the
+    texture, give the same registration bit for bit."""
+    o = oriented
+    flo = np.ascontiguousarray(o.flo[:, :, :22])
+    runs = [nrb.register_images(o.ref, o.rpix, o.rxyz, flo, o.fpix, o.fxyz,
+                                _params(floating_margin=m, floating_texture=t, padding=padding), warped=False)
+            for m, t in ((0, 0), (2, 1), (8, 1), (8, 0))]
+    g0, _, _, r0 = runs[0]
+    assert r0.objective_evaluations > 0
+    for g, _, _, r in runs[1:]:
+        assert r.objective_evaluations == r0.objective_evaluations
+        assert r.gradient_evaluations == r0.gradient_evaluations
+        assert r.final_nmi == r0.final_nmi
+        assert np.array_equal(g, g0)
+
+
 def test_oriented_images_match_the_reference(oriented):
     import oracle
     if not oracle.ref_available():
