@@ -89,7 +89,7 @@ def parse():
                     help="batched/served: finest-level image MB a group of pairs may hold (default: the library's)")
     ap.add_argument("--batch-shapes", default=None,
                     help="batched: sizes to draw from, 'nz,ny,nx;nz,ny,nx;...' (default: config 3's four sizes)")
-    ap.add_argument("--kernel", choices=["objective", "gradient", "velocity", "compose"], default=None,
+    ap.add_argument("--kernel", choices=["objective", "gradient", "velocity", "compose", "ops"], default=None,
                     help="profiling mode: run only `--steps` fused evaluations at the finest level "
                          "of the workload (for ncu captures); prints per-launch device times")
     return ap.parse_args()
@@ -147,6 +147,8 @@ def run_kernel_only(args):
     shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else SHAPE
     if args.kernel in ("velocity", "compose"):
         return run_velocity_only(args, shape)
+    if args.kernel == "ops":
+        return run_ops_only(args, shape)
     pair = phantom.brain_pair(shape, seed=args.seed)
     nz, ny, nx = shape
     dim, pix = (nx, ny, nz), (1.0, 1.0, 1.0)
@@ -179,6 +181,100 @@ def run_kernel_only(args):
                       "timing": {k: {"launches": v[0], "avg_us": (v[1] / v[0] * 1e3) if v[0] else None,
                                      "GBps": (v[2] / (v[1] / 1e3) / 1e9) if v[1] else None}
                                  for k, v in out.items()}}))
+    return 0
+
+
+def run_ops_only(args, shape):
+    """Each standalone entry point of the hot path (the staged, per-`Compute`-call kernels a
+    platform binding calls; the fused evaluation is --kernel objective / gradient) once per
+    repetition on the workload's finest level: rescaled brain-like pair, 5 mm grid with
+    N(0, 3 mm) displacements. CUDA events on the launching stream around each call, a 256 MiB
+    buffer written between calls (inputs larger than L2 or flushed), median of --steps calls
+    after --warmup; achieved = the op's algorithmic bytes / its device time."""
+    import torch
+    import ctypes
+    import niftyreg_b200 as nrb
+    from niftyreg_b200 import phantom
+
+    pair = phantom.brain_pair(shape, seed=args.seed)
+    nz, ny, nx = shape
+    dim, pix = (nx, ny, nz), (1.0, 1.0, 1.0)
+    cdim, cpix, cxyz = nrb.control_grid_header(dim, pix, (5.0, 5.0, 5.0))
+    rng = np.random.default_rng(args.seed)
+    cx, cy, cz = cdim
+    zz, yy, xx = np.meshgrid(np.arange(cz), np.arange(cy), np.arange(cx), indexing="ij")
+    ident = np.concatenate([(5.0 * v - 5.0).ravel() for v in (xx, yy, zz)]).astype(np.float32)
+    cpp = ident + rng.normal(0, 3.0, ident.size).astype(np.float32)
+    g = nrb.make_geometry(dim, pix, nrb.identity_header(pix), dim, pix, nrb.identity_header(pix), cdim, cpix, cxyz)
+    n, c = nx * ny * nz, int(np.prod(cdim))
+    ref = torch.from_numpy(pair.reference.ravel().copy()).cuda()
+    flo = torch.from_numpy(pair.floating.ravel().copy()).cuda()
+    raw = flo.clone()
+    nrb.intensity_rescale(ref, n, 2.0, BINS + 1.0)
+    nrb.intensity_rescale(flo, n, 2.0, BINS + 1.0)
+    cppd = torch.from_numpy(cpp).cuda()
+    ws, nmi = nrb.Workspace(g), nrb.Nmi(BINS + 4, BINS + 4)
+    d = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    w = torch.empty(n, dtype=torch.float32, device="cuda")
+    wg = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    vg = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    node = torch.empty(3 * c, dtype=torch.float32, device="cuda")
+    field = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    img = torch.empty(n, dtype=torch.float32, device="cuda")
+    obj = torch.empty(16, dtype=torch.float64, device="cuda")  # an nrb_objective on the device
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(st.cuda_stream)
+    L = nrb.lib()
+    nrb.get_deformation_field(g, cppd, d, stream=st)
+    nrb.resample_image(g, flo, d, w, stream=st)
+    nrb.get_image_gradient(g, flo, d, wg, stream=st)
+    ops = [
+        ("deformation_field (a1)", 12.0 * n + 12.0 * c, lambda: nrb.get_deformation_field(g, cppd, d, stream=st)),
+        ("resample_linear (a2)", 20.0 * n, lambda: nrb.resample_image(g, flo, d, w, stream=st)),
+        ("image_gradient (a3)", 28.0 * n, lambda: nrb.get_image_gradient(g, flo, d, wg, stream=st)),
+        ("intensity_rescale (a4)", 12.0 * n, lambda: nrb.intensity_rescale(img, n, 2.0, BINS + 1.0, stream=st)),
+        ("nmi_value (a5)", 8.0 * n,
+         lambda: nrb.check(L.nrb_nmi_value(nmi.h, ctypes.byref(g), nrb._p(ref), nrb._p(w), None, nrb._p(obj), None,
+                                           sp))),
+        ("nmi_voxel_gradient (a6)", 32.0 * n, lambda: nrb.nmi_voxel_gradient(nmi, g, ref, w, wg, vg, stream=st)),
+        ("node_convolution (a7 + a8)", 12.0 * n + 12.0 * c,
+         lambda: nrb.convolve_voxel_based_gradient(ws, vg, node, 1.0, stream=st)),
+        ("kernel_convolution_x (a7, whole volume)", 24.0 * n,
+         lambda: nrb.kernel_convolution_cubic(field, 3, dim, pix, 5.0, 0, stream=st)),
+        ("bending_energy (a9)", 12.0 * c,
+         lambda: nrb.check(L.nrb_approx_bending_energy(ws.h, ctypes.byref(ws.g), nrb._p(cppd), nrb._p(obj), None,
+                                                       sp))),
+        ("bending_energy_gradient (a10)", 36.0 * c,
+         lambda: nrb.approx_bending_energy_gradient(ws, cppd, node, 0.005, stream=st)),
+        ("resample_cubic (f2)", 20.0 * n, lambda: nrb.resample_image_order(g, flo, d, w, 3, stream=st)),
+    ]
+    peak, peak_src = peaks()
+    out = {}
+    launches0 = nrb.kernel_launch_count()
+    for name, nbytes, fn in ops:
+        times = []
+        for k in range(args.warmup + args.steps):
+            # in-place ops start from the same input every call (outside the timed region)
+            if name.startswith("kernel_convolution"):
+                field.copy_(vg)
+            if name.startswith("intensity_rescale"):
+                img.copy_(raw)
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            torch.cuda.synchronize()
+            if k >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+        ms = float(np.median(times))
+        gbs = nbytes / (ms / 1e3) / 1e9
+        out[name] = {"median_us": round(ms * 1e3, 2), "algorithmic_mb": round(nbytes / 1e6, 2),
+                     "GBps": round(gbs, 1), "frac_of_" + peak_src + "_hbm": round(gbs / peak, 4)}
+    print(json.dumps({"mode": "kernel-only ops", "voxels": n, "nodes": c, "peak_gbs": peak,
+                      "l2": "256 MiB buffer written before every call", "steps": args.steps, "warmup": args.warmup,
+                      "gpu_launches": nrb.kernel_launch_count() - launches0, "ops": out}))
     return 0
 
 

@@ -514,9 +514,9 @@ nrb_status nrb_f3d_footprint(const int32_t dim[3], const float pixdim[3], const 
  * registers the group as nrb_f3d_register_batch does. Requests that arrive while groups run wait
  * for the next free worker and run beside them; each result is the one nrb_f3d_register_host
  * gives for the same request alone. nrb_server_create uses max_group = 16. While servers exist
- * on a device, its default memory pool keeps freed memory up to the budget (release threshold)
- * and does not reuse memory across streams through inserted dependencies; the pool's previous
- * settings come back when the last server is destroyed. */
+ * on a device, the library's memory pool there keeps freed memory up to the budget (release
+ * threshold); its previous threshold comes back when the last server is destroyed. The
+ * application's default memory pool is not touched. */
 typedef struct nrb_server nrb_server;
 nrb_status nrb_server_create(int slots, int64_t hbm_budget_bytes, nrb_server **out);
 nrb_status nrb_server_create_grouped(int slots, int max_group, int64_t hbm_budget_bytes, nrb_server **out);

@@ -40,6 +40,61 @@ int sm_count() {
     return cache[dev];
 }
 
+// ---- the library's memory pool ----------------------------------------------------------------
+namespace {
+std::mutex g_lib_pool_mu;
+std::vector<cudaMemPool_t> g_lib_pools;  // by device; null until created
+std::vector<char> g_lib_pool_tried;
+}  // namespace
+
+cudaMemPool_t lib_pool() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return lib_pool_of(dev);
+}
+
+cudaMemPool_t lib_pool_of(int dev) {
+    std::lock_guard<std::mutex> lock(g_lib_pool_mu);
+    if ((int)g_lib_pools.size() <= dev) {
+        g_lib_pools.resize(dev + 1, nullptr);
+        g_lib_pool_tried.resize(dev + 1, 0);
+    }
+    if (!g_lib_pool_tried[dev]) {
+        g_lib_pool_tried[dev] = 1;
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
+            uint64_t thr = kLibPoolFloor;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+            // no reuse across streams through inserted dependencies: registrations running on
+            // their own streams (batch workers, server slots) never wait for one another because
+            // the pool handed one of them memory the other freed
+            int no = 0;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+            g_lib_pools[dev] = pool;
+        }
+        cudaGetLastError();
+    }
+    return g_lib_pools[dev];
+}
+
+void lib_pool_keep(uint64_t bytes) {
+    cudaMemPool_t pool = lib_pool();
+    if (!pool) return;
+    std::lock_guard<std::mutex> lock(g_lib_pool_mu);
+    uint64_t cur = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur < bytes)
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &bytes);
+    cudaGetLastError();
+}
+
 // ---- per-kernel timing ----------------------------------------------------------------------
 namespace {
 struct Pending {

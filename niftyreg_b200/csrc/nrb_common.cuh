@@ -68,11 +68,32 @@ inline cudaError_t launch_pdl(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
-// Device allocation tied to an owner's stream: stream-ordered (no device-wide synchronisation,
-// so registrations on other streams keep running) when `st` is set, plain otherwise.
+// The library's own stream-ordered memory pool on the current device (created on first use;
+// null if it cannot be created, and the device's default pool serves instead). Its release
+// threshold starts at kLibPoolFloor, so memory freed between calls stays mapped for the next
+// ones, and lib_pool_keep raises it; the application's default pool is never changed.
+constexpr uint64_t kLibPoolFloor = uint64_t(256) << 20;
+cudaMemPool_t lib_pool();
+cudaMemPool_t lib_pool_of(int device);
+void lib_pool_keep(uint64_t bytes);
+
+// Device allocation tied to an owner's stream: stream-ordered from the library's pool (no
+// device-wide synchronisation, so registrations on other streams keep running) when `st` is set,
+// plain otherwise.
 template <typename T>
 inline cudaError_t dev_alloc(T **p, size_t bytes, cudaStream_t st) {
-    return st ? cudaMallocAsync(reinterpret_cast<void **>(p), bytes, st) : cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    if (!st) return cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    cudaMemPool_t pool = lib_pool();
+    return pool ? cudaMallocFromPoolAsync(reinterpret_cast<void **>(p), bytes, pool, st)
+                : cudaMallocAsync(reinterpret_cast<void **>(p), bytes, st);
+}
+// A call's temporary, stream-ordered from the library's pool on any stream (the legacy default
+// stream included); released with dev_free(p, st) or cudaFreeAsync on the same stream.
+template <typename T>
+inline cudaError_t tmp_alloc(T **p, size_t bytes, cudaStream_t st) {
+    cudaMemPool_t pool = lib_pool();
+    return pool ? cudaMallocFromPoolAsync(reinterpret_cast<void **>(p), bytes, pool, st)
+                : cudaMallocAsync(reinterpret_cast<void **>(p), bytes, st);
 }
 inline void dev_free(void *p, cudaStream_t st) {
     if (!p) return;

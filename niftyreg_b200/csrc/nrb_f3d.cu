@@ -1094,7 +1094,7 @@ nrb_status F3dRegistration::Begin(const float *ref, const float *flo, const Imag
     } else {
         sim_w_ = 1 - penalty;
     }
-    NRB_CUDA(cudaMallocAsync(&obj_, sizeof(nrb_objective), st_));
+    NRB_CUDA(tmp_alloc(&obj_, sizeof(nrb_objective), st_));
     NRB_CUDA(cudaMemsetAsync(obj_, 0, sizeof(nrb_objective), st_));
     const auto tp = std::chrono::steady_clock::now();
     NRB_TRY(BuildPyramid(ref, flo, rd, fd));
@@ -1206,26 +1206,11 @@ nrb_status F3dRegistration::Finish(const float *flo, float *cpp_out, int64_t cap
 
 int64_t registration_footprint(const int32_t dim[3], const float pixdim[3], const nrb_f3d_params *p);
 
-// Raises the release threshold of the device's default memory pool to at least `bytes`: the
-// buffers a registration frees stay in the pool for the next one instead of being unmapped at
-// every synchronisation and mapped again (a measurable share of a registration's time).
-// Never lowers a threshold set by the caller or by a server.
-static void keep_pool(int64_t bytes) {
-    static std::mutex mu;
-    std::lock_guard<std::mutex> lock(mu);
-    int dev = 0;
-    cudaMemPool_t pool;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
-        cudaGetLastError();
-        return;
-    }
-    uint64_t cur = 0;
-    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur < (uint64_t)bytes) {
-        uint64_t v = (uint64_t)bytes;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &v);
-    }
-    cudaGetLastError();
-}
+// Raises the release threshold of the library's memory pool to at least `bytes`: the buffers a
+// registration frees stay in the pool for the next one instead of being unmapped at every
+// synchronisation and mapped again (a measurable share of a registration's time). Never lowers
+// it.
+static void keep_pool(int64_t bytes) { lib_pool_keep(bytes > 0 ? (uint64_t)bytes : 0); }
 
 // One registration of host or device images on `st` (the entry point of the batch and serving
 // drivers, which run several of these concurrently on their own streams).

@@ -1236,9 +1236,9 @@ extern "C" nrb_status nrb_kernel_convolution_cubic(float *img, int nvol, const i
     cubic_taps(temp, radius, k.data());
     const long long nv = (long long)dim[0] * dim[1] * dim[2];
     float *dk = nullptr, *tv = nullptr, *td = nullptr;
-    NRB_CUDA(cudaMallocAsync(&dk, k.size() * 4, st));
-    NRB_CUDA(cudaMallocAsync(&tv, nv * 4, st));
-    NRB_CUDA(cudaMallocAsync(&td, nv * 4, st));
+    NRB_CUDA(tmp_alloc(&dk, k.size() * 4, st));
+    NRB_CUDA(tmp_alloc(&tv, nv * 4, st));
+    NRB_CUDA(tmp_alloc(&td, nv * 4, st));
     NRB_CUDA(cudaMemcpyAsync(dk, k.data(), k.size() * 4, cudaMemcpyHostToDevice, st));
     for (int t = 0; t < nvol; ++t) {
         float *v = img + t * nv;
@@ -1353,7 +1353,7 @@ extern "C" nrb_status nrb_approx_bending_energy(nrb_workspace *ws, const nrb_geo
     nrb_objective *o = obj;
     nrb_objective *tmp = nullptr;
     if (!o) {
-        NRB_CUDA(cudaMallocAsync(&tmp, sizeof(nrb_objective), st));
+        NRB_CUDA(tmp_alloc(&tmp, sizeof(nrb_objective), st));
         o = tmp;
     }
     k_be_sum<<<1, NRB_RED_THREADS, 0, st>>>(ws->be_partials, be_grid(g), 3.0 * (double)nvox(g->cpp_dim), o);
@@ -1535,7 +1535,7 @@ extern "C" nrb_status nrb_intensity_rescale(float *img, int64_t nvox_, float new
     if (!img || nvox_ <= 0) return fail(NRB_ERR_INVALID, "nrb_intensity_rescale: bad argument");
     cudaStream_t st = as_stream(stream);
     float *fred = nullptr;
-    NRB_CUDA(cudaMallocAsync(&fred, 2 * NRB_RED_BLOCKS * sizeof(float), st));
+    NRB_CUDA(tmp_alloc(&fred, 2 * NRB_RED_BLOCKS * sizeof(float), st));
     NRB_TRY(rescale_impl(img, nvox_, new_min, new_max, fred, st));
     NRB_CUDA(cudaFreeAsync(fred, st));
     return NRB_OK;
@@ -1548,8 +1548,8 @@ extern "C" nrb_status nrb_get_maximal_length(const float *node_grad, int64_t nno
     const int np = (int)std::max<long long>(1, std::min<long long>((nnode + NRB_RED_THREADS - 1) / NRB_RED_THREADS, NRB_RED_BLOCKS));
     float *pm = nullptr;
     double *dm = nullptr;
-    NRB_CUDA(cudaMallocAsync(&pm, np * sizeof(float), st));
-    NRB_CUDA(cudaMallocAsync(&dm, sizeof(double), st));
+    NRB_CUDA(tmp_alloc(&pm, np * sizeof(float), st));
+    NRB_CUDA(tmp_alloc(&dm, sizeof(double), st));
     k_maxlen<<<np, NRB_RED_THREADS, 0, st>>>(nnode, node_grad, pm);
     NRB_LAUNCHED("k_maxlen");
     k_maxlen_finish<<<1, 32, 0, st>>>(pm, np, obj, dm);
@@ -1638,7 +1638,7 @@ nrb_status smooth_and_downsample(const float *in, const int32_t idim[3], float *
     for (int i = -radius; i <= radius; ++i)
         k[radius + i] = (float)(std::exp(-(double)(i * i) / (2.0 * temp * temp)) / (temp * 2.506628274631));
     float *dk = nullptr;
-    NRB_CUDA(cudaMallocAsync(&dk, k.size() * 4, st));
+    NRB_CUDA(tmp_alloc(&dk, k.size() * 4, st));
     NRB_CUDA(cudaMemcpyAsync(dk, k.data(), k.size() * 4, cudaMemcpyHostToDevice, st));
     const long long nv = nvox(idim);
     float *v0 = tmp, *d0 = tmp + nv, *v1 = tmp + 2 * nv, *d1 = tmp + 3 * nv;

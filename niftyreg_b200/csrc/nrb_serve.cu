@@ -48,9 +48,9 @@ struct Job {
     nrb_f3d_result result{};
 };
 
-// The device's default memory pool is shared with the host application. While servers exist
-// on a device, its release threshold and internal-dependency reuse are set for them; the values
-// found when the first server was created are put back when the last one is destroyed.
+// The library's memory pool on the device (not the application's default pool). While servers
+// exist on a device, its release threshold and internal-dependency reuse are set for them; the
+// values found when the first server was created are put back when the last one is destroyed.
 struct PoolSettings {
     int servers = 0;
     uint64_t threshold = 0;
@@ -60,11 +60,8 @@ std::mutex g_pool_mu;
 std::map<int, PoolSettings> g_pool_saved;
 
 void pool_acquire(int dev, int64_t budget) {
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
-        cudaGetLastError();
-        return;
-    }
+    cudaMemPool_t pool = lib_pool_of(dev);
+    if (!pool) return;
     std::lock_guard<std::mutex> lock(g_pool_mu);
     PoolSettings& ps = g_pool_saved[dev];
     if (ps.servers++ == 0) {
@@ -85,11 +82,8 @@ void pool_acquire(int dev, int64_t budget) {
 }
 
 void pool_release(int dev) {
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
-        cudaGetLastError();
-        return;
-    }
+    cudaMemPool_t pool = lib_pool_of(dev);
+    if (!pool) return;
     std::lock_guard<std::mutex> lock(g_pool_mu);
     auto it = g_pool_saved.find(dev);
     if (it == g_pool_saved.end() || --it->second.servers > 0) return;
