@@ -132,3 +132,28 @@ def test_server_rejects_oversized(pairs):
     with nrb.Server(slots=1, budget_bytes=nrb.footprint(p.dim, p.pixdim, prm) - 1) as srv:
         with pytest.raises(nrb.NrbError):
             srv.submit(p.reference, p.floating, p.pixdim, prm)
+
+
+def test_default_memory_pool_left_alone(pairs):
+    """Registrations, batches and servers allocate from the library's own memory pool: the
+    application's default pool keeps its release threshold and its reuse setting."""
+    import ctypes
+    nrb.lib()
+    path = next(line.split()[-1] for line in open("/proc/self/maps") if "libcudart" in line)
+    rt = ctypes.CDLL(path)
+
+    def settings():
+        pool, thr, reuse = ctypes.c_void_p(), ctypes.c_uint64(), ctypes.c_int()
+        assert rt.cudaDeviceGetDefaultMemPool(ctypes.byref(pool), 0) == 0
+        assert rt.cudaMemPoolGetAttribute(pool, 4, ctypes.byref(thr)) == 0  # release threshold
+        assert rt.cudaMemPoolGetAttribute(pool, 3, ctypes.byref(reuse)) == 0  # internal dependencies
+        return thr.value, reuse.value
+
+    before = settings()
+    p = pairs[0]
+    nrb.register_host(p.reference, p.floating, p.pixdim, _params())
+    nrb.register_batch([(q.reference, q.floating, q.pixdim) for q in pairs], _params(), concurrency=2)
+    with nrb.Server(slots=2) as srv:
+        srv.wait(srv.submit(p.reference, p.floating, p.pixdim, _params()))
+        assert settings() == before
+    assert settings() == before
