@@ -129,7 +129,8 @@ nrb_status nrb_nmi_value(nrb_nmi *nmi, const nrb_geometry *g, const float *ref,
                          double *nmi_host, void *stream);
 
 /* Adds weight * dNMI/d(warped) * spatial gradient to vgrad, using the log table of the last
- * nrb_nmi_value call. Replaces reg_getVoxelBasedNmiGradient3d (reg-lib/cpu/_reg_nmi.cpp:501-593),
+ * nrb_nmi_value call (the 4x4 Parzen window in FP32 on an FP32 copy of the table when it fits in
+ * 96 KB of shared memory, in FP64 otherwise; the normalisation constant in FP64). Replaces reg_getVoxelBasedNmiGradient3d (reg-lib/cpu/_reg_nmi.cpp:501-593),
  * which reg_nmi::GetVoxelBasedSimilarityMeasureGradientFw (:623-638) runs after recomputing the
  * histogram. */
 nrb_status nrb_nmi_voxel_gradient(nrb_nmi *nmi, const nrb_geometry *g, const float *ref,

@@ -1231,22 +1231,41 @@ __global__ void k_histogram(long long nv, int rb, int fb, const float *__restric
     }
 }
 
+// kF32: the Parzen window in FP32 on an FP32 copy of the log table in shared memory, as the fused
+// gradient runs it (the normalisation constant formed in FP64); otherwise the FP64 window on the
+// global table (tables too large for shared memory).
+template <bool kF32>
 __global__ void k_nmi_voxel_gradient(long long nv, int rb, int fb, const float *__restrict__ ref,
                                      const float *__restrict__ war, const float *__restrict__ wgrad,
                                      const int32_t *__restrict__ mask, const double *__restrict__ logt,
                                      const nrb_objective *__restrict__ last, double weight,
                                      float *__restrict__ vgrad) {
+    extern __shared__ float logf_sm[];
     const double nmi = last->nmi;
     const double scale = weight / (last->entropy[2] * last->entropy[3]);
+    const float nmi_f = (float)nmi, scale_f = (float)scale;
+    if (kF32) {
+        const int total = rb * fb + rb + fb;
+        for (int i = threadIdx.x; i < total; i += blockDim.x) logf_sm[i] = (float)logt[i];
+        __syncthreads();
+    }
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv;
          i += (long long)gridDim.x * blockDim.x) {
         if (mask != nullptr && mask[i] <= -1) continue;
         const float r = ref[i], w = war[i];
         if (!(r == r && w == w)) continue;
-        const double s = nmi_window(r, w, logt, rb, fb, nmi);
-        for (int d = 0; d < 3; ++d) {
-            const float g = wgrad[d * nv + i];
-            if (g == g) vgrad[d * nv + i] += (float)(scale * ((double)g * s));
+        if (kF32) {
+            const float s = nmi_window_f(r, w, logf_sm, rb, fb, nmi_f);
+            for (int d = 0; d < 3; ++d) {
+                const float g = wgrad[d * nv + i];
+                if (g == g) vgrad[d * nv + i] += scale_f * (g * s);
+            }
+        } else {
+            const double s = nmi_window(r, w, logt, rb, fb, nmi);
+            for (int d = 0; d < 3; ++d) {
+                const float g = wgrad[d * nv + i];
+                if (g == g) vgrad[d * nv + i] += (float)(scale * ((double)g * s));
+            }
         }
     }
 }
@@ -2066,8 +2085,18 @@ extern "C" nrb_status nrb_nmi_voxel_gradient(nrb_nmi *nmi, const nrb_geometry *g
     const long long nv = nvox(g->ref_dim);
     const int threads = 256;
     const int grid = (int)std::min<long long>((nv + threads - 1) / threads, 16LL * sm_count());
-    k_nmi_voxel_gradient<<<grid, threads, 0, as_stream(stream)>>>(nv, nmi->rb, nmi->fb, ref, warped, warped_grad,
-                                                                  mask, nmi->logt, nmi->last, weight, vgrad);
+    // the FP32 window when the log table fits in shared memory (64 bins: 19 KB, 128 bins: 70 KB)
+    const size_t log_bytes = (size_t)nmi->total * sizeof(float);
+    if (log_bytes <= 96 * 1024) {
+        NRB_CUDA(cudaFuncSetAttribute(k_nmi_voxel_gradient<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)log_bytes));
+        k_nmi_voxel_gradient<true><<<grid, threads, log_bytes, as_stream(stream)>>>(
+            nv, nmi->rb, nmi->fb, ref, warped, warped_grad, mask, nmi->logt, nmi->last, weight, vgrad);
+    } else {
+        k_nmi_voxel_gradient<false><<<grid, threads, 0, as_stream(stream)>>>(
+            nv, nmi->rb, nmi->fb, ref, warped, warped_grad, mask, nmi->logt, nmi->last, weight, vgrad);
+    }
+    NRB_CUDA(cudaGetLastError());
     NRB_LAUNCHED("k_nmi_voxel_gradient");
     return NRB_OK;
 }
