@@ -1896,10 +1896,11 @@ private:
                 NRB_CUDA(cudaMemsetAsync(vg_bw_.p, 0, 3 * nf * sizeof(float), st_));
                 NRB_TRY(nrb_get_image_gradient(&gfw_, flo_.p, def_fw_.p, nullptr, pad_, wg_fw_.p, st_));
                 NRB_TRY(nrb_get_image_gradient(&gbw_, ref_.p, def_bw_.p, nullptr, pad_, wg_bw_.p, st_));
-                NRB_TRY(nrb_nmi_voxel_gradient(nmi_fw_.h, &gfw_, ref_.p, war_fw_.p, wg_fw_.p, nullptr, 1.0, vg_fw_.p,
-                                               st_));
-                NRB_TRY(nrb_nmi_voxel_gradient(nmi_bw_.h, &gbw_, flo_.p, war_bw_.p, wg_bw_.p, nullptr, 1.0, vg_bw_.p,
-                                               st_));
+                // the FP64 window: the trajectory follows reg_f3d2's
+                NRB_TRY(nmi_voxel_gradient(nmi_fw_.h, &gfw_, ref_.p, war_fw_.p, wg_fw_.p, nullptr, 1.0, vg_fw_.p, st_,
+                                           true));
+                NRB_TRY(nmi_voxel_gradient(nmi_bw_.h, &gbw_, flo_.p, war_bw_.p, wg_bw_.p, nullptr, 1.0, vg_bw_.p, st_,
+                                           true));
             }
             // forward gradient along the backward transformation on the reference grid, and back
             NRB_TRY(Fields(std::max(nr, nf)));

@@ -598,6 +598,11 @@ nrb_status launch_batch_node_stage(const std::vector<BatchPair>& hp, const Batch
                                    nrb_status (*gradient)(const BatchPair *, const OptState *, cudaStream_t, void *),
                                    void *gradient_arg);
 // batched registrations (csrc/nrb_f3d.cu): n pairs advanced together level by level on `st`
+// the NMI voxel gradient (nrb_nmi_voxel_gradient) with the window's precision chosen: fp64 keeps
+// the FP64 window whatever the table size
+nrb_status nmi_voxel_gradient(nrb_nmi *nmi, const nrb_geometry *g, const float *ref, const float *warped,
+                              const float *warped_grad, const int32_t *mask, double weight, float *vgrad,
+                              cudaStream_t st, bool fp64);
 nrb_status register_batch_fused(const nrb_pair *pairs, int n, const nrb_f3d_params *p, nrb_f3d_result *results,
                                 cudaStream_t st, int grad_percent);
 // side stream of `ws` starts after the work queued so far on st / st waits for the side stream

@@ -2076,27 +2076,37 @@ extern "C" nrb_status nrb_nmi_value(nrb_nmi *nmi, const nrb_geometry *g, const f
     return NRB_OK;
 }
 
+namespace nrb {
+// fp64: the FP64 window whatever the table size (the F3D2 driver keeps it, so that its
+// trajectory follows reg_f3d2's); otherwise the FP32 window when the table fits
+nrb_status nmi_voxel_gradient(nrb_nmi *nmi, const nrb_geometry *g, const float *ref, const float *warped,
+                              const float *warped_grad, const int32_t *mask, double weight, float *vgrad,
+                              cudaStream_t st, bool fp64) {
+    const long long nv = nvox(g->ref_dim);
+    const int threads = 256;
+    const int grid = (int)std::min<long long>((nv + threads - 1) / threads, 16LL * sm_count());
+    // the FP32 window when the log table fits in shared memory (64 bins: 19 KB, 128 bins: 70 KB)
+    const size_t log_bytes = (size_t)nmi->total * sizeof(float);
+    if (!fp64 && log_bytes <= 96 * 1024) {
+        NRB_CUDA(cudaFuncSetAttribute(k_nmi_voxel_gradient<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)log_bytes));
+        k_nmi_voxel_gradient<true><<<grid, threads, log_bytes, st>>>(nv, nmi->rb, nmi->fb, ref, warped, warped_grad,
+                                                                     mask, nmi->logt, nmi->last, weight, vgrad);
+    } else {
+        k_nmi_voxel_gradient<false><<<grid, threads, 0, st>>>(nv, nmi->rb, nmi->fb, ref, warped, warped_grad, mask,
+                                                              nmi->logt, nmi->last, weight, vgrad);
+    }
+    NRB_CUDA(cudaGetLastError());
+    NRB_LAUNCHED("k_nmi_voxel_gradient");
+    return NRB_OK;
+}
+}  // namespace nrb
+
 extern "C" nrb_status nrb_nmi_voxel_gradient(nrb_nmi *nmi, const nrb_geometry *g, const float *ref,
                                              const float *warped, const float *warped_grad,
                                              const int32_t *mask, double weight, float *vgrad,
                                              void *stream) {
     if (!nmi || !g || !ref || !warped || !warped_grad || !vgrad)
         return fail(NRB_ERR_INVALID, "nrb_nmi_voxel_gradient: null pointer");
-    const long long nv = nvox(g->ref_dim);
-    const int threads = 256;
-    const int grid = (int)std::min<long long>((nv + threads - 1) / threads, 16LL * sm_count());
-    // the FP32 window when the log table fits in shared memory (64 bins: 19 KB, 128 bins: 70 KB)
-    const size_t log_bytes = (size_t)nmi->total * sizeof(float);
-    if (log_bytes <= 96 * 1024) {
-        NRB_CUDA(cudaFuncSetAttribute(k_nmi_voxel_gradient<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)log_bytes));
-        k_nmi_voxel_gradient<true><<<grid, threads, log_bytes, as_stream(stream)>>>(
-            nv, nmi->rb, nmi->fb, ref, warped, warped_grad, mask, nmi->logt, nmi->last, weight, vgrad);
-    } else {
-        k_nmi_voxel_gradient<false><<<grid, threads, 0, as_stream(stream)>>>(
-            nv, nmi->rb, nmi->fb, ref, warped, warped_grad, mask, nmi->logt, nmi->last, weight, vgrad);
-    }
-    NRB_CUDA(cudaGetLastError());
-    NRB_LAUNCHED("k_nmi_voxel_gradient");
-    return NRB_OK;
+    return nmi_voxel_gradient(nmi, g, ref, warped, warped_grad, mask, weight, vgrad, as_stream(stream), false);
 }
