@@ -18,6 +18,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -228,7 +229,12 @@ extern "C" nrb_status nrb_server_create_grouped(int slots, int max_group, int64_
     s->max_group = max_group;
     s->budget = hbm_budget_bytes > 0 ? hbm_budget_bytes : (int64_t)(0.8 * (double)free_b);
     pool_acquire(dev, s->budget);
-    for (int i = 0; i < slots; ++i) s->workers.emplace_back([s] { s->worker(); });
+    try {
+        for (int i = 0; i < slots; ++i) s->workers.emplace_back([s] { s->worker(); });
+    } catch (const std::system_error&) {
+        nrb_server_destroy(s);  // stops and joins the workers already started
+        return fail(NRB_ERR_INVALID, "nrb_server_create: could not start " + std::to_string(slots) + " worker threads");
+    }
     *out = s;
     return NRB_OK;
 }
@@ -417,13 +423,16 @@ extern "C" nrb_status nrb_f3d_register_batch(const nrb_pair *pairs, int n, const
             }
         }
     };
-    if (workers == 1) {
-        work();
-    } else {
-        std::thread other(work);
-        work();
-        other.join();
+    std::thread other;
+    if (workers == 2) {
+        try {
+            other = std::thread(work);
+        } catch (const std::system_error&) {
+            // no second thread: this one takes every group (the halves of the budget still fit)
+        }
     }
+    work();
+    if (other.joinable()) other.join();
     if (first_error != NRB_OK) return fail(first_error, first_message);
     return NRB_OK;
 }
