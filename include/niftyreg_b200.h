@@ -72,6 +72,11 @@ const char *nrb_last_error(void);
 nrb_status nrb_set_device(int device);
 /* 1 when the library was built for sm_100a and a B200-class device is present. */
 int nrb_device_ok(void);
+/* Returns the current device's unused memory in the library's own memory pool to the driver,
+ * keeping at most keep_bytes mapped (the pool otherwise keeps what registrations and batches
+ * freed, up to the largest working set it has held, for the next ones). Work already queued
+ * keeps its memory. No counterpart in the reference. */
+nrb_status nrb_memory_trim(size_t keep_bytes);
 
 /* ---- deformation and resampling (Compute, reg-lib/Compute.h:6-49) ------------------------ */
 

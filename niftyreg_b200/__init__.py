@@ -711,6 +711,11 @@ def kernel_launch_count() -> int:
     return int(lib().nrb_kernel_launch_count())
 
 
+def memory_trim(keep_bytes: int = 0):
+    """Returns the library pool's unused device memory to the driver, keeping keep_bytes."""
+    check(lib().nrb_memory_trim(ctypes.c_size_t(int(keep_bytes))))
+
+
 def timing_enable(on: bool = True):
     """Brackets every launch of the timed kernels with CUDA events (clears counters)."""
     lib().nrb_timing_enable.restype = None

@@ -217,6 +217,13 @@ extern "C" nrb_status nrb_set_device(int device) {
     return NRB_OK;
 }
 
+extern "C" nrb_status nrb_memory_trim(size_t keep_bytes) {
+    cudaMemPool_t pool = lib_pool();
+    if (!pool) return NRB_OK;  // no pool of the library on this device: nothing held
+    NRB_CUDA(cudaMemPoolTrimTo(pool, keep_bytes));
+    return NRB_OK;
+}
+
 extern "C" int nrb_device_ok(void) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {

@@ -157,3 +157,17 @@ def test_default_memory_pool_left_alone(pairs):
         srv.wait(srv.submit(p.reference, p.floating, p.pixdim, _params()))
         assert settings() == before
     assert settings() == before
+
+
+def test_memory_trim_returns_pool_memory(pairs, plain):
+    """After registrations the library's pool keeps what they freed; nrb_memory_trim gives it
+    back to the driver, and the next registration maps what it needs again, same result."""
+    import torch
+    p = pairs[1]
+    nrb.register_host(p.reference, p.floating, p.pixdim, _params())
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    nrb.memory_trim(0)
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after > free_before
+    _same(nrb.register_host(p.reference, p.floating, p.pixdim, _params()), plain[1])
