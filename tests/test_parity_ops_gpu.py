@@ -140,7 +140,16 @@ def test_nmi_value_and_tables(O, case):
 
 
 def test_nmi_voxel_gradient(O, case):
-    c = case
+    _check_nmi_voxel_gradient(O, case)
+
+
+def test_nmi_voxel_gradient_large_table(O):
+    """180 internal bins: the FP32 copy of the log table (131 KB) does not fit in shared memory,
+    so the FP64 window on the global table runs; the same bar."""
+    _check_nmi_voxel_gradient(O, make_case(seed=6, bins=180))
+
+
+def _check_nmi_voxel_gradient(O, c):
     g = c.geometry()
     dfield, warped = oracle_pipeline(O, c)
     wgrad = O.image_gradient(c.flo, c.fdim, c.flo_ijk, dfield, c.rdim)
