@@ -98,6 +98,7 @@ B200F3dContent::B200F3dContent(NiftiImage& referenceIn, NiftiImage& floatingIn, 
     warpedGradDev.Allocate(3 * nvox * sizeof(float));
     voxelGradDev.Allocate(3 * nvox * sizeof(float));
     cppDev.Allocate(3 * nodeNumber * sizeof(float));
+    snapDev.Allocate(3 * nodeNumber * sizeof(float));
     transGradDev.Allocate(3 * nodeNumber * sizeof(float));
     for (DeviceArray *a : { &defDev, &warpedDev, &warpedGradDev, &voxelGradDev, &transGradDev })
         CheckCuda(cudaMemsetAsync(a->ptr, 0, a->bytes, stream), "cudaMemsetAsync");
@@ -115,7 +116,7 @@ B200F3dContent::~B200F3dContent() {
         cudaStreamSynchronize(stream);
     }
     for (DeviceArray *a : { &refDev, &floDev, &maskDev, &defDev, &warpedDev, &warpedGradDev, &voxelGradDev, &cppDev,
-                            &transGradDev })
+                            &snapDev, &transGradDev })
         a->Free();
     nrb_workspace_destroy(ws);
     if (stream) cudaStreamDestroy(stream);
@@ -138,8 +139,55 @@ void B200F3dContent::UploadImages() {
     CheckCuda(cudaStreamSynchronize(stream), "image upload");
 }
 
-NiftiImage& B200F3dContent::GetDeformationField() { Download(deformationField, defDev); return deformationField; }
-NiftiImage& B200F3dContent::GetWarped() { Download(warped, warpedDev); return warped; }
+void B200F3dContent::MarkDeformationPending() {
+    // a new request supersedes an open one (reg_f3d reads the warp of a request before it asks
+    // for the next field)
+    pendingDef = true;
+    pendingWarp = false;
+    fromSnapshot = false;
+}
+
+bool B200F3dContent::MarkWarpPending(float padding) {
+    if (!pendingDef) return false;
+    pendingWarp = true;
+    pendingPad = padding;
+    return true;
+}
+
+void B200F3dContent::BeforeControlPointsChange() {
+    if (!pendingDef || fromSnapshot) return;
+    CheckCuda(cudaMemcpyAsync(snapDev.ptr, cppDev.ptr, cppDev.bytes, cudaMemcpyDeviceToDevice, stream),
+              "control-point snapshot");
+    fromSnapshot = true;
+}
+
+void B200F3dContent::MaterialiseDeformation() {
+    if (!pendingDef) return;
+    Check(nrb_get_deformation_field(&geom, PendingControlPoints(), maskDev.i(), defDev.f(), stream),
+          "nrb_get_deformation_field");
+    pendingDef = false;
+    fromSnapshot = false;
+}
+
+void B200F3dContent::MaterialiseWarp() {
+    // a recorded warp is of the recorded field, which may already have been computed
+    MaterialiseDeformation();
+    if (!pendingWarp) return;
+    Check(nrb_resample_image(&geom, floDev.f(), defDev.f(), maskDev.i(), pendingPad, warpedDev.f(), stream),
+          "nrb_resample_image");
+    pendingWarp = false;
+}
+
+NiftiImage& B200F3dContent::GetDeformationField() {
+    MaterialiseDeformation();
+    Download(deformationField, defDev);
+    return deformationField;
+}
+NiftiImage& B200F3dContent::GetWarped() {
+    MaterialiseWarp();
+    Download(warped, warpedDev);
+    return warped;
+}
 NiftiImage& B200F3dContent::GetWarpedGradient() { Download(warpedGradient, warpedGradDev); return warpedGradient; }
 NiftiImage& B200F3dContent::GetVoxelBasedMeasureGradient() {
     Download(voxelBasedMeasureGradient, voxelGradDev);
@@ -150,11 +198,21 @@ NiftiImage& B200F3dContent::GetTransformationGradient() {
     Download(transformationGradient, transGradDev);
     return transformationGradient;
 }
-void B200F3dContent::UpdateDeformationField() { Upload(defDev, deformationField); }
-void B200F3dContent::UpdateWarped() { Upload(warpedDev, warped); }
+void B200F3dContent::UpdateDeformationField() {
+    MaterialiseWarp();  // a recorded warp is of the recorded field
+    Upload(defDev, deformationField);
+}
+void B200F3dContent::UpdateWarped() {
+    MaterialiseDeformation();
+    pendingWarp = false;
+    Upload(warpedDev, warped);
+}
 void B200F3dContent::UpdateWarpedGradient() { Upload(warpedGradDev, warpedGradient); }
 void B200F3dContent::UpdateVoxelBasedMeasureGradient() { Upload(voxelGradDev, voxelBasedMeasureGradient); }
-void B200F3dContent::UpdateControlPointGrid() { Upload(cppDev, controlPointGrid); }
+void B200F3dContent::UpdateControlPointGrid() {
+    BeforeControlPointsChange();
+    Upload(cppDev, controlPointGrid);
+}
 void B200F3dContent::UpdateTransformationGradient() { Upload(transGradDev, transformationGradient); }
 void B200F3dContent::ZeroTransformationGradient() {
     CheckCuda(cudaMemsetAsync(transGradDev.ptr, 0, transGradDev.bytes, stream), "cudaMemsetAsync");
@@ -169,14 +227,13 @@ void B200F3dContent::ZeroVoxelBasedMeasureGradient() {
 void B200Compute::GetDeformationField(bool composition, bool bspline) {
     if (composition || !bspline)
         NotOnB200("A composed or non-B-spline deformation field");
-    B200F3dContent& c = Con();
-    Check(nrb_get_deformation_field(&c.Geometry(), c.GetControlPointGridDevice(), c.MaskDevice(),
-                                    c.DeformationFieldDevice(), c.Stream()),
-          "nrb_get_deformation_field");
+    Con().MarkDeformationPending();
 }
 
 void B200Compute::ResampleImage(int interpolation, float paddingValue) {
     B200F3dContent& c = Con();
+    if (interpolation == 1 && c.MarkWarpPending(paddingValue)) return;
+    c.MaterialiseDeformation();
     if (interpolation == 1)
         Check(nrb_resample_image(&c.Geometry(), c.FloatingDevice(), c.DeformationFieldDevice(), c.MaskDevice(),
                                  paddingValue, c.WarpedDevice(), c.Stream()),
@@ -193,6 +250,7 @@ void B200Compute::GetImageGradient(int interpolation, float paddingValue, int ac
     if (activeTimePoint != 0)
         NotOnB200("A multi-channel image gradient");
     B200F3dContent& c = Con();
+    c.MaterialiseDeformation();
     Check(nrb_get_image_gradient(&c.Geometry(), c.FloatingDevice(), c.DeformationFieldDevice(), c.MaskDevice(),
                                  paddingValue, c.WarpedGradientDevice(), c.Stream()),
           "nrb_get_image_gradient");
@@ -249,6 +307,7 @@ void B200Compute::UpdateControlPointPosition(float *currentDof, const float *bes
     if (!(optimiseX && optimiseY && optimiseZ))
         NotOnB200("Optimising a subset of the axes");
     B200F3dContent& c = Con();
+    c.BeforeControlPointsChange();
     Check(nrb_update_control_point_position(currentDof, bestDof, gradient, scale, 3 * int64_t(c.NodeNumber()),
                                             c.Stream()),
           "nrb_update_control_point_position");
@@ -294,6 +353,18 @@ void reg_nmi_b200::Bind(B200F3dContent& con) {
 double reg_nmi_b200::GetSimilarityMeasureValueFw() {
     if (this->timePointWeights[0] <= 0) return 0;
     B200F3dContent& c = *bound;
+    if (c.WarpPending() && c.FusedObjectiveOk()) {
+        // field, warp and histogram in one pass; the same histogram, so the same NMI and tables
+        // as the three steps would give
+        nrb_objective o;
+        const nrb_status s = nrb_f3d_objective(c.Workspace(), nmi, &c.Geometry(), c.ReferenceDevice(),
+                                               c.FloatingDevice(), c.MaskDevice(), c.PendingControlPoints(),
+                                               c.PendingPadding(), 1.0, 0.0, nullptr, &o, c.Stream());
+        if (s == NRB_OK) return this->timePointWeights[0] * o.nmi;
+        if (s != NRB_ERR_UNSUPPORTED) Check(s, "nrb_f3d_objective");
+        c.DisableFusedObjective();  // a grid not aligned with the reference: the three steps
+    }
+    c.MaterialiseWarp();
     double value = 0;
     Check(nrb_nmi_value(nmi, &c.Geometry(), c.ReferenceDevice(), c.WarpedDevice(), c.MaskDevice(), nullptr, &value,
                         c.Stream()),
@@ -306,6 +377,7 @@ void reg_nmi_b200::GetVoxelBasedSimilarityMeasureGradientFw(int currentTimePoint
         NotOnB200("A multi-channel NMI gradient");
     if (this->timePointWeights[0] <= 0) return;
     B200F3dContent& c = *bound;
+    c.MaterialiseWarp();
     // the histogram at the current warp first, as reg_nmi::GetVoxelBasedSimilarityMeasureGradientFw
     Check(nrb_nmi_value(nmi, &c.Geometry(), c.ReferenceDevice(), c.WarpedDevice(), c.MaskDevice(), nullptr, nullptr,
                         c.Stream()),
@@ -386,6 +458,7 @@ void B200Optimiser::StoreCurrentDof() {
 }
 
 void B200Optimiser::RestoreBestDof() {
+    con.BeforeControlPointsChange();
     CheckCuda(cudaMemcpyAsync(this->currentDof, this->bestDof, this->dofNumber * sizeof(float),
                               cudaMemcpyDeviceToDevice, con.Stream()),
               "RestoreBestDof");

@@ -90,6 +90,23 @@ public:
     // the reference and floating intensities after the measure rescaled the host copies
     void UploadImages();
 
+    // Lazy deformation field and warped image. B200Compute::GetDeformationField and a linear
+    // ResampleImage record the request; the NMI value of a recorded warp is then one fused pass
+    // over the voxels (nrb_f3d_objective) that writes neither array, and the first reader of
+    // either array computes it from the control points of the request. Control points that
+    // change while a request is open are first saved, so a later reader still sees the field of
+    // the request's control points.
+    void MarkDeformationPending();
+    bool MarkWarpPending(float padding);  // false when no field is pending (warp now instead)
+    bool WarpPending() const { return pendingDef && pendingWarp; }
+    const float* PendingControlPoints() const { return fromSnapshot ? snapDev.f() : cppDev.f(); }
+    float PendingPadding() const { return pendingPad; }
+    void BeforeControlPointsChange();
+    void MaterialiseDeformation();
+    void MaterialiseWarp();
+    bool FusedObjectiveOk() const { return fusedOk; }
+    void DisableFusedObjective() { fusedOk = false; }
+
     const nrb_geometry& Geometry() const { return geom; }
     nrb_workspace* Workspace() const { return ws; }
     cudaStream_t Stream() const { return stream; }
@@ -114,6 +131,10 @@ private:
     size_t nodeNumber = 0;
     nrb_platform::DeviceArray refDev, floDev, maskDev, defDev, warpedDev, warpedGradDev, voxelGradDev,
         cppDev, transGradDev;
+    nrb_platform::DeviceArray snapDev;  // the control points of an open request, once they change
+    bool pendingDef = false, pendingWarp = false, fromSnapshot = false;
+    float pendingPad = 0.f;
+    bool fusedOk = true;  // the fused objective applies (a grid aligned with the reference)
 };
 
 // Compute on the device (reg-lib/Compute.h:6-49; CUDA counterpart reg-lib/cuda/CudaCompute.h).
