@@ -62,19 +62,42 @@ __device__ double block_sum_d(double v, double *red) {
 // positions, summed squares (cross terms doubled) accumulated in double. The stencil sums use
 // the reference's order without contraction: each node's terms are bit-identical to the CPU's.
 // grad/step (optional): the positions are the line search's trial values cpp - cur_len * grad
-__global__ void __launch_bounds__(NRB_RED_THREADS)
+//
+// Three threads per node, one per component (threads k * NRB_RED_THREADS + j of a block), so 27
+// loads per thread are in flight and three times as many warps hide their latency. Node lane j
+// (component 0) adds the other components' terms in the reference's order and accumulates its
+// nodes in the grid-stride order of a one-thread-per-node loop; the block sum is the same tree
+// as block_sum_d over the NRB_RED_THREADS node lanes, so every partial is unchanged bit for bit.
+__global__ void __launch_bounds__(3 * NRB_RED_THREADS, 2)
 k_be_value(int cx, int cy, int cz, const float *__restrict__ cpp, BeBasis B,
            double *__restrict__ partials, const float *__restrict__ grad, const OptState *__restrict__ step) {
     __shared__ double red[NRB_RED_THREADS];
+    __shared__ BeTerms other[2][NRB_RED_THREADS];  // components 1 and 2 of the lane's node
     const float scale = grad ? -step->cur_len : 0.f;
+    const int j = threadIdx.x % NRB_RED_THREADS, k = threadIdx.x / NRB_RED_THREADS;
     const int ix = cx - 2, iy = cy - 2, iz = cz - 2;
     const long long ni = (ix > 0 && iy > 0 && iz > 0) ? (long long)ix * iy * iz : 0;
     double acc = 0;
-    for (long long n = blockIdx.x * (long long)NRB_RED_THREADS + threadIdx.x; n < ni;
-         n += (long long)gridDim.x * NRB_RED_THREADS)
-        acc += be_node_value(cx, cy, cz, ix, iy, cpp, B, grad, scale, n);
-    const double tot = block_sum_d(acc, red);
-    if (threadIdx.x == 0) partials[blockIdx.x] = tot;
+    for (long long base = blockIdx.x * (long long)NRB_RED_THREADS; base < ni; base += (long long)gridDim.x * NRB_RED_THREADS) {
+        const long long n = base + j;
+        BeTerms t{ 0.f, 0.f, 0.f, 0.f };
+        if (n < ni) t = be_node_component<true>(cx, cy, cz, ix, iy, cpp, B, grad, scale, n, k);
+        if (k > 0) other[k - 1][j] = t;
+        __syncthreads();
+        if (k == 0 && n < ni) {
+            double s = be_add_component(0.0, t, 0);
+            s = be_add_component(s, other[0][j], 1);
+            acc += be_add_component(s, other[1][j], 2);
+        }
+        __syncthreads();  // `other` is rewritten by the next round
+    }
+    if (k == 0) red[j] = acc;
+    __syncthreads();
+    for (int s = NRB_RED_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
 }
 
 __global__ void k_be_sum(const double *__restrict__ partials, int n, double norm,
@@ -345,11 +368,14 @@ __global__ void k_nodes(int cx, int cy, int cz, int nsx, int nsy, int nsz,
 // each pair's elements computed exactly as the plain kernels compute them
 // ---------------------------------------------------------------------------------------------
 // bending-energy value partials of every pair in INIT or LINE: work unit = one block of the plain
-// k_be_value (same node range, same shared-memory tree), persistent blocks of NRB_RED_THREADS
-__global__ void __launch_bounds__(NRB_RED_THREADS)
+// k_be_value (same node range, three threads per node, same shared-memory tree), persistent
+// blocks of 3 * NRB_RED_THREADS
+__global__ void __launch_bounds__(3 * NRB_RED_THREADS, 2)
 k_b_be_value(const BatchPair *__restrict__ pairs, const OptState *__restrict__ states, int npairs, BeBasis B) {
     __shared__ BatchList L;
     __shared__ double red[NRB_RED_THREADS];
+    __shared__ BeTerms other[2][NRB_RED_THREADS];
+    const int j = threadIdx.x % NRB_RED_THREADS, kc = threadIdx.x / NRB_RED_THREADS;
     batch_list_build(states, npairs, (1u << PH_INIT) | (1u << PH_LINE),
                      [&](int q, int& u, int& w) {
                          const BatchPair& b = pairs[q];
@@ -368,10 +394,27 @@ k_b_be_value(const BatchPair *__restrict__ pairs, const OptState *__restrict__ s
         const int ix = cx - 2, iy = cy - 2, iz = cz - 2;
         const long long ni = (ix > 0 && iy > 0 && iz > 0) ? (long long)ix * iy * iz : 0;
         double acc = 0;
-        for (long long n = (long long)v * NRB_RED_THREADS + threadIdx.x; n < ni; n += (long long)P.n_be * NRB_RED_THREADS)
-            acc += be_node_value(cx, cy, cz, ix, iy, P.best, B, grad, scale, n);
-        const double tot = block_sum_d(acc, red);
-        if (threadIdx.x == 0) P.be_partials[v] = tot;
+        // the unit's bounds are the same for every thread of the block (one pair per unit)
+        for (long long base = (long long)v * NRB_RED_THREADS; base < ni; base += (long long)P.n_be * NRB_RED_THREADS) {
+            const long long n = base + j;
+            BeTerms t{ 0.f, 0.f, 0.f, 0.f };
+            if (n < ni) t = be_node_component<true>(cx, cy, cz, ix, iy, P.best, B, grad, scale, n, kc);
+            if (kc > 0) other[kc - 1][j] = t;
+            __syncthreads();
+            if (kc == 0 && n < ni) {
+                double s = be_add_component(0.0, t, 0);
+                s = be_add_component(s, other[0][j], 1);
+                acc += be_add_component(s, other[1][j], 2);
+            }
+            __syncthreads();
+        }
+        if (kc == 0) red[j] = acc;
+        __syncthreads();
+        for (int s = NRB_RED_THREADS / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) P.be_partials[v] = red[0];
         __syncthreads();  // red is reused by the next unit
     }
 }
@@ -1112,7 +1155,7 @@ nrb_status launch_be_value(nrb_workspace *ws, const nrb_geometry *g, const float
                            const float *grad, const OptState *step) {
     const int grid = be_grid(g);
     KernelTimer timer(TK_BE_VALUE, 12.0 * (double)nvox(g->cpp_dim), st);
-    k_be_value<<<grid, NRB_RED_THREADS, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2], cpp, be_basis(),
+    k_be_value<<<grid, 3 * NRB_RED_THREADS, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2], cpp, be_basis(),
                                                   ws->be_partials, grad, step);
     NRB_LAUNCHED("k_be_value");
     return NRB_OK;
@@ -1436,9 +1479,9 @@ nrb_status launch_batch_be_value(const std::vector<BatchPair>& hp, const BatchPa
                                  cudaStream_t st) {
     long long units = 0;
     for (const BatchPair& b : hp) units += b.n_be;
-    const int grid = (int)std::max(1LL, std::min(units, 8LL * sm_count()));
+    const int grid = (int)std::max(1LL, std::min(units, 2LL * sm_count()));
     KernelTimer timer(TK_BE_VALUE, 0.0, st);
-    k_b_be_value<<<grid, NRB_RED_THREADS, 0, st>>>(d, states, (int)hp.size(), be_basis());
+    k_b_be_value<<<grid, 3 * NRB_RED_THREADS, 0, st>>>(d, states, (int)hp.size(), be_basis());
     NRB_CUDA(cudaGetLastError());
     NRB_LAUNCHED("k_b_be_value");
     return NRB_OK;

@@ -388,46 +388,57 @@ WalkPlan plan_walk(const nrb_geometry *g, int ty, long long (*slots_for)(size_t 
 struct BeBasis {
     float v[6][27];  // xx, yy, zz, xy, yz, xz
 };
-// the bending-energy value term of interior node n (of ix * iy * iz interior nodes)
-__device__ __forceinline__ double be_node_value(int cx, int cy, int cz, int ix, int iy, const float *__restrict__ cpp,
-                                                const BeBasis& B, const float *__restrict__ grad, float scale,
-                                                long long n) {
+// One component's share of an interior node's bending-energy term: the squares of its three
+// second derivatives and the float sum of its three squared cross derivatives.
+struct BeTerms {
+    float xx, yy, zz, cross;
+};
+// Component k of interior node n (of ix * iy * iz interior nodes): its 6 stencil sums over the 27
+// points in (c, b, a) order without contraction, then the squares. `full_unroll` keeps all 27
+// loads in flight (a thread that evaluates one component); otherwise one c-plane at a time.
+template <bool full_unroll>
+__device__ __forceinline__ BeTerms be_node_component(int cx, int cy, int cz, int ix, int iy,
+                                                     const float *__restrict__ cpp, const BeBasis& B,
+                                                     const float *__restrict__ grad, float scale, long long n, int k) {
     const long long nc = (long long)cx * cy * cz;
     const int x = 1 + (int)(n % ix);
     const int y = 1 + (int)((n / ix) % iy);
     const int z = 1 + (int)(n / ((long long)ix * iy));
     auto sq = [](float v) { return __fmul_rn(v, v); };
-    // one component at a time: its 6 stencil sums over the 27 points in (c, b, a) order, then
-    // its terms in the reference expression's order (the first three squares of component 0
-    // summed in float, every later term added in double), so only 6 sums are live at once
+    float d[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) d[t] = 0.f;
+#pragma unroll(full_unroll ? 3 : 1)
+    for (int c = -1; c < 2; ++c)
+#pragma unroll
+        for (int b = -1; b < 2; ++b)
+#pragma unroll
+            for (int a = -1; a < 2; ++a) {
+                const int i = 9 * (c + 1) + 3 * (b + 1) + (a + 1);
+                const long long idx = ((long long)(z + c) * cy + y + b) * cx + x + a;
+                const float v = trial_cp(cpp, grad, scale, k * nc + idx);
+#pragma unroll
+                for (int t = 0; t < 6; ++t) d[t] = __fadd_rn(d[t], __fmul_rn(B.v[t][i], v));
+            }
+    return BeTerms{ sq(d[0]), sq(d[1]), sq(d[2]), __fadd_rn(__fadd_rn(sq(d[3]), sq(d[4])), sq(d[5])) };
+}
+// Adds component k's terms to the node's sum in the reference expression's order: the first
+// three squares of component 0 summed in float, every later term added in double.
+__device__ __forceinline__ double be_add_component(double s, const BeTerms& t, int k) {
+    if (k == 0) return __dadd_rn((double)__fadd_rn(__fadd_rn(t.xx, t.yy), t.zz), __dmul_rn(2.0, (double)t.cross));
+    s = __dadd_rn(s, (double)t.xx);
+    s = __dadd_rn(s, (double)t.yy);
+    s = __dadd_rn(s, (double)t.zz);
+    return __dadd_rn(s, __dmul_rn(2.0, (double)t.cross));
+}
+// the bending-energy value term of interior node n, one component at a time (only 6 sums live)
+__device__ __forceinline__ double be_node_value(int cx, int cy, int cz, int ix, int iy, const float *__restrict__ cpp,
+                                                const BeBasis& B, const float *__restrict__ grad, float scale,
+                                                long long n) {
     double s = 0.0;
 #pragma unroll 1
-    for (int k = 0; k < 3; ++k) {
-        float d[6];
-#pragma unroll
-        for (int t = 0; t < 6; ++t) d[t] = 0.f;
-#pragma unroll 1
-        for (int c = -1; c < 2; ++c)
-#pragma unroll
-            for (int b = -1; b < 2; ++b)
-#pragma unroll
-                for (int a = -1; a < 2; ++a) {
-                    const int i = 9 * (c + 1) + 3 * (b + 1) + (a + 1);
-                    const long long idx = ((long long)(z + c) * cy + y + b) * cx + x + a;
-                    const float v = trial_cp(cpp, grad, scale, k * nc + idx);
-#pragma unroll
-                    for (int t = 0; t < 6; ++t) d[t] = __fadd_rn(d[t], __fmul_rn(B.v[t][i], v));
-                }
-        const float cross = __fadd_rn(__fadd_rn(sq(d[3]), sq(d[4])), sq(d[5]));
-        if (k == 0) {
-            s = __dadd_rn((double)__fadd_rn(__fadd_rn(sq(d[0]), sq(d[1])), sq(d[2])), __dmul_rn(2.0, (double)cross));
-        } else {
-            s = __dadd_rn(s, (double)sq(d[0]));
-            s = __dadd_rn(s, (double)sq(d[1]));
-            s = __dadd_rn(s, (double)sq(d[2]));
-            s = __dadd_rn(s, __dmul_rn(2.0, (double)cross));
-        }
-    }
+    for (int k = 0; k < 3; ++k)
+        s = be_add_component(s, be_node_component<false>(cx, cy, cz, ix, iy, cpp, B, grad, scale, n, k), k);
     return s;
 }
 
