@@ -118,85 +118,149 @@ __device__ __forceinline__ float identity_pos(const Mat34& M, int k, int x, int 
 }
 
 // reg_spline_approxBendingEnergyGradient3D (reg-lib/cpu/_reg_localTrans_regul.cpp:286-451),
-// first half: the 18 derivative values of every node from zero-padded stencils of the
+// first half: the 6 derivative values of component k of node n from zero-padded stencils of the
 // displacements, cross terms doubled. Layout der[(3 * t + k) * nc + node].
+__device__ __forceinline__ void be_node_derivatives_k(int cx, int cy, int cz, const Mat34& M,
+                                                      const float *__restrict__ cpp, const BeBasis& B,
+                                                      float *__restrict__ der, long long n, int k) {
+    const long long nc = (long long)cx * cy * cz;
+    const int x = (int)(n % cx);
+    const int y = (int)((n / cx) % cy);
+    const int z = (int)(n / ((long long)cx * cy));
+    // row k of the grid matrix picked by selects (a runtime index into the parameter would copy
+    // the matrix to local memory)
+    float m[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) m[q] = k == 0 ? M.m[q] : (k == 1 ? M.m[4 + q] : M.m[8 + q]);
+    float d[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) d[t] = 0.f;
+#pragma unroll
+    for (int c = -1; c < 2; ++c)
+#pragma unroll
+        for (int b = -1; b < 2; ++b)
+#pragma unroll
+            for (int a = -1; a < 2; ++a) {
+                const int i = 9 * (c + 1) + 3 * (b + 1) + (a + 1);
+                const int X = x + a, Y = y + b, Z = z + c;
+                if (X < 0 || Y < 0 || Z < 0 || X >= cx || Y >= cy || Z >= cz) continue;
+                const long long idx = ((long long)Z * cy + Y) * cx + X;
+                const float id = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[0], (float)X), __fmul_rn(m[1], (float)Y)),
+                                                     __fmul_rn(m[2], (float)Z)), m[3]);  // identity_pos
+                const float v = __fsub_rn(__ldg(&cpp[k * nc + idx]), id);
+#pragma unroll
+                for (int t = 0; t < 6; ++t) d[t] = __fadd_rn(d[t], __fmul_rn(B.v[t][i], v));
+            }
+#pragma unroll
+    for (int t = 0; t < 3; ++t) der[(3 * t + k) * nc + n] = d[t];
+#pragma unroll
+    for (int t = 3; t < 6; ++t) der[(3 * t + k) * nc + n] = (float)(2.0 * (double)d[t]);
+}
+
+// all three components of node n at once (the batched stage's element): the same sums, each
+// component's in the same order as be_node_derivatives_k
 __device__ __forceinline__ void be_node_derivatives(int cx, int cy, int cz, const Mat34& M, const float *__restrict__ cpp,
                                                     const BeBasis& B, float *__restrict__ der, long long n) {
     const long long nc = (long long)cx * cy * cz;
-    {
-        const int x = (int)(n % cx);
-        const int y = (int)((n / cx) % cy);
-        const int z = (int)(n / ((long long)cx * cy));
-        float d[3][6];
+    const int x = (int)(n % cx);
+    const int y = (int)((n / cx) % cy);
+    const int z = (int)(n / ((long long)cx * cy));
+    float d[3][6];
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
+    for (int k = 0; k < 3; ++k)
 #pragma unroll
-            for (int t = 0; t < 6; ++t) d[k][t] = 0.f;
-        int i = 0;
-        for (int c = -1; c < 2; ++c)
-            for (int b = -1; b < 2; ++b)
-                for (int a = -1; a < 2; ++a, ++i) {
-                    const int X = x + a, Y = y + b, Z = z + c;
-                    if (X < 0 || Y < 0 || Z < 0 || X >= cx || Y >= cy || Z >= cz) continue;
-                    const long long idx = ((long long)Z * cy + Y) * cx + X;
+        for (int t = 0; t < 6; ++t) d[k][t] = 0.f;
+    int i = 0;
+    for (int c = -1; c < 2; ++c)
+        for (int b = -1; b < 2; ++b)
+            for (int a = -1; a < 2; ++a, ++i) {
+                const int X = x + a, Y = y + b, Z = z + c;
+                if (X < 0 || Y < 0 || Z < 0 || X >= cx || Y >= cy || Z >= cz) continue;
+                const long long idx = ((long long)Z * cy + Y) * cx + X;
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const float v = __fsub_rn(__ldg(&cpp[k * nc + idx]), identity_pos(M, k, X, Y, Z));
+                for (int k = 0; k < 3; ++k) {
+                    const float v = __fsub_rn(__ldg(&cpp[k * nc + idx]), identity_pos(M, k, X, Y, Z));
 #pragma unroll
-                        for (int t = 0; t < 6; ++t) d[k][t] = __fadd_rn(d[k][t], __fmul_rn(B.v[t][i], v));
-                    }
+                    for (int t = 0; t < 6; ++t) d[k][t] = __fadd_rn(d[k][t], __fmul_rn(B.v[t][i], v));
                 }
+            }
 #pragma unroll
-        for (int t = 0; t < 3; ++t)
+    for (int t = 0; t < 3; ++t)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) der[(3 * t + k) * nc + n] = d[k][t];
+        for (int k = 0; k < 3; ++k) der[(3 * t + k) * nc + n] = d[k][t];
 #pragma unroll
-        for (int t = 3; t < 6; ++t)
+    for (int t = 3; t < 6; ++t)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) der[(3 * t + k) * nc + n] = (float)(2.0 * (double)d[k][t]);
-    }
+        for (int k = 0; k < 3; ++k) der[(3 * t + k) * nc + n] = (float)(2.0 * (double)d[k][t]);
 }
 
+// one thread per (node, component): component k = blockIdx.y
 __global__ void k_be_derivatives(int cx, int cy, int cz, Mat34 M, const float *__restrict__ cpp,
                                  BeBasis B, float *__restrict__ der) {
     const long long nc = (long long)cx * cy * cz;
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nc;
          n += (long long)gridDim.x * blockDim.x)
-        be_node_derivatives(cx, cy, cz, M, cpp, B, der, n);
+        be_node_derivatives_k(cx, cy, cz, M, cpp, B, der, n, (int)blockIdx.y);
 }
 
 // second half: the same stencils applied to the derivative values of the 27 neighbours,
-// grad += weight / #nodes * sum.
+// grad += weight / #nodes * sum, for component k of node n: the sum runs over the neighbours
+// in (z, y, x) order and the 6 derivative kinds within each, as for all components at once.
+__device__ __forceinline__ void be_node_accumulate_k(int cx, int cy, int cz, const float *__restrict__ der,
+                                                     const BeBasis& B, float ratio, float *__restrict__ grad,
+                                                     long long n, int k) {
+    const long long nc = (long long)cx * cy * cz;
+    const int x = (int)(n % cx);
+    const int y = (int)((n / cx) % cy);
+    const int z = (int)(n / ((long long)cx * cy));
+    float g = 0.f;
+#pragma unroll
+    for (int c = -1; c < 2; ++c)
+#pragma unroll
+        for (int b = -1; b < 2; ++b)
+#pragma unroll
+            for (int e = -1; e < 2; ++e) {
+                const int a = 9 * (c + 1) + 3 * (b + 1) + (e + 1);
+                const int X = x + e, Y = y + b, Z = z + c;
+                if (X < 0 || Y < 0 || Z < 0 || X >= cx || Y >= cy || Z >= cz) continue;
+                const long long j = ((long long)Z * cy + Y) * cx + X;
+#pragma unroll
+                for (int t = 0; t < 6; ++t) g = __fadd_rn(g, __fmul_rn(__ldg(&der[(3 * t + k) * nc + j]), B.v[t][a]));
+            }
+    grad[k * nc + n] = __fadd_rn(grad[k * nc + n], __fmul_rn(ratio, g));
+}
+
+// all three components of node n at once (the batched stage's element), each in the order of
+// be_node_accumulate_k
 __device__ __forceinline__ void be_node_accumulate(int cx, int cy, int cz, const float *__restrict__ der, const BeBasis& B,
                                                    float ratio, float *__restrict__ grad, long long n) {
     const long long nc = (long long)cx * cy * cz;
-    {
-        const int x = (int)(n % cx);
-        const int y = (int)((n / cx) % cy);
-        const int z = (int)(n / ((long long)cx * cy));
-        float g[3] = { 0.f, 0.f, 0.f };
-        int a = 0;
-        for (int Z = z - 1; Z < z + 2; ++Z)
-            for (int Y = y - 1; Y < y + 2; ++Y)
-                for (int X = x - 1; X < x + 2; ++X, ++a) {
-                    if (X < 0 || Y < 0 || Z < 0 || X >= cx || Y >= cy || Z >= cz) continue;
-                    const long long j = ((long long)Z * cy + Y) * cx + X;
+    const int x = (int)(n % cx);
+    const int y = (int)((n / cx) % cy);
+    const int z = (int)(n / ((long long)cx * cy));
+    float g[3] = { 0.f, 0.f, 0.f };
+    int a = 0;
+    for (int Z = z - 1; Z < z + 2; ++Z)
+        for (int Y = y - 1; Y < y + 2; ++Y)
+            for (int X = x - 1; X < x + 2; ++X, ++a) {
+                if (X < 0 || Y < 0 || Z < 0 || X >= cx || Y >= cy || Z >= cz) continue;
+                const long long j = ((long long)Z * cy + Y) * cx + X;
 #pragma unroll
-                    for (int t = 0; t < 6; ++t)
+                for (int t = 0; t < 6; ++t)
 #pragma unroll
-                        for (int k = 0; k < 3; ++k) g[k] = __fadd_rn(g[k], __fmul_rn(__ldg(&der[(3 * t + k) * nc + j]), B.v[t][a]));
-                }
+                    for (int k = 0; k < 3; ++k) g[k] = __fadd_rn(g[k], __fmul_rn(__ldg(&der[(3 * t + k) * nc + j]), B.v[t][a]));
+            }
 #pragma unroll
-        for (int k = 0; k < 3; ++k) grad[k * nc + n] = __fadd_rn(grad[k * nc + n], __fmul_rn(ratio, g[k]));
-    }
+    for (int k = 0; k < 3; ++k) grad[k * nc + n] = __fadd_rn(grad[k * nc + n], __fmul_rn(ratio, g[k]));
 }
 
+// one thread per (node, component): component k = blockIdx.y
 __global__ void k_be_accumulate(int cx, int cy, int cz, const float *__restrict__ der, BeBasis B,
                                 float ratio, float *__restrict__ grad) {
     const long long nc = (long long)cx * cy * cz;
     for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < nc;
          n += (long long)gridDim.x * blockDim.x)
-        be_node_accumulate(cx, cy, cz, der, B, ratio, grad, n);
+        be_node_accumulate_k(cx, cy, cz, der, B, ratio, grad, n, (int)blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1415,7 +1479,7 @@ namespace nrb {
 nrb_status launch_be_derivatives(nrb_workspace *ws, const nrb_geometry *g, const float *cpp, cudaStream_t st) {
     const long long nc = nvox(g->cpp_dim);
     KernelTimer timer(TK_BE_GRADIENT, (12.0 + 72.0) * (double)nc, st);
-    k_be_derivatives<<<grid_for(nc, 128), 128, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2],
+    k_be_derivatives<<<dim3(grid_for(nc, 128), 3), 128, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2],
                                                         to_mat34(g->cpp_xyz), cpp, be_basis(), ws->be_deriv);
     NRB_LAUNCHED("k_be_derivatives");
     return NRB_OK;
@@ -1428,7 +1492,7 @@ nrb_status launch_be_accumulate(nrb_workspace *ws, const nrb_geometry *g, float 
     const long long nc = nvox(g->cpp_dim);
     KernelTimer timer(TK_BE_GRADIENT, (72.0 + 24.0) * (double)nc, st);
     const float ratio = weight / (float)nc;
-    k_be_accumulate<<<grid_for(nc, 128), 128, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2], ws->be_deriv,
+    k_be_accumulate<<<dim3(grid_for(nc, 128), 3), 128, 0, st>>>(g->cpp_dim[0], g->cpp_dim[1], g->cpp_dim[2], ws->be_deriv,
                                                        be_basis(), ratio, node_grad);
     NRB_LAUNCHED("k_be_accumulate");
     return NRB_OK;
