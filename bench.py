@@ -23,6 +23,8 @@ rank 0 prints one JSON line with the whole-job rate and the slowest rank's devic
 from __future__ import annotations
 
 import argparse
+import contextlib
+import gc
 import json
 import math
 import os
@@ -294,6 +296,19 @@ def peaks():
         return 6650.0, "fallback"
 
 
+@contextlib.contextmanager
+def collector_paused():
+    """Python's cyclic garbage collector off inside a timed region (as timeit does): a full
+    collection in a process holding torch's objects takes tens of milliseconds, and one that
+    falls between a registration's return and its closing event would be counted as GPU time."""
+    gc.collect()
+    gc.disable()
+    try:
+        yield
+    finally:
+        gc.enable()
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
@@ -313,6 +328,14 @@ class ClockSampler:
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+            return
+        # the timed region starts once nvidia-smi has its first sample: its start-up (NVML
+        # initialisation) then lies before the region instead of inside one of its steps
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 5.0 and self.p.poll() is None:
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.p is None:
@@ -511,15 +534,16 @@ def run_b200(args):
     sampler.start()
     launches0 = nrb.kernel_launch_count()
     events, results = [], []
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()  # L2 flush between timed steps, outside the events
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        results.append(step())
-        e1.record(stream)
-        events.append((e0, e1))
-    torch.cuda.synchronize()
+    with collector_paused():
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()  # L2 flush between timed steps, outside the events
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            results.append(step())
+            e1.record(stream)
+            events.append((e0, e1))
+        torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     clocks = sampler.stop()
@@ -540,10 +564,11 @@ def run_b200(args):
     # ---- e2e: host buffers through the C ABI, copies inside the timed region ------------------
     barrier()
     e2e_s = []
-    for _ in range(0 if args.no_e2e else args.steps):
-        t0 = time.perf_counter()
-        cpp_np, res = nrb.register_host(ref_h.numpy().reshape(SHAPE), flo_h.numpy().reshape(SHAPE), pix, params)
-        e2e_s.append(time.perf_counter() - t0)
+    with collector_paused():
+        for _ in range(0 if args.no_e2e else args.steps):
+            t0 = time.perf_counter()
+            cpp_np, res = nrb.register_host(ref_h.numpy().reshape(SHAPE), flo_h.numpy().reshape(SHAPE), pix, params)
+            e2e_s.append(time.perf_counter() - t0)
     e2e_max = max_over_ranks(float(sum(e2e_s)), world, dev)
     e2e_value = replica_rate(world, len(e2e_s), e2e_max) if e2e_s else None
 
@@ -691,9 +716,10 @@ def run_batched(args, emit=True):
         nrb.register_host(p.reference, p.floating, p.pixdim, params)
     sampler = _gpu_clock_sampler()
     sampler.start()
-    t0 = time.perf_counter()
-    plain = [] if args.batch_only else [nrb.register_host(p.reference, p.floating, p.pixdim, params) for p in pairs]
-    t_plain = time.perf_counter() - t0
+    with collector_paused():
+        t0 = time.perf_counter()
+        plain = [] if args.batch_only else [nrb.register_host(p.reference, p.floating, p.pixdim, params) for p in pairs]
+        t_plain = time.perf_counter() - t0
     bparams = nrb.default_params(levels=BATCH_LEVELS, max_iterations=BATCH_MAXIT, bending_energy=BE,
                                  spacing=(SPACING,), ref_bins=BINS, flo_bins=BINS,
                                  batch_gradient_percent=args.grad_percent, verbose=int(args.verbose),
@@ -703,9 +729,10 @@ def run_batched(args, emit=True):
     # warm-up of the batched path as the plain one had: the same batch once, untimed (device
     # memory pools and texture arrays grown to the groups' footprint, as in a running server)
     nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], bparams, args.concurrency)
-    t0 = time.perf_counter()
-    batched = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], bparams, args.concurrency)
-    t_batch = time.perf_counter() - t0
+    with collector_paused():
+        t0 = time.perf_counter()
+        batched = nrb.register_batch([(p.reference, p.floating, p.pixdim) for p in pairs], bparams, args.concurrency)
+        t_batch = time.perf_counter() - t0
     clocks = sampler.stop()
     kt = None
     if args.kernel_timing:
