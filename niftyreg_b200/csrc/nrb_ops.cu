@@ -313,29 +313,48 @@ __device__ __forceinline__ void conv_x_rows(int nx, int ny, int nz, const float 
         }
     }
     for (int i = threadIdx.x; i < 2 * R + 1; i += CONV_X_THREADS) Ks[i] = K[i];
+    // each sample's sum of in-row kernel weights (the same for every row without NaN), summed in
+    // the order of the check-free loop below
+    float *dens = Ks + 2 * R + 1;
+    for (int j = threadIdx.x; j < ns; j += CONV_X_THREADS) {
+        const int sj = samples[j];
+        const int k0 = max(0, sj - R), k1 = min(nx - 1, sj + R);
+        float den = 0.f;
+        for (int k = k0; k <= k1; ++k) den += K[k - sj + R];
+        dens[j] = den;
+    }
     // rows without NaN (the fused gradient never writes one) take the check-free sum: the
     // same operations in the same order as conv_at when every tap counts
     const bool any_nan = __syncthreads_or(nan) != 0;
-    const int per_c = nr * ns;
-    for (int i = threadIdx.x; i < 3 * per_c; i += CONV_X_THREADS) {
-        const int c = i / per_c, rem = i - c * per_c;
-        const int r = rem / ns, j = rem - r * ns;
-        const float *row = rows + (c * CONV_X_ROWS + r) * nx;
-        const int sj = samples[j];
-        float v;
-        if (any_nan) {
-            v = conv_at(sj, nx, R, Ks, [&](int k) { return row[k]; });
-        } else {
-            float num = 0.f, den = 0.f;
-            const int k0 = max(0, sj - R), k1 = min(nx - 1, sj + R);
-            const float *w = Ks - sj + R;
-            for (int k = k0; k <= k1; ++k) {
-                num = fmaf(w[k], row[k], num);
-                den += w[k];
+    if (ns <= 0) return;  // no sample on this axis: nothing to write
+    // outputs (component c, row r < CONV_X_ROWS, sample j) in the order cr = c * CONV_X_ROWS + r,
+    // then j; a thread steps by CONV_X_THREADS outputs with carried counters (no division per
+    // output); rows beyond the block's last (r >= nr) are skipped
+    int j = threadIdx.x % ns, cr = threadIdx.x / ns;
+    const int dj = CONV_X_THREADS % ns, dcr = CONV_X_THREADS / ns;
+    for (; cr < 3 * CONV_X_ROWS; cr += dcr) {
+        const int c = cr / CONV_X_ROWS, r = cr % CONV_X_ROWS;
+        if (r < nr) {
+            const float *row = rows + cr * nx;
+            const int sj = samples[j];
+            float v;
+            if (any_nan) {
+                v = conv_at(sj, nx, R, Ks, [&](int k) { return row[k]; });
+            } else {
+                float num = 0.f;
+                const int k0 = max(0, sj - R), k1 = min(nx - 1, sj + R);
+                const float *w = Ks - sj + R;
+#pragma unroll 4
+                for (int k = k0; k <= k1; ++k) num = fmaf(w[k], row[k], num);
+                v = num / dens[j];
             }
-            v = num / den;
+            out[(c * nrow + r0 + r) * ns + j] = v;
         }
-        out[(c * nrow + r0 + r) * ns + j] = v;
+        j += dj;
+        if (j >= ns) {
+            j -= ns;
+            ++cr;
+        }
     }
 }
 
@@ -806,17 +825,21 @@ __global__ void k_cg_update(long long n, float *__restrict__ g, float *__restric
         }
         return;
     }
-    __shared__ double gam;
-    if (threadIdx.x == 0) {
-        double gg = 0, dgg = 0;
-        for (int i = 0; i < np; ++i) {
-            gg += partials[2 * i];
-            dgg += partials[2 * i + 1];
-        }
-        gam = dgg / gg;
+    // the partials are copied to shared memory by the whole block, then summed in index order by
+    // two threads (gg and dgg side by side), instead of one thread's chain of global loads
+    __shared__ double sp[2 * NRB_RED_BLOCKS];
+    __shared__ double sgg, sdgg;
+    for (int i = threadIdx.x; i < 2 * np; i += blockDim.x) sp[i] = partials[i];
+    __syncthreads();
+    if (threadIdx.x == 0 || threadIdx.x == 32) {
+        const int q = threadIdx.x == 0 ? 0 : 1;
+        double sum = 0;
+        for (int i = 0; i < np; ++i) sum += sp[2 * i + q];
+        if (q == 0) sgg = sum;
+        else sdgg = sum;
     }
     __syncthreads();
-    const double gm = gam;
+    const double gm = sdgg / sgg;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         const float a1 = -g[i];
@@ -1249,7 +1272,8 @@ nrb_status launch_convolve_to_nodes(nrb_workspace *ws, const nrb_geometry *g, co
     // compulsory traffic of the whole voxel->node step: the voxel gradient once, the nodes once
     KernelTimer timer(TK_CONV, 12.0 * (double)nx * ny * nz + 12.0 * (double)nvox(g->cpp_dim), st);
     // x pass: one block per row
-    const size_t smem = ((size_t)3 * CONV_X_ROWS * nx + 2 * ws->ax[0].radius + 1) * 4;  // nx <= 2048: <= 197 KB
+    // rows | kernel taps | per-sample weight sums (nx <= 2048: <= 205 KB)
+    const size_t smem = ((size_t)3 * CONV_X_ROWS * nx + 2 * ws->ax[0].radius + 1 + nsx) * 4;
     if (smem > 227 * 1024) return fail(NRB_ERR_UNSUPPORTED, "convolution: rows and kernel exceed shared memory");
     if (smem > 48 * 1024) NRB_CUDA(cudaFuncSetAttribute(k_conv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int xblocks = (int)(((long long)ny * nz + CONV_X_ROWS - 1) / CONV_X_ROWS);
@@ -1569,14 +1593,15 @@ nrb_status launch_batch_node_stage(const std::vector<BatchPair>& hp, const Batch
     }
     NRB_TRY(gradient(d, states, st, gradient_arg));
     // x pass: shared rows for the widest reference
-    int nx = 0, R = 0;
+    int nx = 0, R = 0, nsx = 0;
     long long xb = 0;
     for (const BatchPair& b : hp) {
         nx = std::max(nx, b.rdim[0]);
         R = std::max(R, b.radius[0]);
+        nsx = std::max(nsx, b.ns[0]);
         xb += b.xblocks;
     }
-    const size_t smem = ((size_t)3 * CONV_X_ROWS * nx + 2 * R + 1) * 4;
+    const size_t smem = ((size_t)3 * CONV_X_ROWS * nx + 2 * R + 1 + nsx) * 4;
     if (smem > 227 * 1024) return fail(NRB_ERR_UNSUPPORTED, "convolution: rows and kernel exceed shared memory");
     NRB_CUDA(cudaFuncSetAttribute(k_b_conv_x, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per = 0;
