@@ -157,43 +157,6 @@ __device__ __forceinline__ void be_node_derivatives_k(int cx, int cy, int cz, co
     for (int t = 3; t < 6; ++t) der[(3 * t + k) * nc + n] = (float)(2.0 * (double)d[t]);
 }
 
-// all three components of node n at once (the batched stage's element): the same sums, each
-// component's in the same order as be_node_derivatives_k
-__device__ __forceinline__ void be_node_derivatives(int cx, int cy, int cz, const Mat34& M, const float *__restrict__ cpp,
-                                                    const BeBasis& B, float *__restrict__ der, long long n) {
-    const long long nc = (long long)cx * cy * cz;
-    const int x = (int)(n % cx);
-    const int y = (int)((n / cx) % cy);
-    const int z = (int)(n / ((long long)cx * cy));
-    float d[3][6];
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-#pragma unroll
-        for (int t = 0; t < 6; ++t) d[k][t] = 0.f;
-    int i = 0;
-    for (int c = -1; c < 2; ++c)
-        for (int b = -1; b < 2; ++b)
-            for (int a = -1; a < 2; ++a, ++i) {
-                const int X = x + a, Y = y + b, Z = z + c;
-                if (X < 0 || Y < 0 || Z < 0 || X >= cx || Y >= cy || Z >= cz) continue;
-                const long long idx = ((long long)Z * cy + Y) * cx + X;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const float v = __fsub_rn(__ldg(&cpp[k * nc + idx]), identity_pos(M, k, X, Y, Z));
-#pragma unroll
-                    for (int t = 0; t < 6; ++t) d[k][t] = __fadd_rn(d[k][t], __fmul_rn(B.v[t][i], v));
-                }
-            }
-#pragma unroll
-    for (int t = 0; t < 3; ++t)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) der[(3 * t + k) * nc + n] = d[k][t];
-#pragma unroll
-    for (int t = 3; t < 6; ++t)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) der[(3 * t + k) * nc + n] = (float)(2.0 * (double)d[k][t]);
-}
-
 // one thread per (node, component): component k = blockIdx.y
 __global__ void k_be_derivatives(int cx, int cy, int cz, Mat34 M, const float *__restrict__ cpp,
                                  BeBasis B, float *__restrict__ der) {
@@ -228,30 +191,6 @@ __device__ __forceinline__ void be_node_accumulate_k(int cx, int cy, int cz, con
                 for (int t = 0; t < 6; ++t) g = __fadd_rn(g, __fmul_rn(__ldg(&der[(3 * t + k) * nc + j]), B.v[t][a]));
             }
     grad[k * nc + n] = __fadd_rn(grad[k * nc + n], __fmul_rn(ratio, g));
-}
-
-// all three components of node n at once (the batched stage's element), each in the order of
-// be_node_accumulate_k
-__device__ __forceinline__ void be_node_accumulate(int cx, int cy, int cz, const float *__restrict__ der, const BeBasis& B,
-                                                   float ratio, float *__restrict__ grad, long long n) {
-    const long long nc = (long long)cx * cy * cz;
-    const int x = (int)(n % cx);
-    const int y = (int)((n / cx) % cy);
-    const int z = (int)(n / ((long long)cx * cy));
-    float g[3] = { 0.f, 0.f, 0.f };
-    int a = 0;
-    for (int Z = z - 1; Z < z + 2; ++Z)
-        for (int Y = y - 1; Y < y + 2; ++Y)
-            for (int X = x - 1; X < x + 2; ++X, ++a) {
-                if (X < 0 || Y < 0 || Z < 0 || X >= cx || Y >= cy || Z >= cz) continue;
-                const long long j = ((long long)Z * cy + Y) * cx + X;
-#pragma unroll
-                for (int t = 0; t < 6; ++t)
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) g[k] = __fadd_rn(g[k], __fmul_rn(__ldg(&der[(3 * t + k) * nc + j]), B.v[t][a]));
-            }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) grad[k * nc + n] = __fadd_rn(grad[k * nc + n], __fmul_rn(ratio, g[k]));
 }
 
 // one thread per (node, component): component k = blockIdx.y
@@ -508,12 +447,14 @@ __global__ void k_b_be_derivatives(const BatchPair *__restrict__ pairs, const Op
     batch_list_build(states, npairs, 1u << PH_GRAD,
                      [&](int q, int& u, int& w) {
                          const BatchPair& b = pairs[q];
-                         u = b.be_w > 0 ? (int)b.nnode : 0;
+                         u = b.be_w > 0 ? (int)(3 * b.nnode) : 0;  // one element per (component, node)
                          w = 1;
                      }, L);
-    batch_elements(L, [&](int p, long long n) {
+    batch_elements(L, [&](int p, long long e) {
         const BatchPair& P = pairs[p];
-        be_node_derivatives(P.cdim[0], P.cdim[1], P.cdim[2], P.grid_xyz, P.best, B, P.be_der, n);
+        const int k = (int)(e / P.nnode);
+        const long long n = e - k * P.nnode;
+        be_node_derivatives_k(P.cdim[0], P.cdim[1], P.cdim[2], P.grid_xyz, P.best, B, P.be_der, n, k);
     });
 }
 
@@ -523,12 +464,14 @@ __global__ void k_b_be_accumulate(const BatchPair *__restrict__ pairs, const Opt
     batch_list_build(states, npairs, 1u << PH_GRAD,
                      [&](int q, int& u, int& w) {
                          const BatchPair& b = pairs[q];
-                         u = b.be_w > 0 ? (int)b.nnode : 0;
+                         u = b.be_w > 0 ? (int)(3 * b.nnode) : 0;  // one element per (component, node)
                          w = 1;
                      }, L);
-    batch_elements(L, [&](int p, long long n) {
+    batch_elements(L, [&](int p, long long e) {
         const BatchPair& P = pairs[p];
-        be_node_accumulate(P.cdim[0], P.cdim[1], P.cdim[2], P.be_der, B, P.be_ratio, P.grad, n);
+        const int k = (int)(e / P.nnode);
+        const long long n = e - k * P.nnode;
+        be_node_accumulate_k(P.cdim[0], P.cdim[1], P.cdim[2], P.be_der, B, P.be_ratio, P.grad, n, k);
     });
 }
 
@@ -1585,7 +1528,7 @@ nrb_status launch_batch_node_stage(const std::vector<BatchPair>& hp, const Batch
     if (be) {
         NRB_CUDA(cudaEventRecord(fork, st));
         NRB_CUDA(cudaStreamWaitEvent(side, fork, 0));
-        const int g = batch_grid(hp, [](const BatchPair& b) { return b.nnode; }, 128, 16);
+        const int g = batch_grid(hp, [](const BatchPair& b) { return 3 * b.nnode; }, 128, 16);
         KernelTimer timer(TK_BE_GRADIENT, 0.0, side);
         k_b_be_derivatives<<<g, 128, 0, side>>>(d, states, np, be_basis());
         NRB_CUDA(cudaGetLastError());
@@ -1628,7 +1571,7 @@ nrb_status launch_batch_node_stage(const std::vector<BatchPair>& hp, const Batch
     if (be) {
         NRB_CUDA(cudaEventRecord(join, side));
         NRB_CUDA(cudaStreamWaitEvent(st, join, 0));
-        const int g = batch_grid(hp, [](const BatchPair& b) { return b.nnode; }, 128, 16);
+        const int g = batch_grid(hp, [](const BatchPair& b) { return 3 * b.nnode; }, 128, 16);
         KernelTimer timer2(TK_BE_GRADIENT, 0.0, st);
         k_b_be_accumulate<<<g, 128, 0, st>>>(d, states, np, be_basis());
         NRB_CUDA(cudaGetLastError());
